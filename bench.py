@@ -1,0 +1,452 @@
+"""Benchmark of the B200 PISO step: cell-steps/s of a batched workload (one JSON line on rank 0).
+
+Workloads (``--workload``):
+
+* ``batched_cavities_256`` (default): 256 independent 2D lid-driven cavities, side
+  s_i = round(exp(U(ln 32, ln 256))) (seed 6), Re_i = exp(U(ln 100, ln 5000)), viscosity 1/Re_i,
+  lid speed 1, unit box, dt_i = 0.5 h_i (CFL 0.5), 2 correctors, BiCGStab advection and CG pressure
+  solves to 1e-6 (RMS residual), FP32 fields with FP64 Krylov reductions, all simulations advanced
+  by one launch per stage and the step replayed as a CUDA graph.
+* ``lid_cavity_64``: the reference's minimal lid-driven cavity, 64x64, Re 1000, dt 0.01.
+
+A "step" is one PISO time step of every simulation in the workload; ``value`` is the whole-job
+throughput in cell-steps/s with all state resident in HBM.  ``e2e`` measures the same step through
+the public API with the state uploaded from pinned host buffers and downloaded again every step.
+``--impl reference`` times the reference algorithm's CPU restatement (the FP64 oracle; the reference
+itself has no CPU implementation of the step) on a bounded sample of the same workload.
+
+Multi-GPU (torchrun): every rank advances its own batch (seed + rank), no collective on the data
+path ("weak" scaling); timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+METRIC = "PISO cell-steps/s fwd & fwd+bwd, batched vs plain, at stated err, 1 B200"
+
+
+# ------------------------------------------------------------------------------------------ workloads
+
+def cavity_coords(n):
+    xs = np.linspace(0.0, 1.0, n + 1)
+    Y, X = np.meshgrid(xs, xs, indexing="ij")
+    return np.stack([X, Y])[None]
+
+
+def batched_cavity_params(num=256, seed=6):
+    rng = np.random.default_rng(seed)
+    sides = np.rint(np.exp(rng.uniform(np.log(32), np.log(256), num))).astype(int)
+    re = np.exp(rng.uniform(np.log(100), np.log(5000), num))
+    return sides, re
+
+
+def make_cavity_domain(n, viscosity, dtype, device="cuda"):
+    import torch
+    from pict_b200 import PISOtorch
+    dom = PISOtorch.Domain(2, torch.tensor([viscosity], dtype=dtype), name="cavity%d" % n, dtype=dtype,
+                           device=device, passiveScalarChannels=0)
+    coords = torch.tensor(cavity_coords(n), dtype=dtype, device=device).contiguous()
+    blk = dom.CreateBlock(vertexCoordinates=coords, name="cavity")
+    blk.CloseAllBoundaries()
+    blk.CloseBoundary("-y", torch.tensor([[1.0, 0.0]], dtype=dtype, device=device))
+    dom.PrepareSolve()
+    return dom
+
+
+def build_workload(name, rank=0, dtype=None):
+    import torch
+    dtype = torch.float32 if dtype is None else dtype
+    if name == "batched_cavities_256":
+        sides, re = batched_cavity_params(256, 6 + rank)
+        doms = [make_cavity_domain(int(s), 1.0 / r, dtype) for s, r in zip(sides, re)]
+        dts = [0.5 / s for s in sides]
+        return dict(domains=doms, dts=dts, sides=sides, re=re, tol=1e-6, correctors=2)
+    if name == "lid_cavity_64":
+        doms = [make_cavity_domain(64, 1e-3, dtype)]
+        return dict(domains=doms, dts=[0.01], sides=np.array([64]), re=np.array([1000.0]), tol=1e-6, correctors=2)
+    raise KeyError(name)
+
+
+# ------------------------------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index=0):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------------------------------ helpers
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def oracle_step_rate(sides, re, dts, n_sims, steps, tol=1e-6):
+    """Time the FP64 oracle PISO step on the first `n_sims` simulations (CPU, single thread)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import piso_oracle as po
+    cells = 0
+    t_total = 0.0
+    for s, r, dt in list(zip(sides, re, dts))[:n_sims]:
+        d = po.ODomain(2, 1.0 / r)
+        b = d.create_block(coords=cavity_coords(int(s)))
+        d.close_all(b)
+        d.close_boundary(b, "-y", np.array([[1.0, 0.0]]))
+        d.prepare()
+        po.piso_step(d, dt, adv_tol=tol, p_tol=tol)  # warm-up step (not timed)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            po.piso_step(d, dt, adv_tol=tol, p_tol=tol)
+        t_total += time.perf_counter() - t0
+        cells += int(s) * int(s) * steps
+    return cells / t_total, t_total, cells
+
+
+def sample_indices(sides, k):
+    """k simulations at evenly spaced size quantiles (a representative bounded sample)."""
+    order = np.argsort(sides)
+    if len(order) <= k:
+        return order
+    q = [(j + 0.5) / k for j in range(k)]
+    return order[[int(x * len(order)) for x in q]]
+
+
+def cg_algorithmic_bytes(dims, esz):
+    """Algorithmic bytes per cell and CG iteration: read K coefficients, r, p_old; write p_new, q
+    (phase 1); read x, p, q, r; write x, r (phase 2)."""
+    K = 2 * dims + 1
+    return esz * (K + 10)
+
+
+# ------------------------------------------------------------------------------------------ arms
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    w = args.workload
+    if w == "batched_cavities_256":
+        sides, re = batched_cavity_params(256, 6)
+        dts = [0.5 / s for s in sides]
+    else:
+        sides, re, dts = np.array([64]), np.array([1000.0]), [0.01]
+    # bounded sample: 4 simulations at evenly spaced size quantiles, one PISO step each per timed step
+    sel = sample_indices(sides, 4)
+    n_sample = len(sel)
+    times = []
+    cells = 0
+    for _ in range(args.steps):
+        r, t, c = oracle_step_rate(sides[sel], re[sel], [dts[i] for i in sel], n_sample, 1)
+        times.append(t)
+        cells = c
+    value = cells * len(times) / sum(times)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": w, "sample": "%d simulations at size quantiles %s, one PISO step each" % (n_sample, [int(sides[i]) for i in sel])},
+        "cpu_baseline": {"value": value, "unit": "cell-steps/s", "cores": 1, "kind": "port",
+                         "sample": "%d simulations x %d steps, FP64 NumPy/SciPy restatement" % (n_sample, args.steps)},
+        "e2e": {"value": value, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_pict(args, rank, world):
+    import torch
+    import torch.distributed as dist
+    from pict_b200.batch import BatchDomain
+    from pict_b200.engine import PISOStepper
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    wl = build_workload(args.workload, rank)
+    doms = wl["domains"]
+    batch = BatchDomain(doms, time_steps=wl["dts"])
+    st = PISOStepper(batch, time_step=float(wl["dts"][0]), corrector_steps=wl["correctors"],
+                     advection_tol=wl["tol"], pressure_tol=wl["tol"], max_iterations=5000,
+                     p_group_size=args.group_size, adv_group_size=args.group_size)
+    cells = batch.getTotalSize()
+    # warm-up (eager), then capture one step as a CUDA graph
+    for _ in range(args.warmup):
+        st.step()
+    torch.cuda.synchronize()
+    st.check()
+    if not args.no_graph:
+        st.capture(steps=1)
+    torch.cuda.synchronize()
+
+    def one_step():
+        if args.no_graph:
+            st.step()
+        else:
+            st.replay()
+
+    for _ in range(max(args.warmup, 3)):
+        one_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    sampler = ClockSampler(dev.index)
+    sampler.start()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        one_step()
+    e1.record()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    adv_infos, p_infos = st.check()
+    t = torch.tensor([ms], device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    total_cells = cells * world
+    value = total_cells * args.steps / (ms_max * 1e-3)
+
+    # roofline of the dominant kernel (persistent CG): eager pass with events around each CG launch
+    roof = roofline_pass(st, batch, args, dev)
+
+    # end-to-end through the public API with host buffers
+    e2e = e2e_pass(st, batch, args, dev, cells, world)
+
+    # accuracy: two smallest simulations, FP32 GPU vs FP64 oracle with tight solves
+    err = accuracy_check(wl, args) if (rank == 0 and not args.skip_err) else None
+
+    # CPU baseline (bounded sample, rank 0)
+    cpu = None
+    if rank == 0 and not args.skip_cpu:
+        sel = sample_indices(wl["sides"], 4)
+        n_s = len(sel)
+        rate, tt, c = oracle_step_rate(wl["sides"][sel], wl["re"][sel], [wl["dts"][i] for i in sel], n_s, 2)
+        cpu = {"value": rate, "unit": "cell-steps/s", "cores": 1, "kind": "port",
+               "sample": "sides %s x 2 PISO steps each (FP64 NumPy/SciPy restatement, %.1f s)" % (
+                   [int(wl["sides"][i]) for i in sel], tt)}
+    iters_adv = [i.usedIterations for i in adv_infos]
+    iters_p = [[i.usedIterations for i in p] for p in p_infos]
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "simulations": len(doms), "cells_per_gpu": cells,
+                       "pass": "forward", "solver_tol": wl["tol"], "correctors": wl["correctors"],
+                       "cuda_graph": not args.no_graph, "l2": "working set > L2 (126 MB), no flush",
+                       "parallelism": "independent batches per GPU" if world > 1 else "single GPU"},
+            "clocks": clocks,
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": st.kernels_per_step() * args.steps,
+            "err": err,
+            "solver_iterations": {"advection_max": int(max(iters_adv)), "advection_mean": float(np.mean(iters_adv)),
+                                  "pressure_max": [int(max(p)) for p in iters_p],
+                                  "pressure_mean": [float(np.mean(p)) for p in iters_p]},
+        }
+        print(json.dumps(line), flush=True)
+
+
+def roofline_pass(st, batch, args, dev):
+    import torch
+    from pict_b200 import PISOtorch as P
+    esz = 4 if batch.getDtype() == torch.float32 else 8
+    events = []
+    steps = max(1, min(args.steps, 5))
+    # snapshot the state so the extra steps do not change what e2e sees
+    for _ in range(steps):
+        evs = st.step_with_events()
+        events.append(evs)
+    torch.cuda.synchronize()
+    cg_ms = []
+    cg_bytes = []
+    per_cell = cg_algorithmic_bytes(batch.getSpatialDims(), esz)
+    sim_cells = batch._sim_cells.cpu().numpy()
+    n_s = np.diff(sim_cells)
+    for evs in events:
+        for (a, b, info) in evs["cg"]:
+            cg_ms.append(a.elapsed_time(b))
+            its = np.array([i.usedIterations for i in P.decode_infos(info)])
+            # iterations + the initial pass over the cells
+            cg_bytes.append(float(np.sum((its + 1) * n_s) * per_cell))
+    ms = float(np.mean(cg_ms))
+    byt = float(np.mean(cg_bytes))
+    achieved = byt / (ms * 1e-3) / 1e9
+    peak, kind = measured_peaks()
+    return {"kernel": "k_cg (persistent CG, pressure solve)", "bound": "hbm", "achieved": achieved, "peak": peak,
+            "peak_kind": kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+            "algorithmic_bytes_per_launch": byt, "avg_launch_ms": ms,
+            "bytes_per_cell_iteration": per_cell}
+
+
+def e2e_pass(st, batch, args, dev, cells, world):
+    import torch
+    blocks = batch.getBlocks()
+    host_v = [torch.empty(b.velocity.shape, dtype=b.velocity.dtype, pin_memory=True) for b in blocks]
+    host_p = [torch.empty(b.pressure.shape, dtype=b.pressure.dtype, pin_memory=True) for b in blocks]
+    for hv, hp, b in zip(host_v, host_p, blocks):
+        hv.copy_(b.velocity)
+        hp.copy_(b.pressure)
+    torch.cuda.synchronize()
+    h2d = sum(h.numel() * h.element_size() for h in host_v + host_p)
+    steps = max(1, min(args.steps, 20))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        for hv, hp, b in zip(host_v, host_p, blocks):
+            b.velocity.copy_(hv, non_blocking=True)
+            b.pressure.copy_(hp, non_blocking=True)
+        if args.no_graph:
+            st.step()
+        else:
+            st.replay()
+        for hv, hp, b in zip(host_v, host_p, blocks):
+            hv.copy_(b.velocity, non_blocking=True)
+            hp.copy_(b.pressure, non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    return {"value": cells * world * steps / (ms * 1e-3), "unit": "cell-steps/s", "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": h2d, "steps": steps}
+
+
+def accuracy_check(wl, args):
+    """Relative error of the FP32 batched step against the FP64 oracle (tight solves) on the two
+    smallest simulations after 10 steps."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import piso_oracle as po
+    from pict_b200.batch import BatchDomain
+    from pict_b200.engine import PISOStepper
+    order = np.argsort(wl["sides"])[:2]
+    doms = [make_cavity_domain(int(wl["sides"][i]), 1.0 / wl["re"][i], torch.float32) for i in order]
+    dts = [wl["dts"][i] for i in order]
+    b = BatchDomain(doms, time_steps=dts)
+    st = PISOStepper(b, time_step=dts[0], advection_tol=wl["tol"], pressure_tol=wl["tol"])
+    steps = 10
+    for _ in range(steps):
+        st.step()
+    st.check()
+    out = {"steps": steps, "sims": [int(wl["sides"][i]) for i in order]}
+    eu, ep = [], []
+    for k, i in enumerate(order):
+        s = int(wl["sides"][i])
+        d = po.ODomain(2, 1.0 / wl["re"][i])
+        bi = d.create_block(coords=cavity_coords(s))
+        d.close_all(bi)
+        d.close_boundary(bi, "-y", np.array([[1.0, 0.0]]))
+        d.prepare()
+        for _ in range(steps):
+            po.piso_step(d, dts[k], adv_tol=1e-12, p_tol=1e-12)
+        u = doms[k].getBlock(0).velocity.double().cpu().numpy().reshape(2, -1)
+        p = doms[k].getBlock(0).pressure.double().cpu().numpy().reshape(-1)
+        ur, pr = d.velocity_global(), d.pressure_global()
+        eu.append(float(np.abs(u - ur).max() / np.abs(ur).max()))
+        ep.append(float(np.abs(p - pr).max() / np.abs(pr).max()))
+    out["velocity_rel_max"] = max(eu)
+    out["pressure_rel_max"] = max(ep)
+    out["reference"] = "FP64 oracle, solver tol 1e-12"
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="pict", choices=["pict", "reference"])
+    ap.add_argument("--workload", default="batched_cavities_256", choices=["batched_cavities_256", "lid_cavity_64"])
+    ap.add_argument("--group-size", type=int, default=0)
+    ap.add_argument("--no-graph", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-err", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_pict(args, rank, world)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,220 @@
+/*
+ * pict_b200.h -- C ABI of the B200-native PISO step (libpict_b200.so).
+ *
+ * This is the drop-in boundary of the build: plain C structs, raw device
+ * pointers and sizes, no torch types.  The Python package ``pict_b200``
+ * (module ``pict_b200.PISOtorch``) binds these entry points with ctypes and
+ * mirrors the reference's pybind11 ``PISOtorch`` operator surface on top of
+ * them.  Each entry point below cites the reference interface it replaces
+ * (paths relative to the PICT repository; "PISOtorch.cpp" is
+ * extensions/PISOtorch.cpp, "kernel.cu" is
+ * extensions/PISO_multiblock_cuda_kernel.cu).
+ *
+ * Conventions
+ *  - Every compute entry point is stream-ordered on the given stream, performs
+ *    no host synchronisation and no device allocation, and returns a
+ *    pict_status_t (PICT_OK == 0).  The last error message is available from
+ *    pict_last_error().
+ *  - Scalars use the domain dtype (PICT_F32 or PICT_F64); the Krylov inner
+ *    products, norms and convergence tests are always accumulated in FP64.
+ *  - Faces are indexed [-x,+x,-y,+y,-z,+z] = 0..5; axis = face>>1,
+ *    upper = face&1.  Cells are flattened x-fastest per block; global vectors
+ *    concatenate the blocks; vector fields are component-major [D][N].
+ *  - System matrices are structured stencils: coef[K][N], K = 2D+1, in the
+ *    order [diag,-x,+x,-y,+y,-z,+z]; faces on fixed boundaries hold 0.
+ *  - A "system" (sim) is an independent simulation inside a batched domain;
+ *    blocks of one system are contiguous and systems never connect.
+ */
+#ifndef PICT_B200_H
+#define PICT_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t pict_status_t;
+#define PICT_OK 0
+#define PICT_ERR_ARG 1        /* invalid argument or size */
+#define PICT_ERR_CUDA 2       /* CUDA launch/runtime error */
+#define PICT_ERR_UNSUPPORTED 3
+#define PICT_ERR_NO_DEVICE 4
+
+#define PICT_F32 0
+#define PICT_F64 1
+
+#define PICT_FACE_FIXED 0
+#define PICT_FACE_PERIODIC 1
+#define PICT_FACE_CONNECTED 2
+
+#define PICT_MAX_BLOCK_FACES 6
+
+/* One block face (BoundaryGPU, domain_structs_gpu.h:253-263). */
+typedef struct pict_face {
+    int32_t type;          /* PICT_FACE_* */
+    int32_t conn_block;    /* connected: index of the other block */
+    int32_t conn_axes[3];  /* connected: ConnectedBoundary::axes (domain_structs.h:329-338) */
+    int32_t vel_static;    /* fixed: 1 if velocity is a static [D] vector */
+    const void* velocity;  /* fixed: boundary velocity [D] or [D][face cells] (device) */
+    const void* transform; /* fixed: boundary transform [face cells][2D^2+1] or NULL */
+    void* velocity_grad;   /* fixed: gradient of velocity (adjoint), same layout, or NULL */
+} pict_face_t;
+
+/* One structured block (BlockGPU, domain_structs_gpu.h:266-305). */
+typedef struct pict_block {
+    int32_t size[3];          /* x, y, z cells (1 for unused axes) */
+    int32_t offset;           /* first global cell index of this block */
+    int32_t sim;              /* system index */
+    int32_t viscosity_static; /* 1: viscosity is [1], 0: [cells] */
+    int32_t source_static;    /* 1: source is [D], 0: [D][cells] */
+    int32_t pad0;
+    void* velocity;           /* [D][cells] block velocity u^n (device) */
+    void* pressure;           /* [cells] block pressure (device) */
+    const void* transform;    /* [cells][2D^2+1] (M, Minv, det) or NULL */
+    const void* viscosity;    /* NULL (use system viscosity), [1] or [cells] */
+    const void* source;       /* NULL, [D] or [D][cells] velocity source */
+    void* velocity_grad;      /* adjoint of velocity or NULL */
+    void* pressure_grad;      /* adjoint of pressure or NULL */
+    void* viscosity_grad;     /* adjoint of block viscosity or NULL */
+    void* source_grad;        /* adjoint of velocity source or NULL */
+    pict_face_t face[PICT_MAX_BLOCK_FACES];
+} pict_block_t;
+
+/* A (possibly batched) domain.  All pointers are device pointers unless noted.
+ * Mirrors DomainGPU (domain_structs_gpu.h:307-370) with stencil storage. */
+typedef struct pict_domain {
+    int32_t dims;
+    int32_t num_blocks;
+    int32_t num_cells;        /* N, all systems */
+    int32_t num_sims;
+    int32_t dtype;            /* PICT_F32 / PICT_F64 */
+    int32_t max_sim_cells;    /* host hint: largest system */
+    const pict_block_t* blocks;    /* [num_blocks] block table (device copy) */
+    const int32_t* nbr;            /* [2D][N] neighbour cell across each face, -1 on fixed faces */
+    const int32_t* cell_block;     /* [N] block index of each cell */
+    const int32_t* sim_cells;      /* [num_sims+1] cell range of each system */
+    const int32_t* sim_blocks;     /* [num_sims+1] block range of each system */
+    const void* sim_viscosity;     /* [num_sims] domain viscosity per system */
+    const void* sim_dt;            /* [num_sims] time step per system, or NULL (use the scalar argument) */
+    void* C;                  /* [K][N] advection matrix */
+    void* A;                  /* [N] its diagonal */
+    void* P;                  /* [K][N] pressure matrix */
+    void* velocity_rhs;       /* [D][N] */
+    void* velocity_result;    /* [D][N] */
+    void* pressure_rhs;       /* [D][N] (H/A vector field) */
+    void* pressure_rhs_div;   /* [N] */
+    void* pressure_result;    /* [N] */
+} pict_domain_t;
+
+/* Per right-hand-side solver report (LinearSolverResultInfo, bicgstab_solver.h:20-25). */
+typedef struct pict_solve_info {
+    double final_residual;
+    int32_t used_iterations;
+    int32_t converged;
+    int32_t finite;
+    int32_t status;           /* 0 ok, 1 barrier timeout, 2 not started */
+} pict_solve_info_t;
+
+#define PICT_CONV_NORM2 0
+#define PICT_CONV_NORM2_NORMALIZED 1
+#define PICT_CONV_ABS_SUM 2
+#define PICT_CONV_ABS_MEAN 3
+#define PICT_CONV_ABS_MAX 4
+
+/* Parameters of a linear solve (PISOtorch.SolveLinear arguments, PISOtorch.cpp:559-563). */
+typedef struct pict_solve_params {
+    int32_t max_iterations;
+    int32_t use_bicg;          /* 1: BiCGStab, 0: CG */
+    int32_t nrhs;              /* right-hand sides per system sharing the matrix (BiCG: D components) */
+    int32_t x_is_zero;         /* 1: skip the initial A*x (x must hold zeros) */
+    int32_t transpose;         /* solve with A^T (adjoint solves) */
+    int32_t convergence;       /* PICT_CONV_*; only NORM2 and NORM2_NORMALIZED are supported */
+    int32_t group_size;        /* CTAs cooperating on one system (0: automatic) */
+    int32_t threads;           /* threads per CTA (0: automatic) */
+    int32_t subtract_mean;     /* 1: x -= mean(x) per system after the solve (sim.py:1243-1244) */
+    int32_t write_block_pressure; /* 1: also copy x into the blocks' pressure (CopyPressureResultToBlocks) */
+    double tolerance;
+} pict_solve_params_t;
+
+/* ---------------- version / library ---------------- */
+const char* pict_version(void);
+const char* pict_last_error(void);
+int32_t pict_sizeof_block(void);   /* sizeof(pict_block_t), for binding checks */
+int32_t pict_sizeof_domain(void);  /* sizeof(pict_domain_t) */
+
+/* ---------------- host-side topology (no GPU needed) ----------------
+ * Replaces the per-thread neighbour resolution of the reference
+ * (resolveNeighborCell / computeConnectedPos, kernel.cu:326-345, 432-477) and
+ * the connection checks of Domain::PrepareSolve (domain_structs.cpp:2554-2676)
+ * with a precomputed table.  host_blocks is a HOST array.
+ * nbr_out: [2*dims][num_cells], cell_block_out: [num_cells] (host buffers). */
+pict_status_t pict_build_topology(const pict_block_t* host_blocks, int32_t num_blocks, int32_t dims,
+                                  int32_t num_cells, int32_t* nbr_out, int32_t* cell_block_out);
+
+/* ---------------- assembly (forward) ---------------- */
+/* SetupAdvectionMatrix (PISOtorch.cpp:531-533 -> kernel.cu:4510 PISO_build_matrix):
+ * writes C and A from the blocks' velocity.  non_ortho_flags must be 0. */
+pict_status_t pict_setup_advection_matrix(const pict_domain_t* dom, double dt, int32_t non_ortho_flags,
+                                          void* stream);
+/* SetupAdvectionVelocity (PISOtorch.cpp:537-539 -> kernel.cu:4677 kPISO_build_advection_RHS). */
+pict_status_t pict_setup_advection_velocity(const pict_domain_t* dom, double dt, int32_t non_ortho_flags,
+                                            int32_t apply_pressure_gradient, void* stream);
+/* Fused SetupAdvectionMatrix + SetupAdvectionVelocity in one pass over the cells. */
+pict_status_t pict_setup_advection(const pict_domain_t* dom, double dt, void* stream);
+/* SetupPressureMatrix (PISOtorch.cpp:544-546 -> kernel.cu:4797 PISO_build_pressure_matrix). */
+pict_status_t pict_setup_pressure_matrix(const pict_domain_t* dom, int32_t non_ortho_flags, void* stream);
+/* SetupPressureRHS (PISOtorch.cpp:547-549 -> kernel.cu:5121 PISO_build_pressure_rhs
+ * + kernel.cu:5374 k_computePressureRHSdivergenceFromFlux). */
+pict_status_t pict_setup_pressure_rhs(const pict_domain_t* dom, double dt, int32_t non_ortho_flags,
+                                      int32_t time_step_norm, void* stream);
+/* SetupPressureRHSdiv (PISOtorch.cpp:550-552 -> kernel.cu:5374). */
+pict_status_t pict_setup_pressure_rhs_div(const pict_domain_t* dom, double dt, int32_t non_ortho_flags,
+                                          int32_t time_step_norm, void* stream);
+/* SetupPressureCorrection (PISOtorch.cpp:541-543): matrix + RHS + div, matrix and RHS fused. */
+pict_status_t pict_setup_pressure_correction(const pict_domain_t* dom, double dt, int32_t non_ortho_flags,
+                                             int32_t time_step_norm, void* stream);
+/* CorrectVelocity (PISOtorch.cpp:553-555 -> kernel.cu:6163, version 1 "FD").
+ * write_block_velocity=1 additionally stores the result in the blocks' velocity
+ * (CopyVelocityResultToBlocks fused). */
+pict_status_t pict_correct_velocity(const pict_domain_t* dom, double dt, int32_t version,
+                                    int32_t time_step_norm, int32_t write_block_velocity, void* stream);
+/* Copy{Velocity,Pressure}Result{To,From}Blocks (PISOtorch.cpp:561-566 -> kernel.cu:6543-6733). */
+pict_status_t pict_copy_velocity_result_to_blocks(const pict_domain_t* dom, void* stream);
+pict_status_t pict_copy_velocity_result_from_blocks(const pict_domain_t* dom, void* stream);
+pict_status_t pict_copy_pressure_result_to_blocks(const pict_domain_t* dom, void* stream);
+pict_status_t pict_copy_pressure_result_from_blocks(const pict_domain_t* dom, void* stream);
+/* ComputeVelocityDivergence (PISOtorch.cpp:556 -> kernel.cu:6333): div of the blocks' velocity, out [N]. */
+pict_status_t pict_velocity_divergence(const pict_domain_t* dom, void* out, void* stream);
+
+/* ---------------- linear solves ---------------- */
+/* Bytes of scratch memory a solve needs (vectors, reduction partials, barriers). */
+int64_t pict_solve_workspace_bytes(const pict_domain_t* dom, const pict_solve_params_t* params);
+/* SolveLinear (PISOtorch.cpp:559-563 -> kernel.cu:7070 -> cgSolveGPU cg.cu:114 / bicgstabSolveGPU bicg.cu:47)
+ * on a stencil matrix coef [K][N] of the domain's topology.  rhs, x: [nrhs][N].
+ * info_out: device array [num_sims][nrhs] of pict_solve_info_t.  workspace: device memory of
+ * pict_solve_workspace_bytes() bytes. */
+pict_status_t pict_solve(const pict_domain_t* dom, const void* coef, const void* rhs, void* x,
+                         const pict_solve_params_t* params, void* info_out, void* workspace,
+                         int64_t workspace_bytes, void* stream);
+
+/* ---------------- matrix export / utilities ---------------- */
+/* CSR materialisation of a stencil matrix in the reference's row layout (rows sorted by
+ * column, kernel.cu:3846-3860).  row_out [N+1] must be computed first by pict_csr_row_ptr. */
+pict_status_t pict_csr_row_ptr(const pict_domain_t* dom, int32_t* row_out, void* stream);
+pict_status_t pict_stencil_to_csr(const pict_domain_t* dom, const void* coef, const int32_t* row,
+                                  void* value_out, int32_t* index_out, void* stream);
+pict_status_t pict_csr_to_stencil(const pict_domain_t* dom, const void* value, const int32_t* row,
+                                  const int32_t* index, void* coef_out, void* stream);
+/* CoordsToTransforms / CoordsToFaceTransforms (grid_gen.cu:341-375, 468-514). coords [D][(z+1)][y+1][x+1]. */
+pict_status_t pict_coords_to_transforms(const void* coords, int32_t dims, const int32_t* size_xyz,
+                                        int32_t dtype, void* out, void* stream);
+pict_status_t pict_coords_to_face_transforms(const void* coords, int32_t dims, const int32_t* size_xyz,
+                                             int32_t dtype, void* out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PICT_B200_H */

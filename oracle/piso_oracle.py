@@ -1,0 +1,892 @@
+"""FP64 CPU oracle of PICT's PISO time step (test infrastructure only).
+
+This module is the checker for the CUDA implementation in ``pict_b200``: a
+NumPy / SciPy-sparse restatement of the reference discretisation for the
+orthogonal PISO path (``non_orthogonal=False``), on single- and multi-block
+structured grids with fixed (Dirichlet), periodic and connected boundaries and
+optional per-cell coordinate transforms.  It is imported only by ``tests/``,
+``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py``; the
+product path never calls it.
+
+Every function cites the reference source it restates (paths relative to the
+PICT repository):
+
+* kernel.cu   = extensions/PISO_multiblock_cuda_kernel.cu
+* cg.cu       = extensions/cg_solver_kernel.cu
+* bicg.cu     = extensions/bicgstab_solver_kernel.cu
+* grid_gen.cu = extensions/grid_gen.cu
+* sim.py      = PISOtorch_simulation.py
+
+Layout conventions (identical to the reference):
+
+* faces / boundaries are indexed ``[-x, +x, -y, +y, -z, +z]`` = 0..2D-1,
+  axis = face >> 1, upper side = face & 1 (kernel.cu:196-225);
+* cells of a block are flattened x-fastest; global vectors concatenate the
+  blocks (``globalOffset``) and vector fields are component-major
+  ``[D][N]`` (kernel.cu:166-172);
+* stencil coefficients are stored as ``coef[K][N]`` with K = 2D+1 in the order
+  ``[diag, -x, +x, -y, +y, -z, +z]`` (the reference's ``rowValues`` order,
+  kernel.cu:3693-3694, before its CSR sort).
+
+Pinning: golden fixtures produced by the reference's own CUDA build
+(``tests/golden/``, generated by ``tests/golden/make_ref_fixtures.py``) are
+compared against this oracle in ``tests/test_oracle_golden.py``.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import numpy as np
+import scipy.sparse as sp
+
+FACE_NAMES = ["-x", "+x", "-y", "+y", "-z", "+z"]
+AXIS_NAMES = ["x", "y", "z"]
+
+
+def face_index(face) -> int:
+    """Face string or index -> index (domain_structs.cpp:134-155)."""
+    if isinstance(face, str):
+        return FACE_NAMES.index(face)
+    return int(face)
+
+
+def axis_index(axis) -> int:
+    if isinstance(axis, str):
+        return AXIS_NAMES.index(axis)
+    return int(axis)
+
+
+# --------------------------------------------------------------------------
+# transforms from vertex coordinates (grid_gen.cu)
+# --------------------------------------------------------------------------
+
+def _det_inv(M):
+    """Determinant and inverse of a stack of DxD matrices."""
+    det = np.linalg.det(M)
+    inv = np.linalg.inv(M)
+    return det, inv
+
+
+def coords_to_transforms(coords: np.ndarray) -> np.ndarray:
+    """Cell transforms from vertex coordinates, grid_gen.cu:284-339.
+
+    coords: [1, D, (z+1), y+1, x+1] -> transforms [1, (z), y, x, 2D^2+1] with
+    per cell M (row-major, M[i][k] = d x_i / d xi_k from the difference of the
+    opposite face centres), Minv and det(M).
+    """
+    c = np.asarray(coords, dtype=np.float64)
+    D = c.shape[1]
+    v = c[0]  # [D, (z+1), y+1, x+1]
+    # face centres: average of the 2^(D-1) vertices of each face
+    sl = lambda lo_hi, ax: tuple(
+        (slice(1, None) if lo_hi else slice(0, -1)) if a == ax else slice(None) for a in range(D))
+    # move to cell-centred index space with explicit loops over the vertex corners
+    cell_shape = tuple(s - 1 for s in v.shape[1:])
+    M = np.zeros(cell_shape + (D, D))
+    for k in range(D):  # direction
+        # numpy axis of direction k in the spatial array (zyx order)
+        nax = D - 1 - k
+        upper = np.zeros((D,) + cell_shape)
+        lower = np.zeros((D,) + cell_shape)
+        for corner in range(1 << D):
+            idx = []
+            for n in range(D):  # numpy spatial axis n -> direction D-1-n
+                kk = D - 1 - n
+                bit = (corner >> kk) & 1
+                idx.append(slice(1, None) if bit else slice(0, -1))
+            val = v[(slice(None),) + tuple(idx)]
+            if (corner >> k) & 1:
+                upper += val
+            else:
+                lower += val
+        norm = 1.0 / (1 << (D - 1))
+        diff = (upper - lower) * norm  # [D(comp), cells]
+        for i in range(D):
+            M[..., i, k] = diff[i]
+    det, inv = _det_inv(M)
+    T = np.concatenate([M.reshape(cell_shape + (D * D,)), inv.reshape(cell_shape + (D * D,)),
+                        det[..., None]], axis=-1)
+    return T[None]
+
+
+def coords_to_face_transforms(coords: np.ndarray) -> np.ndarray:
+    """Face transforms (staggered), grid_gen.cu:383-466.
+
+    Returns [1, D, (z+1), y+1, x+1, 2D^2+1]; channel ``dim`` holds the transform
+    of the lower face of cell ``pos`` along ``dim``.  Entries whose tangential
+    index is the last vertex index are left zero (grid_gen.cu:392-397).
+    """
+    c = np.asarray(coords, dtype=np.float64)
+    D = c.shape[1]
+    v = c[0]
+    vshape = v.shape[1:]  # zyx vertex grid
+    size = np.array(list(reversed(vshape)))  # x,y,z vertex counts
+    n = int(np.prod(vshape))
+    grids = np.meshgrid(*[np.arange(s) for s in vshape], indexing="ij")
+    P = np.stack([grids[D - 1 - a].reshape(-1) for a in range(D)], 1)  # (n, D) xyz
+    nfv = 1 << (D - 1)
+    nev = 1 << max(D - 2, 0)
+
+    def gather(Q):
+        Qc = np.clip(Q, 0, size - 1)
+        idx = tuple(Qc[:, D - 1 - m] for m in range(D))
+        return v[(slice(None),) + idx].T  # (n, D comp)
+
+    out = np.zeros((D, n, 2 * D * D + 1))
+    for dim in range(D):
+        valid = np.ones(n, dtype=bool)
+        for i in range(1, D):
+            t_ax = (dim + i) % D
+            valid &= P[:, t_ax] != size[t_ax] - 1
+        t = np.zeros((n, D, D))
+        norm_w = np.full(n, 0.5)
+        for is_upper in range(2):
+            sign = 2 * is_upper - 1
+            at_b = (P[:, dim] == size[dim] - 1) if is_upper else (P[:, dim] == 0)
+            F = P.copy()
+            F[:, dim] += np.where(at_b, 0, sign)
+            norm_w = np.where(at_b, 1.0, norm_w)
+            for vi in range(nfv):
+                Vp = F.copy()
+                for i in range(1, D):
+                    Vp[:, (dim + i) % D] += 1 if (vi & i) != 0 else 0
+                t[:, :, dim] += gather(Vp) * sign
+        t[:, :, dim] *= (norm_w / nfv)[:, None]
+        for k in range(1, D):
+            tdim = (dim + k) % D
+            for vi in range(nfv):
+                Vp = P.copy()
+                for i in range(1, D):
+                    Vp[:, (dim + i) % D] += 1 if (vi & i) != 0 else 0
+                tsign = 1.0 if (vi & k) else -1.0
+                t[:, :, tdim] += gather(Vp) * tsign
+            t[:, :, tdim] *= 1.0 / nev
+        tv = t[valid]
+        det = np.linalg.det(tv)
+        inv = np.linalg.inv(tv)
+        out[dim, valid] = np.concatenate([tv.reshape(-1, D * D), inv.reshape(-1, D * D), det[:, None]], 1)
+    return out.reshape((1, D) + tuple(vshape) + (2 * D * D + 1,))
+
+
+def boundary_transform_from_face_transforms(face_T: np.ndarray, face: int) -> np.ndarray:
+    """Slice of the face transforms on a block face, domain_structs.cpp:1809-1835.
+
+    face_T: [1, D, (z+1), y+1, x+1, T] -> [1, (z'), y', x', T] with the face axis of size 1.
+    """
+    D = face_T.shape[1]
+    axis = face >> 1
+    upper = face & 1
+    idx = [slice(None), axis]
+    for dim in range(D - 1, -1, -1):
+        if dim == axis:
+            idx.append(slice(-1, None) if upper else slice(0, 1))
+        else:
+            idx.append(slice(0, -1))
+    idx.append(slice(None))
+    return np.ascontiguousarray(face_T[tuple(idx)])
+
+
+# --------------------------------------------------------------------------
+# domain model
+# --------------------------------------------------------------------------
+
+@dataclass
+class OBoundary:
+    kind: str  # 'fixed' | 'periodic' | 'connected'
+    velocity: Optional[np.ndarray] = None  # fixed: [1,D] static or [1,D,face zyx]
+    transform: Optional[np.ndarray] = None  # fixed: [1, face zyx, T]
+    block: int = -1  # connected: other block index
+    axes: Optional[List[int]] = None  # connected: axes as in ConnectedBoundary (domain_structs.h:329-338)
+
+
+@dataclass
+class OBlock:
+    size: List[int]  # x,y,z (len D)
+    velocity: np.ndarray  # [1, D, zyx]
+    pressure: np.ndarray  # [1, 1, zyx]
+    transform: Optional[np.ndarray] = None  # [1, zyx, T]
+    face_transform: Optional[np.ndarray] = None
+    viscosity: Optional[np.ndarray] = None  # None, [1] static, or [1,1,zyx]
+    source: Optional[np.ndarray] = None  # None, [1,D] static, or [1,D,zyx]
+    boundaries: List[OBoundary] = field(default_factory=list)
+
+    @property
+    def ncells(self):
+        return int(np.prod(self.size))
+
+
+class ODomain:
+    """Host model of a PICT domain (domain_structs.h:563-787), FP64."""
+
+    def __init__(self, dims: int, viscosity: float):
+        self.dims = dims
+        self.viscosity = float(viscosity)
+        self.blocks: List[OBlock] = []
+
+    # ---- construction, mirroring Domain::CreateBlock / Block::* ----
+    def create_block(self, size=None, velocity=None, pressure=None, coords=None):
+        D = self.dims
+        if velocity is not None:
+            velocity = np.asarray(velocity, dtype=np.float64)
+            zyx = velocity.shape[2:]
+        elif coords is not None:
+            zyx = tuple(s - 1 for s in np.asarray(coords).shape[2:])
+        else:
+            zyx = tuple(reversed(size))
+        size_xyz = list(reversed(zyx))
+        if velocity is None:
+            velocity = np.zeros((1, D) + tuple(zyx))
+        if pressure is None:
+            pressure = np.zeros((1, 1) + tuple(zyx))
+        b = OBlock(size=size_xyz, velocity=np.array(velocity, dtype=np.float64),
+                   pressure=np.array(pressure, dtype=np.float64))
+        b.boundaries = [OBoundary("periodic") for _ in range(2 * D)]
+        if coords is not None:
+            b.transform = coords_to_transforms(coords)
+            b.face_transform = coords_to_face_transforms(coords)
+        self.blocks.append(b)
+        return len(self.blocks) - 1
+
+    def _fixed(self, bi, face, velocity=None):
+        b = self.blocks[bi]
+        D = self.dims
+        vel = np.zeros((1, D)) if velocity is None else np.asarray(velocity, dtype=np.float64)
+        tr = None
+        if b.face_transform is not None:
+            tr = boundary_transform_from_face_transforms(b.face_transform, face)
+        b.boundaries[face] = OBoundary("fixed", velocity=vel, transform=tr)
+
+    def _close_connected(self, bi, face):
+        """Block::CloseConnectedBoudary with useFixed=True, domain_structs.cpp:1773-1807."""
+        bnd = self.blocks[bi].boundaries[face]
+        if bnd.kind == "connected":
+            self._fixed(bnd.block, bnd.axes[0])
+        elif bnd.kind == "periodic":
+            self._fixed(bi, face ^ 1)
+
+    def close_boundary(self, bi, face, velocity=None):
+        """Block::CloseBoundary(face, velocity), domain_structs.cpp:1979-1986."""
+        face = face_index(face)
+        self._close_connected(bi, face)
+        self._fixed(bi, face, velocity)
+
+    def close_all(self, bi):
+        for f in range(2 * self.dims):
+            self.close_boundary(bi, f)
+
+    def make_periodic(self, bi, axis):
+        """Block::MakePeriodic, domain_structs.cpp:1936-1955."""
+        axis = axis_index(axis)
+        lo, hi = axis << 1, (axis << 1) | 1
+        b = self.blocks[bi]
+        if not (b.boundaries[lo].kind == "periodic" and b.boundaries[hi].kind == "periodic"):
+            if b.boundaries[lo].kind == "connected":
+                self._close_connected(bi, lo)
+            if b.boundaries[hi].kind == "connected":
+                self._close_connected(bi, hi)
+            b.boundaries[lo] = OBoundary("periodic")
+            b.boundaries[hi] = OBoundary("periodic")
+
+    def connect(self, b1, face1, b2, face2, axis1=-1, axis2=-1):
+        """Block::ConnectBlock -> ConnectBlocks, domain_structs.cpp:1064-1097, 1924-1930."""
+        face1, face2 = face_index(face1), face_index(face2)
+        axis1 = face_index(axis1) if axis1 != -1 else -1
+        axis2 = face_index(axis2) if axis2 != -1 else -1
+        self._close_connected(b1, face1)
+        self._close_connected(b2, face2)
+        D = self.dims
+        axes1 = [face2]
+        axes2 = [face1]
+        if D > 1:
+            axes1.append(axis1)
+            f1d, f2d = face1 >> 1, face2 >> 1
+            swapped = False
+            if D == 2 or (axis1 >> 1) == (f2d + 1) % D:
+                axes2.append((((f1d + 1) % D) << 1) | (axis1 & 1))
+            else:
+                assert (axis2 >> 1) == (f2d + 1) % D, "Invalid connection."
+                axes2.append((((f1d + 2) % D) << 1) | (axis2 & 1))
+                swapped = True
+            if D > 2:
+                axes1.append(axis2)
+                if not swapped:
+                    axes2.append((((f1d + 2) % D) << 1) | (axis2 & 1))
+                else:
+                    axes2.append((((f1d + 1) % D) << 1) | (axis1 & 1))
+        self.blocks[b1].boundaries[face1] = OBoundary("connected", block=b2, axes=axes1)
+        self.blocks[b2].boundaries[face2] = OBoundary("connected", block=b1, axes=axes2)
+
+    # ---- topology ----
+    def prepare(self):
+        """Global offsets and per-cell neighbour tables (Domain::PrepareSolve, domain_structs.cpp:2554-2676;
+        neighbour resolution kernel.cu:326-345, 432-477)."""
+        D = self.dims
+        self.offsets = []
+        n = 0
+        for b in self.blocks:
+            self.offsets.append(n)
+            n += b.ncells
+        self.N = n
+        N = n
+        self.blk = np.zeros(N, dtype=np.int64)
+        self.loc = np.zeros(N, dtype=np.int64)
+        self.pos = np.zeros((N, 3), dtype=np.int64)
+        for bi, b in enumerate(self.blocks):
+            o = self.offsets[bi]
+            nb = b.ncells
+            l = np.arange(nb)
+            sx = b.size[0]
+            sy = b.size[1] if D > 1 else 1
+            self.blk[o:o + nb] = bi
+            self.loc[o:o + nb] = l
+            self.pos[o:o + nb, 0] = l % sx
+            self.pos[o:o + nb, 1] = (l // sx) % sy
+            self.pos[o:o + nb, 2] = l // (sx * sy)
+        K = 2 * D
+        self.nb = np.full((K, N), -1, dtype=np.int64)  # neighbour global index, -1 for fixed
+        self.fixed = np.zeros((K, N), dtype=bool)
+        self.ncomp = np.zeros((K, N), dtype=np.int64)  # component used at the neighbour
+        self.flip = np.ones((K, N))  # flux sign flip across connections
+        for f in range(K):
+            a = f >> 1
+            up = f & 1
+            for bi, b in enumerate(self.blocks):
+                o = self.offsets[bi]
+                sl = slice(o, o + b.ncells)
+                p = self.pos[sl]
+                stride = [1, b.size[0], b.size[0] * (b.size[1] if D > 1 else 1)]
+                at = (p[:, a] == (b.size[a] - 1)) if up else (p[:, a] == 0)
+                gi = np.arange(o, o + b.ncells)
+                nbv = gi + (stride[a] if up else -stride[a])
+                ncomp = np.full(b.ncells, a)
+                flip = np.ones(b.ncells)
+                fixed = np.zeros(b.ncells, dtype=bool)
+                bnd = b.boundaries[f]
+                if bnd.kind == "fixed":
+                    nbv = np.where(at, -1, nbv)
+                    fixed = at.copy()
+                elif bnd.kind == "periodic":
+                    q = p.copy()
+                    q[:, a] = 0 if up else b.size[a] - 1
+                    wrap = o + q[:, 0] + stride[1] * q[:, 1] + stride[2] * q[:, 2]
+                    nbv = np.where(at, wrap, nbv)
+                elif bnd.kind == "connected":
+                    ob = self.blocks[bnd.block]
+                    oo = self.offsets[bnd.block]
+                    ostride = [1, ob.size[0], ob.size[0] * (ob.size[1] if D > 1 else 1)]
+                    q = p.copy()  # computeConnectedPos, kernel.cu:326-345
+                    ca = bnd.axes[0] >> 1
+                    q[:, ca] = ob.size[ca] - 1 if (bnd.axes[0] & 1) else 0
+                    if D > 1:
+                        ax = (a + 1) % D
+                        ca1 = bnd.axes[1] >> 1
+                        q[:, ca1] = (ob.size[ca1] - 1 - p[:, ax]) if (bnd.axes[1] & 1) else p[:, ax]
+                        if D > 2:
+                            ax2 = (a + 2) % D
+                            ca2 = bnd.axes[2] >> 1
+                            q[:, ca2] = (ob.size[ca2] - 1 - p[:, ax2]) if (bnd.axes[2] & 1) else p[:, ax2]
+                    conn = oo + q[:, 0] + ostride[1] * q[:, 1] + ostride[2] * q[:, 2]
+                    nbv = np.where(at, conn, nbv)
+                    ncomp = np.where(at, ca, ncomp)
+                    other_up = bnd.axes[0] & 1
+                    flip = np.where(at & (other_up == up), -1.0, 1.0)
+                self.nb[f, sl] = nbv
+                self.fixed[f, sl] = fixed
+                self.ncomp[f, sl] = ncomp
+                self.flip[f, sl] = flip
+        self._gather_static()
+
+    def _gather_static(self):
+        D = self.dims
+        N = self.N
+        self.det = np.ones(N)
+        self.Minv = np.zeros((N, D, D))
+        for i in range(D):
+            self.Minv[:, i, i] = 1.0
+        for bi, b in enumerate(self.blocks):
+            o = self.offsets[bi]
+            sl = slice(o, o + b.ncells)
+            if b.transform is not None:
+                T = b.transform.reshape(b.ncells, -1)
+                self.Minv[sl] = T[:, D * D:2 * D * D].reshape(-1, D, D)
+                self.det[sl] = T[:, -1]
+
+    # ---- per-step gathers ----
+    def velocity_global(self):
+        D = self.dims
+        u = np.zeros((D, self.N))
+        for bi, b in enumerate(self.blocks):
+            o = self.offsets[bi]
+            u[:, o:o + b.ncells] = b.velocity.reshape(D, -1)
+        return u
+
+    def pressure_global(self):
+        p = np.zeros(self.N)
+        for bi, b in enumerate(self.blocks):
+            o = self.offsets[bi]
+            p[o:o + b.ncells] = b.pressure.reshape(-1)
+        return p
+
+    def set_velocity_global(self, u):
+        D = self.dims
+        for bi, b in enumerate(self.blocks):
+            o = self.offsets[bi]
+            b.velocity = u[:, o:o + b.ncells].reshape(b.velocity.shape).copy()
+
+    def set_pressure_global(self, p):
+        for bi, b in enumerate(self.blocks):
+            o = self.offsets[bi]
+            b.pressure = p[o:o + b.ncells].reshape(b.pressure.shape).copy()
+
+    def viscosity_cells(self):
+        """getViscosityBlock, kernel.cu:1801-1822."""
+        nu = np.full(self.N, self.viscosity)
+        for bi, b in enumerate(self.blocks):
+            if b.viscosity is None:
+                continue
+            o = self.offsets[bi]
+            v = np.asarray(b.viscosity, dtype=np.float64)
+            if v.ndim == 1:  # static
+                nu[o:o + b.ncells] = v[0]
+            else:
+                nu[o:o + b.ncells] = v.reshape(-1)
+        return nu
+
+    def source_cells(self):
+        """getBlockVelocitySource, kernel.cu:2241-2251."""
+        D = self.dims
+        s = np.zeros((D, self.N))
+        for bi, b in enumerate(self.blocks):
+            if b.source is None:
+                continue
+            o = self.offsets[bi]
+            v = np.asarray(b.source, dtype=np.float64)
+            if v.ndim == 2:  # static [1,D]
+                s[:, o:o + b.ncells] = v.reshape(D, 1)
+            else:
+                s[:, o:o + b.ncells] = v.reshape(D, -1)
+        return s
+
+    def boundary_cell_data(self):
+        """Per face: boundary velocity [D,N], contravariant normal boundary flux [N] and
+        boundary Laplace coefficient [N] at fixed faces (getFixedBoundaryData kernel.cu:2374-2433,
+        getContravariantComponentBoundaryFixed kernel.cu:728-748, getLaplaceCoefficientOrthogonalBoundary
+        kernel.cu:1434-1447)."""
+        D = self.dims
+        N = self.N
+        K = 2 * D
+        bvel = np.zeros((K, D, N))
+        bflux = np.zeros((K, N))
+        balpha = np.ones((K, N))
+        for f in range(K):
+            a = f >> 1
+            for bi, b in enumerate(self.blocks):
+                bnd = b.boundaries[f]
+                if bnd.kind != "fixed":
+                    continue
+                o = self.offsets[bi]
+                sl = slice(o, o + b.ncells)
+                p = self.pos[sl]
+                at = self.fixed[f, sl]
+                bsize = list(b.size) + [1] * (3 - D)
+                bsize[a] = 1
+                bflat = p[:, 0] * (1 if a != 0 else 0) + bsize[0] * (p[:, 1] if a != 1 else 0) \
+                    + bsize[0] * bsize[1] * (p[:, 2] if a != 2 else 0)
+                vel = np.asarray(bnd.velocity, dtype=np.float64)
+                if vel.ndim == 2:
+                    v = np.repeat(vel.reshape(D, 1), b.ncells, axis=1)
+                else:
+                    v = vel.reshape(D, -1)[:, bflat]
+                if bnd.transform is not None:
+                    T = bnd.transform.reshape(-1, 2 * D * D + 1)[bflat]
+                    Minv = T[:, D * D:2 * D * D].reshape(-1, D, D)
+                    det = T[:, -1]
+                    contra = det * np.einsum("nj,jn->n", Minv[:, a, :], v)
+                    alpha = det * np.einsum("nj,nj->n", Minv[:, a, :], Minv[:, a, :])
+                else:
+                    contra = v[a]
+                    alpha = np.ones(b.ncells)
+                bvel[f, :, sl] = np.where(at[None], v, 0.0)
+                bflux[f, sl] = np.where(at, contra, 0.0)
+                balpha[f, sl] = np.where(at, alpha, 1.0)
+        return bvel, bflux, balpha
+
+    def clone(self):
+        import copy
+        return copy.deepcopy(self)
+
+
+# --------------------------------------------------------------------------
+# assembly (kernel.cu)
+# --------------------------------------------------------------------------
+
+def contravariant(dom: ODomain, u: np.ndarray, comp: np.ndarray, idx: np.ndarray) -> np.ndarray:
+    """det * Minv[comp] . u at cells idx (VelocityToContravariantComponent, kernel.cu:479-494)."""
+    Mrow = dom.Minv[idx, comp, :]  # [n, D]
+    return dom.det[idx] * np.einsum("nj,jn->n", Mrow, u[:, idx])
+
+
+def laplace_coef(dom: ODomain, comp: np.ndarray, idx: np.ndarray) -> np.ndarray:
+    """det * |Minv[comp]|^2 (getLaplaceCoefficientOrthogonal, kernel.cu:1209-1224)."""
+    Mrow = dom.Minv[idx, comp, :]
+    return dom.det[idx] * np.einsum("nj,nj->n", Mrow, Mrow)
+
+
+def face_fluxes(dom: ODomain, u: np.ndarray, bflux: np.ndarray) -> np.ndarray:
+    """computeFluxesNDLoop, kernel.cu:1552-1630: per face the (unsigned) contravariant face flux,
+    central average of the two cells, or the prescribed boundary flux at fixed faces."""
+    D = dom.dims
+    N = dom.N
+    allc = np.arange(N)
+    fl = np.zeros((2 * D, N))
+    for f in range(2 * D):
+        a = f >> 1
+        velC = contravariant(dom, u, np.full(N, a), allc)
+        nb = dom.nb[f]
+        ok = nb >= 0
+        velN = np.zeros(N)
+        velN[ok] = contravariant(dom, u, dom.ncomp[f][ok], nb[ok]) * dom.flip[f][ok]
+        fl[f] = np.where(dom.fixed[f], bflux[f], 0.5 * (velN + velC))
+    return fl
+
+
+def advection_matrix(dom: ODomain, dt: float):
+    """PISO_build_matrix, kernel.cu:3601-3865 (orthogonal terms only, nonOrthoFlags=0).
+
+    Returns (coef[K,N], A[N]) with coefficients divided by det as the reference does.
+    """
+    D = dom.dims
+    N = dom.N
+    K = 2 * D + 1
+    u = dom.velocity_global()
+    _, bflux, _ = dom.boundary_cell_data()
+    fl = face_fluxes(dom, u, bflux)
+    nu = dom.viscosity_cells()
+    allc = np.arange(N)
+    det = dom.det
+    diag = det / dt
+    coef = np.zeros((K, N))
+    alpha_p = [laplace_coef(dom, np.full(N, d), allc) for d in range(D)]
+    for f in range(2 * D):
+        d = f >> 1
+        sign = 2 * (f & 1) - 1
+        fixed = dom.fixed[f]
+        nb = dom.nb[f]
+        ok = ~fixed
+        ff = sign * 0.5 * fl[f]
+        alpha_n = np.zeros(N)
+        nu_n = np.zeros(N)
+        alpha_n[ok] = laplace_coef(dom, dom.ncomp[f][ok], nb[ok])
+        nu_n[ok] = nu[nb[ok]]
+        vc = 0.5 * (alpha_p[d] * nu + alpha_n * nu_n)
+        diag = diag + np.where(ok, ff + vc, 2.0 * nu * alpha_p[d])  # slip=0 for Dirichlet walls
+        coef[f + 1] = np.where(ok, ff - vc, 0.0)
+    coef[0] = diag
+    coef = coef / det[None]
+    return coef, coef[0].copy()
+
+
+def advection_rhs(dom: ODomain, dt: float):
+    """kPISO_build_advection_RHS, kernel.cu:4281-4385 (FIXED boundaries, no pressure gradient)."""
+    D = dom.dims
+    u = dom.velocity_global()
+    bvel, bflux, balpha = dom.boundary_cell_data()
+    nu = dom.viscosity_cells()
+    src = dom.source_cells()
+    det = dom.det
+    rhs = det[None] * u / dt
+    for f in range(2 * D):
+        fixed = dom.fixed[f]
+        sign = 2 * (f & 1) - 1
+        flux = bflux[f] * sign
+        for c in range(D):
+            vel = bvel[f, c]
+            add = -vel * flux + vel * nu * 2.0 * balpha[f]
+            rhs[c] = rhs[c] + np.where(fixed, add, 0.0)
+    rhs = rhs / det[None] + src
+    return rhs
+
+
+def pressure_matrix(dom: ODomain, A: np.ndarray):
+    """PISO_build_pressure_matrix, kernel.cu:4797-4963 (no face transforms, no non-ortho terms)."""
+    D = dom.dims
+    N = dom.N
+    K = 2 * D + 1
+    allc = np.arange(N)
+    raP = 1.0 / A
+    coef = np.zeros((K, N))
+    for f in range(2 * D):
+        d = f >> 1
+        ok = ~dom.fixed[f]
+        nb = dom.nb[f]
+        alphaP = laplace_coef(dom, np.full(N, d), allc)
+        alphaN = np.zeros(N)
+        raN = np.zeros(N)
+        alphaN[ok] = laplace_coef(dom, dom.ncomp[f][ok], nb[ok])
+        raN[ok] = 1.0 / A[nb[ok]]
+        c = np.where(ok, 0.5 * (alphaP * raP + alphaN * raN), 0.0)
+        coef[0] -= c
+        coef[f + 1] = c
+    return coef
+
+
+def pressure_rhs(dom: ODomain, dt: float, Ccoef: np.ndarray, A: np.ndarray, u_star: np.ndarray):
+    """PISO_build_pressure_rhs, kernel.cu:5121-5240 (with boundary sources, the compiled default)."""
+    D = dom.dims
+    N = dom.N
+    u = dom.velocity_global()
+    bvel, bflux, balpha = dom.boundary_cell_data()
+    nu = dom.viscosity_cells()
+    src = dom.source_cells()
+    det = dom.det
+    allc = np.arange(N)
+    h = np.zeros((D, N))
+    for c in range(D):
+        H = np.zeros(N)
+        S = np.zeros(N)
+        for f in range(2 * D):
+            nb = dom.nb[f]
+            ok = (nb >= 0) & (nb != allc)
+            H[ok] += Ccoef[f + 1][ok] * u_star[c][nb[ok]]
+            fixed = dom.fixed[f]
+            sign = 2 * (f & 1) - 1
+            vel = bvel[f, c]
+            S += np.where(fixed, -vel * bflux[f] * sign + vel * nu * 2.0 * balpha[f], 0.0)
+        S = S / det + src[c]
+        h[c] = (u[c] / dt - H + S) / A
+    return h
+
+
+def divergence(dom: ODomain, h: np.ndarray):
+    """k_computePressureRHSdivergenceFromFlux, kernel.cu:5374-5419 (no time-step norm)."""
+    D = dom.dims
+    _, bflux, _ = dom.boundary_cell_data()
+    fl = face_fluxes(dom, h, bflux)
+    div = np.zeros(dom.N)
+    for d in range(D):
+        div += fl[2 * d + 1] - fl[2 * d]
+    return div
+
+
+def pressure_gradient_fd(dom: ODomain, p: np.ndarray):
+    """getPressureGradient, kernel.cu:801-834 with getPressureAtWithBounds kernel.cu:2160-2239."""
+    D = dom.dims
+    N = dom.N
+    g = np.zeros((D, N))
+    for d in range(D):
+        lo, hi = 2 * d, 2 * d + 1
+        fac = np.full(N, 0.5)
+        lo_fixed = dom.fixed[lo]
+        hi_fixed = dom.fixed[hi]
+        nbl = np.where(lo_fixed, np.arange(N), dom.nb[lo])
+        nbh = np.where(hi_fixed, np.arange(N), dom.nb[hi])
+        fac = np.where(lo_fixed | hi_fixed, 1.0, fac)
+        g[d] = (p[nbh] - p[nbl]) * fac
+    # matmul(pressureGrad, Minv): g_j = sum_i g_i Minv[i][j]
+    return np.einsum("in,nij->jn", g, dom.Minv)
+
+
+def correct_velocity(dom: ODomain, p_blocks: np.ndarray, A: np.ndarray, h: np.ndarray):
+    """PISO_update_velocity (version 1, FD), kernel.cu:5947-5980."""
+    g = pressure_gradient_fd(dom, p_blocks)
+    return h - g / A[None]
+
+
+# --------------------------------------------------------------------------
+# CSR export in the reference ordering
+# --------------------------------------------------------------------------
+
+def stencil_to_csr(dom: ODomain, coef: np.ndarray):
+    """CSR (value, index, row) with each row sorted by column like kernel.cu:3846-3860."""
+    D = dom.dims
+    N = dom.N
+    cols = [np.arange(N)] + [dom.nb[f] for f in range(2 * D)]
+    rows_v, rows_i, row_ptr = [], [], [0]
+    C = np.stack(cols, 0)
+    V = coef
+    for i in range(N):
+        c = C[:, i]
+        v = V[:, i]
+        m = c >= 0
+        order = np.argsort(c[m], kind="stable")
+        rows_i.append(c[m][order])
+        rows_v.append(v[m][order])
+        row_ptr.append(row_ptr[-1] + int(m.sum()))
+    return np.concatenate(rows_v), np.concatenate(rows_i), np.array(row_ptr)
+
+
+def stencil_to_scipy(dom: ODomain, coef: np.ndarray) -> sp.csr_matrix:
+    D = dom.dims
+    N = dom.N
+    rows, cols, vals = [np.arange(N)], [np.arange(N)], [coef[0]]
+    for f in range(2 * D):
+        ok = dom.nb[f] >= 0
+        rows.append(np.arange(N)[ok])
+        cols.append(dom.nb[f][ok])
+        vals.append(coef[f + 1][ok])
+    return sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(N, N))
+
+
+# --------------------------------------------------------------------------
+# Krylov solvers with the reference's iteration semantics
+# --------------------------------------------------------------------------
+
+@dataclass
+class SolveInfo:
+    finalResidual: float
+    usedIterations: int
+    converged: bool
+    isFiniteResidual: bool
+
+
+def _crit(r):
+    """NORM2_NORMALIZED: ||r||_2 / sqrt(n) (cg.cu:85-90)."""
+    return float(np.sqrt(np.dot(r, r)) / math.sqrt(r.shape[0]))
+
+
+def cg(A, b, x0=None, tol=1e-5, maxit=5000, dtype=np.float64):
+    """cgSolveGPU without rank-deficiency, residual reset or best-result, cg.cu:236-427."""
+    b = np.asarray(b, dtype=dtype)
+    x = np.zeros_like(b) if x0 is None else np.array(x0, dtype=dtype)
+    A = A.astype(dtype)
+    r = b - A @ x
+    p = r.copy()
+    rho = float(np.dot(r, r))
+    info = SolveInfo(0.0, -1, False, True)
+    for i in range(maxit):
+        q = A @ p
+        alpha = rho / float(np.dot(p, q))
+        x = x + alpha * p
+        r = r - alpha * q
+        crit = _crit(r)
+        if not math.isfinite(crit):
+            return x, SolveInfo(crit, i, False, False)
+        info = SolveInfo(crit, i, False, True)
+        if crit < tol:
+            info.converged = True
+            break
+        rhop = rho
+        rho = float(np.dot(r, r))
+        beta = rho / rhop
+        p = beta * p + r
+    return x, info
+
+
+def bicgstab(A, b, x0=None, tol=1e-5, maxit=5000, dtype=np.float64):
+    """bicgstabSolveGPU without preconditioner, bicg.cu:240-360."""
+    b = np.asarray(b, dtype=dtype)
+    x = np.zeros_like(b) if x0 is None else np.array(x0, dtype=dtype)
+    A = A.astype(dtype)
+    r = b - A @ x
+    rw = r.copy()
+    p = r.copy()
+    v = np.zeros_like(b)
+    nrmr0 = _crit(r)
+    if nrmr0 < tol:
+        return x, SolveInfo(nrmr0, -1, True, True)
+    rho = 0.0
+    alpha = omega = 0.0
+    info = SolveInfo(0.0, -1, False, True)
+    for i in range(maxit):
+        rhop = rho
+        rho = float(np.dot(rw, r))
+        if i > 0:
+            beta = (rho / rhop) * (alpha / omega)
+            p = r + beta * (p - omega * v)
+        v = A @ p
+        alpha = rho / float(np.dot(rw, v))
+        r = r - alpha * v
+        x = x + alpha * p
+        nrmr = _crit(r)
+        if not math.isfinite(nrmr):
+            return x, SolveInfo(nrmr, i, False, False)
+        info = SolveInfo(nrmr, i, False, True)
+        if nrmr < tol:
+            info.converged = True
+            break
+        s = r
+        t = A @ s
+        omega = float(np.dot(t, r)) / float(np.dot(t, t))
+        x = x + omega * s
+        r = r - omega * t
+        nrmr = _crit(r)
+        info.finalResidual = nrmr
+        if nrmr < tol:
+            info = SolveInfo(nrmr, i + 1, True, True)
+            break
+    return x, info
+
+
+def solve(A, b, use_bicg: bool, tol: float, maxit: int = 5000, method: str = "iterative"):
+    """Linear solve as the simulation driver issues it (diff.py:245-293): an all-zero RHS gives x=0."""
+    if not np.any(b != 0):
+        return np.zeros_like(b), SolveInfo(0.0, 0, True, True)
+    if method == "direct":
+        import scipy.sparse.linalg as spla
+        x = spla.spsolve(A.tocsc(), b)
+        return x, SolveInfo(0.0, 0, True, True)
+    if use_bicg:
+        return bicgstab(A, b, tol=tol, maxit=maxit)
+    return cg(A, b, tol=tol, maxit=maxit)
+
+
+# --------------------------------------------------------------------------
+# PISO step (sim.py:1054-1327, orthogonal branch)
+# --------------------------------------------------------------------------
+
+@dataclass
+class StepResult:
+    C: np.ndarray
+    A: np.ndarray
+    velocityRHS: np.ndarray
+    u_star: np.ndarray
+    P: np.ndarray
+    pressureRHS: np.ndarray
+    pressureRHSdiv: np.ndarray
+    pressure: np.ndarray
+    velocity: np.ndarray
+    infos: list
+
+
+def piso_step(dom: ODomain, dt: float, corrector_steps: int = 2, adv_tol: float = 1e-5,
+              p_tol: float = 1e-5, method: str = "iterative", maxit: int = 5000,
+              normalize_pressure: bool = True) -> StepResult:
+    """One PISO step, Simulation._PISO_split_step with non_orthogonal=False, sim.py:1054-1327.
+
+    Updates the block velocity and pressure of ``dom`` in place and returns the intermediate fields
+    of the last corrector for inspection.
+    """
+    D = dom.dims
+    N = dom.N
+    infos = []
+    Ccoef, A = advection_matrix(dom, dt)
+    rhs = advection_rhs(dom, dt)
+    Cm = stencil_to_scipy(dom, Ccoef)
+    u_star = np.zeros((D, N))
+    for c in range(D):  # nBatches = D, solved one after another (bicg.cu:221)
+        u_star[c], info = solve(Cm, rhs[c], True, adv_tol, maxit, method)
+        infos.append(("adv", c, info))
+    u_cur = u_star
+    P = h = div = p = None
+    for _ in range(corrector_steps):
+        P = pressure_matrix(dom, A)
+        h = pressure_rhs(dom, dt, Ccoef, A, u_cur)
+        div = divergence(dom, h)
+        Pm = stencil_to_scipy(dom, P)
+        p, info = solve(Pm, div, False, p_tol, maxit, method)
+        infos.append(("p", 0, info))
+        if normalize_pressure:
+            p = p - p.mean()  # sim.py:1243-1244
+        dom.set_pressure_global(p)  # CopyPressureResultToBlocks
+        u_cur = correct_velocity(dom, p, A, h)
+    dom.set_velocity_global(u_cur)  # CopyVelocityResultToBlocks
+    return StepResult(Ccoef, A, rhs, u_star, P, h, div, p, u_cur, infos)
+
+
+def run_steps(dom: ODomain, steps: int, dt: float, **kw):
+    res = None
+    for _ in range(steps):
+        res = piso_step(dom, dt, **kw)
+    return res

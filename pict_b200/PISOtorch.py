@@ -1,0 +1,1947 @@
+"""Drop-in host mirror of the reference's ``PISOtorch`` extension module.
+
+Same class names, method names, argument names, defaults and error behaviour as
+the reference's pybind11 module (extensions/PISOtorch.cpp:25-655, backed by
+extensions/domain_structs.{h,cpp}), implemented as a thin Python layer over the
+C ABI of ``libpict_b200.so`` (include/pict_b200.h).  Field memory stays in
+torch tensors owned by Python; the native code receives raw device pointers in
+a packed block table (the reference's "atlas", domain_structs.cpp:2992-3261),
+re-packed by ``Domain.UpdateDomainData()`` exactly when the reference requires
+it.
+
+Differences in representation (not in results):
+
+* ``Domain.C`` / ``Domain.P`` are :class:`StencilMatrix` objects: the system
+  matrices are stored as per-cell stencil coefficients ``coef[K][N]``; the
+  reference's CSR arrays ``value/index/row`` are materialised on demand in the
+  reference's row layout (rows sorted by column).
+* Linear solves run as persistent CUDA kernels; ``SolveLinear`` still returns
+  one ``LinearSolverResultInfo`` per right-hand side.
+
+Scope: the orthogonal PISO path (``nonOrthoFlags=0``) with fixed Dirichlet,
+periodic and connected block boundaries, per-cell transforms, block/global
+viscosity and velocity sources, in 2D and 3D, float32 and float64.  Passive
+scalar transport, non-orthogonal corrections, the FVM velocity correctors and
+ILU preconditioning raise ``NotImplementedError``.
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+import warnings
+import weakref
+from typing import List, Optional
+
+import torch
+
+from . import _lib
+from ._lib import BlockDesc, DomainDesc, Face, SolveInfo, SolveParams, check
+
+# ------------------------------------------------------------------------------------------------
+# enums and small types (PISOtorch.cpp:30-58, 544-558)
+# ------------------------------------------------------------------------------------------------
+
+
+class BoundaryType(enum.IntEnum):
+    DIRICHLET = 0
+    DIRICHLET_VARYING = 1
+    NEUMANN = 10
+    FIXED = 30
+    CONNECTED = 20
+    PERIODIC = 21
+
+
+class BoundaryConditionType(enum.IntEnum):
+    DIRICHLET = 0
+    NEUMANN = 1
+
+
+class ConvergenceCriterion(enum.IntEnum):
+    NORM2 = 0
+    NORM2_NORMALIZED = 1
+    ABS_SUM = 2
+    ABS_MEAN = 3
+    ABS_MAX = 4
+
+
+# pybind11 export_values(): enum members are also module attributes
+DIRICHLET_VARYING = BoundaryType.DIRICHLET_VARYING
+FIXED = BoundaryType.FIXED
+CONNECTED = BoundaryType.CONNECTED
+PERIODIC = BoundaryType.PERIODIC
+DIRICHLET = BoundaryConditionType.DIRICHLET
+NEUMANN = BoundaryConditionType.NEUMANN
+NORM2 = ConvergenceCriterion.NORM2
+NORM2_NORMALIZED = ConvergenceCriterion.NORM2_NORMALIZED
+ABS_SUM = ConvergenceCriterion.ABS_SUM
+ABS_MEAN = ConvergenceCriterion.ABS_MEAN
+ABS_MAX = ConvergenceCriterion.ABS_MAX
+
+
+class Int4:
+    """I4 (domain_structs_gpu.h:120-125)."""
+
+    def __init__(self, x=0, y=0, z=0, w=0):
+        self.x, self.y, self.z, self.w = int(x), int(y), int(z), int(w)
+
+    def __getitem__(self, i):
+        if 0 <= i < 4:
+            return (self.x, self.y, self.z, self.w)[i]
+        raise IndexError(i)
+
+    def __len__(self):
+        return 4
+
+    def __str__(self):
+        return "I4(%d,%d,%d,%d)" % (self.x, self.y, self.z, self.w)
+
+    __repr__ = __str__
+
+
+class LinearSolverResultInfo:
+    """bicgstab_solver.h:20-34."""
+
+    def __init__(self, finalResidual=0.0, usedIterations=-1, converged=False, isFiniteResidual=True):
+        self.finalResidual = float(finalResidual)
+        self.usedIterations = int(usedIterations)
+        self.converged = bool(converged)
+        self.isFiniteResidual = bool(isFiniteResidual)
+
+    def __str__(self):
+        return "LinearSolverResultInfo(finalResidual=%g, usedIterations=%d, converged=%d, isFiniteResidual=%d)" % (
+            self.finalResidual, self.usedIterations, self.converged, self.isFiniteResidual)
+
+    __repr__ = __str__
+
+
+FACE_NAMES = ["-x", "+x", "-y", "+y", "-z", "+z"]
+AXIS_NAMES = ["x", "y", "z"]
+
+
+def _face_index(face) -> int:
+    """BoundarySideToIndex, domain_structs.cpp:134-155."""
+    if isinstance(face, str):
+        if face not in FACE_NAMES:
+            raise ValueError("Invalid boundary side '%s'" % face)
+        return FACE_NAMES.index(face)
+    return int(face)
+
+
+def _axis_index(axis) -> int:
+    if isinstance(axis, str):
+        if axis not in AXIS_NAMES:
+            raise ValueError("Invalid axis '%s'" % axis)
+        return AXIS_NAMES.index(axis)
+    return int(axis)
+
+
+def _check(cond, msg):
+    if not cond:
+        raise RuntimeError(msg)
+
+
+def _dtype_code(dtype):
+    if dtype == torch.float32:
+        return _lib.PICT_F32
+    if dtype == torch.float64:
+        return _lib.PICT_F64
+    raise TypeError("dtype must be torch.float32 or torch.float64")
+
+
+def _stream_ptr():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ptr(t: Optional[torch.Tensor]):
+    return None if t is None else t.data_ptr()
+
+
+def _transform_size(dims):
+    return 2 * dims * dims + 1
+
+
+def _as_scalar(v, default=None):
+    if v is None:
+        return default
+    if isinstance(v, torch.Tensor):
+        return v.reshape(-1)[0].item()
+    return v
+
+
+# ------------------------------------------------------------------------------------------------
+# CSR / stencil matrices (domain_structs.h:54-90)
+# ------------------------------------------------------------------------------------------------
+
+
+class CSRmatrix:
+    """Generic CSR matrix container with the reference's interface."""
+
+    def __init__(self, value, index=None, row=None, device=None):
+        if isinstance(value, torch.Tensor):
+            self.value = value
+            self.index = index
+            self.row = row
+        else:  # CSRmatrix(numValues, numRows, dtype, device)
+            numValues, numRows, dtype = int(value), int(index), row
+            self.value = torch.zeros(numValues, dtype=dtype, device=device)
+            self.index = torch.zeros(numValues, dtype=torch.int32, device=device)
+            self.row = torch.zeros(numRows + 1, dtype=torch.int32, device=device)
+        self._changed = False
+
+    def setValue(self, tensor):
+        _check(tensor.dim() == 1 and tensor.size(0) == self.getSize(), "CSR value size must not change.")
+        self.value = tensor
+        self._changed = True
+
+    def CreateValue(self):
+        self.setValue(torch.zeros_like(self.value))
+
+    def getDevice(self):
+        return self.value.device
+
+    def getDtype(self):
+        return self.value.dtype
+
+    def copy(self):
+        return CSRmatrix(self.value, self.index, self.row)
+
+    def clone(self):
+        return CSRmatrix(self.value.clone(), self.index, self.row)
+
+    def detach(self):
+        self.value = self.value.detach()
+
+    def WithZeroValue(self):
+        return CSRmatrix(torch.zeros_like(self.value), self.index, self.row)
+
+    def toType(self, dtype):
+        return CSRmatrix(self.value.to(dtype), self.index, self.row)
+
+    def getSize(self):
+        return self.value.size(0)
+
+    def getRows(self):
+        return self.row.size(0) - 1
+
+    def IsTensorChanged(self):
+        return self._changed
+
+    def __str__(self):
+        return "CSRmatrix(rows=%d, nnz=%d)" % (self.getRows(), self.getSize())
+
+
+class StencilMatrix(CSRmatrix):
+    """System matrix of a prepared domain stored as stencil coefficients ``coef[K][N]``.
+
+    ``value``/``index``/``row`` give the reference CSR layout (computed on demand);
+    assigning ``value`` (``setValue``) converts back to stencil storage.
+    """
+
+    def __init__(self, domain, coef: torch.Tensor):
+        self._domain_ref = weakref.ref(domain)
+        self.coef = coef
+        self._changed = False
+
+    # -- CSR views --
+    def _domain(self):
+        d = self._domain_ref()
+        if d is None:
+            raise RuntimeError("StencilMatrix: the domain is expired.")
+        return d
+
+    def _csr(self):
+        d = self._domain()
+        row, index = d._csr_structure()
+        value = torch.empty(index.numel(), dtype=self.coef.dtype, device=self.coef.device)
+        check(_lib.load().pict_stencil_to_csr(ctypes.byref(d._desc), _ptr(self.coef.contiguous()), _ptr(row),
+                                              _ptr(value), _ptr(index), _stream_ptr()), "stencil_to_csr")
+        return value, index, row
+
+    @property
+    def value(self):
+        return self._csr()[0]
+
+    @property
+    def index(self):
+        return self._domain()._csr_structure()[1]
+
+    @property
+    def row(self):
+        return self._domain()._csr_structure()[0]
+
+    def setValue(self, tensor):
+        d = self._domain()
+        row, index = d._csr_structure()
+        _check(tensor.dim() == 1 and tensor.size(0) == index.numel(), "CSR value size must not change.")
+        coef = torch.empty_like(self.coef)
+        check(_lib.load().pict_csr_to_stencil(ctypes.byref(d._desc), _ptr(tensor.contiguous()), _ptr(row),
+                                              _ptr(index), _ptr(coef), _stream_ptr()), "csr_to_stencil")
+        self.coef = coef
+        self._changed = True
+
+    def setCoef(self, coef):
+        _check(coef.shape == self.coef.shape, "stencil shape must not change.")
+        self.coef = coef
+        self._changed = True
+
+    def CreateValue(self):
+        self.setCoef(torch.zeros_like(self.coef))
+
+    def getDevice(self):
+        return self.coef.device
+
+    def getDtype(self):
+        return self.coef.dtype
+
+    def getSize(self):
+        return self._domain()._csr_structure()[1].numel()
+
+    def getRows(self):
+        return self.coef.size(1)
+
+    def copy(self):
+        return StencilMatrix(self._domain(), self.coef)
+
+    def clone(self):
+        return StencilMatrix(self._domain(), self.coef.clone())
+
+    def detach(self):
+        self.coef = self.coef.detach()
+
+    def WithZeroValue(self):
+        return StencilMatrix(self._domain(), torch.zeros_like(self.coef))
+
+    def toType(self, dtype):
+        return StencilMatrix(self._domain(), self.coef.to(dtype))
+
+    def __str__(self):
+        return "StencilMatrix(K=%d, rows=%d)" % (self.coef.size(0), self.coef.size(1))
+
+
+# ------------------------------------------------------------------------------------------------
+# boundaries (domain_structs.h:92-375)
+# ------------------------------------------------------------------------------------------------
+
+
+class Boundary:
+    def __init__(self, btype, domain):
+        self.type = btype
+        self._domain_ref = weakref.ref(domain)
+        self._changed = True
+
+    def getParentDomain(self):
+        d = self._domain_ref()
+        _check(d is not None, "Parent domain expired.")
+        return d
+
+    def getSpatialDims(self):
+        return self.getParentDomain().getSpatialDims()
+
+    def getDtype(self):
+        return self.getParentDomain().getDtype()
+
+    def getDevice(self):
+        return self.getParentDomain().getDevice()
+
+    def IsTensorChanged(self):
+        return self._changed
+
+    def __str__(self):
+        return "%s()" % self.type.name
+
+
+class PeriodicBoundary(Boundary):
+    def __init__(self, domain):
+        super().__init__(BoundaryType.PERIODIC, domain)
+
+    def Copy(self):
+        return PeriodicBoundary(self.getParentDomain())
+
+    Clone = Copy
+
+
+class ConnectedBoundary(Boundary):
+    """domain_structs.h:329-352; ``axes`` starts with the connected face of the other block."""
+
+    def __init__(self, block, axes, domain):
+        super().__init__(BoundaryType.CONNECTED, domain)
+        self._block_ref = weakref.ref(block)
+        self.axes = list(axes)
+
+    def getConnectedBlock(self):
+        b = self._block_ref()
+        _check(b is not None, "ConnectedBlock is expired.")
+        return b
+
+    def getConnectedFace(self):
+        return self.axes[0] >> 1
+
+    def getConnectionAxis(self, axis):
+        return self.axes[axis] >> 1
+
+    def getConnectionAxisDirection(self, axis):
+        return self.axes[axis] & 1
+
+    def __str__(self):
+        s = 'CONNECTED(to="%s", face=%s' % (self.getConnectedBlock().name, FACE_NAMES[self.axes[0]])
+        for k in range(1, len(self.axes)):
+            s += ", axis%d=%s" % (k, FACE_NAMES[self.axes[k]])
+        return s + ")"
+
+
+class FixedBoundary(Boundary):
+    """Prescribed boundary: Dirichlet velocity, 0-Neumann pressure (domain_structs.cpp:304-796)."""
+
+    def __init__(self, domain, velocity=None, velocityType=BoundaryConditionType.DIRICHLET, passiveScalar=None,
+                 transform=None):
+        super().__init__(BoundaryType.FIXED, domain)
+        self._size = None  # x,y,z with 1 along the face axis
+        self._axis = -1
+        self.velocityGrad = torch.empty(0)
+        self.passiveScalar = None
+        self.passiveScalarGrad = None
+        self.passiveScalarTypes = None
+        self.transform = None
+        dims = domain.getSpatialDims()
+        if velocity is not None and velocity.dim() > 2:
+            self._setSizeFromTensor(velocity, True)
+        elif passiveScalar is not None and passiveScalar.dim() > 2:
+            self._setSizeFromTensor(passiveScalar, True)
+        elif transform is not None:
+            self._setSizeFromTensor(transform, False)
+        elif velocity is not None:
+            _check(velocity.dim() > 1, "Velocity must be 1-3D and either static (shape NC) or varying (shape NCDHW).")
+        elif passiveScalar is not None:
+            raise RuntimeError("Can't create FixedBoundary from static passive scalar alone.")
+        if velocity is not None:
+            self.setVelocity(velocity)
+        else:
+            self.CreateVelocity(True)
+        self.setVelocityType(velocityType)
+        if passiveScalar is not None:
+            self.setPassiveScalar(passiveScalar)
+        elif domain.hasPassiveScalar():
+            self.CreatePassiveScalar(True)
+        if transform is not None:
+            self.setTransform(transform)
+
+    # -- size --
+    def _setSizeFromTensor(self, t, channelsFirst):
+        dims = self.getSpatialDims()
+        _check(t.dim() == dims + 2, "Invalid tensor for boundary shape.")
+        off = 1 if channelsFirst else 0
+        size = [t.size(dims + off - d) for d in range(dims)]
+        self._setSize(size)
+
+    def _setSize(self, size):
+        _check(self._size is None, "Internal Error: FixedBoundary already has a size set.")
+        dims = self.getSpatialDims()
+        has1 = False
+        for d in range(dims):
+            if size[d] == 1:
+                _check(not has1, "Invalid boundary shape: only one dimension must be 1.")
+                has1 = True
+                self._axis = d
+            else:
+                _check(size[d] > 2, "Invalid boundary shape: grid size must be at least 3.")
+        _check(has1, "Invalid boundary shape: one dimension must be 1.")
+        self._size = list(size) + [1] * (3 - dims)
+
+    def hasSize(self):
+        return self._size is not None
+
+    def getSizes(self):
+        dims = self.getSpatialDims()
+        s = self._size if self._size is not None else [1, 1, 1]
+        return Int4(s[0], s[1], s[2], dims)
+
+    def getStrides(self):
+        s = self.getSizes()
+        return Int4(1, s.x, s.x * s.y, s.x * s.y * s.z)
+
+    def _face_cells(self):
+        s = self.getSizes()
+        return s.x * s.y * s.z
+
+    # -- velocity --
+    @property
+    def velocity(self):
+        return self._velocity
+
+    @property
+    def velocityType(self):
+        return self._velocityType
+
+    @property
+    def isVelocityStatic(self):
+        return self._velocityStatic
+
+    def setVelocity(self, t):
+        dims = self.getSpatialDims()
+        _check(t.is_cuda, "velocity must be a CUDA tensor")
+        _check(t.is_contiguous(), "velocity must be contiguous")
+        _check(t.size(0) == 1, "Batches are not yet supported (velocity).")
+        _check(t.size(1) == dims, "Velocity channels are invalid. Velocity must be %dD and either static (shape NC) or varying (shape NCDHW)." % dims)
+        _check(t.dim() == 2 or t.dim() == 2 + dims,
+               "Velocity spatial dimensions are invalid. Velocity must be %dD and either static (shape NC) or varying (shape NCDHW)." % dims)
+        _check(t.dtype == self.getDtype(), "Velocity dtype must match domain.")
+        static = t.dim() == 2
+        if not static and self.hasSize():
+            s = self.getSizes()
+            _check(all(t.size(dims + 1 - d) == [s.x, s.y, s.z][d] for d in range(dims)),
+                   "New velocity spatial dimensions must match existing fields.")
+        if self.velocityGrad is not None and self.velocityGrad.numel() > 0:
+            _check(self.velocityGrad.dim() == t.dim(), "New velocity does not match existing gradient tensor.")
+        self._velocity = t
+        self._velocityStatic = static
+        self._changed = True
+
+    def setVelocityType(self, velocityType):
+        _check(velocityType == BoundaryConditionType.DIRICHLET,
+               "Invalid velocity boundary type: Currently only Dirichlet boundaries are supported")
+        self._velocityType = BoundaryConditionType(velocityType)
+
+    def CreateVelocity(self, createStatic):
+        dims = self.getSpatialDims()
+        if createStatic:
+            v = torch.zeros((1, dims), dtype=self.getDtype(), device=self.getDevice())
+        else:
+            _check(self.hasSize(), "FixedBoundary is missing size to create a varying velocity.")
+            s = self.getSizes()
+            v = torch.zeros([1, dims] + [[s.x, s.y, s.z][dims - 1 - d] for d in range(dims)], dtype=self.getDtype(),
+                            device=self.getDevice())
+        self.setVelocity(v)
+
+    def getVelocityVarying(self, size=None):
+        if self._velocityStatic:
+            _check(self.hasSize() or size is not None,
+                   "FixedBoundary has no fields with spatial dimensions to infer varying velocity shape.")
+            s = self.getSizes() if self.hasSize() else size
+            dims = self.getSpatialDims()
+            shape = [[s[0], s[1], s[2]][dims - 1 - d] for d in range(dims)]
+            v = self._velocity.reshape([1, dims] + [1] * dims)
+            return v.repeat([1, 1] + shape).clone().contiguous()
+        return self._velocity
+
+    def makeVelocityVarying(self, size=None):
+        if self._velocityStatic:
+            self.setVelocity(self.getVelocityVarying(size))
+
+    def getVelocity(self, computational):
+        _check(self.hasSize(), "FixedBoundary has no size set.")
+        v = self.getVelocityVarying(None)
+        if computational and self.hasTransform():
+            return TransformVectors(v, self.transform, True)
+        return v
+
+    def GetFluxes(self):
+        """Boundary-normal fluxes det * (Minv u)_axis (domain_structs.cpp:527-542)."""
+        _check(self.hasSize(), "FixedBoundary has no size set.")
+        v = self.getVelocityVarying(None)
+        if self.hasTransform():
+            det = self.transform[..., -1]
+            f = det.unsqueeze(1) * TransformVectors(v, self.transform, True)
+        else:
+            f = v
+        return f[:, self._axis:self._axis + 1].clone()
+
+    def setVelocityGrad(self, t):
+        _check(t.shape == self._velocity.shape, "FixedBoundary.velocity_grad must match velocity.")
+        self.velocityGrad = t
+        self._changed = True
+
+    def CreateVelocityGrad(self):
+        self.setVelocityGrad(torch.zeros_like(self._velocity))
+
+    # -- passive scalar (stored, not transported) --
+    def setPassiveScalar(self, t):
+        self.passiveScalar = t
+        self._changed = True
+
+    def CreatePassiveScalar(self, createStatic):
+        ch = self.getParentDomain().getPassiveScalarChannels()
+        self.setPassiveScalar(torch.zeros((1, ch), dtype=self.getDtype(), device=self.getDevice()))
+        self.passiveScalarTypes = [self._velocityType] * ch
+
+    def hasPassiveScalar(self):
+        return self.passiveScalar is not None
+
+    def getPassiveScalarChannels(self):
+        return self.getParentDomain().getPassiveScalarChannels()
+
+    def isPassiveScalarStatic(self):
+        return self.passiveScalar is None or self.passiveScalar.dim() == 2
+
+    def isPassiveScalarBoundaryTypeStatic(self):
+        return self.passiveScalarTypes is None or len(set(self.passiveScalarTypes)) < 2
+
+    def setPassiveScalarType(self, t):
+        ch = self.getPassiveScalarChannels()
+        self.passiveScalarTypes = list(t) if isinstance(t, (list, tuple)) else [t] * ch
+
+    # -- transform --
+    def hasTransform(self):
+        return self.transform is not None
+
+    def setTransform(self, t):
+        dims = self.getSpatialDims()
+        _check(t.is_cuda and t.is_contiguous(), "transform must be a contiguous CUDA tensor")
+        _check(t.size(0) == 1, "Batches are not yet supported (transform).")
+        _check(t.dim() == 2 + dims, "Transform spatial dimensions are invalid. Transform must be 1-3D and have shape NDHWT. Dimensionality must match velocity.")
+        if self.hasSize():
+            s = self.getSizes()
+            _check(all(t.size(dims - d) == [s.x, s.y, s.z][d] for d in range(dims)),
+                   "Transform spatial dimensions must match existing fields.")
+        else:
+            self._setSizeFromTensor(t, False)
+        _check(t.size(-1) == _transform_size(dims), "Transform channels must match spatial dimensions")
+        self.transform = t
+        self._changed = True
+
+    def clearTransform(self):
+        if self.transform is not None:
+            self.transform = None
+            self._changed = True
+
+    def DetachFwd(self):
+        self._velocity = self._velocity.detach()
+        if self.transform is not None:
+            self.transform = self.transform.detach()
+
+    def DetachGrad(self):
+        self.velocityGrad = self.velocityGrad.detach()
+
+    def Detach(self):
+        self.DetachFwd()
+        self.DetachGrad()
+
+    def Copy(self):
+        return FixedBoundary(self.getParentDomain(), self._velocity, self._velocityType, self.passiveScalar, self.transform)
+
+    def Clone(self):
+        return FixedBoundary(self.getParentDomain(), self._velocity.clone(), self._velocityType,
+                             None if self.passiveScalar is None else self.passiveScalar.clone(),
+                             None if self.transform is None else self.transform.clone())
+
+    def __str__(self):
+        return "FIXED(%dD, size=%s, vStatic=%s, transform=%s)" % (
+            self.getSpatialDims(), self.getSizes() if self.hasSize() else "?", self._velocityStatic, self.hasTransform())
+
+
+# ------------------------------------------------------------------------------------------------
+# blocks (domain_structs.h:354-540)
+# ------------------------------------------------------------------------------------------------
+
+
+class Block:
+    def __init__(self, domain, velocity=None, pressure=None, passiveScalar=None, vertexCoordinates=None, name="Block",
+                 size=None):
+        self._domain_ref = weakref.ref(domain)
+        self.name = name
+        dims = domain.getSpatialDims()
+        dtype, device = domain.getDtype(), domain.getDevice()
+        if size is None:
+            _check(velocity is not None or pressure is not None or passiveScalar is not None or vertexCoordinates is not None,
+                   "At least one field (velocity, pressure, passiveScalar, vertexCoordinates) or the size must be given to create a block.")
+        if velocity is not None:
+            _check(velocity.is_cuda and velocity.is_contiguous(), "velocity must be a contiguous CUDA tensor")
+            _check(velocity.dim() == dims + 2, "Velocity dimensionality must match domain. Layout should be NC<spatial-dims>, e.g. NCDHW for 3D.")
+            _check(velocity.size(1) == dims, "The velocity channels must match the spatial dimensions.")
+            _check(velocity.size(0) == 1, "Batches are not yet supported.")
+            for d in range(2, velocity.dim()):
+                _check(velocity.size(d) > 2, "all spatial dimensions must be at least 3.")
+            _check(velocity.dtype == dtype, "Velocity dtype must match domain.")
+            self.velocity = velocity
+        else:
+            if size is not None:
+                zyx = [size[dims - 1 - d] for d in range(dims)]
+            elif pressure is not None:
+                zyx = list(pressure.shape[2:])
+            elif passiveScalar is not None:
+                zyx = list(passiveScalar.shape[2:])
+            else:
+                zyx = [s - 1 for s in vertexCoordinates.shape[2:]]
+            _check(len(zyx) == dims, "Field dimensionality must match domain. Layout should be NC<spatial-dims>, e.g. NCDHW for 3D.")
+            for s in zyx:
+                _check(s > 2, "all spatial dimensions must be at least 3.")
+            self.velocity = torch.zeros([1, dims] + zyx, dtype=dtype, device=device)
+        self.boundaries = [PeriodicBoundary(domain) for _ in range(2 * dims)]
+        self.pressure = None
+        if pressure is not None:
+            self.setPressure(pressure)
+        else:
+            self.CreatePressure()
+        self.passiveScalar = None
+        if passiveScalar is not None:
+            self.setPassiveScalar(passiveScalar)
+        elif domain.hasPassiveScalar():
+            self.CreatePassiveScalar()
+        self.viscosity = None
+        self.velocitySource = None
+        self.isVelocitySourceStatic = False
+        self.vertexCoordinates = None
+        self.transform = None
+        self.faceTransform = None
+        self.velocityGrad = torch.empty(0)
+        self.pressureGrad = torch.empty(0)
+        self.viscosityGrad = None
+        self.velocitySourceGrad = None
+        self.passiveScalarGrad = torch.empty(0)
+        self.globalOffset = 0
+        self.csrOffset = 0
+        self._changed = True
+        if vertexCoordinates is not None:
+            self.setVertexCoordinates(vertexCoordinates)
+
+    def getParentDomain(self):
+        d = self._domain_ref()
+        _check(d is not None, "Parent domain expired.")
+        return d
+
+    def getSpatialDims(self):
+        return self.getParentDomain().getSpatialDims()
+
+    def getDtype(self):
+        return self.velocity.dtype
+
+    def getDevice(self):
+        return self.velocity.device
+
+    def getDim(self, dim):
+        return self.velocity.size(dim)
+
+    def getAxis(self, dim):
+        _check(0 <= dim < self.getSpatialDims(), "Axis index must be within spatial dimensions")
+        return self.velocity.size(self.velocity.dim() - 1 - dim)
+
+    def getSizes(self):
+        dims = self.getSpatialDims()
+        s = [self.getAxis(d) for d in range(dims)] + [1] * (3 - dims)
+        return Int4(s[0], s[1], s[2], dims)
+
+    def getStrides(self):
+        s = self.getSizes()
+        return Int4(1, s.x, s.x * s.y, s.x * s.y * s.z)
+
+    def _ncells(self):
+        return self.getStrides().w
+
+    def _check_tensor(self, t, channels, allow_static, name):
+        dims = self.getSpatialDims()
+        _check(t.is_cuda, "%s must be a CUDA tensor" % name)
+        _check(t.is_contiguous(), "%s must be contiguous" % name)
+        _check(t.dtype == self.getDtype(), "%s dtype must match the domain." % name)
+        _check(t.size(0) == 1, "%s: batches are not yet supported." % name)
+        _check(t.size(1) == channels, "%s: channel dimension must be %d." % (name, channels))
+        if allow_static and t.dim() == 2:
+            return
+        _check(t.dim() == dims + 2, "%s: spatial dimensions must match the block." % name)
+        _check(list(t.shape[2:]) == list(self.velocity.shape[2:]), "%s: spatial size must match the block." % name)
+
+    # -- fields --
+    def setVelocity(self, v):
+        self._check_tensor(v, self.getSpatialDims(), False, "Velocity")
+        self.velocity = v
+        self._changed = True
+
+    def getVelocity(self, computational):
+        if computational:
+            _check(self.hasTransform(), "Coordinates or Transformations are required to compute computational velocities.")
+            return TransformVectors(self.velocity, self.transform, True)
+        return self.velocity
+
+    def CreateVelocity(self):
+        self.setVelocity(torch.zeros_like(self.velocity))
+
+    def setPressure(self, p):
+        self._check_tensor(p, 1, False, "Pressure")
+        self.pressure = p
+        self._changed = True
+
+    def CreatePressure(self):
+        self.pressure = torch.zeros([1, 1] + list(self.velocity.shape[2:]), dtype=self.getDtype(), device=self.getDevice())
+        self._changed = True
+
+    def setPassiveScalar(self, s):
+        ch = self.getPassiveScalarChannels()
+        _check(ch > 0, "Passive scalars are not active.")
+        self._check_tensor(s, ch, False, "Passive Scalar")
+        self.passiveScalar = s
+        self._changed = True
+
+    def CreatePassiveScalar(self):
+        ch = self.getPassiveScalarChannels()
+        _check(ch > 0, "Passive scalars are not active.")
+        self.passiveScalar = torch.zeros([1, ch] + list(self.velocity.shape[2:]), dtype=self.getDtype(), device=self.getDevice())
+        self._changed = True
+
+    def hasPassiveScalar(self):
+        return self.getParentDomain().hasPassiveScalar()
+
+    def getPassiveScalarChannels(self):
+        return self.getParentDomain().getPassiveScalarChannels()
+
+    def hasPassiveScalarViscosity(self):
+        return False
+
+    def setVelocitySource(self, t):
+        self._check_tensor(t, self.getSpatialDims(), True, "VelocitySource")
+        if self.velocitySourceGrad is not None:
+            _check(self.velocitySourceGrad.dim() == t.dim(), "New velocity source does not match existing gradient tensor.")
+        self.velocitySource = t
+        self.isVelocitySourceStatic = t.dim() == 2
+        self._changed = True
+
+    def hasVelocitySource(self):
+        return self.velocitySource is not None
+
+    def CreateVelocitySource(self, createStatic):
+        dims = self.getSpatialDims()
+        if createStatic:
+            t = torch.zeros((1, dims), dtype=self.getDtype(), device=self.getDevice())
+        else:
+            t = torch.zeros_like(self.velocity)
+        self.setVelocitySource(t)
+
+    def clearVelocitySource(self):
+        if self.velocitySource is not None:
+            self.velocitySource = None
+            self._changed = True
+
+    def setViscosity(self, v):
+        self._check_tensor(v, 1, True, "BlockViscosity")
+        if self.viscosityGrad is not None:
+            _check(self.viscosityGrad.dim() == v.dim(), "New block viscosity does not match existing gradient tensor.")
+        self.viscosity = v
+        self._changed = True
+
+    def hasViscosity(self):
+        return self.viscosity is not None
+
+    def isViscosityStatic(self):
+        return self.viscosity is None or self.viscosity.dim() == 2
+
+    def clearViscosity(self):
+        if self.viscosity is not None:
+            self.viscosity = None
+            self._changed = True
+
+    # -- gradients (adjoint fields) --
+    def setVelocityGrad(self, t):
+        self._check_tensor(t, self.getSpatialDims(), False, "VelocityGrad")
+        self.velocityGrad = t
+        self._changed = True
+
+    def CreateVelocityGrad(self):
+        self.setVelocityGrad(torch.zeros_like(self.velocity))
+
+    def setPressureGrad(self, t):
+        self._check_tensor(t, 1, False, "PressureGrad")
+        self.pressureGrad = t
+        self._changed = True
+
+    def CreatePressureGrad(self):
+        self.setPressureGrad(torch.zeros_like(self.pressure))
+
+    def setVelocitySourceGrad(self, t):
+        self.velocitySourceGrad = t
+        self._changed = True
+
+    def hasVelocitySourceGrad(self):
+        return self.velocitySourceGrad is not None
+
+    def CreateVelocitySourceGrad(self):
+        if self.velocitySource is not None:
+            self.setVelocitySourceGrad(torch.zeros_like(self.velocitySource))
+        else:
+            self.clearVelocitySourceGrad()
+
+    def clearVelocitySourceGrad(self):
+        if self.velocitySourceGrad is not None:
+            self.velocitySourceGrad = None
+            self._changed = True
+
+    def setViscosityGrad(self, t):
+        self.viscosityGrad = t
+        self._changed = True
+
+    def CreateViscosityGrad(self):
+        if self.viscosity is not None:
+            self.setViscosityGrad(torch.zeros_like(self.viscosity))
+
+    def hasViscosityGrad(self):
+        return self.viscosityGrad is not None
+
+    def clearViscosityGrad(self):
+        if self.viscosityGrad is not None:
+            self.viscosityGrad = None
+            self._changed = True
+
+    def CreateVelocityGradOnBoundaries(self):
+        for b in self.boundaries:
+            if isinstance(b, FixedBoundary):
+                b.CreateVelocityGrad()
+
+    def DetachFwd(self):
+        self.velocity = self.velocity.detach()
+        self.pressure = self.pressure.detach()
+        if self.velocitySource is not None:
+            self.velocitySource = self.velocitySource.detach()
+        if self.viscosity is not None:
+            self.viscosity = self.viscosity.detach()
+        for b in self.boundaries:
+            if isinstance(b, FixedBoundary):
+                b.DetachFwd()
+
+    def DetachGrad(self):
+        self.velocityGrad = self.velocityGrad.detach()
+        self.pressureGrad = self.pressureGrad.detach()
+        for b in self.boundaries:
+            if isinstance(b, FixedBoundary):
+                b.DetachGrad()
+
+    def Detach(self):
+        self.DetachFwd()
+        self.DetachGrad()
+
+    def IsTensorChanged(self):
+        return self._changed or any(b.IsTensorChanged() for b in self.boundaries)
+
+    def _set_unchanged(self):
+        self._changed = False
+        for b in self.boundaries:
+            b._changed = False
+
+    # -- coordinates and transforms --
+    def setVertexCoordinates(self, coords):
+        """Block::setVertexCoordinates, domain_structs.cpp:2001-2019."""
+        _check(coords.is_cuda and coords.is_contiguous(), "vertex coordinates must be a contiguous CUDA tensor")
+        _check(coords.dim() == self.velocity.dim(), "new vertex coordinates dimensions must match velocity.")
+        _check(coords.size(0) == 1, "batches are not yet supported.")
+        _check(coords.size(1) == self.getSpatialDims(), "vertex coordinates channel dimension must match spatial dimensions.")
+        for d in range(2, self.velocity.dim()):
+            _check(self.velocity.size(d) == coords.size(d) - 1, "vertex coordinates spatial dimension must match velocity's +1.")
+        _check(coords.dtype == self.velocity.dtype, "Vertex coordinates and velocity must have same dtype.")
+        self.clearCoordsTransforms()
+        self.vertexCoordinates = coords
+        self.transform = CoordsToTransforms(coords)
+        self.faceTransform = CoordsToFaceTransforms(coords)
+        self._UpdateBoundaryTransforms()
+        self._changed = True
+
+    def hasVertexCoordinates(self):
+        return self.vertexCoordinates is not None
+
+    def getCellCoordinates(self):
+        _check(self.hasVertexCoordinates(), "VertexCoordinates are required to compute cell coordinates.")
+        dims = self.getSpatialDims()
+        pool = {1: torch.nn.functional.avg_pool1d, 2: torch.nn.functional.avg_pool2d, 3: torch.nn.functional.avg_pool3d}[dims]
+        return pool(self.vertexCoordinates, 2, 1)
+
+    def setTransform(self, transform, faceTransform=None):
+        dims = self.getSpatialDims()
+        _check(transform.is_cuda and transform.is_contiguous(), "transform must be a contiguous CUDA tensor")
+        _check(transform.dim() == self.velocity.dim(), "new ransform dimensions must match velocity.")
+        _check(transform.size(-1) == _transform_size(dims), "Transform channels must match spatial dimensions")
+        self.clearCoordsTransforms()
+        self.transform = transform
+        self.faceTransform = faceTransform
+        self._UpdateBoundaryTransforms()
+        self._changed = True
+
+    def hasTransform(self):
+        return self.transform is not None
+
+    def hasFaceTransform(self):
+        return self.faceTransform is not None
+
+    def getCellSizes(self):
+        if self.hasTransform():
+            return torch.abs(self.transform[..., -1]).unsqueeze(1)
+        return torch.ones_like(self.pressure)
+
+    def clearCoordsTransforms(self):
+        self._changed = self._changed or self.hasTransform() or self.hasFaceTransform() or self.hasVertexCoordinates()
+        self.transform = None
+        self.faceTransform = None
+        self.vertexCoordinates = None
+
+    def GetCoordinateOrientation(self):
+        if not self.hasTransform():
+            return 1
+        s = torch.sign(self.transform[..., -1])
+        smin, smax = int(s.min().item()), int(s.max().item())
+        return 0 if smin != smax else smin
+
+    def _GetFaceTransformBoundarySlice(self, face):
+        """domain_structs.cpp:1809-1835."""
+        _check(self.hasFaceTransform(), "faceTransform missing to slice for boundary.")
+        dims = self.getSpatialDims()
+        axis, upper = face >> 1, face & 1
+        idx = [slice(None), axis]
+        for d in range(dims - 1, -1, -1):
+            if d == axis:
+                idx.append(slice(-1, None) if upper else slice(0, 1))
+            else:
+                idx.append(slice(0, -1))
+        idx.append(slice(None))
+        return self.faceTransform[tuple(idx)].clone().contiguous()
+
+    def _UpdateBoundaryTransforms(self):
+        if not self.hasFaceTransform():
+            return
+        for f, b in enumerate(self.boundaries):
+            if isinstance(b, FixedBoundary):
+                b.setTransform(self._GetFaceTransformBoundarySlice(f))
+
+    # -- boundaries --
+    def _check_face(self, face):
+        _check(0 <= face < 2 * self.getSpatialDims(),
+               "Face index must be in [0, dims*2) or one of {-x, +x, -y, +y, -z, +z} for exising spatial dimensions.")
+
+    def _setBoundary(self, faceIndex, boundary):
+        """Block::setBoundary, domain_structs.cpp:1653-1741."""
+        face = _face_index(faceIndex)
+        self._check_face(face)
+        dims = self.getSpatialDims()
+        if isinstance(boundary, FixedBoundary):
+            if boundary.hasSize():
+                _check(boundary.getSizes()[face >> 1] == 1, "Boundary axis size must be 1.")
+                for k in range(1, dims):
+                    ax = ((face >> 1) + k) % dims
+                    _check(boundary.getSizes()[ax] == self.getAxis(ax), "Boundary size must match block.")
+            else:
+                s = [self.getAxis(d) for d in range(dims)]
+                s[face >> 1] = 1
+                boundary._setSize(s)
+            if self.hasTransform() != boundary.hasTransform():
+                print("Warning: Only one of Block and FixedBoundary has a transformation set.")
+        elif isinstance(boundary, ConnectedBoundary):
+            other = boundary.getConnectedBlock()
+            for k in range(1, dims):
+                ax = ((face >> 1) + k) % dims
+                _check(self.getAxis(ax) == other.getAxis(boundary.getConnectionAxis(k)),
+                       "%s connection axis size does not match." % ("First" if k == 1 else "Second"))
+        self.boundaries[face] = boundary
+        self._changed = True
+
+    def getBoundary(self, faceIndex):
+        face = _face_index(faceIndex)
+        _check(0 <= face < 2 * self.getSpatialDims(), "Invalid boundary location specified.")
+        return self.boundaries[face]
+
+    def getBoundaries(self):
+        return list(self.boundaries)
+
+    def hasPrescribedBoundary(self):
+        return any(isinstance(b, FixedBoundary) for b in self.boundaries)
+
+    def getFixedBoundaries(self):
+        return [(i, b) for i, b in enumerate(self.boundaries) if isinstance(b, FixedBoundary)]
+
+    def isAllFixedBoundariesPassiveScalarTypeStatic(self):
+        return all(b.isPassiveScalarBoundaryTypeStatic() for _, b in self.getFixedBoundaries())
+
+    def _MakeFixedBoundary(self, face, velocity=None, passiveScalar=None):
+        """domain_structs.cpp:1897-1922."""
+        d = self.getParentDomain()
+        transform = self._GetFaceTransformBoundarySlice(face) if self.hasFaceTransform() else None
+        fb = FixedBoundary(d, velocity, BoundaryConditionType.DIRICHLET, passiveScalar, transform)
+        self._setBoundary(face, fb)
+
+    def _CloseConnectedBoundary(self, face):
+        """Block::CloseConnectedBoudary with useFixed, domain_structs.cpp:1773-1807."""
+        b = self.boundaries[face]
+        if isinstance(b, ConnectedBoundary):
+            b.getConnectedBlock()._MakeFixedBoundary(b.axes[0])
+        elif isinstance(b, PeriodicBoundary):
+            self._MakeFixedBoundary(face ^ 1)
+
+    def CloseBoundary(self, faceIndex, velocity=None, passiveScalar=None):
+        face = _face_index(faceIndex)
+        self._check_face(face)
+        self._CloseConnectedBoundary(face)
+        self._MakeFixedBoundary(face, velocity, passiveScalar)
+
+    def CloseAllBoundaries(self):
+        for f in range(2 * self.getSpatialDims()):
+            self.CloseBoundary(f)
+
+    def ConnectBlock(self, faceIndex, otherBlock, otherFaceIndex, axis1Index=-1, axis2Index=-1):
+        """Block::ConnectBlock -> ConnectBlocks, domain_structs.cpp:1064-1097, 1924-1930."""
+        face1 = _face_index(faceIndex)
+        face2 = _face_index(otherFaceIndex)
+        a1 = _face_index(axis1Index) if axis1Index not in (-1, "") else -1
+        a2 = _face_index(axis2Index) if axis2Index not in (-1, "") else -1
+        self._check_face(face1)
+        self._CloseConnectedBoundary(face1)
+        otherBlock._check_face(face2)
+        otherBlock._CloseConnectedBoundary(face2)
+        _check(self.getParentDomain() is otherBlock.getParentDomain(), "The blocks must belong to the same domain.")
+        dims = self.getSpatialDims()
+        axes1, axes2 = [face2], [face1]
+        if dims > 1:
+            axes1.append(a1)
+            f1d, f2d = face1 >> 1, face2 >> 1
+            swapped = False
+            if dims == 2 or (a1 >> 1) == (f2d + 1) % dims:
+                axes2.append((((f1d + 1) % dims) << 1) | (a1 & 1))
+            else:
+                _check((a2 >> 1) == (f2d + 1) % dims, "Invalid connection.")
+                axes2.append((((f1d + 2) % dims) << 1) | (a2 & 1))
+                swapped = True
+            if dims > 2:
+                axes1.append(a2)
+                if not swapped:
+                    axes2.append((((f1d + 2) % dims) << 1) | (a2 & 1))
+                else:
+                    axes2.append((((f1d + 1) % dims) << 1) | (a1 & 1))
+        d = self.getParentDomain()
+        self._setBoundary(face1, ConnectedBoundary(otherBlock, axes1, d))
+        otherBlock._setBoundary(face2, ConnectedBoundary(self, axes2, d))
+
+    def MakePeriodic(self, axisIndex):
+        axis = _axis_index(axisIndex)
+        _check(0 <= axis < self.getSpatialDims(), "Axis index must be in [0, dims) or one of {x, y, z} for exising spatial dimensions.")
+        lo, hi = axis << 1, (axis << 1) | 1
+        bl, bh = self.boundaries[lo], self.boundaries[hi]
+        if not (isinstance(bl, PeriodicBoundary) and isinstance(bh, PeriodicBoundary)):
+            if isinstance(bl, ConnectedBoundary):
+                self._CloseConnectedBoundary(lo)
+            if isinstance(bh, ConnectedBoundary):
+                self._CloseConnectedBoundary(hi)
+            d = self.getParentDomain()
+            if not isinstance(self.boundaries[lo], PeriodicBoundary):
+                self._setBoundary(lo, PeriodicBoundary(d))
+            if not isinstance(self.boundaries[hi], PeriodicBoundary):
+                self._setBoundary(hi, PeriodicBoundary(d))
+
+    def MakeAllPeriodic(self):
+        for a in range(self.getSpatialDims()):
+            self.MakePeriodic(a)
+
+    def ComputeCSRSize(self):
+        """domain_structs.cpp:2151-2161."""
+        s = self.getSizes()
+        sz = [s.x, s.y, s.z]
+        n = s.x * s.y * s.z * (2 * self.getSpatialDims() + 1)
+        for d in range(self.getSpatialDims()):
+            area = sz[(d + 1) % 3] * sz[(d + 2) % 3]
+            if isinstance(self.boundaries[2 * d], FixedBoundary):
+                n -= area
+            if isinstance(self.boundaries[2 * d + 1], FixedBoundary):
+                n -= area
+        return n
+
+    # -- velocity statistics --
+    def getMaxVelocity(self, withBounds=True, computational=False):
+        m = torch.max(torch.abs(self.getVelocity(computational)))
+        if withBounds:
+            for b in self.boundaries:
+                if isinstance(b, FixedBoundary):
+                    m = torch.maximum(m, torch.max(torch.abs(b.getVelocity(computational))))
+        return m
+
+    def getMaxVelocityMagnitude(self, withBounds=True, computational=False):
+        m = torch.max(torch.linalg.vector_norm(self.getVelocity(computational), dim=1))
+        if withBounds:
+            for b in self.boundaries:
+                if isinstance(b, FixedBoundary):
+                    m = torch.maximum(m, torch.max(torch.linalg.vector_norm(b.getVelocity(computational), dim=1)))
+        return m
+
+    def __str__(self):
+        s = self.getSizes()
+        return 'Block("%s", size=%s, boundaries=[%s])' % (self.name, s, ", ".join(str(b) for b in self.boundaries))
+
+
+# ------------------------------------------------------------------------------------------------
+# domain (domain_structs.h:563-787)
+# ------------------------------------------------------------------------------------------------
+
+
+class Domain:
+    def __init__(self, spatialDims, viscosity, name="Domain", dtype=torch.float32, device=None,
+                 passiveScalarChannels=1, scalarViscosity=None):
+        _check(0 < spatialDims < 4, "spatialDims must be 1, 2, or 3.")
+        _check(passiveScalarChannels >= 0, "passiveScalarChannels can't be negative.")
+        self.name = name
+        self._dims = int(spatialDims)
+        self._dtype = dtype
+        _dtype_code(dtype)
+        device = torch.device("cuda") if device is None else torch.device(device)
+        _check(device.type == "cuda", "device must be a CUDA device.")
+        if device.index is None:
+            device = torch.device("cuda", 0)
+        self._device = device
+        self._psc = int(passiveScalarChannels)
+        self.blocks: List[Block] = []
+        self.passiveScalarViscosity = scalarViscosity
+        self.setViscosity(viscosity)
+        self._initialized = False
+        self._changed = True
+        self._csr_struct = None
+        self.viscosityGrad = None
+        self.passiveScalarViscosityGrad = None
+
+    # -- basic properties --
+    def getSpatialDims(self):
+        return self._dims
+
+    def getDtype(self):
+        return self._dtype
+
+    def getDevice(self):
+        return self._device
+
+    def getPassiveScalarChannels(self):
+        return self._psc
+
+    def hasPassiveScalar(self):
+        return self._psc > 0
+
+    def getNumBlocks(self):
+        return len(self.blocks)
+
+    def getBlock(self, index):
+        return self.blocks[index]
+
+    def getBlocks(self):
+        return list(self.blocks)
+
+    def getTotalSize(self):
+        return sum(b._ncells() for b in self.blocks)
+
+    def getMaxBlockSize(self):
+        return max(b._ncells() for b in self.blocks)
+
+    def IsInitialized(self):
+        return self._initialized
+
+    def IsTensorChanged(self):
+        return self._changed or any(b.IsTensorChanged() for b in self.blocks)
+
+    def setViscosity(self, viscosity):
+        _check(isinstance(viscosity, torch.Tensor) and not viscosity.is_cuda, "viscosity must be a host tensor")
+        _check(viscosity.dim() == 1 and viscosity.size(0) == 1, "viscosity must be a scalar.")
+        self.viscosity = viscosity
+        if getattr(self, "_initialized", False):
+            self._sim_visc.copy_(viscosity.to(self._dtype), non_blocking=False)
+
+    def hasBlockViscosity(self):
+        return any(b.hasViscosity() for b in self.blocks)
+
+    def hasPassiveScalarViscosity(self):
+        return self.passiveScalarViscosity is not None
+
+    def isPassiveScalarViscosityStatic(self):
+        return self.passiveScalarViscosity is None or self.passiveScalarViscosity.size(0) == 1
+
+    def setScalarViscosity(self, v):
+        self.passiveScalarViscosity = v
+
+    def clearScalarViscosity(self):
+        self.passiveScalarViscosity = None
+
+    def hasPassiveScalarBlockViscosity(self):
+        return False
+
+    # -- blocks --
+    def CreateBlock(self, velocity=None, pressure=None, passiveScalar=None, vertexCoordinates=None, name="Block"):
+        b = Block(self, velocity, pressure, passiveScalar, vertexCoordinates, name)
+        _check(b.getDevice() == self._device, "Block has wrong device")
+        self.AddBlock(b)
+        return b
+
+    def CreateBlockWithSize(self, size, name="Block"):
+        size = [size[0], size[1], size[2]] if not isinstance(size, Int4) else [size.x, size.y, size.z]
+        _check(size[0] > 2, "size.x must be at least 3.")
+        if self._dims > 1:
+            _check(size[1] > 2, "size.y must be at least 3.")
+        if self._dims > 2:
+            _check(size[2] > 2, "size.z must be at least 3.")
+        b = Block(self, name=name, size=size[:self._dims])
+        self.AddBlock(b)
+        return b
+
+    def AddBlock(self, block):
+        _check(block.getSpatialDims() == self._dims, "Number of block spatial dimensions does not match domain.")
+        _check(block.getDtype() == self._dtype, "Data typ does not match.")
+        self.blocks.append(block)
+        self._initialized = False
+
+    def _block_index(self, block):
+        for i, b in enumerate(self.blocks):
+            if b is block:
+                return i
+        return -1
+
+    # -- statistics --
+    def getMaxVelocity(self, withBounds=True, computational=False):
+        _check(len(self.blocks) > 0, "Domain does not contain any blocks.")
+        m = self.blocks[0].getMaxVelocity(withBounds, computational)
+        for b in self.blocks[1:]:
+            m = torch.maximum(m, b.getMaxVelocity(withBounds, computational))
+        return m
+
+    def getMaxVelocityMagnitude(self, withBounds=True, computational=False):
+        _check(len(self.blocks) > 0, "Domain does not contain any blocks.")
+        m = self.blocks[0].getMaxVelocityMagnitude(withBounds, computational)
+        for b in self.blocks[1:]:
+            m = torch.maximum(m, b.getMaxVelocityMagnitude(withBounds, computational))
+        return m
+
+    def hasVertexCoordinates(self):
+        return len(self.blocks) > 0 and all(b.hasVertexCoordinates() for b in self.blocks)
+
+    def getVertexCoordinates(self):
+        _check(len(self.blocks) > 0, "Domain does not contain any blocks.")
+        out = []
+        for b in self.blocks:
+            _check(b.hasVertexCoordinates(), "a block is missing vertex coordinates")
+            out.append(b.vertexCoordinates)
+        return out
+
+    def GetCoordinateOrientation(self):
+        _check(len(self.blocks) > 0, "Domain does not contain any blocks.")
+        s = self.blocks[0].GetCoordinateOrientation()
+        for b in self.blocks[1:]:
+            if b.GetCoordinateOrientation() != s:
+                return 0
+        return s
+
+    def hasPrescribedBoundary(self):
+        return any(b.hasPrescribedBoundary() for b in self.blocks)
+
+    def isAllFixedBoundariesPassiveScalarTypeStatic(self):
+        return all(b.isAllFixedBoundariesPassiveScalarTypeStatic() for b in self.blocks)
+
+    def GetBoundaryFluxBalance(self):
+        """Domain::GetGlobalFluxBalance, domain_structs.cpp:2460-2493."""
+        s = torch.zeros([1], dtype=self._dtype, device=self._device)
+        for b in self.blocks:
+            for i, bnd in enumerate(b.boundaries):
+                if isinstance(bnd, FixedBoundary):
+                    f = torch.sum(bnd.GetFluxes())
+                    s = s + (f if (i & 1) else -f)
+        return s
+
+    def CheckBoundaryFluxBalance(self, eps=1e-5):
+        return abs(self.GetBoundaryFluxBalance().item()) < eps
+
+    # -- preparation (Domain::PrepareSolve, domain_structs.cpp:2554-2676) --
+    def PrepareSolve(self):
+        _check(len(self.blocks) > 0, "Domain does not contain any blocks.")
+        _check(self.viscosity.dtype == self._dtype, "Data type of viscosity does not match.")
+        dims = self._dims
+        N = 0
+        csr = 0
+        for b in self.blocks:
+            b.globalOffset = N
+            b.csrOffset = csr
+            csr += b.ComputeCSRSize()
+            N += b._ncells()
+            for f, bnd in enumerate(b.boundaries):
+                if isinstance(bnd, ConnectedBoundary):
+                    other = bnd.getConnectedBlock()
+                    _check(self._block_index(other) >= 0, "Connected block is not part of this domain.")
+                    ob = other.boundaries[bnd.axes[0]]
+                    _check(isinstance(ob, ConnectedBoundary),
+                           "Mismatch in block connection: connected block is not connected at the target face.")
+                    _check(ob.getConnectedBlock() is b,
+                           "Mismatch in block connection: connected block is connected to a different block at the target face.")
+                    _check(ob.axes[0] == f,
+                           "Mismatch in block connection: connected block is connected to a different face of the source block.")
+                elif isinstance(bnd, PeriodicBoundary):
+                    _check(isinstance(b.boundaries[f ^ 1], PeriodicBoundary), "Opposite boundary must also be periodic.")
+        self._N = N
+        self._K = 2 * dims + 1
+        opts = dict(dtype=self._dtype, device=self._device)
+        self.C = StencilMatrix(self, torch.zeros((self._K, N), **opts))
+        self.P = StencilMatrix(self, torch.zeros((self._K, N), **opts))
+        self.CGrad = self.C.WithZeroValue()
+        self.PGrad = self.P.WithZeroValue()
+        self.A = torch.zeros(N, **opts)
+        self.AGrad = torch.empty(0)
+        if self.hasPassiveScalar():
+            self.scalarRHS = torch.zeros(N * self._psc, **opts)
+            self.scalarResult = torch.zeros(N * self._psc, **opts)
+        else:
+            self.scalarRHS = torch.empty(0, **opts)
+            self.scalarResult = torch.empty(0, **opts)
+        self.velocityRHS = torch.zeros(N * dims, **opts)
+        self.velocityResult = torch.zeros(N * dims, **opts)
+        self.pressureRHS = torch.zeros(N * dims, **opts)
+        self.pressureRHSdiv = torch.zeros(N, **opts)
+        self.pressureResult = torch.zeros(N, **opts)
+        for name in ["scalarRHSGrad", "scalarResultGrad", "velocityRHSGrad", "velocityResultGrad", "pressureRHSGrad",
+                     "pressureRHSdivGrad", "pressureResultGrad"]:
+            setattr(self, name, torch.empty(0))
+        # topology on the host (native), then upload
+        self._sim_visc = self.viscosity.to(self._dtype).to(self._device)
+        self._sim_cells = torch.tensor([0, N], dtype=torch.int32, device=self._device)
+        self._sim_blocks = torch.tensor([0, len(self.blocks)], dtype=torch.int32, device=self._device)
+        host_blocks = self._pack_blocks()
+        nbr = torch.empty((2 * dims, N), dtype=torch.int32)
+        cell_block = torch.empty(N, dtype=torch.int32)
+        check(_lib.load().pict_build_topology(host_blocks, len(self.blocks), dims, N, nbr.data_ptr(),
+                                              cell_block.data_ptr()), "build_topology")
+        self._nbr = nbr.to(self._device)
+        self._cell_block = cell_block.to(self._device)
+        self._csr_struct = None
+        self._initialized = True
+        self.UpdateDomainData()
+
+    def _pack_blocks(self):
+        """Host block table with raw device pointers (Domain::UpdateDomainGPU, domain_structs.cpp:3040-3261)."""
+        arr = (BlockDesc * len(self.blocks))()
+        index = {id(b): i for i, b in enumerate(self.blocks)}
+        for bi, b in enumerate(self.blocks):
+            d = arr[bi]
+            s = b.getSizes()
+            d.size[0], d.size[1], d.size[2] = s.x, s.y, s.z
+            d.offset = b.globalOffset
+            d.sim = 0
+            d.velocity = _ptr(b.velocity)
+            d.pressure = _ptr(b.pressure)
+            d.transform = _ptr(b.transform) if b.hasTransform() else None
+            if b.viscosity is not None:
+                d.viscosity = _ptr(b.viscosity)
+                d.viscosity_static = 1 if b.viscosity.dim() == 2 else 0
+            if b.velocitySource is not None:
+                d.source = _ptr(b.velocitySource)
+                d.source_static = 1 if b.isVelocitySourceStatic else 0
+            d.velocity_grad = _ptr(b.velocityGrad) if b.velocityGrad.numel() > 0 else None
+            d.pressure_grad = _ptr(b.pressureGrad) if b.pressureGrad.numel() > 0 else None
+            d.viscosity_grad = _ptr(b.viscosityGrad) if b.viscosityGrad is not None else None
+            d.source_grad = _ptr(b.velocitySourceGrad) if b.velocitySourceGrad is not None else None
+            for f, bnd in enumerate(b.boundaries):
+                F = d.face[f]
+                if isinstance(bnd, FixedBoundary):
+                    F.type = _lib.PICT_FACE_FIXED
+                    F.vel_static = 1 if bnd.isVelocityStatic else 0
+                    F.velocity = _ptr(bnd.velocity)
+                    F.transform = _ptr(bnd.transform) if bnd.hasTransform() else None
+                    F.velocity_grad = _ptr(bnd.velocityGrad) if bnd.velocityGrad is not None and bnd.velocityGrad.numel() > 0 else None
+                elif isinstance(bnd, PeriodicBoundary):
+                    F.type = _lib.PICT_FACE_PERIODIC
+                elif isinstance(bnd, ConnectedBoundary):
+                    F.type = _lib.PICT_FACE_CONNECTED
+                    F.conn_block = index[id(bnd.getConnectedBlock())]
+                    for k in range(len(bnd.axes)):
+                        F.conn_axes[k] = bnd.axes[k]
+                else:
+                    raise NotImplementedError("boundary type %s is not supported" % type(bnd).__name__)
+        return arr
+
+    def UpdateDomainData(self):
+        """Re-pack raw pointers after tensors were replaced (Domain::UpdateDomain, domain_structs.cpp:3031-3038)."""
+        _check(self._initialized, "Domain is not initialized.")
+        host = self._pack_blocks()
+        raw = bytes(host)
+        if getattr(self, "_blocks_raw", None) != raw:
+            buf = torch.frombuffer(bytearray(raw), dtype=torch.uint8).pin_memory()
+            if getattr(self, "_blocks_dev", None) is None or self._blocks_dev.numel() != buf.numel():
+                self._blocks_dev = torch.empty(buf.numel(), dtype=torch.uint8, device=self._device)
+            self._blocks_dev.copy_(buf, non_blocking=True)
+            self._blocks_raw = raw
+            self._blocks_host = buf
+        self._desc = self._make_desc()
+        self._changed = False
+        for b in self.blocks:
+            b._set_unchanged()
+
+    def _make_desc(self, C=None, P=None):
+        d = DomainDesc()
+        d.dims = self._dims
+        d.num_blocks = len(self.blocks)
+        d.num_cells = self._N
+        d.num_sims = 1
+        d.dtype = _dtype_code(self._dtype)
+        d.max_sim_cells = self._N
+        d.blocks = self._blocks_dev.data_ptr()
+        d.nbr = _ptr(self._nbr)
+        d.cell_block = _ptr(self._cell_block)
+        d.sim_cells = _ptr(self._sim_cells)
+        d.sim_blocks = _ptr(self._sim_blocks)
+        d.sim_viscosity = _ptr(self._sim_visc)
+        d.sim_dt = None
+        d.C = _ptr(self.C.coef if C is None else C)
+        d.A = _ptr(self.A)
+        d.P = _ptr(self.P.coef if P is None else P)
+        d.velocity_rhs = _ptr(self.velocityRHS)
+        d.velocity_result = _ptr(self.velocityResult)
+        d.pressure_rhs = _ptr(self.pressureRHS)
+        d.pressure_rhs_div = _ptr(self.pressureRHSdiv)
+        d.pressure_result = _ptr(self.pressureResult)
+        return d
+
+    def _check_ready(self):
+        _check(len(self.blocks) > 0, "Domain does not contain blocks.")
+        _check(self._initialized, "Domain is not initialized.")
+        _check(not self.IsTensorChanged(), "Domain's tensors have been changed, use UpdateDomain() to set the new pointers.")
+        # keep the packed global pointers in sync with the current tensors
+        self._desc = self._make_desc()
+
+    def _csr_structure(self):
+        if self._csr_struct is None:
+            row = torch.empty(self._N + 1, dtype=torch.int32, device=self._device)
+            check(_lib.load().pict_csr_row_ptr(ctypes.byref(self._desc), _ptr(row), _stream_ptr()), "csr_row_ptr")
+            nnz = int(row[-1].item())
+            index = torch.empty(nnz, dtype=torch.int32, device=self._device)
+            tmp = torch.empty(nnz, dtype=self._dtype, device=self._device)
+            check(_lib.load().pict_stencil_to_csr(ctypes.byref(self._desc), _ptr(self.C.coef), _ptr(row), _ptr(tmp),
+                                                  _ptr(index), _stream_ptr()), "stencil_to_csr")
+            self._csr_struct = (row, index)
+        return self._csr_struct
+
+    # -- global field setters (domain_structs.cpp:2750-2828) --
+    def _set_global(self, name, t, size):
+        _check(t.is_cuda and t.is_contiguous() and t.dim() == 1, "%s must be a contiguous 1D CUDA tensor" % name)
+        _check(t.size(0) == size, "%s has the wrong size (%d, expected %d)" % (name, t.size(0), size))
+        _check(t.dtype == self._dtype, "%s dtype must match the domain" % name)
+        setattr(self, name, t)
+        self._changed = True
+
+    def setA(self, t):
+        self._set_global("A", t, self._N)
+
+    def CreateA(self):
+        self.setA(torch.zeros(self._N, dtype=self._dtype, device=self._device))
+
+    def setVelocityRHS(self, t):
+        self._set_global("velocityRHS", t, self._N * self._dims)
+
+    def setVelocityResult(self, t):
+        self._set_global("velocityResult", t, self._N * self._dims)
+
+    def setPressureRHS(self, t):
+        self._set_global("pressureRHS", t, self._N * self._dims)
+
+    def setPressureRHSdiv(self, t):
+        self._set_global("pressureRHSdiv", t, self._N)
+
+    def setPressureResult(self, t):
+        self._set_global("pressureResult", t, self._N)
+
+    def setScalarRHS(self, t):
+        self._set_global("scalarRHS", t, self._N * self._psc)
+
+    def setScalarResult(self, t):
+        self._set_global("scalarResult", t, self._N * self._psc)
+
+    def CreateVelocityRHS(self):
+        self.setVelocityRHS(torch.zeros(self._N * self._dims, dtype=self._dtype, device=self._device))
+
+    def CreateVelocityResult(self):
+        self.setVelocityResult(torch.zeros(self._N * self._dims, dtype=self._dtype, device=self._device))
+
+    def CreatePressureRHS(self):
+        self.setPressureRHS(torch.zeros(self._N * self._dims, dtype=self._dtype, device=self._device))
+
+    def CreatePressureRHSdiv(self):
+        self.setPressureRHSdiv(torch.zeros(self._N, dtype=self._dtype, device=self._device))
+
+    def CreatePressureResult(self):
+        self.setPressureResult(torch.zeros(self._N, dtype=self._dtype, device=self._device))
+
+    def CreateVelocityOnBlocks(self):
+        for b in self.blocks:
+            b.CreateVelocity()
+
+    def CreatePressureOnBlocks(self):
+        for b in self.blocks:
+            b.CreatePressure()
+
+    def CreateVelocityGradOnBlocks(self):
+        for b in self.blocks:
+            b.CreateVelocityGrad()
+
+    def CreatePressureGradOnBlocks(self):
+        for b in self.blocks:
+            b.CreatePressureGrad()
+
+    def CreateVelocitySourceGradOnBlocks(self):
+        for b in self.blocks:
+            b.CreateVelocitySourceGrad()
+
+    def CreateVelocityGradOnBoundaries(self):
+        for b in self.blocks:
+            b.CreateVelocityGradOnBoundaries()
+
+    def CreateViscosityGrad(self):
+        self.viscosityGrad = torch.zeros_like(self.viscosity)
+
+    def setViscosityGrad(self, t):
+        self.viscosityGrad = t
+
+    def hasViscosityGrad(self):
+        return self.viscosityGrad is not None
+
+    def clearViscosityGrad(self):
+        self.viscosityGrad = None
+
+    # -- copies --
+    def DetachFwd(self):
+        for b in self.blocks:
+            b.DetachFwd()
+        for name in ["A", "velocityRHS", "velocityResult", "pressureRHS", "pressureRHSdiv", "pressureResult"]:
+            if hasattr(self, name):
+                setattr(self, name, getattr(self, name).detach())
+        if hasattr(self, "C"):
+            self.C.detach()
+            self.P.detach()
+
+    def DetachGrad(self):
+        for b in self.blocks:
+            b.DetachGrad()
+
+    def Detach(self):
+        self.DetachFwd()
+        self.DetachGrad()
+
+    def _copy_structure(self, clone, newName):
+        d = Domain(self._dims, self.viscosity.clone() if clone else self.viscosity, newName or (self.name + "_copy"),
+                   self._dtype, self._device, self._psc)
+        mapping = {}
+        for b in self.blocks:
+            nb = Block(d, b.velocity.clone() if clone else b.velocity, b.pressure.clone() if clone else b.pressure,
+                       None, None, b.name)
+            nb.transform = None if b.transform is None else (b.transform.clone() if clone else b.transform)
+            nb.faceTransform = None if b.faceTransform is None else (b.faceTransform.clone() if clone else b.faceTransform)
+            nb.vertexCoordinates = None if b.vertexCoordinates is None else (b.vertexCoordinates.clone() if clone else b.vertexCoordinates)
+            if b.viscosity is not None:
+                nb.viscosity = b.viscosity.clone() if clone else b.viscosity
+            if b.velocitySource is not None:
+                nb.velocitySource = b.velocitySource.clone() if clone else b.velocitySource
+                nb.isVelocitySourceStatic = b.isVelocitySourceStatic
+            d.AddBlock(nb)
+            mapping[id(b)] = nb
+        for b in self.blocks:
+            nb = mapping[id(b)]
+            for f, bnd in enumerate(b.boundaries):
+                if isinstance(bnd, FixedBoundary):
+                    fb = FixedBoundary(d, bnd.velocity.clone() if clone else bnd.velocity, bnd.velocityType, None,
+                                       None if bnd.transform is None else (bnd.transform.clone() if clone else bnd.transform))
+                    nb.boundaries[f] = fb
+                    fb._size = list(bnd._size) if bnd._size is not None else None
+                    fb._axis = bnd._axis
+                elif isinstance(bnd, ConnectedBoundary):
+                    nb.boundaries[f] = ConnectedBoundary(mapping[id(bnd.getConnectedBlock())], bnd.axes, d)
+                else:
+                    nb.boundaries[f] = PeriodicBoundary(d)
+        return d
+
+    def Copy(self, newName=None):
+        return self._copy_structure(False, newName)
+
+    def Clone(self, newName=None):
+        return self._copy_structure(True, newName)
+
+    def __str__(self):
+        return 'Domain("%s", %dD, blocks=%d, cells=%d, dtype=%s)' % (
+            self.name, self._dims, len(self.blocks), self.getTotalSize(), self._dtype)
+
+
+# ------------------------------------------------------------------------------------------------
+# operators (PISOtorch.cpp:529-601)
+# ------------------------------------------------------------------------------------------------
+
+
+def _time_step(timeStep, domain):
+    _check(isinstance(timeStep, torch.Tensor), "timeStep must be a tensor")
+    _check(not timeStep.is_cuda, "timeStep must be a host tensor")
+    _check(timeStep.dim() == 1 and timeStep.size(0) == 1, "timeStep must be 1D." if timeStep.dim() != 1 else "timeStep must be a scalar.")
+    _check(timeStep.dtype == domain.getDtype(), "Data type of timeStep does not match.")
+    return float(timeStep.item())
+
+
+def _non_ortho(flags):
+    if int(flags) != 0:
+        raise NotImplementedError("non-orthogonal corrections (nonOrthoFlags != 0) are not implemented in pict_b200")
+
+
+def SetupAdvectionMatrix(domain, timeStep, nonOrthoFlags, forPassiveScalar=False, passiveScalarChannel=0):
+    """Implicit advection-diffusion matrix C and its diagonal A (kernel.cu:3601-3865)."""
+    if forPassiveScalar:
+        raise NotImplementedError("passive scalar transport is not implemented in pict_b200")
+    _non_ortho(nonOrthoFlags)
+    domain._check_ready()
+    dt = _time_step(timeStep, domain)
+    check(_lib.load().pict_setup_advection_matrix(ctypes.byref(domain._desc), dt, 0, _stream_ptr()), "SetupAdvectionMatrix")
+
+
+def SetupAdvectionVelocity(domain, timeStep, nonOrthoFlags, applyPressureGradient=False):
+    """Velocity RHS of the advection-diffusion solve (kernel.cu:4281-4385)."""
+    _non_ortho(nonOrthoFlags)
+    domain._check_ready()
+    dt = _time_step(timeStep, domain)
+    check(_lib.load().pict_setup_advection_velocity(ctypes.byref(domain._desc), dt, 0, int(bool(applyPressureGradient)),
+                                                    _stream_ptr()), "SetupAdvectionVelocity")
+
+
+def SetupAdvectionScalar(domain, timeStep, nonOrthoFlags):
+    raise NotImplementedError("passive scalar transport is not implemented in pict_b200")
+
+
+def SetupPressureCorrection(domain, timeStep, nonOrthoMode=0, useFaceTransform=False, timeStepNorm=False):
+    """Pressure matrix, H/A RHS and its divergence (kernel.cu:4797-5419)."""
+    _non_ortho(nonOrthoMode)
+    if useFaceTransform:
+        raise NotImplementedError("face-transform pressure assembly is not implemented in pict_b200")
+    domain._check_ready()
+    dt = _time_step(timeStep, domain)
+    check(_lib.load().pict_setup_pressure_correction(ctypes.byref(domain._desc), dt, 0, int(bool(timeStepNorm)),
+                                                     _stream_ptr()), "SetupPressureCorrection")
+
+
+def SetupPressureMatrix(domain, timeStep, nonOrthoMode=0, useFaceTransform=False):
+    _non_ortho(nonOrthoMode)
+    if useFaceTransform:
+        raise NotImplementedError("face-transform pressure assembly is not implemented in pict_b200")
+    domain._check_ready()
+    _time_step(timeStep, domain)
+    check(_lib.load().pict_setup_pressure_matrix(ctypes.byref(domain._desc), 0, _stream_ptr()), "SetupPressureMatrix")
+
+
+def SetupPressureRHS(domain, timeStep, nonOrthoMode=0, useFaceTransform=False, timeStepNorm=False):
+    _non_ortho(nonOrthoMode)
+    if useFaceTransform:
+        raise NotImplementedError("face-transform pressure assembly is not implemented in pict_b200")
+    domain._check_ready()
+    dt = _time_step(timeStep, domain)
+    check(_lib.load().pict_setup_pressure_rhs(ctypes.byref(domain._desc), dt, 0, int(bool(timeStepNorm)), _stream_ptr()),
+          "SetupPressureRHS")
+
+
+def SetupPressureRHSdiv(domain, timeStep, nonOrthoMode=0, useFaceTransform=False, timeStepNorm=False):
+    _non_ortho(nonOrthoMode)
+    if useFaceTransform:
+        raise NotImplementedError("face-transform pressure assembly is not implemented in pict_b200")
+    domain._check_ready()
+    dt = _time_step(timeStep, domain)
+    check(_lib.load().pict_setup_pressure_rhs_div(ctypes.byref(domain._desc), dt, 0, int(bool(timeStepNorm)),
+                                                  _stream_ptr()), "SetupPressureRHSdiv")
+
+
+def CorrectVelocity(domain, timeStep, version=0, timeStepNorm=False):
+    """u = H/A - grad(p)/A with finite-difference pressure gradients (kernel.cu:5947-5980)."""
+    if version not in (0, 1):
+        raise NotImplementedError("only the finite-difference velocity corrector (version 0/1) is implemented in pict_b200")
+    domain._check_ready()
+    dt = _time_step(timeStep, domain)
+    check(_lib.load().pict_correct_velocity(ctypes.byref(domain._desc), dt, 1, int(bool(timeStepNorm)), 0,
+                                            _stream_ptr()), "CorrectVelocity")
+
+
+def _copy(domain, fn, what):
+    domain._check_ready()
+    check(getattr(_lib.load(), fn)(ctypes.byref(domain._desc), _stream_ptr()), what)
+
+
+def CopyVelocityResultToBlocks(domain):
+    _copy(domain, "pict_copy_velocity_result_to_blocks", "CopyVelocityResultToBlocks")
+
+
+def CopyVelocityResultFromBlocks(domain):
+    _copy(domain, "pict_copy_velocity_result_from_blocks", "CopyVelocityResultFromBlocks")
+
+
+def CopyPressureResultToBlocks(domain):
+    _copy(domain, "pict_copy_pressure_result_to_blocks", "CopyPressureResultToBlocks")
+
+
+def CopyPressureResultFromBlocks(domain):
+    _copy(domain, "pict_copy_pressure_result_from_blocks", "CopyPressureResultFromBlocks")
+
+
+def CopyScalarResultToBlocks(domain):
+    raise NotImplementedError("passive scalar transport is not implemented in pict_b200")
+
+
+def CopyScalarResultFromBlocks(domain):
+    raise NotImplementedError("passive scalar transport is not implemented in pict_b200")
+
+
+def ComputeVelocityDivergence(domain):
+    """Flux divergence of the blocks' velocity (kernel.cu:6333-6388)."""
+    domain._check_ready()
+    out = torch.zeros_like(domain.pressureResult)
+    check(_lib.load().pict_velocity_divergence(ctypes.byref(domain._desc), _ptr(out), _stream_ptr()),
+          "ComputeVelocityDivergence")
+    return out
+
+
+def CoordsToTransforms(coords):
+    """Cell transforms (M, Minv, det) from vertex coordinates (grid_gen.cu:341-375)."""
+    _check(coords.is_cuda and coords.is_contiguous(), "coords must be a contiguous CUDA tensor")
+    _check(2 < coords.dim() < 6, "coords must have batch and channel dimension and be 1-3D.")
+    _check(coords.size(0) == 1, "coords batch dimension must be 1.")
+    dims = coords.dim() - 2
+    _check(coords.size(1) == dims, "coords channel dimension must match spatial dimensionality.")
+    size = [coords.size(-1 - d) - 1 for d in range(dims)]
+    out = torch.zeros([1] + [size[dims - 1 - d] for d in range(dims)] + [_transform_size(dims)],
+                      dtype=coords.dtype, device=coords.device)
+    sz = (ctypes.c_int32 * 3)(*(size + [1] * (3 - dims)))
+    check(_lib.load().pict_coords_to_transforms(_ptr(coords), dims, sz, _dtype_code(coords.dtype), _ptr(out),
+                                                _stream_ptr()), "CoordsToTransforms")
+    return out
+
+
+def CoordsToFaceTransforms(coords):
+    """Staggered face transforms from vertex coordinates (grid_gen.cu:468-514)."""
+    _check(coords.is_cuda and coords.is_contiguous(), "coords must be a contiguous CUDA tensor")
+    dims = coords.dim() - 2
+    size = [coords.size(-1 - d) - 1 for d in range(dims)]
+    out = torch.zeros([1, dims] + list(coords.shape[2:]) + [_transform_size(dims)], dtype=coords.dtype,
+                      device=coords.device)
+    sz = (ctypes.c_int32 * 3)(*(size + [1] * (3 - dims)))
+    check(_lib.load().pict_coords_to_face_transforms(_ptr(coords), dims, sz, _dtype_code(coords.dtype), _ptr(out),
+                                                     _stream_ptr()), "CoordsToFaceTransforms")
+    return out
+
+
+def TransformVectors(vectors, transforms, inverse=False):
+    """Per-cell vector transform (kernel.cu:7152-7224): M u, or Minv u with ``inverse``."""
+    dims = vectors.size(1)
+    tr = transforms.reshape(-1, _transform_size(dims))
+    off = dims * dims if inverse else 0
+    M = tr[:, off:off + dims * dims].reshape(-1, dims, dims)
+    v = torch.movedim(vectors, 1, -1).reshape(-1, dims, 1)
+    out = torch.bmm(M, v).reshape(list(vectors.shape[:1]) + list(vectors.shape[2:]) + [dims])
+    return torch.movedim(out, -1, 1).contiguous()
+
+
+# ------------------------------------------------------------------------------------------------
+# linear solves (PISOtorch.cpp:559-563 -> kernel.cu:7021-7103)
+# ------------------------------------------------------------------------------------------------
+
+_warned = set()
+
+
+def _warn_once(key, msg):
+    if key not in _warned:
+        _warned.add(key)
+        warnings.warn(msg)
+
+
+class _Workspace:
+    """Scratch memory for the Krylov kernels, allocated through torch's caching allocator."""
+
+    def __init__(self):
+        self.buf = None
+
+    def get(self, nbytes, device):
+        if self.buf is None or self.buf.numel() < nbytes or self.buf.device != device:
+            self.buf = torch.empty(int(nbytes), dtype=torch.uint8, device=device)
+        return self.buf
+
+
+def _solve_params(nrhs, maxit, tol, conv, use_bicg, transpose, x_zero=False, subtract_mean=False,
+                  write_block_pressure=False, group_size=0, threads=0):
+    p = SolveParams()
+    p.max_iterations = int(maxit)
+    p.use_bicg = int(bool(use_bicg))
+    p.nrhs = int(nrhs)
+    p.x_is_zero = int(bool(x_zero))
+    p.transpose = int(bool(transpose))
+    p.convergence = int(conv)
+    p.group_size = int(group_size)
+    p.threads = int(threads)
+    p.subtract_mean = int(bool(subtract_mean))
+    p.write_block_pressure = int(bool(write_block_pressure))
+    p.tolerance = float(tol)
+    return p
+
+
+def solve_stencil(domain, coef, rhs, x, params, info=None, stream=None):
+    """Launch one stencil solve on the domain's topology (no host synchronisation).
+
+    rhs and x are [nrhs*N] device vectors; returns the device info tensor ([nrhs] SolveInfo records).
+    """
+    lib = _lib.load()
+    desc = domain._desc
+    ws_bytes = lib.pict_solve_workspace_bytes(ctypes.byref(desc), ctypes.byref(params))
+    _check(ws_bytes > 0, "solve: invalid workspace size")
+    ws = domain.__dict__.setdefault("_ws", _Workspace()).get(ws_bytes, coef.device)
+    if info is None:
+        info = torch.empty(params.nrhs * desc.num_sims * _lib.SOLVE_INFO_BYTES, dtype=torch.uint8, device=coef.device)
+    st = _stream_ptr() if stream is None else stream
+    check(lib.pict_solve(ctypes.byref(desc), _ptr(coef), _ptr(rhs), _ptr(x), ctypes.byref(params), _ptr(info),
+                         _ptr(ws), ws_bytes, st), "SolveLinear")
+    return info
+
+
+def decode_infos(info_tensor):
+    raw = info_tensor.cpu().numpy().tobytes()
+    n = len(raw) // _lib.SOLVE_INFO_BYTES
+    arr = (SolveInfo * n).from_buffer_copy(raw)
+    out = []
+    for r in arr:
+        li = LinearSolverResultInfo(r.final_residual, r.used_iterations, bool(r.converged), bool(r.finite))
+        li.status = int(r.status)
+        out.append(li)
+    return out
+
+
+def SolveLinear(A, RHS, x, maxIterations=1000, tolerance=1e-8, convergenceCriterion=ConvergenceCriterion.NORM2_NORMALIZED,
+                useBiCG=False, matrixRankDeficient=False, residualResetSteps=0, transposeA=False, printResidual=False,
+                returnBestResult=False, BiCGwithPreconditioner=True):
+    """Solve A x = RHS for every length-n slice of RHS; returns one LinearSolverResultInfo per slice."""
+    _check(isinstance(A, StencilMatrix), "SolveLinear: A must be a system matrix of a prepared domain (domain.C, domain.P or a copy).")
+    domain = A._domain()
+    n = A.getRows()
+    _check(RHS.is_cuda and RHS.is_contiguous(), "RHS must be a contiguous CUDA tensor")
+    _check(RHS.dim() == 1, "RHS must be a vector.")
+    _check(RHS.size(0) % n == 0, "Size of RHS must be a multiple of the matrix size.")
+    _check(RHS.dtype == A.getDtype(), "Data type of RHS must match A.")
+    _check(x.is_cuda and x.is_contiguous() and x.dim() == 1, "x must be a vector.")
+    _check(x.size(0) == RHS.size(0), "Size of x must match RHS.")
+    _check(x.dtype == A.getDtype(), "Data type of x must match A.")
+    maxit = int(_as_scalar(maxIterations))
+    tol = float(_as_scalar(tolerance))
+    conv = int(convergenceCriterion)
+    if conv not in (0, 1):
+        raise NotImplementedError("only NORM2 and NORM2_NORMALIZED convergence criteria are implemented in pict_b200")
+    if matrixRankDeficient:
+        raise NotImplementedError("matrixRankDeficient is not implemented in pict_b200")
+    if returnBestResult:
+        _warn_once("best", "returnBestResult is not implemented in pict_b200; the final iterate is returned")
+    if residualResetSteps:
+        _warn_once("reset", "residualResetSteps is ignored by pict_b200")
+    if useBiCG and BiCGwithPreconditioner:
+        _warn_once("ilu", "ILU preconditioning is not implemented in pict_b200; BiCGStab runs unpreconditioned")
+    if domain.IsTensorChanged():
+        raise RuntimeError("Domain's tensors have been changed, use UpdateDomain() to set the new pointers.")
+    domain._desc = domain._make_desc()
+    nb = RHS.size(0) // n
+    infos = []
+    coef = A.coef.contiguous()
+    if useBiCG:
+        p = _solve_params(nb, maxit, tol, conv, True, transposeA)
+        info = solve_stencil(domain, coef, RHS, x, p)
+        infos = decode_infos(info)
+    else:
+        for k in range(nb):
+            p = _solve_params(1, maxit, tol, conv, False, transposeA)
+            info = solve_stencil(domain, coef, RHS[k * n:(k + 1) * n], x[k * n:(k + 1) * n], p)
+            infos.extend(decode_infos(info))
+    if printResidual:
+        for i, inf in enumerate(infos):
+            print("%sCG RHS %d: %s" % ("Bi" if useBiCG else "", i, inf))
+    return infos
+
+
+def SparseOuterProduct(a, b, out_pattern):
+    """out.value[ij] = a_i * b_j on the sparsity pattern of out (cg.cu:869-908)."""
+    _check(isinstance(out_pattern, StencilMatrix), "SparseOuterProduct: out_pattern must be a domain matrix")
+    d = out_pattern._domain()
+    N = out_pattern.getRows()
+    coef = torch.empty_like(out_pattern.coef)
+    coef[0] = a * b
+    nbr = d._nbr.long()
+    for f in range(2 * d.getSpatialDims()):
+        j = nbr[f]
+        ok = j >= 0
+        coef[f + 1] = torch.where(ok, a * b[j.clamp(min=0)], torch.zeros_like(a))
+    out_pattern.setCoef(coef)

@@ -1,0 +1,197 @@
+// common.cuh -- device-side helpers shared by the PISO kernels.
+//
+// The reference resolves neighbours per thread through a switch over boundary
+// types (resolveNeighborCell / computeConnectedPos, kernel.cu:326-345,
+// 432-477).  Here the topology is precomputed once per domain into a
+// neighbour table nbr[2D][N] (pict_build_topology); kernels only need the
+// face type to tell connected faces apart (their neighbour lives in another
+// block, possibly with permuted axes).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "pict_b200.h"
+
+namespace pict {
+
+template <int D> struct TS { static constexpr int value = 2 * D * D + 1; };  // transform stride
+
+struct CellPos {
+    int b;       // block index
+    int l;       // local (block) flat index
+    int p[3];    // x, y, z
+};
+
+__device__ __forceinline__ void unflatten(int l, const int32_t* size, int* p) {
+    const int sx = size[0], sy = size[1];
+    p[0] = l % sx;
+    const int t = l / sx;
+    p[1] = t % sy;
+    p[2] = t / sy;
+}
+
+__device__ __forceinline__ bool at_face(const int* p, const int32_t* size, int f) {
+    const int a = f >> 1;
+    return (f & 1) ? (p[a] == size[a] - 1) : (p[a] == 0);
+}
+
+// Flat index into the face arrays of a fixed boundary: position with the face axis set to 0,
+// flattened with the boundary's own size (block size with 1 along the face axis),
+// like getFixedBoundaryData (kernel.cu:2420-2428).
+__device__ __forceinline__ int boundary_flat(const int* p, const int32_t* size, int f) {
+    const int a = f >> 1;
+    int bs[3] = {size[0], size[1], size[2]};
+    bs[a] = 1;
+    int q[3] = {p[0], p[1], p[2]};
+    q[a] = 0;
+    return q[0] + bs[0] * (q[1] + bs[1] * q[2]);
+}
+
+__device__ __forceinline__ int face_cells(const int32_t* size, int f) {
+    const int a = f >> 1;
+    int n = 1;
+    for (int k = 0; k < 3; ++k) n *= (k == a) ? 1 : size[k];
+    return n;
+}
+
+template <typename T, int D>
+__device__ __forceinline__ T tr_det(const T* tr) { return tr ? tr[2 * D * D] : T(1); }
+
+// Minv[r][c]
+template <typename T, int D>
+__device__ __forceinline__ T tr_minv(const T* tr, int r, int c) { return tr[D * D + r * D + c]; }
+
+// Contravariant component c of vector u: det * Minv[c] . u (VelocityToContravariantComponent, kernel.cu:479-494).
+template <typename T, int D>
+__device__ __forceinline__ T contravariant(const T* tr, int c, const T* u) {
+    if (!tr) return u[c];
+    T s = 0;
+#pragma unroll
+    for (int k = 0; k < D; ++k) s += tr_minv<T, D>(tr, c, k) * u[k];
+    return tr_det<T, D>(tr) * s;
+}
+
+// Orthogonal Laplace coefficient det * |Minv[c]|^2 (getLaplaceCoefficientOrthogonal, kernel.cu:1209-1224).
+template <typename T, int D>
+__device__ __forceinline__ T laplace_coef(const T* tr, int c) {
+    if (!tr) return T(1);
+    T s = 0;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        const T m = tr_minv<T, D>(tr, c, k);
+        s += m * m;
+    }
+    return tr_det<T, D>(tr) * s;
+}
+
+template <typename T, int D>
+__device__ __forceinline__ const T* cell_transform(const pict_block_t& B, int l) {
+    return B.transform ? reinterpret_cast<const T*>(B.transform) + (size_t)l * TS<D>::value : nullptr;
+}
+
+template <typename T>
+__device__ __forceinline__ int block_cells(const pict_block_t& B) { return B.size[0] * B.size[1] * B.size[2]; }
+
+// Viscosity at a cell of a block (getViscosityBlock, kernel.cu:1801-1822).
+template <typename T>
+__device__ __forceinline__ T cell_viscosity(const pict_domain_t& dom, const pict_block_t& B, int l) {
+    if (B.viscosity) {
+        const T* v = reinterpret_cast<const T*>(B.viscosity);
+        return B.viscosity_static ? v[0] : v[l];
+    }
+    return reinterpret_cast<const T*>(dom.sim_viscosity)[B.sim];
+}
+
+// Velocity source component c (getBlockVelocitySource, kernel.cu:2241-2251).
+template <typename T>
+__device__ __forceinline__ T cell_source(const pict_block_t& B, int l, int c, int ncells) {
+    if (!B.source) return T(0);
+    const T* s = reinterpret_cast<const T*>(B.source);
+    return B.source_static ? s[c] : s[(size_t)c * ncells + l];
+}
+
+template <typename T>
+__device__ __forceinline__ T sim_time_step(const pict_domain_t& dom, int sim, double dt) {
+    return dom.sim_dt ? reinterpret_cast<const T*>(dom.sim_dt)[sim] : T(dt);
+}
+
+// Neighbour across face f of a cell: block, local index, the component of the neighbour that is
+// aligned with this face's axis, and the flux sign across the connection (computeFluxesNDLoop,
+// kernel.cu:1589-1606; computeConnectedPosWithChannel kernel.cu:349-360).
+struct Nbr {
+    int j;      // global index, -1 on fixed faces
+    int b;      // block
+    int l;      // local index in block b
+    int comp;   // neighbour component aligned with this face's axis
+    int flip;   // -1 if the connection joins two lower or two upper faces
+    int back;   // face of the neighbour pointing back to this cell
+};
+
+__device__ __forceinline__ Nbr neighbour(const pict_domain_t& dom, const pict_block_t& B, int b, const int* p,
+                                         int i, int f) {
+    Nbr n;
+    n.j = dom.nbr[(size_t)f * dom.num_cells + i];
+    n.b = b;
+    n.comp = f >> 1;
+    n.flip = 1;
+    n.back = f ^ 1;
+    if (n.j >= 0 && at_face(p, B.size, f) && B.face[f].type == PICT_FACE_CONNECTED) {
+        const pict_face_t& F = B.face[f];
+        n.b = F.conn_block;
+        n.comp = F.conn_axes[0] >> 1;
+        n.flip = ((F.conn_axes[0] & 1) == (f & 1)) ? -1 : 1;
+        n.back = F.conn_axes[0];
+    }
+    n.l = (n.j >= 0) ? n.j - dom.blocks[n.b].offset : -1;
+    return n;
+}
+
+// Boundary data of a fixed face: velocity vector, contravariant flux along the face axis and the
+// boundary Laplace coefficient (getFixedBoundaryData kernel.cu:2374-2433,
+// getContravariantComponentBoundaryFixed kernel.cu:728-748, kernel.cu:1434-1447).
+template <typename T, int D>
+struct FixedFace {
+    T vel[D];
+    T contra;
+    T alpha;
+};
+
+template <typename T, int D>
+__device__ __forceinline__ FixedFace<T, D> fixed_face(const pict_block_t& B, const int* p, int f) {
+    FixedFace<T, D> r;
+    const pict_face_t& F = B.face[f];
+    const int a = f >> 1;
+    const int bf = boundary_flat(p, B.size, f);
+    const T* v = reinterpret_cast<const T*>(F.velocity);
+    if (F.vel_static) {
+#pragma unroll
+        for (int c = 0; c < D; ++c) r.vel[c] = v[c];
+    } else {
+        const int nf = face_cells(B.size, f);
+#pragma unroll
+        for (int c = 0; c < D; ++c) r.vel[c] = v[(size_t)c * nf + bf];
+    }
+    const T* tr = F.transform ? reinterpret_cast<const T*>(F.transform) + (size_t)bf * TS<D>::value : nullptr;
+    r.contra = contravariant<T, D>(tr, a, r.vel);
+    r.alpha = laplace_coef<T, D>(tr, a);
+    return r;
+}
+
+template <typename T, int D>
+__device__ __forceinline__ void load_block_vec(const pict_block_t& B, const void* base, int l, T* u) {
+    const T* v = reinterpret_cast<const T*>(base);
+    const int n = B.size[0] * B.size[1] * B.size[2];
+#pragma unroll
+    for (int c = 0; c < D; ++c) u[c] = v[(size_t)c * n + l];
+}
+
+template <typename T, int D>
+__device__ __forceinline__ void load_global_vec(const T* v, int N, int j, T* u) {
+#pragma unroll
+    for (int c = 0; c < D; ++c) u[c] = v[(size_t)c * N + j];
+}
+
+// grid-stride loop helper
+#define PICT_CELL_LOOP(i, N) for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < (N); i += blockDim.x * gridDim.x)
+
+}  // namespace pict

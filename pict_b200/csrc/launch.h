@@ -1,0 +1,18 @@
+// launch.h -- host-side launch helpers and error reporting for libpict_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+#include "pict_b200.h"
+
+namespace pict {
+
+// Records the last error message (thread local) and returns the code.
+pict_status_t set_error(pict_status_t code, const char* msg);
+// cudaGetLastError after a launch -> PICT_ERR_CUDA with the kernel name.
+pict_status_t check_launch(const char* what);
+// Number of SMs of the current device (cached per device).
+int device_sm_count();
+// grid for a grid-stride per-cell kernel: enough CTAs to cover N, capped at a few waves
+int cell_grid(int n, int threads);
+
+}  // namespace pict

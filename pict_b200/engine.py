@@ -1,0 +1,220 @@
+"""Fused PISO step engine: the whole time step as a short, host-sync-free launch sequence.
+
+``PISOStepper`` advances a prepared ``PISOtorch.Domain`` (one simulation, or a
+batch of independent simulations packed into one domain by
+``pict_b200.batch``) by full PISO steps with the same sequence as the
+reference driver's orthogonal branch (``Simulation._PISO_split_step``,
+PISOtorch_simulation.py:1054-1327):
+
+1. advection matrix C, diagonal A and velocity RHS in one pass
+   (SetupAdvectionMatrix + SetupAdvectionVelocity);
+2. one persistent BiCGStab launch for all D velocity components;
+3. per corrector: pressure matrix (first corrector only: it depends on A and
+   the metrics alone, so rebuilding it is redundant) + H/A RHS + divergence,
+   one persistent CG launch that also removes the mean pressure and writes the
+   blocks' pressure (CopyPressureResultToBlocks), then the velocity
+   correction, which on the last corrector also stores the blocks' velocity
+   (CopyVelocityResultToBlocks).
+
+No host synchronisation happens inside a step; solver reports land in a device
+buffer and are checked by :meth:`check` (raising ``LinsolveError`` like the
+reference's wrapper, PISOtorch_diff.py:199-243).  The sequence is CUDA-graph
+capturable (:meth:`capture`).
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional
+
+import torch
+
+from . import _lib
+from ._lib import check
+from . import PISOtorch as P
+
+
+class LinsolveError(RuntimeError):
+    pass
+
+
+def default_tolerance(dtype):
+    """_get_solver_tolerance, PISOtorch_diff.py:183-189."""
+    return 1e-8 if dtype == torch.float64 else 1e-5
+
+
+class PISOStepper:
+    def __init__(self, domain, time_step=None, corrector_steps: int = 2, advection_tol: Optional[float] = None,
+                 pressure_tol: Optional[float] = None, max_iterations: int = 5000, adv_group_size: int = 0,
+                 p_group_size: int = 0, threads: int = 0, normalize_pressure: bool = True):
+        self.domain = domain
+        self.dims = domain.getSpatialDims()
+        self.corrector_steps = int(corrector_steps)
+        dt = domain.getDtype()
+        self.adv_tol = default_tolerance(dt) if advection_tol is None else float(advection_tol)
+        self.p_tol = default_tolerance(dt) if pressure_tol is None else float(pressure_tol)
+        self.max_iterations = int(max_iterations)
+        self.normalize_pressure = normalize_pressure
+        self.time_step = time_step
+        self.adv_params = P._solve_params(self.dims, self.max_iterations, self.adv_tol, _lib.PICT_CONV_NORM2_NORMALIZED,
+                                          True, False, x_zero=True, group_size=adv_group_size, threads=threads)
+        self.p_params = P._solve_params(1, self.max_iterations, self.p_tol, _lib.PICT_CONV_NORM2_NORMALIZED, False,
+                                        False, x_zero=True, subtract_mean=normalize_pressure, write_block_pressure=True,
+                                        group_size=p_group_size, threads=threads)
+        self._graph = None
+        self._graph_steps = 0
+        self._prepare()
+
+    def _prepare(self):
+        d = self.domain
+        d._check_ready()
+        self.desc = d._desc
+        lib = _lib.load()
+        ns = self.desc.num_sims
+        dev = d.getDevice()
+        self.info_bytes = _lib.SOLVE_INFO_BYTES
+        # per step: adv (ns*D) + corrector_steps pressure solves (ns each)
+        self.n_adv_info = ns * self.dims
+        self.n_p_info = ns
+        nbytes_adv = self.n_adv_info * self.info_bytes
+        nbytes_p = self.n_p_info * self.info_bytes
+        self.info = torch.zeros(nbytes_adv + self.corrector_steps * nbytes_p, dtype=torch.uint8, device=dev)
+        self.info_adv = self.info[:nbytes_adv]
+        self.info_p = [self.info[nbytes_adv + k * nbytes_p: nbytes_adv + (k + 1) * nbytes_p]
+                       for k in range(self.corrector_steps)]
+        ws = max(lib.pict_solve_workspace_bytes(ctypes.byref(self.desc), ctypes.byref(self.adv_params)),
+                 lib.pict_solve_workspace_bytes(ctypes.byref(self.desc), ctypes.byref(self.p_params)))
+        self.ws = torch.empty(int(ws), dtype=torch.uint8, device=dev)
+        self.ws_bytes = int(ws)
+        self.lib = lib
+
+    def _dt(self, time_step):
+        ts = self.time_step if time_step is None else time_step
+        if isinstance(ts, torch.Tensor):
+            ts = float(ts.item())
+        return float(ts)
+
+    def step(self, time_step=None, stream=None):
+        """Launch one PISO step (no host synchronisation)."""
+        d = self.domain
+        lib = self.lib
+        desc = ctypes.byref(self.desc)
+        st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream if stream is None else stream)
+        dt = self._dt(time_step)
+        D = self.dims
+        check(lib.pict_setup_advection(desc, dt, st), "advection setup")
+        check(lib.pict_solve(desc, P._ptr(d.C.coef), P._ptr(d.velocityRHS), P._ptr(d.velocityResult),
+                             ctypes.byref(self.adv_params), P._ptr(self.info_adv), P._ptr(self.ws), self.ws_bytes, st),
+              "advection solve")
+        for k in range(self.corrector_steps):
+            if k == 0:
+                check(lib.pict_setup_pressure_correction(desc, dt, 0, 0, st), "pressure setup")
+            else:
+                check(lib.pict_setup_pressure_rhs(desc, dt, 0, 0, st), "pressure rhs")
+            check(lib.pict_solve(desc, P._ptr(d.P.coef), P._ptr(d.pressureRHSdiv), P._ptr(d.pressureResult),
+                                 ctypes.byref(self.p_params), P._ptr(self.info_p[k]), P._ptr(self.ws), self.ws_bytes, st),
+                  "pressure solve")
+            last = k == self.corrector_steps - 1
+            check(lib.pict_correct_velocity(desc, dt, 1, 0, 1 if last else 0, st), "velocity correction")
+        if self.corrector_steps == 0:
+            check(lib.pict_copy_velocity_result_to_blocks(desc, st), "copy velocity")
+
+    def kernels_per_step(self):
+        """Kernels of this library launched per step: advection setup 1; per solve init-info, solver and
+        finish-info 3; per corrector pressure setup 2 (matrix/RHS, divergence), correction 1."""
+        n = 1 + 3
+        n += self.corrector_steps * (2 + 3 + 1)
+        if self.corrector_steps == 0:
+            n += 1
+        return n
+
+    def step_with_events(self, time_step=None):
+        """Eager step with CUDA events around each Krylov launch (timing of the dominant kernels).
+
+        Returns {"bicg": [(start, end, info)], "cg": [(start, end, info), ...]} with copies of the
+        solver reports of each launch.
+        """
+        d = self.domain
+        lib = self.lib
+        desc = ctypes.byref(self.desc)
+        cs = torch.cuda.current_stream()
+        st = ctypes.c_void_p(cs.cuda_stream)
+        dt = self._dt(time_step)
+        out = {"bicg": [], "cg": []}
+
+        def ev():
+            e = torch.cuda.Event(enable_timing=True)
+            e.record(cs)
+            return e
+
+        check(lib.pict_setup_advection(desc, dt, st), "advection setup")
+        a = ev()
+        check(lib.pict_solve(desc, P._ptr(d.C.coef), P._ptr(d.velocityRHS), P._ptr(d.velocityResult),
+                             ctypes.byref(self.adv_params), P._ptr(self.info_adv), P._ptr(self.ws), self.ws_bytes, st),
+              "advection solve")
+        b = ev()
+        out["bicg"].append((a, b, self.info_adv.clone()))
+        for k in range(self.corrector_steps):
+            if k == 0:
+                check(lib.pict_setup_pressure_correction(desc, dt, 0, 0, st), "pressure setup")
+            else:
+                check(lib.pict_setup_pressure_rhs(desc, dt, 0, 0, st), "pressure rhs")
+            a = ev()
+            check(lib.pict_solve(desc, P._ptr(d.P.coef), P._ptr(d.pressureRHSdiv), P._ptr(d.pressureResult),
+                                 ctypes.byref(self.p_params), P._ptr(self.info_p[k]), P._ptr(self.ws), self.ws_bytes, st),
+                  "pressure solve")
+            b = ev()
+            out["cg"].append((a, b, self.info_p[k].clone()))
+            last = k == self.corrector_steps - 1
+            check(lib.pict_correct_velocity(desc, dt, 1, 0, 1 if last else 0, st), "velocity correction")
+        return out
+
+    def infos(self):
+        """Decode the solver reports of the last step: (advection [ns*D], [pressure [ns]] per corrector)."""
+        all_infos = P.decode_infos(self.info)
+        adv = all_infos[:self.n_adv_info]
+        ps = [all_infos[self.n_adv_info + k * self.n_p_info: self.n_adv_info + (k + 1) * self.n_p_info]
+              for k in range(self.corrector_steps)]
+        return adv, ps
+
+    def check(self):
+        """Raise LinsolveError if any solve of the last step failed (synchronises)."""
+        adv, ps = self.infos()
+        for name, lst in [("advection", adv)] + [("pressure %d" % k, p) for k, p in enumerate(ps)]:
+            for i, inf in enumerate(lst):
+                if getattr(inf, "status", 0) == 1:
+                    raise LinsolveError("%s solve: inter-CTA barrier timed out (system %d)" % (name, i))
+                if not inf.isFiniteResidual:
+                    raise LinsolveError("%s solve reported non-finite residual for RHS %d: %s" % (name, i, inf))
+                if not inf.converged:
+                    raise LinsolveError("%s solve RHS %d did not converge: %s" % (name, i, inf))
+        return adv, ps
+
+    # ---------------- CUDA graph ----------------
+    def capture(self, steps: int = 1, time_step=None):
+        """Capture `steps` PISO steps into a CUDA graph (replay with :meth:`replay`).
+
+        One eager step runs first (module loading, allocator warm-up); the blocks' velocity and
+        pressure are restored afterwards, so capturing does not advance the simulation.
+        """
+        d = self.domain
+        saved = [(b.velocity.clone(), b.pressure.clone()) for b in d.getBlocks()]
+        torch.cuda.synchronize()
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            self.step(time_step)
+        torch.cuda.current_stream().wait_stream(s)
+        torch.cuda.synchronize()
+        for b, (v, p) in zip(d.getBlocks(), saved):
+            b.velocity.copy_(v)
+            b.pressure.copy_(p)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            for _ in range(steps):
+                self.step(time_step)
+        self._graph = g
+        self._graph_steps = steps
+        return g
+
+    def replay(self):
+        self._graph.replay()

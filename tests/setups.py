@@ -1,0 +1,241 @@
+"""Domain setups shared by the oracle and the CUDA path (test infrastructure).
+
+A setup is a plain dict ("spec") describing blocks, vertex coordinates,
+initial fields and boundary operations; ``build_oracle`` turns it into an FP64
+``oracle.piso_oracle.ODomain`` and ``build_product`` into a prepared
+``pict_b200.PISOtorch.Domain`` built through the same public API calls a
+reference user makes (CreateBlock, CloseAllBoundaries, CloseBoundary,
+MakePeriodic, ConnectBlock, PrepareSolve).
+
+The cases follow the reference's test setups (tests/test_setups.py:30-300):
+single closed blocks with a lid, periodic blocks, two connected blocks, 3D
+blocks, stretched and distorted (rotated) grids.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if os.path.join(ROOT, "oracle") not in sys.path:
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import piso_oracle as po  # noqa: E402
+
+
+# ------------------------------------------------------------------ grids
+
+def tensor_grid(xs, ys, zs=None):
+    """Vertex coordinates [1, D, (z), y, x] of a tensor-product grid from 1D vertex arrays."""
+    if zs is None:
+        Y, X = np.meshgrid(ys, xs, indexing="ij")
+        return np.stack([X, Y])[None]
+    Z, Y, X = np.meshgrid(zs, ys, xs, indexing="ij")
+    return np.stack([X, Y, Z])[None]
+
+
+def stretched(n, length=1.0, beta=1.5, both=True):
+    """Vertex positions clustered towards the ends with tanh stretching."""
+    s = np.linspace(-1.0, 1.0, n + 1) if both else np.linspace(0.0, 1.0, n + 1)
+    if both:
+        v = np.tanh(beta * s) / np.tanh(beta)
+        return (v + 1.0) * 0.5 * length
+    v = 1.0 - np.tanh(beta * (1.0 - s)) / np.tanh(beta)
+    return v * length
+
+
+def rotate_distort(coords, angle=0.3):
+    """Rotate vertices around the grid centre with a smooth radial falloff (a non-orthogonal grid)."""
+    c = coords.copy()
+    x, y = c[0, 0], c[0, 1]
+    cx, cy = x.mean(), y.mean()
+    r = np.sqrt((x - cx) ** 2 + (y - cy) ** 2)
+    rmax = 0.45 * min(x.max() - x.min(), y.max() - y.min())
+    w = np.where(r < rmax, np.sin(0.5 * np.pi * (1 - r / rmax)), 0.0) * angle
+    dx, dy = x - cx, y - cy
+    c[0, 0] = cx + np.cos(w) * dx - np.sin(w) * dy
+    c[0, 1] = cy + np.sin(w) * dx + np.cos(w) * dy
+    return c
+
+
+def _rand_field(rng, shape, scale=1.0):
+    return (rng.standard_normal(shape) * scale).astype(np.float64)
+
+
+# ------------------------------------------------------------------ cases
+
+def case(name, seed=0):
+    rng = np.random.default_rng(seed)
+    if name == "cavity2d":
+        n = 12
+        coords = tensor_grid(np.linspace(0, 1, n + 1), np.linspace(0, 1, n + 1))
+        return dict(dims=2, viscosity=1e-2, blocks=[dict(coords=coords, velocity=_rand_field(rng, (1, 2, n, n), 0.2))],
+                    ops=[("close_all", 0), ("close", 0, "-y", np.array([[1.0, 0.0]]))])
+    if name == "cavity2d_refined":
+        nx, ny = 10, 14
+        coords = tensor_grid(stretched(nx, 1.0, 1.2), stretched(ny, 1.5, 1.6))
+        return dict(dims=2, viscosity=5e-3, blocks=[dict(coords=coords, velocity=_rand_field(rng, (1, 2, ny, nx), 0.3))],
+                    ops=[("close_all", 0), ("close", 0, "+y", np.array([[1.0, 0.0]]))])
+    if name == "distorted2d":
+        n = 12
+        coords = rotate_distort(tensor_grid(np.linspace(0, 1, n + 1), np.linspace(0, 1, n + 1)), 0.35)
+        return dict(dims=2, viscosity=1e-2, blocks=[dict(coords=coords, velocity=_rand_field(rng, (1, 2, n, n), 0.2))],
+                    ops=[("close_all", 0), ("close", 0, "-y", np.array([[1.0, 0.0]]))])
+    if name == "periodic2d":
+        nx, ny = 9, 7
+        visc = np.abs(_rand_field(rng, (1, 1, ny, nx), 1e-2)) + 1e-3
+        return dict(dims=2, viscosity=1e-2,
+                    blocks=[dict(size=[nx, ny], velocity=_rand_field(rng, (1, 2, ny, nx), 0.5), viscosity=visc,
+                                 source=np.array([[0.3, -0.1]]))],
+                    ops=[("periodic", 0, "x"), ("close", 0, "-y"), ("close", 0, "+y")])
+    if name == "fullperiodic2d":
+        n = 8
+        coords = tensor_grid(np.linspace(0, 2, n + 1), np.linspace(0, 1, n + 1))
+        return dict(dims=2, viscosity=2e-2,
+                    blocks=[dict(coords=coords, velocity=_rand_field(rng, (1, 2, n, n), 0.5),
+                                 source=_rand_field(rng, (1, 2, n, n), 0.1))],
+                    ops=[])
+    if name == "inflow2d":
+        nx, ny = 12, 8
+        coords = tensor_grid(np.linspace(0, 3, nx + 1), np.linspace(0, 1, ny + 1))
+        inflow = np.zeros((1, 2, ny, 1))
+        inflow[0, 0, :, 0] = 1.0 + 0.1 * rng.standard_normal(ny)
+        outflow = np.zeros((1, 2, ny, 1))
+        outflow[0, 0, :, 0] = inflow[0, 0].sum() / ny
+        return dict(dims=2, viscosity=1e-2, blocks=[dict(coords=coords, velocity=_rand_field(rng, (1, 2, ny, nx), 0.2))],
+                    ops=[("close_all", 0), ("close", 0, "-x", inflow), ("close", 0, "+x", outflow)])
+    if name == "twoblock2d":
+        ny, n1, n2 = 8, 6, 7
+        c1 = tensor_grid(np.linspace(0, 1, n1 + 1), np.linspace(0, 1, ny + 1))
+        c2 = tensor_grid(np.linspace(1, 2.5, n2 + 1), np.linspace(0, 1, ny + 1))
+        return dict(dims=2, viscosity=1e-2,
+                    blocks=[dict(coords=c1, velocity=_rand_field(rng, (1, 2, ny, n1), 0.3)),
+                            dict(coords=c2, velocity=_rand_field(rng, (1, 2, ny, n2), 0.3))],
+                    ops=[("close_all", 0), ("close_all", 1), ("connect", 0, "+x", 1, "-x", "-y"),
+                         ("close", 0, "+y", np.array([[1.0, 0.0]]))])
+    if name == "twoblock2d_rotated":
+        # block 1's +x face joins block 2's +y face with the tangential axis inverted: exercises the
+        # connected-face axis permutation and the flux sign flip (kernel.cu:1589-1606)
+        n = 7
+        c1 = tensor_grid(np.linspace(0, 1, n + 1), np.linspace(0, 1, n + 1))
+        c2 = tensor_grid(np.linspace(0, 1, n + 1), np.linspace(0, 1, n + 1))
+        return dict(dims=2, viscosity=1e-2,
+                    blocks=[dict(coords=c1, velocity=_rand_field(rng, (1, 2, n, n), 0.3)),
+                            dict(coords=c2, velocity=_rand_field(rng, (1, 2, n, n), 0.3))],
+                    ops=[("close_all", 0), ("close_all", 1), ("connect", 0, "+x", 1, "+y", "-x"),
+                         ("close", 0, "-y", np.array([[1.0, 0.0]]))])
+    if name == "channel3d":
+        nx, ny, nz = 6, 5, 4
+        coords = tensor_grid(np.linspace(0, 2, nx + 1), stretched(ny, 1.0, 1.5), np.linspace(0, 1, nz + 1))
+        return dict(dims=3, viscosity=1e-2,
+                    blocks=[dict(coords=coords, velocity=_rand_field(rng, (1, 3, nz, ny, nx), 0.3),
+                                 source=np.array([[0.2, 0.0, 0.0]]))],
+                    ops=[("periodic", 0, "x"), ("periodic", 0, "z"), ("close", 0, "-y"), ("close", 0, "+y")])
+    if name == "cavity3d":
+        n = 5
+        coords = tensor_grid(np.linspace(0, 1, n + 1), np.linspace(0, 1, n + 1), np.linspace(0, 1, n + 1))
+        return dict(dims=3, viscosity=1e-2, blocks=[dict(coords=coords, velocity=_rand_field(rng, (1, 3, n, n, n), 0.2))],
+                    ops=[("close_all", 0), ("close", 0, "+y", np.array([[1.0, 0.0, 0.0]]))])
+    if name == "twoblock3d":
+        nx1, nx2, ny, nz = 4, 5, 4, 3
+        c1 = tensor_grid(np.linspace(0, 1, nx1 + 1), np.linspace(0, 1, ny + 1), np.linspace(0, 1, nz + 1))
+        c2 = tensor_grid(np.linspace(1, 2, nx2 + 1), np.linspace(0, 1, ny + 1), np.linspace(0, 1, nz + 1))
+        return dict(dims=3, viscosity=1e-2,
+                    blocks=[dict(coords=c1, velocity=_rand_field(rng, (1, 3, nz, ny, nx1), 0.3)),
+                            dict(coords=c2, velocity=_rand_field(rng, (1, 3, nz, ny, nx2), 0.3))],
+                    ops=[("close_all", 0), ("close_all", 1), ("connect", 0, "+x", 1, "-x", "-y", "-z"),
+                         ("close", 0, "+y", np.array([[1.0, 0.0, 0.0]]))])
+    raise KeyError(name)
+
+
+CASES_2D = ["cavity2d", "cavity2d_refined", "distorted2d", "periodic2d", "fullperiodic2d", "inflow2d", "twoblock2d",
+            "twoblock2d_rotated"]
+CASES_3D = ["channel3d", "cavity3d", "twoblock3d"]
+ALL_CASES = CASES_2D + CASES_3D
+
+
+def lid_cavity(n, viscosity=1e-3, lid=1.0, dims=2):
+    """The reference's minimal lid-driven cavity (minimal_lid_sample.py:33-66): uniform n^D vertex grid on [0,1]^D,
+    all walls closed, lid velocity on -y."""
+    xs = np.linspace(0, 1, n + 1)
+    if dims == 2:
+        coords = tensor_grid(xs, xs)
+        lidv = np.array([[lid, 0.0]])
+    else:
+        coords = tensor_grid(xs, xs, xs)
+        lidv = np.array([[lid, 0.0, 0.0]])
+    return dict(dims=dims, viscosity=viscosity, blocks=[dict(coords=coords)],
+                ops=[("close_all", 0), ("close", 0, "-y", lidv)])
+
+
+# ------------------------------------------------------------------ builders
+
+def build_oracle(spec) -> po.ODomain:
+    d = po.ODomain(spec["dims"], spec["viscosity"])
+    for b in spec["blocks"]:
+        bi = d.create_block(size=b.get("size"), velocity=b.get("velocity"), pressure=b.get("pressure"),
+                            coords=b.get("coords"))
+        ob = d.blocks[bi]
+        if b.get("viscosity") is not None:
+            ob.viscosity = np.asarray(b["viscosity"], dtype=np.float64)
+        if b.get("source") is not None:
+            ob.source = np.asarray(b["source"], dtype=np.float64)
+    for op in spec["ops"]:
+        if op[0] == "close_all":
+            d.close_all(op[1])
+        elif op[0] == "close":
+            d.close_boundary(op[1], op[2], None if len(op) < 4 else op[3])
+        elif op[0] == "periodic":
+            d.make_periodic(op[1], op[2])
+        elif op[0] == "connect":
+            d.connect(op[1], op[2], op[3], op[4], *op[5:])
+        else:
+            raise KeyError(op[0])
+    d.prepare()
+    return d
+
+
+def build_product(spec, dtype=None, device="cuda", module=None):
+    """Build through the PISOtorch API of `module` (default: pict_b200.PISOtorch; the reference's own
+    compiled module has the same API and is used by tests/golden/make_ref_fixtures.py)."""
+    import torch
+    if module is None:
+        from pict_b200 import PISOtorch
+    else:
+        PISOtorch = module
+    dtype = torch.float64 if dtype is None else dtype
+    t = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=dtype, device=device).contiguous()
+    dom = PISOtorch.Domain(spec["dims"], torch.tensor([spec["viscosity"]], dtype=dtype), name="test", dtype=dtype,
+                           device=device, passiveScalarChannels=0)
+    blocks = []
+    for b in spec["blocks"]:
+        kw = {}
+        if b.get("velocity") is not None:
+            kw["velocity"] = t(b["velocity"])
+        if b.get("coords") is not None:
+            kw["vertexCoordinates"] = t(b["coords"])
+        if not kw:
+            size = list(b["size"]) + [1] * (3 - len(b["size"]))
+            blk = dom.CreateBlockWithSize(PISOtorch.Int4(size[0], size[1], size[2], spec["dims"]), name="block")
+        else:
+            blk = dom.CreateBlock(name="block", **kw)
+        if b.get("viscosity") is not None:
+            blk.setViscosity(t(b["viscosity"]))
+        if b.get("source") is not None:
+            blk.setVelocitySource(t(b["source"]))
+        blocks.append(blk)
+    for op in spec["ops"]:
+        if op[0] == "close_all":
+            blocks[op[1]].CloseAllBoundaries()
+        elif op[0] == "close":
+            blocks[op[1]].CloseBoundary(op[2], None if len(op) < 4 else t(op[3]))
+        elif op[0] == "periodic":
+            blocks[op[1]].MakePeriodic(op[2])
+        elif op[0] == "connect":
+            blocks[op[1]].ConnectBlock(op[2], blocks[op[3]], op[4], *op[5:])
+        else:
+            raise KeyError(op[0])
+    dom.PrepareSolve()
+    return dom

@@ -1,0 +1,85 @@
+"""CPU checks of the C-ABI library: it loads, exports every symbol declared in include/pict_b200.h,
+its struct layouts match the ctypes binding, and the host-side topology builder agrees with the
+oracle's neighbour tables.  No GPU compute calls."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from setups import ALL_CASES, build_oracle, case
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared_symbols():
+    src = open(os.path.join(ROOT, "include", "pict_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(pict_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_loads_and_exports_all_declared_symbols():
+    from pict_b200 import _lib
+    lib = _lib.load()
+    syms = _declared_symbols()
+    assert len(syms) >= 20
+    missing = [s for s in syms if not hasattr(lib, s)]
+    assert not missing, missing
+    assert set(syms) <= set(_lib.SIGNATURES), set(syms) - set(_lib.SIGNATURES)
+    assert lib.pict_version().decode().startswith("pict_b200")
+    assert lib.pict_sizeof_block() == ctypes.sizeof(_lib.BlockDesc)
+    assert lib.pict_sizeof_domain() == ctypes.sizeof(_lib.DomainDesc)
+
+
+def _pack_from_oracle(od):
+    from pict_b200 import _lib
+    arr = (_lib.BlockDesc * len(od.blocks))()
+    for bi, b in enumerate(od.blocks):
+        d = arr[bi]
+        s = list(b.size) + [1] * (3 - od.dims)
+        d.size[0], d.size[1], d.size[2] = s
+        d.offset = od.offsets[bi]
+        for f, bnd in enumerate(b.boundaries):
+            F = d.face[f]
+            if bnd.kind == "fixed":
+                F.type = _lib.PICT_FACE_FIXED
+            elif bnd.kind == "periodic":
+                F.type = _lib.PICT_FACE_PERIODIC
+            else:
+                F.type = _lib.PICT_FACE_CONNECTED
+                F.conn_block = bnd.block
+                for k, a in enumerate(bnd.axes):
+                    F.conn_axes[k] = a
+    return arr
+
+
+@pytest.mark.parametrize("name", ALL_CASES)
+def test_topology_matches_oracle(name):
+    from pict_b200 import _lib
+    od = build_oracle(case(name))
+    arr = _pack_from_oracle(od)
+    nbr = np.empty((2 * od.dims, od.N), dtype=np.int32)
+    cb = np.empty(od.N, dtype=np.int32)
+    st = _lib.load().pict_build_topology(arr, len(od.blocks), od.dims, od.N, nbr.ctypes.data, cb.ctypes.data)
+    assert st == 0, _lib.load().pict_last_error()
+    assert np.array_equal(nbr, od.nb)
+    assert np.array_equal(cb, od.blk)
+
+
+def test_topology_rejects_inconsistent_connections():
+    from pict_b200 import _lib
+    od = build_oracle(case("twoblock2d"))
+    arr = _pack_from_oracle(od)
+    arr[1].face[0].conn_axes[0] = 0  # break the back-connection
+    nbr = np.empty((4, od.N), dtype=np.int32)
+    cb = np.empty(od.N, dtype=np.int32)
+    st = _lib.load().pict_build_topology(arr, 2, 2, od.N, nbr.ctypes.data, cb.ctypes.data)
+    assert st != 0
+    assert b"not mutual" in _lib.load().pict_last_error()
+    arr = _pack_from_oracle(build_oracle(case("periodic2d")))
+    arr[0].face[1].type = _lib.PICT_FACE_FIXED  # periodic -x without periodic +x
+    od2 = build_oracle(case("periodic2d"))
+    nbr = np.empty((4, od2.N), dtype=np.int32)
+    cb = np.empty(od2.N, dtype=np.int32)
+    assert _lib.load().pict_build_topology(arr, 1, 2, od2.N, nbr.ctypes.data, cb.ctypes.data) != 0
