@@ -1,0 +1,586 @@
+"""Drop-in mirror of the reference's simulation driver (PISOtorch_simulation.py).
+
+``Simulation`` keeps the reference's constructor arguments, properties, hook
+stages (``prep_fn``) and run loop (PISOtorch_simulation.py:398-1518).  Two
+execution paths produce the same step:
+
+* the generic path issues the operators one by one exactly like the reference's
+  ``_PISO_split_step`` orthogonal branch (sim.py:1054-1327), so every
+  ``prep_fn`` stage fires and the differentiable backend can record the graph;
+* the fused path (no hooks, not differentiable, FD corrector, GPU solves) hands
+  the whole step to :class:`pict_b200.engine.PISOStepper`, which launches it
+  without host synchronisation.
+
+Non-orthogonal correction terms are not implemented: with
+``non_orthogonal=True`` the driver verifies that every block's metric is
+orthogonal (the correction terms then vanish identically) and otherwise raises
+``NotImplementedError``.  Image/VTK output belongs to the reference's
+post-processing utilities and is not part of this package; the corresponding
+arguments are accepted and ignored with a warning.
+"""
+from __future__ import annotations
+
+import logging
+import numbers
+import signal
+import warnings
+from contextlib import nullcontext
+
+import numpy as np
+import torch
+
+from . import PISOtorch
+from .engine import LinsolveError, PISOStepper, default_tolerance
+
+_LOG = logging.getLogger("PISOsim")
+cpu_device = torch.device("cpu")
+
+
+class StopHandler:
+    """SIGINT handler polled by the run loop (sim.py:27-50)."""
+
+    def __init__(self, log=None):
+        self._log = log
+        self.reset()
+
+    def stop(self):
+        if self._log is not None:
+            self._log.warning("Simulation interrupted, stopping..." if not self._stop else "Simulation still stopping...")
+        self._stop = True
+
+    def signal_stop(self, sig, frame):
+        self.stop()
+
+    def __call__(self):
+        return self._stop
+
+    def register_signal(self):
+        signal.signal(signal.SIGINT, self.signal_stop)
+
+    def unregister_signal(self):
+        signal.signal(signal.SIGINT, signal.SIG_DFL)
+
+    def reset(self):
+        self._stop = False
+
+
+def ntonp(t):
+    return t.detach().cpu().numpy() if isinstance(t, torch.Tensor) else np.asarray(t)
+
+
+def get_max_time_step(domain, time_step_target, CFL_cond=0.8, with_transformations=True):
+    """sim.py:55-64."""
+    max_vel = float(domain.getMaxVelocity(True, with_transformations).item())
+    max_time_step = CFL_cond / max_vel
+    if max_time_step >= time_step_target:
+        return time_step_target, 1
+    ss = int(np.ceil(time_step_target / max_time_step))
+    return time_step_target / ss, ss
+
+
+def metrics_are_orthogonal(domain, rtol=1e-6):
+    """True if every cell transform has mutually orthogonal Minv rows (non-orthogonal terms vanish)."""
+    D = domain.getSpatialDims()
+    for b in domain.getBlocks():
+        if not b.hasTransform():
+            continue
+        T = b.transform.reshape(-1, 2 * D * D + 1)
+        Minv = T[:, D * D:2 * D * D].reshape(-1, D, D)
+        G = torch.bmm(Minv, Minv.transpose(1, 2))
+        diag = torch.diagonal(G, dim1=1, dim2=2)
+        off = G - torch.diag_embed(diag)
+        scale = diag.abs().max(dim=1).values.clamp_min(1e-300)
+        if (off.abs().amax(dim=(1, 2)) / scale).max().item() > rtol:
+            return False
+    return True
+
+
+class Simulation:
+    NON_ORTHO_DIRECT_MATRIX = 1
+    NON_ORTHO_DIRECT_RHS = 2
+    NON_ORTHO_DIAGONAL_MATRIX = 4
+    NON_ORTHO_DIAGONAL_RHS = 8
+    NON_ORTHO_CENTER_MATRIX = 16
+    _NON_ORTHO_MODE = NON_ORTHO_CENTER_MATRIX | NON_ORTHO_DIRECT_MATRIX | NON_ORTHO_DIAGONAL_RHS
+
+    def __init__(self, domain=None, *, time_step=1.0, substeps=1, corrector_steps=2, density_viscosity=None,
+                 adaptive_CFL=0.8, prep_fn=None, advection_use_BiCG=True, pressure_use_BiCG=False,
+                 scipy_solve_advection=False, scipy_solve_pressure=False, preconditionBiCG=False,
+                 BiCG_precondition_fallback=True, advection_tol=None, pressure_tol=None, convergence_tol=None,
+                 solver_double_fallback=False, advect_non_ortho_steps=1, pressure_non_ortho_steps=1,
+                 advect_reuse_result=False, pressure_reuse_result=False, normalize_pressure_result=True,
+                 pressure_return_best_result=False, advect_passive_scalar=True, pressure_time_step_normalized=False,
+                 velocity_corrector="FD", non_orthogonal=True, differentiable=False,
+                 exclude_advection_solve_gradients=False, exclude_pressure_solve_gradients=False, log_dir=None,
+                 log_interval=0, log_images=True, log_vtk=False, norm_vel=False, block_layout=None,
+                 output_mode3D="slice", log_fn=None, output_resampling_coords=None, output_resampling_shape=None,
+                 output_resampling_fill_max_steps=0, save_domain_name=None, stop_fn=lambda: False):
+        if density_viscosity is not None:
+            raise NotImplementedError("Simulation.density_viscosity is superseded by Domain.scalarViscosity.")
+        self.domain = domain
+        self.prep_fn = prep_fn
+        self.non_orthogonal = non_orthogonal
+        self.time_step = time_step
+        self.substeps = substeps
+        self.corrector_steps = corrector_steps
+        self.convergence_tol = convergence_tol
+        self.adaptive_CFL = adaptive_CFL
+        self.scipy_solve_advection = scipy_solve_advection
+        self.advection_use_BiCG = advection_use_BiCG
+        self.advect_non_ortho_steps = advect_non_ortho_steps
+        self.advection_tol = advection_tol
+        self.advect_passive_scalar = advect_passive_scalar
+        self.advect_reuse_result = advect_reuse_result
+        self.scipy_solve_pressure = scipy_solve_pressure
+        self.pressure_use_BiCG = pressure_use_BiCG
+        self.pressure_non_ortho_steps = pressure_non_ortho_steps
+        self.pressure_tol = pressure_tol
+        self.normalize_pressure_result = normalize_pressure_result
+        self.pressure_return_best_result = pressure_return_best_result
+        self.pressure_time_step_normalized = pressure_time_step_normalized
+        self.pressure_reuse_result = pressure_reuse_result
+        self.solver_double_fallback = solver_double_fallback
+        self.linear_solve_max_iterations = 5000
+        self.preconditionBiCG = preconditionBiCG
+        self.BiCG_precondition_fallback = BiCG_precondition_fallback
+        self._velocity_corrector_versions = {"FD": 1, "FVM_CENTER": 5, "FVM_FACE": 6}
+        self.velocity_corrector = velocity_corrector
+        self.log_dir = log_dir
+        self.log_interval = log_interval or 0
+        self.log_images = log_images
+        self.log_vtk = log_vtk
+        self.norm_vel = norm_vel
+        self.block_layout = block_layout
+        self.log_fn = log_fn
+        self.save_domain_name = save_domain_name
+        self.differentiable = differentiable
+        self.exclude_advection_solve_gradients = exclude_advection_solve_gradients
+        self.exclude_pressure_solve_gradients = exclude_pressure_solve_gradients
+        self.stop_fn = stop_fn
+        self.use_fused_step = True
+        self._stepper = None
+        self._stepper_key = None
+        self.reset_step_counters()
+
+    # ------------------------------------------------------------------ properties (sim.py:478-860)
+    @property
+    def domain(self):
+        return self._domain
+
+    @domain.setter
+    def domain(self, domain):
+        if domain is not None:
+            if not isinstance(domain, PISOtorch.Domain):
+                raise TypeError("domain must be a PISOtorch.Domain object or None.")
+            if not domain.IsInitialized():
+                raise RuntimeError("domain must be initilized. Call domain.PrepareSolve() before assignment.")
+        self._domain = domain
+        self._stepper = None
+
+    def _check_domain(self):
+        if self._domain is None:
+            raise ValueError("no domain set.")
+
+    def _get_dtype(self):
+        self._check_domain()
+        return self.domain.getBlock(0).velocity.dtype
+
+    @property
+    def differentiable(self):
+        return self._differentiable
+
+    @differentiable.setter
+    def differentiable(self, differentiable):
+        if not isinstance(differentiable, bool):
+            raise TypeError("differentiable must be bool.")
+        self._differentiable = differentiable
+        if differentiable:
+            from . import PISOtorch_diff
+            self._backend = PISOtorch_diff
+        else:
+            self._backend = PISOtorch
+
+    @property
+    def non_orthogonal(self):
+        return self._non_orthogonal
+
+    @non_orthogonal.setter
+    def non_orthogonal(self, v):
+        if not isinstance(v, bool):
+            raise TypeError("non_orthogonal must be bool.")
+        self._non_orthogonal = v
+
+    @property
+    def time_step(self):
+        return self._time_step
+
+    @time_step.setter
+    def time_step(self, v):
+        if not isinstance(v, numbers.Real):
+            raise TypeError("time_step must be float.")
+        self._time_step = v
+
+    def _get_time_step_torch(self):
+        return torch.tensor([self._time_step], device=cpu_device, dtype=self._get_dtype())
+
+    @property
+    def substeps(self):
+        return self._substeps
+
+    @substeps.setter
+    def substeps(self, v):
+        if isinstance(v, str) and v.upper() == "ADAPTIVE":
+            v = -1
+        elif not isinstance(v, numbers.Integral):
+            raise TypeError("substeps must be integral type or 'ADAPTIVE'.")
+        elif not v > 0 and v not in (-1, -2):
+            raise ValueError("substeps must be positive.")
+        self._substeps = v
+
+    @property
+    def corrector_steps(self):
+        return self._corrector_steps
+
+    @corrector_steps.setter
+    def corrector_steps(self, v):
+        if not isinstance(v, numbers.Integral):
+            raise TypeError("corrector_steps must be integral type.")
+        if v < 0:
+            raise ValueError("corrector_steps must not be negative.")
+        self._corrector_steps = v
+
+    @property
+    def advection_tol(self):
+        return default_tolerance(self._get_dtype()) if self._advection_tol is None else self._advection_tol
+
+    @advection_tol.setter
+    def advection_tol(self, v):
+        if v is not None and not (isinstance(v, numbers.Real) and v > 0):
+            raise ValueError("advection_tol must be positive float or None.")
+        self._advection_tol = v
+
+    @property
+    def pressure_tol(self):
+        return default_tolerance(self._get_dtype()) if self._pressure_tol is None else self._pressure_tol
+
+    @pressure_tol.setter
+    def pressure_tol(self, v):
+        if v is not None and not (isinstance(v, numbers.Real) and v > 0):
+            raise ValueError("pressure_tol must be positive float or None.")
+        self._pressure_tol = v
+
+    @property
+    def velocity_corrector(self):
+        return self._velocity_corrector
+
+    @velocity_corrector.setter
+    def velocity_corrector(self, v):
+        if v not in self._velocity_corrector_versions:
+            raise ValueError("velocity_corrector must be one of: %s" % (list(self._velocity_corrector_versions.keys()),))
+        self._velocity_corrector = v
+        self._velocity_corrector_version = self._velocity_corrector_versions[v]
+
+    @property
+    def stop_fn(self):
+        return self._stop_fn
+
+    @stop_fn.setter
+    def stop_fn(self, v):
+        if v is None:
+            v = lambda: False
+        if not callable(v):
+            raise TypeError("stop_fn must be callable or None.")
+        self._stop_fn = v
+
+    def _check_stop(self):
+        return self._stop_fn is not None and self._stop_fn()
+
+    @property
+    def prep_fn(self):
+        return self._prep_fn
+
+    @prep_fn.setter
+    def prep_fn(self, v):
+        if not (v is None or isinstance(v, dict)):
+            raise TypeError("prep_fn must be dict or None.")
+        self._prep_fn = v
+
+    def _run_prep_fn(self, name, **kwargs):
+        if self._prep_fn and name in self._prep_fn and self._prep_fn[name] is not None:
+            fns = self._prep_fn[name]
+            if not isinstance(fns, (list, tuple)):
+                fns = [fns]
+            for fn in fns:
+                if fn is not None:
+                    fn(**kwargs)
+
+    # ------------------------------------------------------------------ counters
+    def reset_total_step(self):
+        self.total_step = 0
+
+    def reset_total_time(self):
+        self.total_time = 0
+
+    def end_step(self, time_step=0):
+        self.total_step += 1
+        self.total_time += float(ntonp(time_step).reshape(-1)[0])
+
+    def reset_step_counters(self):
+        self.reset_total_step()
+        self.reset_total_time()
+
+    # ------------------------------------------------------------------ solves (sim.py:861-904)
+    def linear_solve(self, csrMat, rhs, x=None, use_BiCG=False, tol=None, max_iter=None, matrix_rank_deficient=False,
+                     residual_reset_step=0, use_scipy=False, return_best_result=False):
+        if use_scipy:
+            raise NotImplementedError("SciPy solves are not part of the B200 step; use the GPU solvers")
+        if max_iter is None:
+            max_iter = self.linear_solve_max_iterations
+        tol = default_tolerance(rhs.dtype) if tol is None else tol
+        if self._backend is PISOtorch:
+            if x is None:
+                x = torch.zeros_like(rhs)
+            if bool(rhs.eq(0).all()):
+                x.zero_()
+                return x, True
+            infos = PISOtorch.SolveLinear(csrMat, rhs, x, max_iter, tol, PISOtorch.ConvergenceCriterion.NORM2_NORMALIZED,
+                                          use_BiCG, False, residual_reset_step, False, False, return_best_result,
+                                          BiCGwithPreconditioner=False)
+            _check_infos(infos, use_BiCG, tol, max_iter, return_best_result)
+            return x, True
+        return self._backend.linear_solve_GPU(csrMat, rhs, transpose=False, use_BiCG=use_BiCG, tol=tol,
+                                              max_iter=max_iter, return_best_result=return_best_result), True
+
+    # ------------------------------------------------------------------ step
+    def _fused_eligible(self):
+        d = self.domain
+        return (self.use_fused_step and not self.differentiable and not self._prep_fn and self.convergence_tol is None
+                and self._velocity_corrector_version == 1 and not self.pressure_time_step_normalized
+                and not self.scipy_solve_advection and not self.scipy_solve_pressure and self.advection_use_BiCG
+                and not self.pressure_use_BiCG and self.normalize_pressure_result
+                and not (self.advect_passive_scalar and d.hasPassiveScalar()))
+
+    def _check_non_ortho(self):
+        if self.non_orthogonal:
+            key = ("ortho", id(self.domain))
+            if getattr(self, "_ortho_checked", None) != key:
+                if not metrics_are_orthogonal(self.domain):
+                    raise NotImplementedError("non-orthogonal correction terms are not implemented in pict_b200; "
+                                              "this domain's metrics are not orthogonal")
+                self._ortho_checked = key
+
+    def _get_stepper(self):
+        key = (id(self.domain), self.corrector_steps, self.advection_tol, self.pressure_tol,
+               self.linear_solve_max_iterations)
+        if self._stepper is None or self._stepper_key != key:
+            self._stepper = PISOStepper(self.domain, corrector_steps=self.corrector_steps,
+                                        advection_tol=self.advection_tol, pressure_tol=self.pressure_tol,
+                                        max_iterations=self.linear_solve_max_iterations)
+            self._stepper_key = key
+        return self._stepper
+
+    def _PISO_split_step(self, iterations, time_step=None):
+        self._check_domain()
+        self._check_non_ortho()
+        if time_step is None:
+            time_step = self._get_time_step_torch()
+        if isinstance(iterations, torch.Tensor):
+            iterations = int(iterations.numpy()[0])
+        assert iterations > 0
+        domain = self.domain
+        if self._fused_eligible():
+            if domain.IsTensorChanged():
+                domain.UpdateDomainData()
+            st = self._get_stepper()
+            st.desc = domain._make_desc()
+            for _ in range(iterations):
+                st.step(time_step)
+                st.check()
+                if self._check_stop():
+                    break
+                self.end_step(time_step)
+            return True
+        return self._PISO_split_step_ops(iterations, time_step)
+
+    def _PISO_split_step_ops(self, iterations, time_step):
+        """Operator-by-operator step, sim.py:1054-1327 (orthogonal branch)."""
+        domain = self.domain
+        B = self._backend
+        vcv = self._velocity_corrector_version
+        solve_ok = True
+        advect_use_prev_result = self.advect_reuse_result and not self.differentiable
+        for step in range(iterations):
+            if self.convergence_tol is not None:
+                B.CopyVelocityResultFromBlocks(domain)
+                last_vel = domain.velocityResult.clone().detach()
+            self._run_prep_fn("PRE", domain=domain, local_step=step, time_step=time_step, total_step=self.total_step,
+                              total_time=self.total_time)
+            domain.UpdateDomainData()
+            if self.advect_passive_scalar and domain.hasPassiveScalar():
+                raise NotImplementedError("passive scalar transport is not implemented in pict_b200")
+            self._run_prep_fn("PRE_VELOCITY_SETUP", domain=domain, local_step=step, time_step=time_step,
+                              total_step=self.total_step, total_time=self.total_time)
+            B.SetupAdvectionMatrix(domain, time_step, 0)
+            B.SetupAdvectionVelocity(domain, time_step, 0, False)
+            self._run_prep_fn("POST_VELOCITY_SETUP", domain=domain, no_step=0, local_step=step, time_step=time_step,
+                              total_step=self.total_step, total_time=self.total_time)
+            with torch.no_grad() if self.exclude_advection_solve_gradients else nullcontext():
+                x = None if not advect_use_prev_result else domain.velocityResult
+                velocityResult, solve_ok = self.linear_solve(domain.C, domain.velocityRHS, x=x,
+                                                             use_BiCG=self.advection_use_BiCG,
+                                                             use_scipy=self.scipy_solve_advection, tol=self.advection_tol)
+            domain.setVelocityResult(velocityResult)
+            domain.UpdateDomainData()
+            self._run_prep_fn("POST_PREDICTION", domain=domain, local_step=step, time_step=time_step,
+                              total_step=self.total_step, total_time=self.total_time)
+            if self._check_stop():
+                break
+            for cstep in range(self.corrector_steps):
+                B.SetupPressureCorrection(domain, time_step, 0, False, timeStepNorm=self.pressure_time_step_normalized)
+                self._run_prep_fn("POST_PRESSURE_SETUP", domain=domain, local_step=step, time_step=time_step,
+                                  total_step=self.total_step, total_time=self.total_time)
+                with torch.no_grad() if self.exclude_pressure_solve_gradients else nullcontext():
+                    pressureResult, solve_ok = self.linear_solve(domain.P, domain.pressureRHSdiv, x=None,
+                                                                 use_BiCG=self.pressure_use_BiCG,
+                                                                 use_scipy=self.scipy_solve_pressure,
+                                                                 tol=self.pressure_tol,
+                                                                 return_best_result=self.pressure_return_best_result)
+                if self.normalize_pressure_result:
+                    pressureResult = pressureResult - torch.mean(pressureResult)
+                domain.setPressureResult(pressureResult)
+                domain.UpdateDomainData()
+                self._run_prep_fn("POST_PRESSURE_RESULT", domain=domain, local_step=step, time_step=time_step,
+                                  total_step=self.total_step, total_time=self.total_time)
+                self._run_prep_fn("POST_PRESSURE_NON_ORTHO", domain=domain, local_step=step, time_step=time_step,
+                                  total_step=self.total_step, total_time=self.total_time)
+                B.CopyPressureResultToBlocks(domain)
+                B.CorrectVelocity(domain, time_step, version=vcv, timeStepNorm=self.pressure_time_step_normalized)
+                self._run_prep_fn("POST_VELOCITY_CORRECTION", domain=domain, local_step=step, time_step=time_step,
+                                  total_step=self.total_step, total_time=self.total_time)
+                if self._check_stop():
+                    break
+            B.CopyVelocityResultToBlocks(domain)
+            self._run_prep_fn("POST", domain=domain, local_step=step, time_step=time_step, total_step=self.total_step,
+                              total_time=self.total_time)
+            if self.convergence_tol is not None:
+                diff = torch.max(torch.abs(last_vel - domain.velocityResult)).item()
+                if diff < self.convergence_tol:
+                    _LOG.info("Simulation step max difference is under convergence tolerance.")
+                    solve_ok = False
+            if not solve_ok or self._check_stop():
+                break
+            self.end_step(time_step)
+        return solve_ok
+
+    def _PISO_adaptive_step(self, CFL_cond=None, max_subsetps=1000):
+        """sim.py:1329-1372."""
+        time_step_target = self.time_step
+        domain = self.domain
+        CFL_cond = CFL_cond if CFL_cond is not None else self.adaptive_CFL
+        substep = 0
+        while time_step_target > 0 and not np.isclose(time_step_target, 0):
+            max_vel = float(domain.getMaxVelocity(True, True).item())
+            max_time_step = time_step_target if np.isclose(max_vel, 0) else CFL_cond / max_vel
+            if max_time_step >= time_step_target:
+                ts = time_step_target
+            else:
+                ts = time_step_target / int(np.ceil(time_step_target / max_time_step))
+            time_step_target -= ts
+            ok = self._PISO_split_step(iterations=1, time_step=torch.tensor([ts], dtype=self._get_dtype()))
+            substep += 1
+            if not ok or self._check_stop():
+                return False
+        return True
+
+    def make_divergence_free(self, iterations=1, max_iter=1000):
+        """Pressure projection of the current velocity with A = 1, dt = 1 (sim.py:985-1052)."""
+        self._check_domain()
+        self._check_non_ortho()
+        domain = self.domain
+        B = self._backend
+        time_step = torch.tensor([1], device=cpu_device, dtype=domain.A.dtype)
+        domain.setA(torch.ones_like(domain.A))
+        solve_ok = True
+        for step in range(iterations):
+            domain.UpdateDomainData()
+            B.CopyVelocityResultFromBlocks(domain)
+            domain.setPressureRHS(domain.velocityResult)
+            domain.UpdateDomainData()
+            B.SetupPressureMatrix(domain, time_step, 0, False)
+            B.SetupPressureRHSdiv(domain, time_step, 0, False, timeStepNorm=self.pressure_time_step_normalized)
+            pressureResult, solve_ok = self.linear_solve(domain.P, domain.pressureRHSdiv, use_BiCG=self.pressure_use_BiCG,
+                                                         tol=self.pressure_tol, max_iter=max_iter)
+            if self.normalize_pressure_result:
+                pressureResult = pressureResult - torch.mean(pressureResult)
+            domain.setPressureResult(pressureResult)
+            domain.UpdateDomainData()
+            B.CopyPressureResultToBlocks(domain)
+            B.CorrectVelocity(domain, time_step, version=self._velocity_corrector_version,
+                              timeStepNorm=self.pressure_time_step_normalized)
+            B.CopyVelocityResultToBlocks(domain)
+            self.end_step(time_step)
+        return solve_ok
+
+    def run(self, iterations, static=False, log_domain=True):
+        """sim.py:1374-1518 without image/VTK output."""
+        self._check_domain()
+        if static:
+            raise NotImplementedError("passive scalar transport is not implemented in pict_b200")
+        domain = self.domain
+        if self.log_interval > 0 and (self.log_images or self.log_vtk):
+            warnings.warn("image/VTK output is not part of pict_b200; log_images/log_vtk are ignored")
+        if domain.GetCoordinateOrientation() == 0:
+            _LOG.warning("Domain coordinate systems have mixed orientation. This can lead to issues with the simulation.")
+        flux = abs(float(domain.GetBoundaryFluxBalance().item()))
+        if flux > float(self.pressure_tol):
+            _LOG.warning("Domain boundary is not divergence free (flux balance: %.03e). This can prevent pressure solve "
+                         "convergence.", flux)
+            return False
+        sim_ok = True
+        substeps = self.substeps
+        time_step = None
+        adaptive = substeps == -1
+        if substeps == -2:
+            ts, substeps = get_max_time_step(domain, self.time_step, 0.8, with_transformations=True)
+            time_step = torch.tensor([ts], dtype=self._get_dtype())
+        for it in range(1, iterations + 1):
+            try:
+                if adaptive:
+                    sim_ok = self._PISO_adaptive_step()
+                else:
+                    sim_ok = self._PISO_split_step(iterations=substeps, time_step=time_step)
+            except LinsolveError:
+                _LOG.exception("Simulation failed in major step %d (total step %d):", it, self.total_step)
+                break
+            max_mag = float(domain.getMaxVelocityMagnitude(False).item())
+            if np.isnan(max_mag):
+                _LOG.warning("NaN encountered in velocity, stopping")
+                sim_ok = False
+                break
+            if self.log_interval > 0 and it % self.log_interval == 0:
+                div = PISOtorch.ComputeVelocityDivergence(domain).abs()
+                p = domain.pressureResult
+                _LOG.info("%d/%d Stats: max mag=%.03e, p mean=%.03e min=%.03e max=%.03e, |div| mean=%.03e max=%.03e",
+                          it, iterations, max_mag, p.mean().item(), p.min().item(), p.max().item(),
+                          div.mean().item(), div.max().item())
+            if self.log_fn is not None:
+                self.log_fn(domain=domain, out_dir=self.log_dir, it=it, out_it=0, total_step=self.total_step)
+            if self._check_stop() or not sim_ok:
+                break
+        return sim_ok
+
+
+def _check_infos(infos, use_BiCG, tol, max_iter, return_best_result):
+    """_check_solver_return_infos, PISOtorch_diff.py:199-243."""
+    if any(not i.isFiniteResidual for i in infos):
+        bad = [k for k, i in enumerate(infos) if not i.isFiniteResidual]
+        raise LinsolveError("Linear solve (BiCG:%s, tol:%.03e) reported non-finite residual for RHS %s of %d. Solver infos:\n%s."
+                            % (use_BiCG, tol, bad, len(infos), "\n".join("\t%s" % i for i in infos)))
+    if any(not i.converged for i in infos):
+        bad = [k for k, i in enumerate(infos) if not i.converged]
+        msg = "Linear solve (BiCG:%s, tol:%.03e) RHS %s of %d did not converge after %d iterations." % (
+            use_BiCG, tol, bad, len(infos), max_iter)
+        if return_best_result:
+            _LOG.warning(msg)
+        else:
+            raise LinsolveError(msg)

@@ -208,7 +208,7 @@ def build_product(spec, dtype=None, device="cuda", module=None):
     dtype = torch.float64 if dtype is None else dtype
     t = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=dtype, device=device).contiguous()
     dom = PISOtorch.Domain(spec["dims"], torch.tensor([spec["viscosity"]], dtype=dtype), name="test", dtype=dtype,
-                           device=device, passiveScalarChannels=0)
+                           device=torch.device(device), passiveScalarChannels=0)
     blocks = []
     for b in spec["blocks"]:
         kw = {}
