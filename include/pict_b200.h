@@ -96,6 +96,10 @@ typedef struct pict_domain {
     const int32_t* cell_block;     /* [N] block index of each cell */
     const int32_t* sim_cells;      /* [num_sims+1] cell range of each system */
     const int32_t* sim_blocks;     /* [num_sims+1] block range of each system */
+    const int32_t* tiles;          /* [num_tiles][4] Krylov work tiles: system, block, first cell, cell count */
+    const int32_t* sim_tiles;      /* [num_sims+1] tile range of each system */
+    int32_t num_tiles;
+    int32_t tile_cells;            /* upper bound of cells per tile */
     const void* sim_viscosity;     /* [num_sims] domain viscosity per system */
     const void* sim_dt;            /* [num_sims] time step per system, or NULL (use the scalar argument) */
     void* C;                  /* [K][N] advection matrix */
@@ -131,7 +135,7 @@ typedef struct pict_solve_params {
     int32_t x_is_zero;         /* 1: skip the initial A*x (x must hold zeros) */
     int32_t transpose;         /* solve with A^T (adjoint solves) */
     int32_t convergence;       /* PICT_CONV_*; only NORM2 and NORM2_NORMALIZED are supported */
-    int32_t group_size;        /* CTAs cooperating on one system (0: automatic) */
+    int32_t group_size;        /* upper bound of CTAs of the persistent launch (0: automatic) */
     int32_t threads;           /* threads per CTA (0: automatic) */
     int32_t subtract_mean;     /* 1: x -= mean(x) per system after the solve (sim.py:1243-1244) */
     int32_t write_block_pressure; /* 1: also copy x into the blocks' pressure (CopyPressureResultToBlocks) */
@@ -152,6 +156,14 @@ int32_t pict_sizeof_domain(void);  /* sizeof(pict_domain_t) */
  * nbr_out: [2*dims][num_cells], cell_block_out: [num_cells] (host buffers). */
 pict_status_t pict_build_topology(const pict_block_t* host_blocks, int32_t num_blocks, int32_t dims,
                                   int32_t num_cells, int32_t* nbr_out, int32_t* cell_block_out);
+
+/* Work tiles for the Krylov kernels: every block is cut into contiguous runs of at most
+ * tile_cells cells; tiles of one system are contiguous.  tiles_out: [max_tiles][4] (system, block,
+ * first global cell, count), sim_tiles_out: [num_sims+1].  *num_tiles_out receives the count
+ * (also when max_tiles is too small, then PICT_ERR_ARG is returned).  Host buffers. */
+pict_status_t pict_build_tiles(const pict_block_t* host_blocks, int32_t num_blocks, int32_t num_sims,
+                               int32_t tile_cells, int32_t* tiles_out, int32_t max_tiles, int32_t* sim_tiles_out,
+                               int32_t* num_tiles_out);
 
 /* ---------------- assembly (forward) ---------------- */
 /* SetupAdvectionMatrix (PISOtorch.cpp:531-533 -> kernel.cu:4510 PISO_build_matrix):

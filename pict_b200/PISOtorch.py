@@ -156,6 +156,21 @@ def _ptr(t: Optional[torch.Tensor]):
     return None if t is None else t.data_ptr()
 
 
+TILE_CELLS = 2048  # cells per Krylov work tile (upper bound 2048, see krylov.cu)
+
+
+def build_tiles(host_blocks, num_blocks, num_sims, device, tile_cells=TILE_CELLS):
+    """Krylov work tiles of a block table (pict_build_tiles): returns (tiles [T,4] int32, sim_tiles [S+1])."""
+    lib = _lib.load()
+    cnt = ctypes.c_int32(0)
+    sim_tiles = torch.empty(num_sims + 1, dtype=torch.int32)
+    lib.pict_build_tiles(host_blocks, num_blocks, num_sims, tile_cells, None, 0, sim_tiles.data_ptr(), ctypes.byref(cnt))
+    tiles = torch.empty((max(cnt.value, 1), 4), dtype=torch.int32)
+    check(lib.pict_build_tiles(host_blocks, num_blocks, num_sims, tile_cells, tiles.data_ptr(), cnt.value,
+                               sim_tiles.data_ptr(), ctypes.byref(cnt)), "build_tiles")
+    return tiles[:cnt.value].to(device), sim_tiles.to(device), cnt.value
+
+
 def _transform_size(dims):
     return 2 * dims * dims + 1
 
@@ -1388,6 +1403,7 @@ class Domain:
                                               cell_block.data_ptr()), "build_topology")
         self._nbr = nbr.to(self._device)
         self._cell_block = cell_block.to(self._device)
+        self._tiles, self._sim_tiles, self._num_tiles = build_tiles(host_blocks, len(self.blocks), 1, self._device)
         self._csr_struct = None
         self._initialized = True
         self.UpdateDomainData()
@@ -1464,6 +1480,10 @@ class Domain:
         d.cell_block = _ptr(self._cell_block)
         d.sim_cells = _ptr(self._sim_cells)
         d.sim_blocks = _ptr(self._sim_blocks)
+        d.tiles = _ptr(self._tiles)
+        d.sim_tiles = _ptr(self._sim_tiles)
+        d.num_tiles = self._num_tiles
+        d.tile_cells = TILE_CELLS
         d.sim_viscosity = _ptr(self._sim_visc)
         d.sim_dt = None
         d.C = _ptr(self.C.coef if C is None else C)

@@ -80,6 +80,10 @@ class DomainDesc(ctypes.Structure):
         ("cell_block", c_vp),
         ("sim_cells", c_vp),
         ("sim_blocks", c_vp),
+        ("tiles", c_vp),
+        ("sim_tiles", c_vp),
+        ("num_tiles", c_i32),
+        ("tile_cells", c_i32),
         ("sim_viscosity", c_vp),
         ("sim_dt", c_vp),
         ("C", c_vp),
@@ -130,6 +134,7 @@ SIGNATURES = {
     "pict_sizeof_block": (c_i32, []),
     "pict_sizeof_domain": (c_i32, []),
     "pict_build_topology": (c_i32, [ctypes.POINTER(BlockDesc), c_i32, c_i32, c_i32, c_vp, c_vp]),
+    "pict_build_tiles": (c_i32, [ctypes.POINTER(BlockDesc), c_i32, c_i32, c_i32, c_vp, c_i32, c_vp, c_vp]),
     "pict_setup_advection_matrix": (c_i32, [_PD, ctypes.c_double, c_i32, c_vp]),
     "pict_setup_advection_velocity": (c_i32, [_PD, ctypes.c_double, c_i32, c_i32, c_vp]),
     "pict_setup_advection": (c_i32, [_PD, ctypes.c_double, c_vp]),

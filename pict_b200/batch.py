@@ -115,6 +115,7 @@ class BatchDomain:
         self._cell_block = cb.to(dev)
         self._sim_cells = torch.tensor(sim_cells, dtype=torch.int32, device=dev)
         self._sim_blocks = torch.tensor(sim_blocks, dtype=torch.int32, device=dev)
+        self._tiles, self._sim_tiles, self._num_tiles = P.build_tiles(self._host_blocks, len(host), self.num_sims, dev)
         self._sim_visc = torch.tensor([float(self.domains[i].viscosity.item()) for i in self.order],
                                       dtype=self._dtype, device=dev)
         self.max_sim_cells = max(sim_cells[k + 1] - sim_cells[k] for k in range(self.num_sims))
@@ -169,6 +170,10 @@ class BatchDomain:
         d.cell_block = self._cell_block.data_ptr()
         d.sim_cells = self._sim_cells.data_ptr()
         d.sim_blocks = self._sim_blocks.data_ptr()
+        d.tiles = self._tiles.data_ptr()
+        d.sim_tiles = self._sim_tiles.data_ptr()
+        d.num_tiles = self._num_tiles
+        d.tile_cells = P.TILE_CELLS
         d.sim_viscosity = self._sim_visc.data_ptr()
         d.sim_dt = None if self._sim_dt is None else self._sim_dt.data_ptr()
         d.C = self.C.coef.data_ptr()

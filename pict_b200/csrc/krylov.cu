@@ -1,25 +1,30 @@
-// krylov.cu -- persistent CG and BiCGStab on structured stencil matrices.
+// krylov.cu -- persistent, tiled CG and BiCGStab on structured stencil matrices.
 //
 // Replaces the reference's host-driven Krylov loops (cgSolveGPU,
 // extensions/cg_solver_kernel.cu:114-456; bicgstabSolveGPU,
 // extensions/bicgstab_solver_kernel.cu:47-395), which issue one cuSPARSE SpMV
 // plus several cuBLAS calls with host round trips per iteration, by one
-// persistent launch per solve:
+// persistent launch per solve that advances every system of a (batched) domain
+// in lock step:
 //
-//  * a group of G cooperating CTAs owns one system (simulation) at a time and
-//    pulls the next system from a device work queue, so a batch of uneven
-//    systems is solved in a single launch;
+//  * the cells of all systems are cut into tiles (contiguous runs of at most
+//    tile_cells cells inside one block, pict_build_tiles); each CTA owns a fixed
+//    set of tiles (round robin) and, per phase, sweeps its tiles of the systems
+//    that are still iterating, so uneven systems share the SMs and converged
+//    systems cost nothing;
+//  * one bounded grid barrier per phase (two per CG iteration, four per
+//    BiCGStab iteration); every wait has an iteration limit after which the
+//    kernel records an error and returns;
+//  * inner products are accumulated in FP64, reduced per tile inside the CTA
+//    and then per system over the tile partials in a fixed order, so results do
+//    not depend on the number of CTAs and are bitwise reproducible;
 //  * the stencil SpMV reads structured neighbours directly (i +- stride) and
-//    falls back to the precomputed neighbour table only on block faces;
-//  * vector updates are fused into the SpMV sweeps (the search direction is
-//    formed on the fly for the neighbours, double-buffered), leaving two
-//    group-wide reductions per CG iteration and four per BiCGStab iteration;
-//  * inner products and norms are accumulated in FP64 with a fixed reduction
-//    order (deterministic), for FP32 and FP64 vectors alike;
-//  * BiCGStab advances all D velocity components at once (shared matrix
-//    loads), each with its own scalars and convergence state;
-//  * every inter-CTA wait is bounded: on timeout the kernel records an error
-//    and returns (the host reports it through pict_solve_info_t.status).
+//    uses the precomputed neighbour table only on block faces; the search
+//    direction is formed on the fly for the neighbours (double buffered), so
+//    vector updates need no extra pass;
+//  * BiCGStab advances all right-hand sides of a system (the D velocity
+//    components) together, sharing the matrix loads, each with its own scalars
+//    and convergence state.
 //
 // Iteration semantics, stopping rule and reported iteration counts follow the
 // reference: CG cg.cu:236-427, BiCGStab bicg.cu:240-360, convergence criterion
@@ -36,8 +41,14 @@
 
 namespace pict {
 
-constexpr int KR_NV = 8;      // partial-sum slots per reduction
-constexpr int KR_MAX_WARPS = 16;
+constexpr int KR_NV = 8;         // values per tile partial
+constexpr int KR_SLOTS = 16;     // tiles per CTA (one warp reduces the system of each slot)
+constexpr int KR_THREADS = 512;  // threads per CTA
+constexpr int KR_CPT = 4;        // cells per thread per tile: tile_cells <= KR_CPT * KR_THREADS
+constexpr int KR_MAX_TILE = KR_CPT * KR_THREADS;
+
+// ctrl words in the workspace header
+enum { CTRL_ERR = 0, CTRL_DONE = 1, CTRL_BAR_COUNT = 2, CTRL_BAR_GEN = 3 };
 
 template <typename T>
 struct KArgs {
@@ -52,17 +63,13 @@ struct KArgs {
     T* v0;
     T* v1;
     T* t;
-    int* queue;
-    int* err;
-    int* group_sys;
-    unsigned* sync;       // [ngroups][32]
-    double* partials;     // [ngroups][2][G][KR_NV]
+    int* ctrl;
+    double* partials;  // [2][num_tiles][KR_NV]
     pict_solve_info_t* info;
     int maxit;
     double tol;
     int normalized;
-    int nrhs;
-    int G;
+    int nrhs;  // stride of the info records per system
     int x_zero;
     int sub_mean;
     int write_bp;
@@ -74,26 +81,29 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
-// Bounded barrier of the G CTAs of one group (sense by generation counter).
-__device__ bool group_barrier(unsigned* sync, int G, int* err) {
+// Bounded barrier over all CTAs of the launch (generation counter).
+__device__ bool grid_barrier(int* ctrl) {
     __shared__ int s_ok;
     __syncthreads();
+    if (gridDim.x == 1) return *(volatile int*)(ctrl + CTRL_ERR) == 0;
     if (threadIdx.x == 0) {
         int ok = 1;
-        volatile unsigned* vgen = sync + 1;
+        unsigned* count = reinterpret_cast<unsigned*>(ctrl + CTRL_BAR_COUNT);
+        unsigned* gen = reinterpret_cast<unsigned*>(ctrl + CTRL_BAR_GEN);
+        volatile unsigned* vgen = gen;
         const unsigned g0 = *vgen;
         __threadfence();
-        const unsigned arrived = atomicAdd(sync, 1u);
-        if (arrived == (unsigned)(G - 1)) {
-            atomicExch(sync, 0u);
+        const unsigned arrived = atomicAdd(count, 1u);
+        if (arrived == gridDim.x - 1) {
+            atomicExch(count, 0u);
             __threadfence();
-            atomicAdd(sync + 1, 1u);
+            atomicAdd(gen, 1u);
         } else {
             long long spins = 0;
             while (*vgen == g0) {
-                if (++spins > PICT_SPIN_LIMIT) { ok = 0; atomicExch(err, 1); break; }
-                if (*(volatile int*)err) { ok = 0; break; }
-                __nanosleep(64);
+                if (++spins > PICT_SPIN_LIMIT) { ok = 0; atomicExch(ctrl + CTRL_ERR, 1); break; }
+                if (*(volatile int*)(ctrl + CTRL_ERR)) { ok = 0; break; }
+                __nanosleep(32);
             }
         }
         __threadfence();
@@ -103,12 +113,12 @@ __device__ bool group_barrier(unsigned* sync, int G, int* err) {
     return s_ok != 0;
 }
 
-// Sum NV doubles over the CTA, then over the G CTAs of the group (fixed order).
-template <int NV, typename T>
-__device__ bool reduce(double (&v)[NV], const KArgs<T>& a, int grp, int rank, int& phase) {
-    __shared__ double s_red[KR_MAX_WARPS][KR_NV];
+// Block-wide sum of NV values; the result is returned to every thread.
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV]) {
+    __shared__ double s_red[KR_THREADS / 32][KR_NV];
     __shared__ double s_out[KR_NV];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = (blockDim.x + 31) >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
 #pragma unroll
     for (int k = 0; k < NV; ++k) {
         const double w = warp_sum(v[k]);
@@ -124,68 +134,80 @@ __device__ bool reduce(double (&v)[NV], const KArgs<T>& a, int grp, int rank, in
         }
     }
     __syncthreads();
-    if (a.G > 1) {
-        double* part = a.partials + ((size_t)(grp * 2 + phase) * a.G) * KR_NV;
-        if (threadIdx.x == 0) {
-#pragma unroll
-            for (int k = 0; k < NV; ++k) part[rank * KR_NV + k] = s_out[k];
-        }
-        if (!group_barrier(a.sync + grp * 32, a.G, a.err)) return false;
-        if (threadIdx.x < NV) {
-            double s = 0;
-            for (int r = 0; r < a.G; ++r) s += __ldcg(part + r * KR_NV + threadIdx.x);
-            s_out[threadIdx.x] = s;
-        }
-        phase ^= 1;
-        __syncthreads();
-    }
 #pragma unroll
     for (int k = 0; k < NV; ++k) v[k] = s_out[k];
     __syncthreads();
-    return true;
 }
 
-// Fetch the next system for this group from the work queue (-1: none left, -2: aborted).
-template <typename T>
-__device__ int next_system(const KArgs<T>& a, int grp, int rank) {
-    __shared__ int s_sys;
-    if (a.G == 1) {
-        if (threadIdx.x == 0) s_sys = atomicAdd(a.queue, 1);
-        __syncthreads();
-    } else {
-        if (rank == 0 && threadIdx.x == 0) {
-            const int s = atomicAdd(a.queue, 1);
-            *(volatile int*)(a.group_sys + grp) = s;
-        }
-        if (!group_barrier(a.sync + grp * 32, a.G, a.err)) return -2;
-        if (threadIdx.x == 0) s_sys = *(volatile int*)(a.group_sys + grp);
-        __syncthreads();
-    }
-    const int s = s_sys;
+// Per-CTA tile bookkeeping in shared memory.
+struct TileSlots {
+    int n;                       // slots used by this CTA
+    int tile[KR_SLOTS];
+    int sim[KR_SLOTS];
+    int block[KR_SLOTS];
+    int start[KR_SLOTS];
+    int count[KR_SLOTS];
+    int t0[KR_SLOTS];            // tile range of the slot's system
+    int t1[KR_SLOTS];
+    int owner[KR_SLOTS];         // 1 if this slot holds the first tile of its system
+};
+
+__device__ void load_slots(const pict_domain_t& dom, TileSlots& S) {
+    const int nt = dom.num_tiles;
+    if (threadIdx.x == 0) S.n = (int)blockIdx.x < nt ? (nt - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x : 0;
     __syncthreads();
-    return s < a.dom.num_sims ? s : -1;
+    if ((int)threadIdx.x < S.n) {
+        const int j = threadIdx.x;
+        const int t = blockIdx.x + j * gridDim.x;
+        const int* tt = dom.tiles + 4 * t;
+        S.tile[j] = t;
+        S.sim[j] = tt[0];
+        S.block[j] = tt[1];
+        S.start[j] = tt[2];
+        S.count[j] = tt[3];
+        S.t0[j] = dom.sim_tiles[tt[0]];
+        S.t1[j] = dom.sim_tiles[tt[0] + 1];
+        S.owner[j] = (t == S.t0[j]);
+    }
+    __syncthreads();
 }
 
-// Iterate the cells [lo,hi) of the system's blocks [b0,b1) owned by this CTA.
-#define KR_FOR_CELLS(...)                                                                  \
-    for (int bb = b0; bb < b1; ++bb) {                                                     \
-        const pict_block_t& B = dom.blocks[bb];                                            \
-        const int bo = B.offset;                                                           \
-        const int bn = B.size[0] * B.size[1] * B.size[2];                                  \
-        const int cs = max(bo, lo), ce = min(bo + bn, hi);                                 \
-        for (int i = cs + (int)threadIdx.x; i < ce; i += blockDim.x) {                     \
-            const int l = i - bo;                                                          \
-            int p[3];                                                                      \
-            unflatten(l, B.size, p);                                                       \
-            __VA_ARGS__                                                                    \
-        }                                                                                  \
+// Sum the tile partials of each slot's system (one warp per slot, fixed order) into out[slot][k].
+// Only slots whose bit is set in `mask` are reduced.
+template <int NV>
+__device__ void system_sums(const double* partials, const TileSlots& S, unsigned mask, double (*out)[KR_NV]) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (warp < S.n && (mask & (1u << warp))) {
+        double acc[NV];
+#pragma unroll
+        for (int k = 0; k < NV; ++k) acc[k] = 0.0;
+        for (int t = S.t0[warp] + lane; t < S.t1[warp]; t += 32) {
+#pragma unroll
+            for (int k = 0; k < NV; ++k) acc[k] += __ldcg(partials + (size_t)t * KR_NV + k);
+        }
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            const double s = warp_sum(acc[k]);
+            if (lane == 0) out[warp][k] = s;
+        }
     }
+    __syncthreads();
+}
+
+// Write a tile partial (NV values, already block-summed) from thread 0.
+template <int NV>
+__device__ __forceinline__ void put_partial(double* partials, int tile, const double (&v)[NV]) {
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) partials[(size_t)tile * KR_NV + k] = v[k];
+    }
+}
 
 // One stencil row applied to a vector given by `load(j)`; TRANS applies the transposed matrix
 // (the coefficient of row j pointing back to i).
 template <typename T, int D, bool TRANS, typename F>
-__device__ __forceinline__ T spmv_row(const pict_domain_t& dom, const T* coef, int N, int i, const pict_block_t& B,
-                                      const int* p, F load) {
+__device__ __forceinline__ T spmv_row(const pict_domain_t& dom, const T* __restrict__ coef, int N, int i,
+                                      const pict_block_t& B, const int* p, F load) {
     T acc = coef[i] * load(i);
     const int stride[3] = {1, B.size[0], B.size[0] * B.size[1]};
 #pragma unroll
@@ -213,299 +235,490 @@ __device__ __forceinline__ double conv_crit(double sq, int normalized, int n) {
     return normalized ? nrm / sqrt((double)n) : nrm;
 }
 
+__device__ __forceinline__ int done_count(const int* ctrl) { return *(volatile const int*)(ctrl + CTRL_DONE); }
+
+__device__ __forceinline__ pict_solve_info_t fresh_info() {
+    pict_solve_info_t inf;
+    inf.final_residual = 0.0;
+    inf.used_iterations = -1;
+    inf.converged = 0;
+    inf.finite = 1;
+    inf.status = 0;
+    return inf;
+}
+
 // ---------------------------------------------------------------------------------------------
 // CG (cg.cu:236-427)
 // ---------------------------------------------------------------------------------------------
 template <typename T, int D, bool TRANS>
-__global__ void __launch_bounds__(512) k_cg(KArgs<T> a) {
+__global__ void __launch_bounds__(KR_THREADS) k_cg(KArgs<T> a) {
     const pict_domain_t& dom = a.dom;
     const int N = dom.num_cells;
-    const int G = a.G;
-    const int grp = blockIdx.x / G, rank = blockIdx.x % G;
+    __shared__ TileSlots S;
+    __shared__ double s_sum[KR_SLOTS][KR_NV];
+    __shared__ double s_rho[KR_SLOTS], s_beta[KR_SLOTS], s_alpha[KR_SLOTS];
+    __shared__ unsigned s_active;  // bit per slot
+    __shared__ pict_solve_info_t s_info[KR_SLOTS];
+    load_slots(dom, S);
+    const T* __restrict__ coef = a.coef;
+    const T* __restrict__ bv = a.b;
+    T* __restrict__ x = a.x;
+    T* __restrict__ r = a.r;
+    T* __restrict__ q = a.t;
+    T* pc = a.p0;
+    T* pn = a.p1;
     int phase = 0;
-    for (;;) {
-        const int s = next_system(a, grp, rank);
-        if (s < 0) return;
-        const int c0 = dom.sim_cells[s], c1 = dom.sim_cells[s + 1];
-        const int b0 = dom.sim_blocks[s], b1 = dom.sim_blocks[s + 1];
-        const int n = c1 - c0;
-        const int chunk = (n + G - 1) / G;
-        const int lo = c0 + rank * chunk, hi = min(c1, lo + chunk);
-        const T* coef = a.coef;
-        const T* bv = a.b;
-        T* x = a.x;
-        T* r = a.r;
-        T* q = a.t;
-        T* pc = a.p0;
-        T* pn = a.p1;
-        // initial residual r = b - A x
+    double* part = a.partials;
+    const size_t pstride = (size_t)dom.num_tiles * KR_NV;
+
+    // ---- initial residual r = b - A x, |r|^2, |b|^2 per tile
+    for (int j = 0; j < S.n; ++j) {
+        const pict_block_t& B = dom.blocks[S.block[j]];
         double acc[2] = {0.0, 0.0};
-        KR_FOR_CELLS({
+        const int s0 = S.start[j], s1 = s0 + S.count[j];
+        for (int i = s0 + threadIdx.x; i < s1; i += blockDim.x) {
+            int p[3];
+            unflatten(i - B.offset, B.size, p);
             const T bi = bv[i];
             T ri = bi;
-            if (!a.x_zero) ri -= spmv_row<T, D, TRANS>(dom, coef, N, i, B, p, [&](int j) { return x[j]; });
+            if (!a.x_zero) ri -= spmv_row<T, D, TRANS>(dom, coef, N, i, B, p, [&](int jj) { return x[jj]; });
             r[i] = ri;
             pc[i] = T(0);
-            if (a.x_zero) x[i] = T(0);
             acc[0] += (double)ri * (double)ri;
             acc[1] += (double)bi * (double)bi;
-        })
-        if (!reduce<2>(acc, a, grp, rank, phase)) return;
-        pict_solve_info_t info;
-        info.final_residual = 0.0;
-        info.used_iterations = -1;
-        info.converged = 0;
-        info.finite = 1;
-        info.status = 0;
-        if (acc[1] == 0.0) {
-            KR_FOR_CELLS({ x[i] = T(0); })
-            info.converged = 1;
-            info.used_iterations = 0;
-        } else {
-            double rho = acc[0];
-            double beta = 0.0;
-            for (int it = 0; it < a.maxit; ++it) {
-                // p <- r + beta p (on the fly for neighbours), q = A p
-                double pq[1] = {0.0};
-                const T bt = (T)beta;
-                KR_FOR_CELLS({
-                    const T pi = r[i] + bt * pc[i];
-                    const T qi = spmv_row<T, D, TRANS>(dom, coef, N, i, B, p, [&](int j) { return r[j] + bt * pc[j]; });
-                    pn[i] = pi;
-                    q[i] = qi;
-                    pq[0] += (double)pi * (double)qi;
-                })
-                if (!reduce<1>(pq, a, grp, rank, phase)) return;
-                const double alpha = rho / pq[0];
-                const T at = (T)alpha;
-                double rr[1] = {0.0};
-                KR_FOR_CELLS({
-                    x[i] += at * pn[i];
-                    const T ri = r[i] - at * q[i];
-                    r[i] = ri;
-                    rr[0] += (double)ri * (double)ri;
-                })
-                if (!reduce<1>(rr, a, grp, rank, phase)) return;
-                const double crit = conv_crit(rr[0], a.normalized, n);
-                info.used_iterations = it;
-                info.final_residual = crit;
-                if (!isfinite(crit)) { info.finite = 0; break; }
-                if (crit < a.tol) { info.converged = 1; break; }
-                beta = rr[0] / rho;
-                rho = rr[0];
-                T* tmp = pc; pc = pn; pn = tmp;
-            }
         }
-        if (a.sub_mean || a.write_bp) {
-            double sm[1] = {0.0};
-            if (a.sub_mean) {
-                KR_FOR_CELLS({ sm[0] += (double)x[i]; })
-                if (!reduce<1>(sm, a, grp, rank, phase)) return;
+        block_sum<2>(acc);
+        put_partial<2>(part + phase * pstride, S.tile[j], acc);
+    }
+    if (!grid_barrier(a.ctrl)) return;
+    system_sums<2>(part + phase * pstride, S, 0xffffffffu, s_sum);
+    phase ^= 1;
+    if (threadIdx.x == 0) {
+        unsigned act = 0;
+        for (int j = 0; j < S.n; ++j) {
+            pict_solve_info_t inf = fresh_info();
+            s_rho[j] = s_sum[j][0];
+            s_beta[j] = 0.0;
+            if (s_sum[j][1] == 0.0) {
+                inf.converged = 1;
+                inf.used_iterations = 0;
+                if (S.owner[j]) atomicAdd(a.ctrl + CTRL_DONE, 1);
+            } else {
+                act |= 1u << j;
             }
-            const T mean = a.sub_mean ? (T)(sm[0] / (double)n) : T(0);
-            KR_FOR_CELLS({
+            s_info[j] = inf;
+        }
+        s_active = act;
+    }
+    __syncthreads();
+    // x = 0 where the iteration starts from zero or the right-hand side vanishes
+    for (int j = 0; j < S.n; ++j) {
+        if (!a.x_zero && ((s_active >> j) & 1u)) continue;
+        for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) x[i] = T(0);
+    }
+
+    for (int it = 0; it < a.maxit; ++it) {
+        // phase 1: p <- r + beta p (on the fly for neighbours), q = A p, p.q
+        for (int j = 0; j < S.n; ++j) {
+            if (!((s_active >> j) & 1u)) continue;
+            const pict_block_t& B = dom.blocks[S.block[j]];
+            const T bt = (T)s_beta[j];
+            double acc[1] = {0.0};
+            const int s0 = S.start[j], s1 = s0 + S.count[j];
+            T pi[KR_CPT], qi[KR_CPT];
+#pragma unroll
+            for (int k = 0; k < KR_CPT; ++k) {
+                const int i = s0 + threadIdx.x + k * blockDim.x;
+                if (i < s1) {
+                    int p[3];
+                    unflatten(i - B.offset, B.size, p);
+                    pi[k] = r[i] + bt * pc[i];
+                    qi[k] = spmv_row<T, D, TRANS>(dom, coef, N, i, B, p, [&](int jj) { return r[jj] + bt * pc[jj]; });
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < KR_CPT; ++k) {
+                const int i = s0 + threadIdx.x + k * blockDim.x;
+                if (i < s1) {
+                    pn[i] = pi[k];
+                    q[i] = qi[k];
+                    acc[0] += (double)pi[k] * (double)qi[k];
+                }
+            }
+            block_sum<1>(acc);
+            put_partial<1>(part + phase * pstride, S.tile[j], acc);
+        }
+        if (!grid_barrier(a.ctrl)) return;
+        if (done_count(a.ctrl) == dom.num_sims) break;
+        system_sums<1>(part + phase * pstride, S, s_active, s_sum);
+        phase ^= 1;
+        if ((int)threadIdx.x < S.n && ((s_active >> threadIdx.x) & 1u))
+            s_alpha[threadIdx.x] = s_rho[threadIdx.x] / s_sum[threadIdx.x][0];
+        __syncthreads();
+        // phase 2: x += alpha p, r -= alpha q, r.r
+        for (int j = 0; j < S.n; ++j) {
+            if (!((s_active >> j) & 1u)) continue;
+            const T al = (T)s_alpha[j];
+            double acc[1] = {0.0};
+            const int s0 = S.start[j], s1 = s0 + S.count[j];
+#pragma unroll
+            for (int k = 0; k < KR_CPT; ++k) {
+                const int i = s0 + threadIdx.x + k * blockDim.x;
+                if (i < s1) {
+                    x[i] += al * pn[i];
+                    const T ri = r[i] - al * q[i];
+                    r[i] = ri;
+                    acc[0] += (double)ri * (double)ri;
+                }
+            }
+            block_sum<1>(acc);
+            put_partial<1>(part + phase * pstride, S.tile[j], acc);
+        }
+        if (!grid_barrier(a.ctrl)) return;
+        system_sums<1>(part + phase * pstride, S, s_active, s_sum);
+        phase ^= 1;
+        if (threadIdx.x == 0) {
+            unsigned act = s_active;
+            for (int j = 0; j < S.n; ++j) {
+                if (!((act >> j) & 1u)) continue;
+                const double rr = s_sum[j][0];
+                const int n = dom.sim_cells[S.sim[j] + 1] - dom.sim_cells[S.sim[j]];
+                const double crit = conv_crit(rr, a.normalized, n);
+                s_info[j].used_iterations = it;
+                s_info[j].final_residual = crit;
+                bool fin = false;
+                if (!isfinite(crit)) { s_info[j].finite = 0; fin = true; }
+                else if (crit < a.tol) { s_info[j].converged = 1; fin = true; }
+                else {
+                    s_beta[j] = rr / s_rho[j];
+                    s_rho[j] = rr;
+                }
+                if (fin) {
+                    act &= ~(1u << j);
+                    if (S.owner[j]) atomicAdd(a.ctrl + CTRL_DONE, 1);
+                }
+            }
+            s_active = act;
+        }
+        __syncthreads();
+        T* tmp = pc; pc = pn; pn = tmp;
+    }
+    // ---- mean removal (sim.py:1243-1244) and copy into the blocks' pressure
+    if (a.sub_mean || a.write_bp) {
+        if (a.sub_mean) {
+            for (int j = 0; j < S.n; ++j) {
+                double acc[1] = {0.0};
+                for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) acc[0] += (double)x[i];
+                block_sum<1>(acc);
+                put_partial<1>(part + phase * pstride, S.tile[j], acc);
+            }
+            if (!grid_barrier(a.ctrl)) return;
+            system_sums<1>(part + phase * pstride, S, 0xffffffffu, s_sum);
+            phase ^= 1;
+        }
+        for (int j = 0; j < S.n; ++j) {
+            const pict_block_t& B = dom.blocks[S.block[j]];
+            const int n = dom.sim_cells[S.sim[j] + 1] - dom.sim_cells[S.sim[j]];
+            const T mean = a.sub_mean ? (T)(s_sum[j][0] / (double)n) : T(0);
+            T* pb = reinterpret_cast<T*>(B.pressure);
+            for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) {
                 const T v = x[i] - mean;
                 x[i] = v;
-                if (a.write_bp) reinterpret_cast<T*>(B.pressure)[l] = v;
-            })
+                if (a.write_bp) pb[i - B.offset] = v;
+            }
         }
-        if (rank == 0 && threadIdx.x == 0) a.info[s] = info;
-        __syncthreads();
     }
+    if ((int)threadIdx.x < S.n && S.owner[threadIdx.x]) a.info[S.sim[threadIdx.x]] = s_info[threadIdx.x];
 }
 
 // ---------------------------------------------------------------------------------------------
 // BiCGStab without preconditioner (bicg.cu:240-360), NR right-hand sides sharing the matrix
 // ---------------------------------------------------------------------------------------------
 template <typename T, int D, int NR, bool TRANS>
-__global__ void __launch_bounds__(512) k_bicgstab(KArgs<T> a) {
+__global__ void __launch_bounds__(KR_THREADS) k_bicgstab(KArgs<T> a) {
     const pict_domain_t& dom = a.dom;
     const int N = dom.num_cells;
-    const int G = a.G;
-    const int grp = blockIdx.x / G, rank = blockIdx.x % G;
+    const size_t NS = (size_t)N;
+    __shared__ TileSlots S;
+    __shared__ double s_sum[KR_SLOTS][KR_NV];
+    __shared__ double s_rho[KR_SLOTS][NR], s_alpha[KR_SLOTS][NR], s_omega[KR_SLOTS][NR], s_beta[KR_SLOTS][NR],
+        s_rwr[KR_SLOTS][NR];
+    __shared__ unsigned s_act[KR_SLOTS];  // bit per component
+    __shared__ unsigned s_any;            // bit per slot with an active component
+    __shared__ pict_solve_info_t s_info[KR_SLOTS][NR];
+    load_slots(dom, S);
+    const T* __restrict__ coef = a.coef;
+    T* __restrict__ x = a.x;
+    T* __restrict__ r = a.r;
+    const T* __restrict__ rw = a.rw;
+    T* __restrict__ tv = a.t;
+    T* pc = a.p0;
+    T* pn = a.p1;
+    T* vc = a.v0;
+    T* vn = a.v1;
     int phase = 0;
-    for (;;) {
-        const int s = next_system(a, grp, rank);
-        if (s < 0) return;
-        const int c0 = dom.sim_cells[s], c1 = dom.sim_cells[s + 1];
-        const int b0 = dom.sim_blocks[s], b1 = dom.sim_blocks[s + 1];
-        const int n = c1 - c0;
-        const int chunk = (n + G - 1) / G;
-        const int lo = c0 + rank * chunk, hi = min(c1, lo + chunk);
-        const T* coef = a.coef;
-        const size_t NS = (size_t)N;
-        T* pc = a.p0; T* pn = a.p1;
-        T* vc = a.v0; T* vn = a.v1;
-        // init: r = b - A x, rw = r, p = v = 0
+    double* part = a.partials;
+    const size_t pstride = (size_t)dom.num_tiles * KR_NV;
+    const int total = dom.num_sims * NR;
+
+    // ---- init: r = b - A x, rw = r, p = v = 0
+    for (int j = 0; j < S.n; ++j) {
+        const pict_block_t& B = dom.blocks[S.block[j]];
         double acc[2 * NR];
 #pragma unroll
         for (int k = 0; k < 2 * NR; ++k) acc[k] = 0.0;
-        KR_FOR_CELLS({
+        for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) {
+            int p[3];
+            unflatten(i - B.offset, B.size, p);
 #pragma unroll
             for (int c = 0; c < NR; ++c) {
-                const T* xc = a.x + c * NS;
+                const T* xc = x + c * NS;
                 const T bi = a.b[c * NS + i];
                 T ri = bi;
-                if (!a.x_zero) ri -= spmv_row<T, D, TRANS>(dom, coef, N, i, B, p, [&](int j) { return xc[j]; });
-                if (a.x_zero) a.x[c * NS + i] = T(0);
-                a.r[c * NS + i] = ri;
+                if (!a.x_zero) ri -= spmv_row<T, D, TRANS>(dom, coef, N, i, B, p, [&](int jj) { return xc[jj]; });
+                r[c * NS + i] = ri;
                 a.rw[c * NS + i] = ri;
                 pc[c * NS + i] = T(0);
                 vc[c * NS + i] = T(0);
                 acc[c] += (double)ri * (double)ri;
                 acc[NR + c] += (double)bi * (double)bi;
             }
-        })
-        if (!reduce<2 * NR>(acc, a, grp, rank, phase)) return;
-        pict_solve_info_t info[NR];
-        double rho[NR], alpha[NR], omega[NR], beta[NR], rwr[NR];
-        int active = 0, zero = 0;
-#pragma unroll
-        for (int c = 0; c < NR; ++c) {
-            info[c].final_residual = 0.0;
-            info[c].used_iterations = -1;
-            info[c].converged = 0;
-            info[c].finite = 1;
-            info[c].status = 0;
-            rho[c] = 0.0; alpha[c] = 0.0; omega[c] = 0.0; beta[c] = 0.0;
-            rwr[c] = acc[c];
-            if (acc[NR + c] == 0.0) {
-                zero |= 1 << c;
-                info[c].converged = 1;
-                info[c].used_iterations = 0;
-            } else {
-                const double nrmr0 = conv_crit(acc[c], a.normalized, n);
-                if (nrmr0 < a.tol) {
-                    info[c].converged = 1;
-                    info[c].used_iterations = -1;
-                    info[c].final_residual = nrmr0;
-                } else {
-                    active |= 1 << c;
-                }
-            }
         }
-        if (zero) {
-            KR_FOR_CELLS({
-#pragma unroll
-                for (int c = 0; c < NR; ++c)
-                    if (zero & (1 << c)) a.x[c * NS + i] = T(0);
-            })
-        }
-        for (int it = 0; it < a.maxit && active; ++it) {
-#pragma unroll
+        block_sum<2 * NR>(acc);
+        put_partial<2 * NR>(part + phase * pstride, S.tile[j], acc);
+    }
+    if (!grid_barrier(a.ctrl)) return;
+    system_sums<2 * NR>(part + phase * pstride, S, 0xffffffffu, s_sum);
+    phase ^= 1;
+    if (threadIdx.x == 0) {
+        unsigned any = 0;
+        for (int j = 0; j < S.n; ++j) {
+            unsigned act = 0;
+            const int n = dom.sim_cells[S.sim[j] + 1] - dom.sim_cells[S.sim[j]];
             for (int c = 0; c < NR; ++c) {
-                if (!(active & (1 << c))) continue;
-                const double rhop = rho[c];
-                rho[c] = rwr[c];
-                beta[c] = it > 0 ? (rho[c] / rhop) * (alpha[c] / omega[c]) : 0.0;
+                pict_solve_info_t inf = fresh_info();
+                s_rho[j][c] = 0.0; s_alpha[j][c] = 0.0; s_omega[j][c] = 0.0; s_beta[j][c] = 0.0;
+                s_rwr[j][c] = s_sum[j][c];
+                bool fin = false;
+                if (s_sum[j][NR + c] == 0.0) {
+                    inf.converged = 1;
+                    inf.used_iterations = 0;
+                    fin = true;
+                } else {
+                    const double nrmr0 = conv_crit(s_sum[j][c], a.normalized, n);
+                    if (nrmr0 < a.tol) {
+                        inf.converged = 1;
+                        inf.used_iterations = -1;
+                        inf.final_residual = nrmr0;
+                        fin = true;
+                    } else {
+                        act |= 1u << c;
+                    }
+                }
+                if (fin && S.owner[j]) atomicAdd(a.ctrl + CTRL_DONE, 1);
+                s_info[j][c] = inf;
             }
-            // phase A: p = r + beta (p - omega v) on the fly, v = A p, rw.v
-            double rwv[NR];
+            s_act[j] = act;
+            if (act) any |= 1u << j;
+        }
+        s_any = any;
+    }
+    __syncthreads();
+    // x = 0 where the iteration starts from zero or the right-hand side vanishes
+    for (int j = 0; j < S.n; ++j) {
+        for (int c = 0; c < NR; ++c) {
+            const bool zero_rhs = s_info[j][c].converged && s_info[j][c].used_iterations == 0;
+            if (a.x_zero || zero_rhs)
+                for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) x[c * NS + i] = T(0);
+        }
+    }
+
+    for (int it = 0; it < a.maxit; ++it) {
+        if ((int)threadIdx.x < S.n) {
+            const int j = threadIdx.x;
+            for (int c = 0; c < NR; ++c) {
+                if (!((s_act[j] >> c) & 1u)) continue;
+                const double rhop = s_rho[j][c];
+                s_rho[j][c] = s_rwr[j][c];
+                s_beta[j][c] = it > 0 ? (s_rho[j][c] / rhop) * (s_alpha[j][c] / s_omega[j][c]) : 0.0;
+            }
+        }
+        __syncthreads();
+        // phase A: p = r + beta (p - omega v) on the fly, v = A p, rw.v
+        for (int j = 0; j < S.n; ++j) {
+            if (!((s_any >> j) & 1u)) continue;
+            const unsigned act = s_act[j];
+            const pict_block_t& B = dom.blocks[S.block[j]];
+            double acc[NR];
 #pragma unroll
-            for (int c = 0; c < NR; ++c) rwv[c] = 0.0;
-            KR_FOR_CELLS({
+            for (int c = 0; c < NR; ++c) acc[c] = 0.0;
+            for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) {
+                int p[3];
+                unflatten(i - B.offset, B.size, p);
 #pragma unroll
                 for (int c = 0; c < NR; ++c) {
-                    if (!(active & (1 << c))) continue;
-                    const T bt = (T)beta[c], om = (T)omega[c];
-                    const T* rc = a.r + c * NS;
+                    if (!((act >> c) & 1u)) continue;
+                    const T bt = (T)s_beta[j][c], om = (T)s_omega[j][c];
+                    const T* rc = r + c * NS;
                     const T* pcc = pc + c * NS;
                     const T* vcc = vc + c * NS;
                     const T pi = rc[i] + bt * (pcc[i] - om * vcc[i]);
                     const T vi = spmv_row<T, D, TRANS>(dom, coef, N, i, B, p,
-                                                       [&](int j) { return rc[j] + bt * (pcc[j] - om * vcc[j]); });
+                                                       [&](int jj) { return rc[jj] + bt * (pcc[jj] - om * vcc[jj]); });
                     pn[c * NS + i] = pi;
                     vn[c * NS + i] = vi;
-                    rwv[c] += (double)a.rw[c * NS + i] * (double)vi;
-                }
-            })
-            if (!reduce<NR>(rwv, a, grp, rank, phase)) return;
-#pragma unroll
-            for (int c = 0; c < NR; ++c)
-                if (active & (1 << c)) alpha[c] = rho[c] / rwv[c];
-            // phase B: s = r - alpha v (in r), x += alpha p, |s|^2
-            double ss[NR];
-#pragma unroll
-            for (int c = 0; c < NR; ++c) ss[c] = 0.0;
-            KR_FOR_CELLS({
-#pragma unroll
-                for (int c = 0; c < NR; ++c) {
-                    if (!(active & (1 << c))) continue;
-                    const T al = (T)alpha[c];
-                    const T si = a.r[c * NS + i] - al * vn[c * NS + i];
-                    a.r[c * NS + i] = si;
-                    a.x[c * NS + i] += al * pn[c * NS + i];
-                    ss[c] += (double)si * (double)si;
-                }
-            })
-            if (!reduce<NR>(ss, a, grp, rank, phase)) return;
-#pragma unroll
-            for (int c = 0; c < NR; ++c) {
-                if (!(active & (1 << c))) continue;
-                const double nr = conv_crit(ss[c], a.normalized, n);
-                info[c].used_iterations = it;
-                info[c].final_residual = nr;
-                if (!isfinite(nr)) { info[c].finite = 0; active &= ~(1 << c); }
-                else if (nr < a.tol) { info[c].converged = 1; active &= ~(1 << c); }
-            }
-            if (!active) break;
-            // phase C: t = A s, t.s, t.t
-            double ts[2 * NR];
-#pragma unroll
-            for (int k = 0; k < 2 * NR; ++k) ts[k] = 0.0;
-            KR_FOR_CELLS({
-#pragma unroll
-                for (int c = 0; c < NR; ++c) {
-                    if (!(active & (1 << c))) continue;
-                    const T* sc = a.r + c * NS;
-                    const T ti = spmv_row<T, D, TRANS>(dom, coef, N, i, B, p, [&](int j) { return sc[j]; });
-                    a.t[c * NS + i] = ti;
-                    ts[2 * c] += (double)ti * (double)sc[i];
-                    ts[2 * c + 1] += (double)ti * (double)ti;
-                }
-            })
-            if (!reduce<2 * NR>(ts, a, grp, rank, phase)) return;
-#pragma unroll
-            for (int c = 0; c < NR; ++c)
-                if (active & (1 << c)) omega[c] = ts[2 * c] / ts[2 * c + 1];
-            // phase D: x += omega s, r = s - omega t, r.r, rw.r
-            double rr[2 * NR];
-#pragma unroll
-            for (int k = 0; k < 2 * NR; ++k) rr[k] = 0.0;
-            KR_FOR_CELLS({
-#pragma unroll
-                for (int c = 0; c < NR; ++c) {
-                    if (!(active & (1 << c))) continue;
-                    const T om = (T)omega[c];
-                    const T si = a.r[c * NS + i];
-                    a.x[c * NS + i] += om * si;
-                    const T ri = si - om * a.t[c * NS + i];
-                    a.r[c * NS + i] = ri;
-                    rr[2 * c] += (double)ri * (double)ri;
-                    rr[2 * c + 1] += (double)a.rw[c * NS + i] * (double)ri;
-                }
-            })
-            if (!reduce<2 * NR>(rr, a, grp, rank, phase)) return;
-#pragma unroll
-            for (int c = 0; c < NR; ++c) {
-                if (!(active & (1 << c))) continue;
-                rwr[c] = rr[2 * c + 1];
-                const double nr = conv_crit(rr[2 * c], a.normalized, n);
-                info[c].final_residual = nr;
-                if (nr < a.tol) {
-                    info[c].converged = 1;
-                    info[c].used_iterations = it + 1;
-                    active &= ~(1 << c);
+                    acc[c] += (double)rw[c * NS + i] * (double)vi;
                 }
             }
-            T* tp = pc; pc = pn; pn = tp;
-            T* tv = vc; vc = vn; vn = tv;
+            block_sum<NR>(acc);
+            put_partial<NR>(part + phase * pstride, S.tile[j], acc);
         }
-        if (rank == 0 && threadIdx.x == 0) {
-#pragma unroll
-            for (int c = 0; c < NR; ++c) a.info[s * a.nrhs + c] = info[c];
+        if (!grid_barrier(a.ctrl)) return;
+        if (done_count(a.ctrl) == total) break;
+        system_sums<NR>(part + phase * pstride, S, s_any, s_sum);
+        phase ^= 1;
+        if ((int)threadIdx.x < S.n) {
+            const int j = threadIdx.x;
+            for (int c = 0; c < NR; ++c)
+                if ((s_act[j] >> c) & 1u) s_alpha[j][c] = s_rho[j][c] / s_sum[j][c];
         }
         __syncthreads();
+        // phase B: s = r - alpha v (in r), x += alpha p, |s|^2
+        for (int j = 0; j < S.n; ++j) {
+            if (!((s_any >> j) & 1u)) continue;
+            const unsigned act = s_act[j];
+            double acc[NR];
+#pragma unroll
+            for (int c = 0; c < NR; ++c) acc[c] = 0.0;
+            for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) {
+#pragma unroll
+                for (int c = 0; c < NR; ++c) {
+                    if (!((act >> c) & 1u)) continue;
+                    const T al = (T)s_alpha[j][c];
+                    const T si = r[c * NS + i] - al * vn[c * NS + i];
+                    r[c * NS + i] = si;
+                    x[c * NS + i] += al * pn[c * NS + i];
+                    acc[c] += (double)si * (double)si;
+                }
+            }
+            block_sum<NR>(acc);
+            put_partial<NR>(part + phase * pstride, S.tile[j], acc);
+        }
+        if (!grid_barrier(a.ctrl)) return;
+        system_sums<NR>(part + phase * pstride, S, s_any, s_sum);
+        phase ^= 1;
+        if (threadIdx.x == 0) {
+            unsigned any = 0;
+            for (int j = 0; j < S.n; ++j) {
+                unsigned act = s_act[j];
+                const int n = dom.sim_cells[S.sim[j] + 1] - dom.sim_cells[S.sim[j]];
+                for (int c = 0; c < NR; ++c) {
+                    if (!((act >> c) & 1u)) continue;
+                    const double nr = conv_crit(s_sum[j][c], a.normalized, n);
+                    s_info[j][c].used_iterations = it;
+                    s_info[j][c].final_residual = nr;
+                    bool fin = false;
+                    if (!isfinite(nr)) { s_info[j][c].finite = 0; fin = true; }
+                    else if (nr < a.tol) { s_info[j][c].converged = 1; fin = true; }
+                    if (fin) {
+                        act &= ~(1u << c);
+                        if (S.owner[j]) atomicAdd(a.ctrl + CTRL_DONE, 1);
+                    }
+                }
+                s_act[j] = act;
+                if (act) any |= 1u << j;
+            }
+            s_any = any;
+        }
+        __syncthreads();
+        // phase C: t = A s, t.s, t.t
+        for (int j = 0; j < S.n; ++j) {
+            if (!((s_any >> j) & 1u)) continue;
+            const unsigned act = s_act[j];
+            const pict_block_t& B = dom.blocks[S.block[j]];
+            double acc[2 * NR];
+#pragma unroll
+            for (int k = 0; k < 2 * NR; ++k) acc[k] = 0.0;
+            for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) {
+                int p[3];
+                unflatten(i - B.offset, B.size, p);
+#pragma unroll
+                for (int c = 0; c < NR; ++c) {
+                    if (!((act >> c) & 1u)) continue;
+                    const T* sc = r + c * NS;
+                    const T ti = spmv_row<T, D, TRANS>(dom, coef, N, i, B, p, [&](int jj) { return sc[jj]; });
+                    tv[c * NS + i] = ti;
+                    acc[2 * c] += (double)ti * (double)sc[i];
+                    acc[2 * c + 1] += (double)ti * (double)ti;
+                }
+            }
+            block_sum<2 * NR>(acc);
+            put_partial<2 * NR>(part + phase * pstride, S.tile[j], acc);
+        }
+        if (!grid_barrier(a.ctrl)) return;
+        system_sums<2 * NR>(part + phase * pstride, S, s_any, s_sum);
+        phase ^= 1;
+        if ((int)threadIdx.x < S.n) {
+            const int j = threadIdx.x;
+            for (int c = 0; c < NR; ++c)
+                if ((s_act[j] >> c) & 1u) s_omega[j][c] = s_sum[j][2 * c] / s_sum[j][2 * c + 1];
+        }
+        __syncthreads();
+        // phase D: x += omega s, r = s - omega t, r.r, rw.r
+        for (int j = 0; j < S.n; ++j) {
+            if (!((s_any >> j) & 1u)) continue;
+            const unsigned act = s_act[j];
+            double acc[2 * NR];
+#pragma unroll
+            for (int k = 0; k < 2 * NR; ++k) acc[k] = 0.0;
+            for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) {
+#pragma unroll
+                for (int c = 0; c < NR; ++c) {
+                    if (!((act >> c) & 1u)) continue;
+                    const T om = (T)s_omega[j][c];
+                    const T si = r[c * NS + i];
+                    x[c * NS + i] += om * si;
+                    const T ri = si - om * tv[c * NS + i];
+                    r[c * NS + i] = ri;
+                    acc[2 * c] += (double)ri * (double)ri;
+                    acc[2 * c + 1] += (double)rw[c * NS + i] * (double)ri;
+                }
+            }
+            block_sum<2 * NR>(acc);
+            put_partial<2 * NR>(part + phase * pstride, S.tile[j], acc);
+        }
+        if (!grid_barrier(a.ctrl)) return;
+        system_sums<2 * NR>(part + phase * pstride, S, s_any, s_sum);
+        phase ^= 1;
+        if (threadIdx.x == 0) {
+            unsigned any = 0;
+            for (int j = 0; j < S.n; ++j) {
+                unsigned act = s_act[j];
+                const int n = dom.sim_cells[S.sim[j] + 1] - dom.sim_cells[S.sim[j]];
+                for (int c = 0; c < NR; ++c) {
+                    if (!((act >> c) & 1u)) continue;
+                    s_rwr[j][c] = s_sum[j][2 * c + 1];
+                    const double nr = conv_crit(s_sum[j][2 * c], a.normalized, n);
+                    s_info[j][c].final_residual = nr;
+                    if (nr < a.tol) {
+                        s_info[j][c].converged = 1;
+                        s_info[j][c].used_iterations = it + 1;
+                        act &= ~(1u << c);
+                        if (S.owner[j]) atomicAdd(a.ctrl + CTRL_DONE, 1);
+                    }
+                }
+                s_act[j] = act;
+                if (act) any |= 1u << j;
+            }
+            s_any = any;
+        }
+        __syncthreads();
+        T* tp = pc; pc = pn; pn = tp;
+        T* tq = vc; vc = vn; vn = tq;
+    }
+    if ((int)threadIdx.x < S.n && S.owner[threadIdx.x]) {
+        const int j = threadIdx.x;
+        for (int c = 0; c < NR; ++c) a.info[S.sim[j] * a.nrhs + c] = s_info[j][c];
     }
 }
 
@@ -520,8 +733,8 @@ __global__ void k_init_info(pict_solve_info_t* info, int n) {
 }
 
 // status 1 for every system if any barrier timed out
-__global__ void k_finish_info(pict_solve_info_t* info, int n, const int* err) {
-    if (*err == 0) return;
+__global__ void k_finish_info(pict_solve_info_t* info, int n, const int* ctrl) {
+    if (ctrl[CTRL_ERR] == 0) return;
     PICT_CELL_LOOP(i, n) { info[i].status = 1; info[i].converged = 0; }
 }
 
@@ -529,101 +742,51 @@ __global__ void k_finish_info(pict_solve_info_t* info, int n, const int* err) {
 // host side: launch plan and workspace
 // ---------------------------------------------------------------------------------------------
 
-struct Plan {
-    int threads;
-    int G;
-    int ngroups;
-    bool coop;
-    int nvec;
-    int nrhs_launch;  // right-hand sides per launch
-    size_t header_bytes;
-    size_t vec_bytes;
-    size_t total;
-};
-
 static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 
-// Workspace header sized for the largest possible plan (32 CTAs per SM), so its layout does not
-// depend on the occupancy-derived plan: [queue, err] | group_sys[NG] | sync[NG][32] | partials.
-static int max_ctas() { return device_sm_count() * 32; }
-static int max_groups(const pict_domain_t* dom) { return dom->num_sims < max_ctas() ? dom->num_sims : max_ctas(); }
-static size_t off_group_sys() { return align256(256); }
-static size_t off_sync(const pict_domain_t* dom) { return off_group_sys() + align256(sizeof(int) * max_groups(dom)); }
-static size_t off_partials(const pict_domain_t* dom) { return off_sync(dom) + align256(sizeof(unsigned) * 32 * max_groups(dom)); }
+// workspace: ctrl (256 B) | partials [2][num_tiles][KR_NV] doubles | vectors
 static size_t header_bytes(const pict_domain_t* dom) {
-    return off_partials(dom) + align256(sizeof(double) * 2 * (size_t)max_ctas() * KR_NV);
+    return align256(256) + align256(sizeof(double) * 2 * (size_t)dom->num_tiles * KR_NV);
+}
+
+static int nrhs_per_launch(const pict_solve_params_t* prm) {
+    return prm->use_bicg ? (prm->nrhs > 3 ? 3 : prm->nrhs) : 1;
+}
+
+static size_t vec_bytes(const pict_domain_t* dom, const pict_solve_params_t* prm) {
+    const size_t esz = dom->dtype == PICT_F64 ? 8 : 4;
+    return align256(esz * (size_t)dom->num_cells * nrhs_per_launch(prm));
+}
+
+static size_t workspace_total(const pict_domain_t* dom, const pict_solve_params_t* prm) {
+    const int nvec = prm->use_bicg ? 7 : 4;  // bicg: r rw p0 p1 v0 v1 t; cg: r p0 p1 q
+    return header_bytes(dom) + vec_bytes(dom, prm) * nvec;
 }
 
 template <typename KernelT>
-static int max_coresident(KernelT kernel, int threads) {
+static int max_coresident(KernelT kernel) {
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) != cudaSuccess || per_sm < 1) per_sm = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, KR_THREADS, 0) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
     return per_sm * device_sm_count();
 }
 
-static Plan make_plan(const pict_domain_t* dom, const pict_solve_params_t* prm, int coresident) {
-    Plan P;
-    const size_t esz = dom->dtype == PICT_F64 ? 8 : 4;
-    P.nrhs_launch = prm->use_bicg ? (prm->nrhs > 3 ? 3 : prm->nrhs) : 1;
-    P.threads = prm->threads > 0 ? (prm->threads > 512 ? 512 : prm->threads) : 512;
-    int G = prm->group_size;
-    if (G <= 0) {
-        const int target = P.threads * 8;
-        G = (dom->max_sim_cells + target - 1) / target;
-        if (dom->num_sims > 1) {
-            const int share = coresident / dom->num_sims;
-            if (G > share) G = share;
-        }
-    }
-    if (G < 1) G = 1;
-    if (G > coresident) G = coresident;
-    P.G = G;
-    if (G == 1) {
-        P.ngroups = dom->num_sims < coresident ? dom->num_sims : coresident;
-        P.coop = false;
-    } else {
-        int ng = coresident / G;
-        if (ng > dom->num_sims) ng = dom->num_sims;
-        if (ng < 1) ng = 1;
-        P.ngroups = ng;
-        P.coop = true;
-    }
-    if (P.ngroups < 1) P.ngroups = 1;
-    P.nvec = prm->use_bicg ? 7 : 4;  // bicg: r rw p0 p1 v0 v1 t; cg: r p0 p1 q
-    P.header_bytes = header_bytes(dom);
-    P.vec_bytes = align256(esz * (size_t)dom->num_cells * P.nrhs_launch);
-    P.total = P.header_bytes + P.vec_bytes * P.nvec;
-    return P;
-}
-
-template <typename T, int D, bool TRANS>
-static int coresident_for(const pict_solve_params_t* prm, int threads) {
-    if (prm->use_bicg) {
-        const int nr = prm->nrhs >= 3 ? 3 : prm->nrhs;
-        if (nr == 1) return max_coresident(k_bicgstab<T, D, 1, TRANS>, threads);
-        if (nr == 2) return max_coresident(k_bicgstab<T, D, 2, TRANS>, threads);
-        return max_coresident(k_bicgstab<T, D, 3, TRANS>, threads);
-    }
-    return max_coresident(k_cg<T, D, TRANS>, threads);
-}
-
 template <typename T>
-static pict_status_t launch_kernel(void (*kernel)(KArgs<T>), const Plan& P, KArgs<T>& args, cudaStream_t st) {
+static pict_status_t launch_kernel(void (*kernel)(KArgs<T>), int grid, KArgs<T>& args, cudaStream_t st) {
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(P.ngroups * P.G);
-    cfg.blockDim = dim3(P.threads);
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(KR_THREADS);
     cfg.dynamicSmemBytes = 0;
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;
-    attr[0].val.cooperative = P.coop ? 1 : 0;
+    attr[0].val.cooperative = grid > 1 ? 1 : 0;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, args);
     if (e != cudaSuccess) {
         char buf[256];
-        snprintf(buf, sizeof(buf), "krylov launch (grid %d x %d threads, coop %d): %s", P.ngroups * P.G, P.threads,
-                 (int)P.coop, cudaGetErrorString(e));
+        snprintf(buf, sizeof(buf), "krylov launch (grid %d x %d threads): %s", grid, KR_THREADS, cudaGetErrorString(e));
         cudaGetLastError();
         return set_error(PICT_ERR_CUDA, buf);
     }
@@ -634,71 +797,63 @@ template <typename T, int D, bool TRANS>
 static pict_status_t run_solve(const pict_domain_t* dom, const void* coef, const void* rhs, void* x,
                                const pict_solve_params_t* prm, void* info_out, void* ws, int64_t ws_bytes,
                                cudaStream_t st) {
-    const int threads = prm->threads > 0 ? (prm->threads > 512 ? 512 : prm->threads) : 512;
-    const int cores = coresident_for<T, D, TRANS>(prm, threads);
-    const Plan P = make_plan(dom, prm, cores);
-    if ((int64_t)P.total > ws_bytes) return set_error(PICT_ERR_ARG, "solve: workspace too small");
+    if ((int64_t)workspace_total(dom, prm) > ws_bytes) return set_error(PICT_ERR_ARG, "solve: workspace too small");
+    if (dom->tile_cells > KR_MAX_TILE || dom->tile_cells <= 0 || !dom->tiles || !dom->sim_tiles || dom->num_tiles <= 0)
+        return set_error(PICT_ERR_ARG, "solve: invalid tile table (tile_cells must be in [1, 2048])");
     char* base = reinterpret_cast<char*>(ws);
-    int* queue = reinterpret_cast<int*>(base);
-    int* err = queue + 1;
-    int* group_sys = reinterpret_cast<int*>(base + off_group_sys());
-    unsigned* sync = reinterpret_cast<unsigned*>(base + off_sync(dom));
-    double* partials = reinterpret_cast<double*>(base + off_partials(dom));
-    const size_t off = P.header_bytes;
-    T* vec[7];
-    for (int k = 0; k < P.nvec; ++k) vec[k] = reinterpret_cast<T*>(base + off + P.vec_bytes * k);
+    int* ctrl = reinterpret_cast<int*>(base);
+    double* partials = reinterpret_cast<double*>(base + align256(256));
+    const size_t off = header_bytes(dom);
+    const size_t vb = vec_bytes(dom, prm);
+    const int nvec = prm->use_bicg ? 7 : 4;
+    T* vec[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    for (int k = 0; k < nvec; ++k) vec[k] = reinterpret_cast<T*>(base + off + vb * k);
 
     const int nrhs_total = prm->nrhs;
     pict_solve_info_t* info = reinterpret_cast<pict_solve_info_t*>(info_out);
-    {
-        const int ninfo = dom->num_sims * nrhs_total;
-        k_init_info<<<cell_grid(ninfo, 128), 128, 0, st>>>(info, ninfo);
-        pict_status_t s = check_launch("init_info");
-        if (s) return s;
-    }
+    const int ninfo = dom->num_sims * nrhs_total;
+    k_init_info<<<cell_grid(ninfo, 128), 128, 0, st>>>(info, ninfo);
+    pict_status_t s = check_launch("init_info");
+    if (s) return s;
     const size_t NS = (size_t)dom->num_cells;
-    for (int c0 = 0; c0 < nrhs_total; c0 += P.nrhs_launch) {
-        const int nr = (nrhs_total - c0) < P.nrhs_launch ? (nrhs_total - c0) : P.nrhs_launch;
-        if (cudaMemsetAsync(base, 0, P.header_bytes, st) != cudaSuccess) return check_launch("workspace memset");
+    const int per = nrhs_per_launch(prm);
+    for (int c0 = 0; c0 < nrhs_total; c0 += per) {
+        const int nr = (nrhs_total - c0) < per ? (nrhs_total - c0) : per;
+        if (cudaMemsetAsync(ctrl, 0, 256, st) != cudaSuccess) return check_launch("workspace memset");
         KArgs<T> a;
         a.dom = *dom;
         a.coef = reinterpret_cast<const T*>(coef);
         a.b = reinterpret_cast<const T*>(rhs) + c0 * NS;
         a.x = reinterpret_cast<T*>(x) + c0 * NS;
-        a.queue = queue;
-        a.err = err;
-        a.group_sys = group_sys;
-        a.sync = sync;
+        a.ctrl = ctrl;
         a.partials = partials;
         a.maxit = prm->max_iterations;
         a.tol = prm->tolerance;
         a.normalized = prm->convergence == PICT_CONV_NORM2_NORMALIZED;
-        a.G = P.G;
         a.x_zero = prm->x_is_zero;
         a.sub_mean = prm->subtract_mean;
         a.write_bp = prm->write_block_pressure;
-        pict_status_t s;
+        a.info = info + c0;
+        a.nrhs = nrhs_total;
+        void (*kern)(KArgs<T>) = nullptr;
         if (prm->use_bicg) {
             a.r = vec[0]; a.rw = vec[1]; a.p0 = vec[2]; a.p1 = vec[3]; a.v0 = vec[4]; a.v1 = vec[5]; a.t = vec[6];
-            // infos of this chunk: info[s*nrhs_total + c0 + c]; use a strided view via nrhs = nrhs_total
-            a.info = info + c0;
-            a.nrhs = nrhs_total;
-            if (nr == 1) s = launch_kernel<T>(k_bicgstab<T, D, 1, TRANS>, P, a, st);
-            else if (nr == 2) s = launch_kernel<T>(k_bicgstab<T, D, 2, TRANS>, P, a, st);
-            else s = launch_kernel<T>(k_bicgstab<T, D, 3, TRANS>, P, a, st);
+            kern = nr == 1 ? k_bicgstab<T, D, 1, TRANS> : (nr == 2 ? k_bicgstab<T, D, 2, TRANS> : k_bicgstab<T, D, 3, TRANS>);
         } else {
             a.r = vec[0]; a.p0 = vec[1]; a.p1 = vec[2]; a.t = vec[3];
             a.rw = nullptr; a.v0 = nullptr; a.v1 = nullptr;
-            a.info = info + c0;  // CG writes info[s] -> per-launch view; stride handled below
-            a.nrhs = 1;
-            if (nrhs_total == 1) {
-                s = launch_kernel<T>(k_cg<T, D, TRANS>, P, a, st);
-            } else {
-                return set_error(PICT_ERR_UNSUPPORTED, "CG with several right-hand sides per system: split on the host");
-            }
+            kern = k_cg<T, D, TRANS>;
         }
+        // grid: every CTA owns at most KR_SLOTS tiles; all CTAs must be co-resident
+        const int cores = max_coresident(kern);
+        int grid = dom->num_tiles < cores ? dom->num_tiles : cores;
+        if (prm->group_size > 0 && grid > prm->group_size) grid = prm->group_size;
+        const int min_grid = (dom->num_tiles + KR_SLOTS - 1) / KR_SLOTS;
+        if (grid < min_grid) grid = min_grid;
+        if (grid > cores) return set_error(PICT_ERR_ARG, "solve: too many tiles for one persistent launch (raise tile_cells)");
+        s = launch_kernel<T>(kern, grid, a, st);
         if (s) return s;
-        k_finish_info<<<1, 128, 0, st>>>(info, dom->num_sims * nrhs_total, err);
+        k_finish_info<<<1, 128, 0, st>>>(info, ninfo, ctrl);
         s = check_launch("finish_info");
         if (s) return s;
     }
@@ -713,10 +868,7 @@ extern "C" {
 
 int64_t pict_solve_workspace_bytes(const pict_domain_t* dom, const pict_solve_params_t* prm) {
     if (!dom || !prm) return -1;
-    // vectors do not depend on the launch plan and the header is sized for the largest plan
-    const Plan P = make_plan(dom, prm, max_ctas());
-    const size_t t = P.total;
-    return (int64_t)t;
+    return (int64_t)workspace_total(dom, prm);
 }
 
 pict_status_t pict_solve(const pict_domain_t* dom, const void* coef, const void* rhs, void* x,

@@ -116,3 +116,33 @@ extern "C" pict_status_t pict_build_topology(const pict_block_t* blocks, int32_t
     }
     return PICT_OK;
 }
+
+extern "C" pict_status_t pict_build_tiles(const pict_block_t* blocks, int32_t num_blocks, int32_t num_sims,
+                                          int32_t tile_cells, int32_t* tiles, int32_t max_tiles, int32_t* sim_tiles,
+                                          int32_t* num_tiles_out) {
+    using pict::set_error;
+    if (!blocks || !sim_tiles || !num_tiles_out || num_blocks <= 0 || num_sims <= 0 || tile_cells <= 0)
+        return set_error(PICT_ERR_ARG, "tiles: invalid argument");
+    int32_t n = 0;
+    int32_t sim = 0;
+    sim_tiles[0] = 0;
+    for (int b = 0; b < num_blocks; ++b) {
+        const pict_block_t& B = blocks[b];
+        if (B.sim < sim || B.sim >= num_sims) return set_error(PICT_ERR_ARG, "tiles: blocks must be ordered by system");
+        while (sim < B.sim) sim_tiles[++sim] = n;
+        const int cells = B.size[0] * B.size[1] * B.size[2];
+        for (int c = 0; c < cells; c += tile_cells) {
+            if (tiles && n < max_tiles) {
+                tiles[4 * n + 0] = B.sim;
+                tiles[4 * n + 1] = b;
+                tiles[4 * n + 2] = B.offset + c;
+                tiles[4 * n + 3] = (cells - c) < tile_cells ? (cells - c) : tile_cells;
+            }
+            ++n;
+        }
+    }
+    while (sim < num_sims) sim_tiles[++sim] = n;
+    *num_tiles_out = n;
+    if (!tiles || n > max_tiles) return set_error(PICT_ERR_ARG, "tiles: output buffer too small");
+    return PICT_OK;
+}
