@@ -139,6 +139,9 @@ typedef struct pict_solve_params {
     int32_t threads;           /* threads per CTA (0: automatic) */
     int32_t subtract_mean;     /* 1: x -= mean(x) per system after the solve (sim.py:1243-1244) */
     int32_t write_block_pressure; /* 1: also copy x into the blocks' pressure (CopyPressureResultToBlocks) */
+    int32_t variant;           /* CG only: 0 classic order (cg.cu:236-427, two reductions per iteration),
+                                  1 single-reduction recurrence (Chronopoulos-Gear): same iterates in exact
+                                  arithmetic, one grid-wide reduction per iteration */
     double tolerance;
 } pict_solve_params_t;
 

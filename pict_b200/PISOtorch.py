@@ -1858,7 +1858,7 @@ class _Workspace:
 
 
 def _solve_params(nrhs, maxit, tol, conv, use_bicg, transpose, x_zero=False, subtract_mean=False,
-                  write_block_pressure=False, group_size=0, threads=0):
+                  write_block_pressure=False, group_size=0, threads=0, variant=0):
     p = SolveParams()
     p.max_iterations = int(maxit)
     p.use_bicg = int(bool(use_bicg))
@@ -1870,6 +1870,7 @@ def _solve_params(nrhs, maxit, tol, conv, use_bicg, transpose, x_zero=False, sub
     p.threads = int(threads)
     p.subtract_mean = int(bool(subtract_mean))
     p.write_block_pressure = int(bool(write_block_pressure))
+    p.variant = int(variant)
     p.tolerance = float(tol)
     return p
 

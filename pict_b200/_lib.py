@@ -119,6 +119,7 @@ class SolveParams(ctypes.Structure):
         ("threads", c_i32),
         ("subtract_mean", c_i32),
         ("write_block_pressure", c_i32),
+        ("variant", c_i32),
         ("tolerance", ctypes.c_double),
     ]
 

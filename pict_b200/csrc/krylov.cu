@@ -139,6 +139,23 @@ __device__ __forceinline__ void block_sum(double (&v)[NV]) {
     __syncthreads();
 }
 
+// Per-phase tile partials: every tile's values are reduced within each warp (shuffles, no block
+// synchronisation) into s_warp[slot][warp][k]; after all tiles of the phase, flush_partials() sums
+// over the warps in a fixed order and writes the tile partials (one __syncthreads per phase).
+struct PhaseRed {
+    double v[KR_SLOTS][KR_THREADS / 32][KR_NV];
+};
+
+template <int NV>
+__device__ __forceinline__ void warp_partial(PhaseRed& R, int slot, const double (&acc)[NV]) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        const double w = warp_sum(acc[k]);
+        if (lane == 0) R.v[slot][warp][k] = w;
+    }
+}
+
 // Per-CTA tile bookkeeping in shared memory.
 struct TileSlots {
     int n;                       // slots used by this CTA
@@ -194,12 +211,16 @@ __device__ void system_sums(const double* partials, const TileSlots& S, unsigned
     __syncthreads();
 }
 
-// Write a tile partial (NV values, already block-summed) from thread 0.
+// Sum the warp partials of the slots in `mask` and write the tile partials (fixed order).
 template <int NV>
-__device__ __forceinline__ void put_partial(double* partials, int tile, const double (&v)[NV]) {
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int k = 0; k < NV; ++k) partials[(size_t)tile * KR_NV + k] = v[k];
+__device__ __forceinline__ void flush_partials(PhaseRed& R, const TileSlots& S, unsigned mask, double* partials) {
+    __syncthreads();
+    const int nwarps = blockDim.x >> 5;
+    const int j = threadIdx.x / NV, k = threadIdx.x % NV;
+    if (j < S.n && ((mask >> j) & 1u)) {
+        double s = 0.0;
+        for (int w = 0; w < nwarps; ++w) s += R.v[j][w][k];
+        partials[(size_t)S.tile[j] * KR_NV + k] = s;
     }
 }
 
@@ -255,6 +276,7 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg(KArgs<T> a) {
     const pict_domain_t& dom = a.dom;
     const int N = dom.num_cells;
     __shared__ TileSlots S;
+    __shared__ PhaseRed R;
     __shared__ double s_sum[KR_SLOTS][KR_NV];
     __shared__ double s_rho[KR_SLOTS], s_beta[KR_SLOTS], s_alpha[KR_SLOTS];
     __shared__ unsigned s_active;  // bit per slot
@@ -287,9 +309,9 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg(KArgs<T> a) {
             acc[0] += (double)ri * (double)ri;
             acc[1] += (double)bi * (double)bi;
         }
-        block_sum<2>(acc);
-        put_partial<2>(part + phase * pstride, S.tile[j], acc);
+        warp_partial<2>(R, j, acc);
     }
+    flush_partials<2>(R, S, 0xffffffffu, part + phase * pstride);
     if (!grid_barrier(a.ctrl)) return;
     system_sums<2>(part + phase * pstride, S, 0xffffffffu, s_sum);
     phase ^= 1;
@@ -345,9 +367,9 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg(KArgs<T> a) {
                     acc[0] += (double)pi[k] * (double)qi[k];
                 }
             }
-            block_sum<1>(acc);
-            put_partial<1>(part + phase * pstride, S.tile[j], acc);
+            warp_partial<1>(R, j, acc);
         }
+        flush_partials<1>(R, S, s_active, part + phase * pstride);
         if (!grid_barrier(a.ctrl)) return;
         if (done_count(a.ctrl) == dom.num_sims) break;
         system_sums<1>(part + phase * pstride, S, s_active, s_sum);
@@ -371,9 +393,9 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg(KArgs<T> a) {
                     acc[0] += (double)ri * (double)ri;
                 }
             }
-            block_sum<1>(acc);
-            put_partial<1>(part + phase * pstride, S.tile[j], acc);
+            warp_partial<1>(R, j, acc);
         }
+        flush_partials<1>(R, S, s_active, part + phase * pstride);
         if (!grid_barrier(a.ctrl)) return;
         system_sums<1>(part + phase * pstride, S, s_active, s_sum);
         phase ^= 1;
@@ -409,9 +431,201 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg(KArgs<T> a) {
             for (int j = 0; j < S.n; ++j) {
                 double acc[1] = {0.0};
                 for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) acc[0] += (double)x[i];
-                block_sum<1>(acc);
-                put_partial<1>(part + phase * pstride, S.tile[j], acc);
+                warp_partial<1>(R, j, acc);
             }
+            flush_partials<1>(R, S, 0xffffffffu, part + phase * pstride);
+            if (!grid_barrier(a.ctrl)) return;
+            system_sums<1>(part + phase * pstride, S, 0xffffffffu, s_sum);
+            phase ^= 1;
+        }
+        for (int j = 0; j < S.n; ++j) {
+            const pict_block_t& B = dom.blocks[S.block[j]];
+            const int n = dom.sim_cells[S.sim[j] + 1] - dom.sim_cells[S.sim[j]];
+            const T mean = a.sub_mean ? (T)(s_sum[j][0] / (double)n) : T(0);
+            T* pb = reinterpret_cast<T*>(B.pressure);
+            for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) {
+                const T v = x[i] - mean;
+                x[i] = v;
+                if (a.write_bp) pb[i - B.offset] = v;
+            }
+        }
+    }
+    if ((int)threadIdx.x < S.n && S.owner[threadIdx.x]) a.info[S.sim[threadIdx.x]] = s_info[threadIdx.x];
+}
+
+// ---------------------------------------------------------------------------------------------
+// CG, single-reduction recurrence (Chronopoulos & Gear 1989): with w = A r, s = A p,
+//   p_i = r_i + b_i p_{i-1},  s_i = w_i + b_i s_{i-1},  x += a_i p_i,  r_{i+1} = r_i - a_i s_i,
+//   w_{i+1} = A r_{i+1},  g_{i+1} = (r_{i+1}, r_{i+1}),  d_{i+1} = (w_{i+1}, r_{i+1}),
+//   b_{i+1} = g_{i+1} / g_i,  a_{i+1} = g_{i+1} / (d_{i+1} - b_{i+1} g_{i+1} / a_i).
+// The same iterates as classic CG in exact arithmetic; one fused sweep (r_{i+1} of the neighbours
+// formed on the fly) and one grid-wide reduction per iteration.  Stopping rule and reported
+// iteration counts as cg.cu:303-397.
+// ---------------------------------------------------------------------------------------------
+template <typename T, int D, bool TRANS>
+__global__ void __launch_bounds__(KR_THREADS) k_cg1(KArgs<T> a) {
+    const pict_domain_t& dom = a.dom;
+    const int N = dom.num_cells;
+    __shared__ TileSlots S;
+    __shared__ PhaseRed R;
+    __shared__ double s_sum[KR_SLOTS][KR_NV];
+    __shared__ double s_g[KR_SLOTS], s_alpha[KR_SLOTS], s_beta[KR_SLOTS];
+    __shared__ unsigned s_active;
+    __shared__ pict_solve_info_t s_info[KR_SLOTS];
+    load_slots(dom, S);
+    const T* __restrict__ coef = a.coef;
+    const T* __restrict__ bv = a.b;
+    T* __restrict__ x = a.x;
+    T* __restrict__ p = a.t;
+    T* rc = a.r;   // r_i
+    T* rn = a.rw;  // r_{i+1}
+    T* wc = a.p0;
+    T* wn = a.p1;
+    T* sc = a.v0;
+    T* sn = a.v1;
+    int phase = 0;
+    double* part = a.partials;
+    const size_t pstride = (size_t)dom.num_tiles * KR_NV;
+
+    // ---- init: r0 = b - A x0 (when x0 != 0: extra sweep), w0 = A r0, g0, d0, |b|^2
+    if (!a.x_zero) {
+        for (int j = 0; j < S.n; ++j) {
+            const pict_block_t& B = dom.blocks[S.block[j]];
+            for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) {
+                int q[3];
+                unflatten(i - B.offset, B.size, q);
+                rc[i] = bv[i] - spmv_row<T, D, TRANS>(dom, coef, N, i, B, q, [&](int jj) { return x[jj]; });
+            }
+        }
+        if (!grid_barrier(a.ctrl)) return;
+    }
+    const T* r0 = a.x_zero ? bv : rc;
+    for (int j = 0; j < S.n; ++j) {
+        const pict_block_t& B = dom.blocks[S.block[j]];
+        double acc[3] = {0.0, 0.0, 0.0};
+        for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) {
+            int q[3];
+            unflatten(i - B.offset, B.size, q);
+            const T ri = r0[i];
+            const T wi = spmv_row<T, D, TRANS>(dom, coef, N, i, B, q, [&](int jj) { return r0[jj]; });
+            if (a.x_zero) { rc[i] = ri; x[i] = T(0); }
+            wc[i] = wi;
+            sc[i] = T(0);
+            p[i] = T(0);
+            const T bi = bv[i];
+            acc[0] += (double)ri * (double)ri;
+            acc[1] += (double)wi * (double)ri;
+            acc[2] += (double)bi * (double)bi;
+        }
+        warp_partial<3>(R, j, acc);
+    }
+    flush_partials<3>(R, S, 0xffffffffu, part + phase * pstride);
+    if (!grid_barrier(a.ctrl)) return;
+    system_sums<3>(part + phase * pstride, S, 0xffffffffu, s_sum);
+    phase ^= 1;
+    if (threadIdx.x == 0) {
+        unsigned act = 0;
+        for (int j = 0; j < S.n; ++j) {
+            pict_solve_info_t inf = fresh_info();
+            s_g[j] = s_sum[j][0];
+            s_alpha[j] = s_sum[j][0] / s_sum[j][1];
+            s_beta[j] = 0.0;
+            if (s_sum[j][2] == 0.0) {
+                inf.converged = 1;
+                inf.used_iterations = 0;
+                if (S.owner[j]) atomicAdd(a.ctrl + CTRL_DONE, 1);
+            } else {
+                act |= 1u << j;
+            }
+            s_info[j] = inf;
+        }
+        s_active = act;
+    }
+    __syncthreads();
+    for (int j = 0; j < S.n; ++j) {
+        if ((s_active >> j) & 1u) continue;
+        for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) x[i] = T(0);
+    }
+
+    for (int it = 0; it < a.maxit; ++it) {
+        for (int j = 0; j < S.n; ++j) {
+            if (!((s_active >> j) & 1u)) continue;
+            const pict_block_t& B = dom.blocks[S.block[j]];
+            const T al = (T)s_alpha[j], bt = (T)s_beta[j];
+            double acc[2] = {0.0, 0.0};
+            const int s0 = S.start[j], s1 = s0 + S.count[j];
+            T rni[KR_CPT], wni[KR_CPT], pi[KR_CPT], si[KR_CPT];
+#pragma unroll
+            for (int k = 0; k < KR_CPT; ++k) {
+                const int i = s0 + threadIdx.x + k * blockDim.x;
+                if (i < s1) {
+                    int q[3];
+                    unflatten(i - B.offset, B.size, q);
+                    pi[k] = rc[i] + bt * p[i];
+                    si[k] = wc[i] + bt * sc[i];
+                    rni[k] = rc[i] - al * si[k];
+                    wni[k] = spmv_row<T, D, TRANS>(dom, coef, N, i, B, q,
+                                                   [&](int jj) { return rc[jj] - al * (wc[jj] + bt * sc[jj]); });
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < KR_CPT; ++k) {
+                const int i = s0 + threadIdx.x + k * blockDim.x;
+                if (i < s1) {
+                    x[i] += al * pi[k];
+                    p[i] = pi[k];
+                    sn[i] = si[k];
+                    rn[i] = rni[k];
+                    wn[i] = wni[k];
+                    acc[0] += (double)rni[k] * (double)rni[k];
+                    acc[1] += (double)wni[k] * (double)rni[k];
+                }
+            }
+            warp_partial<2>(R, j, acc);
+        }
+        flush_partials<2>(R, S, s_active, part + phase * pstride);
+        if (!grid_barrier(a.ctrl)) return;
+        if (done_count(a.ctrl) == dom.num_sims) break;
+        system_sums<2>(part + phase * pstride, S, s_active, s_sum);
+        phase ^= 1;
+        if (threadIdx.x == 0) {
+            unsigned act = s_active;
+            for (int j = 0; j < S.n; ++j) {
+                if (!((act >> j) & 1u)) continue;
+                const double g = s_sum[j][0], d = s_sum[j][1];
+                const int n = dom.sim_cells[S.sim[j] + 1] - dom.sim_cells[S.sim[j]];
+                const double crit = conv_crit(g, a.normalized, n);
+                s_info[j].used_iterations = it;
+                s_info[j].final_residual = crit;
+                bool fin = false;
+                if (!isfinite(crit)) { s_info[j].finite = 0; fin = true; }
+                else if (crit < a.tol) { s_info[j].converged = 1; fin = true; }
+                else {
+                    const double bnew = g / s_g[j];
+                    s_alpha[j] = g / (d - bnew * g / s_alpha[j]);
+                    s_beta[j] = bnew;
+                    s_g[j] = g;
+                }
+                if (fin) {
+                    act &= ~(1u << j);
+                    if (S.owner[j]) atomicAdd(a.ctrl + CTRL_DONE, 1);
+                }
+            }
+            s_active = act;
+        }
+        __syncthreads();
+        T* t0 = rc; rc = rn; rn = t0;
+        T* t1 = wc; wc = wn; wn = t1;
+        T* t2 = sc; sc = sn; sn = t2;
+    }
+    if (a.sub_mean || a.write_bp) {
+        if (a.sub_mean) {
+            for (int j = 0; j < S.n; ++j) {
+                double acc[1] = {0.0};
+                for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) acc[0] += (double)x[i];
+                warp_partial<1>(R, j, acc);
+            }
+            flush_partials<1>(R, S, 0xffffffffu, part + phase * pstride);
             if (!grid_barrier(a.ctrl)) return;
             system_sums<1>(part + phase * pstride, S, 0xffffffffu, s_sum);
             phase ^= 1;
@@ -440,6 +654,7 @@ __global__ void __launch_bounds__(KR_THREADS) k_bicgstab(KArgs<T> a) {
     const int N = dom.num_cells;
     const size_t NS = (size_t)N;
     __shared__ TileSlots S;
+    __shared__ PhaseRed R;
     __shared__ double s_sum[KR_SLOTS][KR_NV];
     __shared__ double s_rho[KR_SLOTS][NR], s_alpha[KR_SLOTS][NR], s_omega[KR_SLOTS][NR], s_beta[KR_SLOTS][NR],
         s_rwr[KR_SLOTS][NR];
@@ -484,9 +699,9 @@ __global__ void __launch_bounds__(KR_THREADS) k_bicgstab(KArgs<T> a) {
                 acc[NR + c] += (double)bi * (double)bi;
             }
         }
-        block_sum<2 * NR>(acc);
-        put_partial<2 * NR>(part + phase * pstride, S.tile[j], acc);
+        warp_partial<2 * NR>(R, j, acc);
     }
+    flush_partials<2 * NR>(R, S, 0xffffffffu, part + phase * pstride);
     if (!grid_barrier(a.ctrl)) return;
     system_sums<2 * NR>(part + phase * pstride, S, 0xffffffffu, s_sum);
     phase ^= 1;
@@ -570,9 +785,9 @@ __global__ void __launch_bounds__(KR_THREADS) k_bicgstab(KArgs<T> a) {
                     acc[c] += (double)rw[c * NS + i] * (double)vi;
                 }
             }
-            block_sum<NR>(acc);
-            put_partial<NR>(part + phase * pstride, S.tile[j], acc);
+            warp_partial<NR>(R, j, acc);
         }
+        flush_partials<NR>(R, S, s_any, part + phase * pstride);
         if (!grid_barrier(a.ctrl)) return;
         if (done_count(a.ctrl) == total) break;
         system_sums<NR>(part + phase * pstride, S, s_any, s_sum);
@@ -601,9 +816,9 @@ __global__ void __launch_bounds__(KR_THREADS) k_bicgstab(KArgs<T> a) {
                     acc[c] += (double)si * (double)si;
                 }
             }
-            block_sum<NR>(acc);
-            put_partial<NR>(part + phase * pstride, S.tile[j], acc);
+            warp_partial<NR>(R, j, acc);
         }
+        flush_partials<NR>(R, S, s_any, part + phase * pstride);
         if (!grid_barrier(a.ctrl)) return;
         system_sums<NR>(part + phase * pstride, S, s_any, s_sum);
         phase ^= 1;
@@ -652,9 +867,9 @@ __global__ void __launch_bounds__(KR_THREADS) k_bicgstab(KArgs<T> a) {
                     acc[2 * c + 1] += (double)ti * (double)ti;
                 }
             }
-            block_sum<2 * NR>(acc);
-            put_partial<2 * NR>(part + phase * pstride, S.tile[j], acc);
+            warp_partial<2 * NR>(R, j, acc);
         }
+        flush_partials<2 * NR>(R, S, s_any, part + phase * pstride);
         if (!grid_barrier(a.ctrl)) return;
         system_sums<2 * NR>(part + phase * pstride, S, s_any, s_sum);
         phase ^= 1;
@@ -684,9 +899,9 @@ __global__ void __launch_bounds__(KR_THREADS) k_bicgstab(KArgs<T> a) {
                     acc[2 * c + 1] += (double)rw[c * NS + i] * (double)ri;
                 }
             }
-            block_sum<2 * NR>(acc);
-            put_partial<2 * NR>(part + phase * pstride, S.tile[j], acc);
+            warp_partial<2 * NR>(R, j, acc);
         }
+        flush_partials<2 * NR>(R, S, s_any, part + phase * pstride);
         if (!grid_barrier(a.ctrl)) return;
         system_sums<2 * NR>(part + phase * pstride, S, s_any, s_sum);
         phase ^= 1;
@@ -759,7 +974,7 @@ static size_t vec_bytes(const pict_domain_t* dom, const pict_solve_params_t* prm
 }
 
 static size_t workspace_total(const pict_domain_t* dom, const pict_solve_params_t* prm) {
-    const int nvec = prm->use_bicg ? 7 : 4;  // bicg: r rw p0 p1 v0 v1 t; cg: r p0 p1 q
+    const int nvec = (prm->use_bicg || prm->variant == 1) ? 7 : 4;  // bicg / cg1: 7 vectors; cg: r p0 p1 q
     return header_bytes(dom) + vec_bytes(dom, prm) * nvec;
 }
 
@@ -805,7 +1020,7 @@ static pict_status_t run_solve(const pict_domain_t* dom, const void* coef, const
     double* partials = reinterpret_cast<double*>(base + align256(256));
     const size_t off = header_bytes(dom);
     const size_t vb = vec_bytes(dom, prm);
-    const int nvec = prm->use_bicg ? 7 : 4;
+    const int nvec = (prm->use_bicg || prm->variant == 1) ? 7 : 4;
     T* vec[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     for (int k = 0; k < nvec; ++k) vec[k] = reinterpret_cast<T*>(base + off + vb * k);
 
@@ -839,6 +1054,9 @@ static pict_status_t run_solve(const pict_domain_t* dom, const void* coef, const
         if (prm->use_bicg) {
             a.r = vec[0]; a.rw = vec[1]; a.p0 = vec[2]; a.p1 = vec[3]; a.v0 = vec[4]; a.v1 = vec[5]; a.t = vec[6];
             kern = nr == 1 ? k_bicgstab<T, D, 1, TRANS> : (nr == 2 ? k_bicgstab<T, D, 2, TRANS> : k_bicgstab<T, D, 3, TRANS>);
+        } else if (prm->variant == 1) {
+            a.r = vec[0]; a.rw = vec[1]; a.p0 = vec[2]; a.p1 = vec[3]; a.v0 = vec[4]; a.v1 = vec[5]; a.t = vec[6];
+            kern = k_cg1<T, D, TRANS>;
         } else {
             a.r = vec[0]; a.p0 = vec[1]; a.p1 = vec[2]; a.t = vec[3];
             a.rw = nullptr; a.v0 = nullptr; a.v1 = nullptr;
@@ -880,6 +1098,8 @@ pict_status_t pict_solve(const pict_domain_t* dom, const void* coef, const void*
     if (prm->max_iterations < 0) return set_error(PICT_ERR_ARG, "solve: max_iterations must be >= 0");
     if (!(prm->convergence == PICT_CONV_NORM2 || prm->convergence == PICT_CONV_NORM2_NORMALIZED))
         return set_error(PICT_ERR_UNSUPPORTED, "solve: only NORM2 and NORM2_NORMALIZED convergence criteria are supported");
+    if (prm->variant != 0 && (prm->use_bicg || prm->variant != 1))
+        return set_error(PICT_ERR_ARG, "solve: variant 1 (single-reduction) applies to CG only");
     if (!prm->use_bicg && prm->nrhs != 1)
         return set_error(PICT_ERR_UNSUPPORTED, "solve: CG takes one right-hand side per call");
     cudaStream_t st = (cudaStream_t)stream;

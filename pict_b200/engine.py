@@ -45,7 +45,7 @@ def default_tolerance(dtype):
 class PISOStepper:
     def __init__(self, domain, time_step=None, corrector_steps: int = 2, advection_tol: Optional[float] = None,
                  pressure_tol: Optional[float] = None, max_iterations: int = 5000, adv_group_size: int = 0,
-                 p_group_size: int = 0, threads: int = 0, normalize_pressure: bool = True):
+                 p_group_size: int = 0, threads: int = 0, normalize_pressure: bool = True, cg_variant: int = 1):
         self.domain = domain
         self.dims = domain.getSpatialDims()
         self.corrector_steps = int(corrector_steps)
@@ -59,7 +59,7 @@ class PISOStepper:
                                           True, False, x_zero=True, group_size=adv_group_size, threads=threads)
         self.p_params = P._solve_params(1, self.max_iterations, self.p_tol, _lib.PICT_CONV_NORM2_NORMALIZED, False,
                                         False, x_zero=True, subtract_mean=normalize_pressure, write_block_pressure=True,
-                                        group_size=p_group_size, threads=threads)
+                                        group_size=p_group_size, threads=threads, variant=cg_variant)
         self._graph = None
         self._graph_steps = 0
         self._prepare()

@@ -37,8 +37,8 @@ def test_batch_equals_individual_steps():
             assert np.array_equal(_np(b1.pressure), _np(b2.pressure))
 
 
-@pytest.mark.parametrize("use_bicg", [False, True])
-def test_solver_independent_of_grid_size(use_bicg):
+@pytest.mark.parametrize("use_bicg,variant", [(False, 0), (False, 1), (True, 0)])
+def test_solver_independent_of_grid_size(use_bicg, variant):
     from pict_b200 import PISOtorch as P
     spec = lid_cavity(96, viscosity=1e-3)
     d = build_product(spec, torch.float32)
@@ -53,7 +53,7 @@ def test_solver_independent_of_grid_size(use_bicg):
     outs = []
     for grid in [0, 1, 2, 3]:
         x = torch.zeros_like(rhs)
-        prm = P._solve_params(nrhs, 2000, 1e-7, 1, use_bicg, False, x_zero=True, group_size=grid)
+        prm = P._solve_params(nrhs, 2000, 1e-7, 1, use_bicg, False, x_zero=True, group_size=grid, variant=variant)
         infos = P.decode_infos(P.solve_stencil(d, coef, rhs, x, prm))
         assert all(i.converged for i in infos)
         outs.append((_np(x), [i.usedIterations for i in infos]))

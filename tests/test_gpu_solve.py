@@ -49,7 +49,8 @@ def test_bicgstab_velocity(name, group_size):
 
 @pytest.mark.parametrize("name", ALL_CASES)
 @pytest.mark.parametrize("group_size", [1, 4])
-def test_cg_pressure(name, group_size):
+@pytest.mark.parametrize("variant", [0, 1])
+def test_cg_pressure(name, group_size, variant):
     from pict_b200 import PISOtorch as P
     spec = case(name)
     od = build_oracle(spec)
@@ -63,7 +64,7 @@ def test_cg_pressure(name, group_size):
     P.CopyVelocityResultFromBlocks(pd)
     P.SetupPressureCorrection(pd, ts)
     x = torch.zeros_like(pd.pressureRHSdiv)
-    params = P._solve_params(1, 2000, 1e-12, 1, False, False, x_zero=True, group_size=group_size)
+    params = P._solve_params(1, 2000, 1e-12, 1, False, False, x_zero=True, group_size=group_size, variant=variant)
     info = P.decode_infos(P.solve_stencil(pd, pd.P.coef, pd.pressureRHSdiv, x, params))[0]
     xref, iref = po.cg(Pm, div, tol=1e-12, maxit=2000)
     assert info.converged and info.isFiniteResidual, info
