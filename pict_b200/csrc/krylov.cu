@@ -48,7 +48,10 @@ constexpr int KR_CPT = 4;        // cells per thread per tile: tile_cells <= KR_
 constexpr int KR_MAX_TILE = KR_CPT * KR_THREADS;
 
 // ctrl words in the workspace header
-enum { CTRL_ERR = 0, CTRL_DONE = 1, CTRL_BAR_COUNT = 2, CTRL_BAR_GEN = 3 };
+// CTRL_DONE counts finished systems (classic CG / BiCGStab: increments and reads are always separated
+// by a grid barrier).  The single-reduction CG has one barrier per iteration, so completions of
+// iteration i go to CTRL_DONE_PAR + (i & 1) and are read only after the barrier of iteration i+1.
+enum { CTRL_ERR = 0, CTRL_DONE = 1, CTRL_BAR_COUNT = 2, CTRL_BAR_GEN = 3, CTRL_DONE_PAR = 4 };
 
 template <typename T>
 struct KArgs {
@@ -533,7 +536,7 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg1(KArgs<T> a) {
             if (s_sum[j][2] == 0.0) {
                 inf.converged = 1;
                 inf.used_iterations = 0;
-                if (S.owner[j]) atomicAdd(a.ctrl + CTRL_DONE, 1);
+                if (S.owner[j]) atomicAdd(a.ctrl + CTRL_DONE_PAR + 1, 1);  // iteration -1
             } else {
                 act |= 1u << j;
             }
@@ -547,6 +550,7 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg1(KArgs<T> a) {
         for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) x[i] = T(0);
     }
 
+    int cum[2] = {0, 0};  // completions per iteration parity, as read by this CTA
     for (int it = 0; it < a.maxit; ++it) {
         for (int j = 0; j < S.n; ++j) {
             if (!((s_active >> j) & 1u)) continue;
@@ -585,7 +589,9 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg1(KArgs<T> a) {
         }
         flush_partials<2>(R, S, s_active, part + phase * pstride);
         if (!grid_barrier(a.ctrl)) return;
-        if (done_count(a.ctrl) == dom.num_sims) break;
+        // completions of iteration it-1 are complete and stable here (see CTRL_DONE_PAR)
+        cum[(it - 1) & 1] = *(volatile const int*)(a.ctrl + CTRL_DONE_PAR + ((it - 1) & 1));
+        if (cum[0] + cum[1] == dom.num_sims) break;
         system_sums<2>(part + phase * pstride, S, s_active, s_sum);
         phase ^= 1;
         if (threadIdx.x == 0) {
@@ -608,7 +614,7 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg1(KArgs<T> a) {
                 }
                 if (fin) {
                     act &= ~(1u << j);
-                    if (S.owner[j]) atomicAdd(a.ctrl + CTRL_DONE, 1);
+                    if (S.owner[j]) atomicAdd(a.ctrl + CTRL_DONE_PAR + (it & 1), 1);
                 }
             }
             s_active = act;

@@ -59,3 +59,20 @@ def test_solver_independent_of_grid_size(use_bicg, variant):
         outs.append((_np(x), [i.usedIterations for i in infos]))
     for x, its in outs[1:]:
         assert np.array_equal(x, outs[0][0]) and its == outs[0][1]
+
+
+def test_many_uneven_systems_single_reduction_cg():
+    """Many systems converging at different iterations in one persistent launch (exit decision must be
+    identical in every CTA; a disagreement would surface as a barrier timeout)."""
+    from pict_b200.batch import BatchDomain
+    from pict_b200.engine import PISOStepper
+    rng = np.random.default_rng(5)
+    sides = rng.integers(12, 80, size=48)
+    doms = [build_product(lid_cavity(int(s), viscosity=float(1e-3 + 1e-2 * rng.random())), torch.float32) for s in sides]
+    b = BatchDomain(doms, time_steps=[0.5 / s for s in sides])
+    for variant in (0, 1):
+        st = PISOStepper(b, time_step=0.01, advection_tol=1e-6, pressure_tol=1e-6, cg_variant=variant)
+        for _ in range(3):
+            st.step()
+        adv, ps = st.check()
+        assert all(i.status == 0 for i in adv) and all(i.status == 0 for p in ps for i in p)
