@@ -227,79 +227,31 @@ __device__ __forceinline__ void flush_partials(PhaseRed& R, const TileSlots& S, 
     }
 }
 
-// Shared-memory staging of one value per cell for a tile and its halo: segment 0 holds local cells
-// [l0-1, l0+cnt+1) (the tile with its x neighbours), segments 2a-1 / 2a the cells one stride below /
-// above along axis a (rows in 2D, rows and planes in 3D).
-template <typename T, int D>
-struct Stage {
-    T v[2 * D - 1][KR_MAX_TILE + 2];
-};
-
-// One sweep over a tile: stage value(global index) for the tile and its halo with independent,
-// coalesced loads, evaluate the stencil row (A value)_i (TRANS: A^T) from shared memory -- neighbours
-// across block faces (periodic / connected) are read from global memory through the neighbour table,
-// fixed faces contribute nothing -- and call cell(i, value_i, Av_i) for each cell.  The per-cell
-// callbacks run after all stencils of the thread, so their global loads overlap.
-template <typename T, int D, bool TRANS, typename V, typename C>
-__device__ __forceinline__ void staged_sweep(const pict_domain_t& dom, const T* __restrict__ coef, const pict_block_t& B,
-                                             int s0, int cnt, Stage<T, D>& st, V value, C cell) {
-    const int N = dom.num_cells;
-    const int off = B.offset;
-    const int nb = B.size[0] * B.size[1] * B.size[2];
-    const int l0 = s0 - off;
+// One stencil row applied to a vector given by `load(j)`; TRANS applies the transposed matrix
+// (the coefficient of row j pointing back to i).
+template <typename T, int D, bool TRANS, typename F>
+__device__ __forceinline__ T spmv_row(const pict_domain_t& dom, const T* __restrict__ coef, int N, int i,
+                                      const pict_block_t& B, const int* p, F load) {
+    T acc = coef[i] * load(i);
     const int stride[3] = {1, B.size[0], B.size[0] * B.size[1]};
-    for (int k = threadIdx.x; k < cnt + 2; k += blockDim.x) {
-        const int l = l0 - 1 + k;
-        if (l >= 0 && l < nb) st.v[0][k] = value(off + l);
-        if (k < cnt) {
 #pragma unroll
-            for (int a = 1; a < D; ++a) {
-                const int lm = l0 + k - stride[a], lp = l0 + k + stride[a];
-                if (lm >= 0) st.v[2 * a - 1][k] = value(off + lm);
-                if (lp < nb) st.v[2 * a][k] = value(off + lp);
-            }
+    for (int f = 0; f < 2 * D; ++f) {
+        const int a = f >> 1;
+        const bool up = f & 1;
+        const bool at = up ? (p[a] == B.size[a] - 1) : (p[a] == 0);
+        int j, back = f ^ 1;
+        if (!at) {
+            j = i + (up ? stride[a] : -stride[a]);
+        } else {
+            j = dom.nbr[(size_t)f * N + i];
+            if (j >= 0 && B.face[f].type == PICT_FACE_CONNECTED) back = B.face[f].conn_axes[0];
+        }
+        if (j >= 0) {
+            const T c = TRANS ? coef[(size_t)(back + 1) * N + j] : coef[(size_t)(f + 1) * N + i];
+            acc += c * load(j);
         }
     }
-    __syncthreads();
-    T own[KR_CPT], av[KR_CPT];
-#pragma unroll
-    for (int u = 0; u < KR_CPT; ++u) {
-        const int k = threadIdx.x + u * blockDim.x;
-        if (k < cnt) {
-            const int l = l0 + k, i = s0 + k;
-            int p[3];
-            unflatten(l, B.size, p);
-            own[u] = st.v[0][k + 1];
-            T acc = coef[i] * own[u];
-#pragma unroll
-            for (int f = 0; f < 2 * D; ++f) {
-                const int a = f >> 1;
-                const bool up = f & 1;
-                const bool at = up ? (p[a] == B.size[a] - 1) : (p[a] == 0);
-                T nv;
-                int j, back = f ^ 1;
-                if (!at) {
-                    nv = (a == 0) ? st.v[0][k + (up ? 2 : 0)] : st.v[up ? 2 * a : 2 * a - 1][k];
-                    j = i + (up ? stride[a] : -stride[a]);
-                } else {
-                    j = dom.nbr[(size_t)f * N + i];
-                    if (j >= 0 && B.face[f].type == PICT_FACE_CONNECTED) back = B.face[f].conn_axes[0];
-                    nv = (j >= 0) ? value(j) : T(0);
-                }
-                T c;
-                if (TRANS) c = (j >= 0) ? coef[(size_t)(back + 1) * N + j] : T(0);
-                else c = coef[(size_t)(f + 1) * N + i];  // zero on fixed faces
-                acc += c * nv;
-            }
-            av[u] = acc;
-        }
-    }
-#pragma unroll
-    for (int u = 0; u < KR_CPT; ++u) {
-        const int k = threadIdx.x + u * blockDim.x;
-        if (k < cnt) cell(s0 + k, own[u], av[u]);
-    }
-    __syncthreads();
+    return acc;
 }
 
 __device__ __forceinline__ double conv_crit(double sq, int normalized, int n) {
@@ -328,8 +280,6 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg(KArgs<T> a) {
     const int N = dom.num_cells;
     __shared__ TileSlots S;
     __shared__ PhaseRed R;
-    extern __shared__ __align__(16) unsigned char kr_dyn_smem[];
-    Stage<T, D>& st = *reinterpret_cast<Stage<T, D>*>(kr_dyn_smem);
     __shared__ double s_sum[KR_SLOTS][KR_NV];
     __shared__ double s_rho[KR_SLOTS], s_beta[KR_SLOTS], s_alpha[KR_SLOTS];
     __shared__ unsigned s_active;  // bit per slot
@@ -351,24 +301,16 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg(KArgs<T> a) {
         const pict_block_t& B = dom.blocks[S.block[j]];
         double acc[2] = {0.0, 0.0};
         const int s0 = S.start[j], s1 = s0 + S.count[j];
-        if (!a.x_zero) {
-            staged_sweep<T, D, TRANS>(dom, coef, B, s0, S.count[j], st, [&](int jj) { return x[jj]; },
-                                      [&](int i, T, T ax) {
-                                          const T bi = bv[i];
-                                          const T ri = bi - ax;
-                                          r[i] = ri;
-                                          pc[i] = T(0);
-                                          acc[0] += (double)ri * (double)ri;
-                                          acc[1] += (double)bi * (double)bi;
-                                      });
-        } else {
-            for (int i = s0 + threadIdx.x; i < s1; i += blockDim.x) {
-                const T bi = bv[i];
-                r[i] = bi;
-                pc[i] = T(0);
-                acc[0] += (double)bi * (double)bi;
-                acc[1] += (double)bi * (double)bi;
-            }
+        for (int i = s0 + threadIdx.x; i < s1; i += blockDim.x) {
+            int p[3];
+            unflatten(i - B.offset, B.size, p);
+            const T bi = bv[i];
+            T ri = bi;
+            if (!a.x_zero) ri -= spmv_row<T, D, TRANS>(dom, coef, N, i, B, p, [&](int jj) { return x[jj]; });
+            r[i] = ri;
+            pc[i] = T(0);
+            acc[0] += (double)ri * (double)ri;
+            acc[1] += (double)bi * (double)bi;
         }
         warp_partial<2>(R, j, acc);
     }
@@ -407,15 +349,27 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg(KArgs<T> a) {
             const pict_block_t& B = dom.blocks[S.block[j]];
             const T bt = (T)s_beta[j];
             double acc[1] = {0.0};
-            const T* rr = r;
-            const T* pp = pc;
-            staged_sweep<T, D, TRANS>(dom, coef, B, S.start[j], S.count[j], st,
-                                      [&](int jj) { return rr[jj] + bt * pp[jj]; },
-                                      [&](int i, T pi, T qi) {
-                                          pn[i] = pi;
-                                          q[i] = qi;
-                                          acc[0] += (double)pi * (double)qi;
-                                      });
+            const int s0 = S.start[j], s1 = s0 + S.count[j];
+            T pi[KR_CPT], qi[KR_CPT];
+#pragma unroll
+            for (int k = 0; k < KR_CPT; ++k) {
+                const int i = s0 + threadIdx.x + k * blockDim.x;
+                if (i < s1) {
+                    int p[3];
+                    unflatten(i - B.offset, B.size, p);
+                    pi[k] = r[i] + bt * pc[i];
+                    qi[k] = spmv_row<T, D, TRANS>(dom, coef, N, i, B, p, [&](int jj) { return r[jj] + bt * pc[jj]; });
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < KR_CPT; ++k) {
+                const int i = s0 + threadIdx.x + k * blockDim.x;
+                if (i < s1) {
+                    pn[i] = pi[k];
+                    q[i] = qi[k];
+                    acc[0] += (double)pi[k] * (double)qi[k];
+                }
+            }
             warp_partial<1>(R, j, acc);
         }
         flush_partials<1>(R, S, s_active, part + phase * pstride);
@@ -517,8 +471,6 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg1(KArgs<T> a) {
     const int N = dom.num_cells;
     __shared__ TileSlots S;
     __shared__ PhaseRed R;
-    extern __shared__ __align__(16) unsigned char kr_dyn_smem[];
-    Stage<T, D>& st = *reinterpret_cast<Stage<T, D>*>(kr_dyn_smem);
     __shared__ double s_sum[KR_SLOTS][KR_NV];
     __shared__ double s_g[KR_SLOTS], s_alpha[KR_SLOTS], s_beta[KR_SLOTS];
     __shared__ unsigned s_active;
@@ -542,8 +494,11 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg1(KArgs<T> a) {
     if (!a.x_zero) {
         for (int j = 0; j < S.n; ++j) {
             const pict_block_t& B = dom.blocks[S.block[j]];
-            staged_sweep<T, D, TRANS>(dom, coef, B, S.start[j], S.count[j], st, [&](int jj) { return x[jj]; },
-                                      [&](int i, T, T ax) { rc[i] = bv[i] - ax; });
+            for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) {
+                int q[3];
+                unflatten(i - B.offset, B.size, q);
+                rc[i] = bv[i] - spmv_row<T, D, TRANS>(dom, coef, N, i, B, q, [&](int jj) { return x[jj]; });
+            }
         }
         if (!grid_barrier(a.ctrl)) return;
     }
@@ -551,17 +506,20 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg1(KArgs<T> a) {
     for (int j = 0; j < S.n; ++j) {
         const pict_block_t& B = dom.blocks[S.block[j]];
         double acc[3] = {0.0, 0.0, 0.0};
-        staged_sweep<T, D, TRANS>(dom, coef, B, S.start[j], S.count[j], st, [&](int jj) { return r0[jj]; },
-                                  [&](int i, T ri, T wi) {
-                                      if (a.x_zero) { rc[i] = ri; x[i] = T(0); }
-                                      wc[i] = wi;
-                                      sc[i] = T(0);
-                                      p[i] = T(0);
-                                      const T bi = bv[i];
-                                      acc[0] += (double)ri * (double)ri;
-                                      acc[1] += (double)wi * (double)ri;
-                                      acc[2] += (double)bi * (double)bi;
-                                  });
+        for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) {
+            int q[3];
+            unflatten(i - B.offset, B.size, q);
+            const T ri = r0[i];
+            const T wi = spmv_row<T, D, TRANS>(dom, coef, N, i, B, q, [&](int jj) { return r0[jj]; });
+            if (a.x_zero) { rc[i] = ri; x[i] = T(0); }
+            wc[i] = wi;
+            sc[i] = T(0);
+            p[i] = T(0);
+            const T bi = bv[i];
+            acc[0] += (double)ri * (double)ri;
+            acc[1] += (double)wi * (double)ri;
+            acc[2] += (double)bi * (double)bi;
+        }
         warp_partial<3>(R, j, acc);
     }
     flush_partials<3>(R, S, 0xffffffffu, part + phase * pstride);
@@ -599,22 +557,34 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg1(KArgs<T> a) {
             const pict_block_t& B = dom.blocks[S.block[j]];
             const T al = (T)s_alpha[j], bt = (T)s_beta[j];
             double acc[2] = {0.0, 0.0};
-            const T* rr = rc;
-            const T* ww = wc;
-            const T* ss = sc;
-            staged_sweep<T, D, TRANS>(dom, coef, B, S.start[j], S.count[j], st,
-                                      [&](int jj) { return rr[jj] - al * (ww[jj] + bt * ss[jj]); },
-                                      [&](int i, T rni, T wni) {
-                                          const T pi = rr[i] + bt * p[i];
-                                          const T si = ww[i] + bt * ss[i];
-                                          x[i] += al * pi;
-                                          p[i] = pi;
-                                          sn[i] = si;
-                                          rn[i] = rni;
-                                          wn[i] = wni;
-                                          acc[0] += (double)rni * (double)rni;
-                                          acc[1] += (double)wni * (double)rni;
-                                      });
+            const int s0 = S.start[j], s1 = s0 + S.count[j];
+            T rni[KR_CPT], wni[KR_CPT], pi[KR_CPT], si[KR_CPT];
+#pragma unroll
+            for (int k = 0; k < KR_CPT; ++k) {
+                const int i = s0 + threadIdx.x + k * blockDim.x;
+                if (i < s1) {
+                    int q[3];
+                    unflatten(i - B.offset, B.size, q);
+                    pi[k] = rc[i] + bt * p[i];
+                    si[k] = wc[i] + bt * sc[i];
+                    rni[k] = rc[i] - al * si[k];
+                    wni[k] = spmv_row<T, D, TRANS>(dom, coef, N, i, B, q,
+                                                   [&](int jj) { return rc[jj] - al * (wc[jj] + bt * sc[jj]); });
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < KR_CPT; ++k) {
+                const int i = s0 + threadIdx.x + k * blockDim.x;
+                if (i < s1) {
+                    x[i] += al * pi[k];
+                    p[i] = pi[k];
+                    sn[i] = si[k];
+                    rn[i] = rni[k];
+                    wn[i] = wni[k];
+                    acc[0] += (double)rni[k] * (double)rni[k];
+                    acc[1] += (double)wni[k] * (double)rni[k];
+                }
+            }
             warp_partial<2>(R, j, acc);
         }
         flush_partials<2>(R, S, s_active, part + phase * pstride);
@@ -691,8 +661,6 @@ __global__ void __launch_bounds__(KR_THREADS) k_bicgstab(KArgs<T> a) {
     const size_t NS = (size_t)N;
     __shared__ TileSlots S;
     __shared__ PhaseRed R;
-    extern __shared__ __align__(16) unsigned char kr_dyn_smem[];
-    Stage<T, D>& st = *reinterpret_cast<Stage<T, D>*>(kr_dyn_smem);
     __shared__ double s_sum[KR_SLOTS][KR_NV];
     __shared__ double s_rho[KR_SLOTS][NR], s_alpha[KR_SLOTS][NR], s_omega[KR_SLOTS][NR], s_beta[KR_SLOTS][NR],
         s_rwr[KR_SLOTS][NR];
@@ -720,25 +688,22 @@ __global__ void __launch_bounds__(KR_THREADS) k_bicgstab(KArgs<T> a) {
         double acc[2 * NR];
 #pragma unroll
         for (int k = 0; k < 2 * NR; ++k) acc[k] = 0.0;
+        for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) {
+            int p[3];
+            unflatten(i - B.offset, B.size, p);
 #pragma unroll
-        for (int c = 0; c < NR; ++c) {
-            const T* xc = x + c * NS;
-            const T* bc = a.b + c * NS;
-            auto init_cell = [&](int i, T ax) {
-                const T bi = bc[i];
-                const T ri = bi - ax;
+            for (int c = 0; c < NR; ++c) {
+                const T* xc = x + c * NS;
+                const T bi = a.b[c * NS + i];
+                T ri = bi;
+                if (!a.x_zero) ri -= spmv_row<T, D, TRANS>(dom, coef, N, i, B, p, [&](int jj) { return xc[jj]; });
                 r[c * NS + i] = ri;
                 a.rw[c * NS + i] = ri;
                 pc[c * NS + i] = T(0);
                 vc[c * NS + i] = T(0);
                 acc[c] += (double)ri * (double)ri;
                 acc[NR + c] += (double)bi * (double)bi;
-            };
-            if (!a.x_zero)
-                staged_sweep<T, D, TRANS>(dom, coef, B, S.start[j], S.count[j], st, [&](int jj) { return xc[jj]; },
-                                          [&](int i, T, T ax) { init_cell(i, ax); });
-            else
-                for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) init_cell(i, T(0));
+            }
         }
         warp_partial<2 * NR>(R, j, acc);
     }
@@ -808,20 +773,23 @@ __global__ void __launch_bounds__(KR_THREADS) k_bicgstab(KArgs<T> a) {
             double acc[NR];
 #pragma unroll
             for (int c = 0; c < NR; ++c) acc[c] = 0.0;
+            for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) {
+                int p[3];
+                unflatten(i - B.offset, B.size, p);
 #pragma unroll
-            for (int c = 0; c < NR; ++c) {
-                if (!((act >> c) & 1u)) continue;
-                const T bt = (T)s_beta[j][c], om = (T)s_omega[j][c];
-                const T* rc = r + c * NS;
-                const T* pcc = pc + c * NS;
-                const T* vcc = vc + c * NS;
-                staged_sweep<T, D, TRANS>(dom, coef, B, S.start[j], S.count[j], st,
-                                          [&](int jj) { return rc[jj] + bt * (pcc[jj] - om * vcc[jj]); },
-                                          [&](int i, T pi, T vi) {
-                                              pn[c * NS + i] = pi;
-                                              vn[c * NS + i] = vi;
-                                              acc[c] += (double)rw[c * NS + i] * (double)vi;
-                                          });
+                for (int c = 0; c < NR; ++c) {
+                    if (!((act >> c) & 1u)) continue;
+                    const T bt = (T)s_beta[j][c], om = (T)s_omega[j][c];
+                    const T* rc = r + c * NS;
+                    const T* pcc = pc + c * NS;
+                    const T* vcc = vc + c * NS;
+                    const T pi = rc[i] + bt * (pcc[i] - om * vcc[i]);
+                    const T vi = spmv_row<T, D, TRANS>(dom, coef, N, i, B, p,
+                                                       [&](int jj) { return rc[jj] + bt * (pcc[jj] - om * vcc[jj]); });
+                    pn[c * NS + i] = pi;
+                    vn[c * NS + i] = vi;
+                    acc[c] += (double)rw[c * NS + i] * (double)vi;
+                }
             }
             warp_partial<NR>(R, j, acc);
         }
@@ -892,16 +860,18 @@ __global__ void __launch_bounds__(KR_THREADS) k_bicgstab(KArgs<T> a) {
             double acc[2 * NR];
 #pragma unroll
             for (int k = 0; k < 2 * NR; ++k) acc[k] = 0.0;
+            for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) {
+                int p[3];
+                unflatten(i - B.offset, B.size, p);
 #pragma unroll
-            for (int c = 0; c < NR; ++c) {
-                if (!((act >> c) & 1u)) continue;
-                const T* sc = r + c * NS;
-                staged_sweep<T, D, TRANS>(dom, coef, B, S.start[j], S.count[j], st, [&](int jj) { return sc[jj]; },
-                                          [&](int i, T si, T ti) {
-                                              tv[c * NS + i] = ti;
-                                              acc[2 * c] += (double)ti * (double)si;
-                                              acc[2 * c + 1] += (double)ti * (double)ti;
-                                          });
+                for (int c = 0; c < NR; ++c) {
+                    if (!((act >> c) & 1u)) continue;
+                    const T* sc = r + c * NS;
+                    const T ti = spmv_row<T, D, TRANS>(dom, coef, N, i, B, p, [&](int jj) { return sc[jj]; });
+                    tv[c * NS + i] = ti;
+                    acc[2 * c] += (double)ti * (double)sc[i];
+                    acc[2 * c + 1] += (double)ti * (double)ti;
+                }
             }
             warp_partial<2 * NR>(R, j, acc);
         }
@@ -1015,21 +985,19 @@ static size_t workspace_total(const pict_domain_t* dom, const pict_solve_params_
 }
 
 template <typename KernelT>
-static int max_coresident(KernelT kernel, size_t smem) {
-    // the dynamic shared memory (tile staging) exceeds the default 48 KB for FP64 / 3D
-    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+static int max_coresident(KernelT kernel) {
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, KR_THREADS, smem) != cudaSuccess || per_sm < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, KR_THREADS, 0) != cudaSuccess || per_sm < 1)
         per_sm = 1;
     return per_sm * device_sm_count();
 }
 
 template <typename T>
-static pict_status_t launch_kernel(void (*kernel)(KArgs<T>), int grid, size_t smem, KArgs<T>& args, cudaStream_t st) {
+static pict_status_t launch_kernel(void (*kernel)(KArgs<T>), int grid, KArgs<T>& args, cudaStream_t st) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(KR_THREADS);
-    cfg.dynamicSmemBytes = smem;
+    cfg.dynamicSmemBytes = 0;
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;
@@ -1101,14 +1069,13 @@ static pict_status_t run_solve(const pict_domain_t* dom, const void* coef, const
             kern = k_cg<T, D, TRANS>;
         }
         // grid: every CTA owns at most KR_SLOTS tiles; all CTAs must be co-resident
-        const size_t smem = sizeof(Stage<T, D>);
-        const int cores = max_coresident(kern, smem);
+        const int cores = max_coresident(kern);
         int grid = dom->num_tiles < cores ? dom->num_tiles : cores;
         if (prm->group_size > 0 && grid > prm->group_size) grid = prm->group_size;
         const int min_grid = (dom->num_tiles + KR_SLOTS - 1) / KR_SLOTS;
         if (grid < min_grid) grid = min_grid;
         if (grid > cores) return set_error(PICT_ERR_ARG, "solve: too many tiles for one persistent launch (raise tile_cells)");
-        s = launch_kernel<T>(kern, grid, smem, a, st);
+        s = launch_kernel<T>(kern, grid, a, st);
         if (s) return s;
         k_finish_info<<<1, 128, 0, st>>>(info, ninfo, ctrl);
         s = check_launch("finish_info");
