@@ -6,9 +6,7 @@
  * (module ``pict_b200.PISOtorch``) binds these entry points with ctypes and
  * mirrors the reference's pybind11 ``PISOtorch`` operator surface on top of
  * them.  Each entry point below cites the reference interface it replaces
- * (paths relative to the PICT repository; "PISOtorch.cpp" is
- * extensions/PISOtorch.cpp, "kernel.cu" is
- * extensions/PISO_multiblock_cuda_kernel.cu).
+ * (file:line, paths relative to the PICT repository).
  *
  * Conventions
  *  - Every compute entry point is stream-ordered on the given stream, performs
@@ -51,18 +49,18 @@ typedef int32_t pict_status_t;
 
 #define PICT_MAX_BLOCK_FACES 6
 
-/* One block face (BoundaryGPU, domain_structs_gpu.h:253-263). */
+/* One block face (BoundaryGPU, extensions/domain_structs_gpu.h:253-263). */
 typedef struct pict_face {
     int32_t type;          /* PICT_FACE_* */
     int32_t conn_block;    /* connected: index of the other block */
-    int32_t conn_axes[3];  /* connected: ConnectedBoundary::axes (domain_structs.h:329-338) */
+    int32_t conn_axes[3];  /* connected: ConnectedBoundary::axes (extensions/domain_structs.h:329-338) */
     int32_t vel_static;    /* fixed: 1 if velocity is a static [D] vector */
     const void* velocity;  /* fixed: boundary velocity [D] or [D][face cells] (device) */
     const void* transform; /* fixed: boundary transform [face cells][2D^2+1] or NULL */
     void* velocity_grad;   /* fixed: gradient of velocity (adjoint), same layout, or NULL */
 } pict_face_t;
 
-/* One structured block (BlockGPU, domain_structs_gpu.h:266-305). */
+/* One structured block (BlockGPU, extensions/domain_structs_gpu.h:266-305). */
 typedef struct pict_block {
     int32_t size[3];          /* x, y, z cells (1 for unused axes) */
     int32_t offset;           /* first global cell index of this block */
@@ -83,7 +81,7 @@ typedef struct pict_block {
 } pict_block_t;
 
 /* A (possibly batched) domain.  All pointers are device pointers unless noted.
- * Mirrors DomainGPU (domain_structs_gpu.h:307-370) with stencil storage. */
+ * Mirrors DomainGPU (extensions/domain_structs_gpu.h:307-370) with stencil storage. */
 typedef struct pict_domain {
     int32_t dims;
     int32_t num_blocks;
@@ -112,7 +110,7 @@ typedef struct pict_domain {
     void* pressure_result;    /* [N] */
 } pict_domain_t;
 
-/* Per right-hand-side solver report (LinearSolverResultInfo, bicgstab_solver.h:20-25). */
+/* Per right-hand-side solver report (LinearSolverResultInfo, extensions/bicgstab_solver.h:20-25). */
 typedef struct pict_solve_info {
     double final_residual;
     int32_t used_iterations;
@@ -127,7 +125,7 @@ typedef struct pict_solve_info {
 #define PICT_CONV_ABS_MEAN 3
 #define PICT_CONV_ABS_MAX 4
 
-/* Parameters of a linear solve (PISOtorch.SolveLinear arguments, PISOtorch.cpp:559-563). */
+/* Parameters of a linear solve (PISOtorch.SolveLinear arguments, extensions/PISOtorch.cpp:559-563). */
 typedef struct pict_solve_params {
     int32_t max_iterations;
     int32_t use_bicg;          /* 1: BiCGStab, 0: CG */
@@ -137,9 +135,9 @@ typedef struct pict_solve_params {
     int32_t convergence;       /* PICT_CONV_*; only NORM2 and NORM2_NORMALIZED are supported */
     int32_t group_size;        /* upper bound of CTAs of the persistent launch (0: automatic) */
     int32_t threads;           /* threads per CTA (0: automatic) */
-    int32_t subtract_mean;     /* 1: x -= mean(x) per system after the solve (sim.py:1243-1244) */
+    int32_t subtract_mean;     /* 1: x -= mean(x) per system after the solve (PISOtorch_simulation.py:1243-1244) */
     int32_t write_block_pressure; /* 1: also copy x into the blocks' pressure (CopyPressureResultToBlocks) */
-    int32_t variant;           /* CG only: 0 classic order (cg.cu:236-427, two reductions per iteration),
+    int32_t variant;           /* CG only: 0 classic order (extensions/cg_solver_kernel.cu:236-427, two reductions per iteration),
                                   1 single-reduction recurrence (Chronopoulos-Gear): same iterates in exact
                                   arithmetic, one grid-wide reduction per iteration */
     double tolerance;
@@ -153,8 +151,8 @@ int32_t pict_sizeof_domain(void);  /* sizeof(pict_domain_t) */
 
 /* ---------------- host-side topology (no GPU needed) ----------------
  * Replaces the per-thread neighbour resolution of the reference
- * (resolveNeighborCell / computeConnectedPos, kernel.cu:326-345, 432-477) and
- * the connection checks of Domain::PrepareSolve (domain_structs.cpp:2554-2676)
+ * (resolveNeighborCell / computeConnectedPos, extensions/PISO_multiblock_cuda_kernel.cu:326-345, 432-477) and
+ * the connection checks of Domain::PrepareSolve (extensions/domain_structs.cpp:2554-2676)
  * with a precomputed table.  host_blocks is a HOST array.
  * nbr_out: [2*dims][num_cells], cell_block_out: [num_cells] (host buffers). */
 pict_status_t pict_build_topology(const pict_block_t* host_blocks, int32_t num_blocks, int32_t dims,
@@ -169,44 +167,44 @@ pict_status_t pict_build_tiles(const pict_block_t* host_blocks, int32_t num_bloc
                                int32_t* num_tiles_out);
 
 /* ---------------- assembly (forward) ---------------- */
-/* SetupAdvectionMatrix (PISOtorch.cpp:531-533 -> kernel.cu:4510 PISO_build_matrix):
+/* SetupAdvectionMatrix (extensions/PISOtorch.cpp:531-533 -> extensions/PISO_multiblock_cuda_kernel.cu:4510 PISO_build_matrix):
  * writes C and A from the blocks' velocity.  non_ortho_flags must be 0. */
 pict_status_t pict_setup_advection_matrix(const pict_domain_t* dom, double dt, int32_t non_ortho_flags,
                                           void* stream);
-/* SetupAdvectionVelocity (PISOtorch.cpp:537-539 -> kernel.cu:4677 kPISO_build_advection_RHS). */
+/* SetupAdvectionVelocity (extensions/PISOtorch.cpp:537-539 -> extensions/PISO_multiblock_cuda_kernel.cu:4677 kPISO_build_advection_RHS). */
 pict_status_t pict_setup_advection_velocity(const pict_domain_t* dom, double dt, int32_t non_ortho_flags,
                                             int32_t apply_pressure_gradient, void* stream);
 /* Fused SetupAdvectionMatrix + SetupAdvectionVelocity in one pass over the cells. */
 pict_status_t pict_setup_advection(const pict_domain_t* dom, double dt, void* stream);
-/* SetupPressureMatrix (PISOtorch.cpp:544-546 -> kernel.cu:4797 PISO_build_pressure_matrix). */
+/* SetupPressureMatrix (extensions/PISOtorch.cpp:544-546 -> extensions/PISO_multiblock_cuda_kernel.cu:4797 PISO_build_pressure_matrix). */
 pict_status_t pict_setup_pressure_matrix(const pict_domain_t* dom, int32_t non_ortho_flags, void* stream);
-/* SetupPressureRHS (PISOtorch.cpp:547-549 -> kernel.cu:5121 PISO_build_pressure_rhs
- * + kernel.cu:5374 k_computePressureRHSdivergenceFromFlux). */
+/* SetupPressureRHS (extensions/PISOtorch.cpp:547-549 -> extensions/PISO_multiblock_cuda_kernel.cu:5121 PISO_build_pressure_rhs
+ * + extensions/PISO_multiblock_cuda_kernel.cu:5374 k_computePressureRHSdivergenceFromFlux). */
 pict_status_t pict_setup_pressure_rhs(const pict_domain_t* dom, double dt, int32_t non_ortho_flags,
                                       int32_t time_step_norm, void* stream);
-/* SetupPressureRHSdiv (PISOtorch.cpp:550-552 -> kernel.cu:5374). */
+/* SetupPressureRHSdiv (extensions/PISOtorch.cpp:550-552 -> extensions/PISO_multiblock_cuda_kernel.cu:5374). */
 pict_status_t pict_setup_pressure_rhs_div(const pict_domain_t* dom, double dt, int32_t non_ortho_flags,
                                           int32_t time_step_norm, void* stream);
-/* SetupPressureCorrection (PISOtorch.cpp:541-543): matrix + RHS + div, matrix and RHS fused. */
+/* SetupPressureCorrection (extensions/PISOtorch.cpp:541-543): matrix + RHS + div, matrix and RHS fused. */
 pict_status_t pict_setup_pressure_correction(const pict_domain_t* dom, double dt, int32_t non_ortho_flags,
                                              int32_t time_step_norm, void* stream);
-/* CorrectVelocity (PISOtorch.cpp:553-555 -> kernel.cu:6163, version 1 "FD").
+/* CorrectVelocity (extensions/PISOtorch.cpp:553-555 -> extensions/PISO_multiblock_cuda_kernel.cu:6163, version 1 "FD").
  * write_block_velocity=1 additionally stores the result in the blocks' velocity
  * (CopyVelocityResultToBlocks fused). */
 pict_status_t pict_correct_velocity(const pict_domain_t* dom, double dt, int32_t version,
                                     int32_t time_step_norm, int32_t write_block_velocity, void* stream);
-/* Copy{Velocity,Pressure}Result{To,From}Blocks (PISOtorch.cpp:561-566 -> kernel.cu:6543-6733). */
+/* Copy{Velocity,Pressure}Result{To,From}Blocks (extensions/PISOtorch.cpp:561-566 -> extensions/PISO_multiblock_cuda_kernel.cu:6543-6733). */
 pict_status_t pict_copy_velocity_result_to_blocks(const pict_domain_t* dom, void* stream);
 pict_status_t pict_copy_velocity_result_from_blocks(const pict_domain_t* dom, void* stream);
 pict_status_t pict_copy_pressure_result_to_blocks(const pict_domain_t* dom, void* stream);
 pict_status_t pict_copy_pressure_result_from_blocks(const pict_domain_t* dom, void* stream);
-/* ComputeVelocityDivergence (PISOtorch.cpp:556 -> kernel.cu:6333): div of the blocks' velocity, out [N]. */
+/* ComputeVelocityDivergence (extensions/PISOtorch.cpp:556 -> extensions/PISO_multiblock_cuda_kernel.cu:6333): div of the blocks' velocity, out [N]. */
 pict_status_t pict_velocity_divergence(const pict_domain_t* dom, void* out, void* stream);
 
 /* ---------------- linear solves ---------------- */
 /* Bytes of scratch memory a solve needs (vectors, reduction partials, barriers). */
 int64_t pict_solve_workspace_bytes(const pict_domain_t* dom, const pict_solve_params_t* params);
-/* SolveLinear (PISOtorch.cpp:559-563 -> kernel.cu:7070 -> cgSolveGPU cg.cu:114 / bicgstabSolveGPU bicg.cu:47)
+/* SolveLinear (extensions/PISOtorch.cpp:559-563 -> extensions/PISO_multiblock_cuda_kernel.cu:7070 -> cgSolveGPU extensions/cg_solver_kernel.cu:114 / bicgstabSolveGPU extensions/bicgstab_solver_kernel.cu:47)
  * on a stencil matrix coef [K][N] of the domain's topology.  rhs, x: [nrhs][N].
  * info_out: device array [num_sims][nrhs] of pict_solve_info_t.  workspace: device memory of
  * pict_solve_workspace_bytes() bytes. */
@@ -214,15 +212,16 @@ pict_status_t pict_solve(const pict_domain_t* dom, const void* coef, const void*
                          const pict_solve_params_t* params, void* info_out, void* workspace,
                          int64_t workspace_bytes, void* stream);
 
+
 /* ---------------- matrix export / utilities ---------------- */
 /* CSR materialisation of a stencil matrix in the reference's row layout (rows sorted by
- * column, kernel.cu:3846-3860).  row_out [N+1] must be computed first by pict_csr_row_ptr. */
+ * column, extensions/PISO_multiblock_cuda_kernel.cu:3846-3860).  row_out [N+1] must be computed first by pict_csr_row_ptr. */
 pict_status_t pict_csr_row_ptr(const pict_domain_t* dom, int32_t* row_out, void* stream);
 pict_status_t pict_stencil_to_csr(const pict_domain_t* dom, const void* coef, const int32_t* row,
                                   void* value_out, int32_t* index_out, void* stream);
 pict_status_t pict_csr_to_stencil(const pict_domain_t* dom, const void* value, const int32_t* row,
                                   const int32_t* index, void* coef_out, void* stream);
-/* CoordsToTransforms / CoordsToFaceTransforms (grid_gen.cu:341-375, 468-514). coords [D][(z+1)][y+1][x+1]. */
+/* CoordsToTransforms / CoordsToFaceTransforms (extensions/grid_gen.cu:341-375, 468-514). coords [D][(z+1)][y+1][x+1]. */
 pict_status_t pict_coords_to_transforms(const void* coords, int32_t dims, const int32_t* size_xyz,
                                         int32_t dtype, void* out, void* stream);
 pict_status_t pict_coords_to_face_transforms(const void* coords, int32_t dims, const int32_t* size_xyz,

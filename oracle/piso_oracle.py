@@ -20,13 +20,13 @@ PICT repository):
 Layout conventions (identical to the reference):
 
 * faces / boundaries are indexed ``[-x, +x, -y, +y, -z, +z]`` = 0..2D-1,
-  axis = face >> 1, upper side = face & 1 (kernel.cu:196-225);
+  axis = face >> 1, upper side = face & 1 (extensions/PISO_multiblock_cuda_kernel.cu:196-225);
 * cells of a block are flattened x-fastest; global vectors concatenate the
   blocks (``globalOffset``) and vector fields are component-major
-  ``[D][N]`` (kernel.cu:166-172);
+  ``[D][N]`` (extensions/PISO_multiblock_cuda_kernel.cu:166-172);
 * stencil coefficients are stored as ``coef[K][N]`` with K = 2D+1 in the order
   ``[diag, -x, +x, -y, +y, -z, +z]`` (the reference's ``rowValues`` order,
-  kernel.cu:3693-3694, before its CSR sort).
+  extensions/PISO_multiblock_cuda_kernel.cu:3693-3694, before its CSR sort).
 
 Pinning: golden fixtures produced by the reference's own CUDA build
 (``tests/golden/``, generated by ``tests/golden/make_ref_fixtures.py``) are
@@ -46,7 +46,7 @@ AXIS_NAMES = ["x", "y", "z"]
 
 
 def face_index(face) -> int:
-    """Face string or index -> index (domain_structs.cpp:134-155)."""
+    """Face string or index -> index (extensions/domain_structs.cpp:134-155)."""
     if isinstance(face, str):
         return FACE_NAMES.index(face)
     return int(face)
@@ -70,7 +70,7 @@ def _det_inv(M):
 
 
 def coords_to_transforms(coords: np.ndarray) -> np.ndarray:
-    """Cell transforms from vertex coordinates, grid_gen.cu:284-339.
+    """Cell transforms from vertex coordinates, extensions/grid_gen.cu:284-339.
 
     coords: [1, D, (z+1), y+1, x+1] -> transforms [1, (z), y, x, 2D^2+1] with
     per cell M (row-major, M[i][k] = d x_i / d xi_k from the difference of the
@@ -112,11 +112,11 @@ def coords_to_transforms(coords: np.ndarray) -> np.ndarray:
 
 
 def coords_to_face_transforms(coords: np.ndarray) -> np.ndarray:
-    """Face transforms (staggered), grid_gen.cu:383-466.
+    """Face transforms (staggered), extensions/grid_gen.cu:383-466.
 
     Returns [1, D, (z+1), y+1, x+1, 2D^2+1]; channel ``dim`` holds the transform
     of the lower face of cell ``pos`` along ``dim``.  Entries whose tangential
-    index is the last vertex index are left zero (grid_gen.cu:392-397).
+    index is the last vertex index are left zero (extensions/grid_gen.cu:392-397).
     """
     c = np.asarray(coords, dtype=np.float64)
     D = c.shape[1]
@@ -171,7 +171,7 @@ def coords_to_face_transforms(coords: np.ndarray) -> np.ndarray:
 
 
 def boundary_transform_from_face_transforms(face_T: np.ndarray, face: int) -> np.ndarray:
-    """Slice of the face transforms on a block face, domain_structs.cpp:1809-1835.
+    """Slice of the face transforms on a block face, extensions/domain_structs.cpp:1809-1835.
 
     face_T: [1, D, (z+1), y+1, x+1, T] -> [1, (z'), y', x', T] with the face axis of size 1.
     """
@@ -198,7 +198,7 @@ class OBoundary:
     velocity: Optional[np.ndarray] = None  # fixed: [1,D] static or [1,D,face zyx]
     transform: Optional[np.ndarray] = None  # fixed: [1, face zyx, T]
     block: int = -1  # connected: other block index
-    axes: Optional[List[int]] = None  # connected: axes as in ConnectedBoundary (domain_structs.h:329-338)
+    axes: Optional[List[int]] = None  # connected: axes as in ConnectedBoundary (extensions/domain_structs.h:329-338)
 
 
 @dataclass
@@ -218,7 +218,7 @@ class OBlock:
 
 
 class ODomain:
-    """Host model of a PICT domain (domain_structs.h:563-787), FP64."""
+    """Host model of a PICT domain (extensions/domain_structs.h:563-787), FP64."""
 
     def __init__(self, dims: int, viscosity: float):
         self.dims = dims
@@ -259,7 +259,7 @@ class ODomain:
         b.boundaries[face] = OBoundary("fixed", velocity=vel, transform=tr)
 
     def _close_connected(self, bi, face):
-        """Block::CloseConnectedBoudary with useFixed=True, domain_structs.cpp:1773-1807."""
+        """Block::CloseConnectedBoudary with useFixed=True, extensions/domain_structs.cpp:1773-1807."""
         bnd = self.blocks[bi].boundaries[face]
         if bnd.kind == "connected":
             self._fixed(bnd.block, bnd.axes[0])
@@ -267,7 +267,7 @@ class ODomain:
             self._fixed(bi, face ^ 1)
 
     def close_boundary(self, bi, face, velocity=None):
-        """Block::CloseBoundary(face, velocity), domain_structs.cpp:1979-1986."""
+        """Block::CloseBoundary(face, velocity), extensions/domain_structs.cpp:1979-1986."""
         face = face_index(face)
         self._close_connected(bi, face)
         self._fixed(bi, face, velocity)
@@ -277,7 +277,7 @@ class ODomain:
             self.close_boundary(bi, f)
 
     def make_periodic(self, bi, axis):
-        """Block::MakePeriodic, domain_structs.cpp:1936-1955."""
+        """Block::MakePeriodic, extensions/domain_structs.cpp:1936-1955."""
         axis = axis_index(axis)
         lo, hi = axis << 1, (axis << 1) | 1
         b = self.blocks[bi]
@@ -290,7 +290,7 @@ class ODomain:
             b.boundaries[hi] = OBoundary("periodic")
 
     def connect(self, b1, face1, b2, face2, axis1=-1, axis2=-1):
-        """Block::ConnectBlock -> ConnectBlocks, domain_structs.cpp:1064-1097, 1924-1930."""
+        """Block::ConnectBlock -> ConnectBlocks, extensions/domain_structs.cpp:1064-1097, 1924-1930."""
         face1, face2 = face_index(face1), face_index(face2)
         axis1 = face_index(axis1) if axis1 != -1 else -1
         axis2 = face_index(axis2) if axis2 != -1 else -1
@@ -320,8 +320,8 @@ class ODomain:
 
     # ---- topology ----
     def prepare(self):
-        """Global offsets and per-cell neighbour tables (Domain::PrepareSolve, domain_structs.cpp:2554-2676;
-        neighbour resolution kernel.cu:326-345, 432-477)."""
+        """Global offsets and per-cell neighbour tables (Domain::PrepareSolve, extensions/domain_structs.cpp:2554-2676;
+        neighbour resolution extensions/PISO_multiblock_cuda_kernel.cu:326-345, 432-477)."""
         D = self.dims
         self.offsets = []
         n = 0
@@ -376,7 +376,7 @@ class ODomain:
                     ob = self.blocks[bnd.block]
                     oo = self.offsets[bnd.block]
                     ostride = [1, ob.size[0], ob.size[0] * (ob.size[1] if D > 1 else 1)]
-                    q = p.copy()  # computeConnectedPos, kernel.cu:326-345
+                    q = p.copy()  # computeConnectedPos, extensions/PISO_multiblock_cuda_kernel.cu:326-345
                     ca = bnd.axes[0] >> 1
                     q[:, ca] = ob.size[ca] - 1 if (bnd.axes[0] & 1) else 0
                     if D > 1:
@@ -441,7 +441,7 @@ class ODomain:
             b.pressure = p[o:o + b.ncells].reshape(b.pressure.shape).copy()
 
     def viscosity_cells(self):
-        """getViscosityBlock, kernel.cu:1801-1822."""
+        """getViscosityBlock, extensions/PISO_multiblock_cuda_kernel.cu:1801-1822."""
         nu = np.full(self.N, self.viscosity)
         for bi, b in enumerate(self.blocks):
             if b.viscosity is None:
@@ -455,7 +455,7 @@ class ODomain:
         return nu
 
     def source_cells(self):
-        """getBlockVelocitySource, kernel.cu:2241-2251."""
+        """getBlockVelocitySource, extensions/PISO_multiblock_cuda_kernel.cu:2241-2251."""
         D = self.dims
         s = np.zeros((D, self.N))
         for bi, b in enumerate(self.blocks):
@@ -471,9 +471,9 @@ class ODomain:
 
     def boundary_cell_data(self):
         """Per face: boundary velocity [D,N], contravariant normal boundary flux [N] and
-        boundary Laplace coefficient [N] at fixed faces (getFixedBoundaryData kernel.cu:2374-2433,
-        getContravariantComponentBoundaryFixed kernel.cu:728-748, getLaplaceCoefficientOrthogonalBoundary
-        kernel.cu:1434-1447)."""
+        boundary Laplace coefficient [N] at fixed faces (getFixedBoundaryData extensions/PISO_multiblock_cuda_kernel.cu:2374-2433,
+        getContravariantComponentBoundaryFixed extensions/PISO_multiblock_cuda_kernel.cu:728-748, getLaplaceCoefficientOrthogonalBoundary
+        extensions/PISO_multiblock_cuda_kernel.cu:1434-1447)."""
         D = self.dims
         N = self.N
         K = 2 * D
@@ -523,19 +523,19 @@ class ODomain:
 # --------------------------------------------------------------------------
 
 def contravariant(dom: ODomain, u: np.ndarray, comp: np.ndarray, idx: np.ndarray) -> np.ndarray:
-    """det * Minv[comp] . u at cells idx (VelocityToContravariantComponent, kernel.cu:479-494)."""
+    """det * Minv[comp] . u at cells idx (VelocityToContravariantComponent, extensions/PISO_multiblock_cuda_kernel.cu:479-494)."""
     Mrow = dom.Minv[idx, comp, :]  # [n, D]
     return dom.det[idx] * np.einsum("nj,jn->n", Mrow, u[:, idx])
 
 
 def laplace_coef(dom: ODomain, comp: np.ndarray, idx: np.ndarray) -> np.ndarray:
-    """det * |Minv[comp]|^2 (getLaplaceCoefficientOrthogonal, kernel.cu:1209-1224)."""
+    """det * |Minv[comp]|^2 (getLaplaceCoefficientOrthogonal, extensions/PISO_multiblock_cuda_kernel.cu:1209-1224)."""
     Mrow = dom.Minv[idx, comp, :]
     return dom.det[idx] * np.einsum("nj,nj->n", Mrow, Mrow)
 
 
 def face_fluxes(dom: ODomain, u: np.ndarray, bflux: np.ndarray) -> np.ndarray:
-    """computeFluxesNDLoop, kernel.cu:1552-1630: per face the (unsigned) contravariant face flux,
+    """computeFluxesNDLoop, extensions/PISO_multiblock_cuda_kernel.cu:1552-1630: per face the (unsigned) contravariant face flux,
     central average of the two cells, or the prescribed boundary flux at fixed faces."""
     D = dom.dims
     N = dom.N
@@ -553,7 +553,7 @@ def face_fluxes(dom: ODomain, u: np.ndarray, bflux: np.ndarray) -> np.ndarray:
 
 
 def advection_matrix(dom: ODomain, dt: float):
-    """PISO_build_matrix, kernel.cu:3601-3865 (orthogonal terms only, nonOrthoFlags=0).
+    """PISO_build_matrix, extensions/PISO_multiblock_cuda_kernel.cu:3601-3865 (orthogonal terms only, nonOrthoFlags=0).
 
     Returns (coef[K,N], A[N]) with coefficients divided by det as the reference does.
     """
@@ -589,7 +589,7 @@ def advection_matrix(dom: ODomain, dt: float):
 
 
 def advection_rhs(dom: ODomain, dt: float):
-    """kPISO_build_advection_RHS, kernel.cu:4281-4385 (FIXED boundaries, no pressure gradient)."""
+    """kPISO_build_advection_RHS, extensions/PISO_multiblock_cuda_kernel.cu:4281-4385 (FIXED boundaries, no pressure gradient)."""
     D = dom.dims
     u = dom.velocity_global()
     bvel, bflux, balpha = dom.boundary_cell_data()
@@ -610,7 +610,7 @@ def advection_rhs(dom: ODomain, dt: float):
 
 
 def pressure_matrix(dom: ODomain, A: np.ndarray):
-    """PISO_build_pressure_matrix, kernel.cu:4797-4963 (no face transforms, no non-ortho terms)."""
+    """PISO_build_pressure_matrix, extensions/PISO_multiblock_cuda_kernel.cu:4797-4963 (no face transforms, no non-ortho terms)."""
     D = dom.dims
     N = dom.N
     K = 2 * D + 1
@@ -633,7 +633,7 @@ def pressure_matrix(dom: ODomain, A: np.ndarray):
 
 
 def pressure_rhs(dom: ODomain, dt: float, Ccoef: np.ndarray, A: np.ndarray, u_star: np.ndarray):
-    """PISO_build_pressure_rhs, kernel.cu:5121-5240 (with boundary sources, the compiled default)."""
+    """PISO_build_pressure_rhs, extensions/PISO_multiblock_cuda_kernel.cu:5121-5240 (with boundary sources, the compiled default)."""
     D = dom.dims
     N = dom.N
     u = dom.velocity_global()
@@ -660,7 +660,7 @@ def pressure_rhs(dom: ODomain, dt: float, Ccoef: np.ndarray, A: np.ndarray, u_st
 
 
 def divergence(dom: ODomain, h: np.ndarray):
-    """k_computePressureRHSdivergenceFromFlux, kernel.cu:5374-5419 (no time-step norm)."""
+    """k_computePressureRHSdivergenceFromFlux, extensions/PISO_multiblock_cuda_kernel.cu:5374-5419 (no time-step norm)."""
     D = dom.dims
     _, bflux, _ = dom.boundary_cell_data()
     fl = face_fluxes(dom, h, bflux)
@@ -671,7 +671,7 @@ def divergence(dom: ODomain, h: np.ndarray):
 
 
 def pressure_gradient_fd(dom: ODomain, p: np.ndarray):
-    """getPressureGradient, kernel.cu:801-834 with getPressureAtWithBounds kernel.cu:2160-2239."""
+    """getPressureGradient, extensions/PISO_multiblock_cuda_kernel.cu:801-834 with getPressureAtWithBounds extensions/PISO_multiblock_cuda_kernel.cu:2160-2239."""
     D = dom.dims
     N = dom.N
     g = np.zeros((D, N))
@@ -689,7 +689,7 @@ def pressure_gradient_fd(dom: ODomain, p: np.ndarray):
 
 
 def correct_velocity(dom: ODomain, p_blocks: np.ndarray, A: np.ndarray, h: np.ndarray):
-    """PISO_update_velocity (version 1, FD), kernel.cu:5947-5980."""
+    """PISO_update_velocity (version 1, FD), extensions/PISO_multiblock_cuda_kernel.cu:5947-5980."""
     g = pressure_gradient_fd(dom, p_blocks)
     return h - g / A[None]
 
@@ -699,7 +699,7 @@ def correct_velocity(dom: ODomain, p_blocks: np.ndarray, A: np.ndarray, h: np.nd
 # --------------------------------------------------------------------------
 
 def stencil_to_csr(dom: ODomain, coef: np.ndarray):
-    """CSR (value, index, row) with each row sorted by column like kernel.cu:3846-3860."""
+    """CSR (value, index, row) with each row sorted by column like extensions/PISO_multiblock_cuda_kernel.cu:3846-3860."""
     D = dom.dims
     N = dom.N
     cols = [np.arange(N)] + [dom.nb[f] for f in range(2 * D)]
@@ -742,12 +742,12 @@ class SolveInfo:
 
 
 def _crit(r):
-    """NORM2_NORMALIZED: ||r||_2 / sqrt(n) (cg.cu:85-90)."""
+    """NORM2_NORMALIZED: ||r||_2 / sqrt(n) (extensions/cg_solver_kernel.cu:85-90)."""
     return float(np.sqrt(np.dot(r, r)) / math.sqrt(r.shape[0]))
 
 
 def cg(A, b, x0=None, tol=1e-5, maxit=5000, dtype=np.float64):
-    """cgSolveGPU without rank-deficiency, residual reset or best-result, cg.cu:236-427."""
+    """cgSolveGPU without rank-deficiency, residual reset or best-result, extensions/cg_solver_kernel.cu:236-427."""
     b = np.asarray(b, dtype=dtype)
     x = np.zeros_like(b) if x0 is None else np.array(x0, dtype=dtype)
     A = A.astype(dtype)
@@ -775,7 +775,7 @@ def cg(A, b, x0=None, tol=1e-5, maxit=5000, dtype=np.float64):
 
 
 def bicgstab(A, b, x0=None, tol=1e-5, maxit=5000, dtype=np.float64):
-    """bicgstabSolveGPU without preconditioner, bicg.cu:240-360."""
+    """bicgstabSolveGPU without preconditioner, extensions/bicgstab_solver_kernel.cu:240-360."""
     b = np.asarray(b, dtype=dtype)
     x = np.zeros_like(b) if x0 is None else np.array(x0, dtype=dtype)
     A = A.astype(dtype)
@@ -820,7 +820,7 @@ def bicgstab(A, b, x0=None, tol=1e-5, maxit=5000, dtype=np.float64):
 
 
 def solve(A, b, use_bicg: bool, tol: float, maxit: int = 5000, method: str = "iterative"):
-    """Linear solve as the simulation driver issues it (diff.py:245-293): an all-zero RHS gives x=0."""
+    """Linear solve as the simulation driver issues it (PISOtorch_diff.py:245-293): an all-zero RHS gives x=0."""
     if not np.any(b != 0):
         return np.zeros_like(b), SolveInfo(0.0, 0, True, True)
     if method == "direct":
@@ -833,7 +833,7 @@ def solve(A, b, use_bicg: bool, tol: float, maxit: int = 5000, method: str = "it
 
 
 # --------------------------------------------------------------------------
-# PISO step (sim.py:1054-1327, orthogonal branch)
+# PISO step (PISOtorch_simulation.py:1054-1327, orthogonal branch)
 # --------------------------------------------------------------------------
 
 @dataclass
@@ -853,7 +853,7 @@ class StepResult:
 def piso_step(dom: ODomain, dt: float, corrector_steps: int = 2, adv_tol: float = 1e-5,
               p_tol: float = 1e-5, method: str = "iterative", maxit: int = 5000,
               normalize_pressure: bool = True) -> StepResult:
-    """One PISO step, Simulation._PISO_split_step with non_orthogonal=False, sim.py:1054-1327.
+    """One PISO step, Simulation._PISO_split_step with non_orthogonal=False, PISOtorch_simulation.py:1054-1327.
 
     Updates the block velocity and pressure of ``dom`` in place and returns the intermediate fields
     of the last corrector for inspection.
@@ -865,7 +865,7 @@ def piso_step(dom: ODomain, dt: float, corrector_steps: int = 2, adv_tol: float 
     rhs = advection_rhs(dom, dt)
     Cm = stencil_to_scipy(dom, Ccoef)
     u_star = np.zeros((D, N))
-    for c in range(D):  # nBatches = D, solved one after another (bicg.cu:221)
+    for c in range(D):  # nBatches = D, solved one after another (extensions/bicgstab_solver_kernel.cu:221)
         u_star[c], info = solve(Cm, rhs[c], True, adv_tol, maxit, method)
         infos.append(("adv", c, info))
     u_cur = u_star
@@ -878,7 +878,7 @@ def piso_step(dom: ODomain, dt: float, corrector_steps: int = 2, adv_tol: float 
         p, info = solve(Pm, div, False, p_tol, maxit, method)
         infos.append(("p", 0, info))
         if normalize_pressure:
-            p = p - p.mean()  # sim.py:1243-1244
+            p = p - p.mean()  # PISOtorch_simulation.py:1243-1244
         dom.set_pressure_global(p)  # CopyPressureResultToBlocks
         u_cur = correct_velocity(dom, p, A, h)
     dom.set_velocity_global(u_cur)  # CopyVelocityResultToBlocks

@@ -5,7 +5,7 @@ the reference's pybind11 module (extensions/PISOtorch.cpp:25-655, backed by
 extensions/domain_structs.{h,cpp}), implemented as a thin Python layer over the
 C ABI of ``libpict_b200.so`` (include/pict_b200.h).  Field memory stays in
 torch tensors owned by Python; the native code receives raw device pointers in
-a packed block table (the reference's "atlas", domain_structs.cpp:2992-3261),
+a packed block table (the reference's "atlas", extensions/domain_structs.cpp:2992-3261),
 re-packed by ``Domain.UpdateDomainData()`` exactly when the reference requires
 it.
 
@@ -38,7 +38,7 @@ from . import _lib
 from ._lib import BlockDesc, DomainDesc, Face, SolveInfo, SolveParams, check
 
 # ------------------------------------------------------------------------------------------------
-# enums and small types (PISOtorch.cpp:30-58, 544-558)
+# enums and small types (extensions/PISOtorch.cpp:30-58, 544-558)
 # ------------------------------------------------------------------------------------------------
 
 
@@ -79,7 +79,7 @@ ABS_MAX = ConvergenceCriterion.ABS_MAX
 
 
 class Int4:
-    """I4 (domain_structs_gpu.h:120-125)."""
+    """I4 (extensions/domain_structs_gpu.h:120-125)."""
 
     def __init__(self, x=0, y=0, z=0, w=0):
         self.x, self.y, self.z, self.w = int(x), int(y), int(z), int(w)
@@ -99,7 +99,7 @@ class Int4:
 
 
 class LinearSolverResultInfo:
-    """bicgstab_solver.h:20-34."""
+    """extensions/bicgstab_solver.h:20-34."""
 
     def __init__(self, finalResidual=0.0, usedIterations=-1, converged=False, isFiniteResidual=True):
         self.finalResidual = float(finalResidual)
@@ -119,7 +119,7 @@ AXIS_NAMES = ["x", "y", "z"]
 
 
 def _face_index(face) -> int:
-    """BoundarySideToIndex, domain_structs.cpp:134-155."""
+    """BoundarySideToIndex, extensions/domain_structs.cpp:134-155."""
     if isinstance(face, str):
         if face not in FACE_NAMES:
             raise ValueError("Invalid boundary side '%s'" % face)
@@ -184,7 +184,7 @@ def _as_scalar(v, default=None):
 
 
 # ------------------------------------------------------------------------------------------------
-# CSR / stencil matrices (domain_structs.h:54-90)
+# CSR / stencil matrices (extensions/domain_structs.h:54-90)
 # ------------------------------------------------------------------------------------------------
 
 
@@ -334,7 +334,7 @@ class StencilMatrix(CSRmatrix):
 
 
 # ------------------------------------------------------------------------------------------------
-# boundaries (domain_structs.h:92-375)
+# boundaries (extensions/domain_structs.h:92-375)
 # ------------------------------------------------------------------------------------------------
 
 
@@ -376,7 +376,7 @@ class PeriodicBoundary(Boundary):
 
 
 class ConnectedBoundary(Boundary):
-    """domain_structs.h:329-352; ``axes`` starts with the connected face of the other block."""
+    """extensions/domain_structs.h:329-352; ``axes`` starts with the connected face of the other block."""
 
     def __init__(self, block, axes, domain):
         super().__init__(BoundaryType.CONNECTED, domain)
@@ -405,7 +405,7 @@ class ConnectedBoundary(Boundary):
 
 
 class FixedBoundary(Boundary):
-    """Prescribed boundary: Dirichlet velocity, 0-Neumann pressure (domain_structs.cpp:304-796)."""
+    """Prescribed boundary: Dirichlet velocity, 0-Neumann pressure (extensions/domain_structs.cpp:304-796)."""
 
     def __init__(self, domain, velocity=None, velocityType=BoundaryConditionType.DIRICHLET, passiveScalar=None,
                  transform=None):
@@ -550,7 +550,7 @@ class FixedBoundary(Boundary):
         return v
 
     def GetFluxes(self):
-        """Boundary-normal fluxes det * (Minv u)_axis (domain_structs.cpp:527-542)."""
+        """Boundary-normal fluxes det * (Minv u)_axis (extensions/domain_structs.cpp:527-542)."""
         _check(self.hasSize(), "FixedBoundary has no size set.")
         v = self.getVelocityVarying(None)
         if self.hasTransform():
@@ -644,7 +644,7 @@ class FixedBoundary(Boundary):
 
 
 # ------------------------------------------------------------------------------------------------
-# blocks (domain_structs.h:354-540)
+# blocks (extensions/domain_structs.h:354-540)
 # ------------------------------------------------------------------------------------------------
 
 
@@ -929,7 +929,7 @@ class Block:
 
     # -- coordinates and transforms --
     def setVertexCoordinates(self, coords):
-        """Block::setVertexCoordinates, domain_structs.cpp:2001-2019."""
+        """Block::setVertexCoordinates, extensions/domain_structs.cpp:2001-2019."""
         _check(coords.is_cuda and coords.is_contiguous(), "vertex coordinates must be a contiguous CUDA tensor")
         _check(coords.dim() == self.velocity.dim(), "new vertex coordinates dimensions must match velocity.")
         _check(coords.size(0) == 1, "batches are not yet supported.")
@@ -989,7 +989,7 @@ class Block:
         return 0 if smin != smax else smin
 
     def _GetFaceTransformBoundarySlice(self, face):
-        """domain_structs.cpp:1809-1835."""
+        """extensions/domain_structs.cpp:1809-1835."""
         _check(self.hasFaceTransform(), "faceTransform missing to slice for boundary.")
         dims = self.getSpatialDims()
         axis, upper = face >> 1, face & 1
@@ -1015,7 +1015,7 @@ class Block:
                "Face index must be in [0, dims*2) or one of {-x, +x, -y, +y, -z, +z} for exising spatial dimensions.")
 
     def _setBoundary(self, faceIndex, boundary):
-        """Block::setBoundary, domain_structs.cpp:1653-1741."""
+        """Block::setBoundary, extensions/domain_structs.cpp:1653-1741."""
         face = _face_index(faceIndex)
         self._check_face(face)
         dims = self.getSpatialDims()
@@ -1058,14 +1058,14 @@ class Block:
         return all(b.isPassiveScalarBoundaryTypeStatic() for _, b in self.getFixedBoundaries())
 
     def _MakeFixedBoundary(self, face, velocity=None, passiveScalar=None):
-        """domain_structs.cpp:1897-1922."""
+        """extensions/domain_structs.cpp:1897-1922."""
         d = self.getParentDomain()
         transform = self._GetFaceTransformBoundarySlice(face) if self.hasFaceTransform() else None
         fb = FixedBoundary(d, velocity, BoundaryConditionType.DIRICHLET, passiveScalar, transform)
         self._setBoundary(face, fb)
 
     def _CloseConnectedBoundary(self, face):
-        """Block::CloseConnectedBoudary with useFixed, domain_structs.cpp:1773-1807."""
+        """Block::CloseConnectedBoudary with useFixed, extensions/domain_structs.cpp:1773-1807."""
         b = self.boundaries[face]
         if isinstance(b, ConnectedBoundary):
             b.getConnectedBlock()._MakeFixedBoundary(b.axes[0])
@@ -1083,7 +1083,7 @@ class Block:
             self.CloseBoundary(f)
 
     def ConnectBlock(self, faceIndex, otherBlock, otherFaceIndex, axis1Index=-1, axis2Index=-1):
-        """Block::ConnectBlock -> ConnectBlocks, domain_structs.cpp:1064-1097, 1924-1930."""
+        """Block::ConnectBlock -> ConnectBlocks, extensions/domain_structs.cpp:1064-1097, 1924-1930."""
         face1 = _face_index(faceIndex)
         face2 = _face_index(otherFaceIndex)
         a1 = _face_index(axis1Index) if axis1Index not in (-1, "") else -1
@@ -1136,7 +1136,7 @@ class Block:
             self.MakePeriodic(a)
 
     def ComputeCSRSize(self):
-        """domain_structs.cpp:2151-2161."""
+        """extensions/domain_structs.cpp:2151-2161."""
         s = self.getSizes()
         sz = [s.x, s.y, s.z]
         n = s.x * s.y * s.z * (2 * self.getSpatialDims() + 1)
@@ -1171,7 +1171,7 @@ class Block:
 
 
 # ------------------------------------------------------------------------------------------------
-# domain (domain_structs.h:563-787)
+# domain (extensions/domain_structs.h:563-787)
 # ------------------------------------------------------------------------------------------------
 
 
@@ -1332,7 +1332,7 @@ class Domain:
         return all(b.isAllFixedBoundariesPassiveScalarTypeStatic() for b in self.blocks)
 
     def GetBoundaryFluxBalance(self):
-        """Domain::GetGlobalFluxBalance, domain_structs.cpp:2460-2493."""
+        """Domain::GetGlobalFluxBalance, extensions/domain_structs.cpp:2460-2493."""
         s = torch.zeros([1], dtype=self._dtype, device=self._device)
         for b in self.blocks:
             for i, bnd in enumerate(b.boundaries):
@@ -1344,7 +1344,7 @@ class Domain:
     def CheckBoundaryFluxBalance(self, eps=1e-5):
         return abs(self.GetBoundaryFluxBalance().item()) < eps
 
-    # -- preparation (Domain::PrepareSolve, domain_structs.cpp:2554-2676) --
+    # -- preparation (Domain::PrepareSolve, extensions/domain_structs.cpp:2554-2676) --
     def PrepareSolve(self):
         _check(len(self.blocks) > 0, "Domain does not contain any blocks.")
         _check(self.viscosity.dtype == self._dtype, "Data type of viscosity does not match.")
@@ -1409,7 +1409,7 @@ class Domain:
         self.UpdateDomainData()
 
     def _pack_blocks(self):
-        """Host block table with raw device pointers (Domain::UpdateDomainGPU, domain_structs.cpp:3040-3261)."""
+        """Host block table with raw device pointers (Domain::UpdateDomainGPU, extensions/domain_structs.cpp:3040-3261)."""
         arr = (BlockDesc * len(self.blocks))()
         index = {id(b): i for i, b in enumerate(self.blocks)}
         for bi, b in enumerate(self.blocks):
@@ -1451,7 +1451,7 @@ class Domain:
         return arr
 
     def UpdateDomainData(self):
-        """Re-pack raw pointers after tensors were replaced (Domain::UpdateDomain, domain_structs.cpp:3031-3038)."""
+        """Re-pack raw pointers after tensors were replaced (Domain::UpdateDomain, extensions/domain_structs.cpp:3031-3038)."""
         _check(self._initialized, "Domain is not initialized.")
         host = self._pack_blocks()
         raw = bytes(host)
@@ -1515,7 +1515,7 @@ class Domain:
             self._csr_struct = (row, index)
         return self._csr_struct
 
-    # -- global field setters (domain_structs.cpp:2750-2828) --
+    # -- global field setters (extensions/domain_structs.cpp:2750-2828) --
     def _set_global(self, name, t, size):
         _check(t.is_cuda and t.is_contiguous() and t.dim() == 1, "%s must be a contiguous 1D CUDA tensor" % name)
         _check(t.size(0) == size, "%s has the wrong size (%d, expected %d)" % (name, t.size(0), size))
@@ -1664,7 +1664,7 @@ class Domain:
 
 
 # ------------------------------------------------------------------------------------------------
-# operators (PISOtorch.cpp:529-601)
+# operators (extensions/PISOtorch.cpp:529-601)
 # ------------------------------------------------------------------------------------------------
 
 
@@ -1682,7 +1682,7 @@ def _non_ortho(flags):
 
 
 def SetupAdvectionMatrix(domain, timeStep, nonOrthoFlags, forPassiveScalar=False, passiveScalarChannel=0):
-    """Implicit advection-diffusion matrix C and its diagonal A (kernel.cu:3601-3865)."""
+    """Implicit advection-diffusion matrix C and its diagonal A (extensions/PISO_multiblock_cuda_kernel.cu:3601-3865)."""
     if forPassiveScalar:
         raise NotImplementedError("passive scalar transport is not implemented in pict_b200")
     _non_ortho(nonOrthoFlags)
@@ -1692,7 +1692,7 @@ def SetupAdvectionMatrix(domain, timeStep, nonOrthoFlags, forPassiveScalar=False
 
 
 def SetupAdvectionVelocity(domain, timeStep, nonOrthoFlags, applyPressureGradient=False):
-    """Velocity RHS of the advection-diffusion solve (kernel.cu:4281-4385)."""
+    """Velocity RHS of the advection-diffusion solve (extensions/PISO_multiblock_cuda_kernel.cu:4281-4385)."""
     _non_ortho(nonOrthoFlags)
     domain._check_ready()
     dt = _time_step(timeStep, domain)
@@ -1705,7 +1705,7 @@ def SetupAdvectionScalar(domain, timeStep, nonOrthoFlags):
 
 
 def SetupPressureCorrection(domain, timeStep, nonOrthoMode=0, useFaceTransform=False, timeStepNorm=False):
-    """Pressure matrix, H/A RHS and its divergence (kernel.cu:4797-5419)."""
+    """Pressure matrix, H/A RHS and its divergence (extensions/PISO_multiblock_cuda_kernel.cu:4797-5419)."""
     _non_ortho(nonOrthoMode)
     if useFaceTransform:
         raise NotImplementedError("face-transform pressure assembly is not implemented in pict_b200")
@@ -1745,7 +1745,7 @@ def SetupPressureRHSdiv(domain, timeStep, nonOrthoMode=0, useFaceTransform=False
 
 
 def CorrectVelocity(domain, timeStep, version=0, timeStepNorm=False):
-    """u = H/A - grad(p)/A with finite-difference pressure gradients (kernel.cu:5947-5980)."""
+    """u = H/A - grad(p)/A with finite-difference pressure gradients (extensions/PISO_multiblock_cuda_kernel.cu:5947-5980)."""
     if version not in (0, 1):
         raise NotImplementedError("only the finite-difference velocity corrector (version 0/1) is implemented in pict_b200")
     domain._check_ready()
@@ -1784,7 +1784,7 @@ def CopyScalarResultFromBlocks(domain):
 
 
 def ComputeVelocityDivergence(domain):
-    """Flux divergence of the blocks' velocity (kernel.cu:6333-6388)."""
+    """Flux divergence of the blocks' velocity (extensions/PISO_multiblock_cuda_kernel.cu:6333-6388)."""
     domain._check_ready()
     out = torch.zeros_like(domain.pressureResult)
     check(_lib.load().pict_velocity_divergence(ctypes.byref(domain._desc), _ptr(out), _stream_ptr()),
@@ -1793,7 +1793,7 @@ def ComputeVelocityDivergence(domain):
 
 
 def CoordsToTransforms(coords):
-    """Cell transforms (M, Minv, det) from vertex coordinates (grid_gen.cu:341-375)."""
+    """Cell transforms (M, Minv, det) from vertex coordinates (extensions/grid_gen.cu:341-375)."""
     _check(coords.is_cuda and coords.is_contiguous(), "coords must be a contiguous CUDA tensor")
     _check(2 < coords.dim() < 6, "coords must have batch and channel dimension and be 1-3D.")
     _check(coords.size(0) == 1, "coords batch dimension must be 1.")
@@ -1809,7 +1809,7 @@ def CoordsToTransforms(coords):
 
 
 def CoordsToFaceTransforms(coords):
-    """Staggered face transforms from vertex coordinates (grid_gen.cu:468-514)."""
+    """Staggered face transforms from vertex coordinates (extensions/grid_gen.cu:468-514)."""
     _check(coords.is_cuda and coords.is_contiguous(), "coords must be a contiguous CUDA tensor")
     dims = coords.dim() - 2
     size = [coords.size(-1 - d) - 1 for d in range(dims)]
@@ -1822,7 +1822,7 @@ def CoordsToFaceTransforms(coords):
 
 
 def TransformVectors(vectors, transforms, inverse=False):
-    """Per-cell vector transform (kernel.cu:7152-7224): M u, or Minv u with ``inverse``."""
+    """Per-cell vector transform (extensions/PISO_multiblock_cuda_kernel.cu:7152-7224): M u, or Minv u with ``inverse``."""
     dims = vectors.size(1)
     tr = transforms.reshape(-1, _transform_size(dims))
     off = dims * dims if inverse else 0
@@ -1833,7 +1833,7 @@ def TransformVectors(vectors, transforms, inverse=False):
 
 
 # ------------------------------------------------------------------------------------------------
-# linear solves (PISOtorch.cpp:559-563 -> kernel.cu:7021-7103)
+# linear solves (extensions/PISOtorch.cpp:559-563 -> extensions/PISO_multiblock_cuda_kernel.cu:7021-7103)
 # ------------------------------------------------------------------------------------------------
 
 _warned = set()
@@ -1954,7 +1954,7 @@ def SolveLinear(A, RHS, x, maxIterations=1000, tolerance=1e-8, convergenceCriter
 
 
 def SparseOuterProduct(a, b, out_pattern):
-    """out.value[ij] = a_i * b_j on the sparsity pattern of out (cg.cu:869-908)."""
+    """out.value[ij] = a_i * b_j on the sparsity pattern of out (extensions/cg_solver_kernel.cu:869-908)."""
     _check(isinstance(out_pattern, StencilMatrix), "SparseOuterProduct: out_pattern must be a domain matrix")
     d = out_pattern._domain()
     N = out_pattern.getRows()

@@ -5,7 +5,7 @@ stages (``prep_fn``) and run loop (PISOtorch_simulation.py:398-1518).  Two
 execution paths produce the same step:
 
 * the generic path issues the operators one by one exactly like the reference's
-  ``_PISO_split_step`` orthogonal branch (sim.py:1054-1327), so every
+  ``_PISO_split_step`` orthogonal branch (PISOtorch_simulation.py:1054-1327), so every
   ``prep_fn`` stage fires and the differentiable backend can record the graph;
 * the fused path (no hooks, not differentiable, FD corrector, GPU solves) hands
   the whole step to :class:`pict_b200.engine.PISOStepper`, which launches it
@@ -37,7 +37,7 @@ cpu_device = torch.device("cpu")
 
 
 class StopHandler:
-    """SIGINT handler polled by the run loop (sim.py:27-50)."""
+    """SIGINT handler polled by the run loop (PISOtorch_simulation.py:27-50)."""
 
     def __init__(self, log=None):
         self._log = log
@@ -69,7 +69,7 @@ def ntonp(t):
 
 
 def get_max_time_step(domain, time_step_target, CFL_cond=0.8, with_transformations=True):
-    """sim.py:55-64."""
+    """PISOtorch_simulation.py:55-64."""
     max_vel = float(domain.getMaxVelocity(True, with_transformations).item())
     max_time_step = CFL_cond / max_vel
     if max_time_step >= time_step_target:
@@ -162,7 +162,7 @@ class Simulation:
         self._stepper_key = None
         self.reset_step_counters()
 
-    # ------------------------------------------------------------------ properties (sim.py:478-860)
+    # ------------------------------------------------------------------ properties (PISOtorch_simulation.py:478-860)
     @property
     def domain(self):
         return self._domain
@@ -329,7 +329,7 @@ class Simulation:
         self.reset_total_step()
         self.reset_total_time()
 
-    # ------------------------------------------------------------------ solves (sim.py:861-904)
+    # ------------------------------------------------------------------ solves (PISOtorch_simulation.py:861-904)
     def linear_solve(self, csrMat, rhs, x=None, use_BiCG=False, tol=None, max_iter=None, matrix_rank_deficient=False,
                      residual_reset_step=0, use_scipy=False, return_best_result=False):
         if use_scipy:
@@ -403,7 +403,7 @@ class Simulation:
         return self._PISO_split_step_ops(iterations, time_step)
 
     def _PISO_split_step_ops(self, iterations, time_step):
-        """Operator-by-operator step, sim.py:1054-1327 (orthogonal branch)."""
+        """Operator-by-operator step, PISOtorch_simulation.py:1054-1327 (orthogonal branch)."""
         domain = self.domain
         B = self._backend
         vcv = self._velocity_corrector_version
@@ -473,7 +473,7 @@ class Simulation:
         return solve_ok
 
     def _PISO_adaptive_step(self, CFL_cond=None, max_subsetps=1000):
-        """sim.py:1329-1372."""
+        """PISOtorch_simulation.py:1329-1372."""
         time_step_target = self.time_step
         domain = self.domain
         CFL_cond = CFL_cond if CFL_cond is not None else self.adaptive_CFL
@@ -493,7 +493,7 @@ class Simulation:
         return True
 
     def make_divergence_free(self, iterations=1, max_iter=1000):
-        """Pressure projection of the current velocity with A = 1, dt = 1 (sim.py:985-1052)."""
+        """Pressure projection of the current velocity with A = 1, dt = 1 (PISOtorch_simulation.py:985-1052)."""
         self._check_domain()
         self._check_non_ortho()
         domain = self.domain
@@ -522,7 +522,7 @@ class Simulation:
         return solve_ok
 
     def run(self, iterations, static=False, log_domain=True):
-        """sim.py:1374-1518 without image/VTK output."""
+        """PISOtorch_simulation.py:1374-1518 without image/VTK output."""
         self._check_domain()
         if static:
             raise NotImplementedError("passive scalar transport is not implemented in pict_b200")

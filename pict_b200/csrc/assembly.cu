@@ -5,13 +5,13 @@
 // arrays, coalesced) instead of the reference's sorted CSR rows.
 //
 // Reference kernels restated here (kernel.cu = extensions/PISO_multiblock_cuda_kernel.cu):
-//   PISO_build_matrix            kernel.cu:3601-3865
-//   kPISO_build_advection_RHS    kernel.cu:4281-4385
-//   PISO_build_pressure_matrix   kernel.cu:4797-4963
-//   PISO_build_pressure_rhs      kernel.cu:5121-5240
-//   k_computePressureRHSdivergenceFromFlux kernel.cu:5374-5419
-//   PISO_update_velocity (FD)    kernel.cu:5947-5980 with getPressureGradient kernel.cu:801-834
-//   k_computeVelocityDivergenceFromFlux    kernel.cu:6333-6357
+//   PISO_build_matrix            extensions/PISO_multiblock_cuda_kernel.cu:3601-3865
+//   kPISO_build_advection_RHS    extensions/PISO_multiblock_cuda_kernel.cu:4281-4385
+//   PISO_build_pressure_matrix   extensions/PISO_multiblock_cuda_kernel.cu:4797-4963
+//   PISO_build_pressure_rhs      extensions/PISO_multiblock_cuda_kernel.cu:5121-5240
+//   k_computePressureRHSdivergenceFromFlux extensions/PISO_multiblock_cuda_kernel.cu:5374-5419
+//   PISO_update_velocity (FD)    extensions/PISO_multiblock_cuda_kernel.cu:5947-5980 with getPressureGradient extensions/PISO_multiblock_cuda_kernel.cu:801-834
+//   k_computeVelocityDivergenceFromFlux    extensions/PISO_multiblock_cuda_kernel.cu:6333-6357
 #include "common.cuh"
 #include "launch.h"
 
@@ -22,7 +22,7 @@ namespace pict {
 // ---------------------------------------------------------------------------------------------
 
 // Pressure gradient by central differences, one-sided at fixed faces, times Minv^T
-// (getPressureGradient kernel.cu:801-834, getPressureAtWithBounds kernel.cu:2160-2239).
+// (getPressureGradient extensions/PISO_multiblock_cuda_kernel.cu:801-834, getPressureAtWithBounds extensions/PISO_multiblock_cuda_kernel.cu:2160-2239).
 template <typename T, int D>
 __device__ __forceinline__ void pressure_grad_fd(const pict_domain_t& dom, const pict_block_t& B, int b,
                                                  const int* p, int i, int l, const T* tr, T* g) {
@@ -95,7 +95,7 @@ __global__ void k_adv_setup(pict_domain_t dom, double dt_arg, int apply_pgrad) {
             off[f] = T(0);
             if (n.j < 0) {
                 // prescribed (fixed Dirichlet) face: diffusion towards the wall value, no advective
-                // term in the matrix (kernel.cu:3801-3833); wall sources on the RHS (kernel.cu:4307-4327)
+                // term in the matrix (extensions/PISO_multiblock_cuda_kernel.cu:3801-3833); wall sources on the RHS (extensions/PISO_multiblock_cuda_kernel.cu:4307-4327)
                 if (MATRIX) diag += T(2) * nu * alpha_p[a];
                 if (RHS) {
                     const FixedFace<T, D> ff = fixed_face<T, D>(B, p, f);
@@ -295,7 +295,7 @@ __global__ void k_correct_velocity(pict_domain_t dom, double dt_arg, int time_st
 }
 
 // ---------------------------------------------------------------------------------------------
-// copies between global result vectors and block fields (kernel.cu:6543-6733)
+// copies between global result vectors and block fields (extensions/PISO_multiblock_cuda_kernel.cu:6543-6733)
 // ---------------------------------------------------------------------------------------------
 
 template <typename T, bool TO_BLOCKS, bool VECTOR>
@@ -316,7 +316,7 @@ __global__ void k_copy_result(pict_domain_t dom, int D) {
 }
 
 // ---------------------------------------------------------------------------------------------
-// transforms from vertex coordinates (grid_gen.cu:284-339 and 383-466)
+// transforms from vertex coordinates (extensions/grid_gen.cu:284-339 and 383-466)
 // ---------------------------------------------------------------------------------------------
 
 template <typename T, int D>
@@ -504,7 +504,7 @@ __global__ void k_stencil_to_csr(pict_domain_t dom, const T* coef, const int32_t
             const int j = dom.nbr[(size_t)f * N + i];
             if (j >= 0) { cols[n] = j; vals[n] = coef[(size_t)(f + 1) * N + i]; ++n; }
         }
-        // insertion sort by column (stable), kernel.cu:3846-3860 sorts rows by column index
+        // insertion sort by column (stable), extensions/PISO_multiblock_cuda_kernel.cu:3846-3860 sorts rows by column index
         for (int a = 1; a < n; ++a) {
             const int c = cols[a];
             const T v = vals[a];

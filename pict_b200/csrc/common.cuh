@@ -1,7 +1,7 @@
 // common.cuh -- device-side helpers shared by the PISO kernels.
 //
 // The reference resolves neighbours per thread through a switch over boundary
-// types (resolveNeighborCell / computeConnectedPos, kernel.cu:326-345,
+// types (resolveNeighborCell / computeConnectedPos, extensions/PISO_multiblock_cuda_kernel.cu:326-345,
 // 432-477).  Here the topology is precomputed once per domain into a
 // neighbour table nbr[2D][N] (pict_build_topology); kernels only need the
 // face type to tell connected faces apart (their neighbour lives in another
@@ -37,7 +37,7 @@ __device__ __forceinline__ bool at_face(const int* p, const int32_t* size, int f
 
 // Flat index into the face arrays of a fixed boundary: position with the face axis set to 0,
 // flattened with the boundary's own size (block size with 1 along the face axis),
-// like getFixedBoundaryData (kernel.cu:2420-2428).
+// like getFixedBoundaryData (extensions/PISO_multiblock_cuda_kernel.cu:2420-2428).
 __device__ __forceinline__ int boundary_flat(const int* p, const int32_t* size, int f) {
     const int a = f >> 1;
     int bs[3] = {size[0], size[1], size[2]};
@@ -61,7 +61,7 @@ __device__ __forceinline__ T tr_det(const T* tr) { return tr ? tr[2 * D * D] : T
 template <typename T, int D>
 __device__ __forceinline__ T tr_minv(const T* tr, int r, int c) { return tr[D * D + r * D + c]; }
 
-// Contravariant component c of vector u: det * Minv[c] . u (VelocityToContravariantComponent, kernel.cu:479-494).
+// Contravariant component c of vector u: det * Minv[c] . u (VelocityToContravariantComponent, extensions/PISO_multiblock_cuda_kernel.cu:479-494).
 template <typename T, int D>
 __device__ __forceinline__ T contravariant(const T* tr, int c, const T* u) {
     if (!tr) return u[c];
@@ -71,7 +71,7 @@ __device__ __forceinline__ T contravariant(const T* tr, int c, const T* u) {
     return tr_det<T, D>(tr) * s;
 }
 
-// Orthogonal Laplace coefficient det * |Minv[c]|^2 (getLaplaceCoefficientOrthogonal, kernel.cu:1209-1224).
+// Orthogonal Laplace coefficient det * |Minv[c]|^2 (getLaplaceCoefficientOrthogonal, extensions/PISO_multiblock_cuda_kernel.cu:1209-1224).
 template <typename T, int D>
 __device__ __forceinline__ T laplace_coef(const T* tr, int c) {
     if (!tr) return T(1);
@@ -92,7 +92,7 @@ __device__ __forceinline__ const T* cell_transform(const pict_block_t& B, int l)
 template <typename T>
 __device__ __forceinline__ int block_cells(const pict_block_t& B) { return B.size[0] * B.size[1] * B.size[2]; }
 
-// Viscosity at a cell of a block (getViscosityBlock, kernel.cu:1801-1822).
+// Viscosity at a cell of a block (getViscosityBlock, extensions/PISO_multiblock_cuda_kernel.cu:1801-1822).
 template <typename T>
 __device__ __forceinline__ T cell_viscosity(const pict_domain_t& dom, const pict_block_t& B, int l) {
     if (B.viscosity) {
@@ -102,7 +102,7 @@ __device__ __forceinline__ T cell_viscosity(const pict_domain_t& dom, const pict
     return reinterpret_cast<const T*>(dom.sim_viscosity)[B.sim];
 }
 
-// Velocity source component c (getBlockVelocitySource, kernel.cu:2241-2251).
+// Velocity source component c (getBlockVelocitySource, extensions/PISO_multiblock_cuda_kernel.cu:2241-2251).
 template <typename T>
 __device__ __forceinline__ T cell_source(const pict_block_t& B, int l, int c, int ncells) {
     if (!B.source) return T(0);
@@ -117,7 +117,7 @@ __device__ __forceinline__ T sim_time_step(const pict_domain_t& dom, int sim, do
 
 // Neighbour across face f of a cell: block, local index, the component of the neighbour that is
 // aligned with this face's axis, and the flux sign across the connection (computeFluxesNDLoop,
-// kernel.cu:1589-1606; computeConnectedPosWithChannel kernel.cu:349-360).
+// extensions/PISO_multiblock_cuda_kernel.cu:1589-1606; computeConnectedPosWithChannel extensions/PISO_multiblock_cuda_kernel.cu:349-360).
 struct Nbr {
     int j;      // global index, -1 on fixed faces
     int b;      // block
@@ -147,8 +147,8 @@ __device__ __forceinline__ Nbr neighbour(const pict_domain_t& dom, const pict_bl
 }
 
 // Boundary data of a fixed face: velocity vector, contravariant flux along the face axis and the
-// boundary Laplace coefficient (getFixedBoundaryData kernel.cu:2374-2433,
-// getContravariantComponentBoundaryFixed kernel.cu:728-748, kernel.cu:1434-1447).
+// boundary Laplace coefficient (getFixedBoundaryData extensions/PISO_multiblock_cuda_kernel.cu:2374-2433,
+// getContravariantComponentBoundaryFixed extensions/PISO_multiblock_cuda_kernel.cu:728-748, extensions/PISO_multiblock_cuda_kernel.cu:1434-1447).
 template <typename T, int D>
 struct FixedFace {
     T vel[D];

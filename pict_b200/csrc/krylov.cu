@@ -27,8 +27,8 @@
 //    and convergence state.
 //
 // Iteration semantics, stopping rule and reported iteration counts follow the
-// reference: CG cg.cu:236-427, BiCGStab bicg.cu:240-360, convergence criterion
-// NORM2 / NORM2_NORMALIZED cg.cu:77-110.  As in the Python wrapper
+// reference: CG extensions/cg_solver_kernel.cu:236-427, BiCGStab extensions/bicgstab_solver_kernel.cu:240-360, convergence criterion
+// NORM2 / NORM2_NORMALIZED extensions/cg_solver_kernel.cu:77-110.  As in the Python wrapper
 // (PISOtorch_diff.py:245-293), an all-zero right-hand side yields x = 0.
 #include <cmath>
 #include <cstdio>
@@ -272,7 +272,7 @@ __device__ __forceinline__ pict_solve_info_t fresh_info() {
 }
 
 // ---------------------------------------------------------------------------------------------
-// CG (cg.cu:236-427)
+// CG (extensions/cg_solver_kernel.cu:236-427)
 // ---------------------------------------------------------------------------------------------
 template <typename T, int D, bool TRANS>
 __global__ void __launch_bounds__(KR_THREADS) k_cg(KArgs<T> a) {
@@ -428,7 +428,7 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg(KArgs<T> a) {
         __syncthreads();
         T* tmp = pc; pc = pn; pn = tmp;
     }
-    // ---- mean removal (sim.py:1243-1244) and copy into the blocks' pressure
+    // ---- mean removal (PISOtorch_simulation.py:1243-1244) and copy into the blocks' pressure
     if (a.sub_mean || a.write_bp) {
         if (a.sub_mean) {
             for (int j = 0; j < S.n; ++j) {
@@ -463,7 +463,7 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg(KArgs<T> a) {
 //   b_{i+1} = g_{i+1} / g_i,  a_{i+1} = g_{i+1} / (d_{i+1} - b_{i+1} g_{i+1} / a_i).
 // The same iterates as classic CG in exact arithmetic; one fused sweep (r_{i+1} of the neighbours
 // formed on the fly) and one grid-wide reduction per iteration.  Stopping rule and reported
-// iteration counts as cg.cu:303-397.
+// iteration counts as extensions/cg_solver_kernel.cu:303-397.
 // ---------------------------------------------------------------------------------------------
 template <typename T, int D, bool TRANS>
 __global__ void __launch_bounds__(KR_THREADS) k_cg1(KArgs<T> a) {
@@ -652,7 +652,7 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg1(KArgs<T> a) {
 }
 
 // ---------------------------------------------------------------------------------------------
-// BiCGStab without preconditioner (bicg.cu:240-360), NR right-hand sides sharing the matrix
+// BiCGStab without preconditioner (extensions/bicgstab_solver_kernel.cu:240-360), NR right-hand sides sharing the matrix
 // ---------------------------------------------------------------------------------------------
 template <typename T, int D, int NR, bool TRANS>
 __global__ void __launch_bounds__(KR_THREADS) k_bicgstab(KArgs<T> a) {

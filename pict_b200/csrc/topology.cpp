@@ -1,9 +1,9 @@
 // topology.cpp -- host-side neighbour tables for structured multi-block domains.
 //
 // Restates the neighbour resolution the reference performs per thread inside
-// every kernel (resolveNeighborCell kernel.cu:432-477, computeConnectedPos
-// kernel.cu:326-345) as a one-off table build, plus the connection checks of
-// Domain::PrepareSolve (domain_structs.cpp:2554-2676).
+// every kernel (resolveNeighborCell extensions/PISO_multiblock_cuda_kernel.cu:432-477, computeConnectedPos
+// extensions/PISO_multiblock_cuda_kernel.cu:326-345) as a one-off table build, plus the connection checks of
+// Domain::PrepareSolve (extensions/domain_structs.cpp:2554-2676).
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -36,7 +36,7 @@ extern "C" pict_status_t pict_build_topology(const pict_block_t* blocks, int32_t
         off += (int64_t)B.size[0] * B.size[1] * B.size[2];
     }
     if (off != num_cells) return set_error(PICT_ERR_ARG, "topology: num_cells does not match the blocks");
-    // connection checks (domain_structs.cpp:2575-2650)
+    // connection checks (extensions/domain_structs.cpp:2575-2650)
     for (int b = 0; b < num_blocks; ++b) {
         const pict_block_t& B = blocks[b];
         for (int f = 0; f < 2 * dims; ++f) {

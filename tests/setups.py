@@ -117,7 +117,7 @@ def case(name, seed=0):
                          ("close", 0, "+y", np.array([[1.0, 0.0]]))])
     if name == "twoblock2d_rotated":
         # block 1's +x face joins block 2's +y face with the tangential axis inverted: exercises the
-        # connected-face axis permutation and the flux sign flip (kernel.cu:1589-1606)
+        # connected-face axis permutation and the flux sign flip (extensions/PISO_multiblock_cuda_kernel.cu:1589-1606)
         n = 7
         c1 = tensor_grid(np.linspace(0, 1, n + 1), np.linspace(0, 1, n + 1))
         c2 = tensor_grid(np.linspace(0, 1, n + 1), np.linspace(0, 1, n + 1))

@@ -63,7 +63,7 @@ def test_csr_export_matches_reference_layout(name):
     assert np.array_equal(pd.C.row.cpu().numpy(), r)
     assert np.array_equal(pd.C.index.cpu().numpy(), i)
     _close(_np(pd.C.value), v, 1e-11, "C.value")
-    # the CSR size equals the reference's Block::ComputeCSRSize sum (domain_structs.cpp:2151-2161)
+    # the CSR size equals the reference's Block::ComputeCSRSize sum (extensions/domain_structs.cpp:2151-2161)
     assert pd.C.getSize() == sum(b.ComputeCSRSize() for b in pd.getBlocks())
     # round trip CSR -> stencil
     coef = pd.C.coef.clone()

@@ -1,5 +1,5 @@
 """Krylov solver parity (GPU): persistent CG / BiCGStab kernels vs the oracle's restatement of the
-reference's host loops (cg.cu:236-427, bicg.cu:240-360) and vs a direct solve.
+reference's host loops (extensions/cg_solver_kernel.cu:236-427, extensions/bicgstab_solver_kernel.cu:240-360) and vs a direct solve.
 """
 import numpy as np
 import pytest
