@@ -67,7 +67,7 @@ def build_workload(name, rank=0, dtype=None):
     import torch
     dtype = torch.float32 if dtype is None else dtype
     if name == "batched_cavities_256":
-        sides, re = batched_cavity_params(256, 6 + rank)
+        sides, re = batched_cavity_params(256, rank_seed(rank))
         doms = [make_cavity_domain(int(s), 1.0 / r, dtype) for s, r in zip(sides, re)]
         dts = [0.5 / s for s in sides]
         return dict(domains=doms, dts=dts, sides=sides, re=re, tol=1e-6, correctors=2)
@@ -172,6 +172,24 @@ def sample_indices(sides, k):
     return order[[int(x * len(order)) for x in q]]
 
 
+def rank_seed(rank):
+    """Seed of rank r's batch: every rank advances its own independent simulations."""
+    return 6 + rank
+
+
+def job_totals(cells, ms, world, device):
+    """(cells of all ranks, max elapsed ms over ranks): one all_gather outside the timed region."""
+    import torch
+    if world <= 1:
+        return cells, ms
+    import torch.distributed as dist
+    mine = torch.tensor([float(cells), float(ms)], dtype=torch.float64, device=device)
+    allv = [torch.zeros_like(mine) for _ in range(world)]
+    dist.all_gather(allv, mine)
+    allv = torch.stack(allv).cpu()
+    return int(allv[:, 0].sum().item()), float(allv[:, 1].max().item())
+
+
 def cg_algorithmic_bytes(dims, esz):
     """Algorithmic bytes per cell and CG iteration: read K coefficients, r, p_old; write p_new, q
     (phase 1); read x, p, q, r; write x, r (phase 2)."""
@@ -264,11 +282,7 @@ def run_pict(args, rank, world):
     clocks = sampler.stop()
     ms = e0.elapsed_time(e1)
     adv_infos, p_infos = st.check()
-    t = torch.tensor([ms], device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    total_cells = cells * world
+    total_cells, ms_max = job_totals(cells, ms, world, dev)
     value = total_cells * args.steps / (ms_max * 1e-3)
 
     # roofline of the dominant kernel (persistent CG): eager pass with events around each CG launch
@@ -373,7 +387,8 @@ def e2e_pass(st, batch, args, dev, cells, world):
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
-    return {"value": cells * world * steps / (ms * 1e-3), "unit": "cell-steps/s", "h2d_bytes_per_step": h2d,
+    total_cells, ms_max = job_totals(cells, ms, world, dev)
+    return {"value": total_cells * steps / (ms_max * 1e-3), "unit": "cell-steps/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": h2d, "steps": steps}
 
 
