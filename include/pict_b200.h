@@ -212,6 +212,18 @@ pict_status_t pict_solve(const pict_domain_t* dom, const void* coef, const void*
                          const pict_solve_params_t* params, void* info_out, void* workspace,
                          int64_t workspace_bytes, void* stream);
 
+/* pict_solve without a caller-provided workspace (no counterpart in the reference).  For callers
+ * that hold no device allocator (a plain C or ctypes binding without torch, or a loop that must not
+ * call cudaMalloc, which synchronises the device).  The workspace is a fixed scratch array of
+ * pict_solve_static_scratch_bytes() bytes (8 MiB) in the library's own device memory; the call
+ * allocates nothing.  Solves whose pict_solve_workspace_bytes() exceeds it are rejected with
+ * PICT_ERR_ARG.  The first call on a device looks up the scratch address for that device (make it
+ * before any stream capture).  All calls on a device share the one scratch: calls that overlap in
+ * time (two streams, two host threads) race and must be serialised by the caller.  Nothing in the
+ * scratch has to start at zero; the barrier words are cleared by every call. */
+int64_t pict_solve_static_scratch_bytes(void);
+pict_status_t pict_solve_static(const pict_domain_t* dom, const void* coef, const void* rhs, void* x,
+                                const pict_solve_params_t* params, void* info_out, void* stream);
 
 /* ---------------- matrix export / utilities ---------------- */
 /* CSR materialisation of a stencil matrix in the reference's row layout (rows sorted by

@@ -151,6 +151,8 @@ SIGNATURES = {
     "pict_velocity_divergence": (c_i32, [_PD, c_vp, c_vp]),
     "pict_solve_workspace_bytes": (ctypes.c_int64, [_PD, _PS]),
     "pict_solve": (c_i32, [_PD, c_vp, c_vp, c_vp, _PS, c_vp, c_vp, ctypes.c_int64, c_vp]),
+    "pict_solve_static_scratch_bytes": (ctypes.c_int64, []),
+    "pict_solve_static": (c_i32, [_PD, c_vp, c_vp, c_vp, _PS, c_vp, c_vp]),
     "pict_csr_row_ptr": (c_i32, [_PD, c_vp, c_vp]),
     "pict_stencil_to_csr": (c_i32, [_PD, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "pict_csr_to_stencil": (c_i32, [_PD, c_vp, c_vp, c_vp, c_vp, c_vp]),

@@ -32,6 +32,7 @@
 // (PISOtorch_diff.py:245-293), an all-zero right-hand side yields x = 0.
 #include <cmath>
 #include <cstdio>
+#include <mutex>
 #include "common.cuh"
 #include "launch.h"
 
@@ -1084,11 +1085,67 @@ static pict_status_t run_solve(const pict_domain_t* dom, const void* coef, const
     return PICT_OK;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Fixed scratch for pict_solve_static: callers that hold no device allocator (a plain C or ctypes
+// binding without torch, or a loop that must not call cudaMalloc, which synchronises the device)
+// solve small systems with the workspace placed in this module's own device memory.
+// ---------------------------------------------------------------------------------------------
+constexpr size_t KR_STATIC_SCRATCH_BYTES = size_t(8) << 20;  // 8 MiB: e.g. FP32 CG up to ~290k cells
+static __device__ __align__(256) unsigned char kr_static_scratch[KR_STATIC_SCRATCH_BYTES];
+
+constexpr int KR_MAX_DEVICES = 64;
+static std::mutex g_scratch_mutex;
+static void* g_scratch_ptr[KR_MAX_DEVICES] = {};
+
+// Device address of kr_static_scratch on the current device, looked up once per device.
+static pict_status_t static_scratch(void** out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(PICT_ERR_NO_DEVICE, "solve_static: no current CUDA device");
+    }
+    if (dev < 0 || dev >= KR_MAX_DEVICES) return set_error(PICT_ERR_ARG, "solve_static: device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (!g_scratch_ptr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, kr_static_scratch);
+        if (e != cudaSuccess || !p) {
+            char buf[256];
+            snprintf(buf, sizeof(buf), "solve_static: cudaGetSymbolAddress of the scratch failed: %s", cudaGetErrorString(e));
+            cudaGetLastError();
+            return set_error(PICT_ERR_CUDA, buf);
+        }
+        g_scratch_ptr[dev] = p;
+    }
+    *out = g_scratch_ptr[dev];
+    return PICT_OK;
+}
+
 }  // namespace pict
 
 using namespace pict;
 
 extern "C" {
+
+int64_t pict_solve_static_scratch_bytes(void) { return (int64_t)KR_STATIC_SCRATCH_BYTES; }
+
+pict_status_t pict_solve_static(const pict_domain_t* dom, const void* coef, const void* rhs, void* x,
+                                const pict_solve_params_t* prm, void* info_out, void* stream) {
+    if (!dom || !prm) return set_error(PICT_ERR_ARG, "solve_static: NULL argument");
+    const int64_t need = pict_solve_workspace_bytes(dom, prm);
+    if (need < 0 || need > (int64_t)KR_STATIC_SCRATCH_BYTES) {
+        char buf[256];
+        snprintf(buf, sizeof(buf),
+                 "solve_static: the solve needs %lld bytes of workspace, more than the %lld bytes of static scratch; "
+                 "use pict_solve with a caller-provided workspace",
+                 (long long)need, (long long)KR_STATIC_SCRATCH_BYTES);
+        return set_error(PICT_ERR_ARG, buf);
+    }
+    void* ws = nullptr;
+    const pict_status_t s = static_scratch(&ws);
+    if (s) return s;
+    return pict_solve(dom, coef, rhs, x, prm, info_out, ws, (int64_t)KR_STATIC_SCRATCH_BYTES, stream);
+}
 
 int64_t pict_solve_workspace_bytes(const pict_domain_t* dom, const pict_solve_params_t* prm) {
     if (!dom || !prm) return -1;
