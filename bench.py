@@ -190,6 +190,11 @@ def job_totals(cells, ms, world, device):
     return int(allv[:, 0].sum().item()), float(allv[:, 1].max().item())
 
 
+# DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) over algorithmic bytes of one captured
+# launch of the batched workload (profiles/k_cg1_batched_cavities_256.md)
+NCU_TRAFFIC_RATIO = {"k_cg1": 14.27e9 / 20.12e9}
+
+
 def cg_algorithmic_bytes(dims, esz):
     """Algorithmic bytes per cell and CG iteration: read K coefficients, r, p_old; write p_new, q
     (phase 1); read x, p, q, r; write x, r (phase 2)."""
@@ -245,11 +250,20 @@ def run_pict(args, rank, world):
                      advection_tol=wl["tol"], pressure_tol=wl["tol"], max_iterations=5000,
                      p_group_size=args.group_size, adv_group_size=args.group_size)
     cells = batch.getTotalSize()
-    # warm-up (eager), then capture one step as a CUDA graph
+    # warm-up (eager), then capture one step as a CUDA graph; the algorithmic bytes of every warm-up
+    # CG launch are recorded so that an ncu capture of launch k (-k regex:k_cg -s k -c 1) can be set
+    # against them (the step is deterministic)
+    esz = 4 if batch.getDtype() == torch.float32 else 8
+    per_cell = cg_algorithmic_bytes(batch.getSpatialDims(), esz)
+    n_s = np.diff(batch._sim_cells.cpu().numpy())
+    warm_cg_bytes = []
     for _ in range(args.warmup):
         st.step()
+        _, p_inf = st.check()
+        for p in p_inf:
+            its = np.array([i.usedIterations for i in p])
+            warm_cg_bytes.append(float(np.sum((its + 1) * n_s) * per_cell))
     torch.cuda.synchronize()
-    st.check()
     if not args.no_graph:
         st.capture(steps=1)
     torch.cuda.synchronize()
@@ -287,6 +301,7 @@ def run_pict(args, rank, world):
 
     # roofline of the dominant kernel (persistent CG): eager pass with events around each CG launch
     roof = roofline_pass(st, batch, args, dev)
+    roof["warmup_launch_algorithmic_bytes"] = warm_cg_bytes
 
     # end-to-end through the public API with host buffers
     e2e = e2e_pass(st, batch, args, dev, cells, world)
@@ -353,8 +368,13 @@ def roofline_pass(st, batch, args, dev):
     byt = float(np.mean(cg_bytes))
     achieved = byt / (ms * 1e-3) / 1e9
     peak, kind = measured_peaks()
-    return {"kernel": "k_cg (persistent CG, pressure solve)", "bound": "hbm", "achieved": achieved, "peak": peak,
-            "peak_kind": kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+    kern = "k_cg1" if st.p_params.variant == 1 else "k_cg"
+    ratio = NCU_TRAFFIC_RATIO.get(kern)
+    return {"kernel": "%s (persistent CG, pressure solve)" % kern, "bound": "hbm", "achieved": achieved, "peak": peak,
+            "peak_kind": kind, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": None if ratio is None else ratio * byt,
+            "traffic_note": None if ratio is None else
+            "ncu dram bytes / algorithmic bytes = %.3f on one captured launch (profiles/), scaled to the average launch" % ratio,
             "algorithmic_bytes_per_launch": byt, "avg_launch_ms": ms,
             "bytes_per_cell_iteration": per_cell}
 

@@ -156,7 +156,7 @@ def _ptr(t: Optional[torch.Tensor]):
     return None if t is None else t.data_ptr()
 
 
-TILE_CELLS = 2048  # cells per Krylov work tile (upper bound 2048, see krylov.cu)
+TILE_CELLS = 1024  # cells per Krylov work tile (1..2048; the kernels hold at most 2048)
 
 
 def build_tiles(host_blocks, num_blocks, num_sims, device, tile_cells=TILE_CELLS):
@@ -1403,7 +1403,9 @@ class Domain:
                                               cell_block.data_ptr()), "build_topology")
         self._nbr = nbr.to(self._device)
         self._cell_block = cell_block.to(self._device)
-        self._tiles, self._sim_tiles, self._num_tiles = build_tiles(host_blocks, len(self.blocks), 1, self._device)
+        self._tile_cells = getattr(self, "_tile_cells", TILE_CELLS)
+        self._tiles, self._sim_tiles, self._num_tiles = build_tiles(host_blocks, len(self.blocks), 1, self._device,
+                                                                    self._tile_cells)
         self._csr_struct = None
         self._initialized = True
         self.UpdateDomainData()
@@ -1483,7 +1485,7 @@ class Domain:
         d.tiles = _ptr(self._tiles)
         d.sim_tiles = _ptr(self._sim_tiles)
         d.num_tiles = self._num_tiles
-        d.tile_cells = TILE_CELLS
+        d.tile_cells = self._tile_cells
         d.sim_viscosity = _ptr(self._sim_visc)
         d.sim_dt = None
         d.C = _ptr(self.C.coef if C is None else C)

@@ -30,7 +30,7 @@ class _Coef:
 
 
 class BatchDomain:
-    def __init__(self, domains: Sequence["P.Domain"], time_steps=None, order="largest_first"):
+    def __init__(self, domains: Sequence["P.Domain"], time_steps=None, order="largest_first", tile_cells=None):
         _ok = P._check
         _ok(len(domains) > 0, "BatchDomain needs at least one domain")
         d0 = domains[0]
@@ -49,6 +49,7 @@ class BatchDomain:
         else:
             self.order = list(range(n))
         self.num_sims = n
+        self.tile_cells = P.TILE_CELLS if tile_cells is None else int(tile_cells)
         self._pack(time_steps)
 
     # -- Domain-like accessors used by the step engine --
@@ -115,7 +116,9 @@ class BatchDomain:
         self._cell_block = cb.to(dev)
         self._sim_cells = torch.tensor(sim_cells, dtype=torch.int32, device=dev)
         self._sim_blocks = torch.tensor(sim_blocks, dtype=torch.int32, device=dev)
-        self._tiles, self._sim_tiles, self._num_tiles = P.build_tiles(self._host_blocks, len(host), self.num_sims, dev)
+        self._n_host_blocks = len(host)
+        self._tiles, self._sim_tiles, self._num_tiles = P.build_tiles(self._host_blocks, len(host), self.num_sims, dev,
+                                                                      self.tile_cells)
         self._sim_visc = torch.tensor([float(self.domains[i].viscosity.item()) for i in self.order],
                                       dtype=self._dtype, device=dev)
         self.max_sim_cells = max(sim_cells[k + 1] - sim_cells[k] for k in range(self.num_sims))
@@ -141,6 +144,16 @@ class BatchDomain:
             ts = [float(t) for t in time_steps]
             P._check(len(ts) == self.num_sims, "one time step per batched domain")
             self._sim_dt = torch.tensor([ts[i] for i in self.order], dtype=self._dtype, device=self._device)
+        self._desc = self._make_desc()
+
+    def set_tile_cells(self, tile_cells):
+        """Cells per Krylov work tile (1..2048): rebuilds the tile table.  Steppers created before the
+        change must be re-created (their workspace depends on the tile count)."""
+        tile_cells = int(tile_cells)
+        P._check(1 <= tile_cells <= 2048, "tile_cells must be in [1, 2048]")
+        self.tile_cells = tile_cells
+        self._tiles, self._sim_tiles, self._num_tiles = P.build_tiles(self._host_blocks, self._n_host_blocks,
+                                                                      self.num_sims, self._device, tile_cells)
         self._desc = self._make_desc()
 
     def set_viscosities(self, nus):
@@ -173,7 +186,7 @@ class BatchDomain:
         d.tiles = self._tiles.data_ptr()
         d.sim_tiles = self._sim_tiles.data_ptr()
         d.num_tiles = self._num_tiles
-        d.tile_cells = P.TILE_CELLS
+        d.tile_cells = self.tile_cells
         d.sim_viscosity = self._sim_visc.data_ptr()
         d.sim_dt = None if self._sim_dt is None else self._sim_dt.data_ptr()
         d.C = self.C.coef.data_ptr()

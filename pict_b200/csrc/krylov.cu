@@ -43,16 +43,17 @@
 namespace pict {
 
 constexpr int KR_NV = 8;         // values per tile partial
-constexpr int KR_SLOTS = 16;     // tiles per CTA (one warp reduces the system of each slot)
+constexpr int KR_SLOTS = 32;     // tiles per CTA (lane j of warp 0 holds the scalars of slot j)
 constexpr int KR_THREADS = 512;  // threads per CTA
 constexpr int KR_CPT = 4;        // cells per thread per tile: tile_cells <= KR_CPT * KR_THREADS
 constexpr int KR_MAX_TILE = KR_CPT * KR_THREADS;
 
-// ctrl words in the workspace header
-// CTRL_DONE counts finished systems (classic CG / BiCGStab: increments and reads are always separated
-// by a grid barrier).  The single-reduction CG has one barrier per iteration, so completions of
-// iteration i go to CTRL_DONE_PAR + (i & 1) and are read only after the barrier of iteration i+1.
-enum { CTRL_ERR = 0, CTRL_DONE = 1, CTRL_BAR_COUNT = 2, CTRL_BAR_GEN = 3, CTRL_DONE_PAR = 4 };
+// ctrl words in the workspace header (cleared before every launch)
+// CTRL_BAR_COUNT counts barrier arrivals (monotonic).  CTRL_DONE counts finished systems (classic CG /
+// BiCGStab: increments and reads are always separated by a grid barrier).  The single-reduction CG
+// has one barrier per iteration, so completions of iteration i go to CTRL_DONE_PAR + (i & 1) and are
+// read only after the barrier of iteration i+1.
+enum { CTRL_ERR = 0, CTRL_DONE = 1, CTRL_BAR_COUNT = 2, CTRL_DONE_PAR = 4 };
 
 template <typename T>
 struct KArgs {
@@ -85,33 +86,34 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
-// Bounded barrier over all CTAs of the launch (generation counter).
-__device__ bool grid_barrier(int* ctrl) {
+// Bounded barrier over all CTAs of the launch.  The arrival counter is monotonic: barrier number
+// `epoch` (1, 2, ...) is complete once it reaches epoch * gridDim.x, so each CTA issues one atomic and
+// nothing is reset.  After the wait thread 0 also reads the completion counters into s_ctrl
+// ([CTRL_DONE, CTRL_DONE_PAR, CTRL_DONE_PAR + 1]); they stay valid until the next barrier.
+__device__ bool grid_barrier(int* ctrl, unsigned& epoch, int* s_ctrl) {
     __shared__ int s_ok;
     __syncthreads();
-    if (gridDim.x == 1) return *(volatile int*)(ctrl + CTRL_ERR) == 0;
+    ++epoch;
     if (threadIdx.x == 0) {
         int ok = 1;
-        unsigned* count = reinterpret_cast<unsigned*>(ctrl + CTRL_BAR_COUNT);
-        unsigned* gen = reinterpret_cast<unsigned*>(ctrl + CTRL_BAR_GEN);
-        volatile unsigned* vgen = gen;
-        const unsigned g0 = *vgen;
-        __threadfence();
-        const unsigned arrived = atomicAdd(count, 1u);
-        if (arrived == gridDim.x - 1) {
-            atomicExch(count, 0u);
+        if (gridDim.x > 1) {
+            unsigned* count = reinterpret_cast<unsigned*>(ctrl + CTRL_BAR_COUNT);
+            const unsigned target = epoch * gridDim.x;
             __threadfence();
-            atomicAdd(gen, 1u);
-        } else {
+            atomicAdd(count, 1u);
             long long spins = 0;
-            while (*vgen == g0) {
+            while ((int)(*(volatile unsigned*)count - target) < 0) {
                 if (++spins > PICT_SPIN_LIMIT) { ok = 0; atomicExch(ctrl + CTRL_ERR, 1); break; }
-                if (*(volatile int*)(ctrl + CTRL_ERR)) { ok = 0; break; }
-                __nanosleep(32);
+                if ((spins & 63) == 0 && *(volatile int*)(ctrl + CTRL_ERR)) { ok = 0; break; }
+                __nanosleep(16);
             }
+            __threadfence();
         }
-        __threadfence();
-        s_ok = ok;
+        const int err = *(volatile int*)(ctrl + CTRL_ERR);
+        s_ctrl[0] = *(volatile int*)(ctrl + CTRL_DONE);
+        s_ctrl[1] = *(volatile int*)(ctrl + CTRL_DONE_PAR);
+        s_ctrl[2] = *(volatile int*)(ctrl + CTRL_DONE_PAR + 1);
+        s_ok = ok && err == 0;
     }
     __syncthreads();
     return s_ok != 0;
@@ -171,6 +173,7 @@ struct TileSlots {
     int t0[KR_SLOTS];            // tile range of the slot's system
     int t1[KR_SLOTS];
     int owner[KR_SLOTS];         // 1 if this slot holds the first tile of its system
+    int ncell[KR_SLOTS];         // cells of the slot's system
 };
 
 __device__ void load_slots(const pict_domain_t& dom, TileSlots& S) {
@@ -189,6 +192,7 @@ __device__ void load_slots(const pict_domain_t& dom, TileSlots& S) {
         S.t0[j] = dom.sim_tiles[tt[0]];
         S.t1[j] = dom.sim_tiles[tt[0] + 1];
         S.owner[j] = (t == S.t0[j]);
+        S.ncell[j] = dom.sim_cells[tt[0] + 1] - dom.sim_cells[tt[0]];
     }
     __syncthreads();
 }
@@ -197,19 +201,20 @@ __device__ void load_slots(const pict_domain_t& dom, TileSlots& S) {
 // Only slots whose bit is set in `mask` are reduced.
 template <int NV>
 __device__ void system_sums(const double* partials, const TileSlots& S, unsigned mask, double (*out)[KR_NV]) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (warp < S.n && (mask & (1u << warp))) {
+    const int lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    for (int j = threadIdx.x >> 5; j < S.n; j += nwarps) {
+        if (!(mask & (1u << j))) continue;
         double acc[NV];
 #pragma unroll
         for (int k = 0; k < NV; ++k) acc[k] = 0.0;
-        for (int t = S.t0[warp] + lane; t < S.t1[warp]; t += 32) {
+        for (int t = S.t0[j] + lane; t < S.t1[j]; t += 32) {
 #pragma unroll
             for (int k = 0; k < NV; ++k) acc[k] += __ldcg(partials + (size_t)t * KR_NV + k);
         }
 #pragma unroll
         for (int k = 0; k < NV; ++k) {
             const double s = warp_sum(acc[k]);
-            if (lane == 0) out[warp][k] = s;
+            if (lane == 0) out[j][k] = s;
         }
     }
     __syncthreads();
@@ -260,8 +265,6 @@ __device__ __forceinline__ double conv_crit(double sq, int normalized, int n) {
     return normalized ? nrm / sqrt((double)n) : nrm;
 }
 
-__device__ __forceinline__ int done_count(const int* ctrl) { return *(volatile const int*)(ctrl + CTRL_DONE); }
-
 __device__ __forceinline__ pict_solve_info_t fresh_info() {
     pict_solve_info_t inf;
     inf.final_residual = 0.0;
@@ -286,6 +289,8 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg(KArgs<T> a) {
     __shared__ unsigned s_active;  // bit per slot
     __shared__ pict_solve_info_t s_info[KR_SLOTS];
     load_slots(dom, S);
+    __shared__ int s_ctrl[3];
+    unsigned epoch = 0;
     const T* __restrict__ coef = a.coef;
     const T* __restrict__ bv = a.b;
     T* __restrict__ x = a.x;
@@ -316,12 +321,13 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg(KArgs<T> a) {
         warp_partial<2>(R, j, acc);
     }
     flush_partials<2>(R, S, 0xffffffffu, part + phase * pstride);
-    if (!grid_barrier(a.ctrl)) return;
+    if (!grid_barrier(a.ctrl, epoch, s_ctrl)) return;
     system_sums<2>(part + phase * pstride, S, 0xffffffffu, s_sum);
     phase ^= 1;
-    if (threadIdx.x == 0) {
-        unsigned act = 0;
-        for (int j = 0; j < S.n; ++j) {
+    if (threadIdx.x < 32) {  // lane j: slot j
+        const int j = threadIdx.x;
+        bool act = false;
+        if (j < S.n) {
             pict_solve_info_t inf = fresh_info();
             s_rho[j] = s_sum[j][0];
             s_beta[j] = 0.0;
@@ -330,11 +336,12 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg(KArgs<T> a) {
                 inf.used_iterations = 0;
                 if (S.owner[j]) atomicAdd(a.ctrl + CTRL_DONE, 1);
             } else {
-                act |= 1u << j;
+                act = true;
             }
             s_info[j] = inf;
         }
-        s_active = act;
+        const unsigned m = __ballot_sync(0xffffffffu, act);
+        if (j == 0) s_active = m;
     }
     __syncthreads();
     // x = 0 where the iteration starts from zero or the right-hand side vanishes
@@ -374,8 +381,8 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg(KArgs<T> a) {
             warp_partial<1>(R, j, acc);
         }
         flush_partials<1>(R, S, s_active, part + phase * pstride);
-        if (!grid_barrier(a.ctrl)) return;
-        if (done_count(a.ctrl) == dom.num_sims) break;
+        if (!grid_barrier(a.ctrl, epoch, s_ctrl)) return;
+        if (s_ctrl[0] == dom.num_sims) break;
         system_sums<1>(part + phase * pstride, S, s_active, s_sum);
         phase ^= 1;
         if ((int)threadIdx.x < S.n && ((s_active >> threadIdx.x) & 1u))
@@ -400,16 +407,15 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg(KArgs<T> a) {
             warp_partial<1>(R, j, acc);
         }
         flush_partials<1>(R, S, s_active, part + phase * pstride);
-        if (!grid_barrier(a.ctrl)) return;
+        if (!grid_barrier(a.ctrl, epoch, s_ctrl)) return;
         system_sums<1>(part + phase * pstride, S, s_active, s_sum);
         phase ^= 1;
-        if (threadIdx.x == 0) {
-            unsigned act = s_active;
-            for (int j = 0; j < S.n; ++j) {
-                if (!((act >> j) & 1u)) continue;
+        if (threadIdx.x < 32) {
+            const int j = threadIdx.x;
+            bool act = j < S.n && ((s_active >> j) & 1u);
+            if (act) {
                 const double rr = s_sum[j][0];
-                const int n = dom.sim_cells[S.sim[j] + 1] - dom.sim_cells[S.sim[j]];
-                const double crit = conv_crit(rr, a.normalized, n);
+                const double crit = conv_crit(rr, a.normalized, S.ncell[j]);
                 s_info[j].used_iterations = it;
                 s_info[j].final_residual = crit;
                 bool fin = false;
@@ -420,11 +426,12 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg(KArgs<T> a) {
                     s_rho[j] = rr;
                 }
                 if (fin) {
-                    act &= ~(1u << j);
+                    act = false;
                     if (S.owner[j]) atomicAdd(a.ctrl + CTRL_DONE, 1);
                 }
             }
-            s_active = act;
+            const unsigned m = __ballot_sync(0xffffffffu, act);
+            if (j == 0) s_active = m;
         }
         __syncthreads();
         T* tmp = pc; pc = pn; pn = tmp;
@@ -438,13 +445,13 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg(KArgs<T> a) {
                 warp_partial<1>(R, j, acc);
             }
             flush_partials<1>(R, S, 0xffffffffu, part + phase * pstride);
-            if (!grid_barrier(a.ctrl)) return;
+            if (!grid_barrier(a.ctrl, epoch, s_ctrl)) return;
             system_sums<1>(part + phase * pstride, S, 0xffffffffu, s_sum);
             phase ^= 1;
         }
         for (int j = 0; j < S.n; ++j) {
             const pict_block_t& B = dom.blocks[S.block[j]];
-            const int n = dom.sim_cells[S.sim[j] + 1] - dom.sim_cells[S.sim[j]];
+            const int n = S.ncell[j];
             const T mean = a.sub_mean ? (T)(s_sum[j][0] / (double)n) : T(0);
             T* pb = reinterpret_cast<T*>(B.pressure);
             for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) {
@@ -477,6 +484,8 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg1(KArgs<T> a) {
     __shared__ unsigned s_active;
     __shared__ pict_solve_info_t s_info[KR_SLOTS];
     load_slots(dom, S);
+    __shared__ int s_ctrl[3];
+    unsigned epoch = 0;
     const T* __restrict__ coef = a.coef;
     const T* __restrict__ bv = a.b;
     T* __restrict__ x = a.x;
@@ -501,7 +510,7 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg1(KArgs<T> a) {
                 rc[i] = bv[i] - spmv_row<T, D, TRANS>(dom, coef, N, i, B, q, [&](int jj) { return x[jj]; });
             }
         }
-        if (!grid_barrier(a.ctrl)) return;
+        if (!grid_barrier(a.ctrl, epoch, s_ctrl)) return;
     }
     const T* r0 = a.x_zero ? bv : rc;
     for (int j = 0; j < S.n; ++j) {
@@ -524,12 +533,13 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg1(KArgs<T> a) {
         warp_partial<3>(R, j, acc);
     }
     flush_partials<3>(R, S, 0xffffffffu, part + phase * pstride);
-    if (!grid_barrier(a.ctrl)) return;
+    if (!grid_barrier(a.ctrl, epoch, s_ctrl)) return;
     system_sums<3>(part + phase * pstride, S, 0xffffffffu, s_sum);
     phase ^= 1;
-    if (threadIdx.x == 0) {
-        unsigned act = 0;
-        for (int j = 0; j < S.n; ++j) {
+    if (threadIdx.x < 32) {  // lane j: slot j
+        const int j = threadIdx.x;
+        bool act = false;
+        if (j < S.n) {
             pict_solve_info_t inf = fresh_info();
             s_g[j] = s_sum[j][0];
             s_alpha[j] = s_sum[j][0] / s_sum[j][1];
@@ -539,11 +549,12 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg1(KArgs<T> a) {
                 inf.used_iterations = 0;
                 if (S.owner[j]) atomicAdd(a.ctrl + CTRL_DONE_PAR + 1, 1);  // iteration -1
             } else {
-                act |= 1u << j;
+                act = true;
             }
             s_info[j] = inf;
         }
-        s_active = act;
+        const unsigned m = __ballot_sync(0xffffffffu, act);
+        if (j == 0) s_active = m;
     }
     __syncthreads();
     for (int j = 0; j < S.n; ++j) {
@@ -589,19 +600,18 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg1(KArgs<T> a) {
             warp_partial<2>(R, j, acc);
         }
         flush_partials<2>(R, S, s_active, part + phase * pstride);
-        if (!grid_barrier(a.ctrl)) return;
+        if (!grid_barrier(a.ctrl, epoch, s_ctrl)) return;
         // completions of iteration it-1 are complete and stable here (see CTRL_DONE_PAR)
-        cum[(it - 1) & 1] = *(volatile const int*)(a.ctrl + CTRL_DONE_PAR + ((it - 1) & 1));
+        cum[(it - 1) & 1] = s_ctrl[1 + ((it - 1) & 1)];
         if (cum[0] + cum[1] == dom.num_sims) break;
         system_sums<2>(part + phase * pstride, S, s_active, s_sum);
         phase ^= 1;
-        if (threadIdx.x == 0) {
-            unsigned act = s_active;
-            for (int j = 0; j < S.n; ++j) {
-                if (!((act >> j) & 1u)) continue;
+        if (threadIdx.x < 32) {
+            const int j = threadIdx.x;
+            bool act = j < S.n && ((s_active >> j) & 1u);
+            if (act) {
                 const double g = s_sum[j][0], d = s_sum[j][1];
-                const int n = dom.sim_cells[S.sim[j] + 1] - dom.sim_cells[S.sim[j]];
-                const double crit = conv_crit(g, a.normalized, n);
+                const double crit = conv_crit(g, a.normalized, S.ncell[j]);
                 s_info[j].used_iterations = it;
                 s_info[j].final_residual = crit;
                 bool fin = false;
@@ -614,11 +624,12 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg1(KArgs<T> a) {
                     s_g[j] = g;
                 }
                 if (fin) {
-                    act &= ~(1u << j);
+                    act = false;
                     if (S.owner[j]) atomicAdd(a.ctrl + CTRL_DONE_PAR + (it & 1), 1);
                 }
             }
-            s_active = act;
+            const unsigned m = __ballot_sync(0xffffffffu, act);
+            if (j == 0) s_active = m;
         }
         __syncthreads();
         T* t0 = rc; rc = rn; rn = t0;
@@ -633,13 +644,13 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg1(KArgs<T> a) {
                 warp_partial<1>(R, j, acc);
             }
             flush_partials<1>(R, S, 0xffffffffu, part + phase * pstride);
-            if (!grid_barrier(a.ctrl)) return;
+            if (!grid_barrier(a.ctrl, epoch, s_ctrl)) return;
             system_sums<1>(part + phase * pstride, S, 0xffffffffu, s_sum);
             phase ^= 1;
         }
         for (int j = 0; j < S.n; ++j) {
             const pict_block_t& B = dom.blocks[S.block[j]];
-            const int n = dom.sim_cells[S.sim[j] + 1] - dom.sim_cells[S.sim[j]];
+            const int n = S.ncell[j];
             const T mean = a.sub_mean ? (T)(s_sum[j][0] / (double)n) : T(0);
             T* pb = reinterpret_cast<T*>(B.pressure);
             for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) {
@@ -669,6 +680,8 @@ __global__ void __launch_bounds__(KR_THREADS) k_bicgstab(KArgs<T> a) {
     __shared__ unsigned s_any;            // bit per slot with an active component
     __shared__ pict_solve_info_t s_info[KR_SLOTS][NR];
     load_slots(dom, S);
+    __shared__ int s_ctrl[3];
+    unsigned epoch = 0;
     const T* __restrict__ coef = a.coef;
     T* __restrict__ x = a.x;
     T* __restrict__ r = a.r;
@@ -709,14 +722,14 @@ __global__ void __launch_bounds__(KR_THREADS) k_bicgstab(KArgs<T> a) {
         warp_partial<2 * NR>(R, j, acc);
     }
     flush_partials<2 * NR>(R, S, 0xffffffffu, part + phase * pstride);
-    if (!grid_barrier(a.ctrl)) return;
+    if (!grid_barrier(a.ctrl, epoch, s_ctrl)) return;
     system_sums<2 * NR>(part + phase * pstride, S, 0xffffffffu, s_sum);
     phase ^= 1;
-    if (threadIdx.x == 0) {
-        unsigned any = 0;
-        for (int j = 0; j < S.n; ++j) {
-            unsigned act = 0;
-            const int n = dom.sim_cells[S.sim[j] + 1] - dom.sim_cells[S.sim[j]];
+    if (threadIdx.x < 32) {  // lane j: slot j
+        const int j = threadIdx.x;
+        unsigned act = 0;
+        if (j < S.n) {
+            const int n = S.ncell[j];
             for (int c = 0; c < NR; ++c) {
                 pict_solve_info_t inf = fresh_info();
                 s_rho[j][c] = 0.0; s_alpha[j][c] = 0.0; s_omega[j][c] = 0.0; s_beta[j][c] = 0.0;
@@ -741,9 +754,9 @@ __global__ void __launch_bounds__(KR_THREADS) k_bicgstab(KArgs<T> a) {
                 s_info[j][c] = inf;
             }
             s_act[j] = act;
-            if (act) any |= 1u << j;
         }
-        s_any = any;
+        const unsigned m = __ballot_sync(0xffffffffu, act != 0);
+        if (j == 0) s_any = m;
     }
     __syncthreads();
     // x = 0 where the iteration starts from zero or the right-hand side vanishes
@@ -795,8 +808,8 @@ __global__ void __launch_bounds__(KR_THREADS) k_bicgstab(KArgs<T> a) {
             warp_partial<NR>(R, j, acc);
         }
         flush_partials<NR>(R, S, s_any, part + phase * pstride);
-        if (!grid_barrier(a.ctrl)) return;
-        if (done_count(a.ctrl) == total) break;
+        if (!grid_barrier(a.ctrl, epoch, s_ctrl)) return;
+        if (s_ctrl[0] == total) break;
         system_sums<NR>(part + phase * pstride, S, s_any, s_sum);
         phase ^= 1;
         if ((int)threadIdx.x < S.n) {
@@ -826,14 +839,14 @@ __global__ void __launch_bounds__(KR_THREADS) k_bicgstab(KArgs<T> a) {
             warp_partial<NR>(R, j, acc);
         }
         flush_partials<NR>(R, S, s_any, part + phase * pstride);
-        if (!grid_barrier(a.ctrl)) return;
+        if (!grid_barrier(a.ctrl, epoch, s_ctrl)) return;
         system_sums<NR>(part + phase * pstride, S, s_any, s_sum);
         phase ^= 1;
-        if (threadIdx.x == 0) {
-            unsigned any = 0;
-            for (int j = 0; j < S.n; ++j) {
-                unsigned act = s_act[j];
-                const int n = dom.sim_cells[S.sim[j] + 1] - dom.sim_cells[S.sim[j]];
+        if (threadIdx.x < 32) {
+            const int j = threadIdx.x;
+            unsigned act = j < S.n ? s_act[j] : 0u;
+            if (act) {
+                const int n = S.ncell[j];
                 for (int c = 0; c < NR; ++c) {
                     if (!((act >> c) & 1u)) continue;
                     const double nr = conv_crit(s_sum[j][c], a.normalized, n);
@@ -848,9 +861,9 @@ __global__ void __launch_bounds__(KR_THREADS) k_bicgstab(KArgs<T> a) {
                     }
                 }
                 s_act[j] = act;
-                if (act) any |= 1u << j;
             }
-            s_any = any;
+            const unsigned m = __ballot_sync(0xffffffffu, act != 0);
+            if (j == 0) s_any = m;
         }
         __syncthreads();
         // phase C: t = A s, t.s, t.t
@@ -877,7 +890,7 @@ __global__ void __launch_bounds__(KR_THREADS) k_bicgstab(KArgs<T> a) {
             warp_partial<2 * NR>(R, j, acc);
         }
         flush_partials<2 * NR>(R, S, s_any, part + phase * pstride);
-        if (!grid_barrier(a.ctrl)) return;
+        if (!grid_barrier(a.ctrl, epoch, s_ctrl)) return;
         system_sums<2 * NR>(part + phase * pstride, S, s_any, s_sum);
         phase ^= 1;
         if ((int)threadIdx.x < S.n) {
@@ -909,14 +922,14 @@ __global__ void __launch_bounds__(KR_THREADS) k_bicgstab(KArgs<T> a) {
             warp_partial<2 * NR>(R, j, acc);
         }
         flush_partials<2 * NR>(R, S, s_any, part + phase * pstride);
-        if (!grid_barrier(a.ctrl)) return;
+        if (!grid_barrier(a.ctrl, epoch, s_ctrl)) return;
         system_sums<2 * NR>(part + phase * pstride, S, s_any, s_sum);
         phase ^= 1;
-        if (threadIdx.x == 0) {
-            unsigned any = 0;
-            for (int j = 0; j < S.n; ++j) {
-                unsigned act = s_act[j];
-                const int n = dom.sim_cells[S.sim[j] + 1] - dom.sim_cells[S.sim[j]];
+        if (threadIdx.x < 32) {
+            const int j = threadIdx.x;
+            unsigned act = j < S.n ? s_act[j] : 0u;
+            if (act) {
+                const int n = S.ncell[j];
                 for (int c = 0; c < NR; ++c) {
                     if (!((act >> c) & 1u)) continue;
                     s_rwr[j][c] = s_sum[j][2 * c + 1];
@@ -930,9 +943,9 @@ __global__ void __launch_bounds__(KR_THREADS) k_bicgstab(KArgs<T> a) {
                     }
                 }
                 s_act[j] = act;
-                if (act) any |= 1u << j;
             }
-            s_any = any;
+            const unsigned m = __ballot_sync(0xffffffffu, act != 0);
+            if (j == 0) s_any = m;
         }
         __syncthreads();
         T* tp = pc; pc = pn; pn = tp;
