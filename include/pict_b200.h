@@ -225,6 +225,52 @@ int64_t pict_solve_static_scratch_bytes(void);
 pict_status_t pict_solve_static(const pict_domain_t* dom, const void* coef, const void* rhs, void* x,
                                 const pict_solve_params_t* params, void* info_out, void* stream);
 
+/* ---------------- adjoint (reverse mode) of the orthogonal step ----------------
+ * Gather-form adjoints of the forward operators (no atomics, deterministic).  They read the forward
+ * quantities from explicit global vectors (a per-step tape) and accumulate into global vectors:
+ * velocity_grad [D][N] (velocity at the start of the step), viscosity_grad [N] (per cell),
+ * source_grad [D][N] (NULL: not needed), boundary_velocity_grad [2D][D][N] (per fixed face and
+ * adjacent cell).  pict_adjoint_to_blocks() maps them onto the blocks' gradient tensors.
+ * Replace the *_GRAD kernels behind PISOtorch_diff (extensions/PISO_multiblock_cuda_kernel.cu:3869-4077,
+ * 4388-4478, 4967-5117, 5243-5371, 5423-5453, 6224-6293). */
+
+/* CorrectVelocityGrad (PISOtorch_diff.py:1160-1236, FD version): h_grad = u_grad,
+ * A_grad += u_grad.g/A^2, pressure_grad = -G^T(u_grad/A) (pressure: [N], the corrector's solution). */
+pict_status_t pict_correct_velocity_grad(const pict_domain_t* dom, const void* A, const void* pressure,
+                                         const void* velocity_result_grad, void* A_grad, void* pressure_grad,
+                                         void* pressure_rhs_grad, void* stream);
+/* x -= mean(x) per system (adjoint of the pressure mean removal, PISOtorch_simulation.py:1286-1287). */
+pict_status_t pict_sim_mean_project(const pict_domain_t* dom, void* x, void* stream);
+/* SetupPressureRHSdiv gradient (PISOtorch_diff.py:1067-1158): pressure_rhs_grad += Dv^T div_grad,
+ * boundary_velocity_grad += d div / d boundary velocity. */
+pict_status_t pict_divergence_grad(const pict_domain_t* dom, const void* div_grad, void* pressure_rhs_grad,
+                                   void* boundary_velocity_grad, void* stream);
+/* SetupPressureRHS + SetupPressureMatrix gradients of one corrector (PISOtorch_diff.py:897-1065) with the
+ * pressure solve's matrix gradient -lambda x^T folded in (lambda = P^-T x_grad, x = the solution):
+ * A_grad +=, C_grad (off-diagonal rows) +=, U_grad = (gradient of the velocity used in H/A),
+ * velocity_grad / source_grad / viscosity_grad / boundary_velocity_grad +=. */
+pict_status_t pict_pressure_rhs_grad(const pict_domain_t* dom, double dt, const void* h_grad, const void* h,
+                                     const void* A, const void* C, const void* U, const void* lambda,
+                                     const void* pressure, void* A_grad, void* C_grad, void* U_grad,
+                                     void* velocity_grad, void* source_grad, void* viscosity_grad,
+                                     void* boundary_velocity_grad, void* stream);
+/* SetupAdvectionMatrix + SetupAdvectionVelocity gradients (PISOtorch_diff.py:377-441, 531-613) with the
+ * advection solve's matrix gradient -rhs_grad u*^T folded in (velocity_result: the solution u*). */
+pict_status_t pict_advection_grad(const pict_domain_t* dom, double dt, const void* velocity_result,
+                                  const void* velocity_rhs_grad, const void* C_grad, const void* A_grad,
+                                  void* velocity_grad, void* viscosity_grad, void* boundary_velocity_grad,
+                                  void* source_grad, void* stream);
+/* Accumulators -> gradient tensors of the block table (velocity_grad, viscosity_grad, source_grad, faces'
+ * velocity_grad; static tensors receive the sum) and sim_viscosity_grad [num_sims] for blocks that use
+ * the system viscosity.  block_scratch: device memory of num_blocks doubles. */
+pict_status_t pict_adjoint_to_blocks(const pict_domain_t* dom, const void* velocity_grad, const void* viscosity_grad,
+                                     const void* source_grad, const void* boundary_velocity_grad,
+                                     void* sim_viscosity_grad, void* block_scratch, void* stream);
+/* Copy between a global [ncomp][N] vector and a per-block field (0 velocity, 1 pressure, 2 source,
+ * 3 velocity_grad, 4 pressure_grad, 5 source_grad); accumulate=1 adds instead of overwriting. */
+pict_status_t pict_copy_field(const pict_domain_t* dom, int32_t which, int32_t to_blocks, void* global_vec,
+                              int32_t accumulate, void* stream);
+
 /* ---------------- matrix export / utilities ---------------- */
 /* CSR materialisation of a stencil matrix in the reference's row layout (rows sorted by
  * column, extensions/PISO_multiblock_cuda_kernel.cu:3846-3860).  row_out [N+1] must be computed first by pict_csr_row_ptr. */

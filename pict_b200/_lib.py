@@ -153,6 +153,13 @@ SIGNATURES = {
     "pict_solve": (c_i32, [_PD, c_vp, c_vp, c_vp, _PS, c_vp, c_vp, ctypes.c_int64, c_vp]),
     "pict_solve_static_scratch_bytes": (ctypes.c_int64, []),
     "pict_solve_static": (c_i32, [_PD, c_vp, c_vp, c_vp, _PS, c_vp, c_vp]),
+    "pict_correct_velocity_grad": (c_i32, [_PD, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "pict_sim_mean_project": (c_i32, [_PD, c_vp, c_vp]),
+    "pict_divergence_grad": (c_i32, [_PD, c_vp, c_vp, c_vp, c_vp]),
+    "pict_pressure_rhs_grad": (c_i32, [_PD, ctypes.c_double] + [c_vp] * 15),
+    "pict_advection_grad": (c_i32, [_PD, ctypes.c_double] + [c_vp] * 9),
+    "pict_adjoint_to_blocks": (c_i32, [_PD] + [c_vp] * 7),
+    "pict_copy_field": (c_i32, [_PD, c_i32, c_i32, c_vp, c_i32, c_vp]),
     "pict_csr_row_ptr": (c_i32, [_PD, c_vp, c_vp]),
     "pict_stencil_to_csr": (c_i32, [_PD, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "pict_csr_to_stencil": (c_i32, [_PD, c_vp, c_vp, c_vp, c_vp, c_vp]),

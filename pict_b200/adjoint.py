@@ -1,0 +1,318 @@
+"""Reverse mode of the fused PISO step: taped forward steps, the adjoint step, and a checkpointed
+rollout behind ``torch.autograd.Function``.
+
+The reference differentiates a step operator by operator through ``PISOtorch_diff`` (autograd
+Functions around every Setup*/SolveLinear/CorrectVelocity call, PISOtorch_diff.py:295-1236).  Here
+one forward step records a small tape of global vectors and the reverse step runs the adjoint
+operators of ``libpict_b200`` (adjoint.cu) plus two transposed Krylov solves:
+
+    per corrector k = K-1 .. 0:
+        CorrectVelocity^T      -> h_bar, A_bar, p_bar
+        mean removal^T         -> p_bar - mean(p_bar)
+        CG on P^T lambda = p_bar
+        divergence^T, H/A^T, P(A)^T (with -lambda x^T)  -> A_bar, C_bar, U_bar, parameter gradients
+    BiCGStab on C^T rhs_bar = u*_bar (all components in one launch)
+    advection^T (with -rhs_bar u*^T)   -> gradient of the step's input velocity and parameters
+
+Gradients with respect to the simulation parameters accumulate over all steps: per-cell viscosity
+(reduced to the system / block viscosity), velocity source, boundary velocity of fixed faces.
+
+``rollout()`` keeps only every ``checkpoint_every``-th velocity during the forward pass and, in the
+backward pass, recomputes each window from its checkpoint with taping before reversing it.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Dict, List, Optional, Sequence
+
+import torch
+
+from . import _lib
+from ._lib import check
+from . import PISOtorch as P
+from .engine import PISOStepper, LinsolveError
+
+FIELD_VELOCITY, FIELD_PRESSURE, FIELD_SOURCE, FIELD_VELOCITY_GRAD, FIELD_PRESSURE_GRAD, FIELD_SOURCE_GRAD = range(6)
+
+
+def _p(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+class StepTape:
+    """Forward quantities of one PISO step needed by its adjoint (global layouts)."""
+
+    def __init__(self, N, D, K, correctors, dtype, device):
+        z = lambda *s: torch.empty(*s, dtype=dtype, device=device)
+        self.un = z(D * N)         # velocity at the start of the step
+        self.C = z(K * N)          # advection matrix (stencil)
+        self.A = z(N)              # its diagonal
+        self.ustar = z(D * N)      # advection solve result
+        self.h = [z(D * N) for _ in range(correctors)]   # H/A per corrector
+        self.p = [z(N) for _ in range(correctors)]       # pressure solution per corrector
+        self.U = [None] + [z(D * N) for _ in range(correctors - 1)]  # velocity used in H/A (k >= 1)
+
+
+class PISOAdjoint:
+    """Taped forward steps and adjoint steps of a :class:`PISOStepper` (same domain and settings).
+
+    ``adjoint_advection_tol`` / ``adjoint_pressure_tol`` default to the forward tolerances.
+    """
+
+    def __init__(self, stepper: PISOStepper, adjoint_advection_tol: Optional[float] = None,
+                 adjoint_pressure_tol: Optional[float] = None):
+        self.st = stepper
+        d = stepper.domain
+        P._check(stepper.normalize_pressure, "the adjoint needs normalize_pressure=True (mean-free pressure)")
+        self.dom = d
+        self.lib = stepper.lib
+        self.D = stepper.dims
+        self.K = 2 * self.D + 1
+        self.N = d.getTotalSize()
+        self.dtype = d.getDtype()
+        self.dev = d.getDevice()
+        self.ns = stepper.desc.num_sims
+        self.nc = stepper.corrector_steps
+        P._check(self.nc >= 1, "the adjoint needs at least one corrector")
+        atol = stepper.adv_tol if adjoint_advection_tol is None else float(adjoint_advection_tol)
+        ptol = stepper.p_tol if adjoint_pressure_tol is None else float(adjoint_pressure_tol)
+        ap, pp = stepper.adv_params, stepper.p_params
+        self.adv_params = P._solve_params(self.D, stepper.max_iterations, atol, _lib.PICT_CONV_NORM2_NORMALIZED, True,
+                                          True, x_zero=True, group_size=ap.group_size)
+        self.p_params = P._solve_params(1, stepper.max_iterations, ptol, _lib.PICT_CONV_NORM2_NORMALIZED, False, True,
+                                        x_zero=True, group_size=pp.group_size, variant=pp.variant)
+        N, D, K = self.N, self.D, self.K
+        z = lambda n: torch.zeros(n, dtype=self.dtype, device=self.dev)
+        # per-step work
+        self.Abar, self.Cbar, self.hbar, self.pbar, self.lam = z(N), z(K * N), z(D * N), z(N), z(N)
+        self.Ubar, self.rhsbar, self.unbar = z(D * N), z(D * N), z(D * N)
+        self.Pwork = z(K * N)
+        # parameter accumulators (whole rollout)
+        self.nubar = z(N)
+        self.srcbar = z(D * N)
+        self.vbbar = z(2 * D * D * N)
+        self.info = torch.zeros((D + 1) * self.ns * _lib.SOLVE_INFO_BYTES, dtype=torch.uint8, device=self.dev)
+        self.block_scratch = torch.zeros(max(1, len(d.getBlocks())), dtype=torch.float64, device=self.dev)
+        self.sim_nu_bar = z(self.ns)
+
+    # ------------------------------------------------------------------ state helpers
+    def _stream(self):
+        return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def _desc(self, A=None, C=None, Pm=None):
+        """A copy of the stepper's descriptor with matrix pointers replaced."""
+        src = self.st.domain._desc
+        dsc = _lib.DomainDesc()
+        ctypes.memmove(ctypes.byref(dsc), ctypes.byref(src), ctypes.sizeof(dsc))
+        if A is not None:
+            dsc.A = A.data_ptr()
+        if C is not None:
+            dsc.C = C.data_ptr()
+        if Pm is not None:
+            dsc.P = Pm.data_ptr()
+        return dsc
+
+    def velocity(self, out=None):
+        """The blocks' velocity as a global [D*N] vector."""
+        out = torch.empty(self.D * self.N, dtype=self.dtype, device=self.dev) if out is None else out
+        check(self.lib.pict_copy_field(ctypes.byref(self.st.domain._desc), FIELD_VELOCITY, 0, _p(out), 0,
+                                       self._stream()), "copy velocity")
+        return out
+
+    def set_velocity(self, u):
+        u = u.contiguous()
+        check(self.lib.pict_copy_field(ctypes.byref(self.st.domain._desc), FIELD_VELOCITY, 1, _p(u), 0,
+                                       self._stream()), "set velocity")
+
+    def pressure(self, out=None):
+        """The blocks' pressure as a global [N] vector."""
+        out = torch.empty(self.N, dtype=self.dtype, device=self.dev) if out is None else out
+        check(self.lib.pict_copy_field(ctypes.byref(self.st.domain._desc), FIELD_PRESSURE, 0, _p(out), 0,
+                                       self._stream()), "copy pressure")
+        return out
+
+    def set_pressure(self, p):
+        p = p.contiguous()
+        check(self.lib.pict_copy_field(ctypes.byref(self.st.domain._desc), FIELD_PRESSURE, 1, _p(p), 0,
+                                       self._stream()), "set pressure")
+
+    def set_source(self, src):
+        src = src.contiguous()
+        check(self.lib.pict_copy_field(ctypes.byref(self.st.domain._desc), FIELD_SOURCE, 1, _p(src), 0,
+                                       self._stream()), "set source")
+
+    def zero_parameter_grads(self):
+        self.nubar.zero_()
+        self.srcbar.zero_()
+        self.vbbar.zero_()
+
+    # ------------------------------------------------------------------ forward with tape
+    def new_tape(self):
+        return StepTape(self.N, self.D, self.K, self.nc, self.dtype, self.dev)
+
+    def step_taped(self, tape: StepTape, time_step=None):
+        st = self.st
+        d = st.domain
+        lib = self.lib
+        desc = ctypes.byref(d._desc)
+        s = self._stream()
+        dt = st._dt(time_step)
+        self.velocity(tape.un)
+        check(lib.pict_setup_advection(desc, dt, s), "advection setup")
+        tape.C.copy_(d.C.coef.reshape(-1))
+        tape.A.copy_(d.A)
+        check(lib.pict_solve(desc, P._ptr(d.C.coef), P._ptr(d.velocityRHS), P._ptr(d.velocityResult),
+                             ctypes.byref(st.adv_params), P._ptr(st.info_adv), P._ptr(st.ws), st.ws_bytes, s),
+              "advection solve")
+        tape.ustar.copy_(d.velocityResult)
+        for k in range(self.nc):
+            if k > 0:
+                tape.U[k].copy_(d.velocityResult)
+            if k == 0:
+                check(lib.pict_setup_pressure_correction(desc, dt, 0, 0, s), "pressure setup")
+            else:
+                check(lib.pict_setup_pressure_rhs(desc, dt, 0, 0, s), "pressure rhs")
+            tape.h[k].copy_(d.pressureRHS)
+            check(lib.pict_solve(desc, P._ptr(d.P.coef), P._ptr(d.pressureRHSdiv), P._ptr(d.pressureResult),
+                                 ctypes.byref(st.p_params), P._ptr(st.info_p[k]), P._ptr(st.ws), st.ws_bytes, s),
+                  "pressure solve")
+            tape.p[k].copy_(d.pressureResult)
+            last = k == self.nc - 1
+            check(lib.pict_correct_velocity(desc, dt, 1, 0, 1 if last else 0, s), "velocity correction")
+
+    # ------------------------------------------------------------------ adjoint step
+    def backward_step(self, tape: StepTape, ubar, pbar_out=None, time_step=None):
+        """Reverse one step: ubar = dL/du^{n+1} [D*N] (and dL/dp^{n+1} [N]); returns dL/du^n [D*N].
+        Parameter gradients accumulate into nubar / srcbar / vbbar."""
+        st = self.st
+        lib = self.lib
+        s = self._stream()
+        dt = st._dt(time_step)
+        dsc = self._desc(A=tape.A, C=tape.C, Pm=self.Pwork)
+        desc = ctypes.byref(dsc)
+        self.Abar.zero_()
+        self.Cbar.zero_()
+        self.unbar.zero_()
+        check(lib.pict_setup_pressure_matrix(desc, 0, s), "adjoint pressure matrix")
+        ucur = ubar.contiguous()
+        info_p = self.info[self.D * self.ns * _lib.SOLVE_INFO_BYTES:]
+        info_a = self.info[:self.D * self.ns * _lib.SOLVE_INFO_BYTES]
+        src = _p(self.srcbar)
+        for k in reversed(range(self.nc)):
+            check(lib.pict_correct_velocity_grad(desc, _p(tape.A), _p(tape.p[k]), _p(ucur), _p(self.Abar),
+                                                 _p(self.pbar), _p(self.hbar), s), "correct velocity grad")
+            if k == self.nc - 1 and pbar_out is not None:
+                self.pbar.add_(pbar_out)
+            check(lib.pict_sim_mean_project(desc, _p(self.pbar), s), "mean projection")
+            self.lam.zero_()
+            check(lib.pict_solve(desc, _p(self.Pwork), _p(self.pbar), _p(self.lam), ctypes.byref(self.p_params),
+                                 _p(info_p), P._ptr(st.ws), st.ws_bytes, s), "adjoint pressure solve")
+            self._check_info(info_p, "adjoint pressure")
+            check(lib.pict_divergence_grad(desc, _p(self.lam), _p(self.hbar), _p(self.vbbar), s), "divergence grad")
+            U = tape.ustar if k == 0 else tape.U[k]
+            check(lib.pict_pressure_rhs_grad(desc, dt, _p(self.hbar), _p(tape.h[k]), _p(tape.A), _p(tape.C), _p(U),
+                                             _p(self.lam), _p(tape.p[k]), _p(self.Abar), _p(self.Cbar),
+                                             _p(self.Ubar), _p(self.unbar), src, _p(self.nubar), _p(self.vbbar), s),
+                  "pressure rhs grad")
+            ucur = self.Ubar.clone() if k > 0 else self.Ubar
+        # advection solve (transposed, all components) and assembly
+        self.rhsbar.zero_()
+        check(lib.pict_solve(desc, _p(tape.C), _p(self.Ubar), _p(self.rhsbar), ctypes.byref(self.adv_params),
+                             _p(info_a), P._ptr(st.ws), st.ws_bytes, s), "adjoint advection solve")
+        self._check_info(info_a, "adjoint advection")
+        check(lib.pict_advection_grad(desc, dt, _p(tape.ustar), _p(self.rhsbar), _p(self.Cbar), _p(self.Abar),
+                                      _p(self.unbar), _p(self.nubar), _p(self.vbbar), src, s), "advection grad")
+        return self.unbar.clone()
+
+    def _check_info(self, info, what):
+        if not getattr(self, "check_solves", False):
+            return
+        for i, inf in enumerate(P.decode_infos(info)):
+            if getattr(inf, "status", 0) == 1 or not inf.isFiniteResidual or not inf.converged:
+                raise LinsolveError("%s solve %d failed: %s" % (what, i, inf))
+
+    def parameter_grads_to_blocks(self):
+        """Add the accumulated parameter gradients to the blocks' / boundaries' gradient tensors (those
+        that are set) and return the gradient of the system viscosities [num_sims]."""
+        self.sim_nu_bar.zero_()
+        check(self.lib.pict_adjoint_to_blocks(ctypes.byref(self.st.domain._desc), None, _p(self.nubar), _p(self.srcbar),
+                                              _p(self.vbbar), _p(self.sim_nu_bar), _p(self.block_scratch),
+                                              self._stream()), "adjoint to blocks")
+        return self.sim_nu_bar
+
+
+# ---------------------------------------------------------------------------------------------
+# checkpointed rollout
+# ---------------------------------------------------------------------------------------------
+
+class _Rollout(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, adj, steps, record, checkpoint_every, u0, nu, src):
+        st = adj.st
+        dom = st.domain
+        if nu is not None:
+            dom._sim_visc.copy_(nu.detach())
+        if src is not None:
+            adj.set_source(src.detach())
+        adj.set_velocity(u0.detach())
+        ckpt = {0: u0.detach().clone()}
+        outs = []
+        rec = sorted(set(int(r) for r in record))
+        for t in range(1, steps + 1):
+            st.step()
+            if t % checkpoint_every == 0 and t < steps:
+                ckpt[t] = adj.velocity()
+            if t in rec:
+                outs.append(adj.velocity())
+        if getattr(adj, "check_solves", False):
+            st.check()
+        ctx.final = (adj.velocity(), adj.pressure())
+        ctx.adj = adj
+        ctx.steps = steps
+        ctx.rec = rec
+        ctx.K = checkpoint_every
+        ctx.ckpt = ckpt
+        ctx.has_nu = nu is not None
+        ctx.has_src = src is not None
+        return tuple(outs)
+
+    @staticmethod
+    @torch.autograd.function.once_differentiable
+    def backward(ctx, *grads):
+        adj = ctx.adj
+        steps, K, rec = ctx.steps, ctx.K, ctx.rec
+        gmap = {t: g for t, g in zip(rec, grads)}
+        adj.zero_parameter_grads()
+        ubar = torch.zeros(adj.D * adj.N, dtype=adj.dtype, device=adj.dev)
+        tapes = [adj.new_tape() for _ in range(min(K, steps))]
+        starts = list(range(0, steps, K))
+        for w0 in reversed(starts):
+            w1 = min(w0 + K, steps)
+            adj.set_velocity(ctx.ckpt[w0])
+            for t in range(w0, w1):
+                adj.step_taped(tapes[t - w0])
+            for t in reversed(range(w0, w1)):
+                g = gmap.get(t + 1)
+                if g is not None:
+                    ubar = ubar + g.reshape(-1)
+                ubar = adj.backward_step(tapes[t - w0], ubar)
+        # the recomputation moved the domain state; restore the end of the forward pass
+        adj.set_velocity(ctx.final[0])
+        adj.set_pressure(ctx.final[1])
+        nu_sim = adj.parameter_grads_to_blocks()
+        nu_bar = nu_sim.clone() if ctx.has_nu else None
+        src_bar = adj.srcbar.clone() if ctx.has_src else None
+        return None, None, None, None, ubar, nu_bar, src_bar
+
+
+def rollout(adj: PISOAdjoint, u0, steps: int, record: Sequence[int], checkpoint_every: int = 10, nu=None, src=None):
+    """Run `steps` PISO steps from the global velocity u0 [D*N] and return the velocities after the
+    steps listed in `record` (tuple of [D*N] tensors), differentiable with respect to u0, the system
+    viscosities nu [num_sims] (descriptor order) and a per-cell velocity source src [D*N].
+    The forward keeps every `checkpoint_every`-th velocity; the backward recomputes each window.
+    The backward also adds the parameter gradients to the gradient tensors that are allocated on the
+    domain (block viscosityGrad / velocitySourceGrad, boundary velocityGrad), and leaves the domain in
+    the state at the end of the forward pass."""
+    P._check(steps >= 1 and checkpoint_every >= 1, "steps and checkpoint_every must be >= 1")
+    P._check(all(1 <= int(r) <= steps for r in record) and len(record) > 0, "record steps must be in [1, steps]")
+    return _Rollout.apply(adj, int(steps), tuple(record), int(checkpoint_every), u0, nu, src)
