@@ -306,8 +306,16 @@ def run_pict(args, rank, world):
     # end-to-end through the public API with host buffers
     e2e = e2e_pass(st, batch, args, dev, cells, world)
 
-    # accuracy: two smallest simulations, FP32 GPU vs FP64 oracle with tight solves
+    # forward + backward (adjoint) through the checkpointed rollout
+    fb = fwd_bwd_pass(st, batch, args, dev, cells, world) if not args.skip_bwd else None
+
+    # plain: the same step one simulation at a time (single-domain stepper, CUDA graph), sampled
+    plain = plain_pass(wl, args) if (rank == 0 and not args.skip_plain) else None
+
+    # accuracy: two smallest simulations, FP32 GPU vs FP64 oracle with tight solves; adjoint vs FD
     err = accuracy_check(wl, args) if (rank == 0 and not args.skip_err) else None
+    if err is not None and not args.skip_bwd:
+        err["viscosity_grad"] = grad_check(wl)
 
     # CPU baseline (bounded sample, rank 0)
     cpu = None
@@ -333,6 +341,8 @@ def run_pict(args, rank, world):
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "fwd_bwd": fb,
+            "plain": plain,
             "gpu_launches": st.kernels_per_step() * args.steps,
             "err": err,
             "solver_iterations": {"advection_max": int(max(iters_adv)), "advection_mean": float(np.mean(iters_adv)),
@@ -412,6 +422,116 @@ def e2e_pass(st, batch, args, dev, cells, world):
             "d2h_bytes_per_step": h2d, "steps": steps}
 
 
+def fwd_bwd_pass(st, batch, args, dev, cells, world):
+    """Forward + backward of a checkpointed rollout: loss = mean over simulations of the final mean
+    kinetic energy, gradient with respect to the initial velocity and every simulation's viscosity."""
+    import torch
+    from pict_b200.adjoint import PISOAdjoint, rollout
+    adj = PISOAdjoint(st)
+    adj.use_graph = not args.no_graph
+    R, K = args.fb_steps, args.checkpoint
+    D = batch.getSpatialDims()
+    n_s = torch.diff(batch._sim_cells.long()).to(dev)
+    ns = n_s.numel()
+    w = torch.repeat_interleave(1.0 / (ns * n_s.to(batch.getDtype())), n_s).repeat(D)
+    u0 = adj.velocity().clone()
+    nu0 = batch._sim_visc.clone()
+
+    def run():
+        u0r = u0.clone().requires_grad_(True)
+        nur = nu0.clone().requires_grad_(True)
+        out = rollout(adj, u0r, R, [R], checkpoint_every=K, nu=nur)
+        loss = 0.5 * (w * out[0] * out[0]).sum()
+        loss.backward()
+        return nur.grad
+
+    run()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    g = run()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    adj.set_velocity(u0)
+    batch._sim_visc.copy_(nu0)
+    total_cells, ms_max = job_totals(cells, ms, world, dev)
+    return {"value": total_cells * R / (ms_max * 1e-3), "unit": "cell-steps/s", "steps": R, "checkpoint_every": K,
+            "ms": ms_max, "loss": "mean over simulations of the final mean kinetic energy",
+            "grad": "initial velocity and per-simulation viscosity", "grad_finite": bool(torch.isfinite(g).all())}
+
+
+def plain_pass(wl, args, k=8, steps=10):
+    """The plain single-simulation FP32 step (one domain per simulation, CUDA graph) on k simulations
+    at evenly spaced size quantiles, run one after the other: sum(cells x steps) / sum(time)."""
+    import torch
+    from pict_b200.engine import PISOStepper
+    sel = sample_indices(wl["sides"], k)
+    tot_cells, tot_ms = 0, 0.0
+    for i in sel:
+        s = int(wl["sides"][i])
+        d = make_cavity_domain(s, 1.0 / wl["re"][i], torch.float32)
+        stp = PISOStepper(d, time_step=float(wl["dts"][i]), advection_tol=wl["tol"], pressure_tol=wl["tol"])
+        for _ in range(3):
+            stp.step()
+        stp.capture(steps=1)
+        for _ in range(3):
+            stp.replay()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            stp.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        tot_ms += e0.elapsed_time(e1)
+        tot_cells += s * s * steps
+        del stp, d
+    return {"value": tot_cells / (tot_ms * 1e-3), "unit": "cell-steps/s",
+            "sample": "sides %s, %d steps each, one simulation at a time" % ([int(wl["sides"][i]) for i in sel], steps)}
+
+
+def grad_check(wl, steps=3):
+    """Viscosity gradient of the final mean kinetic energy of the two smallest simulations (FP64,
+    solves to 1e-12): adjoint against central finite differences (relative step 1e-4)."""
+    import torch
+    from pict_b200.batch import BatchDomain
+    from pict_b200.engine import PISOStepper
+    from pict_b200.adjoint import PISOAdjoint, rollout
+    order = np.argsort(wl["sides"])[:2]
+    doms = [make_cavity_domain(int(wl["sides"][i]), 1.0 / wl["re"][i], torch.float64) for i in order]
+    b = BatchDomain(doms, time_steps=[wl["dts"][i] for i in order])
+    st = PISOStepper(b, time_step=float(wl["dts"][order[0]]), advection_tol=1e-12, pressure_tol=1e-12)
+    adj = PISOAdjoint(st)
+    n_s = torch.diff(b._sim_cells.long()).cuda()
+    w = torch.repeat_interleave(1.0 / n_s.double(), n_s).repeat(2)
+    u0 = adj.velocity().clone()
+    nu0 = b._sim_visc.clone()
+    nur = nu0.clone().requires_grad_(True)
+    out = rollout(adj, u0.clone(), steps, [steps], nu=nur)
+    (0.5 * (w * out[0] * out[0]).sum()).backward()
+    errs = []
+    for s in range(2):
+        def loss(e):
+            nu = nu0.clone()
+            nu[s] *= 1 + e
+            b._sim_visc.copy_(nu)
+            adj.set_velocity(u0)
+            for _ in range(steps):
+                st.step()
+            st.check()
+            u = adj.velocity()
+            return float(0.5 * (w * u * u).sum())
+        fd = (loss(1e-4) - loss(-1e-4)) / 2e-4
+        ad = float(nur.grad[s] * nu0[s])
+        errs.append(abs(ad - fd) / max(abs(fd), 1e-30))
+    b._sim_visc.copy_(nu0)
+    return {"rel_err_vs_fd_max": max(errs), "sims": [int(wl["sides"][i]) for i in order], "steps": steps,
+            "dtype": "f64"}
+
+
 def accuracy_check(wl, args):
     """Relative error of the FP32 batched step against the FP64 oracle (tight solves) on the two
     smallest simulations after 10 steps."""
@@ -462,6 +582,10 @@ def main():
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-err", action="store_true")
+    ap.add_argument("--skip-bwd", action="store_true")
+    ap.add_argument("--skip-plain", action="store_true")
+    ap.add_argument("--fb-steps", type=int, default=10, help="steps of the forward+backward rollout")
+    ap.add_argument("--checkpoint", type=int, default=5, help="checkpoint interval of the rollout")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", 0))

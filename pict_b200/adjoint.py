@@ -56,7 +56,9 @@ class StepTape:
 class PISOAdjoint:
     """Taped forward steps and adjoint steps of a :class:`PISOStepper` (same domain and settings).
 
-    ``adjoint_advection_tol`` / ``adjoint_pressure_tol`` default to the forward tolerances.
+    ``adjoint_advection_tol`` / ``adjoint_pressure_tol`` default to the forward tolerances.  With
+    ``use_graph = True`` the untaped forward steps of :func:`rollout` replay the stepper's captured
+    one-step CUDA graph.
     """
 
     def __init__(self, stepper: PISOStepper, adjoint_advection_tol: Optional[float] = None,
@@ -258,8 +260,10 @@ class _Rollout(torch.autograd.Function):
         ckpt = {0: u0.detach().clone()}
         outs = []
         rec = sorted(set(int(r) for r in record))
+        one_step = st.replay if (getattr(adj, "use_graph", False) and st._graph is not None
+                                 and st._graph_steps == 1) else st.step
         for t in range(1, steps + 1):
-            st.step()
+            one_step()
             if t % checkpoint_every == 0 and t < steps:
                 ckpt[t] = adj.velocity()
             if t in rec:
