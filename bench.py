@@ -172,6 +172,15 @@ def sample_indices(sides, k):
     return order[[int(x * len(order)) for x in q]]
 
 
+def precision_kwargs(args):
+    """mixed: FP32 stencils / vectors, FP64 reductions and one FP64 refinement sweep of every pressure
+    solve to an RMS residual of 1e-9, pressure solves warm-started from the latest pressure; fp32: the
+    single FP32 pressure solve from zero (the reference's order)."""
+    if args.precision == "mixed":
+        return {"pressure_refine": 1, "refine_tol": 1e-9, "warm_start_pressure": True}
+    return {}
+
+
 def rank_seed(rank):
     """Seed of rank r's batch: every rank advances its own independent simulations."""
     return 6 + rank
@@ -248,7 +257,7 @@ def run_pict(args, rank, world):
     batch = BatchDomain(doms, time_steps=wl["dts"])
     st = PISOStepper(batch, time_step=float(wl["dts"][0]), corrector_steps=wl["correctors"],
                      advection_tol=wl["tol"], pressure_tol=wl["tol"], max_iterations=5000,
-                     p_group_size=args.group_size, adv_group_size=args.group_size)
+                     p_group_size=args.group_size, adv_group_size=args.group_size, **precision_kwargs(args))
     cells = batch.getTotalSize()
     # warm-up (eager), then capture one step as a CUDA graph; the algorithmic bytes of every warm-up
     # CG launch are recorded so that an ncu capture of launch k (-k regex:k_cg -s k -c 1) can be set
@@ -306,6 +315,10 @@ def run_pict(args, rank, world):
     # end-to-end through the public API with host buffers
     e2e = e2e_pass(st, batch, args, dev, cells, world)
 
+    # the same batched step in plain FP32 (pressure solves from zero to the workload tolerance, no
+    # refinement): faster, at the error reported under fp32_step.err
+    fp32 = fp32_pass(batch, wl, args, dev, cells, world) if (args.precision == "mixed" and not args.skip_fp32) else None
+
     # forward + backward (adjoint) through the checkpointed rollout
     fb = fwd_bwd_pass(st, batch, args, dev, cells, world) if not args.skip_bwd else None
 
@@ -326,6 +339,7 @@ def run_pict(args, rank, world):
         cpu = {"value": rate, "unit": "cell-steps/s", "cores": 1, "kind": "port",
                "sample": "sides %s x 2 PISO steps each (FP64 NumPy/SciPy restatement, %.1f s)" % (
                    [int(wl["sides"][i]) for i in sel], tt)}
+    iters_ref = [[max(i.usedIterations for i in r) for r in row] for row in st.refine_infos()]
     iters_adv = [i.usedIterations for i in adv_infos]
     iters_p = [[i.usedIterations for i in p] for p in p_infos]
     if rank == 0:
@@ -335,6 +349,9 @@ def run_pict(args, rank, world):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": args.workload, "simulations": len(doms), "cells_per_gpu": cells,
                        "pass": "forward", "solver_tol": wl["tol"], "correctors": wl["correctors"],
+                       "precision": args.precision + (" (FP32 fields and Krylov vectors, FP64 reductions, one FP64 "
+                                                      "refinement sweep of each pressure solve to 1e-9, warm-started pressure solves)"
+                                                      if args.precision == "mixed" else " (FP32, FP64 reductions)"),
                        "cuda_graph": not args.no_graph, "l2": "working set > L2 (126 MB), no flush",
                        "parallelism": "independent batches per GPU" if world > 1 else "single GPU"},
             "clocks": clocks,
@@ -342,12 +359,14 @@ def run_pict(args, rank, world):
             "cpu_baseline": cpu,
             "e2e": e2e,
             "fwd_bwd": fb,
+            "fp32_step": fp32,
             "plain": plain,
             "gpu_launches": st.kernels_per_step() * args.steps,
             "err": err,
             "solver_iterations": {"advection_max": int(max(iters_adv)), "advection_mean": float(np.mean(iters_adv)),
                                   "pressure_max": [int(max(p)) for p in iters_p],
-                                  "pressure_mean": [float(np.mean(p)) for p in iters_p]},
+                                  "pressure_mean": [float(np.mean(p)) for p in iters_p],
+                                  "refinement_max": iters_ref},
         }
         print(json.dumps(line), flush=True)
 
@@ -379,13 +398,15 @@ def roofline_pass(st, batch, args, dev):
     achieved = byt / (ms * 1e-3) / 1e9
     peak, kind = measured_peaks()
     kern = "k_cg1" if st.p_params.variant == 1 else "k_cg"
+    launches = len(cg_ms)
     ratio = NCU_TRAFFIC_RATIO.get(kern)
     return {"kernel": "%s (persistent CG, pressure solve)" % kern, "bound": "hbm", "achieved": achieved, "peak": peak,
             "peak_kind": kind, "unit": "GB/s", "frac": achieved / peak,
             "traffic": None if ratio is None else ratio * byt,
             "traffic_note": None if ratio is None else
             "ncu dram bytes / algorithmic bytes = %.3f on one captured launch (profiles/), scaled to the average launch" % ratio,
-            "algorithmic_bytes_per_launch": byt, "avg_launch_ms": ms,
+            "algorithmic_bytes_per_launch": byt, "avg_launch_ms": ms, "launches_timed": launches,
+            "launches": "every CG launch of the step (first pressure solves and refinement solves)",
             "bytes_per_cell_iteration": per_cell}
 
 
@@ -420,6 +441,41 @@ def e2e_pass(st, batch, args, dev, cells, world):
     total_cells, ms_max = job_totals(cells, ms, world, dev)
     return {"value": total_cells * steps / (ms_max * 1e-3), "unit": "cell-steps/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": h2d, "steps": steps}
+
+
+def fp32_pass(batch, wl, args, dev, cells, world):
+    import torch
+    from pict_b200.engine import PISOStepper
+    blocks = batch.getBlocks()
+    saved = [(b.velocity.clone(), b.pressure.clone()) for b in blocks]
+    st = PISOStepper(batch, time_step=float(wl["dts"][0]), corrector_steps=wl["correctors"], advection_tol=wl["tol"],
+                     pressure_tol=wl["tol"], max_iterations=5000)
+    for _ in range(3):
+        st.step()
+    st.capture(steps=1)
+    for _ in range(3):
+        st.replay()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        st.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    st.check()
+    ms = e0.elapsed_time(e1)
+    for b, (v, p) in zip(blocks, saved):
+        b.velocity.copy_(v)
+        b.pressure.copy_(p)
+    total_cells, ms_max = job_totals(cells, ms, world, dev)
+    out = {"value": total_cells * args.steps / (ms_max * 1e-3), "unit": "cell-steps/s",
+           "ms_per_step": ms_max / args.steps, "precision": "FP32, FP64 reductions, pressure solves from zero to %g" % wl["tol"]}
+    if not args.skip_err:
+        a = argparse.Namespace(**vars(args))
+        a.precision = "fp32"
+        out["err"] = accuracy_check(wl, a)
+    return out
 
 
 def fwd_bwd_pass(st, batch, args, dev, cells, world):
@@ -472,7 +528,8 @@ def plain_pass(wl, args, k=8, steps=10):
     for i in sel:
         s = int(wl["sides"][i])
         d = make_cavity_domain(s, 1.0 / wl["re"][i], torch.float32)
-        stp = PISOStepper(d, time_step=float(wl["dts"][i]), advection_tol=wl["tol"], pressure_tol=wl["tol"])
+        stp = PISOStepper(d, time_step=float(wl["dts"][i]), advection_tol=wl["tol"], pressure_tol=wl["tol"],
+                          **precision_kwargs(args))
         for _ in range(3):
             stp.step()
         stp.capture(steps=1)
@@ -544,7 +601,7 @@ def accuracy_check(wl, args):
     doms = [make_cavity_domain(int(wl["sides"][i]), 1.0 / wl["re"][i], torch.float32) for i in order]
     dts = [wl["dts"][i] for i in order]
     b = BatchDomain(doms, time_steps=dts)
-    st = PISOStepper(b, time_step=dts[0], advection_tol=wl["tol"], pressure_tol=wl["tol"])
+    st = PISOStepper(b, time_step=dts[0], advection_tol=wl["tol"], pressure_tol=wl["tol"], **precision_kwargs(args))
     steps = 10
     for _ in range(steps):
         st.step()
@@ -582,7 +639,9 @@ def main():
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-err", action="store_true")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp32"])
     ap.add_argument("--skip-bwd", action="store_true")
+    ap.add_argument("--skip-fp32", action="store_true")
     ap.add_argument("--skip-plain", action="store_true")
     ap.add_argument("--fb-steps", type=int, default=10, help="steps of the forward+backward rollout")
     ap.add_argument("--checkpoint", type=int, default=5, help="checkpoint interval of the rollout")

@@ -225,6 +225,23 @@ int64_t pict_solve_static_scratch_bytes(void);
 pict_status_t pict_solve_static(const pict_domain_t* dom, const void* coef, const void* rhs, void* x,
                                 const pict_solve_params_t* params, void* info_out, void* stream);
 
+/* ---------------- mixed precision: FP64 iterative refinement of a solve ----------------
+ * No counterpart in the reference, which solves once in the domain dtype (cgSolveGPU,
+ * extensions/cg_solver_kernel.cu:114-456).  x64: FP64 accumulator [N] of the solution.
+ * pict_refine_residual: residual = rhs - coef*x in FP64 arithmetic (stored in the domain dtype); x is
+ *   x_init when non-NULL (and x64 is set to it), else x64.  project_mean=1 removes the per-system mean
+ *   of the residual (the unsolvable constant mode of a singular pressure system; needs tile_scratch of
+ *   num_tiles doubles).
+ * pict_refine_update: x64 += correction.
+ * pict_refine_finish: x = x64 (minus its per-system mean), optionally also into the blocks' pressure;
+ *   tile_scratch: num_tiles doubles (needed with subtract_mean). */
+pict_status_t pict_refine_residual(const pict_domain_t* dom, const void* coef, const void* rhs, const void* x_init,
+                                   double* x64, void* residual, int32_t project_mean, double* tile_scratch,
+                                   void* stream);
+pict_status_t pict_refine_update(const pict_domain_t* dom, double* x64, const void* correction, void* stream);
+pict_status_t pict_refine_finish(const pict_domain_t* dom, const double* x64, void* x, int32_t subtract_mean,
+                                 int32_t write_block_pressure, double* tile_scratch, void* stream);
+
 /* ---------------- adjoint (reverse mode) of the orthogonal step ----------------
  * Gather-form adjoints of the forward operators (no atomics, deterministic).  They read the forward
  * quantities from explicit global vectors (a per-step tape) and accumulate into global vectors:

@@ -153,6 +153,9 @@ SIGNATURES = {
     "pict_solve": (c_i32, [_PD, c_vp, c_vp, c_vp, _PS, c_vp, c_vp, ctypes.c_int64, c_vp]),
     "pict_solve_static_scratch_bytes": (ctypes.c_int64, []),
     "pict_solve_static": (c_i32, [_PD, c_vp, c_vp, c_vp, _PS, c_vp, c_vp]),
+    "pict_refine_residual": (c_i32, [_PD, c_vp, c_vp, c_vp, c_vp, c_vp, c_i32, c_vp, c_vp]),
+    "pict_refine_update": (c_i32, [_PD, c_vp, c_vp, c_vp]),
+    "pict_refine_finish": (c_i32, [_PD, c_vp, c_vp, c_i32, c_i32, c_vp, c_vp]),
     "pict_correct_velocity_grad": (c_i32, [_PD, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "pict_sim_mean_project": (c_i32, [_PD, c_vp, c_vp]),
     "pict_divergence_grad": (c_i32, [_PD, c_vp, c_vp, c_vp, c_vp]),

@@ -175,9 +175,7 @@ class PISOAdjoint:
             else:
                 check(lib.pict_setup_pressure_rhs(desc, dt, 0, 0, s), "pressure rhs")
             tape.h[k].copy_(d.pressureRHS)
-            check(lib.pict_solve(desc, P._ptr(d.P.coef), P._ptr(d.pressureRHSdiv), P._ptr(d.pressureResult),
-                                 ctypes.byref(st.p_params), P._ptr(st.info_p[k]), P._ptr(st.ws), st.ws_bytes, s),
-                  "pressure solve")
+            st._pressure_solve(k, desc, s)
             tape.p[k].copy_(d.pressureResult)
             last = k == self.nc - 1
             check(lib.pict_correct_velocity(desc, dt, 1, 0, 1 if last else 0, s), "velocity correction")

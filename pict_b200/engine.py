@@ -45,7 +45,8 @@ def default_tolerance(dtype):
 class PISOStepper:
     def __init__(self, domain, time_step=None, corrector_steps: int = 2, advection_tol: Optional[float] = None,
                  pressure_tol: Optional[float] = None, max_iterations: int = 5000, adv_group_size: int = 0,
-                 p_group_size: int = 0, threads: int = 0, normalize_pressure: bool = True, cg_variant: int = 1):
+                 p_group_size: int = 0, threads: int = 0, normalize_pressure: bool = True, cg_variant: int = 1,
+                 pressure_refine: int = 0, refine_tol: Optional[float] = None, warm_start_pressure: bool = False):
         self.domain = domain
         self.dims = domain.getSpatialDims()
         self.corrector_steps = int(corrector_steps)
@@ -57,9 +58,22 @@ class PISOStepper:
         self.time_step = time_step
         self.adv_params = P._solve_params(self.dims, self.max_iterations, self.adv_tol, _lib.PICT_CONV_NORM2_NORMALIZED,
                                           True, False, x_zero=True, group_size=adv_group_size, threads=threads)
+        # mixed precision: `pressure_refine` FP64 refinement sweeps after the first pressure solve, each
+        # solving the correction of the FP64 residual to `refine_tol`
+        self.pressure_refine = int(pressure_refine)
+        self.refine_tol = (1e-9 if refine_tol is None else float(refine_tol))
+        refine = self.pressure_refine > 0
+        # warm start: every pressure solve starts from pressureResult (the previous corrector's or step's
+        # mean-free pressure) instead of zero; same solution, fewer iterations
+        self.warm_start_pressure = bool(warm_start_pressure)
         self.p_params = P._solve_params(1, self.max_iterations, self.p_tol, _lib.PICT_CONV_NORM2_NORMALIZED, False,
-                                        False, x_zero=True, subtract_mean=normalize_pressure, write_block_pressure=True,
-                                        group_size=p_group_size, threads=threads, variant=cg_variant)
+                                        False, x_zero=not self.warm_start_pressure,
+                                        subtract_mean=normalize_pressure and not refine,
+                                        write_block_pressure=not refine, group_size=p_group_size, threads=threads,
+                                        variant=cg_variant)
+        self.r_params = P._solve_params(1, self.max_iterations, self.refine_tol, _lib.PICT_CONV_NORM2_NORMALIZED, False,
+                                        False, x_zero=True, group_size=p_group_size, threads=threads,
+                                        variant=cg_variant)
         self._graph = None
         self._graph_steps = 0
         self._prepare()
@@ -77,12 +91,23 @@ class PISOStepper:
         self.n_p_info = ns
         nbytes_adv = self.n_adv_info * self.info_bytes
         nbytes_p = self.n_p_info * self.info_bytes
-        self.info = torch.zeros(nbytes_adv + self.corrector_steps * nbytes_p, dtype=torch.uint8, device=dev)
+        nr = self.pressure_refine
+        self.info = torch.zeros(nbytes_adv + self.corrector_steps * (1 + nr) * nbytes_p, dtype=torch.uint8, device=dev)
         self.info_adv = self.info[:nbytes_adv]
         self.info_p = [self.info[nbytes_adv + k * nbytes_p: nbytes_adv + (k + 1) * nbytes_p]
                        for k in range(self.corrector_steps)]
+        base = nbytes_adv + self.corrector_steps * nbytes_p
+        self.info_r = [[self.info[base + (k * nr + m) * nbytes_p: base + (k * nr + m + 1) * nbytes_p]
+                        for m in range(nr)] for k in range(self.corrector_steps)]
+        if nr > 0:
+            N = d.getTotalSize()
+            self._x64 = torch.zeros(N, dtype=torch.float64, device=dev)
+            self._res = torch.zeros(N, dtype=d.getDtype(), device=dev)
+            self._corr = torch.zeros(N, dtype=d.getDtype(), device=dev)
+            self._tile_scratch = torch.zeros(max(1, self.desc.num_tiles), dtype=torch.float64, device=dev)
         ws = max(lib.pict_solve_workspace_bytes(ctypes.byref(self.desc), ctypes.byref(self.adv_params)),
-                 lib.pict_solve_workspace_bytes(ctypes.byref(self.desc), ctypes.byref(self.p_params)))
+                 lib.pict_solve_workspace_bytes(ctypes.byref(self.desc), ctypes.byref(self.p_params)),
+                 lib.pict_solve_workspace_bytes(ctypes.byref(self.desc), ctypes.byref(self.r_params)))
         self.ws = torch.empty(int(ws), dtype=torch.uint8, device=dev)
         self.ws_bytes = int(ws)
         self.lib = lib
@@ -92,6 +117,17 @@ class PISOStepper:
         if isinstance(ts, torch.Tensor):
             ts = float(ts.item())
         return float(ts)
+
+    def _pressure_solve(self, k, desc, st):
+        """Pressure solve of corrector k (plus FP64 refinement sweeps); leaves the mean-free solution in
+        pressureResult and the blocks' pressure."""
+        d = self.domain
+        lib = self.lib
+        check(lib.pict_solve(desc, P._ptr(d.P.coef), P._ptr(d.pressureRHSdiv), P._ptr(d.pressureResult),
+                             ctypes.byref(self.p_params), P._ptr(self.info_p[k]), P._ptr(self.ws), self.ws_bytes, st),
+              "pressure solve")
+        if self.pressure_refine > 0:
+            self._refine_only(k, desc, st)
 
     def step(self, time_step=None, stream=None):
         """Launch one PISO step (no host synchronisation)."""
@@ -110,19 +146,43 @@ class PISOStepper:
                 check(lib.pict_setup_pressure_correction(desc, dt, 0, 0, st), "pressure setup")
             else:
                 check(lib.pict_setup_pressure_rhs(desc, dt, 0, 0, st), "pressure rhs")
-            check(lib.pict_solve(desc, P._ptr(d.P.coef), P._ptr(d.pressureRHSdiv), P._ptr(d.pressureResult),
-                                 ctypes.byref(self.p_params), P._ptr(self.info_p[k]), P._ptr(self.ws), self.ws_bytes, st),
-                  "pressure solve")
+            self._pressure_solve(k, desc, st)
             last = k == self.corrector_steps - 1
             check(lib.pict_correct_velocity(desc, dt, 1, 0, 1 if last else 0, st), "velocity correction")
         if self.corrector_steps == 0:
             check(lib.pict_copy_velocity_result_to_blocks(desc, st), "copy velocity")
 
+    def _refine_only(self, k, desc, st, events=None, ev=None):
+        """FP64 refinement sweeps after the first pressure solve of corrector k: residual of the FP64
+        accumulator, FP32 correction solve, accumulation; then the mean-free result into
+        pressureResult and the blocks' pressure."""
+        d = self.domain
+        lib = self.lib
+        x64 = ctypes.c_void_p(self._x64.data_ptr())
+        for m in range(self.pressure_refine):
+            check(lib.pict_refine_residual(desc, P._ptr(d.P.coef), P._ptr(d.pressureRHSdiv),
+                                           P._ptr(d.pressureResult) if m == 0 else None, x64, P._ptr(self._res),
+                                           int(self.normalize_pressure), ctypes.c_void_p(self._tile_scratch.data_ptr()),
+                                           st), "refine residual")
+            a = ev() if ev else None
+            check(lib.pict_solve(desc, P._ptr(d.P.coef), P._ptr(self._res), P._ptr(self._corr),
+                                 ctypes.byref(self.r_params), P._ptr(self.info_r[k][m]), P._ptr(self.ws),
+                                 self.ws_bytes, st), "refinement solve")
+            if events is not None:
+                events.append((a, ev(), self.info_r[k][m].clone()))
+            check(lib.pict_refine_update(desc, x64, P._ptr(self._corr), st), "refine update")
+        check(lib.pict_refine_finish(desc, x64, P._ptr(d.pressureResult), int(self.normalize_pressure), 1,
+                                     ctypes.c_void_p(self._tile_scratch.data_ptr()), st), "refine finish")
+
     def kernels_per_step(self):
         """Kernels of this library launched per step: advection setup 1; per solve init-info, solver and
-        finish-info 3; per corrector pressure setup 2 (matrix/RHS, divergence), correction 1."""
+        finish-info 3; per corrector pressure setup 2 (matrix/RHS, divergence), correction 1, and the
+        refinement sweeps when enabled."""
         n = 1 + 3
         n += self.corrector_steps * (2 + 3 + 1)
+        if self.pressure_refine > 0:  # per sweep: residual (+2 projection), solve (3), update; partials + finish
+            per = 5 + (2 if self.normalize_pressure else 0)
+            n += self.corrector_steps * (per * self.pressure_refine + (2 if self.normalize_pressure else 1))
         if self.corrector_steps == 0:
             n += 1
         return n
@@ -164,6 +224,8 @@ class PISOStepper:
                   "pressure solve")
             b = ev()
             out["cg"].append((a, b, self.info_p[k].clone()))
+            if self.pressure_refine > 0:
+                self._refine_only(k, desc, st, events=out["cg"], ev=ev)
             last = k == self.corrector_steps - 1
             check(lib.pict_correct_velocity(desc, dt, 1, 0, 1 if last else 0, st), "velocity correction")
         return out
@@ -176,10 +238,16 @@ class PISOStepper:
               for k in range(self.corrector_steps)]
         return adv, ps
 
+    def refine_infos(self):
+        """Reports of the refinement solves of the last step: [corrector][sweep] -> [ns]."""
+        return [[P.decode_infos(t) for t in row] for row in self.info_r]
+
     def check(self):
         """Raise LinsolveError if any solve of the last step failed (synchronises)."""
         adv, ps = self.infos()
-        for name, lst in [("advection", adv)] + [("pressure %d" % k, p) for k, p in enumerate(ps)]:
+        extra = [("pressure %d refinement %d" % (k, m), r) for k, row in enumerate(self.refine_infos())
+                 for m, r in enumerate(row)]
+        for name, lst in [("advection", adv)] + [("pressure %d" % k, p) for k, p in enumerate(ps)] + extra:
             for i, inf in enumerate(lst):
                 if getattr(inf, "status", 0) == 1:
                     raise LinsolveError("%s solve: inter-CTA barrier timed out (system %d)" % (name, i))
