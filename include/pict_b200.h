@@ -283,6 +283,14 @@ pict_status_t pict_advection_grad(const pict_domain_t* dom, double dt, const voi
 pict_status_t pict_adjoint_to_blocks(const pict_domain_t* dom, const void* velocity_grad, const void* viscosity_grad,
                                      const void* source_grad, const void* boundary_velocity_grad,
                                      void* sim_viscosity_grad, void* block_scratch, void* stream);
+/* SparseOuterProduct (extensions/PISOtorch.cpp:564) on the stencil pattern, summed over nrhs stacked
+ * vectors: coef_out[0][i] += scale sum_c a_c[i] b_c[i], coef_out[f+1][i] += scale sum_c a_c[i] b_c[nbr(f,i)]
+ * (the matrix gradient of a linear solve is -b_grad x^T, PISOtorch_diff.py:352-371). */
+pict_status_t pict_stencil_outer_product(const pict_domain_t* dom, const void* a, const void* b, int32_t nrhs,
+                                        void* coef_out, double scale, void* stream);
+/* SetupPressureMatrixGrad (PISOtorch_diff.py:897-965): A_grad += d(P : P_grad)/dA. */
+pict_status_t pict_pressure_matrix_grad(const pict_domain_t* dom, const void* A, const void* P_grad, void* A_grad,
+                                        void* stream);
 /* Copy between a global [ncomp][N] vector and a per-block field (0 velocity, 1 pressure, 2 source,
  * 3 velocity_grad, 4 pressure_grad, 5 source_grad); accumulate=1 adds instead of overwriting. */
 pict_status_t pict_copy_field(const pict_domain_t* dom, int32_t which, int32_t to_blocks, void* global_vec,

@@ -1241,7 +1241,8 @@ class Domain:
         _check(viscosity.dim() == 1 and viscosity.size(0) == 1, "viscosity must be a scalar.")
         self.viscosity = viscosity
         if getattr(self, "_initialized", False):
-            self._sim_visc.copy_(viscosity.to(self._dtype), non_blocking=False)
+            with torch.no_grad():
+                self._sim_visc.copy_(viscosity.detach().to(self._dtype), non_blocking=False)
 
     def hasBlockViscosity(self):
         return any(b.hasViscosity() for b in self.blocks)

@@ -507,6 +507,57 @@ __global__ void k_copy_field(pict_domain_t dom, int which, int to_blocks, T* glo
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// SparseOuterProduct on stencils (extensions/PISO_multiblock_cuda_kernel.cu via PISOtorch.cpp:564,
+// used by the linear-solve gradient -b_grad x^T, PISOtorch_diff.py:352-371):
+//   out[0][i] += s sum_c a_c[i] b_c[i],   out[f+1][i] += s sum_c a_c[i] b_c[j(f,i)]
+// ---------------------------------------------------------------------------------------------
+template <typename T, int D>
+__global__ void k_stencil_outer(pict_domain_t dom, const T* a, const T* bv, int nrhs, T* out, T scale) {
+    const int N = dom.num_cells;
+    PICT_CELL_LOOP(i, N) {
+        T d = 0;
+        for (int c = 0; c < nrhs; ++c) d += a[(size_t)c * N + i] * bv[(size_t)c * N + i];
+        out[i] += scale * d;
+#pragma unroll
+        for (int f = 0; f < 2 * D; ++f) {
+            const int j = dom.nbr[(size_t)f * N + i];
+            if (j < 0) continue;
+            T o = 0;
+            for (int c = 0; c < nrhs; ++c) o += a[(size_t)c * N + i] * bv[(size_t)c * N + j];
+            out[(size_t)(f + 1) * N + i] += scale * o;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// SetupPressureMatrix gradient (PISOtorch_diff.py:897-965): P_f,i = (al_i[a]/A_i + al_j[a']/A_j)/2,
+// P_0,i = -sum_f P_f,i  ->  A_bar_i += -al_i(f>>1)/(2 A_i^2) (P_bar_f,i - P_bar_0,i + P_bar_back,j - P_bar_0,j)
+// ---------------------------------------------------------------------------------------------
+template <typename T, int D>
+__global__ void k_pressure_matrix_grad(pict_domain_t dom, const T* A, const T* Pbar, T* Abar) {
+    const int N = dom.num_cells;
+    PICT_CELL_LOOP(i, N) {
+        const int b = dom.cell_block[i];
+        const pict_block_t& B = dom.blocks[b];
+        const int l = i - B.offset;
+        int p[3];
+        unflatten(l, B.size, p);
+        const T* tr = cell_transform<T, D>(B, l);
+        const T rA = T(1) / A[i];
+        const T p0 = Pbar[i];
+        T acc = 0;
+#pragma unroll
+        for (int f = 0; f < 2 * D; ++f) {
+            const Nbr n = neighbour(dom, B, b, p, i, f);
+            if (n.j < 0) continue;
+            const T g = Pbar[(size_t)(f + 1) * N + i] - p0 + Pbar[(size_t)(n.back + 1) * N + n.j] - Pbar[n.j];
+            acc += laplace_coef<T, D>(tr, f >> 1) * g;
+        }
+        Abar[i] += -T(0.5) * rA * rA * acc;
+    }
+}
+
 #define PICT_ADJ_DISPATCH(NAME, ...)                                                                 \
     do {                                                                                              \
         if (dom->dtype == PICT_F32 && dom->dims == 2) { NAME<float, 2><<<grid, 256, 0, st>>>(__VA_ARGS__); } \
@@ -656,6 +707,40 @@ pict_status_t pict_adjoint_to_blocks(const pict_domain_t* dom, const void* veloc
         s = check_launch("sim_viscosity_grad");
     }
     return s;
+}
+
+pict_status_t pict_stencil_outer_product(const pict_domain_t* dom, const void* a, const void* b, int32_t nrhs,
+                                        void* coef_out, double scale, void* stream) {
+    pict_status_t s = check_dom(dom, "stencil_outer_product");
+    if (s) return s;
+    if (!a || !b || !coef_out || nrhs < 1) return set_error(PICT_ERR_ARG, "stencil_outer_product: bad argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int grid = cell_grid(dom->num_cells, 256);
+    if (dom->dtype == PICT_F32) {
+        if (dom->dims == 2) k_stencil_outer<float, 2><<<grid, 256, 0, st>>>(*dom, (const float*)a, (const float*)b, nrhs, (float*)coef_out, (float)scale);
+        else k_stencil_outer<float, 3><<<grid, 256, 0, st>>>(*dom, (const float*)a, (const float*)b, nrhs, (float*)coef_out, (float)scale);
+    } else {
+        if (dom->dims == 2) k_stencil_outer<double, 2><<<grid, 256, 0, st>>>(*dom, (const double*)a, (const double*)b, nrhs, (double*)coef_out, scale);
+        else k_stencil_outer<double, 3><<<grid, 256, 0, st>>>(*dom, (const double*)a, (const double*)b, nrhs, (double*)coef_out, scale);
+    }
+    return check_launch("stencil_outer_product");
+}
+
+pict_status_t pict_pressure_matrix_grad(const pict_domain_t* dom, const void* A, const void* P_grad, void* A_grad,
+                                        void* stream) {
+    pict_status_t s = check_dom(dom, "pressure_matrix_grad");
+    if (s) return s;
+    if (!A || !P_grad || !A_grad) return set_error(PICT_ERR_ARG, "pressure_matrix_grad: NULL argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int grid = cell_grid(dom->num_cells, 256);
+    if (dom->dtype == PICT_F32) {
+        if (dom->dims == 2) k_pressure_matrix_grad<float, 2><<<grid, 256, 0, st>>>(*dom, (const float*)A, (const float*)P_grad, (float*)A_grad);
+        else k_pressure_matrix_grad<float, 3><<<grid, 256, 0, st>>>(*dom, (const float*)A, (const float*)P_grad, (float*)A_grad);
+    } else {
+        if (dom->dims == 2) k_pressure_matrix_grad<double, 2><<<grid, 256, 0, st>>>(*dom, (const double*)A, (const double*)P_grad, (double*)A_grad);
+        else k_pressure_matrix_grad<double, 3><<<grid, 256, 0, st>>>(*dom, (const double*)A, (const double*)P_grad, (double*)A_grad);
+    }
+    return check_launch("pressure_matrix_grad");
 }
 
 pict_status_t pict_copy_field(const pict_domain_t* dom, int32_t which, int32_t to_blocks, void* global_vec,
