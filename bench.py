@@ -255,9 +255,19 @@ def run_pict(args, rank, world):
     wl = build_workload(args.workload, rank)
     doms = wl["domains"]
     batch = BatchDomain(doms, time_steps=wl["dts"])
-    st = PISOStepper(batch, time_step=float(wl["dts"][0]), corrector_steps=wl["correctors"],
-                     advection_tol=wl["tol"], pressure_tol=wl["tol"], max_iterations=5000,
-                     p_group_size=args.group_size, adv_group_size=args.group_size, **precision_kwargs(args))
+    kw = dict(time_step=float(wl["dts"][0]), corrector_steps=wl["correctors"], advection_tol=wl["tol"],
+              pressure_tol=wl["tol"], max_iterations=5000, **precision_kwargs(args))
+    tuned = None
+    if args.autotune:
+        from pict_b200.autotune import autotune
+        best, table = autotune(batch, kw)
+        kw.update(p_group_size=best["p_group_size"], adv_group_size=best["adv_group_size"],
+                  cg_variant=best["cg_variant"])
+        tuned = {"best": {k: best[k] for k in ("tile_cells", "p_group_size", "cg_variant", "ms_per_step")},
+                 "candidates": len(table)}
+    else:
+        kw.update(p_group_size=args.group_size, adv_group_size=args.group_size)
+    st = PISOStepper(batch, **kw)
     cells = batch.getTotalSize()
     # warm-up (eager), then capture one step as a CUDA graph; the algorithmic bytes of every warm-up
     # CG launch are recorded so that an ncu capture of launch k (-k regex:k_cg -s k -c 1) can be set
@@ -353,6 +363,7 @@ def run_pict(args, rank, world):
                                                       "refinement sweep of each pressure solve to 1e-9, warm-started pressure solves)"
                                                       if args.precision == "mixed" else " (FP32, FP64 reductions)"),
                        "cuda_graph": not args.no_graph, "l2": "working set > L2 (126 MB), no flush",
+                       "autotune": tuned, "tile_cells": batch.tile_cells,
                        "parallelism": "independent batches per GPU" if world > 1 else "single GPU"},
             "clocks": clocks,
             "roofline": roof,
@@ -642,6 +653,7 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp32"])
     ap.add_argument("--skip-bwd", action="store_true")
     ap.add_argument("--skip-fp32", action="store_true")
+    ap.add_argument("--autotune", type=int, default=1, help="1: pick tile size / CTA cap / CG variant by timing")
     ap.add_argument("--skip-plain", action="store_true")
     ap.add_argument("--fb-steps", type=int, default=10, help="steps of the forward+backward rollout")
     ap.add_argument("--checkpoint", type=int, default=5, help="checkpoint interval of the rollout")

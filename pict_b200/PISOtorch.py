@@ -1411,6 +1411,17 @@ class Domain:
         self._initialized = True
         self.UpdateDomainData()
 
+    def set_tile_cells(self, tile_cells):
+        """Cells per Krylov work tile (1..2048): rebuilds the tile table of a prepared domain.  Steppers
+        created before the change must be re-created (their workspace depends on the tile count)."""
+        tile_cells = int(tile_cells)
+        _check(1 <= tile_cells <= 2048, "tile_cells must be in [1, 2048]")
+        self._tile_cells = tile_cells
+        if self._initialized:
+            self._tiles, self._sim_tiles, self._num_tiles = build_tiles(self._pack_blocks(), len(self.blocks), 1,
+                                                                        self._device, tile_cells)
+            self._desc = self._make_desc()
+
     def _pack_blocks(self):
         """Host block table with raw device pointers (Domain::UpdateDomainGPU, extensions/domain_structs.cpp:3040-3261)."""
         arr = (BlockDesc * len(self.blocks))()
