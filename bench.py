@@ -177,7 +177,8 @@ def precision_kwargs(args):
     solve to an RMS residual of 1e-9, pressure solves warm-started from the latest pressure; fp32: the
     single FP32 pressure solve from zero (the reference's order)."""
     if args.precision == "mixed":
-        return {"pressure_refine": 1, "refine_tol": 1e-9, "warm_start_pressure": True}
+        return {"pressure_refine": 1, "refine_tol": 1e-9, "warm_start_pressure": True,
+                "refine_solver": args.refine_solver}
     return {}
 
 
@@ -360,7 +361,7 @@ def run_pict(args, rank, world):
             "config": {"workload": args.workload, "simulations": len(doms), "cells_per_gpu": cells,
                        "pass": "forward", "solver_tol": wl["tol"], "correctors": wl["correctors"],
                        "precision": args.precision + (" (FP32 fields and Krylov vectors, FP64 reductions, one FP64 "
-                                                      "refinement sweep of each pressure solve to 1e-9, warm-started pressure solves)"
+                                                      "refinement sweep of each pressure solve to 1e-9 (multigrid-preconditioned CG corrections), warm-started pressure solves)"
                                                       if args.precision == "mixed" else " (FP32, FP64 reductions)"),
                        "cuda_graph": not args.no_graph, "l2": "working set > L2 (126 MB), no flush",
                        "autotune": tuned, "tile_cells": batch.tile_cells,
@@ -651,6 +652,8 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-err", action="store_true")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp32"])
+    ap.add_argument("--refine-solver", default="mg", choices=["mg", "cg"],
+                    help="solver of the refinement corrections (mixed precision)")
     ap.add_argument("--skip-bwd", action="store_true")
     ap.add_argument("--skip-fp32", action="store_true")
     ap.add_argument("--autotune", type=int, default=1, help="1: pick tile size / CTA cap / CG variant by timing")

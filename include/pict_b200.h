@@ -242,6 +242,30 @@ pict_status_t pict_refine_update(const pict_domain_t* dom, double* x64, const vo
 pict_status_t pict_refine_finish(const pict_domain_t* dom, const double* x64, void* x, int32_t subtract_mean,
                                  int32_t write_block_pressure, double* tile_scratch, void* stream);
 
+/* ---------------- multigrid-preconditioned CG (mixed-precision correction solves) ----------------
+ * No counterpart in the reference.  For domains whose systems are single blocks with fixed or
+ * periodic faces.  A level describes the cells of every block at one coarsening depth. */
+typedef struct pict_mg_level {
+    int32_t num_cells;
+    int32_t num_blocks;
+    int32_t dims;
+    int32_t dtype;
+    const int32_t* blocks;     /* [num_blocks][8]: first cell, size x, y, z, periodic x, y, z, system (device) */
+    const int32_t* cell_block; /* [num_cells] block of each cell (device) */
+    void* coef;                /* [2D+1][num_cells] stencil of the level (device) */
+} pict_mg_level_t;
+
+/* Galerkin coarse operator R A P of `fine` into coarse->coef (aggregates of 2^D cells). */
+pict_status_t pict_mg_galerkin(const pict_mg_level_t* fine, const pict_mg_level_t* coarse, void* stream);
+int64_t pict_pcg_mg_workspace_bytes(const pict_domain_t* dom, const pict_mg_level_t* levels, int32_t num_levels);
+/* `iterations` preconditioned CG iterations on levels[0].coef x = rhs from x = 0, V(1,1)-cycle with damped
+ * Jacobi (omega), prolongation scaled by prolong_scale, coarse_sweeps Jacobi sweeps on the coarsest
+ * level; per-system report (final RMS / 2-norm residual of the recursion) in info_out[num_sims]. */
+pict_status_t pict_pcg_mg(const pict_domain_t* dom, const pict_mg_level_t* levels, int32_t num_levels, const void* rhs,
+                          void* x, int32_t iterations, double tolerance, int32_t convergence, void* info_out,
+                          void* workspace, int64_t workspace_bytes, double omega, double prolong_scale,
+                          int32_t coarse_sweeps, void* stream);
+
 /* ---------------- adjoint (reverse mode) of the orthogonal step ----------------
  * Gather-form adjoints of the forward operators (no atomics, deterministic).  They read the forward
  * quantities from explicit global vectors (a per-step tape) and accumulate into global vectors:

@@ -97,6 +97,18 @@ class DomainDesc(ctypes.Structure):
     ]
 
 
+class MgLevel(ctypes.Structure):
+    _fields_ = [
+        ("num_cells", c_i32),
+        ("num_blocks", c_i32),
+        ("dims", c_i32),
+        ("dtype", c_i32),
+        ("blocks", c_vp),
+        ("cell_block", c_vp),
+        ("coef", c_vp),
+    ]
+
+
 class SolveInfo(ctypes.Structure):
     _fields_ = [
         ("final_residual", ctypes.c_double),
@@ -156,6 +168,10 @@ SIGNATURES = {
     "pict_refine_residual": (c_i32, [_PD, c_vp, c_vp, c_vp, c_vp, c_vp, c_i32, c_vp, c_vp]),
     "pict_refine_update": (c_i32, [_PD, c_vp, c_vp, c_vp]),
     "pict_refine_finish": (c_i32, [_PD, c_vp, c_vp, c_i32, c_i32, c_vp, c_vp]),
+    "pict_mg_galerkin": (c_i32, [ctypes.POINTER(MgLevel), ctypes.POINTER(MgLevel), c_vp]),
+    "pict_pcg_mg_workspace_bytes": (ctypes.c_int64, [_PD, ctypes.POINTER(MgLevel), c_i32]),
+    "pict_pcg_mg": (c_i32, [_PD, ctypes.POINTER(MgLevel), c_i32, c_vp, c_vp, c_i32, ctypes.c_double, c_i32, c_vp, c_vp,
+                            ctypes.c_int64, ctypes.c_double, ctypes.c_double, c_i32, c_vp]),
     "pict_correct_velocity_grad": (c_i32, [_PD, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "pict_sim_mean_project": (c_i32, [_PD, c_vp, c_vp]),
     "pict_divergence_grad": (c_i32, [_PD, c_vp, c_vp, c_vp, c_vp]),

@@ -1,0 +1,493 @@
+// multigrid.cu -- multigrid-preconditioned CG for the pressure correction solve of the mixed precision
+// step (no counterpart in the reference, whose pressure solve is unpreconditioned CG,
+// extensions/cg_solver_kernel.cu:114-456).
+//
+// Scope: domains whose systems are single blocks with fixed or periodic faces (the batched cavities,
+// the periodic channel and box).  Each level coarsens every block by 2 along each axis (aggregates of
+// up to 2^D cells, ceil(n/2) cells per axis); the coarse operator is the Galerkin product R A P with
+// piecewise-constant prolongation P and R = P^T, computed on the device from the fine stencil.  The
+// V-cycle uses one damped-Jacobi sweep before and after the coarse correction (symmetric), a fixed
+// number of Jacobi sweeps on the coarsest level and a scaled prolongation (aggregation coarse
+// operators are too stiff by about 2).  The constant mode of the singular (Neumann / periodic) block
+// operators is removed on the coarsest level and from every preconditioned residual.  The preconditioned CG runs a fixed number of iterations with
+// per-system scalars; every inner product is reduced per work tile and then per system in a fixed
+// order, so results do not depend on the launch shape.
+#include <cmath>
+#include <cstdio>
+#include "common.cuh"
+#include "launch.h"
+
+namespace pict {
+
+struct MgBlock {
+    int off, sx, sy, sz, px, py, pz, sys;
+};
+
+__device__ __forceinline__ MgBlock mg_block(const pict_mg_level_t& L, int b) {
+    const int* t = L.blocks + 8 * b;
+    return MgBlock{t[0], t[1], t[2], t[3], t[4], t[5], t[6], t[7]};
+}
+
+// neighbour of local cell (x,y,z) across face f inside a block (periodic wrap, -1 at a fixed face)
+__device__ __forceinline__ int mg_nbr(const MgBlock& B, int x, int y, int z, int f) {
+    const int a = f >> 1, up = f & 1;
+    int q[3] = {x, y, z};
+    const int n[3] = {B.sx, B.sy, B.sz};
+    const int per[3] = {B.px, B.py, B.pz};
+    q[a] += up ? 1 : -1;
+    if (q[a] < 0 || q[a] >= n[a]) {
+        if (!per[a]) return -1;
+        q[a] = (q[a] + n[a]) % n[a];
+    }
+    return B.off + q[0] + B.sx * (q[1] + B.sy * q[2]);
+}
+
+__device__ __forceinline__ void mg_unflatten(const MgBlock& B, int l, int& x, int& y, int& z) {
+    x = l % B.sx;
+    const int t = l / B.sx;
+    y = t % B.sy;
+    z = t / B.sy;
+}
+
+// y = A x on a level (stencil rows through the structured neighbours)
+template <typename T, int D>
+__device__ __forceinline__ T mg_apply(const pict_mg_level_t& L, const T* coef, const T* xv, int i, const MgBlock& B,
+                                      int x, int y, int z) {
+    const int N = L.num_cells;
+    T acc = coef[i] * xv[i];
+#pragma unroll
+    for (int f = 0; f < 2 * D; ++f) {
+        const int j = mg_nbr(B, x, y, z, f);
+        if (j >= 0) acc += coef[(size_t)(f + 1) * N + i] * xv[j];
+    }
+    return acc;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Galerkin coarse operator: one thread per coarse cell, summing the couplings of its children
+// ---------------------------------------------------------------------------------------------
+template <typename T, int D>
+__global__ void k_mg_galerkin(pict_mg_level_t F, pict_mg_level_t C) {
+    const T* cf = reinterpret_cast<const T*>(F.coef);
+    T* cc = reinterpret_cast<T*>(C.coef);
+    const int Nc = C.num_cells, Nf = F.num_cells;
+    PICT_CELL_LOOP(I, Nc) {
+        const int b = C.cell_block[I];
+        const MgBlock Bc = mg_block(C, b), Bf = mg_block(F, b);
+        int X, Y, Z;
+        mg_unflatten(Bc, I - Bc.off, X, Y, Z);
+        T diag = 0, off[2 * D];
+#pragma unroll
+        for (int f = 0; f < 2 * D; ++f) off[f] = 0;
+        for (int dz = 0; dz < (D == 3 ? 2 : 1); ++dz)
+            for (int dy = 0; dy < 2; ++dy)
+                for (int dx = 0; dx < 2; ++dx) {
+                    const int x = 2 * X + dx, y = 2 * Y + dy, z = 2 * Z + dz;
+                    if (x >= Bf.sx || y >= Bf.sy || z >= Bf.sz) continue;
+                    const int i = Bf.off + x + Bf.sx * (y + Bf.sy * z);
+                    diag += cf[i];
+#pragma unroll
+                    for (int f = 0; f < 2 * D; ++f) {
+                        const int j = mg_nbr(Bf, x, y, z, f);
+                        if (j < 0) continue;
+                        int xj, yj, zj;
+                        mg_unflatten(Bf, j - Bf.off, xj, yj, zj);
+                        const int J = Bc.off + (xj >> 1) + Bc.sx * ((yj >> 1) + Bc.sy * (zj >> 1));
+                        const T c = cf[(size_t)(f + 1) * Nf + i];
+                        if (J == I) diag += c;
+                        else off[f] += c;
+                    }
+                }
+        cc[I] = diag;
+#pragma unroll
+        for (int f = 0; f < 2 * D; ++f) cc[(size_t)(f + 1) * Nc + I] = off[f];
+    }
+}
+
+// x_out = x_in + w (b - A x_in) / diag   (x_in == nullptr: x_out = w b / diag)
+template <typename T, int D>
+__global__ void k_mg_jacobi(pict_mg_level_t L, const T* bv, const T* xin, T* xout, T w) {
+    const T* coef = reinterpret_cast<const T*>(L.coef);
+    PICT_CELL_LOOP(i, L.num_cells) {
+        const T d = coef[i];
+        const T rd = (d != T(0)) ? w / d : T(0);
+        if (!xin) {
+            xout[i] = rd * bv[i];
+        } else {
+            const MgBlock B = mg_block(L, L.cell_block[i]);
+            int x, y, z;
+            mg_unflatten(B, i - B.off, x, y, z);
+            xout[i] = xin[i] + rd * (bv[i] - mg_apply<T, D>(L, coef, xin, i, B, x, y, z));
+        }
+    }
+}
+
+// b_c = R (b - A x) on the children of each coarse cell
+template <typename T, int D>
+__global__ void k_mg_residual_restrict(pict_mg_level_t F, pict_mg_level_t C, const T* bv, const T* xv, T* bc) {
+    const T* cf = reinterpret_cast<const T*>(F.coef);
+    PICT_CELL_LOOP(I, C.num_cells) {
+        const int b = C.cell_block[I];
+        const MgBlock Bc = mg_block(C, b), Bf = mg_block(F, b);
+        int X, Y, Z;
+        mg_unflatten(Bc, I - Bc.off, X, Y, Z);
+        T acc = 0;
+        for (int dz = 0; dz < (D == 3 ? 2 : 1); ++dz)
+            for (int dy = 0; dy < 2; ++dy)
+                for (int dx = 0; dx < 2; ++dx) {
+                    const int x = 2 * X + dx, y = 2 * Y + dy, z = 2 * Z + dz;
+                    if (x >= Bf.sx || y >= Bf.sy || z >= Bf.sz) continue;
+                    const int i = Bf.off + x + Bf.sx * (y + Bf.sy * z);
+                    acc += bv[i] - mg_apply<T, D>(F, cf, xv, i, Bf, x, y, z);
+                }
+        bc[I] = acc;
+    }
+}
+
+// x_f += s P e_c
+template <typename T, int D>
+__global__ void k_mg_prolong_add(pict_mg_level_t F, pict_mg_level_t C, const T* ec, T* xf, T s) {
+    PICT_CELL_LOOP(i, F.num_cells) {
+        const int b = F.cell_block[i];
+        const MgBlock Bf = mg_block(F, b), Bc = mg_block(C, b);
+        int x, y, z;
+        mg_unflatten(Bf, i - Bf.off, x, y, z);
+        xf[i] += s * ec[Bc.off + (x >> 1) + Bc.sx * ((y >> 1) + Bc.sy * (z >> 1))];
+    }
+}
+
+// remove the mean of every block of a (coarse) level: the constant mode of a singular block operator is
+// not determined and Jacobi sweeps let it grow (one CTA per block)
+template <typename T>
+__global__ void k_mg_block_mean_sub(pict_mg_level_t L, T* x) {
+    __shared__ double s_red[32];
+    __shared__ double s_mean;
+    const MgBlock B = mg_block(L, blockIdx.x);
+    const int n = B.sx * B.sy * B.sz;
+    double acc = 0.0;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) acc += (double)x[B.off + k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double v = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += s_red[w];
+        s_mean = v / (double)n;
+    }
+    __syncthreads();
+    const T m = (T)s_mean;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) x[B.off + k] -= m;
+}
+
+// ---------------------------------------------------------------------------------------------
+// PCG vector kernels on the finest level; per-system scalars in FP64
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ double mg_cta_sum(double v, double* s_red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (threadIdx.x < 32) {
+        r = threadIdx.x < (blockDim.x >> 5) ? s_red[threadIdx.x] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+    }
+    return r;
+}
+
+// q = A p and the tile partial of p.q (one CTA per work tile of the domain)
+template <typename T, int D>
+__global__ void k_pcg_spmv_dot(pict_domain_t dom, pict_mg_level_t L, const T* p, T* q, double* part) {
+    __shared__ double s_red[32];
+    const T* coef = reinterpret_cast<const T*>(L.coef);
+    const int t = blockIdx.x;
+    const int s0 = dom.tiles[4 * t + 2], cnt = dom.tiles[4 * t + 3];
+    const MgBlock B = mg_block(L, dom.tiles[4 * t + 1]);
+    double acc = 0.0;
+    for (int i = s0 + threadIdx.x; i < s0 + cnt; i += blockDim.x) {
+        int x, y, z;
+        mg_unflatten(B, i - B.off, x, y, z);
+        const T qi = mg_apply<T, D>(L, coef, p, i, B, x, y, z);
+        q[i] = qi;
+        acc += (double)p[i] * (double)qi;
+    }
+    acc = mg_cta_sum(acc, s_red);
+    if (threadIdx.x == 0) part[t] = acc;
+}
+
+// tile partial sums of v
+template <typename T>
+__global__ void k_pcg_tile_sum(pict_domain_t dom, const T* v, double* part) {
+    __shared__ double s_red[32];
+    const int t = blockIdx.x;
+    const int s0 = dom.tiles[4 * t + 2], cnt = dom.tiles[4 * t + 3];
+    double a = 0.0;
+    for (int i = s0 + threadIdx.x; i < s0 + cnt; i += blockDim.x) a += (double)v[i];
+    a = mg_cta_sum(a, s_red);
+    if (threadIdx.x == 0) part[t] = a;
+}
+
+// v -= mean of its system (sum of the system's tile partials in order); one CTA per tile
+template <typename T>
+__global__ void k_pcg_sub_mean(pict_domain_t dom, T* v, const double* part) {
+    __shared__ double s_red[32];
+    __shared__ double s_mean;
+    const int t = blockIdx.x;
+    const int sim = dom.tiles[4 * t], s0 = dom.tiles[4 * t + 2], cnt = dom.tiles[4 * t + 3];
+    double a = 0.0;
+    for (int k = dom.sim_tiles[sim] + threadIdx.x; k < dom.sim_tiles[sim + 1]; k += blockDim.x) a += part[k];
+    a = mg_cta_sum(a, s_red);
+    if (threadIdx.x == 0) s_mean = a / (double)(dom.sim_cells[sim + 1] - dom.sim_cells[sim]);
+    __syncthreads();
+    const T m = (T)s_mean;
+    for (int i = s0 + threadIdx.x; i < s0 + cnt; i += blockDim.x) v[i] -= m;
+}
+
+// tile partials of r.z and r.r
+template <typename T>
+__global__ void k_pcg_dot2(pict_domain_t dom, const T* r, const T* z, double* part) {
+    __shared__ double s_red[32];
+    const int t = blockIdx.x;
+    const int s0 = dom.tiles[4 * t + 2], cnt = dom.tiles[4 * t + 3];
+    double a = 0.0, c = 0.0;
+    for (int i = s0 + threadIdx.x; i < s0 + cnt; i += blockDim.x) {
+        const double ri = (double)r[i];
+        a += ri * (double)z[i];
+        c += ri * ri;
+    }
+    a = mg_cta_sum(a, s_red);
+    c = mg_cta_sum(c, s_red);
+    if (threadIdx.x == 0) {
+        part[2 * t] = a;
+        part[2 * t + 1] = c;
+    }
+}
+
+// per-system scalars: stage 0 rho = r.z (and |r|^2);  stage 1 alpha = rho / p.q;
+// stage 2 rho' = r.z, beta = rho'/rho, rho = rho'  (one thread per system, tiles in order)
+// sc[s*4 + {0: rho, 1: alpha, 2: beta, 3: |r|^2}]
+__global__ void k_pcg_scalars(pict_domain_t dom, const double* part, int stride, int stage, double* sc) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= dom.num_sims) return;
+    double a = 0.0, c = 0.0;
+    for (int t = dom.sim_tiles[s]; t < dom.sim_tiles[s + 1]; ++t) {
+        a += part[(size_t)stride * t];
+        if (stride > 1) c += part[(size_t)stride * t + 1];
+    }
+    double* S = sc + 4 * s;
+    if (stage == 0) {
+        S[0] = a;
+        S[3] = c;
+        S[2] = 0.0;
+    } else if (stage == 1) {
+        S[1] = (a != 0.0 && S[0] != 0.0 && isfinite(a)) ? S[0] / a : 0.0;
+    } else {
+        S[2] = (S[0] != 0.0 && isfinite(a)) ? a / S[0] : 0.0;
+        S[0] = a;
+        S[3] = c;
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ int cell_sys(const pict_domain_t& dom, int i) { return dom.blocks[dom.cell_block[i]].sim; }
+
+// x += alpha p, r -= alpha q
+template <typename T>
+__global__ void k_pcg_update_xr(pict_domain_t dom, T* x, T* r, const T* p, const T* q, const double* sc) {
+    PICT_CELL_LOOP(i, dom.num_cells) {
+        const T al = (T)sc[4 * cell_sys<T>(dom, i) + 1];
+        x[i] += al * p[i];
+        r[i] -= al * q[i];
+    }
+}
+
+// p = z + beta p  (init: p = z)
+template <typename T>
+__global__ void k_pcg_update_p(pict_domain_t dom, T* p, const T* z, const double* sc, int init) {
+    PICT_CELL_LOOP(i, dom.num_cells) {
+        const T bt = init ? T(0) : (T)sc[4 * cell_sys<T>(dom, i) + 2];
+        p[i] = z[i] + bt * p[i];
+    }
+}
+
+// r = b (x = 0)
+template <typename T>
+__global__ void k_pcg_init(int N, const T* b, T* r, T* x) {
+    PICT_CELL_LOOP(i, N) {
+        r[i] = b[i];
+        x[i] = T(0);
+    }
+}
+
+__global__ void k_pcg_report(pict_domain_t dom, const double* sc, pict_solve_info_t* info, int iterations, double tol,
+                             int normalized) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= dom.num_sims) return;
+    const int n = dom.sim_cells[s + 1] - dom.sim_cells[s];
+    const double nrm = sqrt(sc[4 * s + 3]);
+    const double crit = normalized ? nrm / sqrt((double)n) : nrm;
+    pict_solve_info_t inf;
+    inf.final_residual = crit;
+    inf.used_iterations = iterations;
+    inf.finite = isfinite(crit) ? 1 : 0;
+    inf.converged = (inf.finite && crit < tol) ? 1 : 0;
+    inf.status = 0;
+    info[s] = inf;
+}
+
+template <typename T>
+static size_t vbytes(int n) { return ((size_t)n * sizeof(T) + 255) & ~(size_t)255; }
+
+// workspace: per level x0, x1, b (levels >= 1; level 0: x0, x1) | r, z, p, q | partials | scalars
+template <typename T, int D>
+static pict_status_t run_pcg_mg(const pict_domain_t* dom, const pict_mg_level_t* levels, int nl, const T* rhs, T* xout,
+                                int iterations, double tol, int normalized, pict_solve_info_t* info, char* ws,
+                                int64_t ws_bytes, double omega, double scale, int coarse_sweeps, cudaStream_t st) {
+    const int N = dom->num_cells;
+    // carve the workspace
+    char* w = ws;
+    T* lx0[16];
+    T* lx1[16];
+    T* lb[16];
+    for (int l = 0; l < nl; ++l) {
+        const int n = levels[l].num_cells;
+        lx0[l] = reinterpret_cast<T*>(w); w += vbytes<T>(n);
+        lx1[l] = reinterpret_cast<T*>(w); w += vbytes<T>(n);
+        lb[l] = reinterpret_cast<T*>(w); w += vbytes<T>(n);
+    }
+    T* r = reinterpret_cast<T*>(w); w += vbytes<T>(N);
+    T* z = reinterpret_cast<T*>(w); w += vbytes<T>(N);
+    T* p = reinterpret_cast<T*>(w); w += vbytes<T>(N);
+    T* q = reinterpret_cast<T*>(w); w += vbytes<T>(N);
+    double* part = reinterpret_cast<double*>(w); w += ((size_t)2 * dom->num_tiles * 8 + 255) & ~(size_t)255;
+    double* sc = reinterpret_cast<double*>(w); w += ((size_t)4 * dom->num_sims * 8 + 255) & ~(size_t)255;
+    if ((int64_t)(w - ws) > ws_bytes) return set_error(PICT_ERR_ARG, "pcg_mg: workspace too small");
+
+    auto grid_of = [](int n) { return cell_grid(n, 256); };
+    const T wj = (T)omega, sp = (T)scale;
+    // z = M r (V-cycle); r is the finest right-hand side
+    auto vcycle = [&](const T* rhs0, T* z0) -> pict_status_t {
+        const T* b = rhs0;
+        for (int l = 0; l < nl; ++l) {
+            const pict_mg_level_t& L = levels[l];
+            if (l > 0) b = lb[l];
+            if (l == nl - 1) {
+                // coarsest: Jacobi sweeps from zero (ping-pong), result in lx0
+                k_mg_jacobi<T, D><<<grid_of(L.num_cells), 256, 0, st>>>(L, b, nullptr, lx0[l], wj);
+                for (int k = 1; k < coarse_sweeps; ++k) {
+                    T* src = (k & 1) ? lx0[l] : lx1[l];
+                    T* dst = (k & 1) ? lx1[l] : lx0[l];
+                    k_mg_jacobi<T, D><<<grid_of(L.num_cells), 256, 0, st>>>(L, b, src, dst, wj);
+                }
+                if ((coarse_sweeps & 1) == 0)  // last result in lx1: copy back
+                    cudaMemcpyAsync(lx0[l], lx1[l], sizeof(T) * L.num_cells, cudaMemcpyDeviceToDevice, st);
+                k_mg_block_mean_sub<T><<<L.num_blocks, 64, 0, st>>>(L, lx0[l]);
+                break;
+            }
+            k_mg_jacobi<T, D><<<grid_of(L.num_cells), 256, 0, st>>>(L, b, nullptr, lx0[l], wj);
+            k_mg_residual_restrict<T, D><<<grid_of(levels[l + 1].num_cells), 256, 0, st>>>(L, levels[l + 1], b, lx0[l], lb[l + 1]);
+        }
+        for (int l = nl - 2; l >= 0; --l) {
+            const pict_mg_level_t& L = levels[l];
+            const T* bl = (l == 0) ? rhs0 : lb[l];
+            k_mg_prolong_add<T, D><<<grid_of(L.num_cells), 256, 0, st>>>(L, levels[l + 1], lx0[l + 1], lx0[l], sp);
+            T* dst = (l == 0) ? z0 : lx1[l];
+            k_mg_jacobi<T, D><<<grid_of(L.num_cells), 256, 0, st>>>(L, bl, lx0[l], dst, wj);
+            if (l > 0) cudaMemcpyAsync(lx0[l], lx1[l], sizeof(T) * L.num_cells, cudaMemcpyDeviceToDevice, st);
+        }
+        if (nl == 1) cudaMemcpyAsync(z0, lx0[0], sizeof(T) * N, cudaMemcpyDeviceToDevice, st);
+        // the preconditioned residual of a singular system: keep it mean-free
+        k_pcg_tile_sum<T><<<dom->num_tiles, 256, 0, st>>>(*dom, z0, part);
+        k_pcg_sub_mean<T><<<dom->num_tiles, 256, 0, st>>>(*dom, z0, part);
+        return check_launch("pcg_mg vcycle");
+    };
+
+    const int nt = dom->num_tiles;
+    const int sg = (dom->num_sims + 127) / 128;
+    k_pcg_init<T><<<grid_of(N), 256, 0, st>>>(N, rhs, r, xout);
+    pict_status_t s = vcycle(r, z);
+    if (s) return s;
+    k_pcg_dot2<T><<<nt, 256, 0, st>>>(*dom, r, z, part);
+    k_pcg_scalars<<<sg, 128, 0, st>>>(*dom, part, 2, 0, sc);
+    k_pcg_update_p<T><<<grid_of(N), 256, 0, st>>>(*dom, p, z, sc, 1);
+    for (int it = 0; it < iterations; ++it) {
+        k_pcg_spmv_dot<T, D><<<nt, 256, 0, st>>>(*dom, levels[0], p, q, part);
+        k_pcg_scalars<<<sg, 128, 0, st>>>(*dom, part, 1, 1, sc);
+        k_pcg_update_xr<T><<<grid_of(N), 256, 0, st>>>(*dom, xout, r, p, q, sc);
+        s = vcycle(r, z);
+        if (s) return s;
+        k_pcg_dot2<T><<<nt, 256, 0, st>>>(*dom, r, z, part);
+        k_pcg_scalars<<<sg, 128, 0, st>>>(*dom, part, 2, 2, sc);
+        if (it + 1 < iterations) k_pcg_update_p<T><<<grid_of(N), 256, 0, st>>>(*dom, p, z, sc, 0);
+    }
+    k_pcg_report<<<sg, 128, 0, st>>>(*dom, sc, info, iterations, tol, normalized);
+    return check_launch("pcg_mg");
+}
+
+}  // namespace pict
+
+using namespace pict;
+
+extern "C" {
+
+pict_status_t pict_mg_galerkin(const pict_mg_level_t* fine, const pict_mg_level_t* coarse, void* stream) {
+    if (!fine || !coarse || !fine->coef || !coarse->coef || !fine->blocks || !coarse->blocks || !coarse->cell_block)
+        return set_error(PICT_ERR_ARG, "mg_galerkin: NULL argument");
+    if (fine->num_blocks != coarse->num_blocks || fine->dims != coarse->dims || fine->dtype != coarse->dtype)
+        return set_error(PICT_ERR_ARG, "mg_galerkin: level mismatch");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int grid = cell_grid(coarse->num_cells, 256);
+    if (fine->dtype == PICT_F32) {
+        if (fine->dims == 2) k_mg_galerkin<float, 2><<<grid, 256, 0, st>>>(*fine, *coarse);
+        else k_mg_galerkin<float, 3><<<grid, 256, 0, st>>>(*fine, *coarse);
+    } else {
+        if (fine->dims == 2) k_mg_galerkin<double, 2><<<grid, 256, 0, st>>>(*fine, *coarse);
+        else k_mg_galerkin<double, 3><<<grid, 256, 0, st>>>(*fine, *coarse);
+    }
+    return check_launch("mg_galerkin");
+}
+
+int64_t pict_pcg_mg_workspace_bytes(const pict_domain_t* dom, const pict_mg_level_t* levels, int32_t num_levels) {
+    if (!dom || !levels || num_levels < 1 || num_levels > 16) return -1;
+    const size_t esz = dom->dtype == PICT_F64 ? 8 : 4;
+    auto vb = [&](int n) { return ((size_t)n * esz + 255) & ~(size_t)255; };
+    size_t b = 0;
+    for (int l = 0; l < num_levels; ++l) b += 3 * vb(levels[l].num_cells);
+    b += 4 * vb(dom->num_cells);
+    b += ((size_t)2 * dom->num_tiles * 8 + 255) & ~(size_t)255;
+    b += ((size_t)4 * dom->num_sims * 8 + 255) & ~(size_t)255;
+    return (int64_t)b;
+}
+
+pict_status_t pict_pcg_mg(const pict_domain_t* dom, const pict_mg_level_t* levels, int32_t num_levels, const void* rhs,
+                          void* x, int32_t iterations, double tolerance, int32_t convergence, void* info_out,
+                          void* workspace, int64_t workspace_bytes, double omega, double prolong_scale,
+                          int32_t coarse_sweeps, void* stream) {
+    if (!dom || !levels || !rhs || !x || !info_out || !workspace) return set_error(PICT_ERR_ARG, "pcg_mg: NULL argument");
+    if (num_levels < 1 || num_levels > 16 || iterations < 0 || coarse_sweeps < 1)
+        return set_error(PICT_ERR_ARG, "pcg_mg: bad level count / iterations / sweeps");
+    if (levels[0].num_cells != dom->num_cells || levels[0].num_blocks != dom->num_blocks || !dom->tiles ||
+        dom->num_tiles <= 0)
+        return set_error(PICT_ERR_ARG, "pcg_mg: level 0 must describe the domain (and tiles are needed)");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int norm = convergence == PICT_CONV_NORM2_NORMALIZED;
+    char* ws = reinterpret_cast<char*>(workspace);
+    pict_solve_info_t* info = reinterpret_cast<pict_solve_info_t*>(info_out);
+    if (dom->dtype == PICT_F32) {
+        if (dom->dims == 2)
+            return run_pcg_mg<float, 2>(dom, levels, num_levels, (const float*)rhs, (float*)x, iterations, tolerance, norm,
+                                        info, ws, workspace_bytes, omega, prolong_scale, coarse_sweeps, st);
+        return run_pcg_mg<float, 3>(dom, levels, num_levels, (const float*)rhs, (float*)x, iterations, tolerance, norm,
+                                    info, ws, workspace_bytes, omega, prolong_scale, coarse_sweeps, st);
+    }
+    if (dom->dims == 2)
+        return run_pcg_mg<double, 2>(dom, levels, num_levels, (const double*)rhs, (double*)x, iterations, tolerance, norm,
+                                     info, ws, workspace_bytes, omega, prolong_scale, coarse_sweeps, st);
+    return run_pcg_mg<double, 3>(dom, levels, num_levels, (const double*)rhs, (double*)x, iterations, tolerance, norm,
+                                 info, ws, workspace_bytes, omega, prolong_scale, coarse_sweeps, st);
+}
+
+}  // extern "C"

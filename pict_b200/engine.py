@@ -24,6 +24,7 @@ capturable (:meth:`capture`).
 from __future__ import annotations
 
 import ctypes
+import warnings
 from typing import Optional
 
 import torch
@@ -46,7 +47,8 @@ class PISOStepper:
     def __init__(self, domain, time_step=None, corrector_steps: int = 2, advection_tol: Optional[float] = None,
                  pressure_tol: Optional[float] = None, max_iterations: int = 5000, adv_group_size: int = 0,
                  p_group_size: int = 0, threads: int = 0, normalize_pressure: bool = True, cg_variant: int = 1,
-                 pressure_refine: int = 0, refine_tol: Optional[float] = None, warm_start_pressure: bool = False):
+                 pressure_refine: int = 0, refine_tol: Optional[float] = None, warm_start_pressure: bool = False,
+                 refine_solver: str = "cg", mg_iterations: int = 12):
         self.domain = domain
         self.dims = domain.getSpatialDims()
         self.corrector_steps = int(corrector_steps)
@@ -71,6 +73,11 @@ class PISOStepper:
                                         subtract_mean=normalize_pressure and not refine,
                                         write_block_pressure=not refine, group_size=p_group_size, threads=threads,
                                         variant=cg_variant)
+        # correction solves of the refinement: "cg" (persistent CG) or "mg" (multigrid-preconditioned CG,
+        # single-block systems only; falls back to "cg" otherwise)
+        self.refine_solver = refine_solver
+        self.mg_iterations = int(mg_iterations)
+        self._mg = None
         self.r_params = P._solve_params(1, self.max_iterations, self.refine_tol, _lib.PICT_CONV_NORM2_NORMALIZED, False,
                                         False, x_zero=True, group_size=p_group_size, threads=threads,
                                         variant=cg_variant)
@@ -105,6 +112,14 @@ class PISOStepper:
             self._res = torch.zeros(N, dtype=d.getDtype(), device=dev)
             self._corr = torch.zeros(N, dtype=d.getDtype(), device=dev)
             self._tile_scratch = torch.zeros(max(1, self.desc.num_tiles), dtype=torch.float64, device=dev)
+            if self.refine_solver == "mg":
+                from .multigrid import hierarchy_for
+                try:
+                    self._mg = hierarchy_for(d)
+                    self._mg_ws = torch.empty(self._mg.workspace_bytes(self.desc), dtype=torch.uint8, device=dev)
+                except ValueError as e:
+                    warnings.warn("multigrid refinement not available (%s); using CG" % e)
+                    self._mg = None
         ws = max(lib.pict_solve_workspace_bytes(ctypes.byref(self.desc), ctypes.byref(self.adv_params)),
                  lib.pict_solve_workspace_bytes(ctypes.byref(self.desc), ctypes.byref(self.p_params)),
                  lib.pict_solve_workspace_bytes(ctypes.byref(self.desc), ctypes.byref(self.r_params)))
@@ -165,9 +180,15 @@ class PISOStepper:
                                            int(self.normalize_pressure), ctypes.c_void_p(self._tile_scratch.data_ptr()),
                                            st), "refine residual")
             a = ev() if ev else None
-            check(lib.pict_solve(desc, P._ptr(d.P.coef), P._ptr(self._res), P._ptr(self._corr),
-                                 ctypes.byref(self.r_params), P._ptr(self.info_r[k][m]), P._ptr(self.ws),
-                                 self.ws_bytes, st), "refinement solve")
+            if self._mg is not None:
+                if k == 0 and m == 0:  # the pressure matrix is assembled once per step
+                    self._mg.setup(d.P.coef, st)
+                self._mg.solve(self.desc, self._res, self._corr, self.mg_iterations, self.refine_tol, self.info_r[k][m],
+                               self._mg_ws, st)
+            else:
+                check(lib.pict_solve(desc, P._ptr(d.P.coef), P._ptr(self._res), P._ptr(self._corr),
+                                     ctypes.byref(self.r_params), P._ptr(self.info_r[k][m]), P._ptr(self.ws),
+                                     self.ws_bytes, st), "refinement solve")
             if events is not None:
                 events.append((a, ev(), self.info_r[k][m].clone()))
             check(lib.pict_refine_update(desc, x64, P._ptr(self._corr), st), "refine update")
@@ -180,8 +201,15 @@ class PISOStepper:
         refinement sweeps when enabled."""
         n = 1 + 3
         n += self.corrector_steps * (2 + 3 + 1)
-        if self.pressure_refine > 0:  # per sweep: residual (+2 projection), solve (3), update; partials + finish
-            per = 5 + (2 if self.normalize_pressure else 0)
+        if self.pressure_refine > 0:  # per sweep: residual (+2 projection), solve, update; partials + finish
+            if self._mg is not None:
+                nl, cs, it = self._mg.num_levels, 8, self.mg_iterations
+                v = 4 * (nl - 1) + cs + 1 + 2
+                solve = 1 + v + 3 + it * (6 + v) - 1 + 1
+                n += nl - 1  # Galerkin coarse operators once per step
+            else:
+                solve = 3
+            per = 2 + solve + (2 if self.normalize_pressure else 0)
             n += self.corrector_steps * (per * self.pressure_refine + (2 if self.normalize_pressure else 1))
         if self.corrector_steps == 0:
             n += 1

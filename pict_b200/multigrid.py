@@ -1,0 +1,113 @@
+"""Multigrid hierarchy of a (batched) domain for the multigrid-preconditioned CG of ``libpict_b200``.
+
+Eligible domains: every system is one block whose faces are fixed or periodic (no connections).
+Level l+1 coarsens every block of level l by two along each axis (ceil(n/2) cells, sizes of 1 stay
+1) until every block has at most 4 cells along each axis.  The block tables and cell-to-block maps
+are built once on the host; the coarse stencils are recomputed on the device (Galerkin product)
+whenever the finest matrix changes.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import List, Optional
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import MgLevel, check
+
+MAX_LEVELS = 16
+
+
+def eligible(host_blocks, num_blocks, dims, sim_of_block) -> Optional[str]:
+    """None if a multigrid hierarchy can be built, else the reason."""
+    seen = set()
+    for b in range(num_blocks):
+        B = host_blocks[b]
+        if B.sim in seen:
+            return "a system has more than one block"
+        seen.add(B.sim)
+        for f in range(2 * dims):
+            if B.face[f].type == _lib.PICT_FACE_CONNECTED:
+                return "connected block faces"
+    return None
+
+
+class MGHierarchy:
+    def __init__(self, host_blocks, num_blocks: int, dims: int, dtype, device, cell_block_dev: torch.Tensor,
+                 min_size: int = 4):
+        why = eligible(host_blocks, num_blocks, dims, None)
+        if why is not None:
+            raise ValueError("multigrid not applicable: " + why)
+        self.dims = dims
+        self.K = 2 * dims + 1
+        self.dtype = dtype
+        self.device = device
+        code = _lib.PICT_F64 if dtype == torch.float64 else _lib.PICT_F32
+        sizes = np.array([[host_blocks[b].size[a] for a in range(3)] for b in range(num_blocks)], dtype=np.int64)
+        per = np.array([[1 if (host_blocks[b].face[2 * a].type == _lib.PICT_FACE_PERIODIC) else 0 for a in range(3)]
+                        for b in range(num_blocks)], dtype=np.int64)
+        per[:, dims:] = 0
+        sims = np.array([host_blocks[b].sim for b in range(num_blocks)], dtype=np.int64)
+        self.levels_py = []   # keep tensors alive
+        levels = []
+        for lvl in range(MAX_LEVELS):
+            n = sizes.prod(axis=1)
+            offs = np.concatenate([[0], np.cumsum(n)[:-1]])
+            table = np.zeros((num_blocks, 8), dtype=np.int32)
+            table[:, 0] = offs
+            table[:, 1:4] = sizes
+            table[:, 4:7] = per
+            table[:, 7] = sims
+            blocks_t = torch.tensor(table.reshape(-1), dtype=torch.int32, device=device)
+            if lvl == 0:
+                cb = cell_block_dev
+                coef = None
+            else:
+                cb = torch.tensor(np.repeat(np.arange(num_blocks, dtype=np.int32), n), dtype=torch.int32, device=device)
+                coef = torch.zeros(self.K * int(n.sum()), dtype=dtype, device=device)
+            L = MgLevel()
+            L.num_cells = int(n.sum())
+            L.num_blocks = num_blocks
+            L.dims = dims
+            L.dtype = code
+            L.blocks = blocks_t.data_ptr()
+            L.cell_block = cb.data_ptr()
+            L.coef = coef.data_ptr() if coef is not None else None
+            levels.append(L)
+            self.levels_py.append((blocks_t, cb, coef))
+            if (sizes[:, :dims] <= min_size).all():
+                break
+            sizes = np.where(sizes > 1, (sizes + 1) // 2, 1)
+        self.num_levels = len(levels)
+        self.levels = (MgLevel * self.num_levels)(*levels)
+        self.cells = [int(L.num_cells) for L in levels]
+
+    def setup(self, fine_coef: torch.Tensor, stream):
+        """Point level 0 at the finest stencil and recompute every coarse stencil."""
+        self.levels[0].coef = fine_coef.data_ptr()
+        lib = _lib.load()
+        for l in range(self.num_levels - 1):
+            check(lib.pict_mg_galerkin(ctypes.byref(self.levels[l]), ctypes.byref(self.levels[l + 1]), stream),
+                  "mg galerkin")
+
+    def workspace_bytes(self, desc) -> int:
+        return int(_lib.load().pict_pcg_mg_workspace_bytes(ctypes.byref(desc), self.levels, self.num_levels))
+
+    def solve(self, desc, rhs: torch.Tensor, x: torch.Tensor, iterations: int, tol: float, info: torch.Tensor,
+              ws: torch.Tensor, stream, omega: float = 0.8, prolong_scale: float = 2.0, coarse_sweeps: int = 8):
+        check(_lib.load().pict_pcg_mg(ctypes.byref(desc), self.levels, self.num_levels, ctypes.c_void_p(rhs.data_ptr()),
+                                      ctypes.c_void_p(x.data_ptr()), int(iterations), float(tol),
+                                      _lib.PICT_CONV_NORM2_NORMALIZED, ctypes.c_void_p(info.data_ptr()),
+                                      ctypes.c_void_p(ws.data_ptr()), ws.numel(), float(omega), float(prolong_scale),
+                                      int(coarse_sweeps), stream), "pcg mg")
+
+
+def hierarchy_for(domain) -> MGHierarchy:
+    """Build the hierarchy of a prepared Domain or BatchDomain (raises ValueError if not eligible)."""
+    host = domain._host_blocks if hasattr(domain, "_host_blocks") and not callable(domain._host_blocks) else None
+    if host is None:
+        host = domain._pack_blocks()
+    nb = len(domain.getBlocks())
+    return MGHierarchy(host, nb, domain.getSpatialDims(), domain.getDtype(), domain.getDevice(), domain._cell_block)

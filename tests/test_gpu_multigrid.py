@@ -1,0 +1,145 @@
+"""Multigrid-preconditioned CG (GPU): Galerkin coarse operators against R A R^T assembled with SciPy,
+convergence of the batched preconditioned CG, and the mixed-precision step with multigrid correction
+solves against the FP64 oracle."""
+import ctypes
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import torch
+
+import piso_oracle as po
+from setups import build_oracle, build_product, case, lid_cavity
+
+pytestmark = pytest.mark.gpu
+
+
+def _stencil_matrix(coef, blocks, dims):
+    """SciPy matrix of a level stencil (structured neighbours, periodic wrap)."""
+    K = 2 * dims + 1
+    N = coef.size // K
+    coef = coef.reshape(K, N)
+    rows, cols, vals = [], [], []
+    for (off, sx, sy, sz, px, py, pz, _s) in blocks:
+        n = (sx, sy, sz)
+        per = (px, py, pz)
+        for l in range(sx * sy * sz):
+            q = [l % sx, (l // sx) % sy, l // (sx * sy)]
+            i = off + l
+            rows.append(i); cols.append(i); vals.append(coef[0, i])
+            for f in range(2 * dims):
+                a = f >> 1
+                qq = list(q)
+                qq[a] += 1 if f & 1 else -1
+                if qq[a] < 0 or qq[a] >= n[a]:
+                    if not per[a]:
+                        continue
+                    qq[a] %= n[a]
+                j = off + qq[0] + sx * (qq[1] + sy * qq[2])
+                rows.append(i); cols.append(j); vals.append(coef[f + 1, i])
+    return sp.csr_matrix((vals, (rows, cols)), shape=(N, N))
+
+
+def _aggregation(fine_blocks, coarse_blocks):
+    rows, cols = [], []
+    for fb, cb in zip(fine_blocks, coarse_blocks):
+        off, sx, sy, sz = fb[:4]
+        coff, csx, csy = cb[0], cb[1], cb[2]
+        for l in range(sx * sy * sz):
+            x, y, z = l % sx, (l // sx) % sy, l // (sx * sy)
+            rows.append(coff + (x >> 1) + csx * ((y >> 1) + csy * (z >> 1)))
+            cols.append(off + l)
+    nf = sum(b[1] * b[2] * b[3] for b in fine_blocks)
+    nc = sum(b[1] * b[2] * b[3] for b in coarse_blocks)
+    return sp.csr_matrix((np.ones(len(rows)), (rows, cols)), shape=(nc, nf))
+
+
+def _prepared_batch(dtype, sides=(13, 20, 9)):
+    from pict_b200 import PISOtorch as P
+    from pict_b200.batch import BatchDomain
+    doms = [build_product(lid_cavity(n, viscosity=1e-3), dtype) for n in sides]
+    b = BatchDomain(doms, time_steps=[0.5 / n for n in sides])
+    from pict_b200.engine import PISOStepper
+    st = PISOStepper(b, time_step=0.01, advection_tol=1e-8, pressure_tol=1e-8)
+    st.step()
+    torch.cuda.synchronize()
+    return b, st
+
+
+def test_galerkin_matches_scipy():
+    from pict_b200.multigrid import hierarchy_for
+    b, st = _prepared_batch(torch.float64)
+    mg = hierarchy_for(b)
+    assert mg.num_levels >= 3
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    mg.setup(b.P.coef, s)
+    torch.cuda.synchronize()
+    tables = [t[0].cpu().numpy().reshape(-1, 8) for t in mg.levels_py]
+    A = _stencil_matrix(b.P.coef.cpu().numpy().reshape(-1), tables[0], 2)
+    for l in range(1, mg.num_levels):
+        R = _aggregation(tables[l - 1], tables[l])
+        Ac_ref = (R @ A @ R.T).toarray()
+        Ac = _stencil_matrix(mg.levels_py[l][2].cpu().numpy(), tables[l], 2).toarray()
+        assert np.abs(Ac - Ac_ref).max() <= 1e-12 * np.abs(Ac_ref).max()
+        A = sp.csr_matrix(Ac_ref)
+
+
+def test_pcg_mg_reduces_residual_like_cg():
+    from pict_b200 import PISOtorch as P
+    from pict_b200.multigrid import hierarchy_for
+    b, st = _prepared_batch(torch.float32, sides=(64, 48, 100, 37))
+    mg = hierarchy_for(b)
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    mg.setup(b.P.coef, s)
+    g = torch.Generator(device="cpu").manual_seed(4)
+    rhs = torch.randn(b.getTotalSize(), generator=g).cuda()
+    # mean-free per system
+    sc = b._sim_cells.cpu().numpy()
+    for k in range(len(sc) - 1):
+        rhs[sc[k]:sc[k + 1]] -= rhs[sc[k]:sc[k + 1]].mean()
+    x = torch.zeros_like(rhs)
+    info = torch.zeros(b.num_sims * 24, dtype=torch.uint8, device="cuda")
+    ws = torch.empty(mg.workspace_bytes(b._desc), dtype=torch.uint8, device="cuda")
+    mg.solve(b._desc, rhs, x, 12, 1e-30, info, ws, s)
+    infos = P.decode_infos(info)
+    # true residual of the result, in FP64
+    from pict_b200 import _lib
+    r_true = torch.zeros_like(rhs)
+    x64 = torch.zeros(rhs.numel(), dtype=torch.float64, device="cuda")
+    _lib.check(_lib.load().pict_refine_residual(ctypes.byref(b._desc), b.P.coef.data_ptr(), rhs.data_ptr(), x.data_ptr(),
+                                                ctypes.c_void_p(x64.data_ptr()), r_true.data_ptr(), 0, None, s), "residual")
+    # plain CG with the same budget of 12 iterations, for comparison
+    x_cg = torch.zeros_like(rhs)
+    prm = P._solve_params(1, 12, 1e-30, 1, False, False, x_zero=True)
+    cg_infos = P.decode_infos(P.solve_stencil(b, b.P.coef, rhs, x_cg, prm))
+    torch.cuda.synchronize()
+    for k in range(len(sc) - 1):
+        n = sc[k + 1] - sc[k]
+        r0 = float(rhs[sc[k]:sc[k + 1]].double().norm()) / np.sqrt(n)
+        assert infos[k].finalResidual < 1e-4 * r0, (k, infos[k], r0)
+        rt = float(r_true[sc[k]:sc[k + 1]].double().norm()) / np.sqrt(n)
+        assert rt < 1e-3 * r0, (k, rt, r0)
+        assert infos[k].finalResidual < 0.01 * cg_infos[k].finalResidual
+
+
+def test_refined_step_with_multigrid_within_1e5_of_fp64_oracle():
+    from pict_b200.batch import BatchDomain
+    from pict_b200.engine import PISOStepper
+    specs = [lid_cavity(32, viscosity=1.0 / 1500.0), lid_cavity(33, viscosity=1.0 / 800.0)]
+    doms = [build_product(s_, torch.float32) for s_ in specs]
+    b = BatchDomain(doms, time_steps=[0.5 / 32, 0.5 / 33])
+    st = PISOStepper(b, time_step=0.01, advection_tol=1e-6, pressure_tol=1e-6, pressure_refine=1, refine_tol=1e-9,
+                     warm_start_pressure=True, refine_solver="mg", mg_iterations=10)
+    assert st._mg is not None
+    for _ in range(10):
+        st.step()
+        st.check()
+    for s_, n, d in zip(specs, (32, 33), doms):
+        od = build_oracle(s_)
+        for _ in range(10):
+            po.piso_step(od, 0.5 / n, adv_tol=1e-12, p_tol=1e-12)
+        u = d.getBlock(0).velocity.double().cpu().numpy().reshape(2, -1)
+        p = d.getBlock(0).pressure.double().cpu().numpy().reshape(-1)
+        ur, pr = od.velocity_global(), od.pressure_global()
+        assert np.abs(u - ur).max() / np.abs(ur).max() < 1e-5
+        assert np.abs(p - pr).max() / np.abs(pr).max() < 1e-5
