@@ -9,7 +9,8 @@
 // V-cycle uses one damped-Jacobi sweep before and after the coarse correction (symmetric), a fixed
 // number of Jacobi sweeps on the coarsest level and a scaled prolongation (aggregation coarse
 // operators are too stiff by about 2).  The constant mode of the singular (Neumann / periodic) block
-// operators is removed on the coarsest level and from every preconditioned residual.  The preconditioned CG runs a fixed number of iterations with
+// operators is removed on the coarsest level and from every preconditioned residual (folded into the
+// inner products and the search-direction update).  The preconditioned CG runs a fixed number of iterations with
 // per-system scalars; every inner product is reduced per work tile and then per system in a fixed
 // order, so results do not depend on the launch shape.
 #include <cmath>
@@ -156,28 +157,56 @@ __global__ void k_mg_prolong_add(pict_mg_level_t F, pict_mg_level_t C, const T* 
     }
 }
 
-// remove the mean of every block of a (coarse) level: the constant mode of a singular block operator is
-// not determined and Jacobi sweeps let it grow (one CTA per block)
-template <typename T>
-__global__ void k_mg_block_mean_sub(pict_mg_level_t L, T* x) {
+// coarsest level: `sweeps` damped-Jacobi sweeps from zero and mean removal, one CTA per block with the
+// iterate in shared memory (coarsest blocks hold at most MG_COARSE_MAX cells)
+constexpr int MG_COARSE_MAX = 256;
+
+template <typename T, int D>
+__global__ void k_mg_coarse_solve(pict_mg_level_t L, const T* bv, T* xout, T w, int sweeps) {
+    __shared__ T s_x[2][MG_COARSE_MAX];
     __shared__ double s_red[32];
     __shared__ double s_mean;
+    const T* coef = reinterpret_cast<const T*>(L.coef);
+    const int N = L.num_cells;
     const MgBlock B = mg_block(L, blockIdx.x);
     const int n = B.sx * B.sy * B.sz;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        const T d = coef[B.off + k];
+        s_x[0][k] = (d != T(0)) ? w * bv[B.off + k] / d : T(0);
+    }
+    __syncthreads();
+    int cur = 0;
+    for (int it = 1; it < sweeps; ++it) {
+        for (int k = threadIdx.x; k < n; k += blockDim.x) {
+            const int i = B.off + k;
+            int x, y, z;
+            mg_unflatten(B, k, x, y, z);
+            T acc = coef[i] * s_x[cur][k];
+#pragma unroll
+            for (int f = 0; f < 2 * D; ++f) {
+                const int j = mg_nbr(B, x, y, z, f);
+                if (j >= 0) acc += coef[(size_t)(f + 1) * N + i] * s_x[cur][j - B.off];
+            }
+            const T d = coef[i];
+            s_x[cur ^ 1][k] = s_x[cur][k] + ((d != T(0)) ? w * (bv[i] - acc) / d : T(0));
+        }
+        __syncthreads();
+        cur ^= 1;
+    }
     double acc = 0.0;
-    for (int k = threadIdx.x; k < n; k += blockDim.x) acc += (double)x[B.off + k];
+    for (int k = threadIdx.x; k < n; k += blockDim.x) acc += (double)s_x[cur][k];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = acc;
     __syncthreads();
     if (threadIdx.x == 0) {
         double v = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += s_red[w];
+        for (int wv = 0; wv < (int)(blockDim.x >> 5); ++wv) v += s_red[wv];
         s_mean = v / (double)n;
     }
     __syncthreads();
     const T m = (T)s_mean;
-    for (int k = threadIdx.x; k < n; k += blockDim.x) x[B.off + k] -= m;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) xout[B.off + k] = s_x[cur][k] - m;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -218,77 +247,68 @@ __global__ void k_pcg_spmv_dot(pict_domain_t dom, pict_mg_level_t L, const T* p,
     if (threadIdx.x == 0) part[t] = acc;
 }
 
-// tile partial sums of v
+// tile partials of r.z, r.r, sum(z), sum(r)
 template <typename T>
-__global__ void k_pcg_tile_sum(pict_domain_t dom, const T* v, double* part) {
+__global__ void k_pcg_dot4(pict_domain_t dom, const T* r, const T* z, double* part) {
     __shared__ double s_red[32];
     const int t = blockIdx.x;
     const int s0 = dom.tiles[4 * t + 2], cnt = dom.tiles[4 * t + 3];
-    double a = 0.0;
-    for (int i = s0 + threadIdx.x; i < s0 + cnt; i += blockDim.x) a += (double)v[i];
-    a = mg_cta_sum(a, s_red);
-    if (threadIdx.x == 0) part[t] = a;
-}
-
-// v -= mean of its system (sum of the system's tile partials in order); one CTA per tile
-template <typename T>
-__global__ void k_pcg_sub_mean(pict_domain_t dom, T* v, const double* part) {
-    __shared__ double s_red[32];
-    __shared__ double s_mean;
-    const int t = blockIdx.x;
-    const int sim = dom.tiles[4 * t], s0 = dom.tiles[4 * t + 2], cnt = dom.tiles[4 * t + 3];
-    double a = 0.0;
-    for (int k = dom.sim_tiles[sim] + threadIdx.x; k < dom.sim_tiles[sim + 1]; k += blockDim.x) a += part[k];
-    a = mg_cta_sum(a, s_red);
-    if (threadIdx.x == 0) s_mean = a / (double)(dom.sim_cells[sim + 1] - dom.sim_cells[sim]);
-    __syncthreads();
-    const T m = (T)s_mean;
-    for (int i = s0 + threadIdx.x; i < s0 + cnt; i += blockDim.x) v[i] -= m;
-}
-
-// tile partials of r.z and r.r
-template <typename T>
-__global__ void k_pcg_dot2(pict_domain_t dom, const T* r, const T* z, double* part) {
-    __shared__ double s_red[32];
-    const int t = blockIdx.x;
-    const int s0 = dom.tiles[4 * t + 2], cnt = dom.tiles[4 * t + 3];
-    double a = 0.0, c = 0.0;
+    double a = 0.0, c = 0.0, sz = 0.0, sr = 0.0;
     for (int i = s0 + threadIdx.x; i < s0 + cnt; i += blockDim.x) {
-        const double ri = (double)r[i];
-        a += ri * (double)z[i];
+        const double ri = (double)r[i], zi = (double)z[i];
+        a += ri * zi;
         c += ri * ri;
+        sz += zi;
+        sr += ri;
     }
     a = mg_cta_sum(a, s_red);
     c = mg_cta_sum(c, s_red);
+    sz = mg_cta_sum(sz, s_red);
+    sr = mg_cta_sum(sr, s_red);
     if (threadIdx.x == 0) {
-        part[2 * t] = a;
-        part[2 * t + 1] = c;
+        part[4 * t] = a;
+        part[4 * t + 1] = c;
+        part[4 * t + 2] = sz;
+        part[4 * t + 3] = sr;
     }
 }
 
-// per-system scalars: stage 0 rho = r.z (and |r|^2);  stage 1 alpha = rho / p.q;
-// stage 2 rho' = r.z, beta = rho'/rho, rho = rho'  (one thread per system, tiles in order)
-// sc[s*4 + {0: rho, 1: alpha, 2: beta, 3: |r|^2}]
+// per-system scalars (one warp per system, tiles summed lane-strided in a fixed order):
+// stage 0: rho = r.(z - m), |r|^2, m = mean(z);  stage 1: alpha = rho / p.q;
+// stage 2: rho' = r.(z - m), beta = rho'/rho, rho = rho', |r|^2, m
+// The preconditioned residual z is used mean-free (z - m): the constant mode of a singular system is
+// undetermined.  sc[s*MG_SC + {0: rho, 1: alpha, 2: beta, 3: |r|^2, 4: m}]
+constexpr int MG_SC = 6;
+
 __global__ void k_pcg_scalars(pict_domain_t dom, const double* part, int stride, int stage, double* sc) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (s >= dom.num_sims) return;
-    double a = 0.0, c = 0.0;
-    for (int t = dom.sim_tiles[s]; t < dom.sim_tiles[s + 1]; ++t) {
-        a += part[(size_t)stride * t];
-        if (stride > 1) c += part[(size_t)stride * t + 1];
-    }
-    double* S = sc + 4 * s;
-    if (stage == 0) {
-        S[0] = a;
-        S[3] = c;
-        S[2] = 0.0;
-    } else if (stage == 1) {
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int t = dom.sim_tiles[s] + lane; t < dom.sim_tiles[s + 1]; t += 32)
+        for (int k = 0; k < stride; ++k) v[k] += part[(size_t)stride * t + k];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+    if (lane != 0) return;
+    double* S = sc + MG_SC * s;
+    if (stage == 1) {
+        const double a = v[0];
         S[1] = (a != 0.0 && S[0] != 0.0 && isfinite(a)) ? S[0] / a : 0.0;
-    } else {
-        S[2] = (S[0] != 0.0 && isfinite(a)) ? a / S[0] : 0.0;
-        S[0] = a;
-        S[3] = c;
+        return;
     }
+    const int n = dom.sim_cells[s + 1] - dom.sim_cells[s];
+    const double m = v[2] / (double)n;
+    const double rho = v[0] - m * v[3];
+    if (stage == 0) {
+        S[2] = 0.0;
+    } else {
+        S[2] = (S[0] != 0.0 && isfinite(rho)) ? rho / S[0] : 0.0;
+    }
+    S[0] = rho;
+    S[3] = v[1];
+    S[4] = m;
 }
 
 template <typename T>
@@ -298,18 +318,20 @@ __device__ __forceinline__ int cell_sys(const pict_domain_t& dom, int i) { retur
 template <typename T>
 __global__ void k_pcg_update_xr(pict_domain_t dom, T* x, T* r, const T* p, const T* q, const double* sc) {
     PICT_CELL_LOOP(i, dom.num_cells) {
-        const T al = (T)sc[4 * cell_sys<T>(dom, i) + 1];
+        const T al = (T)sc[MG_SC * cell_sys<T>(dom, i) + 1];
         x[i] += al * p[i];
         r[i] -= al * q[i];
     }
 }
 
-// p = z + beta p  (init: p = z)
+// p = (z - m) + beta p  (init: p = z - m)
 template <typename T>
 __global__ void k_pcg_update_p(pict_domain_t dom, T* p, const T* z, const double* sc, int init) {
     PICT_CELL_LOOP(i, dom.num_cells) {
-        const T bt = init ? T(0) : (T)sc[4 * cell_sys<T>(dom, i) + 2];
-        p[i] = z[i] + bt * p[i];
+        const double* S = sc + MG_SC * cell_sys<T>(dom, i);
+        const T m = (T)S[4];
+        if (init) p[i] = z[i] - m;
+        else p[i] = (z[i] - m) + (T)S[2] * p[i];
     }
 }
 
@@ -327,7 +349,7 @@ __global__ void k_pcg_report(pict_domain_t dom, const double* sc, pict_solve_inf
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= dom.num_sims) return;
     const int n = dom.sim_cells[s + 1] - dom.sim_cells[s];
-    const double nrm = sqrt(sc[4 * s + 3]);
+    const double nrm = sqrt(sc[MG_SC * s + 3]);
     const double crit = normalized ? nrm / sqrt((double)n) : nrm;
     pict_solve_info_t inf;
     inf.final_residual = crit;
@@ -362,8 +384,8 @@ static pict_status_t run_pcg_mg(const pict_domain_t* dom, const pict_mg_level_t*
     T* z = reinterpret_cast<T*>(w); w += vbytes<T>(N);
     T* p = reinterpret_cast<T*>(w); w += vbytes<T>(N);
     T* q = reinterpret_cast<T*>(w); w += vbytes<T>(N);
-    double* part = reinterpret_cast<double*>(w); w += ((size_t)2 * dom->num_tiles * 8 + 255) & ~(size_t)255;
-    double* sc = reinterpret_cast<double*>(w); w += ((size_t)4 * dom->num_sims * 8 + 255) & ~(size_t)255;
+    double* part = reinterpret_cast<double*>(w); w += ((size_t)4 * dom->num_tiles * 8 + 255) & ~(size_t)255;
+    double* sc = reinterpret_cast<double*>(w); w += ((size_t)MG_SC * dom->num_sims * 8 + 255) & ~(size_t)255;
     if ((int64_t)(w - ws) > ws_bytes) return set_error(PICT_ERR_ARG, "pcg_mg: workspace too small");
 
     auto grid_of = [](int n) { return cell_grid(n, 256); };
@@ -375,16 +397,8 @@ static pict_status_t run_pcg_mg(const pict_domain_t* dom, const pict_mg_level_t*
             const pict_mg_level_t& L = levels[l];
             if (l > 0) b = lb[l];
             if (l == nl - 1) {
-                // coarsest: Jacobi sweeps from zero (ping-pong), result in lx0
-                k_mg_jacobi<T, D><<<grid_of(L.num_cells), 256, 0, st>>>(L, b, nullptr, lx0[l], wj);
-                for (int k = 1; k < coarse_sweeps; ++k) {
-                    T* src = (k & 1) ? lx0[l] : lx1[l];
-                    T* dst = (k & 1) ? lx1[l] : lx0[l];
-                    k_mg_jacobi<T, D><<<grid_of(L.num_cells), 256, 0, st>>>(L, b, src, dst, wj);
-                }
-                if ((coarse_sweeps & 1) == 0)  // last result in lx1: copy back
-                    cudaMemcpyAsync(lx0[l], lx1[l], sizeof(T) * L.num_cells, cudaMemcpyDeviceToDevice, st);
-                k_mg_block_mean_sub<T><<<L.num_blocks, 64, 0, st>>>(L, lx0[l]);
+                // coarsest: Jacobi sweeps from zero and mean removal in one launch, result in lx0
+                k_mg_coarse_solve<T, D><<<L.num_blocks, 64, 0, st>>>(L, b, lx0[l], wj, coarse_sweeps);
                 break;
             }
             k_mg_jacobi<T, D><<<grid_of(L.num_cells), 256, 0, st>>>(L, b, nullptr, lx0[l], wj);
@@ -399,28 +413,26 @@ static pict_status_t run_pcg_mg(const pict_domain_t* dom, const pict_mg_level_t*
             if (l > 0) cudaMemcpyAsync(lx0[l], lx1[l], sizeof(T) * L.num_cells, cudaMemcpyDeviceToDevice, st);
         }
         if (nl == 1) cudaMemcpyAsync(z0, lx0[0], sizeof(T) * N, cudaMemcpyDeviceToDevice, st);
-        // the preconditioned residual of a singular system: keep it mean-free
-        k_pcg_tile_sum<T><<<dom->num_tiles, 256, 0, st>>>(*dom, z0, part);
-        k_pcg_sub_mean<T><<<dom->num_tiles, 256, 0, st>>>(*dom, z0, part);
         return check_launch("pcg_mg vcycle");
     };
 
     const int nt = dom->num_tiles;
     const int sg = (dom->num_sims + 127) / 128;
+    const int swg = (dom->num_sims * 32 + 127) / 128;  // one warp per system
     k_pcg_init<T><<<grid_of(N), 256, 0, st>>>(N, rhs, r, xout);
     pict_status_t s = vcycle(r, z);
     if (s) return s;
-    k_pcg_dot2<T><<<nt, 256, 0, st>>>(*dom, r, z, part);
-    k_pcg_scalars<<<sg, 128, 0, st>>>(*dom, part, 2, 0, sc);
+    k_pcg_dot4<T><<<nt, 256, 0, st>>>(*dom, r, z, part);
+    k_pcg_scalars<<<swg, 128, 0, st>>>(*dom, part, 4, 0, sc);
     k_pcg_update_p<T><<<grid_of(N), 256, 0, st>>>(*dom, p, z, sc, 1);
     for (int it = 0; it < iterations; ++it) {
         k_pcg_spmv_dot<T, D><<<nt, 256, 0, st>>>(*dom, levels[0], p, q, part);
-        k_pcg_scalars<<<sg, 128, 0, st>>>(*dom, part, 1, 1, sc);
+        k_pcg_scalars<<<swg, 128, 0, st>>>(*dom, part, 1, 1, sc);
         k_pcg_update_xr<T><<<grid_of(N), 256, 0, st>>>(*dom, xout, r, p, q, sc);
         s = vcycle(r, z);
         if (s) return s;
-        k_pcg_dot2<T><<<nt, 256, 0, st>>>(*dom, r, z, part);
-        k_pcg_scalars<<<sg, 128, 0, st>>>(*dom, part, 2, 2, sc);
+        k_pcg_dot4<T><<<nt, 256, 0, st>>>(*dom, r, z, part);
+        k_pcg_scalars<<<swg, 128, 0, st>>>(*dom, part, 4, 2, sc);
         if (it + 1 < iterations) k_pcg_update_p<T><<<grid_of(N), 256, 0, st>>>(*dom, p, z, sc, 0);
     }
     k_pcg_report<<<sg, 128, 0, st>>>(*dom, sc, info, iterations, tol, normalized);
@@ -457,8 +469,8 @@ int64_t pict_pcg_mg_workspace_bytes(const pict_domain_t* dom, const pict_mg_leve
     size_t b = 0;
     for (int l = 0; l < num_levels; ++l) b += 3 * vb(levels[l].num_cells);
     b += 4 * vb(dom->num_cells);
-    b += ((size_t)2 * dom->num_tiles * 8 + 255) & ~(size_t)255;
-    b += ((size_t)4 * dom->num_sims * 8 + 255) & ~(size_t)255;
+    b += ((size_t)4 * dom->num_tiles * 8 + 255) & ~(size_t)255;
+    b += ((size_t)MG_SC * dom->num_sims * 8 + 255) & ~(size_t)255;
     return (int64_t)b;
 }
 

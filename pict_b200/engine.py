@@ -203,8 +203,8 @@ class PISOStepper:
         n += self.corrector_steps * (2 + 3 + 1)
         if self.pressure_refine > 0:  # per sweep: residual (+2 projection), solve, update; partials + finish
             if self._mg is not None:
-                nl, cs, it = self._mg.num_levels, 8, self.mg_iterations
-                v = 4 * (nl - 1) + cs + 1 + 2
+                nl, it = self._mg.num_levels, self.mg_iterations
+                v = 4 * (nl - 1) + 1
                 solve = 1 + v + 3 + it * (6 + v) - 1 + 1
                 n += nl - 1  # Galerkin coarse operators once per step
             else:

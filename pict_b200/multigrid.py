@@ -80,6 +80,8 @@ class MGHierarchy:
             if (sizes[:, :dims] <= min_size).all():
                 break
             sizes = np.where(sizes > 1, (sizes + 1) // 2, 1)
+        if int(sizes[:, :dims].prod(axis=1).max()) > 256:
+            raise ValueError("multigrid not applicable: coarsest blocks too large")
         self.num_levels = len(levels)
         self.levels = (MgLevel * self.num_levels)(*levels)
         self.cells = [int(L.num_cells) for L in levels]
