@@ -21,6 +21,7 @@ path ("weak" scaling); timing is the max over ranks.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import math
 import os
@@ -178,7 +179,7 @@ def precision_kwargs(args):
     single FP32 pressure solve from zero (the reference's order)."""
     if args.precision == "mixed":
         return {"pressure_refine": 1, "refine_tol": 1e-9, "warm_start_pressure": True,
-                "refine_solver": args.refine_solver}
+                "refine_solver": args.refine_solver, "pressure_first_solve": bool(args.first_solve)}
     return {}
 
 
@@ -385,43 +386,103 @@ def run_pict(args, rank, world):
         print(json.dumps(line), flush=True)
 
 
+def solver_bytes_per_cell(kind, dims, esz, nrhs=1):
+    """Algorithmic bytes per cell and iteration (each array once per pass at minimal fused traffic).
+
+    cg: read K coefficients, r, w, s, p, x; write x, p, s, r, w.
+    bicg: per component 2K + 17 values (two stencil sweeps and the vector updates of one iteration).
+    mg: preconditioned CG iteration = SpMV + dot (K + 2), x/r update (6), dot of r, z (2), direction
+        update (3), plus a V(1,1)-cycle on every level (pre-smoothing 3, residual + restriction K + 2,
+        prolongation 3, post-smoothing K + 3), the levels summing to 4/3 (2D) or 8/7 (3D) of the finest.
+    """
+    K = 2 * dims + 1
+    if kind == "cg":
+        return esz * (K + 10)
+    if kind == "bicg":
+        return esz * (2 * K + 17) * nrhs
+    geo = 4.0 / 3.0 if dims == 2 else 8.0 / 7.0
+    return esz * ((K + 2 + 6 + 2 + 3) + geo * (3 + K + 2 + 3 + K + 3))
+
+
 def roofline_pass(st, batch, args, dev):
+    """Per solver group (persistent BiCGStab, persistent CG, multigrid PCG): algorithmic bytes of the
+    launches (iterations x cells of each system x bytes per cell and iteration) over their CUDA-event
+    time.  The group with the largest time is reported as the dominant kernel."""
     import torch
     from pict_b200 import PISOtorch as P
     esz = 4 if batch.getDtype() == torch.float32 else 8
-    events = []
+    D = batch.getSpatialDims()
     steps = max(1, min(args.steps, 5))
-    # snapshot the state so the extra steps do not change what e2e sees
-    for _ in range(steps):
-        evs = st.step_with_events()
-        events.append(evs)
+    events = [st.step_with_events() for _ in range(steps)]
     torch.cuda.synchronize()
-    cg_ms = []
-    cg_bytes = []
-    per_cell = cg_algorithmic_bytes(batch.getSpatialDims(), esz)
-    sim_cells = batch._sim_cells.cpu().numpy()
-    n_s = np.diff(sim_cells)
+    n_s = np.diff(batch._sim_cells.cpu().numpy())
+    peak, kind_peak = measured_peaks()
+    groups = {}
     for evs in events:
-        for (a, b, info) in evs["cg"]:
-            cg_ms.append(a.elapsed_time(b))
-            its = np.array([i.usedIterations for i in P.decode_infos(info)])
-            # iterations + the initial pass over the cells
-            cg_bytes.append(float(np.sum((its + 1) * n_s) * per_cell))
-    ms = float(np.mean(cg_ms))
-    byt = float(np.mean(cg_bytes))
-    achieved = byt / (ms * 1e-3) / 1e9
-    peak, kind = measured_peaks()
-    kern = "k_cg1" if st.p_params.variant == 1 else "k_cg"
-    launches = len(cg_ms)
-    ratio = NCU_TRAFFIC_RATIO.get(kern)
-    return {"kernel": "%s (persistent CG, pressure solve)" % kern, "bound": "hbm", "achieved": achieved, "peak": peak,
-            "peak_kind": kind, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": None if ratio is None else ratio * byt,
-            "traffic_note": None if ratio is None else
-            "ncu dram bytes / algorithmic bytes = %.3f on one captured launch (profiles/), scaled to the average launch" % ratio,
-            "algorithmic_bytes_per_launch": byt, "avg_launch_ms": ms, "launches_timed": launches,
-            "launches": "every CG launch of the step (first pressure solves and refinement solves)",
-            "bytes_per_cell_iteration": per_cell}
+        for kind, lst in evs.items():
+            g = groups.setdefault(kind, {"ms": 0.0, "bytes": 0.0, "launches": 0})
+            for (a, b, info) in lst:
+                g["ms"] += a.elapsed_time(b)
+                infos = P.decode_infos(info)
+                if kind == "bicg":
+                    its = np.array([i.usedIterations for i in infos]).reshape(-1, D).max(axis=1)
+                    per = solver_bytes_per_cell("bicg", D, esz, nrhs=D)
+                else:
+                    its = np.array([i.usedIterations for i in infos])
+                    per = solver_bytes_per_cell(kind, D, esz)
+                g["bytes"] += float(np.sum((np.maximum(its, 0) + 1) * n_s) * per)
+                g["launches"] += 1
+    if st._mg is not None and "mg" in groups and groups["mg"]["launches"] > 0:
+        # the multigrid solve is ~400 short launches: time it as a captured CUDA graph, as it runs in the
+        # step's graph (eager timing would measure launch overhead)
+        ss = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        run = lambda: st._mg.solve(st.desc, st._res, st._corr, st.mg_iterations, st.refine_tol, st.info_r[0][0],
+                                   st._mg_ws, ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            run()
+        torch.cuda.current_stream().wait_stream(side)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            run()
+        graph.replay()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        reps = 5
+        e0.record()
+        for _ in range(reps):
+            graph.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        ms1 = e0.elapsed_time(e1) / reps
+        g = groups["mg"]
+        per_launch_bytes = g["bytes"] / g["launches"]
+        g["eager_ms"] = g["ms"]
+        g["ms"] = ms1 * g["launches"]
+        del graph
+    names = {"cg": "k_cg1" if st.p_params.variant == 1 else "k_cg", "bicg": "k_bicgstab",
+             "mg": "multigrid PCG (k_mg_* V-cycle + k_pcg_* kernels)"}
+    table = []
+    for kind, g in groups.items():
+        if g["launches"] == 0 or g["ms"] <= 0:
+            continue
+        ach = g["bytes"] / (g["ms"] * 1e-3) / 1e9
+        table.append({"kernel": names[kind], "group": kind, "ms_per_step": g["ms"] / steps,
+                      "achieved": ach, "frac": ach / peak,
+                      "algorithmic_bytes_per_launch": g["bytes"] / g["launches"],
+                      "avg_launch_ms": g["ms"] / g["launches"],
+                      "bytes_per_cell_iteration": solver_bytes_per_cell(kind, D, esz, nrhs=D)})
+    table.sort(key=lambda r: -r["ms_per_step"])
+    top = dict(table[0])
+    ratio = NCU_TRAFFIC_RATIO.get(top["kernel"])
+    top.update({"bound": "hbm", "peak": peak, "peak_kind": kind_peak, "unit": "GB/s",
+                "traffic": None if ratio is None else ratio * top["algorithmic_bytes_per_launch"],
+                "traffic_note": None if ratio is None else
+                "ncu dram bytes / algorithmic bytes on one captured launch (profiles/), scaled to the average launch",
+                "groups": table})
+    return top
 
 
 def e2e_pass(st, batch, args, dev, cells, world):
@@ -656,6 +717,9 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp32"])
     ap.add_argument("--refine-solver", default="mg", choices=["mg", "cg"],
                     help="solver of the refinement corrections (mixed precision)")
+    ap.add_argument("--first-solve", type=int, default=0,
+                    help="mixed precision: 1 = FP32 CG pressure solve before the refinement, 0 = refine from the "
+                         "warm-start pressure")
     ap.add_argument("--skip-bwd", action="store_true")
     ap.add_argument("--skip-fp32", action="store_true")
     ap.add_argument("--autotune", type=int, default=1, help="1: pick tile size / CTA cap / CG variant by timing")

@@ -48,7 +48,7 @@ class PISOStepper:
                  pressure_tol: Optional[float] = None, max_iterations: int = 5000, adv_group_size: int = 0,
                  p_group_size: int = 0, threads: int = 0, normalize_pressure: bool = True, cg_variant: int = 1,
                  pressure_refine: int = 0, refine_tol: Optional[float] = None, warm_start_pressure: bool = False,
-                 refine_solver: str = "cg", mg_iterations: int = 12):
+                 refine_solver: str = "cg", mg_iterations: int = 12, pressure_first_solve: bool = True):
         self.domain = domain
         self.dims = domain.getSpatialDims()
         self.corrector_steps = int(corrector_steps)
@@ -76,6 +76,9 @@ class PISOStepper:
         # correction solves of the refinement: "cg" (persistent CG) or "mg" (multigrid-preconditioned CG,
         # single-block systems only; falls back to "cg" otherwise)
         self.refine_solver = refine_solver
+        # with refinement, the first FP32 pressure solve can be left out: the refinement sweeps then start
+        # from the warm-start pressure (needs warm_start_pressure)
+        self.pressure_first_solve = bool(pressure_first_solve) or not (self.pressure_refine > 0 and self.warm_start_pressure)
         self.mg_iterations = int(mg_iterations)
         self._mg = None
         self.r_params = P._solve_params(1, self.max_iterations, self.refine_tol, _lib.PICT_CONV_NORM2_NORMALIZED, False,
@@ -138,9 +141,10 @@ class PISOStepper:
         pressureResult and the blocks' pressure."""
         d = self.domain
         lib = self.lib
-        check(lib.pict_solve(desc, P._ptr(d.P.coef), P._ptr(d.pressureRHSdiv), P._ptr(d.pressureResult),
-                             ctypes.byref(self.p_params), P._ptr(self.info_p[k]), P._ptr(self.ws), self.ws_bytes, st),
-              "pressure solve")
+        if self.pressure_first_solve:
+            check(lib.pict_solve(desc, P._ptr(d.P.coef), P._ptr(d.pressureRHSdiv), P._ptr(d.pressureResult),
+                                 ctypes.byref(self.p_params), P._ptr(self.info_p[k]), P._ptr(self.ws), self.ws_bytes,
+                                 st), "pressure solve")
         if self.pressure_refine > 0:
             self._refine_only(k, desc, st)
 
@@ -200,7 +204,7 @@ class PISOStepper:
         finish-info 3; per corrector pressure setup 2 (matrix/RHS, divergence), correction 1, and the
         refinement sweeps when enabled."""
         n = 1 + 3
-        n += self.corrector_steps * (2 + 3 + 1)
+        n += self.corrector_steps * (2 + (3 if self.pressure_first_solve else 0) + 1)
         if self.pressure_refine > 0:  # per sweep: residual (+2 projection), solve, update; partials + finish
             if self._mg is not None:
                 nl, it = self._mg.num_levels, self.mg_iterations
@@ -218,8 +222,8 @@ class PISOStepper:
     def step_with_events(self, time_step=None):
         """Eager step with CUDA events around each Krylov launch (timing of the dominant kernels).
 
-        Returns {"bicg": [(start, end, info)], "cg": [(start, end, info), ...]} with copies of the
-        solver reports of each launch.
+        Returns {"bicg": [(start, end, info)], "cg": [...], "mg": [...]} (persistent BiCGStab, persistent CG
+        and multigrid-preconditioned CG solves) with copies of the solver reports of each launch.
         """
         d = self.domain
         lib = self.lib
@@ -227,7 +231,7 @@ class PISOStepper:
         cs = torch.cuda.current_stream()
         st = ctypes.c_void_p(cs.cuda_stream)
         dt = self._dt(time_step)
-        out = {"bicg": [], "cg": []}
+        out = {"bicg": [], "cg": [], "mg": []}
 
         def ev():
             e = torch.cuda.Event(enable_timing=True)
@@ -246,14 +250,15 @@ class PISOStepper:
                 check(lib.pict_setup_pressure_correction(desc, dt, 0, 0, st), "pressure setup")
             else:
                 check(lib.pict_setup_pressure_rhs(desc, dt, 0, 0, st), "pressure rhs")
-            a = ev()
-            check(lib.pict_solve(desc, P._ptr(d.P.coef), P._ptr(d.pressureRHSdiv), P._ptr(d.pressureResult),
-                                 ctypes.byref(self.p_params), P._ptr(self.info_p[k]), P._ptr(self.ws), self.ws_bytes, st),
-                  "pressure solve")
-            b = ev()
-            out["cg"].append((a, b, self.info_p[k].clone()))
+            if self.pressure_first_solve:
+                a = ev()
+                check(lib.pict_solve(desc, P._ptr(d.P.coef), P._ptr(d.pressureRHSdiv), P._ptr(d.pressureResult),
+                                     ctypes.byref(self.p_params), P._ptr(self.info_p[k]), P._ptr(self.ws),
+                                     self.ws_bytes, st), "pressure solve")
+                b = ev()
+                out["cg"].append((a, b, self.info_p[k].clone()))
             if self.pressure_refine > 0:
-                self._refine_only(k, desc, st, events=out["cg"], ev=ev)
+                self._refine_only(k, desc, st, events=out["mg" if self._mg is not None else "cg"], ev=ev)
             last = k == self.corrector_steps - 1
             check(lib.pict_correct_velocity(desc, dt, 1, 0, 1 if last else 0, st), "velocity correction")
         return out
@@ -275,7 +280,8 @@ class PISOStepper:
         adv, ps = self.infos()
         extra = [("pressure %d refinement %d" % (k, m), r) for k, row in enumerate(self.refine_infos())
                  for m, r in enumerate(row)]
-        for name, lst in [("advection", adv)] + [("pressure %d" % k, p) for k, p in enumerate(ps)] + extra:
+        first = [("pressure %d" % k, p) for k, p in enumerate(ps)] if self.pressure_first_solve else []
+        for name, lst in [("advection", adv)] + first + extra:
             for i, inf in enumerate(lst):
                 if getattr(inf, "status", 0) == 1:
                     raise LinsolveError("%s solve: inter-CTA barrier timed out (system %d)" % (name, i))
