@@ -64,6 +64,65 @@ def make_cavity_domain(n, viscosity, dtype, device="cuda"):
     return dom
 
 
+def channel_arrays(nx, ny, nz, seed=2, stretch=2.0, u_center=20.0, amp=0.1, modes=12):
+    """3D channel on [0, 4 pi] x [-1, 1] x [0, 4 pi / 3]: vertex coordinates [1, 3, nz+1, ny+1, nx+1]
+    (uniform in x and z, tanh-stretched in y with factor `stretch`) and the initial velocity
+    [1, 3, nz, ny, nx]: laminar profile u = u_center (1 - y^2) plus the curl of a seeded random vector
+    potential (`modes` Fourier modes in x and z times (1 - y^2)^2, vanishing at the walls), scaled to
+    `amp` * u_center."""
+    rng = np.random.default_rng(seed)
+    lx, lz = 4 * np.pi, 4 * np.pi / 3
+    xv = np.linspace(0, lx, nx + 1)
+    s = np.linspace(-1.0, 1.0, ny + 1)
+    yv = np.tanh(stretch * s) / np.tanh(stretch)
+    zv = np.linspace(0, lz, nz + 1)
+    Z, Y, X = np.meshgrid(zv, yv, xv, indexing="ij")
+    coords = np.stack([X, Y, Z])[None]
+    xc, yc, zc = 0.5 * (xv[1:] + xv[:-1]), 0.5 * (yv[1:] + yv[:-1]), 0.5 * (zv[1:] + zv[:-1])
+    Zc, Yc, Xc = np.meshgrid(zc, yc, xc, indexing="ij")
+    w = (1 - Yc ** 2) ** 2
+    dw = -4 * Yc * (1 - Yc ** 2)
+    dpsi = np.zeros((3, 3) + Xc.shape)  # dpsi[c][axis]
+    for c in range(3):
+        for _ in range(modes):
+            kx = 2 * np.pi / lx * rng.integers(1, 5)
+            kz = 2 * np.pi / lz * rng.integers(1, 5)
+            a, ph = rng.standard_normal(), rng.uniform(0, 2 * np.pi)
+            arg = kx * Xc + kz * Zc + ph
+            dpsi[c][0] += -a * kx * np.sin(arg) * w
+            dpsi[c][1] += a * np.cos(arg) * dw
+            dpsi[c][2] += -a * kz * np.sin(arg) * w
+    up = np.stack([dpsi[2][1] - dpsi[1][2], dpsi[0][2] - dpsi[2][0], dpsi[1][0] - dpsi[0][1]])
+    up *= amp * u_center / max(np.abs(up).max(), 1e-30)
+    vel = up.copy()
+    vel[0] += u_center * (1 - Yc ** 2)
+    return coords, vel[None]
+
+
+def make_channel_domain(nx, ny, nz, dtype, device="cuda", viscosity=1.0 / 180.0):
+    """Periodic channel (x, z periodic, no-slip walls at y = +-1) driven by the constant pressure
+    gradient 1 (u_tau = 1, Re_tau = 1 / viscosity) as a static velocity source."""
+    import torch
+    from pict_b200 import PISOtorch
+    coords, vel = channel_arrays(nx, ny, nz)
+    dom = PISOtorch.Domain(3, torch.tensor([viscosity], dtype=dtype), name="channel", dtype=dtype,
+                           device=device, passiveScalarChannels=0)
+    blk = dom.CreateBlock(velocity=torch.tensor(vel, dtype=dtype, device=device).contiguous(),
+                          vertexCoordinates=torch.tensor(coords, dtype=dtype, device=device).contiguous(),
+                          name="channel")
+    blk.MakePeriodic("x")
+    blk.MakePeriodic("z")
+    blk.CloseBoundary("-y")
+    blk.CloseBoundary("+y")
+    blk.setVelocitySource(torch.tensor([[1.0, 0.0, 0.0]], dtype=dtype, device=device))
+    dom.PrepareSolve()
+    return dom
+
+
+def channel_dt(nx, u_center=20.0):
+    return 0.5 * (4 * np.pi / nx) / u_center
+
+
 def build_workload(name, rank=0, dtype=None):
     import torch
     dtype = torch.float32 if dtype is None else dtype
@@ -75,6 +134,10 @@ def build_workload(name, rank=0, dtype=None):
     if name == "lid_cavity_64":
         doms = [make_cavity_domain(64, 1e-3, dtype)]
         return dict(domains=doms, dts=[0.01], sides=np.array([64]), re=np.array([1000.0]), tol=1e-6, correctors=2)
+    if name == "channel3d_192":
+        doms = [make_channel_domain(192, 96, 96, dtype)]
+        return dict(domains=doms, dts=[channel_dt(192)], sides=None, re=None, tol=1e-6, correctors=2,
+                    kind="channel", refine_tol=1e-10)
     raise KeyError(name)
 
 
@@ -173,13 +236,14 @@ def sample_indices(sides, k):
     return order[[int(x * len(order)) for x in q]]
 
 
-def precision_kwargs(args):
+def precision_kwargs(args, wl=None):
     """mixed: FP32 stencils / vectors, FP64 reductions and one FP64 refinement sweep of every pressure
     solve to an RMS residual of 1e-9, pressure solves warm-started from the latest pressure; fp32: the
     single FP32 pressure solve from zero (the reference's order)."""
     if args.precision == "mixed":
-        return {"pressure_refine": 1, "refine_tol": 1e-9, "warm_start_pressure": True,
-                "refine_solver": args.refine_solver, "pressure_first_solve": bool(args.first_solve)}
+        return {"pressure_refine": 1, "refine_tol": (wl or {}).get("refine_tol", 1e-9), "warm_start_pressure": True,
+                "refine_solver": args.refine_solver, "pressure_first_solve": bool(args.first_solve),
+                "mg_iterations": args.mg_iterations}
     return {}
 
 
@@ -219,6 +283,24 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     w = args.workload
+    if w == "channel3d_192":
+        times, cells = [], 0
+        for _ in range(args.steps):
+            rate, t, c = oracle_channel_rate(48, 24, 24, 1)
+            times.append(t)
+            cells = c
+        value = cells * len(times) / sum(times)
+        line = {
+            "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": w, "sample": "channel 48x24x24 (1/4 resolution), one PISO step per timed step"},
+            "cpu_baseline": {"value": value, "unit": "cell-steps/s", "cores": 1, "kind": "port",
+                             "sample": "channel 48x24x24 x %d steps, FP64 NumPy/SciPy restatement" % args.steps},
+            "e2e": {"value": value, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
+        return
     if w == "batched_cavities_256":
         sides, re = batched_cavity_params(256, 6)
         dts = [0.5 / s for s in sides]
@@ -258,7 +340,7 @@ def run_pict(args, rank, world):
     doms = wl["domains"]
     batch = BatchDomain(doms, time_steps=wl["dts"])
     kw = dict(time_step=float(wl["dts"][0]), corrector_steps=wl["correctors"], advection_tol=wl["tol"],
-              pressure_tol=wl["tol"], max_iterations=5000, **precision_kwargs(args))
+              pressure_tol=wl["tol"], max_iterations=5000, **precision_kwargs(args, wl))
     tuned = None
     if args.autotune:
         from pict_b200.autotune import autotune
@@ -331,22 +413,32 @@ def run_pict(args, rank, world):
 
     # the same batched step in plain FP32 (pressure solves from zero to the workload tolerance, no
     # refinement): faster, at the error reported under fp32_step.err
-    fp32 = fp32_pass(batch, wl, args, dev, cells, world) if (args.precision == "mixed" and not args.skip_fp32) else None
+    cavities = wl.get("kind", "cavity") == "cavity"
+    fp32 = fp32_pass(batch, wl, args, dev, cells, world) if (args.precision == "mixed" and not args.skip_fp32
+                                                            and cavities) else None
 
     # forward + backward (adjoint) through the checkpointed rollout
-    fb = fwd_bwd_pass(st, batch, args, dev, cells, world) if not args.skip_bwd else None
+    fb = fwd_bwd_pass(st, batch, args, dev, cells, world) if (not args.skip_bwd and cavities) else None
 
     # plain: the same step one simulation at a time (single-domain stepper, CUDA graph), sampled
-    plain = plain_pass(wl, args) if (rank == 0 and not args.skip_plain) else None
+    plain = plain_pass(wl, args) if (rank == 0 and not args.skip_plain and cavities) else None
 
     # accuracy: two smallest simulations, FP32 GPU vs FP64 oracle with tight solves; adjoint vs FD
-    err = accuracy_check(wl, args) if (rank == 0 and not args.skip_err) else None
-    if err is not None and not args.skip_bwd:
+    if rank == 0 and not args.skip_err:
+        err = accuracy_check(wl, args) if cavities else channel_accuracy_check(wl, args)
+    else:
+        err = None
+    if err is not None and not args.skip_bwd and cavities:
         err["viscosity_grad"] = grad_check(wl)
 
     # CPU baseline (bounded sample, rank 0)
     cpu = None
-    if rank == 0 and not args.skip_cpu:
+    if rank == 0 and not args.skip_cpu and not cavities:
+        rate, tt, c = oracle_channel_rate(48, 24, 24, 1)
+        cpu = {"value": rate, "unit": "cell-steps/s", "cores": 1, "kind": "port",
+               "sample": "channel 48x24x24 (same setup at 1/4 resolution), 1 PISO step (FP64 NumPy/SciPy "
+                         "restatement, %.1f s)" % tt}
+    elif rank == 0 and not args.skip_cpu:
         sel = sample_indices(wl["sides"], 4)
         n_s = len(sel)
         rate, tt, c = oracle_step_rate(wl["sides"][sel], wl["re"][sel], [wl["dts"][i] for i in sel], n_s, 2)
@@ -664,6 +756,58 @@ def grad_check(wl, steps=3):
             "dtype": "f64"}
 
 
+def _oracle_channel(nx, ny, nz):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import piso_oracle as po
+    coords, vel = channel_arrays(nx, ny, nz)
+    d = po.ODomain(3, 1.0 / 180.0)
+    bi = d.create_block(coords=coords, velocity=vel)
+    d.make_periodic(bi, "x")
+    d.make_periodic(bi, "z")
+    d.close_boundary(bi, "-y")
+    d.close_boundary(bi, "+y")
+    d.blocks[bi].source = np.array([[1.0, 0.0, 0.0]])
+    d.prepare()
+    return po, d
+
+
+def oracle_channel_rate(nx, ny, nz, steps):
+    """FP64 oracle steps of the channel at a reduced resolution (CPU, one core)."""
+    po, d = _oracle_channel(nx, ny, nz)
+    dt = channel_dt(nx)
+    po.piso_step(d, dt, adv_tol=1e-6, p_tol=1e-6)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        po.piso_step(d, dt, adv_tol=1e-6, p_tol=1e-6)
+    t = time.perf_counter() - t0
+    return nx * ny * nz * steps / t, t, nx * ny * nz * steps
+
+
+def channel_accuracy_check(wl, args, n=(24, 12, 12), steps=10):
+    """Per-field relative error of the channel step (same settings, 1/8 resolution) against the FP64
+    oracle with 1e-12 solves after `steps` steps."""
+    import torch
+    from pict_b200.engine import PISOStepper
+    nx, ny, nz = n
+    dom = make_channel_domain(nx, ny, nz, torch.float32)
+    dt = channel_dt(nx)
+    st = PISOStepper(dom, time_step=dt, advection_tol=wl["tol"], pressure_tol=wl["tol"],
+                     **precision_kwargs(args, wl))
+    for _ in range(steps):
+        st.step()
+    st.check()
+    po, d = _oracle_channel(nx, ny, nz)
+    for _ in range(steps):
+        po.piso_step(d, dt, adv_tol=1e-12, p_tol=1e-12)
+    u = dom.getBlock(0).velocity.double().cpu().numpy().reshape(3, -1)
+    p = dom.getBlock(0).pressure.double().cpu().numpy().reshape(-1)
+    ur, pr = d.velocity_global(), d.pressure_global()
+    return {"steps": steps, "grid": "%dx%dx%d" % n,
+            "velocity_rel_max": float(np.abs(u - ur).max() / np.abs(ur).max()),
+            "pressure_rel_max": float(np.abs(p - pr).max() / np.abs(pr).max()),
+            "reference": "FP64 oracle, solver tol 1e-12"}
+
+
 def accuracy_check(wl, args):
     """Relative error of the FP32 batched step against the FP64 oracle (tight solves) on the two
     smallest simulations after 10 steps."""
@@ -709,7 +853,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="pict", choices=["pict", "reference"])
-    ap.add_argument("--workload", default="batched_cavities_256", choices=["batched_cavities_256", "lid_cavity_64"])
+    ap.add_argument("--workload", default="batched_cavities_256",
+                    choices=["batched_cavities_256", "lid_cavity_64", "channel3d_192"])
     ap.add_argument("--group-size", type=int, default=0)
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
@@ -720,6 +865,7 @@ def main():
     ap.add_argument("--first-solve", type=int, default=0,
                     help="mixed precision: 1 = FP32 CG pressure solve before the refinement, 0 = refine from the "
                          "warm-start pressure")
+    ap.add_argument("--mg-iterations", type=int, default=12, help="multigrid PCG iterations per correction")
     ap.add_argument("--skip-bwd", action="store_true")
     ap.add_argument("--skip-fp32", action="store_true")
     ap.add_argument("--autotune", type=int, default=1, help="1: pick tile size / CTA cap / CG variant by timing")

@@ -170,6 +170,32 @@ def lid_cavity(n, viscosity=1e-3, lid=1.0, dims=2):
                 ops=[("close_all", 0), ("close", 0, "-y", lidv)])
 
 
+def spectral_field(n, seed, kmax=8, dims=2):
+    """Seeded Gaussian random vector field on an n^2 periodic grid with energy spectrum ~ k^-3 for
+    1 <= |k| <= kmax (amplitude ~ k^-1.5), each component scaled to max |.| = 1: [1, 2, n, n]."""
+    rng = np.random.default_rng(seed)
+    kx = np.fft.fftfreq(n, 1.0 / n)
+    KX, KY = np.meshgrid(kx, kx, indexing="xy")
+    k = np.sqrt(KX ** 2 + KY ** 2)
+    amp = np.where((k > 0) & (k <= kmax), np.power(np.maximum(k, 1e-9), -1.5), 0.0)
+    comps = []
+    for _ in range(dims):
+        coef = amp * (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))
+        f = np.real(np.fft.ifft2(coef))
+        comps.append(f / np.abs(f).max())
+    return np.stack(comps)[None]
+
+
+def forcing_box(n=128, viscosity=1e-3, seed=3):
+    """Periodic unit box (cell size 1/n) with a smooth random initial velocity and a zero per-cell
+    velocity source: the differentiable forcing setup."""
+    xs = np.linspace(0, 1, n + 1)
+    return dict(dims=2, viscosity=viscosity,
+                blocks=[dict(coords=tensor_grid(xs, xs), velocity=spectral_field(n, seed),
+                             source=np.zeros((1, 2, n, n)))],
+                ops=[])
+
+
 # ------------------------------------------------------------------ builders
 
 def build_oracle(spec) -> po.ODomain:
