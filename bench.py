@@ -456,7 +456,7 @@ def run_pict(args, rank, world):
             "config": {"workload": args.workload, "simulations": len(doms), "cells_per_gpu": cells,
                        "pass": "forward", "solver_tol": wl["tol"], "correctors": wl["correctors"],
                        "precision": args.precision + (" (FP32 fields and Krylov vectors, FP64 reductions, one FP64 "
-                                                      "refinement sweep of each pressure solve to 1e-9 (multigrid-preconditioned CG corrections), warm-started pressure solves)"
+                                                      "refinement sweep of each pressure solve (multigrid-preconditioned CG corrections on near-isotropic grids), warm-started pressure solves)"
                                                       if args.precision == "mixed" else " (FP32, FP64 reductions)"),
                        "cuda_graph": not args.no_graph, "l2": "working set > L2 (126 MB), no flush",
                        "autotune": tuned, "tile_cells": batch.tile_cells,
@@ -860,7 +860,7 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-err", action="store_true")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp32"])
-    ap.add_argument("--refine-solver", default="mg", choices=["mg", "cg"],
+    ap.add_argument("--refine-solver", default="auto", choices=["auto", "mg", "cg"],
                     help="solver of the refinement corrections (mixed precision)")
     ap.add_argument("--first-solve", type=int, default=0,
                     help="mixed precision: 1 = FP32 CG pressure solve before the refinement, 0 = refine from the "

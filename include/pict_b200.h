@@ -250,7 +250,8 @@ typedef struct pict_mg_level {
     int32_t num_blocks;
     int32_t dims;
     int32_t dtype;
-    const int32_t* blocks;     /* [num_blocks][8]: first cell, size x, y, z, periodic x, y, z, system (device) */
+    const int32_t* blocks;     /* [num_blocks][12]: first cell, size x, y, z, periodic x, y, z, system, coarsening
+                                  shift x, y, z from the next finer level (0: kept, 1: halved), unused (device) */
     const int32_t* cell_block; /* [num_cells] block of each cell (device) */
     void* coef;                /* [2D+1][num_cells] stencil of the level (device) */
 } pict_mg_level_t;

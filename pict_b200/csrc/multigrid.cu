@@ -3,8 +3,9 @@
 // extensions/cg_solver_kernel.cu:114-456).
 //
 // Scope: domains whose systems are single blocks with fixed or periodic faces (the batched cavities,
-// the periodic channel and box).  Each level coarsens every block by 2 along each axis (aggregates of
-// up to 2^D cells, ceil(n/2) cells per axis); the coarse operator is the Galerkin product R A P with
+// the periodic channel and box).  Each level coarsens every block by 2 along the axes its coupling is
+// strong in (semi-coarsening on stretched grids, full coarsening on isotropic ones; aggregates of up to
+// 2^D cells, ceil(n/2) cells per coarsened axis); the coarse operator is the Galerkin product R A P with
 // piecewise-constant prolongation P and R = P^T, computed on the device from the fine stencil.  The
 // V-cycle uses one damped-Jacobi sweep before and after the coarse correction (symmetric), a fixed
 // number of Jacobi sweeps on the coarsest level and a scaled prolongation (aggregation coarse
@@ -20,13 +21,17 @@
 
 namespace pict {
 
+// block of a level: first cell, sizes, periodic flags, system, and the coarsening shifts (log2 of the
+// factor, 0 or 1 per axis) from the next finer level
 struct MgBlock {
-    int off, sx, sy, sz, px, py, pz, sys;
+    int off, sx, sy, sz, px, py, pz, sys, shx, shy, shz;
 };
 
+constexpr int MG_BT = 12;  // ints per block-table entry
+
 __device__ __forceinline__ MgBlock mg_block(const pict_mg_level_t& L, int b) {
-    const int* t = L.blocks + 8 * b;
-    return MgBlock{t[0], t[1], t[2], t[3], t[4], t[5], t[6], t[7]};
+    const int* t = L.blocks + MG_BT * b;
+    return MgBlock{t[0], t[1], t[2], t[3], t[4], t[5], t[6], t[7], t[8], t[9], t[10]};
 }
 
 // neighbour of local cell (x,y,z) across face f inside a block (periodic wrap, -1 at a fixed face)
@@ -80,10 +85,10 @@ __global__ void k_mg_galerkin(pict_mg_level_t F, pict_mg_level_t C) {
         T diag = 0, off[2 * D];
 #pragma unroll
         for (int f = 0; f < 2 * D; ++f) off[f] = 0;
-        for (int dz = 0; dz < (D == 3 ? 2 : 1); ++dz)
-            for (int dy = 0; dy < 2; ++dy)
-                for (int dx = 0; dx < 2; ++dx) {
-                    const int x = 2 * X + dx, y = 2 * Y + dy, z = 2 * Z + dz;
+        for (int dz = 0; dz < (1 << Bc.shz); ++dz)
+            for (int dy = 0; dy < (1 << Bc.shy); ++dy)
+                for (int dx = 0; dx < (1 << Bc.shx); ++dx) {
+                    const int x = (X << Bc.shx) + dx, y = (Y << Bc.shy) + dy, z = (Z << Bc.shz) + dz;
                     if (x >= Bf.sx || y >= Bf.sy || z >= Bf.sz) continue;
                     const int i = Bf.off + x + Bf.sx * (y + Bf.sy * z);
                     diag += cf[i];
@@ -93,7 +98,7 @@ __global__ void k_mg_galerkin(pict_mg_level_t F, pict_mg_level_t C) {
                         if (j < 0) continue;
                         int xj, yj, zj;
                         mg_unflatten(Bf, j - Bf.off, xj, yj, zj);
-                        const int J = Bc.off + (xj >> 1) + Bc.sx * ((yj >> 1) + Bc.sy * (zj >> 1));
+                        const int J = Bc.off + (xj >> Bc.shx) + Bc.sx * ((yj >> Bc.shy) + Bc.sy * (zj >> Bc.shz));
                         const T c = cf[(size_t)(f + 1) * Nf + i];
                         if (J == I) diag += c;
                         else off[f] += c;
@@ -133,10 +138,10 @@ __global__ void k_mg_residual_restrict(pict_mg_level_t F, pict_mg_level_t C, con
         int X, Y, Z;
         mg_unflatten(Bc, I - Bc.off, X, Y, Z);
         T acc = 0;
-        for (int dz = 0; dz < (D == 3 ? 2 : 1); ++dz)
-            for (int dy = 0; dy < 2; ++dy)
-                for (int dx = 0; dx < 2; ++dx) {
-                    const int x = 2 * X + dx, y = 2 * Y + dy, z = 2 * Z + dz;
+        for (int dz = 0; dz < (1 << Bc.shz); ++dz)
+            for (int dy = 0; dy < (1 << Bc.shy); ++dy)
+                for (int dx = 0; dx < (1 << Bc.shx); ++dx) {
+                    const int x = (X << Bc.shx) + dx, y = (Y << Bc.shy) + dy, z = (Z << Bc.shz) + dz;
                     if (x >= Bf.sx || y >= Bf.sy || z >= Bf.sz) continue;
                     const int i = Bf.off + x + Bf.sx * (y + Bf.sy * z);
                     acc += bv[i] - mg_apply<T, D>(F, cf, xv, i, Bf, x, y, z);
@@ -153,7 +158,7 @@ __global__ void k_mg_prolong_add(pict_mg_level_t F, pict_mg_level_t C, const T* 
         const MgBlock Bf = mg_block(F, b), Bc = mg_block(C, b);
         int x, y, z;
         mg_unflatten(Bf, i - Bf.off, x, y, z);
-        xf[i] += s * ec[Bc.off + (x >> 1) + Bc.sx * ((y >> 1) + Bc.sy * (z >> 1))];
+        xf[i] += s * ec[Bc.off + (x >> Bc.shx) + Bc.sx * ((y >> Bc.shy) + Bc.sy * (z >> Bc.shz))];
     }
 }
 

@@ -27,6 +27,7 @@ import ctypes
 import warnings
 from typing import Optional
 
+import numpy as np
 import torch
 
 from . import _lib
@@ -73,8 +74,9 @@ class PISOStepper:
                                         subtract_mean=normalize_pressure and not refine,
                                         write_block_pressure=not refine, group_size=p_group_size, threads=threads,
                                         variant=cg_variant)
-        # correction solves of the refinement: "cg" (persistent CG) or "mg" (multigrid-preconditioned CG,
-        # single-block systems only; falls back to "cg" otherwise)
+        # correction solves of the refinement: "cg" (persistent CG), "mg" (multigrid-preconditioned CG,
+        # single-block systems only; falls back to "cg" otherwise) or "auto" (multigrid on near-isotropic
+        # grids, CG on strongly stretched ones)
         self.refine_solver = refine_solver
         # with refinement, the first FP32 pressure solve can be left out: the refinement sweeps then start
         # from the warm-start pressure (needs warm_start_pressure)
@@ -115,13 +117,19 @@ class PISOStepper:
             self._res = torch.zeros(N, dtype=d.getDtype(), device=dev)
             self._corr = torch.zeros(N, dtype=d.getDtype(), device=dev)
             self._tile_scratch = torch.zeros(max(1, self.desc.num_tiles), dtype=torch.float64, device=dev)
-            if self.refine_solver == "mg":
-                from .multigrid import hierarchy_for
+            if self.refine_solver in ("mg", "auto"):
+                from .multigrid import hierarchy_for, axis_strengths
                 try:
+                    if self.refine_solver == "auto":
+                        # point-smoothed multigrid is robust on near-isotropic grids only
+                        st_ = axis_strengths(d)[:, :self.dims]
+                        if float((st_.max(axis=1) / np.maximum(st_.min(axis=1), 1e-300)).max()) > 4.0:
+                            raise ValueError("strongly anisotropic grid")
                     self._mg = hierarchy_for(d)
                     self._mg_ws = torch.empty(self._mg.workspace_bytes(self.desc), dtype=torch.uint8, device=dev)
                 except ValueError as e:
-                    warnings.warn("multigrid refinement not available (%s); using CG" % e)
+                    if self.refine_solver == "mg":
+                        warnings.warn("multigrid refinement not available (%s); using CG" % e)
                     self._mg = None
         ws = max(lib.pict_solve_workspace_bytes(ctypes.byref(self.desc), ctypes.byref(self.adv_params)),
                  lib.pict_solve_workspace_bytes(ctypes.byref(self.desc), ctypes.byref(self.p_params)),

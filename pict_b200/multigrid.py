@@ -1,8 +1,9 @@
 """Multigrid hierarchy of a (batched) domain for the multigrid-preconditioned CG of ``libpict_b200``.
 
 Eligible domains: every system is one block whose faces are fixed or periodic (no connections).
-Level l+1 coarsens every block of level l by two along each axis (ceil(n/2) cells, sizes of 1 stay
-1) until every block has at most 4 cells along each axis.  The block tables and cell-to-block maps
+Level l+1 halves every block of level l along its strongly coupled axes (ceil(n/2) cells; all axes
+on isotropic grids, the stretched axis first on stretched ones) until every block has at most 4
+cells along each axis.  The block tables and cell-to-block maps
 are built once on the host; the coarse stencils are recomputed on the device (Galerkin product)
 whenever the finest matrix changes.
 """
@@ -34,9 +35,31 @@ def eligible(host_blocks, num_blocks, dims, sim_of_block) -> Optional[str]:
     return None
 
 
+def axis_strengths(domain) -> np.ndarray:
+    """Mean orthogonal Laplace coefficient det |Minv row a|^2 per block and axis (the coupling strength
+    of the pressure operator along each axis; 1 without transforms): [num_blocks, 3]."""
+    D = domain.getSpatialDims()
+    out = np.ones((len(domain.getBlocks()), 3))
+    for k, b in enumerate(domain.getBlocks()):
+        tr = getattr(b, "transform", None)
+        if tr is None or tr.numel() == 0:
+            continue
+        t = tr.reshape(-1, 2 * D * D + 1).double()
+        det = t[:, -1]
+        minv = t[:, D * D:2 * D * D].reshape(-1, D, D)
+        alpha = det[:, None] * (minv ** 2).sum(dim=2)
+        out[k, :D] = alpha.mean(dim=0).cpu().numpy()
+    return out
+
+
 class MGHierarchy:
+    """Levels of the multigrid preconditioner.  At every level an axis of a block is halved if its
+    coupling strength is at least `theta` times the strongest of the block (semi-coarsening on stretched
+    grids); strengths of the coarse Galerkin operator grow with the number of fine faces a coarse face
+    sums (the product of the factors of the other axes)."""
+
     def __init__(self, host_blocks, num_blocks: int, dims: int, dtype, device, cell_block_dev: torch.Tensor,
-                 min_size: int = 4):
+                 strengths: Optional[np.ndarray] = None, min_size: int = 4, theta: float = 0.5):
         why = eligible(host_blocks, num_blocks, dims, None)
         if why is not None:
             raise ValueError("multigrid not applicable: " + why)
@@ -50,16 +73,21 @@ class MGHierarchy:
                         for b in range(num_blocks)], dtype=np.int64)
         per[:, dims:] = 0
         sims = np.array([host_blocks[b].sim for b in range(num_blocks)], dtype=np.int64)
+        strength = np.ones((num_blocks, 3)) if strengths is None else np.array(strengths, dtype=np.float64)
+        strength[:, dims:] = 0.0
+        shifts = np.zeros((num_blocks, 3), dtype=np.int64)
         self.levels_py = []   # keep tensors alive
+        self.shifts = []
         levels = []
         for lvl in range(MAX_LEVELS):
             n = sizes.prod(axis=1)
             offs = np.concatenate([[0], np.cumsum(n)[:-1]])
-            table = np.zeros((num_blocks, 8), dtype=np.int32)
+            table = np.zeros((num_blocks, 12), dtype=np.int32)
             table[:, 0] = offs
             table[:, 1:4] = sizes
             table[:, 4:7] = per
             table[:, 7] = sims
+            table[:, 8:11] = shifts
             blocks_t = torch.tensor(table.reshape(-1), dtype=torch.int32, device=device)
             if lvl == 0:
                 cb = cell_block_dev
@@ -77,9 +105,21 @@ class MGHierarchy:
             L.coef = coef.data_ptr() if coef is not None else None
             levels.append(L)
             self.levels_py.append((blocks_t, cb, coef))
+            self.shifts.append(shifts.copy())
             if (sizes[:, :dims] <= min_size).all():
                 break
-            sizes = np.where(sizes > 1, (sizes + 1) // 2, 1)
+            # choose the axes to halve per block
+            can = sizes > 1
+            can[:, dims:] = False
+            s_can = np.where(can, strength, 0.0)
+            smax = s_can.max(axis=1, keepdims=True)
+            shifts = ((s_can >= theta * smax) & can).astype(np.int64)
+            none = shifts.sum(axis=1) == 0
+            shifts[none] = can[none].astype(np.int64)  # degenerate: halve what can be halved
+            fac = 1 << shifts
+            prod = fac[:, :dims].prod(axis=1, keepdims=True)
+            strength[:, :dims] = strength[:, :dims] * prod / fac[:, :dims]
+            sizes = np.where(shifts == 1, (sizes + 1) // 2, sizes)
         if int(sizes[:, :dims].prod(axis=1).max()) > 256:
             raise ValueError("multigrid not applicable: coarsest blocks too large")
         self.num_levels = len(levels)
@@ -112,4 +152,5 @@ def hierarchy_for(domain) -> MGHierarchy:
     if host is None:
         host = domain._pack_blocks()
     nb = len(domain.getBlocks())
-    return MGHierarchy(host, nb, domain.getSpatialDims(), domain.getDtype(), domain.getDevice(), domain._cell_block)
+    return MGHierarchy(host, nb, domain.getSpatialDims(), domain.getDtype(), domain.getDevice(), domain._cell_block,
+                       strengths=axis_strengths(domain))

@@ -20,7 +20,8 @@ def _stencil_matrix(coef, blocks, dims):
     N = coef.size // K
     coef = coef.reshape(K, N)
     rows, cols, vals = [], [], []
-    for (off, sx, sy, sz, px, py, pz, _s) in blocks:
+    for row in blocks:
+        off, sx, sy, sz, px, py, pz = row[:7]
         n = (sx, sy, sz)
         per = (px, py, pz)
         for l in range(sx * sy * sz):
@@ -45,9 +46,10 @@ def _aggregation(fine_blocks, coarse_blocks):
     for fb, cb in zip(fine_blocks, coarse_blocks):
         off, sx, sy, sz = fb[:4]
         coff, csx, csy = cb[0], cb[1], cb[2]
+        hx, hy, hz = cb[8], cb[9], cb[10]
         for l in range(sx * sy * sz):
             x, y, z = l % sx, (l // sx) % sy, l // (sx * sy)
-            rows.append(coff + (x >> 1) + csx * ((y >> 1) + csy * (z >> 1)))
+            rows.append(coff + (x >> hx) + csx * ((y >> hy) + csy * (z >> hz)))
             cols.append(off + l)
     nf = sum(b[1] * b[2] * b[3] for b in fine_blocks)
     nc = sum(b[1] * b[2] * b[3] for b in coarse_blocks)
@@ -74,7 +76,7 @@ def test_galerkin_matches_scipy():
     s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
     mg.setup(b.P.coef, s)
     torch.cuda.synchronize()
-    tables = [t[0].cpu().numpy().reshape(-1, 8) for t in mg.levels_py]
+    tables = [t[0].cpu().numpy().reshape(-1, 12) for t in mg.levels_py]
     A = _stencil_matrix(b.P.coef.cpu().numpy().reshape(-1), tables[0], 2)
     for l in range(1, mg.num_levels):
         R = _aggregation(tables[l - 1], tables[l])
@@ -143,3 +145,43 @@ def test_refined_step_with_multigrid_within_1e5_of_fp64_oracle():
         ur, pr = od.velocity_global(), od.pressure_global()
         assert np.abs(u - ur).max() / np.abs(ur).max() < 1e-5
         assert np.abs(p - pr).max() / np.abs(pr).max() < 1e-5
+
+
+def test_semicoarsening_on_stretched_grid():
+    """A strongly stretched 2D block: the stretched axis is halved first, the Galerkin operators still
+    equal R A R^T, and the preconditioned CG converges."""
+    from pict_b200 import PISOtorch as P
+    from pict_b200.multigrid import hierarchy_for
+    from pict_b200.engine import PISOStepper
+    from setups import tensor_grid, stretched
+    xs = np.linspace(0, 4.0, 65)
+    ys = stretched(48, length=1.0, beta=3.0)
+    spec = dict(dims=2, viscosity=1e-2, blocks=[dict(coords=tensor_grid(xs, ys))],
+                ops=[("periodic", 0, "x"), ("close", 0, "-y"), ("close", 0, "+y")])
+    pd = build_product(spec, torch.float64)
+    st = PISOStepper(pd, time_step=0.01, advection_tol=1e-10, pressure_tol=1e-10)
+    st.step()
+    mg = hierarchy_for(pd)
+    assert mg.shifts[1][0, 1] == 1 and mg.shifts[1][0, 0] == 0   # y (stretched) only
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    mg.setup(pd.P.coef, s)
+    torch.cuda.synchronize()
+    tables = [t[0].cpu().numpy().reshape(-1, 12) for t in mg.levels_py]
+    A = _stencil_matrix(pd.P.coef.cpu().numpy().reshape(-1), tables[0], 2)
+    for l in range(1, mg.num_levels):
+        R = _aggregation(tables[l - 1], tables[l])
+        Ac_ref = (R @ A @ R.T).toarray()
+        Ac = _stencil_matrix(mg.levels_py[l][2].cpu().numpy(), tables[l], 2).toarray()
+        assert np.abs(Ac - Ac_ref).max() <= 1e-12 * np.abs(Ac_ref).max()
+        A = sp.csr_matrix(Ac_ref)
+    g = torch.Generator(device="cpu").manual_seed(8)
+    rhs = torch.randn(pd.getTotalSize(), generator=g, dtype=torch.float64).cuda()
+    rhs -= rhs.mean()
+    x = torch.zeros_like(rhs)
+    info = torch.zeros(24, dtype=torch.uint8, device="cuda")
+    ws = torch.empty(mg.workspace_bytes(pd._desc), dtype=torch.uint8, device="cuda")
+    mg.solve(pd._desc, rhs, x, 16, 1e-30, info, ws, s)
+    inf = P.decode_infos(info)[0]
+    r0 = float(rhs.norm()) / np.sqrt(rhs.numel())
+    # point smoothing with a per-block coarsening choice is only partly robust to the wall stretching
+    assert inf.isFiniteResidual and inf.finalResidual < 0.1 * r0, (inf, r0)
