@@ -279,7 +279,7 @@ __device__ __forceinline__ pict_solve_info_t fresh_info() {
 // CG (extensions/cg_solver_kernel.cu:236-427)
 // ---------------------------------------------------------------------------------------------
 template <typename T, int D, bool TRANS>
-__global__ void __launch_bounds__(KR_THREADS) k_cg(KArgs<T> a) {
+__global__ void __launch_bounds__(KR_THREADS, 2) k_cg(KArgs<T> a) {
     const pict_domain_t& dom = a.dom;
     const int N = dom.num_cells;
     __shared__ TileSlots S;
@@ -474,7 +474,7 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg(KArgs<T> a) {
 // iteration counts as extensions/cg_solver_kernel.cu:303-397.
 // ---------------------------------------------------------------------------------------------
 template <typename T, int D, bool TRANS>
-__global__ void __launch_bounds__(KR_THREADS) k_cg1(KArgs<T> a) {
+__global__ void __launch_bounds__(KR_THREADS, 2) k_cg1(KArgs<T> a) {
     const pict_domain_t& dom = a.dom;
     const int N = dom.num_cells;
     __shared__ TileSlots S;
@@ -667,7 +667,7 @@ __global__ void __launch_bounds__(KR_THREADS) k_cg1(KArgs<T> a) {
 // BiCGStab without preconditioner (extensions/bicgstab_solver_kernel.cu:240-360), NR right-hand sides sharing the matrix
 // ---------------------------------------------------------------------------------------------
 template <typename T, int D, int NR, bool TRANS>
-__global__ void __launch_bounds__(KR_THREADS) k_bicgstab(KArgs<T> a) {
+__global__ void __launch_bounds__(KR_THREADS, 2) k_bicgstab(KArgs<T> a) {
     const pict_domain_t& dom = a.dom;
     const int N = dom.num_cells;
     const size_t NS = (size_t)N;
