@@ -11,7 +11,7 @@
 // number of Jacobi sweeps on the coarsest level and a scaled prolongation (aggregation coarse
 // operators are too stiff by about 2).  The constant mode of the singular (Neumann / periodic) block
 // operators is removed on the coarsest level and from every preconditioned residual (folded into the
-// inner products and the search-direction update).  The preconditioned CG runs a fixed number of iterations with
+// inner products and into the search direction, which the SpMV forms on the fly).  The preconditioned CG runs a fixed number of iterations with
 // per-system scalars; every inner product is reduced per work tile and then per system in a fixed
 // order, so results do not depend on the launch shape.
 #include <cmath>
@@ -28,24 +28,30 @@ struct MgBlock {
 };
 
 constexpr int MG_BT = 12;  // ints per block-table entry
+constexpr int MG_SC = 6;   // per-system PCG scalars: rho, alpha, beta, |r|^2, mean(z), unused
 
 __device__ __forceinline__ MgBlock mg_block(const pict_mg_level_t& L, int b) {
     const int* t = L.blocks + MG_BT * b;
     return MgBlock{t[0], t[1], t[2], t[3], t[4], t[5], t[6], t[7], t[8], t[9], t[10]};
 }
 
-// neighbour of local cell (x,y,z) across face f inside a block (periodic wrap, -1 at a fixed face)
-__device__ __forceinline__ int mg_nbr(const MgBlock& B, int x, int y, int z, int f) {
-    const int a = f >> 1, up = f & 1;
-    int q[3] = {x, y, z};
+// neighbour across face f with its coordinates (q in: cell, out: neighbour); -1 at a fixed face
+__device__ __forceinline__ int mg_nbr_q(const MgBlock& B, int* q, int f) {
+    const int a = f >> 1;
     const int n[3] = {B.sx, B.sy, B.sz};
     const int per[3] = {B.px, B.py, B.pz};
-    q[a] += up ? 1 : -1;
+    q[a] += (f & 1) ? 1 : -1;
     if (q[a] < 0 || q[a] >= n[a]) {
         if (!per[a]) return -1;
         q[a] = (q[a] + n[a]) % n[a];
     }
     return B.off + q[0] + B.sx * (q[1] + B.sy * q[2]);
+}
+
+// neighbour of local cell (x,y,z) across face f inside a block (periodic wrap, -1 at a fixed face)
+__device__ __forceinline__ int mg_nbr(const MgBlock& B, int x, int y, int z, int f) {
+    int q[3] = {x, y, z};
+    return mg_nbr_q(B, q, f);
 }
 
 __device__ __forceinline__ void mg_unflatten(const MgBlock& B, int l, int& x, int& y, int& z) {
@@ -150,15 +156,30 @@ __global__ void k_mg_residual_restrict(pict_mg_level_t F, pict_mg_level_t C, con
     }
 }
 
-// x_f += s P e_c
+// prolongation fused into the post-smoothing sweep: with x' = x_f + s P e_c (formed on the fly for
+// the neighbours), x_out = x' + w (b - A x') / diag
 template <typename T, int D>
-__global__ void k_mg_prolong_add(pict_mg_level_t F, pict_mg_level_t C, const T* ec, T* xf, T s) {
-    PICT_CELL_LOOP(i, F.num_cells) {
+__global__ void k_mg_prolong_jacobi(pict_mg_level_t F, pict_mg_level_t C, const T* bv, const T* xf, const T* ec,
+                                    T* xout, T s, T w) {
+    const T* coef = reinterpret_cast<const T*>(F.coef);
+    const int N = F.num_cells;
+    PICT_CELL_LOOP(i, N) {
         const int b = F.cell_block[i];
         const MgBlock Bf = mg_block(F, b), Bc = mg_block(C, b);
         int x, y, z;
         mg_unflatten(Bf, i - Bf.off, x, y, z);
-        xf[i] += s * ec[Bc.off + (x >> Bc.shx) + Bc.sx * ((y >> Bc.shy) + Bc.sy * (z >> Bc.shz))];
+        const T xi = xf[i] + s * ec[Bc.off + (x >> Bc.shx) + Bc.sx * ((y >> Bc.shy) + Bc.sy * (z >> Bc.shz))];
+        const T d = coef[i];
+        T acc = d * xi;
+#pragma unroll
+        for (int f = 0; f < 2 * D; ++f) {
+            int q[3] = {x, y, z};
+            const int j = mg_nbr_q(Bf, q, f);
+            if (j < 0) continue;
+            const T xj = xf[j] + s * ec[Bc.off + (q[0] >> Bc.shx) + Bc.sx * ((q[1] >> Bc.shy) + Bc.sy * (q[2] >> Bc.shz))];
+            acc += coef[(size_t)(f + 1) * N + i] * xj;
+        }
+        xout[i] = xi + ((d != T(0)) ? w * (bv[i] - acc) / d : T(0));
     }
 }
 
@@ -232,21 +253,32 @@ __device__ __forceinline__ double mg_cta_sum(double v, double* s_red) {
     return r;
 }
 
-// q = A p and the tile partial of p.q (one CTA per work tile of the domain)
+// p_new = (z - m) + beta p_old formed on the fly (also for the neighbours), q = A p_new, and the tile
+// partial of p_new.q (one CTA per work tile of the domain); m, beta per system from sc
 template <typename T, int D>
-__global__ void k_pcg_spmv_dot(pict_domain_t dom, pict_mg_level_t L, const T* p, T* q, double* part) {
+__global__ void k_pcg_spmv_dot(pict_domain_t dom, pict_mg_level_t L, const T* z, const T* pold, T* pnew, T* q,
+                               const double* sc, double* part) {
     __shared__ double s_red[32];
     const T* coef = reinterpret_cast<const T*>(L.coef);
+    const int N = L.num_cells;
     const int t = blockIdx.x;
-    const int s0 = dom.tiles[4 * t + 2], cnt = dom.tiles[4 * t + 3];
+    const int sys = dom.tiles[4 * t], s0 = dom.tiles[4 * t + 2], cnt = dom.tiles[4 * t + 3];
     const MgBlock B = mg_block(L, dom.tiles[4 * t + 1]);
+    const T m = (T)sc[MG_SC * sys + 4], bt = (T)sc[MG_SC * sys + 2];
     double acc = 0.0;
     for (int i = s0 + threadIdx.x; i < s0 + cnt; i += blockDim.x) {
-        int x, y, z;
-        mg_unflatten(B, i - B.off, x, y, z);
-        const T qi = mg_apply<T, D>(L, coef, p, i, B, x, y, z);
+        int x, y, z3;
+        mg_unflatten(B, i - B.off, x, y, z3);
+        const T pi = (z[i] - m) + bt * pold[i];
+        T qi = coef[i] * pi;
+#pragma unroll
+        for (int f = 0; f < 2 * D; ++f) {
+            const int j = mg_nbr(B, x, y, z3, f);
+            if (j >= 0) qi += coef[(size_t)(f + 1) * N + i] * ((z[j] - m) + bt * pold[j]);
+        }
+        pnew[i] = pi;
         q[i] = qi;
-        acc += (double)p[i] * (double)qi;
+        acc += (double)pi * (double)qi;
     }
     acc = mg_cta_sum(acc, s_red);
     if (threadIdx.x == 0) part[t] = acc;
@@ -283,7 +315,6 @@ __global__ void k_pcg_dot4(pict_domain_t dom, const T* r, const T* z, double* pa
 // stage 2: rho' = r.(z - m), beta = rho'/rho, rho = rho', |r|^2, m
 // The preconditioned residual z is used mean-free (z - m): the constant mode of a singular system is
 // undetermined.  sc[s*MG_SC + {0: rho, 1: alpha, 2: beta, 3: |r|^2, 4: m}]
-constexpr int MG_SC = 6;
 
 __global__ void k_pcg_scalars(pict_domain_t dom, const double* part, int stride, int stage, double* sc) {
     const int lane = threadIdx.x & 31;
@@ -319,33 +350,30 @@ __global__ void k_pcg_scalars(pict_domain_t dom, const double* part, int stride,
 template <typename T>
 __device__ __forceinline__ int cell_sys(const pict_domain_t& dom, int i) { return dom.blocks[dom.cell_block[i]].sim; }
 
-// x += alpha p, r -= alpha q
+// x += alpha p, r -= alpha q, and the first pre-smoothing sweep of the next V-cycle on the finest
+// level: x0 = w r / diag
 template <typename T>
-__global__ void k_pcg_update_xr(pict_domain_t dom, T* x, T* r, const T* p, const T* q, const double* sc) {
+__global__ void k_pcg_update_xr(pict_domain_t dom, pict_mg_level_t L, T* x, T* r, const T* p, const T* q,
+                                const double* sc, T* x0, T w) {
+    const T* coef = reinterpret_cast<const T*>(L.coef);
     PICT_CELL_LOOP(i, dom.num_cells) {
         const T al = (T)sc[MG_SC * cell_sys<T>(dom, i) + 1];
         x[i] += al * p[i];
-        r[i] -= al * q[i];
+        const T ri = r[i] - al * q[i];
+        r[i] = ri;
+        const T d = coef[i];
+        x0[i] = (d != T(0)) ? w * ri / d : T(0);
     }
 }
 
-// p = (z - m) + beta p  (init: p = z - m)
+// r = b, x = 0, search directions 0
 template <typename T>
-__global__ void k_pcg_update_p(pict_domain_t dom, T* p, const T* z, const double* sc, int init) {
-    PICT_CELL_LOOP(i, dom.num_cells) {
-        const double* S = sc + MG_SC * cell_sys<T>(dom, i);
-        const T m = (T)S[4];
-        if (init) p[i] = z[i] - m;
-        else p[i] = (z[i] - m) + (T)S[2] * p[i];
-    }
-}
-
-// r = b (x = 0)
-template <typename T>
-__global__ void k_pcg_init(int N, const T* b, T* r, T* x) {
+__global__ void k_pcg_init(int N, const T* b, T* r, T* x, T* p0, T* p1) {
     PICT_CELL_LOOP(i, N) {
         r[i] = b[i];
         x[i] = T(0);
+        p0[i] = T(0);
+        p1[i] = T(0);
     }
 }
 
@@ -395,8 +423,10 @@ static pict_status_t run_pcg_mg(const pict_domain_t* dom, const pict_mg_level_t*
 
     auto grid_of = [](int n) { return cell_grid(n, 256); };
     const T wj = (T)omega, sp = (T)scale;
-    // z = M r (V-cycle); r is the finest right-hand side
-    auto vcycle = [&](const T* rhs0, T* z0) -> pict_status_t {
+    // z = M r (V-cycle); r is the finest right-hand side.  presmoothed: the first finest sweep
+    // (lx0[0] = w r / diag) was already written by the x/r update.  Every level's corrected iterate
+    // ends in lx1 (lx0 on the coarsest), so the prolongation reads it without copies.
+    auto vcycle = [&](const T* rhs0, T* z0, bool presmoothed) -> pict_status_t {
         const T* b = rhs0;
         for (int l = 0; l < nl; ++l) {
             const pict_mg_level_t& L = levels[l];
@@ -406,39 +436,44 @@ static pict_status_t run_pcg_mg(const pict_domain_t* dom, const pict_mg_level_t*
                 k_mg_coarse_solve<T, D><<<L.num_blocks, 64, 0, st>>>(L, b, lx0[l], wj, coarse_sweeps);
                 break;
             }
-            k_mg_jacobi<T, D><<<grid_of(L.num_cells), 256, 0, st>>>(L, b, nullptr, lx0[l], wj);
+            if (l > 0 || !presmoothed) k_mg_jacobi<T, D><<<grid_of(L.num_cells), 256, 0, st>>>(L, b, nullptr, lx0[l], wj);
             k_mg_residual_restrict<T, D><<<grid_of(levels[l + 1].num_cells), 256, 0, st>>>(L, levels[l + 1], b, lx0[l], lb[l + 1]);
         }
+        const T* ec = lx0[nl - 1];
         for (int l = nl - 2; l >= 0; --l) {
             const pict_mg_level_t& L = levels[l];
             const T* bl = (l == 0) ? rhs0 : lb[l];
-            k_mg_prolong_add<T, D><<<grid_of(L.num_cells), 256, 0, st>>>(L, levels[l + 1], lx0[l + 1], lx0[l], sp);
             T* dst = (l == 0) ? z0 : lx1[l];
-            k_mg_jacobi<T, D><<<grid_of(L.num_cells), 256, 0, st>>>(L, bl, lx0[l], dst, wj);
-            if (l > 0) cudaMemcpyAsync(lx0[l], lx1[l], sizeof(T) * L.num_cells, cudaMemcpyDeviceToDevice, st);
+            k_mg_prolong_jacobi<T, D><<<grid_of(L.num_cells), 256, 0, st>>>(L, levels[l + 1], bl, lx0[l], ec, dst, sp, wj);
+            ec = dst;
         }
         if (nl == 1) cudaMemcpyAsync(z0, lx0[0], sizeof(T) * N, cudaMemcpyDeviceToDevice, st);
         return check_launch("pcg_mg vcycle");
     };
 
+    // search directions alternate between p and pb; each is formed from z inside the SpMV
+    T* pb = lx1[0];
     const int nt = dom->num_tiles;
     const int sg = (dom->num_sims + 127) / 128;
     const int swg = (dom->num_sims * 32 + 127) / 128;  // one warp per system
-    k_pcg_init<T><<<grid_of(N), 256, 0, st>>>(N, rhs, r, xout);
-    pict_status_t s = vcycle(r, z);
+    k_pcg_init<T><<<grid_of(N), 256, 0, st>>>(N, rhs, r, xout, p, pb);
+    pict_status_t s = vcycle(r, z, false);
     if (s) return s;
     k_pcg_dot4<T><<<nt, 256, 0, st>>>(*dom, r, z, part);
     k_pcg_scalars<<<swg, 128, 0, st>>>(*dom, part, 4, 0, sc);
-    k_pcg_update_p<T><<<grid_of(N), 256, 0, st>>>(*dom, p, z, sc, 1);
     for (int it = 0; it < iterations; ++it) {
-        k_pcg_spmv_dot<T, D><<<nt, 256, 0, st>>>(*dom, levels[0], p, q, part);
+        k_pcg_spmv_dot<T, D><<<nt, 256, 0, st>>>(*dom, levels[0], z, p, pb, q, sc, part);
         k_pcg_scalars<<<swg, 128, 0, st>>>(*dom, part, 1, 1, sc);
-        k_pcg_update_xr<T><<<grid_of(N), 256, 0, st>>>(*dom, xout, r, p, q, sc);
-        s = vcycle(r, z);
-        if (s) return s;
+        k_pcg_update_xr<T><<<grid_of(N), 256, 0, st>>>(*dom, levels[0], xout, r, pb, q, sc, lx0[0], wj);
+        const bool last = it + 1 == iterations;
+        if (!last) {
+            s = vcycle(r, z, true);
+            if (s) return s;
+        }
+        // on the last iteration only |r|^2 is used (r.z and sum(z) of the stale z are ignored)
         k_pcg_dot4<T><<<nt, 256, 0, st>>>(*dom, r, z, part);
         k_pcg_scalars<<<swg, 128, 0, st>>>(*dom, part, 4, 2, sc);
-        if (it + 1 < iterations) k_pcg_update_p<T><<<grid_of(N), 256, 0, st>>>(*dom, p, z, sc, 0);
+        T* tmp = p; p = pb; pb = tmp;
     }
     k_pcg_report<<<sg, 128, 0, st>>>(*dom, sc, info, iterations, tol, normalized);
     return check_launch("pcg_mg");

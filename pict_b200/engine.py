@@ -216,8 +216,8 @@ class PISOStepper:
         if self.pressure_refine > 0:  # per sweep: residual (+2 projection), solve, update; partials + finish
             if self._mg is not None:
                 nl, it = self._mg.num_levels, self.mg_iterations
-                v = 4 * (nl - 1) + 1
-                solve = 1 + v + 3 + it * (6 + v) - 1 + 1
+                v = 3 * (nl - 1) + 1      # V-cycle; the finest pre-smoothing of later ones is fused
+                solve = 1 + v + 2 + it * 5 + max(it - 1, 0) * (v - 1) + 1
                 n += nl - 1  # Galerkin coarse operators once per step
             else:
                 solve = 3
