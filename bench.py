@@ -483,17 +483,21 @@ def solver_bytes_per_cell(kind, dims, esz, nrhs=1):
 
     cg: read K coefficients, r, w, s, p, x; write x, p, s, r, w.
     bicg: per component 2K + 17 values (two stencil sweeps and the vector updates of one iteration).
-    mg: preconditioned CG iteration = SpMV + dot (K + 2), x/r update (6), dot of r, z (2), direction
-        update (3), plus a V(1,1)-cycle on every level (pre-smoothing 3, residual + restriction K + 2,
-        prolongation 3, post-smoothing K + 3), the levels summing to 4/3 (2D) or 8/7 (3D) of the finest.
+    mg: one preconditioned CG iteration as the fused kernels move it on the finest level: SpMV with
+        the direction update (read K coefficients, z, p_old; write p, q: K + 4), restriction with the
+        x/r update (read r, q, x, p, K coefficients; write r, x and the coarse right-hand side:
+        K + 6 + 2^-D), prolongation with post-smoothing and the r.z partials (read K coefficients, r,
+        the coarse iterate; write z: K + 2 + 2^-D); every coarser level restricts (K + 1 + 2^-D) and
+        prolongs (K + 2 + 2^-D), the coarse levels summing to 1/3 (2D) or 1/7 (3D) of the finest.
     """
     K = 2 * dims + 1
     if kind == "cg":
         return esz * (K + 10)
     if kind == "bicg":
         return esz * (2 * K + 17) * nrhs
-    geo = 4.0 / 3.0 if dims == 2 else 8.0 / 7.0
-    return esz * ((K + 2 + 6 + 2 + 3) + geo * (3 + K + 2 + 3 + K + 3))
+    c = 0.5 ** dims
+    coarse = 1.0 / 3.0 if dims == 2 else 1.0 / 7.0
+    return esz * ((K + 4) + (K + 6 + c) + (K + 2 + c) + coarse * ((K + 1 + c) + (K + 2 + c)))
 
 
 def roofline_pass(st, batch, args, dev):

@@ -254,6 +254,9 @@ typedef struct pict_mg_level {
                                   shift x, y, z from the next finer level (0: kept, 1: halved), unused (device) */
     const int32_t* cell_block; /* [num_cells] block of each cell (device) */
     void* coef;                /* [2D+1][num_cells] stencil of the level (device) */
+    int32_t num_tiles;         /* work tiles of the level (levels >= 1; level 0 runs on the domain's tiles) */
+    int32_t max_block_cells;   /* cells of the largest block of the level */
+    const int32_t* tiles;      /* [num_tiles][4]: system, block, first cell, cell count (device) */
 } pict_mg_level_t;
 
 /* Galerkin coarse operator R A P of `fine` into coarse->coef (aggregates of 2^D cells). */

@@ -106,6 +106,9 @@ class MgLevel(ctypes.Structure):
         ("blocks", c_vp),
         ("cell_block", c_vp),
         ("coef", c_vp),
+        ("num_tiles", c_i32),
+        ("max_block_cells", c_i32),
+        ("tiles", c_vp),
     ]
 
 

@@ -11,9 +11,15 @@
 // number of Jacobi sweeps on the coarsest level and a scaled prolongation (aggregation coarse
 // operators are too stiff by about 2).  The constant mode of the singular (Neumann / periodic) block
 // operators is removed on the coarsest level and from every preconditioned residual (folded into the
-// inner products and into the search direction, which the SpMV forms on the fly).  The preconditioned CG runs a fixed number of iterations with
-// per-system scalars; every inner product is reduced per work tile and then per system in a fixed
-// order, so results do not depend on the launch shape.
+// inner products and into the search direction, which the SpMV forms on the fly).  The preconditioned
+// CG runs a fixed number of iterations with per-system scalars; every inner product is reduced per warp
+// of a work tile and then per system in a fixed order, so results do not depend on the launch shape.
+//
+// Launch structure of one PCG iteration: SpMV (+ direction update, p.q partials); scalars; the finest
+// restriction with the x/r update fused in; the restrictions of the next levels; the V-cycle below a
+// size cutoff in one CTA per block (shared memory); the prolongations up to level 1; the finest
+// prolongation with the r.z partials fused in; scalars.  The pre-smoothing sweep from zero is never
+// stored: x0 = w b / diag is formed where it is read.
 #include <cmath>
 #include <cstdio>
 #include "common.cuh"
@@ -61,20 +67,6 @@ __device__ __forceinline__ void mg_unflatten(const MgBlock& B, int l, int& x, in
     z = t / B.sy;
 }
 
-// y = A x on a level (stencil rows through the structured neighbours)
-template <typename T, int D>
-__device__ __forceinline__ T mg_apply(const pict_mg_level_t& L, const T* coef, const T* xv, int i, const MgBlock& B,
-                                      int x, int y, int z) {
-    const int N = L.num_cells;
-    T acc = coef[i] * xv[i];
-#pragma unroll
-    for (int f = 0; f < 2 * D; ++f) {
-        const int j = mg_nbr(B, x, y, z, f);
-        if (j >= 0) acc += coef[(size_t)(f + 1) * N + i] * xv[j];
-    }
-    return acc;
-}
-
 // ---------------------------------------------------------------------------------------------
 // Galerkin coarse operator: one thread per coarse cell, summing the couplings of its children
 // ---------------------------------------------------------------------------------------------
@@ -116,215 +108,663 @@ __global__ void k_mg_galerkin(pict_mg_level_t F, pict_mg_level_t C) {
     }
 }
 
-// x_out = x_in + w (b - A x_in) / diag   (x_in == nullptr: x_out = w b / diag)
-template <typename T, int D>
-__global__ void k_mg_jacobi(pict_mg_level_t L, const T* bv, const T* xin, T* xout, T w) {
-    const T* coef = reinterpret_cast<const T*>(L.coef);
-    PICT_CELL_LOOP(i, L.num_cells) {
-        const T d = coef[i];
-        const T rd = (d != T(0)) ? w / d : T(0);
-        if (!xin) {
-            xout[i] = rd * bv[i];
+// ---------------------------------------------------------------------------------------------
+// Tile kernels.  One CTA per work tile of a level ([system, block, first cell, count]); each thread
+// handles MG_CPT cells of a pass with branch-free, independent loads.
+// ---------------------------------------------------------------------------------------------
+constexpr int MG_TPB = 256;
+constexpr int MG_CPT = 2;
+constexpr int MG_PASS = MG_TPB * MG_CPT;  // cells of one pass of a tile CTA
+constexpr int MG_STAGE = 4096;            // cells of the shared-memory stage of the 2D tile kernels
+constexpr int MG_NW = MG_TPB / 32;        // warps of a tile CTA (partial sums are written per warp)
+
+struct MgTile {
+    int sys, blk, s0, cnt;
+};
+
+__device__ __forceinline__ MgTile mg_tile(const int32_t* tiles, int t) {
+    const int32_t* p = tiles + 4 * t;
+    return MgTile{p[0], p[1], p[2], p[3]};
+}
+
+template <typename T>
+__device__ __forceinline__ T mg_div(T a, T b);
+template <>
+__device__ __forceinline__ float mg_div<float>(float a, float b) { return __fdividef(a, b); }
+template <>
+__device__ __forceinline__ double mg_div<double>(double a, double b) { return a / b; }
+
+// the pre-smoothing sweep from zero at a cell: x0 = w b / diag
+template <typename T>
+__device__ __forceinline__ T mg_x0(T d, T b, T w) {
+    return (d != T(0)) ? mg_div(w * b, d) : T(0);
+}
+
+// The neighbours of a cell across its 2D faces, branch-free: where a fixed face has no neighbour the
+// index is the cell itself and ok is false (its term is masked), so every gather load is unconditional
+// and the loads of several cells can be in flight together.
+template <int D>
+struct MgNbrs {
+    int j[2 * D];
+    int c[2 * D][3];
+    bool ok[2 * D];
+};
+
+template <int D>
+__device__ __forceinline__ void mg_nbrs(const MgBlock& B, int x, int y, int z, MgNbrs<D>& nb) {
+    const int p[3] = {x, y, z};
+    const int n[3] = {B.sx, B.sy, B.sz};
+    const int per[3] = {B.px, B.py, B.pz};
+#pragma unroll
+    for (int f = 0; f < 2 * D; ++f) {
+        const int a = f >> 1;
+        const int c = p[a];
+        int v;
+        bool ok;
+        if (f & 1) {
+            ok = c + 1 < n[a] || per[a];
+            v = c + 1 < n[a] ? c + 1 : (per[a] ? 0 : c);
         } else {
-            const MgBlock B = mg_block(L, L.cell_block[i]);
-            int x, y, z;
-            mg_unflatten(B, i - B.off, x, y, z);
-            xout[i] = xin[i] + rd * (bv[i] - mg_apply<T, D>(L, coef, xin, i, B, x, y, z));
+            ok = c > 0 || per[a];
+            v = c > 0 ? c - 1 : (per[a] ? n[a] - 1 : c);
         }
+        int q[3] = {x, y, z};
+        q[a] = v;
+        nb.c[f][0] = q[0];
+        nb.c[f][1] = q[1];
+        nb.c[f][2] = q[2];
+        nb.ok[f] = ok;
+        nb.j[f] = B.off + q[0] + B.sx * (q[1] + B.sy * q[2]);
     }
 }
 
-// b_c = R (b - A x) on the children of each coarse cell
-template <typename T, int D>
-__global__ void k_mg_residual_restrict(pict_mg_level_t F, pict_mg_level_t C, const T* bv, const T* xv, T* bc) {
-    const T* cf = reinterpret_cast<const T*>(F.coef);
-    PICT_CELL_LOOP(I, C.num_cells) {
-        const int b = C.cell_block[I];
-        const MgBlock Bc = mg_block(C, b), Bf = mg_block(F, b);
-        int X, Y, Z;
-        mg_unflatten(Bc, I - Bc.off, X, Y, Z);
-        T acc = 0;
-        for (int dz = 0; dz < (1 << Bc.shz); ++dz)
-            for (int dy = 0; dy < (1 << Bc.shy); ++dy)
-                for (int dx = 0; dx < (1 << Bc.shx); ++dx) {
-                    const int x = (X << Bc.shx) + dx, y = (Y << Bc.shy) + dy, z = (Z << Bc.shz) + dz;
-                    if (x >= Bf.sx || y >= Bf.sy || z >= Bf.sz) continue;
-                    const int i = Bf.off + x + Bf.sx * (y + Bf.sy * z);
-                    acc += bv[i] - mg_apply<T, D>(F, cf, xv, i, Bf, x, y, z);
+// right-hand side of the finest V-cycle at a cell: r, or r - alpha q when the PCG update is fused
+template <typename T, bool UPD>
+struct MgRhs {
+    const T* __restrict__ r;
+    const T* __restrict__ q;
+    T al;
+    __device__ __forceinline__ T operator()(int j) const { return UPD ? r[j] - al * q[j] : r[j]; }
+};
+
+__device__ __forceinline__ int mg_coarse_index(const MgBlock& Bc, int x, int y, int z) {
+    return Bc.off + (x >> Bc.shx) + Bc.sx * ((y >> Bc.shy) + Bc.sy * (z >> Bc.shz));
+}
+
+__device__ __forceinline__ double mg_warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// this warp's slot of the partial sums: part[(tile * MG_NW + warp) * stride ..]
+__device__ __forceinline__ double* mg_warp_part(double* part, int stride) {
+    return part + ((size_t)blockIdx.x * MG_NW + (threadIdx.x >> 5)) * stride;
+}
+
+// b_c = R (b - A x0) over the children of each coarse cell.  UPD (finest level): b = r - alpha q is
+// formed on the fly and stored to rn, and x += alpha p (x = alpha p when first) for the children.
+//
+// 2D tiles whose fine rows (children rows plus one halo row on each side) fit the stage (cap cells) take
+// the staged path: b and x0 of those rows are formed once into shared memory, then each coarse cell
+// sums its children's residuals from there (a y-periodic wrap forms x0 of that neighbour from global).
+template <typename T, int D, bool UPD>
+__global__ void __launch_bounds__(MG_TPB, 4) k_mg_restrict(pict_mg_level_t F, pict_mg_level_t C,
+                                                           const T* __restrict__ r, const T* __restrict__ q,
+                                                           T* __restrict__ rn, T* __restrict__ x,
+                                                           const T* __restrict__ p, const double* __restrict__ sc,
+                                                           int first, T* __restrict__ bc, T w, int cap) {
+    extern __shared__ __align__(16) unsigned char mg_stage_raw[];
+    const MgTile tl = mg_tile(C.tiles, blockIdx.x);
+    const MgBlock Bc = mg_block(C, tl.blk), Bf = mg_block(F, tl.blk);
+    const T* __restrict__ cf = reinterpret_cast<const T*>(F.coef);
+    const int Nf = F.num_cells;
+    const T al = UPD ? (T)sc[MG_SC * tl.sys + 1] : T(0);
+    const MgRhs<T, UPD> rhs{r, q, al};
+    const int sx = Bf.sx;
+    int ylo = 0, yhi = -1;
+    if (D == 2) {
+        const int lc0 = tl.s0 - Bc.off, lc1 = lc0 + tl.cnt - 1;
+        ylo = max(0, ((lc0 / Bc.sx) << Bc.shy) - 1);
+        yhi = min(Bf.sy - 1, ((lc1 / Bc.sx + 1) << Bc.shy));
+    }
+    if (D == 2 && (yhi - ylo + 1) * sx <= cap) {
+        T* s_x0 = reinterpret_cast<T*>(mg_stage_raw);
+        T* s_b = s_x0 + cap;
+        T* s_d = s_b + cap;
+        const int lo = Bf.off + ylo * sx, nh = (yhi - ylo + 1) * sx;
+        const int lc0 = tl.s0 - Bc.off, lc1 = lc0 + tl.cnt - 1;
+        const int dq = MG_TPB / sx, dr = MG_TPB - dq * sx;
+        int yy = (int)threadIdx.x / sx, xx = (int)threadIdx.x - yy * sx;
+        yy += ylo;
+        for (int e = threadIdx.x; e < nh; e += MG_TPB) {
+            const int i = lo + e;
+            const T bi = rhs(i), di = cf[i];
+            s_x0[e] = mg_x0(di, bi, w);
+            s_b[e] = bi;
+            s_d[e] = di;
+            if (UPD) {
+                const int par = (xx >> Bc.shx) + Bc.sx * (yy >> Bc.shy);
+                if (par >= lc0 && par <= lc1) {
+                    rn[i] = bi;
+                    x[i] = first ? al * p[i] : x[i] + al * p[i];
                 }
-        bc[I] = acc;
-    }
-}
-
-// prolongation fused into the post-smoothing sweep: with x' = x_f + s P e_c (formed on the fly for
-// the neighbours), x_out = x' + w (b - A x') / diag
-template <typename T, int D>
-__global__ void k_mg_prolong_jacobi(pict_mg_level_t F, pict_mg_level_t C, const T* bv, const T* xf, const T* ec,
-                                    T* xout, T s, T w) {
-    const T* coef = reinterpret_cast<const T*>(F.coef);
-    const int N = F.num_cells;
-    PICT_CELL_LOOP(i, N) {
-        const int b = F.cell_block[i];
-        const MgBlock Bf = mg_block(F, b), Bc = mg_block(C, b);
-        int x, y, z;
-        mg_unflatten(Bf, i - Bf.off, x, y, z);
-        const T xi = xf[i] + s * ec[Bc.off + (x >> Bc.shx) + Bc.sx * ((y >> Bc.shy) + Bc.sy * (z >> Bc.shz))];
-        const T d = coef[i];
-        T acc = d * xi;
-#pragma unroll
-        for (int f = 0; f < 2 * D; ++f) {
-            int q[3] = {x, y, z};
-            const int j = mg_nbr_q(Bf, q, f);
-            if (j < 0) continue;
-            const T xj = xf[j] + s * ec[Bc.off + (q[0] >> Bc.shx) + Bc.sx * ((q[1] >> Bc.shy) + Bc.sy * (q[2] >> Bc.shz))];
-            acc += coef[(size_t)(f + 1) * N + i] * xj;
-        }
-        xout[i] = xi + ((d != T(0)) ? w * (bv[i] - acc) / d : T(0));
-    }
-}
-
-// coarsest level: `sweeps` damped-Jacobi sweeps from zero and mean removal, one CTA per block with the
-// iterate in shared memory (coarsest blocks hold at most MG_COARSE_MAX cells)
-constexpr int MG_COARSE_MAX = 256;
-
-template <typename T, int D>
-__global__ void k_mg_coarse_solve(pict_mg_level_t L, const T* bv, T* xout, T w, int sweeps) {
-    __shared__ T s_x[2][MG_COARSE_MAX];
-    __shared__ double s_red[32];
-    __shared__ double s_mean;
-    const T* coef = reinterpret_cast<const T*>(L.coef);
-    const int N = L.num_cells;
-    const MgBlock B = mg_block(L, blockIdx.x);
-    const int n = B.sx * B.sy * B.sz;
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-        const T d = coef[B.off + k];
-        s_x[0][k] = (d != T(0)) ? w * bv[B.off + k] / d : T(0);
-    }
-    __syncthreads();
-    int cur = 0;
-    for (int it = 1; it < sweeps; ++it) {
-        for (int k = threadIdx.x; k < n; k += blockDim.x) {
-            const int i = B.off + k;
-            int x, y, z;
-            mg_unflatten(B, k, x, y, z);
-            T acc = coef[i] * s_x[cur][k];
-#pragma unroll
-            for (int f = 0; f < 2 * D; ++f) {
-                const int j = mg_nbr(B, x, y, z, f);
-                if (j >= 0) acc += coef[(size_t)(f + 1) * N + i] * s_x[cur][j - B.off];
             }
-            const T d = coef[i];
-            s_x[cur ^ 1][k] = s_x[cur][k] + ((d != T(0)) ? w * (bv[i] - acc) / d : T(0));
+            xx += dr;
+            yy += dq;
+            if (xx >= sx) {
+                xx -= sx;
+                ++yy;
+            }
         }
         __syncthreads();
-        cur ^= 1;
-    }
-    double acc = 0.0;
-    for (int k = threadIdx.x; k < n; k += blockDim.x) acc += (double)s_x[cur][k];
+        auto far = [&](int xq, int yq) -> T {
+            const int j = Bf.off + xq + sx * yq;
+            return mg_x0(cf[j], rhs(j), w);
+        };
+        const int dqc = MG_TPB / Bc.sx, drc = MG_TPB - dqc * Bc.sx;
+        const int l = lc0 + (int)threadIdx.x;
+        int Y = l / Bc.sx, X = l - Y * Bc.sx;
+        for (int k = threadIdx.x; k < tl.cnt; k += MG_TPB) {
+            T acc = T(0);
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = acc;
-    __syncthreads();
+            for (int ch = 0; ch < 4; ++ch) {
+                const int dx = ch & 1, dy = ch >> 1;
+                const int xs = (X << Bc.shx) + dx, ys = (Y << Bc.shy) + dy;
+                const bool valid = !((dx && !Bc.shx) || (dy && !Bc.shy)) && xs < sx && ys < Bf.sy;
+                if (!valid) continue;
+                const int i = Bf.off + xs + sx * ys, c = (ys - ylo) * sx + xs;
+                const T xi = s_x0[c];
+                const T xm = xs > 0 ? s_x0[c - 1] : s_x0[c + sx - 1];
+                const T xp = xs + 1 < sx ? s_x0[c + 1] : s_x0[c - sx + 1];
+                const T ym = ys > 0 ? s_x0[c - sx] : (Bf.py ? far(xs, Bf.sy - 1) : T(0));
+                const T yp = ys + 1 < Bf.sy ? s_x0[c + sx] : (Bf.py ? far(xs, 0) : T(0));
+                T ax = s_d[c] * xi;
+                ax += (xs > 0 || Bf.px) ? cf[(size_t)Nf + i] * xm : T(0);
+                ax += (xs + 1 < sx || Bf.px) ? cf[(size_t)2 * Nf + i] * xp : T(0);
+                ax += (ys > 0 || Bf.py) ? cf[(size_t)3 * Nf + i] * ym : T(0);
+                ax += (ys + 1 < Bf.sy || Bf.py) ? cf[(size_t)4 * Nf + i] * yp : T(0);
+                acc += s_b[c] - ax;
+            }
+            bc[tl.s0 + k] = acc;
+            X += drc;
+            Y += dqc;
+            if (X >= Bc.sx) {
+                X -= Bc.sx;
+                ++Y;
+            }
+        }
+        return;
+    }
+    for (int base = 0; base < tl.cnt; base += MG_PASS) {
+        T acc[MG_CPT];
+#pragma unroll
+        for (int k = 0; k < MG_CPT; ++k) {
+            const int l0 = base + k * MG_TPB + (int)threadIdx.x;
+            const bool live = l0 < tl.cnt;
+            const int l = live ? l0 : tl.cnt - 1;
+            int X, Y, Z;
+            mg_unflatten(Bc, tl.s0 + l - Bc.off, X, Y, Z);
+            acc[k] = T(0);
+#pragma unroll
+            for (int c = 0; c < (1 << D); ++c) {
+                const int dx = c & 1, dy = (c >> 1) & 1, dz = (c >> 2) & 1;
+                int xs = (X << Bc.shx) + dx, ys = (Y << Bc.shy) + dy, zs = (Z << Bc.shz) + dz;
+                const bool valid = !((dx && !Bc.shx) || (dy && !Bc.shy) || (dz && !Bc.shz)) && xs < Bf.sx &&
+                                   ys < Bf.sy && zs < Bf.sz;
+                if (!valid) {  // the first child always exists
+                    xs = X << Bc.shx;
+                    ys = Y << Bc.shy;
+                    zs = Z << Bc.shz;
+                }
+                const int i = Bf.off + xs + Bf.sx * (ys + Bf.sy * zs);
+                MgNbrs<D> nb;
+                mg_nbrs<D>(Bf, xs, ys, zs, nb);
+                const T bi = rhs(i);
+                const T di = cf[i];
+                T ax = di * mg_x0(di, bi, w);
+#pragma unroll
+                for (int f = 0; f < 2 * D; ++f) {
+                    const T cj = cf[(size_t)(f + 1) * Nf + i];
+                    const T xj = mg_x0(cf[nb.j[f]], rhs(nb.j[f]), w);
+                    ax += nb.ok[f] ? cj * xj : T(0);
+                }
+                if (UPD && valid && live) {
+                    rn[i] = bi;
+                    x[i] = first ? al * p[i] : x[i] + al * p[i];
+                }
+                acc[k] += valid ? bi - ax : T(0);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < MG_CPT; ++k) {
+            const int l = base + k * MG_TPB + (int)threadIdx.x;
+            if (l < tl.cnt) bc[tl.s0 + l] = acc[k];
+        }
+    }
+}
+
+// post-smoothing with the coarse correction: x' = x0 + s P e_c (formed on the fly, also for the
+// neighbours), out = x' + w (b - A x') / diag.  DOT (finest level): per-warp partials of b.out, b.b,
+// sum(out), sum(b).
+//
+// 2D tiles whose rows plus one halo row on each side fit the stage (cap cells) take the staged path:
+// x' of every cell of [first - sx, last + sx] is formed once into shared memory (with b and diag), then
+// the stencil reads its neighbours there; a y-periodic wrap reaches outside the stage and forms x' of
+// that neighbour from global memory.
+template <typename T, int D, bool DOT>
+__global__ void __launch_bounds__(MG_TPB, 4) k_mg_prolong(pict_mg_level_t F, pict_mg_level_t C, const int32_t* tiles,
+                                                          const T* __restrict__ bv, const T* __restrict__ ec,
+                                                          T* __restrict__ out, T s, T w, double* __restrict__ part,
+                                                          int cap) {
+    extern __shared__ __align__(16) unsigned char mg_stage_raw[];
+    const MgTile tl = mg_tile(tiles, blockIdx.x);
+    const MgBlock Bf = mg_block(F, tl.blk), Bc = mg_block(C, tl.blk);
+    const T* __restrict__ cf = reinterpret_cast<const T*>(F.coef);
+    const int N = F.num_cells;
+    double a = 0.0, c2 = 0.0, sz = 0.0, sr = 0.0;
+    const int sx = Bf.sx;
+    if (D == 2 && tl.cnt + 2 * sx <= cap) {
+        T* s_x = reinterpret_cast<T*>(mg_stage_raw);
+        T* s_b = s_x + cap;
+        T* s_d = s_b + cap;
+        const int nf = sx * Bf.sy;
+        const int lo = max(Bf.off, tl.s0 - sx), hi = min(Bf.off + nf, tl.s0 + tl.cnt + sx);
+        const int dq = MG_TPB / sx, dr = MG_TPB - dq * sx;
+        int l = lo - Bf.off + (int)threadIdx.x;
+        int y = l / sx, x = l - y * sx;
+        for (int e = threadIdx.x; e < hi - lo; e += MG_TPB) {
+            const int i = lo + e;
+            const T d = cf[i], b = bv[i];
+            s_x[e] = mg_x0(d, b, w) + s * ec[Bc.off + (x >> Bc.shx) + Bc.sx * (y >> Bc.shy)];
+            s_b[e] = b;
+            s_d[e] = d;
+            x += dr;
+            y += dq;
+            if (x >= sx) {
+                x -= sx;
+                ++y;
+            }
+        }
+        __syncthreads();
+        // x' of a neighbour across the y-periodic wrap (outside the stage)
+        auto far = [&](int xq, int yq) -> T {
+            const int j = Bf.off + xq + sx * yq;
+            return mg_x0(cf[j], bv[j], w) + s * ec[Bc.off + (xq >> Bc.shx) + Bc.sx * (yq >> Bc.shy)];
+        };
+        l = tl.s0 - Bf.off + (int)threadIdx.x;
+        y = l / sx;
+        x = l - y * sx;
+        for (int k = threadIdx.x; k < tl.cnt; k += MG_TPB) {
+            const int i = tl.s0 + k, c = i - lo;
+            const T xi = s_x[c], di = s_d[c], bi = s_b[c];
+            const T xm = x > 0 ? s_x[c - 1] : s_x[c + sx - 1];
+            const T xp = x + 1 < sx ? s_x[c + 1] : s_x[c - sx + 1];
+            const bool okm = x > 0 || Bf.px, okp = x + 1 < sx || Bf.px;
+            const T ym = y > 0 ? s_x[c - sx] : (Bf.py ? far(x, Bf.sy - 1) : T(0));
+            const T yp = y + 1 < Bf.sy ? s_x[c + sx] : (Bf.py ? far(x, 0) : T(0));
+            T acc = di * xi;
+            acc += okm ? cf[(size_t)N + i] * xm : T(0);
+            acc += okp ? cf[(size_t)2 * N + i] * xp : T(0);
+            acc += (y > 0 || Bf.py) ? cf[(size_t)3 * N + i] * ym : T(0);
+            acc += (y + 1 < Bf.sy || Bf.py) ? cf[(size_t)4 * N + i] * yp : T(0);
+            const T zi = xi + ((di != T(0)) ? mg_div(w * (bi - acc), di) : T(0));
+            out[i] = zi;
+            if (DOT) {
+                a += (double)bi * (double)zi;
+                c2 += (double)bi * (double)bi;
+                sz += (double)zi;
+                sr += (double)bi;
+            }
+            x += dr;
+            y += dq;
+            if (x >= sx) {
+                x -= sx;
+                ++y;
+            }
+        }
+    } else {
+        for (int base = 0; base < tl.cnt; base += MG_PASS) {
+            T zv[MG_CPT], bvk[MG_CPT];
+#pragma unroll
+            for (int k = 0; k < MG_CPT; ++k) {
+                const int l0 = base + k * MG_TPB + (int)threadIdx.x;
+                const int l = l0 < tl.cnt ? l0 : tl.cnt - 1;
+                const int i = tl.s0 + l;
+                int x, y, z;
+                mg_unflatten(Bf, i - Bf.off, x, y, z);
+                MgNbrs<D> nb;
+                mg_nbrs<D>(Bf, x, y, z, nb);
+                const T di = cf[i], bi = bv[i];
+                const T xi = mg_x0(di, bi, w) + s * ec[mg_coarse_index(Bc, x, y, z)];
+                T acc = di * xi;
+#pragma unroll
+                for (int f = 0; f < 2 * D; ++f) {
+                    const int j = nb.j[f];
+                    const T cj = cf[(size_t)(f + 1) * N + i];
+                    const T xj =
+                        mg_x0(cf[j], bv[j], w) + s * ec[mg_coarse_index(Bc, nb.c[f][0], nb.c[f][1], nb.c[f][2])];
+                    acc += nb.ok[f] ? cj * xj : T(0);
+                }
+                zv[k] = xi + ((di != T(0)) ? mg_div(w * (bi - acc), di) : T(0));
+                bvk[k] = bi;
+            }
+#pragma unroll
+            for (int k = 0; k < MG_CPT; ++k) {
+                const int l = base + k * MG_TPB + (int)threadIdx.x;
+                if (l >= tl.cnt) continue;
+                out[tl.s0 + l] = zv[k];
+                if (DOT) {
+                    const double ri = (double)bvk[k], zi = (double)zv[k];
+                    a += ri * zi;
+                    c2 += ri * ri;
+                    sz += zi;
+                    sr += ri;
+                }
+            }
+        }
+    }
+    if (DOT) {
+        a = mg_warp_sum(a);
+        c2 = mg_warp_sum(c2);
+        sz = mg_warp_sum(sz);
+        sr = mg_warp_sum(sr);
+        if ((threadIdx.x & 31) == 0) {
+            double* P = mg_warp_part(part, 4);
+            P[0] = a;
+            P[1] = c2;
+            P[2] = sz;
+            P[3] = sr;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// The V-cycle below a size cutoff in one launch: one CTA per block runs the levels lv[0..n-1] of its
+// block (restriction down to the coarsest, `sweeps` damped-Jacobi sweeps from zero and mean removal on
+// the coarsest, prolongation and post-smoothing up) with every level's right-hand side, iterate and
+// stencil in shared memory (the stencils are loaded once, at the start).  bin: right-hand side of lv[0]
+// (global), xout: its iterate.
+// ---------------------------------------------------------------------------------------------
+constexpr int MG_SUB_LEVELS = 16;
+constexpr int MG_SUB_THREADS = 512;
+constexpr int MG_SUB_MAX = 2048;            // the cycle moves into one CTA per block from the first level
+constexpr size_t MG_SUB_SMEM = 160 * 1024;  // whose blocks have at most this many cells and whose
+                                            // sub-cycle fits this much shared memory
+
+struct MgSub {
+    pict_mg_level_t lv[MG_SUB_LEVELS];
+    int n;
+};
+
+// shared memory of the sub-cycle: b, x and the 2D+1 stencil rows of every level (this block's cells)
+// and one scratch vector
+static size_t mg_sub_smem(const pict_mg_level_t* lv, int n, size_t esz) {
+    const size_t K = 2 * (size_t)lv[0].dims + 1;
+    size_t c = (size_t)lv[0].max_block_cells;
+    for (int k = 0; k < n; ++k) c += (2 + K) * (size_t)lv[k].max_block_cells;
+    return c * esz;
+}
+
+template <typename T, int D>
+__global__ void __launch_bounds__(MG_SUB_THREADS) k_mg_subcycle(MgSub S, const T* __restrict__ bin,
+                                                                T* __restrict__ xout, T w, T sp, int sweeps) {
+    constexpr int K = 2 * D + 1;
+    extern __shared__ __align__(16) unsigned char mg_sub_raw[];
+    T* sm = reinterpret_cast<T*>(mg_sub_raw);
+    __shared__ int s_off[MG_SUB_LEVELS + 1];
+    __shared__ double s_red[32];
+    __shared__ double s_mean;
+    const int b = blockIdx.x;
     if (threadIdx.x == 0) {
-        double v = 0.0;
-        for (int wv = 0; wv < (int)(blockDim.x >> 5); ++wv) v += s_red[wv];
-        s_mean = v / (double)n;
+        int o = 0;
+        for (int k = 0; k < S.n; ++k) {
+            const MgBlock B = mg_block(S.lv[k], b);
+            s_off[k] = o;
+            o += (2 + K) * B.sx * B.sy * B.sz;
+        }
+        s_off[S.n] = o;
     }
     __syncthreads();
-    const T m = (T)s_mean;
-    for (int k = threadIdx.x; k < n; k += blockDim.x) xout[B.off + k] = s_x[cur][k] - m;
+    T* scr = sm + s_off[S.n];
+    // level k of this block: b at sm + s_off[k], x after it, then the stencil rows
+    for (int k = 0; k < S.n; ++k) {
+        const pict_mg_level_t& L = S.lv[k];
+        const MgBlock B = mg_block(L, b);
+        const int n = B.sx * B.sy * B.sz;
+        const T* __restrict__ cf = reinterpret_cast<const T*>(L.coef);
+        T* sc = sm + s_off[k] + 2 * n;
+        for (int f = 0; f < K; ++f)
+            for (int e = threadIdx.x; e < n; e += blockDim.x) sc[f * n + e] = cf[(size_t)f * L.num_cells + B.off + e];
+        if (k == 0)
+            for (int e = threadIdx.x; e < n; e += blockDim.x) sm[s_off[0] + e] = bin[B.off + e];
+    }
+    __syncthreads();
+    // down: x0 = w b / diag (kept in the level's x), b_c = R (b - A x0)
+    for (int k = 0; k + 1 < S.n; ++k) {
+        const MgBlock Bf = mg_block(S.lv[k], b), Bc = mg_block(S.lv[k + 1], b);
+        const int nf = Bf.sx * Bf.sy * Bf.sz, nc = Bc.sx * Bc.sy * Bc.sz;
+        T* sb = sm + s_off[k];
+        T* sx = sb + nf;
+        const T* sc = sx + nf;
+        T* sbc = sm + s_off[k + 1];
+        for (int e = threadIdx.x; e < nf; e += blockDim.x) sx[e] = mg_x0(sc[e], sb[e], w);
+        __syncthreads();
+        for (int E = threadIdx.x; E < nc; E += blockDim.x) {
+            int X, Y, Z;
+            mg_unflatten(Bc, E, X, Y, Z);
+            T acc = T(0);
+            for (int c = 0; c < (1 << D); ++c) {
+                const int dx = c & 1, dy = (c >> 1) & 1, dz = (c >> 2) & 1;
+                if ((dx && !Bc.shx) || (dy && !Bc.shy) || (dz && !Bc.shz)) continue;
+                const int xs = (X << Bc.shx) + dx, ys = (Y << Bc.shy) + dy, zs = (Z << Bc.shz) + dz;
+                if (xs >= Bf.sx || ys >= Bf.sy || zs >= Bf.sz) continue;
+                const int il = xs + Bf.sx * (ys + Bf.sy * zs);
+                T ax = sc[il] * sx[il];
+#pragma unroll
+                for (int f = 0; f < 2 * D; ++f) {
+                    const int j = mg_nbr(Bf, xs, ys, zs, f);
+                    if (j >= 0) ax += sc[(f + 1) * nf + il] * sx[j - Bf.off];
+                }
+                acc += sb[il] - ax;
+            }
+            sbc[E] = acc;
+        }
+        __syncthreads();
+    }
+    // coarsest: sweeps from zero (ping-pong between x and the scratch vector), then mean removal
+    {
+        const MgBlock B = mg_block(S.lv[S.n - 1], b);
+        const int n = B.sx * B.sy * B.sz;
+        T* sb = sm + s_off[S.n - 1];
+        T* const xa = sb + n;
+        const T* sc = xa + n;
+        for (int e = threadIdx.x; e < n; e += blockDim.x) xa[e] = mg_x0(sc[e], sb[e], w);
+        __syncthreads();
+        int cur = 0;
+        for (int it = 1; it < sweeps; ++it) {
+            const T* xs = cur ? scr : xa;
+            T* xd = cur ? xa : scr;
+            for (int e = threadIdx.x; e < n; e += blockDim.x) {
+                int x, y, z;
+                mg_unflatten(B, e, x, y, z);
+                T acc = sc[e] * xs[e];
+#pragma unroll
+                for (int f = 0; f < 2 * D; ++f) {
+                    const int j = mg_nbr(B, x, y, z, f);
+                    if (j >= 0) acc += sc[(f + 1) * n + e] * xs[j - B.off];
+                }
+                const T d = sc[e];
+                xd[e] = xs[e] + ((d != T(0)) ? mg_div(w * (sb[e] - acc), d) : T(0));
+            }
+            __syncthreads();
+            cur ^= 1;
+        }
+        const T* xr = cur ? scr : xa;
+        double acc = 0.0;
+        for (int e = threadIdx.x; e < n; e += blockDim.x) acc += (double)xr[e];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = acc;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double v = 0.0;
+            for (int wv = 0; wv < (int)(blockDim.x >> 5); ++wv) v += s_red[wv];
+            s_mean = v / (double)n;
+        }
+        __syncthreads();
+        const T m = (T)s_mean;
+        for (int e = threadIdx.x; e < n; e += blockDim.x) xa[e] = xr[e] - m;
+        __syncthreads();
+    }
+    // up: x' = x0 + sp P x_c (scratch), x = x' + w (b - A x') / diag
+    for (int k = S.n - 2; k >= 0; --k) {
+        const MgBlock Bf = mg_block(S.lv[k], b), Bc = mg_block(S.lv[k + 1], b);
+        const int nf = Bf.sx * Bf.sy * Bf.sz, nc = Bc.sx * Bc.sy * Bc.sz;
+        T* sb = sm + s_off[k];
+        T* sx = sb + nf;
+        const T* sc = sx + nf;
+        const T* sxc = sm + s_off[k + 1] + nc;
+        for (int e = threadIdx.x; e < nf; e += blockDim.x) {
+            int x, y, z;
+            mg_unflatten(Bf, e, x, y, z);
+            scr[e] = sx[e] + sp * sxc[(x >> Bc.shx) + Bc.sx * ((y >> Bc.shy) + Bc.sy * (z >> Bc.shz))];
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < nf; e += blockDim.x) {
+            int x, y, z;
+            mg_unflatten(Bf, e, x, y, z);
+            T acc = sc[e] * scr[e];
+#pragma unroll
+            for (int f = 0; f < 2 * D; ++f) {
+                const int j = mg_nbr(Bf, x, y, z, f);
+                if (j >= 0) acc += sc[(f + 1) * nf + e] * scr[j - Bf.off];
+            }
+            const T d = sc[e];
+            sx[e] = scr[e] + ((d != T(0)) ? mg_div(w * (sb[e] - acc), d) : T(0));
+        }
+        __syncthreads();
+    }
+    {
+        const MgBlock B = mg_block(S.lv[0], b);
+        const int n = B.sx * B.sy * B.sz;
+        const T* sx = sm + s_off[0] + n;
+        for (int e = threadIdx.x; e < n; e += blockDim.x) xout[B.off + e] = sx[e];
+    }
 }
 
 // ---------------------------------------------------------------------------------------------
 // PCG vector kernels on the finest level; per-system scalars in FP64
 // ---------------------------------------------------------------------------------------------
-__device__ __forceinline__ double mg_cta_sum(double v, double* s_red) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    __syncthreads();
-    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = v;
-    __syncthreads();
-    double r = 0.0;
-    if (threadIdx.x < 32) {
-        r = threadIdx.x < (blockDim.x >> 5) ? s_red[threadIdx.x] : 0.0;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
-    }
-    return r;
-}
 
-// p_new = (z - m) + beta p_old formed on the fly (also for the neighbours), q = A p_new, and the tile
-// partial of p_new.q (one CTA per work tile of the domain); m, beta per system from sc
+// p_new = (z - m) + beta p_old formed on the fly (also for the neighbours; the first direction passes
+// p_old = z with beta = 0), q = A p_new, and the per-warp partials of p_new.q (one CTA per work tile of
+// the domain); m, beta per system from sc
 template <typename T, int D>
-__global__ void k_pcg_spmv_dot(pict_domain_t dom, pict_mg_level_t L, const T* z, const T* pold, T* pnew, T* q,
-                               const double* sc, double* part) {
-    __shared__ double s_red[32];
-    const T* coef = reinterpret_cast<const T*>(L.coef);
+__global__ void __launch_bounds__(MG_TPB) k_pcg_spmv_dot(pict_domain_t dom, pict_mg_level_t L, const T* __restrict__ z,
+                                                         const T* __restrict__ pold, T* __restrict__ pnew,
+                                                         T* __restrict__ q, const double* __restrict__ sc, int first,
+                                                         double* __restrict__ part) {
+    const T* __restrict__ coef = reinterpret_cast<const T*>(L.coef);
     const int N = L.num_cells;
-    const int t = blockIdx.x;
-    const int sys = dom.tiles[4 * t], s0 = dom.tiles[4 * t + 2], cnt = dom.tiles[4 * t + 3];
-    const MgBlock B = mg_block(L, dom.tiles[4 * t + 1]);
-    const T m = (T)sc[MG_SC * sys + 4], bt = (T)sc[MG_SC * sys + 2];
+    const MgTile tl = mg_tile(dom.tiles, blockIdx.x);
+    const MgBlock B = mg_block(L, tl.blk);
+    const T m = (T)sc[MG_SC * tl.sys + 4];
+    const T bt = first ? T(0) : (T)sc[MG_SC * tl.sys + 2];
     double acc = 0.0;
-    for (int i = s0 + threadIdx.x; i < s0 + cnt; i += blockDim.x) {
-        int x, y, z3;
-        mg_unflatten(B, i - B.off, x, y, z3);
-        const T pi = (z[i] - m) + bt * pold[i];
-        T qi = coef[i] * pi;
+    for (int base = 0; base < tl.cnt; base += MG_PASS) {
+        T pv[MG_CPT], qv[MG_CPT];
 #pragma unroll
-        for (int f = 0; f < 2 * D; ++f) {
-            const int j = mg_nbr(B, x, y, z3, f);
-            if (j >= 0) qi += coef[(size_t)(f + 1) * N + i] * ((z[j] - m) + bt * pold[j]);
+        for (int k = 0; k < MG_CPT; ++k) {
+            const int l0 = base + k * MG_TPB + (int)threadIdx.x;
+            const int l = l0 < tl.cnt ? l0 : tl.cnt - 1;
+            const int i = tl.s0 + l;
+            int x, y, z3;
+            mg_unflatten(B, i - B.off, x, y, z3);
+            MgNbrs<D> nb;
+            mg_nbrs<D>(B, x, y, z3, nb);
+            const T pi = (z[i] - m) + bt * pold[i];
+            T qi = coef[i] * pi;
+#pragma unroll
+            for (int f = 0; f < 2 * D; ++f) {
+                const int j = nb.j[f];
+                const T cj = coef[(size_t)(f + 1) * N + i];
+                const T pj = (z[j] - m) + bt * pold[j];
+                qi += nb.ok[f] ? cj * pj : T(0);
+            }
+            pv[k] = pi;
+            qv[k] = qi;
         }
-        pnew[i] = pi;
-        q[i] = qi;
-        acc += (double)pi * (double)qi;
+#pragma unroll
+        for (int k = 0; k < MG_CPT; ++k) {
+            const int l = base + k * MG_TPB + (int)threadIdx.x;
+            if (l >= tl.cnt) continue;
+            pnew[tl.s0 + l] = pv[k];
+            q[tl.s0 + l] = qv[k];
+            acc += (double)pv[k] * (double)qv[k];
+        }
     }
-    acc = mg_cta_sum(acc, s_red);
-    if (threadIdx.x == 0) part[t] = acc;
+    acc = mg_warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) *mg_warp_part(part, 1) = acc;
 }
 
-// tile partials of r.z, r.r, sum(z), sum(r)
+// per-warp partials of r.z, r.r, sum(z), sum(r) (one CTA per work tile)
 template <typename T>
-__global__ void k_pcg_dot4(pict_domain_t dom, const T* r, const T* z, double* part) {
-    __shared__ double s_red[32];
-    const int t = blockIdx.x;
-    const int s0 = dom.tiles[4 * t + 2], cnt = dom.tiles[4 * t + 3];
+__global__ void __launch_bounds__(MG_TPB) k_pcg_dot4(pict_domain_t dom, const T* r, const T* z, double* part) {
+    const MgTile tl = mg_tile(dom.tiles, blockIdx.x);
     double a = 0.0, c = 0.0, sz = 0.0, sr = 0.0;
-    for (int i = s0 + threadIdx.x; i < s0 + cnt; i += blockDim.x) {
+    for (int i = tl.s0 + threadIdx.x; i < tl.s0 + tl.cnt; i += MG_TPB) {
         const double ri = (double)r[i], zi = (double)z[i];
         a += ri * zi;
         c += ri * ri;
         sz += zi;
         sr += ri;
     }
-    a = mg_cta_sum(a, s_red);
-    c = mg_cta_sum(c, s_red);
-    sz = mg_cta_sum(sz, s_red);
-    sr = mg_cta_sum(sr, s_red);
-    if (threadIdx.x == 0) {
-        part[4 * t] = a;
-        part[4 * t + 1] = c;
-        part[4 * t + 2] = sz;
-        part[4 * t + 3] = sr;
+    a = mg_warp_sum(a);
+    c = mg_warp_sum(c);
+    sz = mg_warp_sum(sz);
+    sr = mg_warp_sum(sr);
+    if ((threadIdx.x & 31) == 0) {
+        double* P = mg_warp_part(part, 4);
+        P[0] = a;
+        P[1] = c;
+        P[2] = sz;
+        P[3] = sr;
     }
 }
 
-// per-system scalars (one warp per system, tiles summed lane-strided in a fixed order):
+// per-system scalars (one warp per system; the per-warp partials of its tiles summed lane-strided in
+// a fixed order):
 // stage 0: rho = r.(z - m), |r|^2, m = mean(z);  stage 1: alpha = rho / p.q;
 // stage 2: rho' = r.(z - m), beta = rho'/rho, rho = rho', |r|^2, m
 // The preconditioned residual z is used mean-free (z - m): the constant mode of a singular system is
 // undetermined.  sc[s*MG_SC + {0: rho, 1: alpha, 2: beta, 3: |r|^2, 4: m}]
-
-__global__ void k_pcg_scalars(pict_domain_t dom, const double* part, int stride, int stage, double* sc) {
+template <int STRIDE>
+__global__ void k_pcg_scalars(pict_domain_t dom, const double* __restrict__ part, int stage, double* sc) {
     const int lane = threadIdx.x & 31;
     const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (s >= dom.num_sims) return;
-    double v[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int t = dom.sim_tiles[s] + lane; t < dom.sim_tiles[s + 1]; t += 32)
-        for (int k = 0; k < stride; ++k) v[k] += part[(size_t)stride * t + k];
+    double v[4] = {0.0, 0.0, 0.0, 0.0}, u[STRIDE];
 #pragma unroll
-    for (int k = 0; k < 4; ++k)
+    for (int k = 0; k < STRIDE; ++k) u[k] = 0.0;
+    // two interleaved accumulators per lane (independent loads in flight), combined in a fixed order
+    const int t1 = dom.sim_tiles[s + 1] * MG_NW;
+    int t = dom.sim_tiles[s] * MG_NW + lane;
+    for (; t + 32 < t1; t += 64) {
+#pragma unroll
+        for (int k = 0; k < STRIDE; ++k) {
+            v[k] += part[(size_t)STRIDE * t + k];
+            u[k] += part[(size_t)STRIDE * (t + 32) + k];
+        }
+    }
+    if (t < t1) {
+#pragma unroll
+        for (int k = 0; k < STRIDE; ++k) v[k] += part[(size_t)STRIDE * t + k];
+    }
+#pragma unroll
+    for (int k = 0; k < STRIDE; ++k) v[k] += u[k];
+#pragma unroll
+    for (int k = 0; k < STRIDE; ++k)
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
     if (lane != 0) return;
@@ -347,33 +787,33 @@ __global__ void k_pcg_scalars(pict_domain_t dom, const double* part, int stride,
     S[4] = m;
 }
 
+// rn = r - alpha q, x += alpha p (x = alpha p when first), and the per-warp partials of
+// (0, rn.rn, 0, sum(rn)) (the PCG update where no V-cycle follows: the last iteration, or a
+// single-level hierarchy)
 template <typename T>
-__device__ __forceinline__ int cell_sys(const pict_domain_t& dom, int i) { return dom.blocks[dom.cell_block[i]].sim; }
-
-// x += alpha p, r -= alpha q, and the first pre-smoothing sweep of the next V-cycle on the finest
-// level: x0 = w r / diag
-template <typename T>
-__global__ void k_pcg_update_xr(pict_domain_t dom, pict_mg_level_t L, T* x, T* r, const T* p, const T* q,
-                                const double* sc, T* x0, T w) {
-    const T* coef = reinterpret_cast<const T*>(L.coef);
-    PICT_CELL_LOOP(i, dom.num_cells) {
-        const T al = (T)sc[MG_SC * cell_sys<T>(dom, i) + 1];
-        x[i] += al * p[i];
+__global__ void __launch_bounds__(MG_TPB) k_pcg_update(pict_domain_t dom, const T* __restrict__ r,
+                                                       const T* __restrict__ q, T* __restrict__ rn, T* __restrict__ x,
+                                                       const T* __restrict__ p, const double* __restrict__ sc, int first,
+                                                       double* __restrict__ part) {
+    const MgTile tl = mg_tile(dom.tiles, blockIdx.x);
+    const T al = (T)sc[MG_SC * tl.sys + 1];
+    double c2 = 0.0, sr = 0.0;
+    for (int l = threadIdx.x; l < tl.cnt; l += MG_TPB) {
+        const int i = tl.s0 + l;
         const T ri = r[i] - al * q[i];
-        r[i] = ri;
-        const T d = coef[i];
-        x0[i] = (d != T(0)) ? w * ri / d : T(0);
+        rn[i] = ri;
+        x[i] = first ? al * p[i] : x[i] + al * p[i];
+        c2 += (double)ri * (double)ri;
+        sr += (double)ri;
     }
-}
-
-// r = b, x = 0, search directions 0
-template <typename T>
-__global__ void k_pcg_init(int N, const T* b, T* r, T* x, T* p0, T* p1) {
-    PICT_CELL_LOOP(i, N) {
-        r[i] = b[i];
-        x[i] = T(0);
-        p0[i] = T(0);
-        p1[i] = T(0);
+    c2 = mg_warp_sum(c2);
+    sr = mg_warp_sum(sr);
+    if ((threadIdx.x & 31) == 0) {
+        double* P = mg_warp_part(part, 4);
+        P[0] = 0.0;
+        P[1] = c2;
+        P[2] = 0.0;
+        P[3] = sr;
     }
 }
 
@@ -393,87 +833,159 @@ __global__ void k_pcg_report(pict_domain_t dom, const double* sc, pict_solve_inf
     info[s] = inf;
 }
 
-template <typename T>
-static size_t vbytes(int n) { return ((size_t)n * sizeof(T) + 255) & ~(size_t)255; }
+// workspace: levels >= 1: b, x | finest: r (two, alternating), z, p (two, alternating), q | per-warp
+// partials | scalars.  Returns the bytes; fills the pointers when ws != nullptr.
+struct MgWork {
+    char* lb[16];
+    char* lx[16];
+    char* r[2];
+    char* z;
+    char* p[2];
+    char* q;
+    double* part;
+    double* sc;
+};
 
-// workspace: per level x0, x1, b (levels >= 1; level 0: x0, x1) | r, z, p, q | partials | scalars
+static size_t mg_carve(const pict_domain_t* dom, const pict_mg_level_t* levels, int nl, size_t esz, char* ws,
+                       MgWork* w) {
+    auto vb = [&](int n) { return ((size_t)n * esz + 255) & ~(size_t)255; };
+    size_t o = 0;
+    auto take = [&](size_t bytes) {
+        char* ptr = ws ? ws + o : nullptr;
+        o += bytes;
+        return ptr;
+    };
+    for (int l = 1; l < nl; ++l) {
+        w->lb[l] = take(vb(levels[l].num_cells));
+        w->lx[l] = take(vb(levels[l].num_cells));
+    }
+    const int N = dom->num_cells;
+    w->r[0] = take(vb(N));
+    w->r[1] = take(vb(N));
+    w->z = take(vb(N));
+    w->p[0] = take(vb(N));
+    w->p[1] = take(vb(N));
+    w->q = take(vb(N));
+    w->part = reinterpret_cast<double*>(take(((size_t)4 * MG_NW * dom->num_tiles * 8 + 255) & ~(size_t)255));
+    w->sc = reinterpret_cast<double*>(take(((size_t)MG_SC * dom->num_sims * 8 + 255) & ~(size_t)255));
+    return o;
+}
+
 template <typename T, int D>
 static pict_status_t run_pcg_mg(const pict_domain_t* dom, const pict_mg_level_t* levels, int nl, const T* rhs, T* xout,
                                 int iterations, double tol, int normalized, pict_solve_info_t* info, char* ws,
                                 int64_t ws_bytes, double omega, double scale, int coarse_sweeps, cudaStream_t st) {
     const int N = dom->num_cells;
-    // carve the workspace
-    char* w = ws;
-    T* lx0[16];
-    T* lx1[16];
+    MgWork W;
+    if ((int64_t)mg_carve(dom, levels, nl, sizeof(T), ws, &W) > ws_bytes)
+        return set_error(PICT_ERR_ARG, "pcg_mg: workspace too small");
+    for (int l = 1; l < nl; ++l)
+        if (levels[l].num_tiles <= 0 || !levels[l].tiles) return set_error(PICT_ERR_ARG, "pcg_mg: level without tiles");
     T* lb[16];
-    for (int l = 0; l < nl; ++l) {
-        const int n = levels[l].num_cells;
-        lx0[l] = reinterpret_cast<T*>(w); w += vbytes<T>(n);
-        lx1[l] = reinterpret_cast<T*>(w); w += vbytes<T>(n);
-        lb[l] = reinterpret_cast<T*>(w); w += vbytes<T>(n);
+    T* lx[16];
+    for (int l = 1; l < nl; ++l) {
+        lb[l] = reinterpret_cast<T*>(W.lb[l]);
+        lx[l] = reinterpret_cast<T*>(W.lx[l]);
     }
-    T* r = reinterpret_cast<T*>(w); w += vbytes<T>(N);
-    T* z = reinterpret_cast<T*>(w); w += vbytes<T>(N);
-    T* p = reinterpret_cast<T*>(w); w += vbytes<T>(N);
-    T* q = reinterpret_cast<T*>(w); w += vbytes<T>(N);
-    double* part = reinterpret_cast<double*>(w); w += ((size_t)4 * dom->num_tiles * 8 + 255) & ~(size_t)255;
-    double* sc = reinterpret_cast<double*>(w); w += ((size_t)MG_SC * dom->num_sims * 8 + 255) & ~(size_t)255;
-    if ((int64_t)(w - ws) > ws_bytes) return set_error(PICT_ERR_ARG, "pcg_mg: workspace too small");
+    T* rbuf[2] = {reinterpret_cast<T*>(W.r[0]), reinterpret_cast<T*>(W.r[1])};
+    T* z = reinterpret_cast<T*>(W.z);
+    T* pbuf[2] = {reinterpret_cast<T*>(W.p[0]), reinterpret_cast<T*>(W.p[1])};
+    T* q = reinterpret_cast<T*>(W.q);
+    double* part = W.part;
+    double* sc = W.sc;
 
-    auto grid_of = [](int n) { return cell_grid(n, 256); };
     const T wj = (T)omega, sp = (T)scale;
-    // z = M r (V-cycle); r is the finest right-hand side.  presmoothed: the first finest sweep
-    // (lx0[0] = w r / diag) was already written by the x/r update.  Every level's corrected iterate
-    // ends in lx1 (lx0 on the coarsest), so the prolongation reads it without copies.
-    auto vcycle = [&](const T* rhs0, T* z0, bool presmoothed) -> pict_status_t {
-        const T* b = rhs0;
-        for (int l = 0; l < nl; ++l) {
-            const pict_mg_level_t& L = levels[l];
-            if (l > 0) b = lb[l];
-            if (l == nl - 1) {
-                // coarsest: Jacobi sweeps from zero and mean removal in one launch, result in lx0
-                k_mg_coarse_solve<T, D><<<L.num_blocks, 64, 0, st>>>(L, b, lx0[l], wj, coarse_sweeps);
-                break;
-            }
-            if (l > 0 || !presmoothed) k_mg_jacobi<T, D><<<grid_of(L.num_cells), 256, 0, st>>>(L, b, nullptr, lx0[l], wj);
-            k_mg_residual_restrict<T, D><<<grid_of(levels[l + 1].num_cells), 256, 0, st>>>(L, levels[l + 1], b, lx0[l], lb[l + 1]);
-        }
-        const T* ec = lx0[nl - 1];
-        for (int l = nl - 2; l >= 0; --l) {
-            const pict_mg_level_t& L = levels[l];
-            const T* bl = (l == 0) ? rhs0 : lb[l];
-            T* dst = (l == 0) ? z0 : lx1[l];
-            k_mg_prolong_jacobi<T, D><<<grid_of(L.num_cells), 256, 0, st>>>(L, levels[l + 1], bl, lx0[l], ec, dst, sp, wj);
-            ec = dst;
-        }
-        if (nl == 1) cudaMemcpyAsync(z0, lx0[0], sizeof(T) * N, cudaMemcpyDeviceToDevice, st);
-        return check_launch("pcg_mg vcycle");
-    };
-
-    // search directions alternate between p and pb; each is formed from z inside the SpMV
-    T* pb = lx1[0];
     const int nt = dom->num_tiles;
     const int sg = (dom->num_sims + 127) / 128;
     const int swg = (dom->num_sims * 32 + 127) / 128;  // one warp per system
-    k_pcg_init<T><<<grid_of(N), 256, 0, st>>>(N, rhs, r, xout, p, pb);
-    pict_status_t s = vcycle(r, z, false);
-    if (s) return s;
-    k_pcg_dot4<T><<<nt, 256, 0, st>>>(*dom, r, z, part);
-    k_pcg_scalars<<<swg, 128, 0, st>>>(*dom, part, 4, 0, sc);
-    for (int it = 0; it < iterations; ++it) {
-        k_pcg_spmv_dot<T, D><<<nt, 256, 0, st>>>(*dom, levels[0], z, p, pb, q, sc, part);
-        k_pcg_scalars<<<swg, 128, 0, st>>>(*dom, part, 1, 1, sc);
-        k_pcg_update_xr<T><<<grid_of(N), 256, 0, st>>>(*dom, levels[0], xout, r, pb, q, sc, lx0[0], wj);
-        const bool last = it + 1 == iterations;
-        if (!last) {
-            s = vcycle(r, z, true);
-            if (s) return s;
+
+    // the cycle runs in one CTA per block from level lc on (lc = 0 only for a single-level hierarchy)
+    int lc = nl - 1;
+    for (int l = 1; l < nl; ++l)
+        if (levels[l].max_block_cells <= MG_SUB_MAX && mg_sub_smem(levels + l, nl - l, sizeof(T)) <= MG_SUB_SMEM) {
+            lc = l;
+            break;
         }
-        // on the last iteration only |r|^2 is used (r.z and sum(z) of the stale z are ignored)
-        k_pcg_dot4<T><<<nt, 256, 0, st>>>(*dom, r, z, part);
-        k_pcg_scalars<<<swg, 128, 0, st>>>(*dom, part, 4, 2, sc);
-        T* tmp = p; p = pb; pb = tmp;
+    if (nl == 1) lc = 0;
+    MgSub sub;
+    sub.n = nl - lc;
+    for (int k = 0; k < sub.n; ++k) sub.lv[k] = levels[lc + k];
+    const size_t sub_smem = mg_sub_smem(sub.lv, sub.n, sizeof(T));
+    if (sub_smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k_mg_subcycle<T, D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)sub_smem);
+        if (e != cudaSuccess) return set_error(PICT_ERR_CUDA, "pcg_mg: sub-cycle shared memory");
+    }
+    // shared-memory stages of the 2D restriction / prolongation: x or x0, b, diag
+    const int cap = D == 2 ? MG_STAGE : 0;
+    const size_t stage3 = D == 2 ? 3 * (size_t)MG_STAGE * sizeof(T) : 0;
+    if (D == 2) {
+        cudaError_t e = cudaFuncSetAttribute(k_mg_restrict<T, D, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)stage3);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_mg_restrict<T, D, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)stage3);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_mg_prolong<T, D, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)stage3);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_mg_prolong<T, D, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)stage3);
+        if (e != cudaSuccess) return set_error(PICT_ERR_CUDA, "pcg_mg: stage shared memory");
+    }
+
+    // z = M r_new (V-cycle) and the per-warp partials of r_new.z, |r_new|^2, sum(z), sum(r_new).  upd:
+    // the finest restriction first forms r_new = r - alpha q (stored to rn) and x += alpha p.
+    auto vcycle = [&](const T* r, bool upd, T* rn, const T* p, int first) -> pict_status_t {
+        const T* rnew = upd ? rn : r;
+        if (lc == 0) {
+            if (upd) k_pcg_update<T><<<nt, MG_TPB, 0, st>>>(*dom, r, q, rn, xout, p, sc, first, part);
+            k_mg_subcycle<T, D><<<levels[0].num_blocks, MG_SUB_THREADS, sub_smem, st>>>(sub, rnew, z, wj, sp,
+                                                                                     coarse_sweeps);
+            k_pcg_dot4<T><<<nt, MG_TPB, 0, st>>>(*dom, rnew, z, part);
+            return check_launch("pcg_mg vcycle");
+        }
+        for (int l = 0; l < lc; ++l) {
+            const pict_mg_level_t& F = levels[l];
+            const pict_mg_level_t& C = levels[l + 1];
+            if (l == 0 && upd)
+                k_mg_restrict<T, D, true><<<C.num_tiles, MG_TPB, stage3, st>>>(F, C, r, q, rn, xout, p, sc, first,
+                                                                                lb[1], wj, cap);
+            else
+                k_mg_restrict<T, D, false><<<C.num_tiles, MG_TPB, stage3, st>>>(
+                    F, C, l == 0 ? r : lb[l], nullptr, nullptr, nullptr, nullptr, nullptr, 0, lb[l + 1], wj, cap);
+        }
+        // levels lc.. in one launch (one CTA per block)
+        k_mg_subcycle<T, D><<<levels[lc].num_blocks, MG_SUB_THREADS, sub_smem, st>>>(sub, lb[lc], lx[lc], wj, sp,
+                                                                                  coarse_sweeps);
+        for (int l = lc - 1; l >= 1; --l)
+            k_mg_prolong<T, D, false><<<levels[l].num_tiles, MG_TPB, stage3, st>>>(
+                levels[l], levels[l + 1], levels[l].tiles, lb[l], lx[l + 1], lx[l], sp, wj, nullptr, cap);
+        k_mg_prolong<T, D, true><<<nt, MG_TPB, stage3, st>>>(levels[0], levels[1], dom->tiles, rnew, lx[1], z, sp, wj,
+                                                             part, cap);
+        return check_launch("pcg_mg vcycle");
+    };
+
+    if (iterations == 0) cudaMemsetAsync(xout, 0, sizeof(T) * N, st);
+    pict_status_t s = vcycle(rhs, false, nullptr, nullptr, 0);
+    if (s) return s;
+    k_pcg_scalars<4><<<swg, 128, 0, st>>>(*dom, part, 0, sc);
+    const T* r = rhs;
+    for (int it = 0; it < iterations; ++it) {
+        T* pnew = pbuf[it & 1];
+        const T* pold = it ? pbuf[(it + 1) & 1] : z;
+        T* rn = rbuf[it & 1];
+        k_pcg_spmv_dot<T, D><<<nt, MG_TPB, 0, st>>>(*dom, levels[0], z, pold, pnew, q, sc, it == 0, part);
+        k_pcg_scalars<1><<<swg, 128, 0, st>>>(*dom, part, 1, sc);
+        if (it + 1 < iterations) {
+            s = vcycle(r, true, rn, pnew, it == 0);
+            if (s) return s;
+        } else {
+            // last iteration: only the update and |r|^2 (r.z and sum(z) are not used)
+            k_pcg_update<T><<<nt, MG_TPB, 0, st>>>(*dom, r, q, rn, xout, pnew, sc, it == 0, part);
+        }
+        k_pcg_scalars<4><<<swg, 128, 0, st>>>(*dom, part, 2, sc);
+        r = rn;
     }
     k_pcg_report<<<sg, 128, 0, st>>>(*dom, sc, info, iterations, tol, normalized);
     return check_launch("pcg_mg");
@@ -504,14 +1016,8 @@ pict_status_t pict_mg_galerkin(const pict_mg_level_t* fine, const pict_mg_level_
 
 int64_t pict_pcg_mg_workspace_bytes(const pict_domain_t* dom, const pict_mg_level_t* levels, int32_t num_levels) {
     if (!dom || !levels || num_levels < 1 || num_levels > 16) return -1;
-    const size_t esz = dom->dtype == PICT_F64 ? 8 : 4;
-    auto vb = [&](int n) { return ((size_t)n * esz + 255) & ~(size_t)255; };
-    size_t b = 0;
-    for (int l = 0; l < num_levels; ++l) b += 3 * vb(levels[l].num_cells);
-    b += 4 * vb(dom->num_cells);
-    b += ((size_t)4 * dom->num_tiles * 8 + 255) & ~(size_t)255;
-    b += ((size_t)MG_SC * dom->num_sims * 8 + 255) & ~(size_t)255;
-    return (int64_t)b;
+    MgWork w;
+    return (int64_t)mg_carve(dom, levels, num_levels, dom->dtype == PICT_F64 ? 8 : 4, nullptr, &w);
 }
 
 pict_status_t pict_pcg_mg(const pict_domain_t* dom, const pict_mg_level_t* levels, int32_t num_levels, const void* rhs,

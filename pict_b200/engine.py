@@ -216,8 +216,11 @@ class PISOStepper:
         if self.pressure_refine > 0:  # per sweep: residual (+2 projection), solve, update; partials + finish
             if self._mg is not None:
                 nl, it = self._mg.num_levels, self.mg_iterations
-                v = 3 * (nl - 1) + 1      # V-cycle; the finest pre-smoothing of later ones is fused
-                solve = 1 + v + 2 + it * 5 + max(it - 1, 0) * (v - 1) + 1
+                v = self._mg.launches_per_vcycle()   # with the PCG update / dot partials fused in
+                if nl == 1:  # separate update, sub-cycle, dot
+                    solve = (v - 1) + 1 + it * 3 + max(it - 1, 0) * v + (1 if it > 0 else 0) + 1
+                else:
+                    solve = v + 1 + it * 3 + max(it - 1, 0) * v + (1 if it > 0 else 0) + 1
                 n += nl - 1  # Galerkin coarse operators once per step
             else:
                 solve = 3

@@ -19,6 +19,9 @@ from . import _lib
 from ._lib import MgLevel, check
 
 MAX_LEVELS = 16
+TILE_CELLS = 512           # cells per work tile of the coarse levels
+SUB_MAX_CELLS = 2048       # the V-cycle runs in one CTA per block from the first level whose blocks have at
+SUB_MAX_SMEM = 160 * 1024  # most this many cells and whose sub-cycle fits this much shared memory
 
 
 def eligible(host_blocks, num_blocks, dims, sim_of_block) -> Optional[str]:
@@ -50,6 +53,16 @@ def axis_strengths(domain) -> np.ndarray:
         alpha = det[:, None] * (minv ** 2).sum(dim=2)
         out[k, :D] = alpha.mean(dim=0).cpu().numpy()
     return out
+
+
+def level_tiles(offs, counts, sims, tile: int = TILE_CELLS) -> np.ndarray:
+    """Work tiles of a coarse level, [num_tiles * 4]: system, block, first cell, cell count (each
+    block split into runs of at most `tile` cells)."""
+    out = []
+    for b, (o, n) in enumerate(zip(offs, counts)):
+        for s0 in range(0, int(n), tile):
+            out.append((int(sims[b]), b, int(o) + s0, min(tile, int(n) - s0)))
+    return np.array(out, dtype=np.int32).reshape(-1)
 
 
 class MGHierarchy:
@@ -103,8 +116,14 @@ class MGHierarchy:
             L.blocks = blocks_t.data_ptr()
             L.cell_block = cb.data_ptr()
             L.coef = coef.data_ptr() if coef is not None else None
+            L.max_block_cells = int(n.max())
+            tiles_t = None
+            if lvl > 0:
+                tiles_t = torch.tensor(level_tiles(offs, n, sims), dtype=torch.int32, device=device)
+                L.num_tiles = tiles_t.numel() // 4
+                L.tiles = tiles_t.data_ptr()
             levels.append(L)
-            self.levels_py.append((blocks_t, cb, coef))
+            self.levels_py.append((blocks_t, cb, coef, tiles_t))
             self.shifts.append(shifts.copy())
             if (sizes[:, :dims] <= min_size).all():
                 break
@@ -125,6 +144,22 @@ class MGHierarchy:
         self.num_levels = len(levels)
         self.levels = (MgLevel * self.num_levels)(*levels)
         self.cells = [int(L.num_cells) for L in levels]
+
+    def sub_level(self) -> int:
+        """First level of the part of the V-cycle that runs in one launch (one CTA per block)."""
+        if self.num_levels == 1:
+            return 0
+        esz = 8 if self.dtype == torch.float64 else 4
+        for l in range(1, self.num_levels):
+            cells = [int(self.levels[k].max_block_cells) for k in range(l, self.num_levels)]
+            smem = esz * (cells[0] + (2 + self.K) * sum(cells))
+            if cells[0] <= SUB_MAX_CELLS and smem <= SUB_MAX_SMEM:
+                return l
+        return self.num_levels - 1
+
+    def launches_per_vcycle(self) -> int:
+        lc = self.sub_level()
+        return 2 * lc + 1 if lc > 0 else 3
 
     def setup(self, fine_coef: torch.Tensor, stream):
         """Point level 0 at the finest stencil and recompute every coarse stencil."""
