@@ -47,6 +47,8 @@ constexpr int KR_SLOTS = 32;     // tiles per CTA (lane j of warp 0 holds the sc
 constexpr int KR_THREADS = 512;  // threads per CTA
 constexpr int KR_CPT = 4;        // cells per thread per tile: tile_cells <= KR_CPT * KR_THREADS
 constexpr int KR_MAX_TILE = KR_CPT * KR_THREADS;
+constexpr int KR_U = 2;          // cells per thread and pass of the phase sweeps (loads of both in flight)
+constexpr int KR_PASS = KR_U * KR_THREADS;
 
 // ctrl words in the workspace header (cleared before every launch)
 // CTRL_BAR_COUNT counts barrier arrivals (monotonic).  CTRL_DONE counts finished systems (classic CG /
@@ -234,7 +236,10 @@ __device__ __forceinline__ void flush_partials(PhaseRed& R, const TileSlots& S, 
 }
 
 // One stencil row applied to a vector given by `load(j)`; TRANS applies the transposed matrix
-// (the coefficient of row j pointing back to i).
+// (the coefficient of row j pointing back to i).  Branch-free gathers: inside a block the neighbour is
+// i +- stride, on a block face it comes from the neighbour table; where there is none (-1) the cell
+// itself is loaded and the term is masked, so all loads of a row (and of the rows a thread handles in
+// one pass) are unconditional and can be in flight together.
 template <typename T, int D, bool TRANS, typename F>
 __device__ __forceinline__ T spmv_row(const pict_domain_t& dom, const T* __restrict__ coef, int N, int i,
                                       const pict_block_t& B, const int* p, F load) {
@@ -245,17 +250,17 @@ __device__ __forceinline__ T spmv_row(const pict_domain_t& dom, const T* __restr
         const int a = f >> 1;
         const bool up = f & 1;
         const bool at = up ? (p[a] == B.size[a] - 1) : (p[a] == 0);
-        int j, back = f ^ 1;
-        if (!at) {
-            j = i + (up ? stride[a] : -stride[a]);
-        } else {
+        int j = i + (up ? stride[a] : -stride[a]);
+        int back = f ^ 1;
+        if (at) {
             j = dom.nbr[(size_t)f * N + i];
-            if (j >= 0 && B.face[f].type == PICT_FACE_CONNECTED) back = B.face[f].conn_axes[0];
+            if (B.face[f].type == PICT_FACE_CONNECTED) back = B.face[f].conn_axes[0];
         }
-        if (j >= 0) {
-            const T c = TRANS ? coef[(size_t)(back + 1) * N + j] : coef[(size_t)(f + 1) * N + i];
-            acc += c * load(j);
-        }
+        const bool ok = j >= 0;
+        const int jj = ok ? j : i;
+        const T c = TRANS ? coef[(size_t)(back + 1) * N + jj] : coef[(size_t)(f + 1) * N + i];
+        const T v = load(jj);
+        acc += ok ? c * v : T(0);
     }
     return acc;
 }
@@ -357,25 +362,26 @@ __global__ void __launch_bounds__(KR_THREADS, 2) k_cg(KArgs<T> a) {
             const pict_block_t& B = dom.blocks[S.block[j]];
             const T bt = (T)s_beta[j];
             double acc[1] = {0.0};
-            const int s0 = S.start[j], s1 = s0 + S.count[j];
-            T pi[KR_CPT], qi[KR_CPT];
+            const int s0 = S.start[j], cnt = S.count[j];
+            for (int base = 0; base < cnt; base += KR_PASS) {
+                T pi[KR_U], qi[KR_U];
 #pragma unroll
-            for (int k = 0; k < KR_CPT; ++k) {
-                const int i = s0 + threadIdx.x + k * blockDim.x;
-                if (i < s1) {
+                for (int k = 0; k < KR_U; ++k) {
+                    const int l = min(base + (int)threadIdx.x + k * KR_THREADS, cnt - 1);
+                    const int i = s0 + l;
                     int p[3];
                     unflatten(i - B.offset, B.size, p);
                     pi[k] = r[i] + bt * pc[i];
                     qi[k] = spmv_row<T, D, TRANS>(dom, coef, N, i, B, p, [&](int jj) { return r[jj] + bt * pc[jj]; });
                 }
-            }
 #pragma unroll
-            for (int k = 0; k < KR_CPT; ++k) {
-                const int i = s0 + threadIdx.x + k * blockDim.x;
-                if (i < s1) {
-                    pn[i] = pi[k];
-                    q[i] = qi[k];
-                    acc[0] += (double)pi[k] * (double)qi[k];
+                for (int k = 0; k < KR_U; ++k) {
+                    const int l = base + (int)threadIdx.x + k * KR_THREADS;
+                    if (l < cnt) {
+                        pn[s0 + l] = pi[k];
+                        q[s0 + l] = qi[k];
+                        acc[0] += (double)pi[k] * (double)qi[k];
+                    }
                 }
             }
             warp_partial<1>(R, j, acc);
@@ -393,15 +399,23 @@ __global__ void __launch_bounds__(KR_THREADS, 2) k_cg(KArgs<T> a) {
             if (!((s_active >> j) & 1u)) continue;
             const T al = (T)s_alpha[j];
             double acc[1] = {0.0};
-            const int s0 = S.start[j], s1 = s0 + S.count[j];
+            const int s0 = S.start[j], cnt = S.count[j];
+            for (int base = 0; base < cnt; base += KR_PASS) {
+                T xi[KR_U], ri[KR_U];
 #pragma unroll
-            for (int k = 0; k < KR_CPT; ++k) {
-                const int i = s0 + threadIdx.x + k * blockDim.x;
-                if (i < s1) {
-                    x[i] += al * pn[i];
-                    const T ri = r[i] - al * q[i];
-                    r[i] = ri;
-                    acc[0] += (double)ri * (double)ri;
+                for (int k = 0; k < KR_U; ++k) {
+                    const int i = s0 + min(base + (int)threadIdx.x + k * KR_THREADS, cnt - 1);
+                    xi[k] = x[i] + al * pn[i];
+                    ri[k] = r[i] - al * q[i];
+                }
+#pragma unroll
+                for (int k = 0; k < KR_U; ++k) {
+                    const int l = base + (int)threadIdx.x + k * KR_THREADS;
+                    if (l < cnt) {
+                        x[s0 + l] = xi[k];
+                        r[s0 + l] = ri[k];
+                        acc[0] += (double)ri[k] * (double)ri[k];
+                    }
                 }
             }
             warp_partial<1>(R, j, acc);
@@ -569,32 +583,34 @@ __global__ void __launch_bounds__(KR_THREADS, 2) k_cg1(KArgs<T> a) {
             const pict_block_t& B = dom.blocks[S.block[j]];
             const T al = (T)s_alpha[j], bt = (T)s_beta[j];
             double acc[2] = {0.0, 0.0};
-            const int s0 = S.start[j], s1 = s0 + S.count[j];
-            T rni[KR_CPT], wni[KR_CPT], pi[KR_CPT], si[KR_CPT];
+            const int s0 = S.start[j], cnt = S.count[j];
+            for (int base = 0; base < cnt; base += KR_PASS) {
+                T rni[KR_U], wni[KR_U], pi[KR_U], si[KR_U], xi[KR_U];
 #pragma unroll
-            for (int k = 0; k < KR_CPT; ++k) {
-                const int i = s0 + threadIdx.x + k * blockDim.x;
-                if (i < s1) {
+                for (int k = 0; k < KR_U; ++k) {
+                    const int i = s0 + min(base + (int)threadIdx.x + k * KR_THREADS, cnt - 1);
                     int q[3];
                     unflatten(i - B.offset, B.size, q);
                     pi[k] = rc[i] + bt * p[i];
                     si[k] = wc[i] + bt * sc[i];
                     rni[k] = rc[i] - al * si[k];
+                    xi[k] = x[i] + al * pi[k];
                     wni[k] = spmv_row<T, D, TRANS>(dom, coef, N, i, B, q,
                                                    [&](int jj) { return rc[jj] - al * (wc[jj] + bt * sc[jj]); });
                 }
-            }
 #pragma unroll
-            for (int k = 0; k < KR_CPT; ++k) {
-                const int i = s0 + threadIdx.x + k * blockDim.x;
-                if (i < s1) {
-                    x[i] += al * pi[k];
-                    p[i] = pi[k];
-                    sn[i] = si[k];
-                    rn[i] = rni[k];
-                    wn[i] = wni[k];
-                    acc[0] += (double)rni[k] * (double)rni[k];
-                    acc[1] += (double)wni[k] * (double)rni[k];
+                for (int k = 0; k < KR_U; ++k) {
+                    const int l = base + (int)threadIdx.x + k * KR_THREADS;
+                    if (l < cnt) {
+                        const int i = s0 + l;
+                        x[i] = xi[k];
+                        p[i] = pi[k];
+                        sn[i] = si[k];
+                        rn[i] = rni[k];
+                        wn[i] = wni[k];
+                        acc[0] += (double)rni[k] * (double)rni[k];
+                        acc[1] += (double)wni[k] * (double)rni[k];
+                    }
                 }
             }
             warp_partial<2>(R, j, acc);
@@ -787,22 +803,40 @@ __global__ void __launch_bounds__(KR_THREADS, 2) k_bicgstab(KArgs<T> a) {
             double acc[NR];
 #pragma unroll
             for (int c = 0; c < NR; ++c) acc[c] = 0.0;
-            for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) {
-                int p[3];
-                unflatten(i - B.offset, B.size, p);
+            const int s0 = S.start[j], cnt = S.count[j];
+            for (int base = 0; base < cnt; base += KR_PASS) {
+                T pv[KR_U][NR], vv[KR_U][NR], wv[KR_U][NR];
 #pragma unroll
-                for (int c = 0; c < NR; ++c) {
-                    if (!((act >> c) & 1u)) continue;
-                    const T bt = (T)s_beta[j][c], om = (T)s_omega[j][c];
-                    const T* rc = r + c * NS;
-                    const T* pcc = pc + c * NS;
-                    const T* vcc = vc + c * NS;
-                    const T pi = rc[i] + bt * (pcc[i] - om * vcc[i]);
-                    const T vi = spmv_row<T, D, TRANS>(dom, coef, N, i, B, p,
-                                                       [&](int jj) { return rc[jj] + bt * (pcc[jj] - om * vcc[jj]); });
-                    pn[c * NS + i] = pi;
-                    vn[c * NS + i] = vi;
-                    acc[c] += (double)rw[c * NS + i] * (double)vi;
+                for (int k = 0; k < KR_U; ++k) {
+                    const int i = s0 + min(base + (int)threadIdx.x + k * KR_THREADS, cnt - 1);
+                    int p[3];
+                    unflatten(i - B.offset, B.size, p);
+#pragma unroll
+                    for (int c = 0; c < NR; ++c) {
+                        pv[k][c] = vv[k][c] = wv[k][c] = T(0);
+                        if (!((act >> c) & 1u)) continue;
+                        const T bt = (T)s_beta[j][c], om = (T)s_omega[j][c];
+                        const T* rc = r + c * NS;
+                        const T* pcc = pc + c * NS;
+                        const T* vcc = vc + c * NS;
+                        pv[k][c] = rc[i] + bt * (pcc[i] - om * vcc[i]);
+                        vv[k][c] = spmv_row<T, D, TRANS>(dom, coef, N, i, B, p,
+                                                         [&](int jj) { return rc[jj] + bt * (pcc[jj] - om * vcc[jj]); });
+                        wv[k][c] = rw[c * NS + i];
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < KR_U; ++k) {
+                    const int l = base + (int)threadIdx.x + k * KR_THREADS;
+                    if (l >= cnt) continue;
+                    const int i = s0 + l;
+#pragma unroll
+                    for (int c = 0; c < NR; ++c) {
+                        if (!((act >> c) & 1u)) continue;
+                        pn[c * NS + i] = pv[k][c];
+                        vn[c * NS + i] = vv[k][c];
+                        acc[c] += (double)wv[k][c] * (double)vv[k][c];
+                    }
                 }
             }
             warp_partial<NR>(R, j, acc);
@@ -825,15 +859,33 @@ __global__ void __launch_bounds__(KR_THREADS, 2) k_bicgstab(KArgs<T> a) {
             double acc[NR];
 #pragma unroll
             for (int c = 0; c < NR; ++c) acc[c] = 0.0;
-            for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) {
+            const int s0 = S.start[j], cnt = S.count[j];
+            for (int base = 0; base < cnt; base += KR_PASS) {
+                T sv[KR_U][NR], xv[KR_U][NR];
 #pragma unroll
-                for (int c = 0; c < NR; ++c) {
-                    if (!((act >> c) & 1u)) continue;
-                    const T al = (T)s_alpha[j][c];
-                    const T si = r[c * NS + i] - al * vn[c * NS + i];
-                    r[c * NS + i] = si;
-                    x[c * NS + i] += al * pn[c * NS + i];
-                    acc[c] += (double)si * (double)si;
+                for (int k = 0; k < KR_U; ++k) {
+                    const int i = s0 + min(base + (int)threadIdx.x + k * KR_THREADS, cnt - 1);
+#pragma unroll
+                    for (int c = 0; c < NR; ++c) {
+                        sv[k][c] = xv[k][c] = T(0);
+                        if (!((act >> c) & 1u)) continue;
+                        const T al = (T)s_alpha[j][c];
+                        sv[k][c] = r[c * NS + i] - al * vn[c * NS + i];
+                        xv[k][c] = x[c * NS + i] + al * pn[c * NS + i];
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < KR_U; ++k) {
+                    const int l = base + (int)threadIdx.x + k * KR_THREADS;
+                    if (l >= cnt) continue;
+                    const int i = s0 + l;
+#pragma unroll
+                    for (int c = 0; c < NR; ++c) {
+                        if (!((act >> c) & 1u)) continue;
+                        r[c * NS + i] = sv[k][c];
+                        x[c * NS + i] = xv[k][c];
+                        acc[c] += (double)sv[k][c] * (double)sv[k][c];
+                    }
                 }
             }
             warp_partial<NR>(R, j, acc);
@@ -874,17 +926,35 @@ __global__ void __launch_bounds__(KR_THREADS, 2) k_bicgstab(KArgs<T> a) {
             double acc[2 * NR];
 #pragma unroll
             for (int k = 0; k < 2 * NR; ++k) acc[k] = 0.0;
-            for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) {
-                int p[3];
-                unflatten(i - B.offset, B.size, p);
+            const int s0 = S.start[j], cnt = S.count[j];
+            for (int base = 0; base < cnt; base += KR_PASS) {
+                T tv2[KR_U][NR], sv[KR_U][NR];
 #pragma unroll
-                for (int c = 0; c < NR; ++c) {
-                    if (!((act >> c) & 1u)) continue;
-                    const T* sc = r + c * NS;
-                    const T ti = spmv_row<T, D, TRANS>(dom, coef, N, i, B, p, [&](int jj) { return sc[jj]; });
-                    tv[c * NS + i] = ti;
-                    acc[2 * c] += (double)ti * (double)sc[i];
-                    acc[2 * c + 1] += (double)ti * (double)ti;
+                for (int k = 0; k < KR_U; ++k) {
+                    const int i = s0 + min(base + (int)threadIdx.x + k * KR_THREADS, cnt - 1);
+                    int p[3];
+                    unflatten(i - B.offset, B.size, p);
+#pragma unroll
+                    for (int c = 0; c < NR; ++c) {
+                        tv2[k][c] = sv[k][c] = T(0);
+                        if (!((act >> c) & 1u)) continue;
+                        const T* scc = r + c * NS;
+                        tv2[k][c] = spmv_row<T, D, TRANS>(dom, coef, N, i, B, p, [&](int jj) { return scc[jj]; });
+                        sv[k][c] = scc[i];
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < KR_U; ++k) {
+                    const int l = base + (int)threadIdx.x + k * KR_THREADS;
+                    if (l >= cnt) continue;
+                    const int i = s0 + l;
+#pragma unroll
+                    for (int c = 0; c < NR; ++c) {
+                        if (!((act >> c) & 1u)) continue;
+                        tv[c * NS + i] = tv2[k][c];
+                        acc[2 * c] += (double)tv2[k][c] * (double)sv[k][c];
+                        acc[2 * c + 1] += (double)tv2[k][c] * (double)tv2[k][c];
+                    }
                 }
             }
             warp_partial<2 * NR>(R, j, acc);
@@ -906,17 +976,36 @@ __global__ void __launch_bounds__(KR_THREADS, 2) k_bicgstab(KArgs<T> a) {
             double acc[2 * NR];
 #pragma unroll
             for (int k = 0; k < 2 * NR; ++k) acc[k] = 0.0;
-            for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) {
+            const int s0 = S.start[j], cnt = S.count[j];
+            for (int base = 0; base < cnt; base += KR_PASS) {
+                T xv[KR_U][NR], rv[KR_U][NR], wv[KR_U][NR];
 #pragma unroll
-                for (int c = 0; c < NR; ++c) {
-                    if (!((act >> c) & 1u)) continue;
-                    const T om = (T)s_omega[j][c];
-                    const T si = r[c * NS + i];
-                    x[c * NS + i] += om * si;
-                    const T ri = si - om * tv[c * NS + i];
-                    r[c * NS + i] = ri;
-                    acc[2 * c] += (double)ri * (double)ri;
-                    acc[2 * c + 1] += (double)rw[c * NS + i] * (double)ri;
+                for (int k = 0; k < KR_U; ++k) {
+                    const int i = s0 + min(base + (int)threadIdx.x + k * KR_THREADS, cnt - 1);
+#pragma unroll
+                    for (int c = 0; c < NR; ++c) {
+                        xv[k][c] = rv[k][c] = wv[k][c] = T(0);
+                        if (!((act >> c) & 1u)) continue;
+                        const T om = (T)s_omega[j][c];
+                        const T si = r[c * NS + i];
+                        xv[k][c] = x[c * NS + i] + om * si;
+                        rv[k][c] = si - om * tv[c * NS + i];
+                        wv[k][c] = rw[c * NS + i];
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < KR_U; ++k) {
+                    const int l = base + (int)threadIdx.x + k * KR_THREADS;
+                    if (l >= cnt) continue;
+                    const int i = s0 + l;
+#pragma unroll
+                    for (int c = 0; c < NR; ++c) {
+                        if (!((act >> c) & 1u)) continue;
+                        x[c * NS + i] = xv[k][c];
+                        r[c * NS + i] = rv[k][c];
+                        acc[2 * c] += (double)rv[k][c] * (double)rv[k][c];
+                        acc[2 * c + 1] += (double)wv[k][c] * (double)rv[k][c];
+                    }
                 }
             }
             warp_partial<2 * NR>(R, j, acc);
