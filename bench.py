@@ -267,7 +267,9 @@ def job_totals(cells, ms, world, device):
 
 # DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) over algorithmic bytes of one captured
 # launch of the batched workload (profiles/k_cg1_batched_cavities_256.md)
-NCU_TRAFFIC_RATIO = {"k_cg1": 14.27e9 / 20.12e9}
+# ncu DRAM bytes / algorithmic bytes on captured launches (profiles/), per solver group: the persistent
+# CG on the channel, the finest-level multigrid PCG kernels and k_bicgstab on the cavity batch
+NCU_TRAFFIC_RATIO = {"cg": 14.27e9 / 20.12e9, "mg": 399.6e6 / 477.0e6, "bicg": 4.155e9 / 6.69e9}
 
 
 def cg_algorithmic_bytes(dims, esz):
@@ -572,7 +574,7 @@ def roofline_pass(st, batch, args, dev):
                       "bytes_per_cell_iteration": solver_bytes_per_cell(kind, D, esz, nrhs=D)})
     table.sort(key=lambda r: -r["ms_per_step"])
     top = dict(table[0])
-    ratio = NCU_TRAFFIC_RATIO.get(top["kernel"])
+    ratio = NCU_TRAFFIC_RATIO.get(top["group"])
     top.update({"bound": "hbm", "peak": peak, "peak_kind": kind_peak, "unit": "GB/s",
                 "traffic": None if ratio is None else ratio * top["algorithmic_bytes_per_launch"],
                 "traffic_note": None if ratio is None else
