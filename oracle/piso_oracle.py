@@ -2,7 +2,7 @@
 
 This module is the checker for the CUDA implementation in ``pict_b200``: a
 NumPy / SciPy-sparse restatement of the reference discretisation for the
-orthogonal PISO path (``non_orthogonal=False``), on single- and multi-block
+PISO path (orthogonal, and with the non-orthogonal terms of ``nonOrthoFlags``), on single- and multi-block
 structured grids with fixed (Dirichlet), periodic and connected boundaries and
 optional per-cell coordinate transforms.  It is imported only by ``tests/``,
 ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py``; the
@@ -397,6 +397,7 @@ class ODomain:
                 self.ncomp[f, sl] = ncomp
                 self.flip[f, sl] = flip
         self._gather_static()
+        self.p_result = np.zeros(N)  # Domain::CreatePressureResult, extensions/domain_structs.cpp:2823-2826
 
     def _gather_static(self):
         D = self.dims
@@ -552,8 +553,9 @@ def face_fluxes(dom: ODomain, u: np.ndarray, bflux: np.ndarray) -> np.ndarray:
     return fl
 
 
-def advection_matrix(dom: ODomain, dt: float):
-    """PISO_build_matrix, extensions/PISO_multiblock_cuda_kernel.cu:3601-3865 (orthogonal terms only, nonOrthoFlags=0).
+def advection_matrix(dom: ODomain, dt: float, non_ortho_flags: int = 0):
+    """PISO_build_matrix, extensions/PISO_multiblock_cuda_kernel.cu:3601-3865 (orthogonal terms, plus the
+    non-orthogonal terms of ``nonortho_matrix_terms`` when non_ortho_flags selects them).
 
     Returns (coef[K,N], A[N]) with coefficients divided by det as the reference does.
     """
@@ -584,12 +586,16 @@ def advection_matrix(dom: ODomain, dt: float):
         diag = diag + np.where(ok, ff + vc, 2.0 * nu * alpha_p[d])  # slip=0 for Dirichlet walls
         coef[f + 1] = np.where(ok, ff - vc, 0.0)
     coef[0] = diag
+    if non_ortho_flags:
+        coef = coef + nonortho_matrix_terms(dom, non_ortho_flags, "adv", nu=nu)
     coef = coef / det[None]
     return coef, coef[0].copy()
 
 
-def advection_rhs(dom: ODomain, dt: float):
-    """kPISO_build_advection_RHS, extensions/PISO_multiblock_cuda_kernel.cu:4281-4385 (FIXED boundaries, no pressure gradient)."""
+def advection_rhs(dom: ODomain, dt: float, non_ortho_flags: int = 0, u_result: Optional[np.ndarray] = None):
+    """kPISO_build_advection_RHS, extensions/PISO_multiblock_cuda_kernel.cu:4281-4385 (FIXED boundaries, no pressure
+    gradient); with non_ortho_flags the explicit non-orthogonal viscous terms of the velocity result
+    `u_result` [D,N] are subtracted before the division by det (kernel.cu:4368)."""
     D = dom.dims
     u = dom.velocity_global()
     bvel, bflux, balpha = dom.boundary_cell_data()
@@ -605,12 +611,17 @@ def advection_rhs(dom: ODomain, dt: float):
             vel = bvel[f, c]
             add = -vel * flux + vel * nu * 2.0 * balpha[f]
             rhs[c] = rhs[c] + np.where(fixed, add, 0.0)
+    if non_ortho_flags:
+        fields = {"vel": u if u_result is None else u_result}
+        for c in range(D):
+            rhs[c] = rhs[c] - nonortho_rhs(dom, non_ortho_flags, "vel", fields, c, True, False, nu=nu)
     rhs = rhs / det[None] + src
     return rhs
 
 
-def pressure_matrix(dom: ODomain, A: np.ndarray):
-    """PISO_build_pressure_matrix, extensions/PISO_multiblock_cuda_kernel.cu:4797-4963 (no face transforms, no non-ortho terms)."""
+def pressure_matrix(dom: ODomain, A: np.ndarray, non_ortho_flags: int = 0):
+    """PISO_build_pressure_matrix, extensions/PISO_multiblock_cuda_kernel.cu:4797-4963 (no face transforms; the
+    non-orthogonal terms of ``nonortho_matrix_terms`` when non_ortho_flags selects them)."""
     D = dom.dims
     N = dom.N
     K = 2 * D + 1
@@ -629,6 +640,8 @@ def pressure_matrix(dom: ODomain, A: np.ndarray):
         c = np.where(ok, 0.5 * (alphaP * raP + alphaN * raN), 0.0)
         coef[0] -= c
         coef[f + 1] = c
+    if non_ortho_flags:
+        coef = coef + nonortho_matrix_terms(dom, non_ortho_flags, "p", A=A)
     return coef
 
 
@@ -670,6 +683,13 @@ def divergence(dom: ODomain, h: np.ndarray):
     return div
 
 
+def pressure_rhs_nonortho(dom: ODomain, non_ortho_flags: int, div: np.ndarray, A: np.ndarray,
+                          p_result: np.ndarray) -> np.ndarray:
+    """k_pressureRHSaddNonOrthoComponents, extensions/PISO_multiblock_cuda_kernel.cu:5423-5453: div plus the explicit
+    non-orthogonal terms of the pressure result (with 1/A, no viscosity)."""
+    return div + nonortho_rhs(dom, non_ortho_flags, "p", {"p": p_result}, 0, False, True, A=A)
+
+
 def pressure_gradient_fd(dom: ODomain, p: np.ndarray):
     """getPressureGradient, extensions/PISO_multiblock_cuda_kernel.cu:801-834 with getPressureAtWithBounds extensions/PISO_multiblock_cuda_kernel.cu:2160-2239."""
     D = dom.dims
@@ -692,6 +712,384 @@ def correct_velocity(dom: ODomain, p_blocks: np.ndarray, A: np.ndarray, h: np.nd
     """PISO_update_velocity (version 1, FD), extensions/PISO_multiblock_cuda_kernel.cu:5947-5980."""
     g = pressure_gradient_fd(dom, p_blocks)
     return h - g / A[None]
+
+
+# --------------------------------------------------------------------------
+# non-orthogonal terms (nonOrthoFlags != 0): tangential Laplacian fluxes on skewed grids
+# --------------------------------------------------------------------------
+
+# bit flags, extensions/PISO_multiblock_cuda.h:9-13; the driver's default set, sim.py:390-396
+NON_ORTHO_DIRECT_MATRIX = 1
+NON_ORTHO_DIRECT_RHS = 2
+NON_ORTHO_DIAGONAL_MATRIX = 4
+NON_ORTHO_DIAGONAL_RHS = 8
+NON_ORTHO_CENTER_MATRIX = 16
+NON_ORTHO_DEFAULT = NON_ORTHO_CENTER_MATRIX | NON_ORTHO_DIRECT_MATRIX | NON_ORTHO_DIAGONAL_RHS
+
+
+def _gidx(dom: ODomain, bi: int, p) -> int:
+    b = dom.blocks[bi]
+    sx = b.size[0]
+    sy = b.size[1] if dom.dims > 1 else 1
+    return dom.offsets[bi] + p[0] + sx * (p[1] + sy * p[2])
+
+
+def _at_bound(dom: ODomain, bi: int, p, face: int) -> bool:
+    """isAtBound, kernel.cu:228-240."""
+    a = face >> 1
+    return p[a] == (dom.blocks[bi].size[a] - 1 if face & 1 else 0)
+
+
+def _is_empty(dom: ODomain, bi: int, face: int) -> bool:
+    """isEmptyBound, kernel.cu:188-194: a prescribed (fixed) face, by type only."""
+    return dom.blocks[bi].boundaries[face].kind == "fixed"
+
+
+def _conn_pos(dom: ODomain, bi: int, face: int, p, offset: int):
+    """computeConnectedPos, kernel.cu:326-345: the cell `offset` layers into the block across the
+    connection of face `face` (offset 0 is the first layer)."""
+    D = dom.dims
+    bnd = dom.blocks[bi].boundaries[face]
+    ob = dom.blocks[bnd.block]
+    a = face >> 1
+    q = list(p)
+    ca = bnd.axes[0] >> 1
+    q[ca] = ob.size[ca] - 1 - offset if bnd.axes[0] & 1 else offset
+    for k in range(1, D):
+        ax = (a + k) % D
+        ca = bnd.axes[k] >> 1
+        q[ca] = ob.size[ca] - 1 - p[ax] if bnd.axes[k] & 1 else p[ax]
+    return bnd.block, q
+
+
+def _conn_dir(dom: ODomain, bi: int, face: int, d: int) -> int:
+    """computeConnectedDir, kernel.cu:314-323 (getAxisRelativeToOther kernel.cu:243-245)."""
+    bnd = dom.blocks[bi].boundaries[face]
+    rel = ((d >> 1) - (face >> 1)) % dom.dims
+    return bnd.axes[rel] ^ (d & 1)
+
+
+def _lap_full(dom: ODomain, g: int) -> np.ndarray:
+    """getLaplaceCoefficientsFull, kernel.cu:1270-1295: alpha[c1][c2] = det Minv[c1].Minv[c2]."""
+    M = dom.Minv[g]
+    return dom.det[g] * (M @ M.T)
+
+
+def _bound_flat(dom: ODomain, bi: int, face: int, p) -> int:
+    a = face >> 1
+    s = list(dom.blocks[bi].size) + [1] * (3 - dom.dims)
+    s[a] = 1
+    q = list(p)
+    q[a] = 0
+    return q[0] + s[0] * (q[1] + s[1] * q[2])
+
+
+def _bound_lap_axis(dom: ODomain, bi: int, face: int, p, axis: int) -> np.ndarray:
+    """getLaplaceCoefficientsNeighbourBoundary, kernel.cu:1469-1491 (fixed boundary transform)."""
+    D = dom.dims
+    bnd = dom.blocks[bi].boundaries[face]
+    if bnd.transform is None:
+        e = np.zeros(D)
+        e[axis] = 1.0
+        return e
+    T = bnd.transform.reshape(-1, 2 * D * D + 1)[_bound_flat(dom, bi, face, p)]
+    Minv = T[D * D:2 * D * D].reshape(D, D)
+    return T[-1] * (Minv @ Minv[axis])
+
+
+def _fixed_data(dom: ODomain, bi: int, face: int, p, comp: int, kind: str) -> float:
+    """getFixedBoundaryData, kernel.cu:2379-2447, fixed boundaries: the velocity component; the fixed
+    boundary pressure is a static zero (domain_structs.cpp:565-576); IS_FIXED_BOUNDARY reads 1."""
+    if kind == "flag":
+        return 1.0
+    if kind == "p":
+        return 0.0
+    vel = np.asarray(dom.blocks[bi].boundaries[face].velocity, dtype=np.float64)
+    if vel.ndim == 2:
+        return float(vel[0, comp])
+    return float(vel.reshape(dom.dims, -1)[comp, _bound_flat(dom, bi, face, p)])
+
+
+def _fixed_type(kind: str) -> str:
+    """getFixedBoundaryType, kernel.cu:2353-2377: velocity Dirichlet, pressure Neumann."""
+    return "neumann" if kind == "p" else "dirichlet"
+
+
+def _block_data(dom: ODomain, bi: int, p, comp: int, kind: str, fields) -> float:
+    """getBlockData, kernel.cu:2322-2330, on the global result vectors (kind 'vel' / 'p'); other kinds read 0."""
+    if fields is None:
+        return 0.0
+    g = _gidx(dom, bi, p)
+    if kind == "vel":
+        return float(fields["vel"][comp, g])
+    if kind == "p":
+        return float(fields["p"][g])
+    return 0.0
+
+
+def corner_value(dom: ODomain, bi: int, p, comp: int, dir1: int, dir2: int, incl0: bool, incl1: bool,
+                 max_depth: int, kind: str, fields=None):
+    """getCornerValue, kernel.cu:2742-2860: walk around the corner of cell `p` between faces dir1 and
+    dir2 in both directions (depth 1: the face neighbours, depth 2: the diagonal cell) until the walks
+    meet, a fixed boundary is hit or max_depth is reached.  Returns (value, cells, boundary type);
+    cells == 0 means the value came from a fixed boundary.  Across a block connection the walk lands
+    on the second cell layer of the connected block (computeConnectedPos with borderOffset 1,
+    kernel.cu:2810), as the reference does."""
+    data = 0.0
+    n = 0
+    btype = "dirichlet"
+    if incl0:
+        data += _block_data(dom, bi, p, comp, kind, fields)
+    n += 1
+    walk = [[dir1, dir2, bi, list(p)], [dir2, dir1, bi, list(p)]]
+    for depth in range(1, max_depth + 1):
+        for d in range(2):
+            w = walk[d]
+            d1, d2, wb, wp = w
+            a = d1 >> 1
+            if _at_bound(dom, wb, wp, d1):
+                bnd = dom.blocks[wb].boundaries[d1]
+                if bnd.kind == "fixed":
+                    btype = _fixed_type(kind)
+                    if _at_bound(dom, wb, wp, d2):
+                        return _fixed_data(dom, wb, d1, wp, comp, kind), 0, btype
+                    q = list(wp)
+                    q[d2 >> 1] += 1 if d2 & 1 else -1
+                    return (_fixed_data(dom, wb, d1, wp, comp, kind) + _fixed_data(dom, wb, d1, q, comp, kind)) * 0.5, 0, btype
+                if bnd.kind == "connected":
+                    nb_, q = _conn_pos(dom, wb, d1, wp, 1)
+                    w[0] = _conn_dir(dom, wb, d1, d2)
+                    w[1] = _conn_dir(dom, wb, d1, d1) ^ 1
+                    w[2], w[3] = nb_, q
+                else:  # periodic
+                    q = list(wp)
+                    q[a] = 0 if d1 & 1 else dom.blocks[wb].size[a] - 1
+                    w[0], w[1], w[3] = d2, d1 ^ 1, q
+            else:
+                q = list(wp)
+                q[a] += 1 if d1 & 1 else -1
+                w[0], w[1], w[3] = d2, d1 ^ 1, q
+            o = walk[d ^ 1]
+            if w[2] == o[2] and w[3] == o[3]:
+                return data / n, n, btype
+            if depth > 1 or incl1:
+                data += _block_data(dom, w[2], w[3], comp, kind, fields)
+            n += 1
+    return data / n, n, btype
+
+
+def _neighbor_info(dom: ODomain, bi: int, p, face: int):
+    """resolveNeighborCell, kernel.cu:432-477, for a face that is not prescribed: the neighbour's block,
+    position and the axis mapping (faces of the neighbour's block for +x, +y, +z of this block)."""
+    D = dom.dims
+    a = face >> 1
+    mapping = [0, 2, 4]
+    if _at_bound(dom, bi, p, face):
+        bnd = dom.blocks[bi].boundaries[face]
+        if bnd.kind == "connected":
+            nb_, q = _conn_pos(dom, bi, face, p, 0)
+            mapping = [_conn_dir(dom, bi, face, mapping[k]) if k < D else mapping[k] for k in range(3)]
+            return nb_, q, mapping
+        q = list(p)
+        q[a] = 0 if face & 1 else dom.blocks[bi].size[a] - 1
+        return bi, q, mapping
+    q = list(p)
+    q[a] += 1 if face & 1 else -1
+    return bi, q, mapping
+
+
+def _neighbor_data(dom: ODomain, bi: int, p, face: int, comp: int, kind: str, fields) -> float:
+    """getBlockDataNeighbor, kernel.cu:2519-2560 (zeroBound false; second layer across connections)."""
+    a = face >> 1
+    if _at_bound(dom, bi, p, face):
+        bnd = dom.blocks[bi].boundaries[face]
+        if bnd.kind == "fixed":
+            return _fixed_data(dom, bi, face, p, comp, kind)
+        if bnd.kind == "connected":
+            nb_, q = _conn_pos(dom, bi, face, p, 1)
+            return _block_data(dom, nb_, q, comp, kind, fields)
+        q = list(p)
+        q[a] = 0 if face & 1 else dom.blocks[bi].size[a] - 1
+        return _block_data(dom, bi, q, comp, kind, fields)
+    q = list(p)
+    q[a] += 1 if face & 1 else -1
+    return _block_data(dom, bi, q, comp, kind, fields)
+
+
+def _diagonal_data(dom: ODomain, bi: int, p, dir1: int, dir2: int, comp: int, kind: str, fields) -> float:
+    """getBlockDataNeighborDiagonal, kernel.cu:2615-2660: two steps (dir2 first if dir1's face is a
+    prescribed type); a fixed face on the way returns its data; no direction remapping across a
+    connection; second layer across connections."""
+    first_empty = _is_empty(dom, bi, dir1)
+    dirs = [dir2, dir1] if first_empty else [dir1, dir2]
+    cb, q = bi, list(p)
+    for bound in dirs:
+        a = bound >> 1
+        if _at_bound(dom, cb, q, bound):
+            bnd = dom.blocks[cb].boundaries[bound]
+            if bnd.kind == "fixed":
+                return _fixed_data(dom, cb, bound, q, comp, kind)
+            if bnd.kind == "connected":
+                cb, q = _conn_pos(dom, cb, bound, q, 1)
+            else:
+                q = list(q)
+                q[a] = 0 if bound & 1 else dom.blocks[cb].size[a] - 1
+        else:
+            q = list(q)
+            q[a] += 1 if bound & 1 else -1
+    return _block_data(dom, cb, q, comp, kind, fields)
+
+
+def nonortho_alpha_interp(dom: ODomain, bi: int, p, with_visc: bool, with_A: bool, A=None, nu=None) -> np.ndarray:
+    """interpolateNonOrthoLaplaceComponents, kernel.cu:1911-1987: per face and tangent axis
+    (axis + i) % D the face-averaged off-diagonal Laplace coefficient, [2D][D-1].  A face counts as
+    prescribed unless the cell is strictly inside along its axis or the face is not a prescribed type
+    (so a cell on one wall also drops the opposite face, as in the reference)."""
+    D = dom.dims
+    g = _gidx(dom, bi, p)
+    aP = _lap_full(dom, g)
+    raP = (1.0 / A[g] if with_A else 1.0) * (nu[g] if with_visc else 1.0)
+    out = np.zeros((2 * D, max(D - 1, 1)))
+    for face in range(2 * D):
+        axis = face >> 1
+        s = dom.blocks[bi].size[axis]
+        if not ((0 < p[axis] < s - 1) or not _is_empty(dom, bi, face)):
+            continue
+        if _at_bound(dom, bi, p, face) and dom.blocks[bi].boundaries[face].kind == "connected":
+            nb_, q = _conn_pos(dom, bi, face, p, 0)
+        else:
+            nb_, q = bi, list(p)
+            if _at_bound(dom, bi, p, face) and dom.blocks[bi].boundaries[face].kind == "periodic":
+                q[axis] = 0 if face & 1 else s - 1
+            else:
+                q[axis] += 1 if face & 1 else -1
+        gN = _gidx(dom, nb_, q)
+        M = dom.Minv[gN]
+        aN = dom.det[gN] * (M @ M[axis])  # getLaplaceCoefficientsSingleAxis, kernel.cu:1298-1320 (no axis mapping)
+        raN = (1.0 / A[gN] if with_A else 1.0) * (nu[gN] if with_visc else 1.0)
+        for i in range(1, D):
+            t = (axis + i) % D
+            out[face, i - 1] = (aP[axis, t] * raP + aN[t] * raN) * 0.5
+    return out
+
+
+def nonortho_matrix_terms(dom: ODomain, flags: int, which: str, A=None, nu=None) -> np.ndarray:
+    """Non-orthogonal stencil terms [K, N]: which='adv' as PISO_build_matrix, kernel.cu:3736-3800 (with
+    viscosity; the caller divides by det afterwards), which='p' as PISO_build_pressure_matrix,
+    kernel.cu:4877-4934 (with 1/A).  A corner interpolated from n cells contributes
+    faceSign * tFaceSign * alpha / n to the diagonal, the face neighbour and the tangential neighbour;
+    a corner on a gradient boundary is replaced by a one-sided difference (3/4, 1/4)."""
+    D = dom.dims
+    N = dom.N
+    add = np.zeros((2 * D + 1, N))
+    incl_nb = bool(flags & NON_ORTHO_DIRECT_MATRIX)
+    incl_diag = bool(flags & NON_ORTHO_CENTER_MATRIX)
+    if D < 2 or not (incl_nb or incl_diag):
+        return add
+    sgn = -1.0 if which == "adv" else 1.0
+    kind = "vel" if which == "adv" else "flag"
+    for g in range(N):
+        bi = int(dom.blk[g])
+        p = [int(v) for v in dom.pos[g]]
+        ai = nonortho_alpha_interp(dom, bi, p, which == "adv", which == "p", A, nu)
+        for face in range(2 * D):
+            if _at_bound(dom, bi, p, face) and _is_empty(dom, bi, face):
+                continue
+            fs = 1.0 if face & 1 else -1.0
+            axis = face >> 1
+            for i in range(1, D):
+                t = (axis + i) % D
+                alpha = ai[face, i - 1]
+                if alpha == 0:
+                    continue
+                for tup in range(2):
+                    tface = 2 * t + tup
+                    ts = 1.0 if tup else -1.0
+                    _, n, btype = corner_value(dom, bi, p, 0, face, tface, False, False, 2, kind, None)
+                    grad = (btype == "neumann") if which == "adv" else True
+                    if n < 1:
+                        if grad:
+                            v = fs * ts * alpha * 0.25
+                            if incl_diag:
+                                add[0, g] += sgn * 3 * v
+                            if incl_nb:
+                                add[face + 1, g] += sgn * 3 * v
+                                add[(tface ^ 1) + 1, g] -= sgn * v
+                    else:
+                        v = fs * ts * alpha / n
+                        if incl_diag:
+                            add[0, g] += sgn * v
+                        if incl_nb:
+                            add[face + 1, g] += sgn * v
+                            add[tface + 1, g] += sgn * v
+    return add
+
+
+def nonortho_rhs(dom: ODomain, flags: int, kind: str, fields, comp: int, with_visc: bool, with_A: bool,
+                 A=None, nu=None) -> np.ndarray:
+    """getNonOrthoLaplaceRHS_v2, kernel.cu:3033-3187, for component `comp` of every cell: the explicit
+    part of the tangential fluxes (corner values of the data in `fields`: kind 'vel' the velocity
+    result, 'p' the pressure result), and for the velocity the tangential gradient of the fixed
+    boundary data on prescribed faces.  The sign assumes the Laplacian on the left-hand side."""
+    D = dom.dims
+    N = dom.N
+    S = np.zeros(N)
+    if not (flags & (NON_ORTHO_DIRECT_RHS | NON_ORTHO_DIAGONAL_RHS)) or D < 2:
+        return S
+    incl1 = bool(flags & NON_ORTHO_DIRECT_RHS)
+    for g in range(N):
+        bi = int(dom.blk[g])
+        p = [int(v) for v in dom.pos[g]]
+        aP = _lap_full(dom, g)
+        raP = (1.0 / A[g] if with_A else 1.0) * (nu[g] if with_visc else 1.0)
+        s = 0.0
+        for face in range(2 * D):
+            axis = face >> 1
+            fs = 1.0 if face & 1 else -1.0
+            if _at_bound(dom, bi, p, face) and _is_empty(dom, bi, face):
+                if kind == "p" or _fixed_type(kind) == "neumann":
+                    continue
+                balpha = _bound_lap_axis(dom, bi, face, p, axis)
+                for i in range(1, D):
+                    t = (axis + i) % D
+                    tlo = p[t] == 0
+                    thi = p[t] == dom.blocks[bi].size[t] - 1
+                    lo, hi = list(p), list(p)
+                    if not tlo:
+                        lo[t] -= 1
+                    if not thi:
+                        hi[t] += 1
+                    df = 1.0 if (tlo or thi) else 0.5
+                    tg = df * (_fixed_data(dom, bi, face, hi, comp, kind) - _fixed_data(dom, bi, face, lo, comp, kind))
+                    bv = nu[g] if with_visc else 1.0
+                    s -= fs * balpha[t] * tg * bv
+                continue
+            nb_, q, mapping = _neighbor_info(dom, bi, p, face)
+            gN = _gidx(dom, nb_, q)
+            M = dom.Minv[gN]
+            am = mapping[axis] >> 1
+            aN = np.array([dom.det[gN] * np.dot(M[mapping[c] >> 1], M[am]) for c in range(D)])
+            raN = (1.0 / A[gN] if with_A else 1.0) * (nu[gN] if with_visc else 1.0)
+            for i in range(1, D):
+                t = (axis + i) % D
+                fa = (aP[axis, t] * raP + aN[t] * raN) * 0.5
+                tg = 0.0
+                for tup in range(2):
+                    tface = 2 * t + tup
+                    ts = 1.0 if tup else -1.0
+                    val, n, btype = corner_value(dom, bi, p, comp, face, tface, False, incl1, 2, kind, fields)
+                    if n == 0 and (btype == "neumann" or kind == "p"):
+                        tother = tface ^ 1
+                        if flags & NON_ORTHO_DIRECT_RHS:
+                            tg += ts * _neighbor_data(dom, bi, p, face, comp, kind, fields) * 0.75
+                            tg += -ts * _neighbor_data(dom, bi, p, tother, comp, kind, fields) * 0.25
+                        if flags & NON_ORTHO_DIAGONAL_RHS:
+                            tg += -ts * _diagonal_data(dom, bi, p, face, tother, comp, kind, fields) * 0.25
+                    else:
+                        tg += ts * val
+                s -= fs * fa * tg
+        S[g] = s
+    return S
 
 
 # --------------------------------------------------------------------------
@@ -757,7 +1155,8 @@ def cg(A, b, x0=None, tol=1e-5, maxit=5000, dtype=np.float64):
     info = SolveInfo(0.0, -1, False, True)
     for i in range(maxit):
         q = A @ p
-        alpha = rho / float(np.dot(p, q))
+        with np.errstate(divide="ignore", invalid="ignore"):  # a vanishing p.q gives inf / nan, as on the device
+            alpha = np.float64(rho) / np.float64(np.dot(p, q))
         x = x + alpha * p
         r = r - alpha * q
         crit = _crit(r)
@@ -769,7 +1168,8 @@ def cg(A, b, x0=None, tol=1e-5, maxit=5000, dtype=np.float64):
             break
         rhop = rho
         rho = float(np.dot(r, r))
-        beta = rho / rhop
+        with np.errstate(divide="ignore", invalid="ignore"):
+            beta = np.float64(rho) / np.float64(rhop)
         p = beta * p + r
     return x, info
 
@@ -789,14 +1189,16 @@ def bicgstab(A, b, x0=None, tol=1e-5, maxit=5000, dtype=np.float64):
     rho = 0.0
     alpha = omega = 0.0
     info = SolveInfo(0.0, -1, False, True)
+    f64 = np.float64
     for i in range(maxit):
         rhop = rho
         rho = float(np.dot(rw, r))
-        if i > 0:
-            beta = (rho / rhop) * (alpha / omega)
-            p = r + beta * (p - omega * v)
-        v = A @ p
-        alpha = rho / float(np.dot(rw, v))
+        with np.errstate(divide="ignore", invalid="ignore"):  # breakdowns give inf / nan, as on the device
+            if i > 0:
+                beta = (f64(rho) / f64(rhop)) * (f64(alpha) / f64(omega))
+                p = r + beta * (p - omega * v)
+            v = A @ p
+            alpha = f64(rho) / f64(np.dot(rw, v))
         r = r - alpha * v
         x = x + alpha * p
         nrmr = _crit(r)
@@ -808,7 +1210,8 @@ def bicgstab(A, b, x0=None, tol=1e-5, maxit=5000, dtype=np.float64):
             break
         s = r
         t = A @ s
-        omega = float(np.dot(t, r)) / float(np.dot(t, t))
+        with np.errstate(divide="ignore", invalid="ignore"):
+            omega = f64(np.dot(t, r)) / f64(np.dot(t, t))
         x = x + omega * s
         r = r - omega * t
         nrmr = _crit(r)
@@ -852,12 +1255,17 @@ class StepResult:
 
 def piso_step(dom: ODomain, dt: float, corrector_steps: int = 2, adv_tol: float = 1e-5,
               p_tol: float = 1e-5, method: str = "iterative", maxit: int = 5000,
-              normalize_pressure: bool = True) -> StepResult:
-    """One PISO step, Simulation._PISO_split_step with non_orthogonal=False, PISOtorch_simulation.py:1054-1327.
+              normalize_pressure: bool = True, non_ortho_flags: int = 0, advect_non_ortho_steps: int = 1,
+              pressure_non_ortho_steps: int = 1) -> StepResult:
+    """One PISO step, Simulation._PISO_split_step, PISOtorch_simulation.py:1054-1327: the orthogonal branch, or
+    with non_ortho_flags the non-orthogonal branch (PISOtorch_simulation.py:1194-1296).
 
     Updates the block velocity and pressure of ``dom`` in place and returns the intermediate fields
     of the last corrector for inspection.
     """
+    if non_ortho_flags:
+        return _piso_step_nonortho(dom, dt, corrector_steps, adv_tol, p_tol, method, maxit, normalize_pressure,
+                                   non_ortho_flags, advect_non_ortho_steps, pressure_non_ortho_steps)
     D = dom.dims
     N = dom.N
     infos = []
@@ -882,6 +1290,48 @@ def piso_step(dom: ODomain, dt: float, corrector_steps: int = 2, adv_tol: float 
         dom.set_pressure_global(p)  # CopyPressureResultToBlocks
         u_cur = correct_velocity(dom, p, A, h)
     dom.set_velocity_global(u_cur)  # CopyVelocityResultToBlocks
+    return StepResult(Ccoef, A, rhs, u_star, P, h, div, p, u_cur, infos)
+
+
+def _piso_step_nonortho(dom, dt, corrector_steps, adv_tol, p_tol, method, maxit, normalize_pressure, flags,
+                        advect_steps, pressure_steps):
+    """The non-orthogonal branch of Simulation._PISO_split_step, PISOtorch_simulation.py:1194-1296: the velocity
+    result is copied from the blocks and feeds the explicit terms of the velocity RHS; every corrector
+    builds P with the non-orthogonal terms, h and div h plus the explicit terms of the current pressure
+    result, solves from zero (each further non-orthogonal pressure step reuses h), subtracts the mean
+    and corrects the velocity."""
+    D = dom.dims
+    N = dom.N
+    infos = []
+    Ccoef, A = advection_matrix(dom, dt, flags)
+    Cm = stencil_to_scipy(dom, Ccoef)
+    u_res = dom.velocity_global()  # CopyVelocityResultFromBlocks
+    rhs = None
+    for _ in range(advect_steps):
+        rhs = advection_rhs(dom, dt, flags, u_res)
+        u_new = np.zeros((D, N))
+        for c in range(D):
+            u_new[c], info = solve(Cm, rhs[c], True, adv_tol, maxit, method)
+            infos.append(("adv", c, info))
+        u_res = u_new
+    u_star = u_res
+    u_cur = u_star
+    P = h = div = p = None
+    for _ in range(corrector_steps):
+        P = pressure_matrix(dom, A, flags)
+        Pm = stencil_to_scipy(dom, P)
+        h = pressure_rhs(dom, dt, Ccoef, A, u_cur)
+        div0 = divergence(dom, h)
+        for _ in range(pressure_steps):
+            div = pressure_rhs_nonortho(dom, flags, div0, A, dom.p_result)
+            p, info = solve(Pm, div, False, p_tol, maxit, method)
+            infos.append(("p", 0, info))
+            if normalize_pressure:
+                p = p - p.mean()
+            dom.p_result = p
+        dom.set_pressure_global(p)  # CopyPressureResultToBlocks
+        u_cur = correct_velocity(dom, p, A, h)
+    dom.set_velocity_global(u_cur)
     return StepResult(Ccoef, A, rhs, u_star, P, h, div, p, u_cur, infos)
 
 

@@ -147,7 +147,77 @@ def case(name, seed=0):
                             dict(coords=c2, velocity=_rand_field(rng, (1, 3, nz, ny, nx2), 0.3))],
                     ops=[("close_all", 0), ("close_all", 1), ("connect", 0, "+x", 1, "-x", "-y", "-z"),
                          ("close", 0, "+y", np.array([[1.0, 0.0, 0.0]]))])
+    if name == "skewed_channel2d":
+        # periodic in x, walls at +-y, skew growing with y (non-orthogonal at the upper wall)
+        nx, ny = 10, 8
+        c = tensor_grid(np.linspace(0, 2, nx + 1), np.linspace(0, 1, ny + 1))
+        c[0, 0] = c[0, 0] + 0.35 * c[0, 1] ** 2
+        return dict(dims=2, viscosity=1e-2,
+                    blocks=[dict(coords=c, velocity=_rand_field(rng, (1, 2, ny, nx), 0.3), source=np.array([[0.2, 0.0]]))],
+                    ops=[("periodic", 0, "x"), ("close", 0, "-y"), ("close", 0, "+y")])
+    if name == "skewed_periodic2d":
+        # uniformly sheared, periodic in both axes
+        nx, ny = 9, 8
+        c = tensor_grid(np.linspace(0, 1, nx + 1), np.linspace(0, 1, ny + 1))
+        c[0, 0] = c[0, 0] + 0.3 * c[0, 1]
+        return dict(dims=2, viscosity=1e-2, blocks=[dict(coords=c, velocity=_rand_field(rng, (1, 2, ny, nx), 0.3))],
+                    ops=[])
+    if name == "skewed_inflow2d":
+        # inflow face with data varying along it (tangential gradient of the boundary data)
+        nx, ny = 12, 8
+        c = tensor_grid(np.linspace(0, 3, nx + 1), np.linspace(0, 1, ny + 1))
+        c[0, 0] = c[0, 0] + 0.25 * c[0, 1]
+        inflow = np.zeros((1, 2, ny, 1))
+        inflow[0, 0, :, 0] = 1.0 + 0.2 * np.sin(np.linspace(0, np.pi, ny))
+        outflow = np.zeros((1, 2, ny, 1))
+        outflow[0, 0, :, 0] = inflow[0, 0].sum() / ny
+        return dict(dims=2, viscosity=1e-2, blocks=[dict(coords=c, velocity=_rand_field(rng, (1, 2, ny, nx), 0.2))],
+                    ops=[("close_all", 0), ("close", 0, "-x", inflow), ("close", 0, "+x", outflow)])
+    if name == "skewed_twoblock2d":
+        ny, n1, n2 = 8, 6, 7
+        c1 = tensor_grid(np.linspace(0, 1, n1 + 1), np.linspace(0, 1, ny + 1))
+        c2 = tensor_grid(np.linspace(1, 2.5, n2 + 1), np.linspace(0, 1, ny + 1))
+        c1[0, 1] = c1[0, 1] + 0.15 * np.sin(np.pi * c1[0, 0]) * c1[0, 1] * (1 - c1[0, 1]) * 4
+        c2[0, 1] = c2[0, 1] + 0.15 * np.sin(np.pi * c2[0, 0] / 2.5) * c2[0, 1] * (1 - c2[0, 1]) * 4
+        return dict(dims=2, viscosity=1e-2,
+                    blocks=[dict(coords=c1, velocity=_rand_field(rng, (1, 2, ny, n1), 0.3)),
+                            dict(coords=c2, velocity=_rand_field(rng, (1, 2, ny, n2), 0.3))],
+                    ops=[("close_all", 0), ("close_all", 1), ("connect", 0, "+x", 1, "-x", "-y"),
+                         ("close", 0, "+y", np.array([[1.0, 0.0]]))])
+    if name == "skewed_twoblock2d_rotated":
+        n = 7
+        c1 = rotate_distort(tensor_grid(np.linspace(0, 1, n + 1), np.linspace(0, 1, n + 1)), 0.3)
+        c2 = tensor_grid(np.linspace(0, 1, n + 1), np.linspace(0, 1, n + 1))
+        c2[0, 0] = c2[0, 0] + 0.2 * c2[0, 1] * (1 - c2[0, 1])
+        return dict(dims=2, viscosity=1e-2,
+                    blocks=[dict(coords=c1, velocity=_rand_field(rng, (1, 2, n, n), 0.3)),
+                            dict(coords=c2, velocity=_rand_field(rng, (1, 2, n, n), 0.3))],
+                    ops=[("close_all", 0), ("close_all", 1), ("connect", 0, "+x", 1, "+y", "-x"),
+                         ("close", 0, "-y", np.array([[1.0, 0.0]]))])
+    if name == "skewed_cavity3d":
+        n = 5
+        c = tensor_grid(np.linspace(0, 1, n + 1), np.linspace(0, 1, n + 1), np.linspace(0, 1, n + 1))
+        c[0, 0] = c[0, 0] + 0.2 * c[0, 1] * c[0, 2]
+        c[0, 2] = c[0, 2] + 0.15 * c[0, 1] ** 2
+        return dict(dims=3, viscosity=1e-2, blocks=[dict(coords=c, velocity=_rand_field(rng, (1, 3, n, n, n), 0.2))],
+                    ops=[("close_all", 0), ("close", 0, "+y", np.array([[1.0, 0.0, 0.0]]))])
+    if name == "skewed_channel3d":
+        nx, ny, nz = 6, 5, 4
+        c = tensor_grid(np.linspace(0, 2, nx + 1), stretched(ny, 1.0, 1.5), np.linspace(0, 1, nz + 1))
+        c[0, 0] = c[0, 0] + 0.3 * c[0, 1]
+        c[0, 2] = c[0, 2] + 0.2 * c[0, 1]
+        return dict(dims=3, viscosity=1e-2,
+                    blocks=[dict(coords=c, velocity=_rand_field(rng, (1, 3, nz, ny, nx), 0.3),
+                                 source=np.array([[0.2, 0.0, 0.0]]))],
+                    ops=[("periodic", 0, "x"), ("periodic", 0, "z"), ("close", 0, "-y"), ("close", 0, "+y")])
     raise KeyError(name)
+
+
+# non-orthogonal grids for the nonOrthoFlags paths (operators pinned on all of them; full steps where the
+# pressure solve converges)
+NONORTHO_CASES = ["distorted2d", "skewed_channel2d", "skewed_periodic2d", "skewed_inflow2d", "skewed_twoblock2d",
+                  "skewed_twoblock2d_rotated", "skewed_cavity3d", "skewed_channel3d"]
+NONORTHO_FLAG_SETS = [25, 27, 19]
 
 
 CASES_2D = ["cavity2d", "cavity2d_refined", "distorted2d", "periodic2d", "fullperiodic2d", "inflow2d", "twoblock2d",
