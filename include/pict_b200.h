@@ -166,9 +166,14 @@ pict_status_t pict_build_tiles(const pict_block_t* host_blocks, int32_t num_bloc
                                int32_t tile_cells, int32_t* tiles_out, int32_t max_tiles, int32_t* sim_tiles_out,
                                int32_t* num_tiles_out);
 
-/* ---------------- assembly (forward) ---------------- */
+/* ---------------- assembly (forward) ----------------
+ * non_ortho_flags: the reference's nonOrthoFlags bits (extensions/PISO_multiblock_cuda.h:9-13): 1 direct
+ * matrix terms, 2 direct RHS terms, 8 diagonal RHS terms, 16 centre matrix terms (4 has no effect, as in
+ * the reference).  The matrix bits add the tangential-flux terms to C / A and P, the RHS bits add the
+ * explicit terms of the current velocityResult to the velocity RHS and of the current pressureResult
+ * to the pressure RHS divergence (extensions/PISO_multiblock_cuda_kernel.cu:1911-1987, 2742-2860, 3033-3187). */
 /* SetupAdvectionMatrix (extensions/PISOtorch.cpp:531-533 -> extensions/PISO_multiblock_cuda_kernel.cu:4510 PISO_build_matrix):
- * writes C and A from the blocks' velocity.  non_ortho_flags must be 0. */
+ * writes C and A from the blocks' velocity. */
 pict_status_t pict_setup_advection_matrix(const pict_domain_t* dom, double dt, int32_t non_ortho_flags,
                                           void* stream);
 /* SetupAdvectionVelocity (extensions/PISOtorch.cpp:537-539 -> extensions/PISO_multiblock_cuda_kernel.cu:4677 kPISO_build_advection_RHS). */

@@ -18,11 +18,12 @@ Differences in representation (not in results):
 * Linear solves run as persistent CUDA kernels; ``SolveLinear`` still returns
   one ``LinearSolverResultInfo`` per right-hand side.
 
-Scope: the orthogonal PISO path (``nonOrthoFlags=0``) with fixed Dirichlet,
+Scope: the PISO path (orthogonal, and the non-orthogonal terms of ``nonOrthoFlags``) with fixed Dirichlet,
 periodic and connected block boundaries, per-cell transforms, block/global
 viscosity and velocity sources, in 2D and 3D, float32 and float64.  Passive
-scalar transport, non-orthogonal corrections, the FVM velocity correctors and
-ILU preconditioning raise ``NotImplementedError``.
+scalar transport, the FVM velocity correctors, face-transform pressure assembly
+and ILU preconditioning raise ``NotImplementedError``; the gradients of the
+non-orthogonal terms are not implemented.
 """
 from __future__ import annotations
 
@@ -1690,28 +1691,42 @@ def _time_step(timeStep, domain):
     return float(timeStep.item())
 
 
+# nonOrthoFlags bits (extensions/PISO_multiblock_cuda.h:9-13); NON_ORTHO_DIAGONAL_MATRIX has no effect in the
+# reference either
+NON_ORTHO_DIRECT_MATRIX = 1
+NON_ORTHO_DIRECT_RHS = 2
+NON_ORTHO_DIAGONAL_MATRIX = 4
+NON_ORTHO_DIAGONAL_RHS = 8
+NON_ORTHO_CENTER_MATRIX = 16
+
+
 def _non_ortho(flags):
-    if int(flags) != 0:
-        raise NotImplementedError("non-orthogonal corrections (nonOrthoFlags != 0) are not implemented in pict_b200")
+    flags = int(flags)
+    _check(0 <= flags < 32, "invalid nonOrthoFlags %d" % flags)
+    return flags
 
 
 def SetupAdvectionMatrix(domain, timeStep, nonOrthoFlags, forPassiveScalar=False, passiveScalarChannel=0):
     """Implicit advection-diffusion matrix C and its diagonal A (extensions/PISO_multiblock_cuda_kernel.cu:3601-3865)."""
     if forPassiveScalar:
         raise NotImplementedError("passive scalar transport is not implemented in pict_b200")
-    _non_ortho(nonOrthoFlags)
+    flags = _non_ortho(nonOrthoFlags)
     domain._check_ready()
     dt = _time_step(timeStep, domain)
-    check(_lib.load().pict_setup_advection_matrix(ctypes.byref(domain._desc), dt, 0, _stream_ptr()), "SetupAdvectionMatrix")
+    check(_lib.load().pict_setup_advection_matrix(ctypes.byref(domain._desc), dt, flags, _stream_ptr()),
+          "SetupAdvectionMatrix")
 
 
 def SetupAdvectionVelocity(domain, timeStep, nonOrthoFlags, applyPressureGradient=False):
-    """Velocity RHS of the advection-diffusion solve (extensions/PISO_multiblock_cuda_kernel.cu:4281-4385)."""
-    _non_ortho(nonOrthoFlags)
+    """Velocity RHS of the advection-diffusion solve (extensions/PISO_multiblock_cuda_kernel.cu:4281-4385).  With
+    non-orthogonal RHS flags the explicit terms are taken from ``domain.velocityResult`` (as in the reference,
+    the caller copies the block velocity there first)."""
+    flags = _non_ortho(nonOrthoFlags)
     domain._check_ready()
     dt = _time_step(timeStep, domain)
-    check(_lib.load().pict_setup_advection_velocity(ctypes.byref(domain._desc), dt, 0, int(bool(applyPressureGradient)),
-                                                    _stream_ptr()), "SetupAdvectionVelocity")
+    check(_lib.load().pict_setup_advection_velocity(ctypes.byref(domain._desc), dt, flags,
+                                                    int(bool(applyPressureGradient)), _stream_ptr()),
+          "SetupAdvectionVelocity")
 
 
 def SetupAdvectionScalar(domain, timeStep, nonOrthoFlags):
@@ -1719,42 +1734,44 @@ def SetupAdvectionScalar(domain, timeStep, nonOrthoFlags):
 
 
 def SetupPressureCorrection(domain, timeStep, nonOrthoMode=0, useFaceTransform=False, timeStepNorm=False):
-    """Pressure matrix, H/A RHS and its divergence (extensions/PISO_multiblock_cuda_kernel.cu:4797-5419)."""
-    _non_ortho(nonOrthoMode)
+    """Pressure matrix, H/A RHS and its divergence (extensions/PISO_multiblock_cuda_kernel.cu:4797-5419); with
+    non-orthogonal RHS flags the explicit terms of ``domain.pressureResult`` are added to the divergence."""
+    flags = _non_ortho(nonOrthoMode)
     if useFaceTransform:
         raise NotImplementedError("face-transform pressure assembly is not implemented in pict_b200")
     domain._check_ready()
     dt = _time_step(timeStep, domain)
-    check(_lib.load().pict_setup_pressure_correction(ctypes.byref(domain._desc), dt, 0, int(bool(timeStepNorm)),
+    check(_lib.load().pict_setup_pressure_correction(ctypes.byref(domain._desc), dt, flags, int(bool(timeStepNorm)),
                                                      _stream_ptr()), "SetupPressureCorrection")
 
 
 def SetupPressureMatrix(domain, timeStep, nonOrthoMode=0, useFaceTransform=False):
-    _non_ortho(nonOrthoMode)
+    flags = _non_ortho(nonOrthoMode)
     if useFaceTransform:
         raise NotImplementedError("face-transform pressure assembly is not implemented in pict_b200")
     domain._check_ready()
     _time_step(timeStep, domain)
-    check(_lib.load().pict_setup_pressure_matrix(ctypes.byref(domain._desc), 0, _stream_ptr()), "SetupPressureMatrix")
+    check(_lib.load().pict_setup_pressure_matrix(ctypes.byref(domain._desc), flags, _stream_ptr()),
+          "SetupPressureMatrix")
 
 
 def SetupPressureRHS(domain, timeStep, nonOrthoMode=0, useFaceTransform=False, timeStepNorm=False):
-    _non_ortho(nonOrthoMode)
+    flags = _non_ortho(nonOrthoMode)
     if useFaceTransform:
         raise NotImplementedError("face-transform pressure assembly is not implemented in pict_b200")
     domain._check_ready()
     dt = _time_step(timeStep, domain)
-    check(_lib.load().pict_setup_pressure_rhs(ctypes.byref(domain._desc), dt, 0, int(bool(timeStepNorm)), _stream_ptr()),
-          "SetupPressureRHS")
+    check(_lib.load().pict_setup_pressure_rhs(ctypes.byref(domain._desc), dt, flags, int(bool(timeStepNorm)),
+                                              _stream_ptr()), "SetupPressureRHS")
 
 
 def SetupPressureRHSdiv(domain, timeStep, nonOrthoMode=0, useFaceTransform=False, timeStepNorm=False):
-    _non_ortho(nonOrthoMode)
+    flags = _non_ortho(nonOrthoMode)
     if useFaceTransform:
         raise NotImplementedError("face-transform pressure assembly is not implemented in pict_b200")
     domain._check_ready()
     dt = _time_step(timeStep, domain)
-    check(_lib.load().pict_setup_pressure_rhs_div(ctypes.byref(domain._desc), dt, 0, int(bool(timeStepNorm)),
+    check(_lib.load().pict_setup_pressure_rhs_div(ctypes.byref(domain._desc), dt, flags, int(bool(timeStepNorm)),
                                                   _stream_ptr()), "SetupPressureRHSdiv")
 
 

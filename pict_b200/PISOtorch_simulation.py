@@ -12,9 +12,9 @@ execution paths produce the same step:
   without host synchronisation.
 
 Non-orthogonal correction terms are not implemented: with
-``non_orthogonal=True`` the driver verifies that every block's metric is
-orthogonal (the correction terms then vanish identically) and otherwise raises
-``NotImplementedError``.  Image/VTK output belongs to the reference's
+``non_orthogonal=True`` and a domain whose metrics are not orthogonal, the step follows the
+reference's non-orthogonal branch operator by operator (on orthogonal metrics the terms vanish
+identically and the fused step runs).  Image/VTK output belongs to the reference's
 post-processing utilities and is not part of this package; the corresponding
 arguments are accepted and ignored with a warning.
 """
@@ -360,14 +360,21 @@ class Simulation:
                 and not self.pressure_use_BiCG and self.normalize_pressure_result
                 and not (self.advect_passive_scalar and d.hasPassiveScalar()))
 
+    def _non_ortho_flags(self):
+        """The nonOrthoFlags of this step: the driver's mode (PISOtorch_simulation.py:390-396, 579-585) when
+        non_orthogonal is set and some block's metric is not exactly orthogonal; 0 otherwise (the terms
+        vanish identically on orthogonal metrics, so the orthogonal step is taken)."""
+        if not self.non_orthogonal:
+            return 0
+        key = id(self.domain)
+        if getattr(self, "_ortho_key", None) != key:
+            self._ortho_flags = 0 if metrics_are_orthogonal(self.domain, rtol=0.0) else Simulation._NON_ORTHO_MODE
+            self._ortho_key = key
+        return self._ortho_flags
+
     def _check_non_ortho(self):
-        if self.non_orthogonal:
-            key = ("ortho", id(self.domain))
-            if getattr(self, "_ortho_checked", None) != key:
-                if not metrics_are_orthogonal(self.domain):
-                    raise NotImplementedError("non-orthogonal correction terms are not implemented in pict_b200; "
-                                              "this domain's metrics are not orthogonal")
-                self._ortho_checked = key
+        if self._non_ortho_flags() and self.differentiable:
+            raise NotImplementedError("gradients of the non-orthogonal terms are not implemented in pict_b200")
 
     def _get_stepper(self):
         key = (id(self.domain), self.corrector_steps, self.advection_tol, self.pressure_tol,
@@ -388,7 +395,7 @@ class Simulation:
             iterations = int(iterations.numpy()[0])
         assert iterations > 0
         domain = self.domain
-        if self._fused_eligible():
+        if self._fused_eligible() and not self._non_ortho_flags():
             if domain.IsTensorChanged():
                 domain.UpdateDomainData()
             st = self._get_stepper()
@@ -403,12 +410,16 @@ class Simulation:
         return self._PISO_split_step_ops(iterations, time_step)
 
     def _PISO_split_step_ops(self, iterations, time_step):
-        """Operator-by-operator step, PISOtorch_simulation.py:1054-1327 (orthogonal branch)."""
+        """Operator-by-operator step, PISOtorch_simulation.py:1054-1327 (orthogonal branch, or the non-orthogonal
+        branch PISOtorch_simulation.py:1194-1296 when the domain's metrics are not orthogonal)."""
         domain = self.domain
         B = self._backend
         vcv = self._velocity_corrector_version
         solve_ok = True
         advect_use_prev_result = self.advect_reuse_result and not self.differentiable
+        flags = self._non_ortho_flags()
+        if flags:
+            return self._PISO_split_step_non_ortho(iterations, time_step, flags)
         for step in range(iterations):
             if self.convergence_tol is not None:
                 B.CopyVelocityResultFromBlocks(domain)
@@ -472,6 +483,98 @@ class Simulation:
             self.end_step(time_step)
         return solve_ok
 
+    def _PISO_split_step_non_ortho(self, iterations, time_step, flags):
+        """The non-orthogonal branch of Simulation._PISO_split_step, PISOtorch_simulation.py:1180-1296: the velocity
+        result is copied from the blocks for the explicit terms of the velocity RHS (advect_non_ortho_steps
+        solves); each corrector builds P once and solves pressure_non_ortho_steps times, the first with
+        a fresh H/A field, the next ones with its divergence plus the explicit terms of the latest pressure
+        result (CG with a residual reset every 100 iterations, as the reference driver asks)."""
+        domain = self.domain
+        B = self._backend
+        vcv = self._velocity_corrector_version
+        solve_ok = True
+        advect_reuse = self.advect_reuse_result and not self.differentiable
+        pressure_reuse = self.pressure_reuse_result and not self.differentiable
+        for step in range(iterations):
+            if self.convergence_tol is not None:
+                B.CopyVelocityResultFromBlocks(domain)
+                last_vel = domain.velocityResult.clone().detach()
+            self._run_prep_fn("PRE", domain=domain, local_step=step, time_step=time_step, total_step=self.total_step,
+                              total_time=self.total_time)
+            domain.UpdateDomainData()
+            if self.advect_passive_scalar and domain.hasPassiveScalar():
+                raise NotImplementedError("passive scalar transport is not implemented in pict_b200")
+            self._run_prep_fn("PRE_VELOCITY_SETUP", domain=domain, local_step=step, time_step=time_step,
+                              total_step=self.total_step, total_time=self.total_time)
+            B.SetupAdvectionMatrix(domain, time_step, flags)
+            B.CopyVelocityResultFromBlocks(domain)
+            for no_step in range(self.advect_non_ortho_steps):
+                B.SetupAdvectionVelocity(domain, time_step, flags, False)
+                self._run_prep_fn("POST_VELOCITY_SETUP", domain=domain, no_step=no_step, local_step=step,
+                                  time_step=time_step, total_step=self.total_step, total_time=self.total_time)
+                with torch.no_grad() if self.exclude_advection_solve_gradients else nullcontext():
+                    x = None if (no_step == 0 or not advect_reuse) else domain.velocityResult
+                    velocityResult, solve_ok = self.linear_solve(domain.C, domain.velocityRHS, x=x,
+                                                                 use_BiCG=self.advection_use_BiCG,
+                                                                 use_scipy=self.scipy_solve_advection,
+                                                                 tol=self.advection_tol)
+                domain.setVelocityResult(velocityResult)
+                domain.UpdateDomainData()
+                if not solve_ok or self._check_stop():
+                    return solve_ok
+            self._run_prep_fn("POST_PREDICTION", domain=domain, local_step=step, time_step=time_step,
+                              total_step=self.total_step, total_time=self.total_time)
+            if self._check_stop():
+                break
+            for cstep in range(self.corrector_steps):
+                B.SetupPressureMatrix(domain, time_step, flags, False)
+                for pstep in range(self.pressure_non_ortho_steps):
+                    if pstep == 0:
+                        B.SetupPressureRHS(domain, time_step, flags, False, timeStepNorm=self.pressure_time_step_normalized)
+                    else:
+                        B.SetupPressureRHSdiv(domain, time_step, flags, False,
+                                              timeStepNorm=self.pressure_time_step_normalized)
+                    self._run_prep_fn("POST_PRESSURE_SETUP", domain=domain, local_step=step, time_step=time_step,
+                                      total_step=self.total_step, total_time=self.total_time)
+                    with torch.no_grad() if self.exclude_pressure_solve_gradients else nullcontext():
+                        x = None if (pstep == 0 or not pressure_reuse) else domain.pressureResult
+                        pressureResult, solve_ok = self.linear_solve(domain.P, domain.pressureRHSdiv, x=x,
+                                                                     residual_reset_step=100,
+                                                                     use_BiCG=self.pressure_use_BiCG,
+                                                                     use_scipy=self.scipy_solve_pressure,
+                                                                     tol=self.pressure_tol,
+                                                                     return_best_result=self.pressure_return_best_result)
+                    if self.normalize_pressure_result:
+                        pressureResult = pressureResult - torch.mean(pressureResult)
+                    domain.setPressureResult(pressureResult)
+                    domain.UpdateDomainData()
+                    self._run_prep_fn("POST_PRESSURE_RESULT", domain=domain, local_step=step, time_step=time_step,
+                                      total_step=self.total_step, total_time=self.total_time)
+                    if not solve_ok:
+                        return solve_ok
+                    if self._check_stop():
+                        break
+                self._run_prep_fn("POST_PRESSURE_NON_ORTHO", domain=domain, local_step=step, time_step=time_step,
+                                  total_step=self.total_step, total_time=self.total_time)
+                B.CopyPressureResultToBlocks(domain)
+                B.CorrectVelocity(domain, time_step, version=vcv, timeStepNorm=self.pressure_time_step_normalized)
+                self._run_prep_fn("POST_VELOCITY_CORRECTION", domain=domain, local_step=step, time_step=time_step,
+                                  total_step=self.total_step, total_time=self.total_time)
+                if self._check_stop():
+                    break
+            B.CopyVelocityResultToBlocks(domain)
+            self._run_prep_fn("POST", domain=domain, local_step=step, time_step=time_step, total_step=self.total_step,
+                              total_time=self.total_time)
+            if self.convergence_tol is not None:
+                diff = torch.max(torch.abs(last_vel - domain.velocityResult)).item()
+                if diff < self.convergence_tol:
+                    _LOG.info("Simulation step max difference is under convergence tolerance.")
+                    solve_ok = False
+            if not solve_ok or self._check_stop():
+                break
+            self.end_step(time_step)
+        return solve_ok
+
     def _PISO_adaptive_step(self, CFL_cond=None, max_subsetps=1000):
         """PISOtorch_simulation.py:1329-1372."""
         time_step_target = self.time_step
@@ -493,31 +596,48 @@ class Simulation:
         return True
 
     def make_divergence_free(self, iterations=1, max_iter=1000):
-        """Pressure projection of the current velocity with A = 1, dt = 1 (PISOtorch_simulation.py:985-1052)."""
+        """Pressure projection of the current velocity with A = 1, dt = 1 (PISOtorch_simulation.py:985-1052), with
+        the non-orthogonal terms (pressure_non_ortho_steps solves) on non-orthogonal metrics."""
         self._check_domain()
         self._check_non_ortho()
         domain = self.domain
         B = self._backend
+        flags = self._non_ortho_flags()
+        pressure_reuse = self.pressure_reuse_result and not self.differentiable
+        if isinstance(iterations, torch.Tensor):
+            iterations = int(iterations.numpy()[0])
         time_step = torch.tensor([1], device=cpu_device, dtype=domain.A.dtype)
         domain.setA(torch.ones_like(domain.A))
         solve_ok = True
         for step in range(iterations):
+            self._run_prep_fn("PRE", domain=domain, local_step=step, time_step=time_step, total_step=self.total_step,
+                              total_time=self.total_time)
             domain.UpdateDomainData()
             B.CopyVelocityResultFromBlocks(domain)
             domain.setPressureRHS(domain.velocityResult)
             domain.UpdateDomainData()
-            B.SetupPressureMatrix(domain, time_step, 0, False)
-            B.SetupPressureRHSdiv(domain, time_step, 0, False, timeStepNorm=self.pressure_time_step_normalized)
-            pressureResult, solve_ok = self.linear_solve(domain.P, domain.pressureRHSdiv, use_BiCG=self.pressure_use_BiCG,
-                                                         tol=self.pressure_tol, max_iter=max_iter)
-            if self.normalize_pressure_result:
-                pressureResult = pressureResult - torch.mean(pressureResult)
-            domain.setPressureResult(pressureResult)
-            domain.UpdateDomainData()
+            B.SetupPressureMatrix(domain, time_step, flags, False)
+            for pstep in range(self.pressure_non_ortho_steps if flags else 1):
+                B.SetupPressureRHSdiv(domain, time_step, flags, False, timeStepNorm=self.pressure_time_step_normalized)
+                x = None if (pstep == 0 or not pressure_reuse) else domain.pressureResult
+                pressureResult, solve_ok = self.linear_solve(domain.P, domain.pressureRHSdiv, x=x,
+                                                             use_BiCG=self.pressure_use_BiCG, tol=self.pressure_tol,
+                                                             max_iter=max_iter,
+                                                             return_best_result=self.pressure_return_best_result)
+                if self.normalize_pressure_result:
+                    pressureResult = pressureResult - torch.mean(pressureResult)
+                domain.setPressureResult(pressureResult)
+                domain.UpdateDomainData()
+                if not solve_ok:
+                    return solve_ok
+                if self._check_stop():
+                    break
             B.CopyPressureResultToBlocks(domain)
             B.CorrectVelocity(domain, time_step, version=self._velocity_corrector_version,
                               timeStepNorm=self.pressure_time_step_normalized)
             B.CopyVelocityResultToBlocks(domain)
+            if not solve_ok or self._check_stop():
+                return solve_ok
             self.end_step(time_step)
         return solve_ok
 

@@ -595,19 +595,34 @@ static pict_status_t check_dom(const pict_domain_t* dom) {
 
 extern "C" {
 
+static pict_status_t adv_matrix(const pict_domain_t* dom, double dt, void* stream) {
+    PICT_DISPATCH(dom, launch_adv, dom, dt, true, false, 0, (cudaStream_t)stream);
+}
+
+static pict_status_t adv_velocity(const pict_domain_t* dom, double dt, int32_t pgrad, void* stream) {
+    PICT_DISPATCH(dom, launch_adv, dom, dt, false, true, pgrad, (cudaStream_t)stream);
+}
+
+static pict_status_t pressure_ops(const pict_domain_t* dom, double dt, bool matrix, bool rhs, bool div, int32_t tsn,
+                                  void* stream) {
+    PICT_DISPATCH(dom, launch_pressure, dom, dt, matrix, rhs, div, tsn, (cudaStream_t)stream);
+}
+
 pict_status_t pict_setup_advection_matrix(const pict_domain_t* dom, double dt, int32_t non_ortho_flags, void* stream) {
     pict_status_t s = check_dom(dom);
     if (s) return s;
-    if (non_ortho_flags != 0) return set_error(PICT_ERR_UNSUPPORTED, "non-orthogonal flags are not supported");
-    PICT_DISPATCH(dom, launch_adv, dom, dt, true, false, 0, (cudaStream_t)stream);
+    s = adv_matrix(dom, dt, stream);
+    if (s || !non_ortho_flags) return s;
+    return nonortho_pass(dom, non_ortho_flags, 0, stream);
 }
 
 pict_status_t pict_setup_advection_velocity(const pict_domain_t* dom, double dt, int32_t non_ortho_flags,
                                             int32_t apply_pressure_gradient, void* stream) {
     pict_status_t s = check_dom(dom);
     if (s) return s;
-    if (non_ortho_flags != 0) return set_error(PICT_ERR_UNSUPPORTED, "non-orthogonal flags are not supported");
-    PICT_DISPATCH(dom, launch_adv, dom, dt, false, true, apply_pressure_gradient, (cudaStream_t)stream);
+    s = adv_velocity(dom, dt, apply_pressure_gradient, stream);
+    if (s || !non_ortho_flags) return s;
+    return nonortho_pass(dom, non_ortho_flags, 1, stream);
 }
 
 pict_status_t pict_setup_advection(const pict_domain_t* dom, double dt, void* stream) {
@@ -619,32 +634,38 @@ pict_status_t pict_setup_advection(const pict_domain_t* dom, double dt, void* st
 pict_status_t pict_setup_pressure_matrix(const pict_domain_t* dom, int32_t non_ortho_flags, void* stream) {
     pict_status_t s = check_dom(dom);
     if (s) return s;
-    if (non_ortho_flags != 0) return set_error(PICT_ERR_UNSUPPORTED, "non-orthogonal flags are not supported");
-    PICT_DISPATCH(dom, launch_pressure, dom, 1.0, true, false, false, 0, (cudaStream_t)stream);
+    s = pressure_ops(dom, 1.0, true, false, false, 0, stream);
+    if (s || !non_ortho_flags) return s;
+    return nonortho_pass(dom, non_ortho_flags, 2, stream);
 }
 
 pict_status_t pict_setup_pressure_rhs(const pict_domain_t* dom, double dt, int32_t non_ortho_flags,
                                       int32_t time_step_norm, void* stream) {
     pict_status_t s = check_dom(dom);
     if (s) return s;
-    if (non_ortho_flags != 0) return set_error(PICT_ERR_UNSUPPORTED, "non-orthogonal flags are not supported");
-    PICT_DISPATCH(dom, launch_pressure, dom, dt, false, true, true, time_step_norm, (cudaStream_t)stream);
+    s = pressure_ops(dom, dt, false, true, true, time_step_norm, stream);
+    if (s || !non_ortho_flags) return s;
+    return nonortho_pass(dom, non_ortho_flags, 3, stream);
 }
 
 pict_status_t pict_setup_pressure_rhs_div(const pict_domain_t* dom, double dt, int32_t non_ortho_flags,
                                           int32_t time_step_norm, void* stream) {
     pict_status_t s = check_dom(dom);
     if (s) return s;
-    if (non_ortho_flags != 0) return set_error(PICT_ERR_UNSUPPORTED, "non-orthogonal flags are not supported");
-    PICT_DISPATCH(dom, launch_pressure, dom, dt, false, false, true, time_step_norm, (cudaStream_t)stream);
+    s = pressure_ops(dom, dt, false, false, true, time_step_norm, stream);
+    if (s || !non_ortho_flags) return s;
+    return nonortho_pass(dom, non_ortho_flags, 3, stream);
 }
 
 pict_status_t pict_setup_pressure_correction(const pict_domain_t* dom, double dt, int32_t non_ortho_flags,
                                              int32_t time_step_norm, void* stream) {
     pict_status_t s = check_dom(dom);
     if (s) return s;
-    if (non_ortho_flags != 0) return set_error(PICT_ERR_UNSUPPORTED, "non-orthogonal flags are not supported");
-    PICT_DISPATCH(dom, launch_pressure, dom, dt, true, true, true, time_step_norm, (cudaStream_t)stream);
+    s = pressure_ops(dom, dt, true, true, true, time_step_norm, stream);
+    if (s || !non_ortho_flags) return s;
+    s = nonortho_pass(dom, non_ortho_flags, 2, stream);
+    if (s) return s;
+    return nonortho_pass(dom, non_ortho_flags, 3, stream);
 }
 
 }  // extern "C"
