@@ -59,7 +59,8 @@ def _get_solver_tolerance_torch(tol=None, dtype=torch.float32):
 
 def check_non_ortho_rhs(non_ortho_flags):
     if non_ortho_flags:
-        raise NotImplementedError("non-orthogonal terms are not implemented in pict_b200")
+        raise NotImplementedError("gradients of the non-orthogonal terms are not implemented in pict_b200 "
+                                  "(the forward operators of pict_b200.PISOtorch compute them)")
     return False
 
 
