@@ -1605,10 +1605,57 @@ class Domain:
             b.CreateVelocityGradOnBoundaries()
 
     def CreateViscosityGrad(self):
+        """Zero gradient of the domain viscosity and of every block viscosity (Domain::CreateViscosityGrad,
+        extensions/domain_structs.cpp:2875-2882)."""
         self.viscosityGrad = torch.zeros_like(self.viscosity)
+        for b in self.blocks:
+            b.CreateViscosityGrad()
 
     def setViscosityGrad(self, t):
         self.viscosityGrad = t
+
+    # -- gradient fields of the global vectors (extensions/PISOtorch.cpp:456-484) --
+    def _grad_vec(self, name, t, n):
+        _check(isinstance(t, torch.Tensor) and t.dim() == 1 and t.numel() == n,
+               "%s must be a 1D tensor with %d elements" % (name, n))
+        _check(t.dtype == self._dtype and t.device == self._device, "%s: dtype/device mismatch" % name)
+        setattr(self, name, t)
+
+    def setAGrad(self, t):
+        self._grad_vec("AGrad", t, self._N)
+
+    def CreateAGrad(self):
+        self.AGrad = torch.zeros(self._N, dtype=self._dtype, device=self._device)
+
+    def setVelocityRHSGrad(self, t):
+        self._grad_vec("velocityRHSGrad", t, self._N * self._dims)
+
+    def CreateVelocityRHSGrad(self):
+        self.velocityRHSGrad = torch.zeros(self._N * self._dims, dtype=self._dtype, device=self._device)
+
+    def setVelocityResultGrad(self, t):
+        self._grad_vec("velocityResultGrad", t, self._N * self._dims)
+
+    def CreateVelocityResultGrad(self):
+        self.velocityResultGrad = torch.zeros(self._N * self._dims, dtype=self._dtype, device=self._device)
+
+    def setPressureRHSGrad(self, t):
+        self._grad_vec("pressureRHSGrad", t, self._N * self._dims)
+
+    def CreatePressureRHSGrad(self):
+        self.pressureRHSGrad = torch.zeros(self._N * self._dims, dtype=self._dtype, device=self._device)
+
+    def setPressureRHSdivGrad(self, t):
+        self._grad_vec("pressureRHSdivGrad", t, self._N)
+
+    def CreatePressureRHSdivGrad(self):
+        self.pressureRHSdivGrad = torch.zeros(self._N, dtype=self._dtype, device=self._device)
+
+    def setPressureResultGrad(self, t):
+        self._grad_vec("pressureResultGrad", t, self._N)
+
+    def CreatePressureResultGrad(self):
+        self.pressureResultGrad = torch.zeros(self._N, dtype=self._dtype, device=self._device)
 
     def hasViscosityGrad(self):
         return self.viscosityGrad is not None
@@ -1811,6 +1858,236 @@ def CopyScalarResultToBlocks(domain):
 
 
 def CopyScalarResultFromBlocks(domain):
+    raise NotImplementedError("passive scalar transport is not implemented in pict_b200")
+
+
+# ------------------------------------------------------------------------------------------------
+# gradient operators (extensions/PISOtorch.cpp:566-593).  They read the gradient fields of the domain
+# (AGrad, CGrad, PGrad, velocityRHSGrad, velocityResultGrad, pressureRHSGrad, pressureRHSdivGrad,
+# pressureResultGrad) and add to the gradient fields of their inputs (blocks' velocity / source /
+# viscosity / pressure gradients, boundaries' velocity gradients, the domain's viscosity gradient and
+# the global gradient vectors), except where the reference assigns: CorrectVelocityGrad writes
+# AGrad and pressureRHSGrad, the Copy*GradFromBlocks / ToBlocks operators copy.  As with the
+# reference, call the matching Create*Grad first for a fresh gradient.  Computed by the same adjoint
+# kernels as the autograd Functions of pict_b200.PISOtorch_diff; the gradients of the non-orthogonal
+# terms and of passive scalars are not implemented.
+# ------------------------------------------------------------------------------------------------
+
+def _need_grad(domain, name, n):
+    t = getattr(domain, name)
+    if t is None or t.numel() != n:
+        setattr(domain, name, torch.zeros(n, dtype=domain.getDtype(), device=domain.getDevice()))
+    return getattr(domain, name)
+
+
+def _grad_ortho_only(flags, what):
+    if int(flags) != 0:
+        raise NotImplementedError("%s: gradients of the non-orthogonal terms are not implemented in pict_b200" % what)
+
+
+def _add_parameter_grads(domain, g):
+    """Add the accumulators of a PISOtorch_diff._Grads to the blocks', boundaries' and domain's gradients."""
+    blocks = domain.getBlocks()
+    D = domain.getSpatialDims()
+
+    def same(t, like):
+        return t is not None and like is not None and t.numel() > 0 and t.shape == like.shape
+
+    old_v = [b.velocityGrad if same(b.velocityGrad, b.velocity) else None for b in blocks]
+    old_s = [b.velocitySourceGrad if same(b.velocitySourceGrad, b.velocitySource) else None for b in blocks]
+    old_n = [b.viscosityGrad if same(b.viscosityGrad, b.viscosity) else None for b in blocks]
+    old_f = [[b.boundaries[f].velocityGrad if (isinstance(b.boundaries[f], FixedBoundary)
+              and same(b.boundaries[f].velocityGrad, b.boundaries[f].velocity)) else None for f in range(2 * D)]
+             for b in blocks]
+    keys = [("VISCOSITY",)]
+    nu = g.to_inputs(keys)[0]
+    for b, ov, os_, on, of in zip(blocks, old_v, old_s, old_n, old_f):
+        if ov is not None:
+            b.setVelocityGrad(b.velocityGrad + ov)
+        if os_ is not None and b.velocitySourceGrad is not None:
+            b.setVelocitySourceGrad(b.velocitySourceGrad + os_)
+        if on is not None and b.viscosityGrad is not None:
+            b.setViscosityGrad(b.viscosityGrad + on)
+        for f in range(2 * D):
+            if of[f] is not None:
+                b.boundaries[f].setVelocityGrad(b.boundaries[f].velocityGrad + of[f])
+    nu = nu.reshape(domain.viscosity.shape).to(domain.viscosity.device, domain.viscosity.dtype)
+    if domain.viscosityGrad is not None and domain.viscosityGrad.shape == nu.shape:
+        domain.viscosityGrad = domain.viscosityGrad + nu
+    else:
+        domain.viscosityGrad = nu
+    domain.UpdateDomainData()
+
+
+def SetupAdvectionMatrixGrad(domain, timeStep, nonOrthoFlags, forPassiveScalar=False, passiveScalarChannel=0):
+    """Gradient of SetupAdvectionMatrix (extensions/PISO_multiblock_cuda_kernel.cu:3869-4077): AGrad and CGrad to the
+    velocity, viscosity and boundary velocity gradients."""
+    from .PISOtorch_diff import _Grads, _p, _stream
+    if forPassiveScalar:
+        raise NotImplementedError("passive scalar transport is not implemented in pict_b200")
+    _grad_ortho_only(nonOrthoFlags, "SetupAdvectionMatrixGrad")
+    domain._check_ready()
+    dt = _time_step(timeStep, domain)
+    g = _Grads(domain)
+    zD = g.z(g.D * g.N)
+    Ab = _need_grad(domain, "AGrad", g.N).contiguous()
+    check(_lib.load().pict_advection_grad(ctypes.byref(domain._desc), dt, _p(zD), _p(zD), _p(domain.CGrad.coef.contiguous()),
+                                          _p(Ab), _p(g.un), _p(g.nu), _p(g.vb), None, _stream()),
+          "SetupAdvectionMatrixGrad")
+    _add_parameter_grads(domain, g)
+
+
+def SetupAdvectionVelocityGrad(domain, timeStep, nonOrthoFlags, applyPressureGradient=False):
+    """Gradient of SetupAdvectionVelocity (extensions/PISO_multiblock_cuda_kernel.cu:4388-4478): velocityRHSGrad to the
+    velocity, source, viscosity and boundary velocity gradients."""
+    from .PISOtorch_diff import _Grads, _p, _stream
+    _grad_ortho_only(nonOrthoFlags, "SetupAdvectionVelocityGrad")
+    if applyPressureGradient:
+        raise NotImplementedError("SetupAdvectionVelocityGrad: no gradient with applyPressureGradient")
+    domain._check_ready()
+    dt = _time_step(timeStep, domain)
+    g = _Grads(domain)
+    zD = g.z(g.D * g.N)
+    rb = _need_grad(domain, "velocityRHSGrad", g.D * g.N).contiguous()
+    check(_lib.load().pict_advection_grad(ctypes.byref(domain._desc), dt, _p(zD), _p(rb), _p(g.z((2 * g.D + 1) * g.N)),
+                                          _p(g.z(g.N)), _p(g.un), _p(g.nu), _p(g.vb), _p(g.src), _stream()),
+          "SetupAdvectionVelocityGrad")
+    _add_parameter_grads(domain, g)
+
+
+def SetupPressureMatrixGrad(domain, timeStep, nonOrthoMode=0, useFaceTransform=False):
+    """Gradient of SetupPressureMatrix (extensions/PISO_multiblock_cuda_kernel.cu:4967-5117): PGrad to AGrad."""
+    from .PISOtorch_diff import _p, _stream
+    _grad_ortho_only(nonOrthoMode, "SetupPressureMatrixGrad")
+    if useFaceTransform:
+        raise NotImplementedError("face-transform pressure assembly is not implemented in pict_b200")
+    domain._check_ready()
+    _time_step(timeStep, domain)
+    Ab = _need_grad(domain, "AGrad", domain.getTotalSize())
+    add = torch.zeros_like(Ab)
+    check(_lib.load().pict_pressure_matrix_grad(ctypes.byref(domain._desc), _p(domain.A), _p(domain.PGrad.coef.contiguous()),
+                                                _p(add), _stream()), "SetupPressureMatrixGrad")
+    domain.AGrad = Ab + add
+
+
+def _pressure_rhs_grad(domain, dt, with_rhs, what):
+    from .PISOtorch_diff import _Grads, _p, _stream
+    lib = _lib.load()
+    g = _Grads(domain)
+    N, D = g.N, g.D
+    desc = ctypes.byref(domain._desc)
+    st = _stream()
+    hb = _need_grad(domain, "pressureRHSGrad", D * N).detach().clone().contiguous()
+    div_grad = _need_grad(domain, "pressureRHSdivGrad", N).contiguous()
+    check(lib.pict_divergence_grad(desc, _p(div_grad), _p(hb), _p(g.vb), st), what)
+    if not with_rhs:
+        domain.pressureRHSGrad = hb
+        _add_parameter_grads(domain, g)
+        return
+    Ab, Cb, Ub = g.z(N), g.z((2 * D + 1) * N), g.z(D * N)
+    zN = g.z(N)
+    check(lib.pict_pressure_rhs_grad(desc, dt, _p(hb), _p(domain.pressureRHS), _p(domain.A), _p(domain.C.coef),
+                                     _p(domain.velocityResult), _p(zN), _p(zN), _p(Ab), _p(Cb), _p(Ub), _p(g.un),
+                                     _p(g.src), _p(g.nu), _p(g.vb), st), what)
+    domain.AGrad = _need_grad(domain, "AGrad", N) + Ab
+    domain.CGrad.setCoef(domain.CGrad.coef + Cb.reshape(domain.CGrad.coef.shape))
+    domain.velocityResultGrad = _need_grad(domain, "velocityResultGrad", D * N) + Ub
+    _add_parameter_grads(domain, g)
+
+
+def SetupPressureRHSGrad(domain, timeStep, nonOrthoMode=0, useFaceTransform=False, timeStepNorm=False):
+    """Gradient of SetupPressureRHS (h = H/A and its divergence, extensions/PISO_multiblock_cuda_kernel.cu:5243-5453):
+    pressureRHSGrad and pressureRHSdivGrad to AGrad, CGrad, velocityResultGrad and the velocity, source,
+    viscosity and boundary velocity gradients."""
+    _grad_ortho_only(nonOrthoMode, "SetupPressureRHSGrad")
+    if useFaceTransform or timeStepNorm:
+        raise NotImplementedError("SetupPressureRHSGrad: no gradient with face transforms / timeStepNorm")
+    domain._check_ready()
+    _pressure_rhs_grad(domain, _time_step(timeStep, domain), True, "SetupPressureRHSGrad")
+
+
+def SetupPressureRHSdivGrad(domain, timeStep, nonOrthoMode=0, useFaceTransform=False, timeStepNorm=False):
+    """Gradient of SetupPressureRHSdiv (extensions/PISO_multiblock_cuda_kernel.cu:5423-5453): pressureRHSdivGrad to
+    pressureRHSGrad and the boundary velocity gradients."""
+    _grad_ortho_only(nonOrthoMode, "SetupPressureRHSdivGrad")
+    if useFaceTransform or timeStepNorm:
+        raise NotImplementedError("SetupPressureRHSdivGrad: no gradient with face transforms / timeStepNorm")
+    domain._check_ready()
+    _pressure_rhs_grad(domain, _time_step(timeStep, domain), False, "SetupPressureRHSdivGrad")
+
+
+def SetupPressureCorrectionGrad(domain, timeStep, nonOrthoMode=0, useFaceTransform=False, timeStepNorm=False):
+    """Gradient of SetupPressureCorrection: SetupPressureMatrixGrad followed by SetupPressureRHSGrad."""
+    SetupPressureMatrixGrad(domain, timeStep, nonOrthoMode, useFaceTransform)
+    SetupPressureRHSGrad(domain, timeStep, nonOrthoMode, useFaceTransform, timeStepNorm)
+
+
+def CorrectVelocityGrad(domain, timeStep, timeStepNorm=False):
+    """Gradient of CorrectVelocity (FD version, extensions/PISO_multiblock_cuda_kernel.cu:6251-6293): velocityResultGrad
+    to pressureRHSGrad and AGrad (assigned, as in the reference) and the blocks' pressure gradients (added)."""
+    from .PISOtorch_diff import _p, _stream
+    if timeStepNorm:
+        raise NotImplementedError("CorrectVelocityGrad: no gradient with timeStepNorm")
+    domain._check_ready()
+    _time_step(timeStep, domain)
+    lib = _lib.load()
+    N, D = domain.getTotalSize(), domain.getSpatialDims()
+    z = lambda n: torch.zeros(n, dtype=domain.getDtype(), device=domain.getDevice())
+    ug = _need_grad(domain, "velocityResultGrad", D * N).contiguous()
+    p_glob = z(N)
+    check(lib.pict_copy_field(ctypes.byref(domain._desc), 1, 0, _p(p_glob), 0, _stream()), "CorrectVelocityGrad")
+    Ab, pb, hb = z(N), z(N), z(D * N)
+    check(lib.pict_correct_velocity_grad(ctypes.byref(domain._desc), _p(domain.A), _p(p_glob), _p(ug), _p(Ab), _p(pb),
+                                         _p(hb), _stream()), "CorrectVelocityGrad")
+    domain.AGrad = Ab
+    domain.pressureRHSGrad = hb
+    for b in domain.getBlocks():
+        if b.pressureGrad is None or b.pressureGrad.shape != b.pressure.shape:
+            b.setPressureGrad(torch.zeros_like(b.pressure))
+    domain.UpdateDomainData()
+    check(lib.pict_copy_field(ctypes.byref(domain._desc), 4, 1, _p(pb), 1, _stream()), "CorrectVelocityGrad")
+
+
+def _copy_grad(domain, which, to_blocks, name, n):
+    from .PISOtorch_diff import _p, _stream
+    domain._check_ready()
+    if to_blocks:
+        vec = _need_grad(domain, name, n).contiguous()
+        for b in domain.getBlocks():
+            if which == 3 and (b.velocityGrad is None or b.velocityGrad.shape != b.velocity.shape):
+                b.setVelocityGrad(torch.zeros_like(b.velocity))
+        domain.UpdateDomainData()
+        check(_lib.load().pict_copy_field(ctypes.byref(domain._desc), which, 1, _p(vec), 0, _stream()), name)
+    else:
+        out = torch.zeros(n, dtype=domain.getDtype(), device=domain.getDevice())
+        check(_lib.load().pict_copy_field(ctypes.byref(domain._desc), which, 0, _p(out), 0, _stream()), name)
+        setattr(domain, name, out)
+
+
+def CopyVelocityResultGradFromBlocks(domain):
+    """velocityResultGrad = the blocks' velocity gradients (gradient of CopyVelocityResultToBlocks)."""
+    _copy_grad(domain, 3, False, "velocityResultGrad", domain.getTotalSize() * domain.getSpatialDims())
+
+
+def CopyVelocityResultGradToBlocks(domain):
+    """The blocks' velocity gradients = velocityResultGrad (gradient of CopyVelocityResultFromBlocks)."""
+    _copy_grad(domain, 3, True, "velocityResultGrad", domain.getTotalSize() * domain.getSpatialDims())
+
+
+def CopyPressureResultGradFromBlocks(domain):
+    """pressureResultGrad = the blocks' pressure gradients (gradient of CopyPressureResultToBlocks)."""
+    _copy_grad(domain, 4, False, "pressureResultGrad", domain.getTotalSize())
+
+
+def CopyScalarResultGradFromBlocks(domain):
+    raise NotImplementedError("passive scalar transport is not implemented in pict_b200")
+
+
+def CopyScalarResultGradToBlocks(domain):
+    raise NotImplementedError("passive scalar transport is not implemented in pict_b200")
+
+
+def SetupAdvectionScalarGrad(domain, timeStep, nonOrthoFlags):
     raise NotImplementedError("passive scalar transport is not implemented in pict_b200")
 
 
