@@ -324,6 +324,16 @@ pict_status_t pict_stencil_outer_product(const pict_domain_t* dom, const void* a
 /* SetupPressureMatrixGrad (PISOtorch_diff.py:897-965): A_grad += d(P : P_grad)/dA. */
 pict_status_t pict_pressure_matrix_grad(const pict_domain_t* dom, const void* A, const void* P_grad, void* A_grad,
                                         void* stream);
+/* Gradients of the non-orthogonal terms (nonOrthoFlags; the non-orthogonal parts of the reference's *_GRAD
+ * kernels, extensions/PISO_multiblock_cuda_kernel.cu:1992-2098, 3212-3392).  what 0: advection matrix, out_bar =
+ * C_grad [K][N] with A_bar = A_grad [N] -> coef_bar = viscosity gradient [N] (per cell); 1: velocity RHS,
+ * out_bar = velocityRHS_grad [D][N] -> data_bar = velocityResult gradient [D][N], coef_bar = viscosity
+ * gradient [N], boundary_velocity_grad [2D][D][N]; 2: pressure matrix, out_bar = P_grad [K][N] -> coef_bar
+ * = A gradient [N]; 3: pressure RHS divergence, out_bar = pressureRHSdiv_grad [N] -> data_bar =
+ * pressureResult gradient [N], coef_bar = A gradient [N].  Accumulates (atomics). */
+pict_status_t pict_nonortho_grad(const pict_domain_t* dom, int32_t flags, int32_t what, const void* out_bar,
+                                 const void* A_bar, void* data_bar, void* coef_bar, void* boundary_velocity_grad,
+                                 void* stream);
 /* Copy between a global [ncomp][N] vector and a per-block field (0 velocity, 1 pressure, 2 source,
  * 3 velocity_grad, 4 pressure_grad, 5 source_grad); accumulate=1 adds instead of overwriting. */
 pict_status_t pict_copy_field(const pict_domain_t* dom, int32_t which, int32_t to_blocks, void* global_vec,

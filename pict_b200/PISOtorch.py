@@ -1869,8 +1869,10 @@ def CopyScalarResultFromBlocks(domain):
 # the global gradient vectors), except where the reference assigns: CorrectVelocityGrad writes
 # AGrad and pressureRHSGrad, the Copy*GradFromBlocks / ToBlocks operators copy.  As with the
 # reference, call the matching Create*Grad first for a fresh gradient.  Computed by the same adjoint
-# kernels as the autograd Functions of pict_b200.PISOtorch_diff; the gradients of the non-orthogonal
-# terms and of passive scalars are not implemented.
+# kernels as the autograd Functions of pict_b200.PISOtorch_diff; with nonOrthoFlags the gradients of
+# the non-orthogonal terms are added as the reference adds them: the explicit right-hand-side terms
+# to velocityResultGrad / pressureResultGrad, the coefficients to the viscosity gradients / AGrad.
+# Passive scalars are not implemented.
 # ------------------------------------------------------------------------------------------------
 
 def _need_grad(domain, name, n):
@@ -1880,9 +1882,13 @@ def _need_grad(domain, name, n):
     return getattr(domain, name)
 
 
-def _grad_ortho_only(flags, what):
-    if int(flags) != 0:
-        raise NotImplementedError("%s: gradients of the non-orthogonal terms are not implemented in pict_b200" % what)
+def _nonortho_grad(domain, flags, what, out_bar, A_bar=None, data_bar=None, coef_bar=None, vb=None, name=""):
+    """Add the gradient of the non-orthogonal terms of one operator (pict_nonortho_grad)."""
+    from .PISOtorch_diff import _p, _stream
+    if flags == 0:
+        return
+    check(_lib.load().pict_nonortho_grad(ctypes.byref(domain._desc), flags, what, _p(out_bar), _p(A_bar), _p(data_bar),
+                                         _p(coef_bar), _p(vb), _stream()), name)
 
 
 def _add_parameter_grads(domain, g):
@@ -1925,23 +1931,26 @@ def SetupAdvectionMatrixGrad(domain, timeStep, nonOrthoFlags, forPassiveScalar=F
     from .PISOtorch_diff import _Grads, _p, _stream
     if forPassiveScalar:
         raise NotImplementedError("passive scalar transport is not implemented in pict_b200")
-    _grad_ortho_only(nonOrthoFlags, "SetupAdvectionMatrixGrad")
+    flags = _non_ortho(nonOrthoFlags)
     domain._check_ready()
     dt = _time_step(timeStep, domain)
     g = _Grads(domain)
     zD = g.z(g.D * g.N)
     Ab = _need_grad(domain, "AGrad", g.N).contiguous()
-    check(_lib.load().pict_advection_grad(ctypes.byref(domain._desc), dt, _p(zD), _p(zD), _p(domain.CGrad.coef.contiguous()),
+    Cb = domain.CGrad.coef.contiguous()
+    check(_lib.load().pict_advection_grad(ctypes.byref(domain._desc), dt, _p(zD), _p(zD), _p(Cb),
                                           _p(Ab), _p(g.un), _p(g.nu), _p(g.vb), None, _stream()),
           "SetupAdvectionMatrixGrad")
+    _nonortho_grad(domain, flags, 0, Cb, A_bar=Ab, coef_bar=g.nu, name="SetupAdvectionMatrixGrad")
     _add_parameter_grads(domain, g)
 
 
 def SetupAdvectionVelocityGrad(domain, timeStep, nonOrthoFlags, applyPressureGradient=False):
     """Gradient of SetupAdvectionVelocity (extensions/PISO_multiblock_cuda_kernel.cu:4388-4478): velocityRHSGrad to the
-    velocity, source, viscosity and boundary velocity gradients."""
+    velocity, source, viscosity and boundary velocity gradients, and with non-orthogonal RHS flags to
+    velocityResultGrad (the explicit terms read domain.velocityResult)."""
     from .PISOtorch_diff import _Grads, _p, _stream
-    _grad_ortho_only(nonOrthoFlags, "SetupAdvectionVelocityGrad")
+    flags = _non_ortho(nonOrthoFlags)
     if applyPressureGradient:
         raise NotImplementedError("SetupAdvectionVelocityGrad: no gradient with applyPressureGradient")
     domain._check_ready()
@@ -1952,25 +1961,30 @@ def SetupAdvectionVelocityGrad(domain, timeStep, nonOrthoFlags, applyPressureGra
     check(_lib.load().pict_advection_grad(ctypes.byref(domain._desc), dt, _p(zD), _p(rb), _p(g.z((2 * g.D + 1) * g.N)),
                                           _p(g.z(g.N)), _p(g.un), _p(g.nu), _p(g.vb), _p(g.src), _stream()),
           "SetupAdvectionVelocityGrad")
+    if flags & (NON_ORTHO_DIRECT_RHS | NON_ORTHO_DIAGONAL_RHS):
+        ub = _need_grad(domain, "velocityResultGrad", g.D * g.N)
+        _nonortho_grad(domain, flags, 1, rb, data_bar=ub, coef_bar=g.nu, vb=g.vb, name="SetupAdvectionVelocityGrad")
     _add_parameter_grads(domain, g)
 
 
 def SetupPressureMatrixGrad(domain, timeStep, nonOrthoMode=0, useFaceTransform=False):
     """Gradient of SetupPressureMatrix (extensions/PISO_multiblock_cuda_kernel.cu:4967-5117): PGrad to AGrad."""
     from .PISOtorch_diff import _p, _stream
-    _grad_ortho_only(nonOrthoMode, "SetupPressureMatrixGrad")
+    flags = _non_ortho(nonOrthoMode)
     if useFaceTransform:
         raise NotImplementedError("face-transform pressure assembly is not implemented in pict_b200")
     domain._check_ready()
     _time_step(timeStep, domain)
     Ab = _need_grad(domain, "AGrad", domain.getTotalSize())
     add = torch.zeros_like(Ab)
-    check(_lib.load().pict_pressure_matrix_grad(ctypes.byref(domain._desc), _p(domain.A), _p(domain.PGrad.coef.contiguous()),
+    Pb = domain.PGrad.coef.contiguous()
+    check(_lib.load().pict_pressure_matrix_grad(ctypes.byref(domain._desc), _p(domain.A), _p(Pb),
                                                 _p(add), _stream()), "SetupPressureMatrixGrad")
+    _nonortho_grad(domain, flags, 2, Pb, coef_bar=add, name="SetupPressureMatrixGrad")
     domain.AGrad = Ab + add
 
 
-def _pressure_rhs_grad(domain, dt, with_rhs, what):
+def _pressure_rhs_grad(domain, dt, with_rhs, what, flags=0):
     from .PISOtorch_diff import _Grads, _p, _stream
     lib = _lib.load()
     g = _Grads(domain)
@@ -1979,9 +1993,15 @@ def _pressure_rhs_grad(domain, dt, with_rhs, what):
     st = _stream()
     hb = _need_grad(domain, "pressureRHSGrad", D * N).detach().clone().contiguous()
     div_grad = _need_grad(domain, "pressureRHSdivGrad", N).contiguous()
+    if flags & (NON_ORTHO_DIRECT_RHS | NON_ORTHO_DIAGONAL_RHS):
+        # explicit terms of pressureResult (k_pressureRHSaddNonOrthoComponents_GRAD)
+        pb = _need_grad(domain, "pressureResultGrad", N)
+        Ab = _need_grad(domain, "AGrad", N)
+        _nonortho_grad(domain, flags, 3, div_grad, data_bar=pb, coef_bar=Ab, name=what)
     check(lib.pict_divergence_grad(desc, _p(div_grad), _p(hb), _p(g.vb), st), what)
+    # the divergence gradient stays in pressureRHSGrad, as the reference scatters it there in place
+    domain.pressureRHSGrad = hb
     if not with_rhs:
-        domain.pressureRHSGrad = hb
         _add_parameter_grads(domain, g)
         return
     Ab, Cb, Ub = g.z(N), g.z((2 * D + 1) * N), g.z(D * N)
@@ -1999,21 +2019,21 @@ def SetupPressureRHSGrad(domain, timeStep, nonOrthoMode=0, useFaceTransform=Fals
     """Gradient of SetupPressureRHS (h = H/A and its divergence, extensions/PISO_multiblock_cuda_kernel.cu:5243-5453):
     pressureRHSGrad and pressureRHSdivGrad to AGrad, CGrad, velocityResultGrad and the velocity, source,
     viscosity and boundary velocity gradients."""
-    _grad_ortho_only(nonOrthoMode, "SetupPressureRHSGrad")
+    flags = _non_ortho(nonOrthoMode)
     if useFaceTransform or timeStepNorm:
         raise NotImplementedError("SetupPressureRHSGrad: no gradient with face transforms / timeStepNorm")
     domain._check_ready()
-    _pressure_rhs_grad(domain, _time_step(timeStep, domain), True, "SetupPressureRHSGrad")
+    _pressure_rhs_grad(domain, _time_step(timeStep, domain), True, "SetupPressureRHSGrad", flags)
 
 
 def SetupPressureRHSdivGrad(domain, timeStep, nonOrthoMode=0, useFaceTransform=False, timeStepNorm=False):
     """Gradient of SetupPressureRHSdiv (extensions/PISO_multiblock_cuda_kernel.cu:5423-5453): pressureRHSdivGrad to
     pressureRHSGrad and the boundary velocity gradients."""
-    _grad_ortho_only(nonOrthoMode, "SetupPressureRHSdivGrad")
+    flags = _non_ortho(nonOrthoMode)
     if useFaceTransform or timeStepNorm:
         raise NotImplementedError("SetupPressureRHSdivGrad: no gradient with face transforms / timeStepNorm")
     domain._check_ready()
-    _pressure_rhs_grad(domain, _time_step(timeStep, domain), False, "SetupPressureRHSdivGrad")
+    _pressure_rhs_grad(domain, _time_step(timeStep, domain), False, "SetupPressureRHSdivGrad", flags)
 
 
 def SetupPressureCorrectionGrad(domain, timeStep, nonOrthoMode=0, useFaceTransform=False, timeStepNorm=False):

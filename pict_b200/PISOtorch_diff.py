@@ -58,10 +58,17 @@ def _get_solver_tolerance_torch(tol=None, dtype=torch.float32):
 
 
 def check_non_ortho_rhs(non_ortho_flags):
-    if non_ortho_flags:
-        raise NotImplementedError("gradients of the non-orthogonal terms are not implemented in pict_b200 "
-                                  "(the forward operators of pict_b200.PISOtorch compute them)")
-    return False
+    """True if the flags add explicit non-orthogonal right-hand-side terms, which read the velocity or
+    pressure result (PISOtorch_diff.py:34-42); those results are then tracked inputs of the operator."""
+    return bool(int(non_ortho_flags) & (PISOtorch.NON_ORTHO_DIRECT_RHS | PISOtorch.NON_ORTHO_DIAGONAL_RHS))
+
+
+def _nonortho_grad(domain, flags, what, out_bar, A_bar=None, data_bar=None, coef_bar=None, vb=None):
+    """Add the gradient of the non-orthogonal terms of one operator (pict_nonortho_grad)."""
+    if int(flags) == 0:
+        return
+    check(_lib.load().pict_nonortho_grad(ctypes.byref(domain._desc), int(flags), what, _p(out_bar), _p(A_bar),
+                                         _p(data_bar), _p(coef_bar), _p(vb), _stream()), "non-orthogonal grad")
 
 
 def _stream():
@@ -304,7 +311,6 @@ def SetupAdvectionMatrix(domain, time_step, non_ortho_flags, forPassiveScalar=Fa
     velocity and viscosity."""
     if forPassiveScalar:
         raise NotImplementedError("passive scalar transport is not implemented in pict_b200")
-    check_non_ortho_rhs(non_ortho_flags)
     keys, tracked = flatten_domain(domain, ["VELOCITY", "BOUNDARY_VELOCITY", "VISCOSITY", "VISCOSITY_BLOCK"])
     dt = _dt(time_step)
 
@@ -331,6 +337,7 @@ def SetupAdvectionMatrix(domain, time_step, non_ortho_flags, forPassiveScalar=Fa
             zD = g.z(g.D * g.N)
             check(_lib.load().pict_advection_grad(ctypes.byref(domain._desc), dt, _p(zD), _p(zD), _p(Cb), _p(Ab),
                                                   _p(g.un), _p(g.nu), _p(g.vb), None, _stream()), "advection grad")
+            _nonortho_grad(domain, non_ortho_flags, 0, Cb, A_bar=Ab, coef_bar=g.nu)
             return tuple(_apply_exclusions("SetupAdvectionMatrix", keys, g.to_inputs(keys)))
 
     return SetupAdvectionMatrixFunction.apply(*tracked)
@@ -345,10 +352,10 @@ _EXCLUDED_GRADIENTS["SetupAdvectionVelocity"] = (set(), set())
 
 def SetupAdvectionVelocity(domain, time_step, non_ortho_flags, apply_pressure_gradient=False):
     """velocityRHS (PISOtorch_diff.py:531-613); differentiable w.r.t. velocity, source, boundary velocity
-    and viscosity."""
-    check_non_ortho_rhs(non_ortho_flags)
+    and viscosity, and with non-orthogonal RHS flags w.r.t. the velocity result."""
+    is_non_ortho = check_non_ortho_rhs(non_ortho_flags)
     keys, tracked = flatten_domain(domain, ["VELOCITY", "VELOCITY_SOURCE", "BOUNDARY_VELOCITY", "VISCOSITY",
-                                            "VISCOSITY_BLOCK"])
+                                            "VISCOSITY_BLOCK"] + (["VELOCITY_RESULT"] if is_non_ortho else []))
     dt = _dt(time_step)
 
     class SetupAdvectionVelocityFunction(torch.autograd.Function):
@@ -373,29 +380,45 @@ def SetupAdvectionVelocity(domain, time_step, non_ortho_flags, apply_pressure_gr
             zD = g.z(g.D * g.N)
             zC = g.z((2 * g.D + 1) * g.N)
             zA = g.z(g.N)
-            check(_lib.load().pict_advection_grad(ctypes.byref(domain._desc), dt, _p(zD), _p(grad_rhs.contiguous()),
+            rb = grad_rhs.contiguous()
+            check(_lib.load().pict_advection_grad(ctypes.byref(domain._desc), dt, _p(zD), _p(rb),
                                                   _p(zC), _p(zA), _p(g.un), _p(g.nu), _p(g.vb), _p(g.src), _stream()),
                   "advection rhs grad")
-            return tuple(_apply_exclusions("SetupAdvectionVelocity", keys, g.to_inputs(keys)))
+            Ub = g.z(g.D * g.N)
+            if is_non_ortho:
+                _nonortho_grad(domain, non_ortho_flags, 1, rb, data_bar=Ub, coef_bar=g.nu, vb=g.vb)
+            grads = g.to_inputs(keys)
+            for i, key in enumerate(keys):
+                if key[0] == "VELOCITY_RESULT":
+                    grads[i] = Ub
+            return tuple(_apply_exclusions("SetupAdvectionVelocity", keys, grads))
 
     return SetupAdvectionVelocityFunction.apply(*tracked)
 
 
-def _pressure_rhs_backward(domain, dt, keys, h_grad, div_grad, P_grad, want_A, want_C, want_U):
-    """Shared backward of SetupPressureCorrection / Matrix / RHS / RHSdiv."""
+def _pressure_rhs_backward(domain, dt, keys, h_grad, div_grad, P_grad, want_A, want_C, want_U, flags=0):
+    """Shared backward of SetupPressureCorrection / Matrix / RHS / RHSdiv.  With non-orthogonal flags the
+    matrix terms add to the A gradient and the explicit RHS terms (read from the pressure result saved by
+    the forward pass) to the pressure result and A gradients."""
     lib = _lib.load()
     g = _Grads(domain)
     N, D = g.N, g.D
     desc = ctypes.byref(domain._desc)
     s = _stream()
     hb = g.z(D * N) if h_grad is None else h_grad.detach().clone().contiguous()
-    if div_grad is not None:
-        check(lib.pict_divergence_grad(desc, _p(div_grad.contiguous()), _p(hb), _p(g.vb), s), "divergence grad")
     Ab = g.z(N)
     Cb = g.z((2 * D + 1) * N)
     Ub = g.z(D * N)
+    Pr = g.z(N)
+    if div_grad is not None:
+        db = div_grad.contiguous()
+        check(lib.pict_divergence_grad(desc, _p(db), _p(hb), _p(g.vb), s), "divergence grad")
+        if check_non_ortho_rhs(flags):
+            _nonortho_grad(domain, flags, 3, db, data_bar=Pr, coef_bar=Ab)
     if P_grad is not None:
-        check(lib.pict_pressure_matrix_grad(desc, _p(domain.A), _p(P_grad.contiguous()), _p(Ab), s), "pressure matrix grad")
+        Pb = P_grad.contiguous()
+        check(lib.pict_pressure_matrix_grad(desc, _p(domain.A), _p(Pb), _p(Ab), s), "pressure matrix grad")
+        _nonortho_grad(domain, flags, 2, Pb, coef_bar=Ab)
     if h_grad is not None or div_grad is not None:
         zN = g.z(N)
         check(lib.pict_pressure_rhs_grad(desc, dt, _p(hb), _p(domain.pressureRHS), _p(domain.A), _p(domain.C.coef),
@@ -411,6 +434,8 @@ def _pressure_rhs_backward(domain, dt, keys, h_grad, div_grad, P_grad, want_A, w
             grads[i] = Ub
         elif key[0] == "PRESSURE_RHS":
             grads[i] = hb
+        elif key[0] == "PRESSURE_RESULT":
+            grads[i] = Pr
     return grads
 
 
@@ -419,9 +444,10 @@ _EXCLUDED_GRADIENTS["SetupPressureCorrection"] = (set(), set())
 
 def SetupPressureCorrection(domain, time_step, non_ortho_flags, use_face_transform=False, timeStepNorm=False):
     """P, pressureRHS (H/A) and pressureRHSdiv (PISOtorch_diff.py:802-895)."""
-    check_non_ortho_rhs(non_ortho_flags)
+    is_non_ortho = check_non_ortho_rhs(non_ortho_flags)
     keys, tracked = flatten_domain(domain, ["VELOCITY", "VELOCITY_SOURCE", "VELOCITY_RESULT", "BOUNDARY_VELOCITY",
-                                            "VISCOSITY", "VISCOSITY_BLOCK", "A", "C"])
+                                            "VISCOSITY", "VISCOSITY_BLOCK", "A", "C"]
+                                   + (["PRESSURE_RESULT"] if is_non_ortho else []))
     dt = _dt(time_step)
 
     class SetupPressureCorrectionFunction(torch.autograd.Function):
@@ -446,7 +472,8 @@ def SetupPressureCorrection(domain, time_step, non_ortho_flags, use_face_transfo
             set_domain_tensors_from_flat(domain, keys, ctx.saved)
             domain.setPressureRHS(ctx.h)
             domain.UpdateDomainData()
-            grads = _pressure_rhs_backward(domain, dt, keys, rhs_grad, div_grad, P_grad, True, True, True)
+            grads = _pressure_rhs_backward(domain, dt, keys, rhs_grad, div_grad, P_grad, True, True, True,
+                                           non_ortho_flags)
             return tuple(_apply_exclusions("SetupPressureCorrection", keys, grads))
 
     return SetupPressureCorrectionFunction.apply(*tracked)
@@ -457,7 +484,6 @@ _EXCLUDED_GRADIENTS["SetupPressureMatrix"] = (set(), set())
 
 def SetupPressureMatrix(domain, time_step, non_ortho_flags, use_face_transform=False):
     """P from A (PISOtorch_diff.py:897-965)."""
-    check_non_ortho_rhs(non_ortho_flags)
     keys, tracked = flatten_domain(domain, ["A"])
     dt = _dt(time_step)
 
@@ -475,7 +501,7 @@ def SetupPressureMatrix(domain, time_step, non_ortho_flags, use_face_transform=F
         def backward(ctx, P_grad):
             set_domain_tensors_from_flat(domain, keys, ctx.saved)
             domain.UpdateDomainData()
-            grads = _pressure_rhs_backward(domain, dt, keys, None, None, P_grad, True, False, False)
+            grads = _pressure_rhs_backward(domain, dt, keys, None, None, P_grad, True, False, False, non_ortho_flags)
             return tuple(_apply_exclusions("SetupPressureMatrix", keys, grads))
 
     return SetupPressureMatrixFunction.apply(*tracked)
@@ -486,9 +512,10 @@ _EXCLUDED_GRADIENTS["SetupPressureRHS"] = (set(), set())
 
 def SetupPressureRHS(domain, time_step, non_ortho_flags, use_face_transform=False, timeStepNorm=False):
     """pressureRHS (H/A) and pressureRHSdiv (PISOtorch_diff.py:967-1065)."""
-    check_non_ortho_rhs(non_ortho_flags)
+    is_non_ortho = check_non_ortho_rhs(non_ortho_flags)
     keys, tracked = flatten_domain(domain, ["VELOCITY", "VELOCITY_SOURCE", "VELOCITY_RESULT", "BOUNDARY_VELOCITY",
-                                            "VISCOSITY", "VISCOSITY_BLOCK", "A", "C"])
+                                            "VISCOSITY", "VISCOSITY_BLOCK", "A", "C"]
+                                   + (["PRESSURE_RESULT"] if is_non_ortho else []))
     dt = _dt(time_step)
 
     class SetupPressureRHSFunction(torch.autograd.Function):
@@ -510,7 +537,8 @@ def SetupPressureRHS(domain, time_step, non_ortho_flags, use_face_transform=Fals
             set_domain_tensors_from_flat(domain, keys, ctx.saved)
             domain.setPressureRHS(ctx.h)
             domain.UpdateDomainData()
-            grads = _pressure_rhs_backward(domain, dt, keys, rhs_grad, div_grad, None, True, True, True)
+            grads = _pressure_rhs_backward(domain, dt, keys, rhs_grad, div_grad, None, True, True, True,
+                                           non_ortho_flags)
             return tuple(_apply_exclusions("SetupPressureRHS", keys, grads))
 
     return SetupPressureRHSFunction.apply(*tracked)
@@ -520,9 +548,11 @@ _EXCLUDED_GRADIENTS["SetupPressureRHSdiv"] = (set(), set())
 
 
 def SetupPressureRHSdiv(domain, time_step, non_ortho_flags, use_face_transform=False, timeStepNorm=False):
-    """pressureRHSdiv from pressureRHS (PISOtorch_diff.py:1067-1158)."""
-    check_non_ortho_rhs(non_ortho_flags)
-    keys, tracked = flatten_domain(domain, ["PRESSURE_RHS", "BOUNDARY_VELOCITY"])
+    """pressureRHSdiv from pressureRHS (PISOtorch_diff.py:1067-1158); with non-orthogonal RHS flags also
+    from the pressure result and A."""
+    is_non_ortho = check_non_ortho_rhs(non_ortho_flags)
+    keys, tracked = flatten_domain(domain, ["PRESSURE_RHS", "BOUNDARY_VELOCITY"]
+                                   + (["PRESSURE_RESULT", "A"] if is_non_ortho else []))
     dt = _dt(time_step)
 
     class SetupPressureRHSdivFunction(torch.autograd.Function):
@@ -543,12 +573,20 @@ def SetupPressureRHSdiv(domain, time_step, non_ortho_flags, use_face_transform=F
             domain.UpdateDomainData()
             g = _Grads(domain)
             hb = g.z(g.D * g.N)
-            check(_lib.load().pict_divergence_grad(ctypes.byref(domain._desc), _p(div_grad.contiguous()), _p(hb),
+            db = div_grad.contiguous()
+            check(_lib.load().pict_divergence_grad(ctypes.byref(domain._desc), _p(db), _p(hb),
                                                    _p(g.vb), _stream()), "divergence grad")
+            Pr, Ab = g.z(g.N), g.z(g.N)
+            if is_non_ortho:
+                _nonortho_grad(domain, non_ortho_flags, 3, db, data_bar=Pr, coef_bar=Ab)
             grads = g.to_inputs(keys)
             for i, key in enumerate(keys):
                 if key[0] == "PRESSURE_RHS":
                     grads[i] = hb
+                elif key[0] == "PRESSURE_RESULT":
+                    grads[i] = Pr
+                elif key[0] == "A":
+                    grads[i] = Ab
             return tuple(_apply_exclusions("SetupPressureRHSdiv", keys, grads))
 
     return SetupPressureRHSdivFunction.apply(*tracked)

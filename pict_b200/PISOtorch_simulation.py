@@ -373,8 +373,9 @@ class Simulation:
         return self._ortho_flags
 
     def _check_non_ortho(self):
-        if self._non_ortho_flags() and self.differentiable:
-            raise NotImplementedError("gradients of the non-orthogonal terms are not implemented in pict_b200")
+        """The non-orthogonal branch runs through the operators of the backend (PISOtorch_diff when
+        differentiable, whose gradient operators include the non-orthogonal terms); nothing to reject."""
+        return self._non_ortho_flags()
 
     def _get_stepper(self):
         key = (id(self.domain), self.corrector_steps, self.advection_tol, self.pressure_tol,

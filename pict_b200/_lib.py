@@ -184,6 +184,7 @@ SIGNATURES = {
     "pict_copy_field": (c_i32, [_PD, c_i32, c_i32, c_vp, c_i32, c_vp]),
     "pict_stencil_outer_product": (c_i32, [_PD, c_vp, c_vp, c_i32, c_vp, ctypes.c_double, c_vp]),
     "pict_pressure_matrix_grad": (c_i32, [_PD, c_vp, c_vp, c_vp, c_vp]),
+    "pict_nonortho_grad": (c_i32, [_PD, c_i32, c_i32] + [c_vp] * 6),
     "pict_csr_row_ptr": (c_i32, [_PD, c_vp, c_vp]),
     "pict_stencil_to_csr": (c_i32, [_PD, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "pict_csr_to_stencil": (c_i32, [_PD, c_vp, c_vp, c_vp, c_vp, c_vp]),

@@ -93,12 +93,23 @@ struct Corner {
     bool neumann;  // boundary type of that fixed boundary
 };
 
-// getCornerValue (extensions/PISO_multiblock_cuda_kernel.cu:2742-2860) without the centre cell, depth 2:
+// What a corner value reads, in the order of getCornerValue (extensions/PISO_multiblock_cuda_kernel.cu:2742-2860)
+// without the centre cell, depth 2: the data cells summed (value = sum / cells), or, when the walk hits a
+// fixed face (cells == 0), the one or two boundary entries averaged.
+struct CornerWalk {
+    int cells;
+    int nvis;
+    int vb[4];
+    int vp[4][3];
+    int fb, ff, nfp;
+    int fp[2][3];
+};
+
 // walk around the corner between faces dir1 and dir2 in both directions until the walks meet
-template <typename T, int D, int KIND>
-__device__ Corner<T> corner_value(const pict_domain_t& dom, int b0, const int* p0, int dir1, int dir2, bool incl1,
-                                  int comp, const T* data) {
-    T acc = T(0);
+template <int D>
+__device__ void corner_walk(const pict_domain_t& dom, int b0, const int* p0, int dir1, int dir2, bool incl1,
+                            CornerWalk& w) {
+    w.nvis = 0;
     int n = 1;
     int wd1[2] = {dir1, dir2}, wd2[2] = {dir2, dir1}, wb[2] = {b0, b0};
     int wp[2][3] = {{p0[0], p0[1], p0[2]}, {p0[0], p0[1], p0[2]}};
@@ -110,18 +121,22 @@ __device__ Corner<T> corner_value(const pict_domain_t& dom, int b0, const int* p
             if (at_face(wp[d], B.size, d1)) {
                 const pict_face_t& F = B.face[d1];
                 if (F.type == PICT_FACE_FIXED) {
-                    Corner<T> r;
-                    r.cells = 0;
-                    r.neumann = (KIND == NK_P);
+                    w.cells = 0;
+                    w.fb = wb[d];
+                    w.ff = d1;
+                    w.fp[0][0] = wp[d][0];
+                    w.fp[0][1] = wp[d][1];
+                    w.fp[0][2] = wp[d][2];
                     if (at_face(wp[d], B.size, d2)) {
-                        r.value = fixed_data<T, D, KIND>(B, d1, wp[d], comp);
+                        w.nfp = 1;
                     } else {
-                        int q[3] = {wp[d][0], wp[d][1], wp[d][2]};
-                        q[d2 >> 1] += (d2 & 1) ? 1 : -1;
-                        r.value = (fixed_data<T, D, KIND>(B, d1, wp[d], comp) + fixed_data<T, D, KIND>(B, d1, q, comp)) *
-                                  T(0.5);
+                        w.nfp = 2;
+                        w.fp[1][0] = wp[d][0];
+                        w.fp[1][1] = wp[d][1];
+                        w.fp[1][2] = wp[d][2];
+                        w.fp[1][d2 >> 1] += (d2 & 1) ? 1 : -1;
                     }
-                    return r;
+                    return;
                 }
                 if (F.type == PICT_FACE_CONNECTED) {
                     int q[3];
@@ -144,19 +159,40 @@ __device__ Corner<T> corner_value(const pict_domain_t& dom, int b0, const int* p
             }
             const int o = d ^ 1;
             if (wb[d] == wb[o] && wp[d][0] == wp[o][0] && wp[d][1] == wp[o][1] && wp[d][2] == wp[o][2]) {
-                Corner<T> r;
-                r.value = acc / T(n);
-                r.cells = n;
-                r.neumann = false;
-                return r;
+                w.cells = n;
+                return;
             }
-            if (depth > 1 || incl1) acc += cell_data<T, KIND>(dom, wb[d], wp[d], data);
+            if (depth > 1 || incl1) {
+                w.vb[w.nvis] = wb[d];
+                w.vp[w.nvis][0] = wp[d][0];
+                w.vp[w.nvis][1] = wp[d][1];
+                w.vp[w.nvis][2] = wp[d][2];
+                ++w.nvis;
+            }
             ++n;
         }
     }
+    w.cells = n;
+}
+
+template <typename T, int D, int KIND>
+__device__ Corner<T> corner_value(const pict_domain_t& dom, int b0, const int* p0, int dir1, int dir2, bool incl1,
+                                  int comp, const T* data) {
+    CornerWalk w;
+    corner_walk<D>(dom, b0, p0, dir1, dir2, incl1, w);
     Corner<T> r;
-    r.value = acc / T(n);
-    r.cells = n;
+    r.cells = w.cells;
+    if (w.cells == 0) {
+        const pict_block_t& B = dom.blocks[w.fb];
+        r.neumann = (KIND == NK_P);
+        r.value = w.nfp == 1 ? fixed_data<T, D, KIND>(B, w.ff, w.fp[0], comp)
+                             : (fixed_data<T, D, KIND>(B, w.ff, w.fp[0], comp) + fixed_data<T, D, KIND>(B, w.ff, w.fp[1], comp)) *
+                                   T(0.5);
+        return r;
+    }
+    T acc = T(0);
+    for (int k = 0; k < w.nvis; ++k) acc += cell_data<T, KIND>(dom, w.vb[k], w.vp[k], data);
+    r.value = acc / T(w.cells);
     r.neumann = false;
     return r;
 }
@@ -397,6 +433,304 @@ __global__ void k_nonortho_rhs(pict_domain_t dom, int flags) {
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// gradients (the non-orthogonal parts of the reference's *_GRAD kernels: scatterNonOrthoLaplaceComponents_GRAD
+// extensions/PISO_multiblock_cuda_kernel.cu:1992-2098, scatterNonOrthoLaplaceRHS_v2_GRAD :3212-3392, and their
+// callers in the matrix and RHS gradient kernels).  The terms are linear in the result fields and in
+// the face coefficients alpha = (a_P r_P + a_N r_N) / 2 with r = viscosity (advection) or 1/A
+// (pressure); each thread recomputes its cell's terms and scatters their adjoints with atomics to
+// the cells they read (the reference scatters with atomics too).
+// ---------------------------------------------------------------------------------------------
+
+// location read by getBlockDataNeighbor: a data cell (true, block nb, position q) or a fixed face (false)
+template <int D>
+__device__ bool neighbor_loc(const pict_domain_t& dom, int b, const int* p, int f, int& nb, int* q) {
+    const pict_block_t& B = dom.blocks[b];
+    const int a = f >> 1;
+    nb = b;
+    q[0] = p[0];
+    q[1] = p[1];
+    q[2] = p[2];
+    if (at_face(p, B.size, f)) {
+        if (B.face[f].type == PICT_FACE_FIXED) return false;
+        if (B.face[f].type == PICT_FACE_CONNECTED) nb = conn_pos<D>(dom, B, f, p, 1, q);
+        else q[a] = (f & 1) ? 0 : B.size[a] - 1;
+    } else {
+        q[a] += (f & 1) ? 1 : -1;
+    }
+    return true;
+}
+
+// location read by getBlockDataNeighborDiagonal
+template <int D>
+__device__ bool diagonal_loc(const pict_domain_t& dom, int b, const int* p, int dir1, int dir2, int& cb, int* q) {
+    const bool first_fixed = face_fixed(dom.blocks[b], dir1);
+    const int dirs[2] = {first_fixed ? dir2 : dir1, first_fixed ? dir1 : dir2};
+    cb = b;
+    q[0] = p[0];
+    q[1] = p[1];
+    q[2] = p[2];
+    for (int s = 0; s < 2; ++s) {
+        const int f = dirs[s];
+        const pict_block_t& B = dom.blocks[cb];
+        const int a = f >> 1;
+        if (at_face(q, B.size, f)) {
+            if (B.face[f].type == PICT_FACE_FIXED) return false;
+            if (B.face[f].type == PICT_FACE_CONNECTED) {
+                int r[3];
+                cb = conn_pos<D>(dom, B, f, q, 1, r);
+                q[0] = r[0];
+                q[1] = r[1];
+                q[2] = r[2];
+            } else {
+                q[a] = (f & 1) ? 0 : B.size[a] - 1;
+            }
+        } else {
+            q[a] += (f & 1) ? 1 : -1;
+        }
+    }
+    return true;
+}
+
+template <typename T>
+__device__ __forceinline__ void atomic_add(T* p, T v) {
+    if (v != T(0)) atomicAdd(p, v);
+}
+
+// matrix terms: M_bar (C_grad / P_grad [K][N]) and, for the advection matrix, A_bar (A = C[0]) to the
+// coefficient adjoint: viscosity (WHICH 0) or A (WHICH 1) per cell
+template <typename T, int D, int WHICH>
+__global__ void k_nonortho_matrix_grad(pict_domain_t dom, int flags, const T* Mbar, const T* Abar, T* coef_bar) {
+    constexpr int K = 2 * D + 1;
+    const int N = dom.num_cells;
+    const T* Ad = reinterpret_cast<const T*>(dom.A);
+    const bool incl_nb = flags & NO_DIRECT_MATRIX, incl_diag = flags & NO_CENTER_MATRIX;
+    const T sgn = WHICH == 0 ? T(-1) : T(1);
+    PICT_CELL_LOOP(i, N) {
+        const int b = dom.cell_block[i];
+        const pict_block_t& B = dom.blocks[b];
+        const int l = i - B.offset;
+        int p[3];
+        unflatten(l, B.size, p);
+        const T* tr = cell_transform<T, D>(B, l);
+        const T raP = WHICH == 0 ? cell_viscosity<T>(dom, B, l) : T(1) / Ad[i];
+        const T scale = WHICH == 0 ? T(1) / tr_det<T, D>(tr) : T(1);
+        T mb[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) mb[k] = Mbar[(size_t)k * N + i] * scale;
+        if (WHICH == 0 && Abar) mb[0] += Abar[i] * scale;
+        T raP_bar = T(0);
+#pragma unroll
+        for (int f = 0; f < 2 * D; ++f) {
+            const int a = f >> 1;
+            const bool fixed = face_fixed(B, f);
+            if (at_face(p, B.size, f) && fixed) continue;
+            if (!((0 < p[a] && p[a] < B.size[a] - 1) || !fixed)) continue;
+            int q[3] = {p[0], p[1], p[2]};
+            int nb = b;
+            if (at_face(p, B.size, f) && B.face[f].type == PICT_FACE_CONNECTED) nb = conn_pos<D>(dom, B, f, p, 0, q);
+            else if (at_face(p, B.size, f)) q[a] = (f & 1) ? 0 : B.size[a] - 1;
+            else q[a] += (f & 1) ? 1 : -1;
+            const pict_block_t& Bn = dom.blocks[nb];
+            const int ln = flat3(Bn.size, q);
+            const int gN = Bn.offset + ln;
+            const T* trn = cell_transform<T, D>(Bn, ln);
+            const T raN = WHICH == 0 ? cell_viscosity<T>(dom, Bn, ln) : T(1) / Ad[gN];
+            const T fs = (f & 1) ? T(1) : T(-1);
+#pragma unroll
+            for (int k = 1; k < D; ++k) {
+                const int t = (a + k) % D;
+                const T aP = lap<T, D>(tr, a, t), aN = lap<T, D>(trn, t, a);
+                // the reference's gradient tests the geometric coefficient, without viscosity or 1/A
+                if ((aP + aN) * T(0.5) == T(0)) continue;
+                T alpha_bar = T(0);  // d L / d alpha
+#pragma unroll
+                for (int tup = 0; tup < 2; ++tup) {
+                    const int tf = 2 * t + tup;
+                    const T ts = tup ? T(1) : T(-1);
+                    CornerWalk w;
+                    corner_walk<D>(dom, b, p, f, tf, false, w);
+                    const bool grad = WHICH == 0 ? false : true;  // fixed velocity faces are Dirichlet
+                    if (w.cells < 1) {
+                        if (grad) {
+                            const T v = fs * ts * T(0.25);
+                            if (incl_diag) alpha_bar += mb[0] * sgn * T(3) * v;
+                            if (incl_nb) alpha_bar += mb[f + 1] * sgn * T(3) * v - mb[(tf ^ 1) + 1] * sgn * v;
+                        }
+                    } else {
+                        const T v = fs * ts / T(w.cells);
+                        if (incl_diag) alpha_bar += mb[0] * sgn * v;
+                        if (incl_nb) alpha_bar += (mb[f + 1] + mb[tf + 1]) * sgn * v;
+                    }
+                }
+                raP_bar += alpha_bar * aP * T(0.5);
+                const T rN_bar = alpha_bar * aN * T(0.5);
+                atomic_add(coef_bar + gN, WHICH == 0 ? rN_bar : rN_bar * (-raN * raN));
+            }
+        }
+        atomic_add(coef_bar + i, WHICH == 0 ? raP_bar : raP_bar * (-raP * raP));
+    }
+}
+
+// RHS terms: out_bar (velocityRHS_grad [D][N], the term entering as -S/det; or pressureRHSdiv_grad [N],
+// entering as +S) to the result field (data_bar), the coefficient adjoint (viscosity / A) and, for the
+// velocity, the fixed boundary velocity (vb_bar [2D][D][N], per adjacent cell)
+template <typename T, int D, int KIND>
+__global__ void k_nonortho_rhs_grad(pict_domain_t dom, int flags, const T* out_bar, T* data_bar, T* coef_bar,
+                                    T* vb_bar) {
+    constexpr int NC = KIND == NK_VEL ? D : 1;
+    const int N = dom.num_cells;
+    const T* Ad = reinterpret_cast<const T*>(dom.A);
+    const T* data = reinterpret_cast<const T*>(KIND == NK_VEL ? dom.velocity_result : dom.pressure_result);
+    const bool incl1 = flags & NO_DIRECT_RHS;
+    PICT_CELL_LOOP(i, N) {
+        const int b = dom.cell_block[i];
+        const pict_block_t& B = dom.blocks[b];
+        const int l = i - B.offset;
+        int p[3];
+        unflatten(l, B.size, p);
+        const T* tr = cell_transform<T, D>(B, l);
+        const T raP = KIND == NK_VEL ? cell_viscosity<T>(dom, B, l) : T(1) / Ad[i];
+        T raP_bar = T(0);
+#pragma unroll 1
+        for (int c = 0; c < NC; ++c) {
+            const T sbar = KIND == NK_VEL ? -out_bar[(size_t)c * N + i] / tr_det<T, D>(tr) : out_bar[i];
+            if (sbar == T(0)) continue;
+            const T* dc = data + (size_t)c * N;
+            T* dcb = data_bar + (size_t)c * N;
+#pragma unroll
+            for (int f = 0; f < 2 * D; ++f) {
+                const int a = f >> 1;
+                const T fs = (f & 1) ? T(1) : T(-1);
+                if (at_face(p, B.size, f) && face_fixed(B, f)) {
+                    if (KIND == NK_P) continue;
+                    const pict_face_t& F = B.face[f];
+                    const int bf = boundary_flat(p, B.size, f);
+                    const T* btr = F.transform ? reinterpret_cast<const T*>(F.transform) + (size_t)bf * TS<D>::value : nullptr;
+#pragma unroll
+                    for (int k = 1; k < D; ++k) {
+                        const int t = (a + k) % D;
+                        const bool tlo = p[t] == 0, thi = p[t] == B.size[t] - 1;
+                        int lo[3] = {p[0], p[1], p[2]}, hi[3] = {p[0], p[1], p[2]};
+                        if (!tlo) lo[t] -= 1;
+                        if (!thi) hi[t] += 1;
+                        const T df = (tlo || thi) ? T(1) : T(0.5);
+                        const T bal = lap<T, D>(btr, t, a);
+                        const T tg = df * (fixed_data<T, D, KIND>(B, f, hi, c) - fixed_data<T, D, KIND>(B, f, lo, c));
+                        raP_bar += sbar * (-fs * bal * tg);
+                        const T wv = sbar * (-fs * bal * raP) * df;
+                        atomic_add(vb_bar + ((size_t)f * D + c) * N + B.offset + flat3(B.size, hi), wv);
+                        atomic_add(vb_bar + ((size_t)f * D + c) * N + B.offset + flat3(B.size, lo), -wv);
+                    }
+                    continue;
+                }
+                int q[3] = {p[0], p[1], p[2]};
+                int nb = b;
+                int map[3] = {0, 2, 4};
+                if (at_face(p, B.size, f) && B.face[f].type == PICT_FACE_CONNECTED) {
+                    nb = conn_pos<D>(dom, B, f, p, 0, q);
+#pragma unroll
+                    for (int k = 0; k < D; ++k) map[k] = conn_dir<D>(B, f, map[k]);
+                } else if (at_face(p, B.size, f)) {
+                    q[a] = (f & 1) ? 0 : B.size[a] - 1;
+                } else {
+                    q[a] += (f & 1) ? 1 : -1;
+                }
+                const pict_block_t& Bn = dom.blocks[nb];
+                const int ln = flat3(Bn.size, q);
+                const int gN = Bn.offset + ln;
+                const T* trn = cell_transform<T, D>(Bn, ln);
+                const T raN = KIND == NK_VEL ? cell_viscosity<T>(dom, Bn, ln) : T(1) / Ad[gN];
+#pragma unroll
+                for (int k = 1; k < D; ++k) {
+                    const int t = (a + k) % D;
+                    const T aN = lap<T, D>(trn, map[t] >> 1, map[a] >> 1);
+                    const T aP = lap<T, D>(tr, a, t);
+                    const T fa = (aP * raP + aN * raN) * T(0.5);
+                    T tg = T(0);
+                    const T tg_bar = sbar * (-fs * fa);
+#pragma unroll
+                    for (int tup = 0; tup < 2; ++tup) {
+                        const int tf = 2 * t + tup;
+                        const T ts = tup ? T(1) : T(-1);
+                        CornerWalk w;
+                        corner_walk<D>(dom, b, p, f, tf, incl1, w);
+                        const bool grad_bound = (w.cells == 0) && (KIND == NK_P);  // fixed velocity faces are Dirichlet
+                        if (grad_bound) {
+                            const int to = tf ^ 1;
+                            int cb;
+                            int r[3];
+                            if (flags & NO_DIRECT_RHS) {
+                                if (neighbor_loc<D>(dom, b, p, f, cb, r)) {
+                                    const int j = dom.blocks[cb].offset + flat3(dom.blocks[cb].size, r);
+                                    tg += ts * dc[j] * T(0.75);
+                                    atomic_add(dcb + j, tg_bar * ts * T(0.75));
+                                }
+                                if (neighbor_loc<D>(dom, b, p, to, cb, r)) {
+                                    const int j = dom.blocks[cb].offset + flat3(dom.blocks[cb].size, r);
+                                    tg -= ts * dc[j] * T(0.25);
+                                    atomic_add(dcb + j, -tg_bar * ts * T(0.25));
+                                }
+                            }
+                            if ((flags & NO_DIAGONAL_RHS) && diagonal_loc<D>(dom, b, p, f, to, cb, r)) {
+                                const int j = dom.blocks[cb].offset + flat3(dom.blocks[cb].size, r);
+                                tg -= ts * dc[j] * T(0.25);
+                                atomic_add(dcb + j, -tg_bar * ts * T(0.25));
+                            }
+                        } else if (w.cells == 0) {
+                            const pict_block_t& Bf = dom.blocks[w.fb];
+                            const T wgt = w.nfp == 1 ? T(1) : T(0.5);
+                            for (int k2 = 0; k2 < w.nfp; ++k2) {
+                                tg += ts * wgt * fixed_data<T, D, KIND>(Bf, w.ff, w.fp[k2], c);
+                                atomic_add(vb_bar + ((size_t)w.ff * D + c) * N + Bf.offset + flat3(Bf.size, w.fp[k2]),
+                                           tg_bar * ts * wgt);
+                            }
+                        } else {
+                            T acc = T(0);
+                            for (int k2 = 0; k2 < w.nvis; ++k2) {
+                                const int j = dom.blocks[w.vb[k2]].offset + flat3(dom.blocks[w.vb[k2]].size, w.vp[k2]);
+                                acc += dc[j];
+                                atomic_add(dcb + j, tg_bar * ts / T(w.cells));
+                            }
+                            tg += ts * (acc / T(w.cells));
+                        }
+                    }
+                    const T fa_bar = sbar * (-fs * tg);
+                    raP_bar += fa_bar * aP * T(0.5);
+                    const T rN_bar = fa_bar * aN * T(0.5);
+                    atomic_add(coef_bar + gN, KIND == NK_VEL ? rN_bar : rN_bar * (-raN * raN));
+                }
+            }
+        }
+        atomic_add(coef_bar + i, KIND == NK_VEL ? raP_bar : raP_bar * (-raP * raP));
+    }
+}
+
+template <typename T, int D>
+static pict_status_t launch_nonortho_grad(const pict_domain_t* dom, int flags, int what, const void* out_bar,
+                                          const void* A_bar, void* data_bar, void* coef_bar, void* vb_bar,
+                                          cudaStream_t st) {
+    const int grid = cell_grid(dom->num_cells, 128);
+    switch (what) {
+        case 0:
+            k_nonortho_matrix_grad<T, D, 0><<<grid, 128, 0, st>>>(*dom, flags, (const T*)out_bar, (const T*)A_bar,
+                                                                  (T*)coef_bar);
+            break;
+        case 1:
+            k_nonortho_rhs_grad<T, D, NK_VEL><<<grid, 128, 0, st>>>(*dom, flags, (const T*)out_bar, (T*)data_bar,
+                                                                    (T*)coef_bar, (T*)vb_bar);
+            break;
+        case 2:
+            k_nonortho_matrix_grad<T, D, 1><<<grid, 128, 0, st>>>(*dom, flags, (const T*)out_bar, nullptr, (T*)coef_bar);
+            break;
+        default:
+            k_nonortho_rhs_grad<T, D, NK_P><<<grid, 128, 0, st>>>(*dom, flags, (const T*)out_bar, (T*)data_bar,
+                                                                  (T*)coef_bar, (T*)vb_bar);
+            break;
+    }
+    return check_launch("nonortho_grad");
+}
+
 template <typename T, int D>
 static pict_status_t launch_nonortho(const pict_domain_t* dom, int flags, int what, cudaStream_t st) {
     const int grid = cell_grid(dom->num_cells, 128);
@@ -425,3 +759,30 @@ pict_status_t nonortho_pass(const pict_domain_t* dom, int32_t flags, int32_t wha
 }
 
 }  // namespace pict
+
+using namespace pict;
+
+extern "C" pict_status_t pict_nonortho_grad(const pict_domain_t* dom, int32_t flags, int32_t what, const void* out_bar,
+                                            const void* A_bar, void* data_bar, void* coef_bar,
+                                            void* boundary_velocity_grad, void* stream) {
+    if (!dom || !out_bar || !coef_bar) return set_error(PICT_ERR_ARG, "nonortho_grad: NULL argument");
+    if (what < 0 || what > 3) return set_error(PICT_ERR_ARG, "nonortho_grad: what must be 0..3");
+    if ((what == 1 || what == 3) && !data_bar) return set_error(PICT_ERR_ARG, "nonortho_grad: data gradient missing");
+    if (what == 1 && !boundary_velocity_grad) return set_error(PICT_ERR_ARG, "nonortho_grad: boundary gradient missing");
+    const bool matrix = (what == 0 || what == 2);
+    if (matrix && !(flags & (NO_DIRECT_MATRIX | NO_CENTER_MATRIX))) return PICT_OK;
+    if (!matrix && !(flags & (NO_DIRECT_RHS | NO_DIAGONAL_RHS))) return PICT_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (dom->dtype == PICT_F32) {
+        if (dom->dims == 2)
+            return launch_nonortho_grad<float, 2>(dom, flags, what, out_bar, A_bar, data_bar, coef_bar, boundary_velocity_grad, st);
+        if (dom->dims == 3)
+            return launch_nonortho_grad<float, 3>(dom, flags, what, out_bar, A_bar, data_bar, coef_bar, boundary_velocity_grad, st);
+    } else if (dom->dtype == PICT_F64) {
+        if (dom->dims == 2)
+            return launch_nonortho_grad<double, 2>(dom, flags, what, out_bar, A_bar, data_bar, coef_bar, boundary_velocity_grad, st);
+        if (dom->dims == 3)
+            return launch_nonortho_grad<double, 3>(dom, flags, what, out_bar, A_bar, data_bar, coef_bar, boundary_velocity_grad, st);
+    }
+    return set_error(PICT_ERR_UNSUPPORTED, "nonortho_grad: unsupported dtype/dims");
+}
