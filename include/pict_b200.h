@@ -78,6 +78,8 @@ typedef struct pict_block {
     void* viscosity_grad;     /* adjoint of block viscosity or NULL */
     void* source_grad;        /* adjoint of velocity source or NULL */
     pict_face_t face[PICT_MAX_BLOCK_FACES];
+    const void* face_transform; /* [D][(z+1)][y+1][x+1][2D^2+1] staggered face transforms or NULL
+                                   (Block::faceTransform; read by the FVM velocity corrector, version 6) */
 } pict_block_t;
 
 /* A (possibly batched) domain.  All pointers are device pointers unless noted.
@@ -193,9 +195,12 @@ pict_status_t pict_setup_pressure_rhs_div(const pict_domain_t* dom, double dt, i
 /* SetupPressureCorrection (extensions/PISOtorch.cpp:541-543): matrix + RHS + div, matrix and RHS fused. */
 pict_status_t pict_setup_pressure_correction(const pict_domain_t* dom, double dt, int32_t non_ortho_flags,
                                              int32_t time_step_norm, void* stream);
-/* CorrectVelocity (extensions/PISOtorch.cpp:553-555 -> extensions/PISO_multiblock_cuda_kernel.cu:6163, version 1 "FD").
- * write_block_velocity=1 additionally stores the result in the blocks' velocity
- * (CopyVelocityResultToBlocks fused). */
+/* CorrectVelocity (extensions/PISOtorch.cpp:553-555 -> extensions/PISO_multiblock_cuda_kernel.cu:6163-6201): version 0/1
+ * finite-difference pressure gradient (PISO_update_velocity :5947-5980), 4 mean of the two face fluxes with
+ * orthogonal metrics (PISO_update_velocity_v4_orthogonal :6053-6160), 5 / 6 finite-volume pressure gradient
+ * with interpolated cell fluxes / staggered face transforms (PISO_update_velocity_PressureFVM :6013-6050,
+ * getPressureGradientFVM :991-1123).  write_block_velocity=1 additionally stores the result in the
+ * blocks' velocity (CopyVelocityResultToBlocks fused). */
 pict_status_t pict_correct_velocity(const pict_domain_t* dom, double dt, int32_t version,
                                     int32_t time_step_norm, int32_t write_block_velocity, void* stream);
 /* Copy{Velocity,Pressure}Result{To,From}Blocks (extensions/PISOtorch.cpp:561-566 -> extensions/PISO_multiblock_cuda_kernel.cu:6543-6733). */

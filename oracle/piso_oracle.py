@@ -714,6 +714,131 @@ def correct_velocity(dom: ODomain, p_blocks: np.ndarray, A: np.ndarray, h: np.nd
     return h - g / A[None]
 
 
+def _cells(dom: ODomain, bi: int):
+    b = dom.blocks[bi]
+    s = list(b.size) + [1] * (3 - dom.dims)
+    for z in range(s[2]):
+        for y in range(s[1]):
+            for x in range(s[0]):
+                yield [x, y, z]
+
+
+def _across(dom: ODomain, bi: int, p, face: int):
+    """The cell across a non-prescribed face (resolveNeighborCell without the second layer): (block, pos,
+    connected boundary or None)."""
+    b = dom.blocks[bi]
+    a = face >> 1
+    if _at_bound(dom, bi, p, face):
+        bnd = b.boundaries[face]
+        if bnd.kind == "connected":
+            ob, q = _conn_pos(dom, bi, face, p, 0)
+            return ob, q, bnd
+        q = list(p)
+        q[a] = 0 if face & 1 else b.size[a] - 1
+        return bi, q, None
+    q = list(p)
+    q[a] += 1 if face & 1 else -1
+    return bi, q, None
+
+
+def pressure_gradient_fvm(dom: ODomain, p: np.ndarray, interpolation: int):
+    """getPressureGradientFVM, extensions/PISO_multiblock_cuda_kernel.cu:991-1123: face pressures times face
+    area vectors (rows of det Minv), interpolation 0 = mean of the two cells' fluxes, 3 = the staggered
+    face transform times the mean pressure.  A prescribed face extrapolates the pressure from the
+    opposite side (half a cell for 0, a full cell for 3) and uses the boundary transform; blocks without
+    a transform take the finite-difference gradient."""
+    D = dom.dims
+    g_fd = pressure_gradient_fd(dom, p)
+    out = np.zeros((D, dom.N))
+    T = 2 * D * D + 1
+    for bi, b in enumerate(dom.blocks):
+        for q in _cells(dom, bi):
+            gi = _gidx(dom, bi, q)
+            if b.transform is None:
+                out[:, gi] = g_fd[:, gi]
+                continue
+            MP, dP, pP = dom.Minv[gi], dom.det[gi], p[gi]
+            grad = np.zeros(D)
+            for face in range(2 * D):
+                a, up = face >> 1, face & 1
+                fs = 1.0 if up else -1.0
+                fluxP = MP[a] * (dP * pP)
+                axisN, tsgn = a, 1.0
+                if _at_bound(dom, bi, q, face) and _is_empty(dom, bi, face):
+                    bnd = b.boundaries[face]
+                    qi = list(q)
+                    qi[a] -= 1 if up else -1
+                    p_in = p[_gidx(dom, bi, qi)]
+                    if interpolation != 3:
+                        Tb = bnd.transform.reshape(-1, T)[_bound_flat(dom, bi, face, q)]
+                        pb = pP + (pP - p_in) * 0.5
+                        grad += Tb[D * D:2 * D * D].reshape(D, D)[a] * (Tb[-1] * pb) * fs
+                        continue
+                    pn = pP + (pP - p_in)
+                    MN, dN = MP, dP
+                else:
+                    ob, qn, cb = _across(dom, bi, q, face)
+                    if cb is not None:
+                        axisN = cb.axes[0] >> 1
+                        if (cb.axes[0] & 1) == up:
+                            tsgn = -1.0
+                    gN = _gidx(dom, ob, qn)
+                    MN, dN, pn = dom.Minv[gN], dom.det[gN], p[gN]
+                if interpolation == 0:
+                    grad += (fluxP + MN[axisN] * (dN * pn * tsgn)) * (0.5 * fs)
+                elif interpolation == 3:
+                    fq = list(q)
+                    fq[a] += up
+                    if D == 2:
+                        F = b.face_transform[0, a, fq[1], fq[0]]
+                    else:
+                        F = b.face_transform[0, a, fq[2], fq[1], fq[0]]
+                    grad += F[D * D:2 * D * D].reshape(D, D)[a] * (F[-1] * (pn + pP) * 0.5 * fs)
+            out[:, gi] = grad / dP
+    return out
+
+
+def correct_velocity_fvm(dom: ODomain, p_blocks: np.ndarray, A: np.ndarray, h: np.ndarray, dt: float,
+                         version: int, time_step_norm: bool = False):
+    """PISO_update_velocity_PressureFVM (versions 5 and 6), extensions/PISO_multiblock_cuda_kernel.cu:6013-6050,
+    6180-6191."""
+    g = pressure_gradient_fvm(dom, p_blocks, 0 if version == 5 else 3)
+    if time_step_norm:
+        g = g * dt
+    return h - g / A[None]
+
+
+def correct_velocity_v4(dom: ODomain, p_blocks: np.ndarray, A: np.ndarray, h: np.ndarray, dt: float):
+    """PISO_update_velocity_v4_orthogonal (version 4), extensions/PISO_multiblock_cuda_kernel.cu:6053-6160: the mean
+    of the two face fluxes (H/A minus the pressure flux through the face, with the orthogonal metrics of
+    the two cells), transformed back; a prescribed face contributes nothing.  As in the reference, the
+    cell's own metric is Minv[0][0] for every component (it is read at the cell position, whose channel
+    is 0), the neighbour's is Minv[d][d] (its aligned axis across a connection)."""
+    D = dom.dims
+    u = np.zeros((D, dom.N))
+    for bi, b in enumerate(dom.blocks):
+        for q in _cells(dom, bi):
+            gi = _gidx(dom, bi, q)
+            ra, pc, det = 1.0 / A[gi], p_blocks[gi], dom.det[gi]
+            t = dom.Minv[gi][0, 0]
+            for d in range(D):
+                cc = det * t
+                v = 0.0
+                for up in (0, 1):
+                    face = 2 * d + up
+                    if _at_bound(dom, bi, q, face) and _is_empty(dom, bi, face):
+                        continue
+                    ob, qn, cb = _across(dom, bi, q, face)
+                    comp = (cb.axes[0] >> 1) if cb is not None else d
+                    gN = _gidx(dom, ob, qn)
+                    tN = dom.Minv[gN][comp, comp]
+                    ccN = dom.det[gN] * tN
+                    dp = (pc - p_blocks[gN]) if up == 0 else (p_blocks[gN] - pc)
+                    v += (cc * h[d, gi] + ccN * h[comp, gN] - (cc * t * ra + ccN * tN / A[gN]) * dp * dt) * 0.25
+                u[d, gi] = v / (det * t)
+    return u
+
+
 # --------------------------------------------------------------------------
 # non-orthogonal terms (nonOrthoFlags != 0): tangential Laplacian fluxes on skewed grids
 # --------------------------------------------------------------------------

@@ -20,10 +20,9 @@ Differences in representation (not in results):
 
 Scope: the PISO path (orthogonal, and the non-orthogonal terms of ``nonOrthoFlags``) with fixed Dirichlet,
 periodic and connected block boundaries, per-cell transforms, block/global
-viscosity and velocity sources, in 2D and 3D, float32 and float64.  Passive
-scalar transport, the FVM velocity correctors, face-transform pressure assembly
-and ILU preconditioning raise ``NotImplementedError``; the gradients of the
-non-orthogonal terms are not implemented.
+viscosity and velocity sources, in 2D and 3D, float32 and float64, with the gradients of all of it;
+velocity correctors 0/1 (finite differences), 4, 5 and 6 (finite volumes).  Passive scalar
+transport, face-transform pressure assembly and ILU preconditioning raise ``NotImplementedError``.
 """
 from __future__ import annotations
 
@@ -1436,6 +1435,7 @@ class Domain:
             d.velocity = _ptr(b.velocity)
             d.pressure = _ptr(b.pressure)
             d.transform = _ptr(b.transform) if b.hasTransform() else None
+            d.face_transform = _ptr(b.faceTransform) if b.hasFaceTransform() else None
             if b.viscosity is not None:
                 d.viscosity = _ptr(b.viscosity)
                 d.viscosity_static = 1 if b.viscosity.dim() == 2 else 0
@@ -1823,13 +1823,27 @@ def SetupPressureRHSdiv(domain, timeStep, nonOrthoMode=0, useFaceTransform=False
 
 
 def CorrectVelocity(domain, timeStep, version=0, timeStepNorm=False):
-    """u = H/A - grad(p)/A with finite-difference pressure gradients (extensions/PISO_multiblock_cuda_kernel.cu:5947-5980)."""
-    if version not in (0, 1):
-        raise NotImplementedError("only the finite-difference velocity corrector (version 0/1) is implemented in pict_b200")
+    """u = H/A - grad(p)/A (extensions/PISO_multiblock_cuda_kernel.cu:6163-6201).  version 0/1: finite-difference
+    pressure gradient (:5947-5980); 4: mean of the two face fluxes with orthogonal metrics (:6053-6160,
+    always scaled by the time step); 5 / 6: finite-volume pressure gradient from interpolated cell
+    fluxes / staggered face transforms (:6013-6050).  Versions 2 and 3 are the reference's smoothing
+    kernels, which it marks as not to be used; they are rejected."""
+    version = int(version)
+    if version not in (0, 1, 4, 5, 6):
+        raise NotImplementedError("CorrectVelocity: version %d is not implemented in pict_b200 (0/1, 4, 5, 6 are)" % version)
     domain._check_ready()
+    if version in (5, 6):
+        for b in domain.getBlocks():
+            if not b.hasTransform():
+                continue
+            _check(version != 6 or b.hasFaceTransform(),
+                   "CorrectVelocity version 6 needs the face transforms of transformed blocks (block %s)" % b.name)
+            for f, bnd in enumerate(b.boundaries):
+                _check(not isinstance(bnd, FixedBoundary) or bnd.hasTransform(),
+                       "CorrectVelocity version %d needs the transform of fixed boundary %d of block %s" % (version, f, b.name))
     dt = _time_step(timeStep, domain)
-    check(_lib.load().pict_correct_velocity(ctypes.byref(domain._desc), dt, 1, int(bool(timeStepNorm)), 0,
-                                            _stream_ptr()), "CorrectVelocity")
+    check(_lib.load().pict_correct_velocity(ctypes.byref(domain._desc), dt, version if version else 1,
+                                            int(bool(timeStepNorm)), 0, _stream_ptr()), "CorrectVelocity")
 
 
 def _copy(domain, fn, what):

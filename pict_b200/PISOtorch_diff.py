@@ -598,7 +598,10 @@ _EXCLUDED_GRADIENTS["CorrectVelocity"] = (set(), set())
 
 
 def CorrectVelocity(domain, time_step, version, timeStepNorm=False):
-    """velocityResult = pressureRHS - grad(p)/A (PISOtorch_diff.py:1160-1236, FD version)."""
+    """velocityResult = pressureRHS - grad(p)/A (PISOtorch_diff.py:1160-1236).  The backward pass is the adjoint
+    of the finite-difference corrector for versions 0/1 and, as in the reference (whose CorrectVelocityGrad
+    has no version argument), also for the finite-volume versions 5 and 6, where it is exact on
+    orthogonal grids; version 4 has no gradient."""
     keys, tracked = flatten_domain(domain, ["A", "PRESSURE", "PRESSURE_RHS"])
 
     class CorrectVelocityFunction(torch.autograd.Function):
@@ -615,8 +618,8 @@ def CorrectVelocity(domain, time_step, version, timeStepNorm=False):
         def backward(ctx, u_grad):
             if not any(ctx.needs_input_grad):
                 return (None,) * len(keys)
-            if timeStepNorm or version not in (0, 1):
-                raise NotImplementedError("CorrectVelocity: gradient only for FD pressure gradients without timeStepNorm")
+            if timeStepNorm or version not in (0, 1, 5, 6):
+                raise NotImplementedError("CorrectVelocity: no gradient for version %d or with timeStepNorm" % version)
             set_domain_tensors_from_flat(domain, keys, ctx.saved)
             domain.UpdateDomainData()
             lib = _lib.load()

@@ -64,6 +64,7 @@ class BlockDesc(ctypes.Structure):
         ("viscosity_grad", c_vp),
         ("source_grad", c_vp),
         ("face", Face * 6),
+        ("face_transform", c_vp),
     ]
 
 

@@ -264,7 +264,89 @@ __global__ void k_flux_divergence(pict_domain_t dom, const T* field, T* out, dou
 // velocity correction u = h - grad(p)/A
 // ---------------------------------------------------------------------------------------------
 
+// Row r of Minv, component c, of a transform that may be absent (identity).
 template <typename T, int D>
+__device__ __forceinline__ T minv_or_id(const T* tr, int r, int c) {
+    return tr ? tr_minv<T, D>(tr, r, c) : (r == c ? T(1) : T(0));
+}
+
+// Finite-volume pressure gradient (getPressureGradientFVM, extensions/PISO_multiblock_cuda_kernel.cu:991-1123): the sum
+// over faces of the face pressure times the face area vector (row of det Minv), divided by the cell's
+// det.  INTERP 0 averages the two cells' fluxes det Minv[axis] p (with the connected neighbour's aligned
+// axis and the sign flip of a connection joining two lower or two upper faces); INTERP 3 takes the
+// staggered face transform times the mean pressure.  A prescribed face extrapolates the pressure from
+// the opposite neighbour, half a cell with the boundary transform (INTERP 0), a full cell (INTERP 3).
+// Blocks without a transform take the finite-difference gradient.  A missing boundary, neighbour or
+// face transform counts as the identity.
+template <typename T, int D, int INTERP>
+__device__ __forceinline__ void pressure_grad_fvm(const pict_domain_t& dom, const pict_block_t& B, int b,
+                                                  const int* p, int i, int l, const T* tr, T* g) {
+    if (!tr) {
+        pressure_grad_fd<T, D>(dom, B, b, p, i, l, tr, g);
+        return;
+    }
+    const T* pb = reinterpret_cast<const T*>(B.pressure);
+    const T pP = pb[l];
+    const T dP = tr_det<T, D>(tr);
+    T acc[D];
+#pragma unroll
+    for (int c = 0; c < D; ++c) acc[c] = T(0);
+#pragma unroll
+    for (int f = 0; f < 2 * D; ++f) {
+        const int a = f >> 1;
+        const int up = f & 1;
+        const T fs = up ? T(1) : T(-1);
+        T pn;
+        const T* trn = tr;
+        int an = a;
+        T tsgn = T(1);
+        if (at_face(p, B.size, f) && B.face[f].type == PICT_FACE_FIXED) {
+            int q[3] = {p[0], p[1], p[2]};
+            if (B.size[a] > 1) q[a] += up ? -1 : 1;
+            const T p_in = pb[q[0] + B.size[0] * (q[1] + B.size[1] * q[2])];
+            if (INTERP != 3) {
+                const pict_face_t& F = B.face[f];
+                const T* bt = F.transform
+                                  ? reinterpret_cast<const T*>(F.transform) + (size_t)boundary_flat(p, B.size, f) * TS<D>::value
+                                  : nullptr;
+                const T v = tr_det<T, D>(bt) * (pP + (pP - p_in) * T(0.5)) * fs;
+#pragma unroll
+                for (int c = 0; c < D; ++c) acc[c] += minv_or_id<T, D>(bt, a, c) * v;
+                continue;
+            }
+            pn = pP + (pP - p_in);
+        } else {
+            const Nbr n = neighbour(dom, B, b, p, i, f);
+            const pict_block_t& Bn = dom.blocks[n.b];
+            pn = reinterpret_cast<const T*>(Bn.pressure)[n.l];
+            trn = cell_transform<T, D>(Bn, n.l);
+            an = n.comp;
+            tsgn = T(n.flip);
+        }
+        if (INTERP == 0) {
+            const T vp = dP * pP, vn = tr_det<T, D>(trn) * pn * tsgn;
+#pragma unroll
+            for (int c = 0; c < D; ++c)
+                acc[c] += (tr_minv<T, D>(tr, a, c) * vp + minv_or_id<T, D>(trn, an, c) * vn) * (T(0.5) * fs);
+        } else {
+            int fp[3] = {p[0], p[1], p[2]};
+            fp[a] += up;
+            const int fx = B.size[0] + 1, fy = D > 1 ? B.size[1] + 1 : 1, fz = D > 2 ? B.size[2] + 1 : 1;
+            const T* ft = B.face_transform
+                              ? reinterpret_cast<const T*>(B.face_transform) +
+                                    ((((size_t)a * fz + fp[2]) * fy + fp[1]) * fx + fp[0]) * TS<D>::value
+                              : nullptr;
+            const T v = tr_det<T, D>(ft) * (pn + pP) * T(0.5) * fs;
+#pragma unroll
+            for (int c = 0; c < D; ++c) acc[c] += minv_or_id<T, D>(ft, a, c) * v;
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < D; ++c) g[c] = acc[c] / dP;
+}
+
+// MODE -1: finite-difference gradient (versions 0/1); 0 / 3: finite-volume gradient (versions 5 / 6)
+template <typename T, int D, int MODE>
 __global__ void k_correct_velocity(pict_domain_t dom, double dt_arg, int time_step_norm, int write_block) {
     const int N = dom.num_cells;
     const T* A = reinterpret_cast<const T*>(dom.A);
@@ -279,7 +361,8 @@ __global__ void k_correct_velocity(pict_domain_t dom, double dt_arg, int time_st
         unflatten(l, B.size, p);
         const T* tr = cell_transform<T, D>(B, l);
         T g[D];
-        pressure_grad_fd<T, D>(dom, B, b, p, i, l, tr, g);
+        if (MODE < 0) pressure_grad_fd<T, D>(dom, B, b, p, i, l, tr, g);
+        else pressure_grad_fvm<T, D, MODE>(dom, B, b, p, i, l, tr, g);
         const T rA = T(1) / A[i];
         const T dt = sim_time_step<T>(dom, B.sim, dt_arg);
         T* ub = reinterpret_cast<T*>(B.velocity);
@@ -290,6 +373,57 @@ __global__ void k_correct_velocity(pict_domain_t dom, double dt_arg, int time_st
             const T v = du + prhs[(size_t)c * N + i];
             vres[(size_t)c * N + i] = v;
             if (write_block) ub[(size_t)c * nc + l] = v;
+        }
+    }
+}
+
+// Version 4 (PISO_update_velocity_v4_orthogonal, extensions/PISO_multiblock_cuda_kernel.cu:6053-6160): per axis the mean of
+// the two face fluxes (cc h + cc_N h_N - (cc t / A + cc_N t_N / A_N) dp dt) / 4 with orthogonal metrics
+// t and cc = det t, transformed back by 1 / (det t); a prescribed face contributes nothing.  The cell's
+// own t is Minv[0][0] for every axis (the reference reads it at the cell position, channel 0), the
+// neighbour's is Minv[d][d] (its component aligned with the face across a connection).
+template <typename T, int D>
+__global__ void k_correct_velocity_v4(pict_domain_t dom, double dt_arg, int write_block) {
+    const int N = dom.num_cells;
+    const T* A = reinterpret_cast<const T*>(dom.A);
+    const T* prhs = reinterpret_cast<const T*>(dom.pressure_rhs);
+    T* vres = reinterpret_cast<T*>(dom.velocity_result);
+    PICT_CELL_LOOP(i, N) {
+        const int b = dom.cell_block[i];
+        const pict_block_t& B = dom.blocks[b];
+        const int l = i - B.offset;
+        const int nc = B.size[0] * B.size[1] * B.size[2];
+        int p[3];
+        unflatten(l, B.size, p);
+        const T* tr = cell_transform<T, D>(B, l);
+        const T det = tr_det<T, D>(tr);
+        const T ra = T(1) / A[i];
+        const T pc = reinterpret_cast<const T*>(B.pressure)[l];
+        const T dt = sim_time_step<T>(dom, B.sim, dt_arg);
+        T* ub = reinterpret_cast<T*>(B.velocity);
+        const T t = minv_or_id<T, D>(tr, 0, 0);
+        const T cc = det * t;
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            const T hb = prhs[(size_t)d * N + i];
+            T v = T(0);
+#pragma unroll
+            for (int up = 0; up < 2; ++up) {
+                const int f = 2 * d + up;
+                if (at_face(p, B.size, f) && B.face[f].type == PICT_FACE_FIXED) continue;
+                const Nbr n = neighbour(dom, B, b, p, i, f);
+                const pict_block_t& Bn = dom.blocks[n.b];
+                const T* trn = cell_transform<T, D>(Bn, n.l);
+                const T tN = minv_or_id<T, D>(trn, n.comp, n.comp);
+                const T ccN = tr_det<T, D>(trn) * tN;
+                const T pN = reinterpret_cast<const T*>(Bn.pressure)[n.l];
+                const T dp = up ? (pN - pc) : (pc - pN);
+                v += (cc * hb + ccN * prhs[(size_t)n.comp * N + n.j] - (cc * t * ra + ccN * tN / A[n.j]) * dp * dt) *
+                     T(0.25);
+            }
+            v /= det * t;
+            vres[(size_t)d * N + i] = v;
+            if (write_block) ub[(size_t)d * nc + l] = v;
         }
     }
 }
@@ -671,8 +805,14 @@ pict_status_t pict_setup_pressure_correction(const pict_domain_t* dom, double dt
 }  // extern "C"
 
 template <typename T, int D>
-static pict_status_t launch_correct(const pict_domain_t* dom, double dt, int tsn, int wb, cudaStream_t st) {
-    k_correct_velocity<T, D><<<cell_grid(dom->num_cells, 256), 256, 0, st>>>(*dom, dt, tsn, wb);
+static pict_status_t launch_correct(const pict_domain_t* dom, double dt, int version, int tsn, int wb, cudaStream_t st) {
+    const int grid = cell_grid(dom->num_cells, 256);
+    switch (version) {
+        case 4: k_correct_velocity_v4<T, D><<<grid, 256, 0, st>>>(*dom, dt, wb); break;
+        case 5: k_correct_velocity<T, D, 0><<<grid, 256, 0, st>>>(*dom, dt, tsn, wb); break;
+        case 6: k_correct_velocity<T, D, 3><<<grid, 256, 0, st>>>(*dom, dt, tsn, wb); break;
+        default: k_correct_velocity<T, D, -1><<<grid, 256, 0, st>>>(*dom, dt, tsn, wb); break;
+    }
     return check_launch("correct_velocity");
 }
 
@@ -727,9 +867,9 @@ pict_status_t pict_correct_velocity(const pict_domain_t* dom, double dt, int32_t
                                     int32_t write_block_velocity, void* stream) {
     pict_status_t s = check_dom(dom);
     if (s) return s;
-    if (!(version == 0 || version == 1))
-        return set_error(PICT_ERR_UNSUPPORTED, "only the finite-difference velocity corrector (version 0/1) is supported");
-    PICT_DISPATCH(dom, launch_correct, dom, dt, time_step_norm, write_block_velocity, (cudaStream_t)stream);
+    if (!(version == 0 || version == 1 || version == 4 || version == 5 || version == 6))
+        return set_error(PICT_ERR_UNSUPPORTED, "velocity corrector versions 0/1 (FD), 4, 5 and 6 (FVM) are supported");
+    PICT_DISPATCH(dom, launch_correct, dom, dt, version, time_step_norm, write_block_velocity, (cudaStream_t)stream);
 }
 
 pict_status_t pict_copy_velocity_result_to_blocks(const pict_domain_t* dom, void* stream) {
