@@ -58,6 +58,10 @@ typedef struct pict_face {
     const void* velocity;  /* fixed: boundary velocity [D] or [D][face cells] (device) */
     const void* transform; /* fixed: boundary transform [face cells][2D^2+1] or NULL */
     void* velocity_grad;   /* fixed: gradient of velocity (adjoint), same layout, or NULL */
+    int32_t scalar_static;   /* fixed: 1 if the passive scalar is a static [C] vector */
+    uint32_t scalar_neumann; /* fixed: bit c set = passive scalar channel c is a Neumann (gradient) boundary */
+    const void* scalar;      /* fixed: passive scalar [C] or [C][face cells], or NULL */
+    void* scalar_grad;       /* fixed: gradient of the passive scalar, same layout, or NULL */
 } pict_face_t;
 
 /* One structured block (BlockGPU, extensions/domain_structs_gpu.h:266-305). */
@@ -80,6 +84,8 @@ typedef struct pict_block {
     pict_face_t face[PICT_MAX_BLOCK_FACES];
     const void* face_transform; /* [D][(z+1)][y+1][x+1][2D^2+1] staggered face transforms or NULL
                                    (Block::faceTransform; read by the FVM velocity corrector, version 6) */
+    void* scalar;             /* [C][cells] passive scalar of the block, or NULL */
+    void* scalar_grad;        /* adjoint of the passive scalar, or NULL */
 } pict_block_t;
 
 /* A (possibly batched) domain.  All pointers are device pointers unless noted.
@@ -110,6 +116,11 @@ typedef struct pict_domain {
     void* pressure_rhs;       /* [D][N] (H/A vector field) */
     void* pressure_rhs_div;   /* [N] */
     void* pressure_result;    /* [N] */
+    int32_t scalar_channels;        /* passive scalar channels C (0: none) */
+    int32_t scalar_viscosity_static; /* 1: scalar_viscosity is [1], 0: [C] */
+    const void* scalar_viscosity;   /* NULL (use the domain viscosity), [1] or [C] */
+    void* scalar_rhs;               /* [C][N] */
+    void* scalar_result;            /* [C][N] */
 } pict_domain_t;
 
 /* Per right-hand-side solver report (LinearSolverResultInfo, extensions/bicgstab_solver.h:20-25). */
@@ -329,6 +340,18 @@ pict_status_t pict_stencil_outer_product(const pict_domain_t* dom, const void* a
 /* SetupPressureMatrixGrad (PISOtorch_diff.py:897-965): A_grad += d(P : P_grad)/dA. */
 pict_status_t pict_pressure_matrix_grad(const pict_domain_t* dom, const void* A, const void* P_grad, void* A_grad,
                                         void* stream);
+/* Passive scalars (extensions/PISO_multiblock_cuda_kernel.cu:3601-3865 with forPassiveScalar, 4079-4183; driver
+ * PISOtorch_simulation.py:1085-1167).  SetupAdvectionMatrix(forPassiveScalar=True, passiveScalarChannel=channel):
+ * C and A of channel `channel`, with the scalar viscosity and the channel's boundary types (no diffusion
+ * through Neumann faces), plus the non-orthogonal matrix terms of `non_ortho_flags`. */
+pict_status_t pict_setup_scalar_matrix(const pict_domain_t* dom, double dt, int32_t non_ortho_flags, int32_t channel,
+                                       void* stream);
+/* SetupAdvectionScalar: scalar_rhs [C][N] = (det s / dt + boundary advection and diffusion terms - the explicit
+ * non-orthogonal terms of scalar_result) / det. */
+pict_status_t pict_setup_scalar_rhs(const pict_domain_t* dom, double dt, int32_t non_ortho_flags, void* stream);
+/* CopyScalarResultToBlocks (to_blocks=1) / CopyScalarResultFromBlocks (0). */
+pict_status_t pict_copy_scalar_result(const pict_domain_t* dom, int32_t to_blocks, void* stream);
+
 /* Gradients of the non-orthogonal terms (nonOrthoFlags; the non-orthogonal parts of the reference's *_GRAD
  * kernels, extensions/PISO_multiblock_cuda_kernel.cu:1992-2098, 3212-3392).  what 0: advection matrix, out_bar =
  * C_grad [K][N] with A_bar = A_grad [N] -> coef_bar = viscosity gradient [N] (per cell); 1: velocity RHS,

@@ -199,6 +199,8 @@ class OBoundary:
     transform: Optional[np.ndarray] = None  # fixed: [1, face zyx, T]
     block: int = -1  # connected: other block index
     axes: Optional[List[int]] = None  # connected: axes as in ConnectedBoundary (extensions/domain_structs.h:329-338)
+    scalar: Optional[np.ndarray] = None  # fixed: passive scalar [1,C] static or [1,C,face zyx]
+    scalar_types: Optional[List[str]] = None  # fixed: 'dirichlet' / 'neumann', one for all channels or one per channel
 
 
 @dataclass
@@ -210,6 +212,7 @@ class OBlock:
     face_transform: Optional[np.ndarray] = None
     viscosity: Optional[np.ndarray] = None  # None, [1] static, or [1,1,zyx]
     source: Optional[np.ndarray] = None  # None, [1,D] static, or [1,D,zyx]
+    scalar: Optional[np.ndarray] = None  # passive scalar [1,C,zyx]
     boundaries: List[OBoundary] = field(default_factory=list)
 
     @property
@@ -220,10 +223,12 @@ class OBlock:
 class ODomain:
     """Host model of a PICT domain (extensions/domain_structs.h:563-787), FP64."""
 
-    def __init__(self, dims: int, viscosity: float):
+    def __init__(self, dims: int, viscosity: float, scalar_channels: int = 0, scalar_viscosity=None):
         self.dims = dims
         self.viscosity = float(viscosity)
         self.blocks: List[OBlock] = []
+        self.scalar_channels = int(scalar_channels)
+        self.scalar_viscosity = None if scalar_viscosity is None else np.asarray(scalar_viscosity, dtype=np.float64).reshape(-1)
 
     # ---- construction, mirroring Domain::CreateBlock / Block::* ----
     def create_block(self, size=None, velocity=None, pressure=None, coords=None):
@@ -249,14 +254,18 @@ class ODomain:
         self.blocks.append(b)
         return len(self.blocks) - 1
 
-    def _fixed(self, bi, face, velocity=None):
+    def _fixed(self, bi, face, velocity=None, scalar=None, scalar_types=None):
         b = self.blocks[bi]
         D = self.dims
         vel = np.zeros((1, D)) if velocity is None else np.asarray(velocity, dtype=np.float64)
         tr = None
         if b.face_transform is not None:
             tr = boundary_transform_from_face_transforms(b.face_transform, face)
-        b.boundaries[face] = OBoundary("fixed", velocity=vel, transform=tr)
+        sc = None
+        if self.scalar_channels:
+            sc = np.zeros((1, self.scalar_channels)) if scalar is None else np.asarray(scalar, dtype=np.float64)
+        b.boundaries[face] = OBoundary("fixed", velocity=vel, transform=tr, scalar=sc,
+                                       scalar_types=list(scalar_types) if scalar_types else ["dirichlet"])
 
     def _close_connected(self, bi, face):
         """Block::CloseConnectedBoudary with useFixed=True, extensions/domain_structs.cpp:1773-1807."""
@@ -266,11 +275,12 @@ class ODomain:
         elif bnd.kind == "periodic":
             self._fixed(bi, face ^ 1)
 
-    def close_boundary(self, bi, face, velocity=None):
-        """Block::CloseBoundary(face, velocity), extensions/domain_structs.cpp:1979-1986."""
+    def close_boundary(self, bi, face, velocity=None, scalar=None, scalar_types=None):
+        """Block::CloseBoundary(face, velocity, passiveScalar), extensions/domain_structs.cpp:1979-1986, and
+        FixedBoundary::setPassiveScalarType (extensions/domain_structs.cpp:622-643)."""
         face = face_index(face)
         self._close_connected(bi, face)
-        self._fixed(bi, face, velocity)
+        self._fixed(bi, face, velocity, scalar, scalar_types)
 
     def close_all(self, bi):
         for f in range(2 * self.dims):
@@ -619,6 +629,100 @@ def advection_rhs(dom: ODomain, dt: float, non_ortho_flags: int = 0, u_result: O
     return rhs
 
 
+# --------------------------------------------------------------------------
+# passive scalars
+# --------------------------------------------------------------------------
+
+def scalar_viscosity(dom: ODomain, c: int) -> float:
+    """getViscosity with forPassiveScalar, kernel.cu:1788-1799: the scalar viscosity ([1] or per channel),
+    else the domain viscosity; block viscosities do not apply to scalars (kernel.cu:1804-1807)."""
+    sv = dom.scalar_viscosity
+    if sv is None:
+        return dom.viscosity
+    return float(sv[0] if sv.size == 1 else sv[c])
+
+
+def scalar_global(dom: ODomain) -> np.ndarray:
+    """The blocks' passive scalars as [C, N] (CopyScalarResultFromBlocks)."""
+    C = dom.scalar_channels
+    return np.concatenate([np.asarray(b.scalar, dtype=np.float64).reshape(C, -1) for b in dom.blocks], axis=1)
+
+
+def _scalar_face_data(dom: ODomain, c: int):
+    """Per face: boundary scalar of channel c [N] and Neumann mask [N] at cells on fixed faces."""
+    D = dom.dims
+    N = dom.N
+    sb = np.zeros((2 * D, N))
+    neu = np.zeros((2 * D, N), dtype=bool)
+    for g in range(N):
+        bi = int(dom.blk[g])
+        p = [int(v) for v in dom.pos[g]]
+        for f in range(2 * D):
+            if dom.fixed[f, g]:
+                sb[f, g] = _fixed_data(dom, bi, f, p, c, "sc")
+                neu[f, g] = _scalar_type(dom, bi, f, c) == "neumann"
+    return sb, neu
+
+
+def scalar_matrix(dom: ODomain, dt: float, channel: int, non_ortho_flags: int = 0):
+    """PISO_build_matrix with forPassiveScalar, kernel.cu:3601-3865: the advection-diffusion matrix with the
+    scalar viscosity of `channel`; a fixed face adds 2 nu alpha to the diagonal only where the channel's
+    boundary type is Dirichlet (slip = 1 for Neumann, kernel.cu:3817-3832).  Returns (coef[K,N], A[N])."""
+    D = dom.dims
+    N = dom.N
+    K = 2 * D + 1
+    u = dom.velocity_global()
+    _, bflux, _ = dom.boundary_cell_data()
+    fl = face_fluxes(dom, u, bflux)
+    nu = scalar_viscosity(dom, channel)
+    _, neu = _scalar_face_data(dom, channel)
+    allc = np.arange(N)
+    det = dom.det
+    diag = det / dt
+    coef = np.zeros((K, N))
+    alpha_p = [laplace_coef(dom, np.full(N, d), allc) for d in range(D)]
+    for f in range(2 * D):
+        d = f >> 1
+        sign = 2 * (f & 1) - 1
+        ok = ~dom.fixed[f]
+        nb = dom.nb[f]
+        ff = sign * 0.5 * fl[f]
+        alpha_n = np.zeros(N)
+        alpha_n[ok] = laplace_coef(dom, dom.ncomp[f][ok], nb[ok])
+        vc = 0.5 * (alpha_p[d] + alpha_n) * nu
+        diag = diag + np.where(ok, ff + vc, np.where(neu[f], 0.0, 2.0 * nu * alpha_p[d]))
+        coef[f + 1] = np.where(ok, ff - vc, 0.0)
+    coef[0] = diag
+    if non_ortho_flags:
+        coef = coef + nonortho_matrix_terms(dom, non_ortho_flags, "sc", nu=np.full(N, nu), channel=channel)
+    coef = coef / det[None]
+    return coef, coef[0].copy()
+
+
+def scalar_rhs(dom: ODomain, dt: float, non_ortho_flags: int = 0, s_result: Optional[np.ndarray] = None):
+    """kPISO_build_scalar_advection_RHS, kernel.cu:4079-4183: per channel det s / dt, at fixed faces minus the
+    boundary scalar times the boundary flux plus nu 2 alpha s_b (Dirichlet) or nu s_b (Neumann), minus nu
+    times the explicit non-orthogonal terms of `s_result` [C,N] (kernel.cu:4165-4167), over det."""
+    D = dom.dims
+    N = dom.N
+    C = dom.scalar_channels
+    s = scalar_global(dom)
+    _, bflux, balpha = dom.boundary_cell_data()
+    det = dom.det
+    rhs = det[None] * s / dt
+    for c in range(C):
+        nu = scalar_viscosity(dom, c)
+        sb, neu = _scalar_face_data(dom, c)
+        for f in range(2 * D):
+            sign = 2 * (f & 1) - 1
+            add = -sb[f] * bflux[f] * sign + np.where(neu[f], sb[f] * nu, sb[f] * nu * 2.0 * balpha[f])
+            rhs[c] = rhs[c] + np.where(dom.fixed[f], add, 0.0)
+        if non_ortho_flags:
+            fields = {"sc": s if s_result is None else s_result}
+            rhs[c] = rhs[c] - nonortho_rhs(dom, non_ortho_flags, "sc", fields, c, True, False, nu=np.full(N, nu))
+    return rhs / det[None]
+
+
 def pressure_matrix(dom: ODomain, A: np.ndarray, non_ortho_flags: int = 0):
     """PISO_build_pressure_matrix, extensions/PISO_multiblock_cuda_kernel.cu:4797-4963 (no face transforms; the
     non-orthogonal terms of ``nonortho_matrix_terms`` when non_ortho_flags selects them)."""
@@ -923,20 +1027,37 @@ def _bound_lap_axis(dom: ODomain, bi: int, face: int, p, axis: int) -> np.ndarra
 
 
 def _fixed_data(dom: ODomain, bi: int, face: int, p, comp: int, kind: str) -> float:
-    """getFixedBoundaryData, kernel.cu:2379-2447, fixed boundaries: the velocity component; the fixed
-    boundary pressure is a static zero (domain_structs.cpp:565-576); IS_FIXED_BOUNDARY reads 1."""
+    """getFixedBoundaryData, kernel.cu:2379-2447, fixed boundaries: the velocity component or passive scalar
+    channel; the fixed boundary pressure is a static zero (domain_structs.cpp:565-576); IS_FIXED_BOUNDARY
+    reads 1."""
     if kind == "flag":
         return 1.0
     if kind == "p":
         return 0.0
+    if kind == "sc":
+        sc = dom.blocks[bi].boundaries[face].scalar
+        if sc is None:
+            return 0.0
+        sc = np.asarray(sc, dtype=np.float64)
+        if sc.ndim == 2:
+            return float(sc[0, comp])
+        return float(sc.reshape(dom.scalar_channels, -1)[comp, _bound_flat(dom, bi, face, p)])
     vel = np.asarray(dom.blocks[bi].boundaries[face].velocity, dtype=np.float64)
     if vel.ndim == 2:
         return float(vel[0, comp])
     return float(vel.reshape(dom.dims, -1)[comp, _bound_flat(dom, bi, face, p)])
 
 
-def _fixed_type(kind: str) -> str:
-    """getFixedBoundaryType, kernel.cu:2353-2377: velocity Dirichlet, pressure Neumann."""
+def _scalar_type(dom: ODomain, bi: int, face: int, comp: int) -> str:
+    types = dom.blocks[bi].boundaries[face].scalar_types or ["dirichlet"]
+    return types[comp] if len(types) > 1 else types[0]
+
+
+def _fixed_type(kind: str, dom: Optional[ODomain] = None, bi: int = 0, face: int = 0, comp: int = 0) -> str:
+    """getFixedBoundaryType, kernel.cu:2353-2377: velocity Dirichlet, pressure Neumann, passive scalar per
+    face and channel."""
+    if kind == "sc":
+        return _scalar_type(dom, bi, face, comp)
     return "neumann" if kind == "p" else "dirichlet"
 
 
@@ -949,6 +1070,8 @@ def _block_data(dom: ODomain, bi: int, p, comp: int, kind: str, fields) -> float
         return float(fields["vel"][comp, g])
     if kind == "p":
         return float(fields["p"][g])
+    if kind == "sc":
+        return float(fields["sc"][comp, g])
     return 0.0
 
 
@@ -975,7 +1098,7 @@ def corner_value(dom: ODomain, bi: int, p, comp: int, dir1: int, dir2: int, incl
             if _at_bound(dom, wb, wp, d1):
                 bnd = dom.blocks[wb].boundaries[d1]
                 if bnd.kind == "fixed":
-                    btype = _fixed_type(kind)
+                    btype = _fixed_type(kind, dom, wb, d1, comp)
                     if _at_bound(dom, wb, wp, d2):
                         return _fixed_data(dom, wb, d1, wp, comp, kind), 0, btype
                     q = list(wp)
@@ -1098,7 +1221,7 @@ def nonortho_alpha_interp(dom: ODomain, bi: int, p, with_visc: bool, with_A: boo
     return out
 
 
-def nonortho_matrix_terms(dom: ODomain, flags: int, which: str, A=None, nu=None) -> np.ndarray:
+def nonortho_matrix_terms(dom: ODomain, flags: int, which: str, A=None, nu=None, channel: int = 0) -> np.ndarray:
     """Non-orthogonal stencil terms [K, N]: which='adv' as PISO_build_matrix, kernel.cu:3736-3800 (with
     viscosity; the caller divides by det afterwards), which='p' as PISO_build_pressure_matrix,
     kernel.cu:4877-4934 (with 1/A).  A corner interpolated from n cells contributes
@@ -1111,12 +1234,12 @@ def nonortho_matrix_terms(dom: ODomain, flags: int, which: str, A=None, nu=None)
     incl_diag = bool(flags & NON_ORTHO_CENTER_MATRIX)
     if D < 2 or not (incl_nb or incl_diag):
         return add
-    sgn = -1.0 if which == "adv" else 1.0
-    kind = "vel" if which == "adv" else "flag"
+    sgn = 1.0 if which == "p" else -1.0
+    kind = {"adv": "vel", "p": "flag", "sc": "sc"}[which]
     for g in range(N):
         bi = int(dom.blk[g])
         p = [int(v) for v in dom.pos[g]]
-        ai = nonortho_alpha_interp(dom, bi, p, which == "adv", which == "p", A, nu)
+        ai = nonortho_alpha_interp(dom, bi, p, which != "p", which == "p", A, nu)
         for face in range(2 * D):
             if _at_bound(dom, bi, p, face) and _is_empty(dom, bi, face):
                 continue
@@ -1130,8 +1253,8 @@ def nonortho_matrix_terms(dom: ODomain, flags: int, which: str, A=None, nu=None)
                 for tup in range(2):
                     tface = 2 * t + tup
                     ts = 1.0 if tup else -1.0
-                    _, n, btype = corner_value(dom, bi, p, 0, face, tface, False, False, 2, kind, None)
-                    grad = (btype == "neumann") if which == "adv" else True
+                    _, n, btype = corner_value(dom, bi, p, channel, face, tface, False, False, 2, kind, None)
+                    grad = (btype == "neumann") if which != "p" else True
                     if n < 1:
                         if grad:
                             v = fs * ts * alpha * 0.25
@@ -1172,7 +1295,7 @@ def nonortho_rhs(dom: ODomain, flags: int, kind: str, fields, comp: int, with_vi
             axis = face >> 1
             fs = 1.0 if face & 1 else -1.0
             if _at_bound(dom, bi, p, face) and _is_empty(dom, bi, face):
-                if kind == "p" or _fixed_type(kind) == "neumann":
+                if kind == "p" or _fixed_type(kind, dom, bi, face, comp) == "neumann":
                     continue
                 balpha = _bound_lap_axis(dom, bi, face, p, axis)
                 for i in range(1, D):

@@ -570,13 +570,26 @@ class FixedBoundary(Boundary):
 
     # -- passive scalar (stored, not transported) --
     def setPassiveScalar(self, t):
+        dims = self.getSpatialDims()
+        _check(t.is_cuda, "passiveScalar must be a CUDA tensor")
+        _check(t.size(0) == 1, "Batches are not yet supported (passiveScalar).")
+        _check(t.size(1) == self.getPassiveScalarChannels(), "Passive scalar channels must match domain.")
+        _check(t.dim() == 2 or t.dim() == 2 + dims, "Passive Scalar spatial dimensions are invalid. Passive Scalar must be "
+               "1-3D and either static (shape NC) or varying (shape NCDHW). Varying dimensionality must match velocity.")
+        _check(t.dtype == self.getDtype(), "Passive Scalar dtype must match domain.")
         self.passiveScalar = t
+        if self.passiveScalarTypes is None:
+            self.passiveScalarTypes = [self._velocityType]
         self._changed = True
 
     def CreatePassiveScalar(self, createStatic):
         ch = self.getParentDomain().getPassiveScalarChannels()
-        self.setPassiveScalar(torch.zeros((1, ch), dtype=self.getDtype(), device=self.getDevice()))
-        self.passiveScalarTypes = [self._velocityType] * ch
+        if createStatic:
+            shape = [1, ch]
+        else:
+            _check(self.hasSize(), "FixedBoundary is missing size to create a varying PassiveScalar.")
+            shape = [1, ch] + [self._size[d] for d in reversed(range(self.getSpatialDims()))]
+        self.setPassiveScalar(torch.zeros(shape, dtype=self.getDtype(), device=self.getDevice()))
 
     def hasPassiveScalar(self):
         return self.passiveScalar is not None
@@ -590,9 +603,25 @@ class FixedBoundary(Boundary):
     def isPassiveScalarBoundaryTypeStatic(self):
         return self.passiveScalarTypes is None or len(set(self.passiveScalarTypes)) < 2
 
+    def _scalar_neumann_mask(self, channels):
+        """Bit c set where passive scalar channel c has a Neumann boundary (one type for all channels when
+        a single type is given)."""
+        types = self.passiveScalarTypes or [self._velocityType]
+        mask = 0
+        for c in range(channels):
+            if BoundaryConditionType(types[c] if len(types) > 1 else types[0]) == BoundaryConditionType.NEUMANN:
+                mask |= 1 << c
+        return mask
+
     def setPassiveScalarType(self, t):
-        ch = self.getPassiveScalarChannels()
-        self.passiveScalarTypes = list(t) if isinstance(t, (list, tuple)) else [t] * ch
+        """One type for every channel, or a list with one type per channel (FixedBoundary::setPassiveScalarType,
+        extensions/domain_structs.cpp:622-643)."""
+        _check(self.hasPassiveScalar(), "FixedBoundary has not passive scalar.")
+        types = list(t) if isinstance(t, (list, tuple)) else [t]
+        _check(len(types) == 1 or len(types) == self.getPassiveScalarChannels(),
+               "Passive scalar boundary conditions must be static or match channels.")
+        self.passiveScalarTypes = [BoundaryConditionType(x) for x in types]
+        self._changed = True
 
     # -- transform --
     def hasTransform(self):
@@ -1426,6 +1455,7 @@ class Domain:
         """Host block table with raw device pointers (Domain::UpdateDomainGPU, extensions/domain_structs.cpp:3040-3261)."""
         arr = (BlockDesc * len(self.blocks))()
         index = {id(b): i for i, b in enumerate(self.blocks)}
+        psc = self._psc if self.hasPassiveScalar() else 0
         for bi, b in enumerate(self.blocks):
             d = arr[bi]
             s = b.getSizes()
@@ -1446,6 +1476,10 @@ class Domain:
             d.pressure_grad = _ptr(b.pressureGrad) if b.pressureGrad.numel() > 0 else None
             d.viscosity_grad = _ptr(b.viscosityGrad) if b.viscosityGrad is not None else None
             d.source_grad = _ptr(b.velocitySourceGrad) if b.velocitySourceGrad is not None else None
+            if psc and b.passiveScalar is not None:
+                d.scalar = _ptr(b.passiveScalar)
+                g = b.passiveScalarGrad
+                d.scalar_grad = _ptr(g) if g is not None and g.numel() > 0 else None
             for f, bnd in enumerate(b.boundaries):
                 F = d.face[f]
                 if isinstance(bnd, FixedBoundary):
@@ -1454,6 +1488,12 @@ class Domain:
                     F.velocity = _ptr(bnd.velocity)
                     F.transform = _ptr(bnd.transform) if bnd.hasTransform() else None
                     F.velocity_grad = _ptr(bnd.velocityGrad) if bnd.velocityGrad is not None and bnd.velocityGrad.numel() > 0 else None
+                    if psc and bnd.passiveScalar is not None:
+                        F.scalar = _ptr(bnd.passiveScalar)
+                        F.scalar_static = 1 if bnd.passiveScalar.dim() == 2 else 0
+                        F.scalar_neumann = bnd._scalar_neumann_mask(psc)
+                        g = bnd.passiveScalarGrad
+                        F.scalar_grad = _ptr(g) if g is not None and g.numel() > 0 else None
                 elif isinstance(bnd, PeriodicBoundary):
                     F.type = _lib.PICT_FACE_PERIODIC
                 elif isinstance(bnd, ConnectedBoundary):
@@ -1509,7 +1549,29 @@ class Domain:
         d.pressure_rhs = _ptr(self.pressureRHS)
         d.pressure_rhs_div = _ptr(self.pressureRHSdiv)
         d.pressure_result = _ptr(self.pressureResult)
+        if self.hasPassiveScalar():
+            d.scalar_channels = self._psc
+            sv = self._scalar_viscosity_device()
+            if sv is not None:
+                d.scalar_viscosity = _ptr(sv)
+                d.scalar_viscosity_static = 1 if sv.numel() == 1 else 0
+            d.scalar_rhs = _ptr(self.scalarRHS) if self.scalarRHS.numel() > 0 else None
+            d.scalar_result = _ptr(self.scalarResult) if self.scalarResult.numel() > 0 else None
         return d
+
+    def _scalar_viscosity_device(self):
+        """The scalar viscosity as a contiguous tensor on the domain's device and dtype (a cached copy when
+        it was given elsewhere)."""
+        sv = self.passiveScalarViscosity
+        if sv is None:
+            return None
+        if sv.device == self._device and sv.dtype == self._dtype and sv.is_contiguous():
+            return sv
+        key = (id(sv), sv._version)
+        if getattr(self, "_sv_key", None) != key:
+            self._sv_dev = sv.detach().to(device=self._device, dtype=self._dtype).contiguous()
+            self._sv_key = key
+        return self._sv_dev
 
     def _check_ready(self):
         _check(len(self.blocks) > 0, "Domain does not contain blocks.")
@@ -1753,13 +1815,26 @@ def _non_ortho(flags):
     return flags
 
 
+def _check_scalar(domain, what):
+    _check(domain.hasPassiveScalar(), "%s: the domain has no passive scalar channels." % what)
+    for b in domain.getBlocks():
+        _check(b.passiveScalar is not None, "%s: block %s has no passive scalar." % (what, b.name))
+
+
 def SetupAdvectionMatrix(domain, timeStep, nonOrthoFlags, forPassiveScalar=False, passiveScalarChannel=0):
-    """Implicit advection-diffusion matrix C and its diagonal A (extensions/PISO_multiblock_cuda_kernel.cu:3601-3865)."""
-    if forPassiveScalar:
-        raise NotImplementedError("passive scalar transport is not implemented in pict_b200")
+    """Implicit advection-diffusion matrix C and its diagonal A (extensions/PISO_multiblock_cuda_kernel.cu:3601-3865); with
+    ``forPassiveScalar`` the matrix of passive scalar channel ``passiveScalarChannel`` (scalar viscosity, no
+    diffusion through the channel's Neumann faces)."""
     flags = _non_ortho(nonOrthoFlags)
     domain._check_ready()
     dt = _time_step(timeStep, domain)
+    if forPassiveScalar:
+        _check_scalar(domain, "SetupAdvectionMatrix")
+        ch = int(passiveScalarChannel)
+        _check(0 <= ch < domain.getPassiveScalarChannels(), "passiveScalarChannel out of range.")
+        check(_lib.load().pict_setup_scalar_matrix(ctypes.byref(domain._desc), dt, flags, ch, _stream_ptr()),
+              "SetupAdvectionMatrix")
+        return
     check(_lib.load().pict_setup_advection_matrix(ctypes.byref(domain._desc), dt, flags, _stream_ptr()),
           "SetupAdvectionMatrix")
 
@@ -1777,7 +1852,13 @@ def SetupAdvectionVelocity(domain, timeStep, nonOrthoFlags, applyPressureGradien
 
 
 def SetupAdvectionScalar(domain, timeStep, nonOrthoFlags):
-    raise NotImplementedError("passive scalar transport is not implemented in pict_b200")
+    """scalarRHS of every passive scalar channel (extensions/PISO_multiblock_cuda_kernel.cu:4079-4183).  With
+    non-orthogonal RHS flags the explicit terms are taken from ``domain.scalarResult``."""
+    flags = _non_ortho(nonOrthoFlags)
+    domain._check_ready()
+    _check_scalar(domain, "SetupAdvectionScalar")
+    dt = _time_step(timeStep, domain)
+    check(_lib.load().pict_setup_scalar_rhs(ctypes.byref(domain._desc), dt, flags, _stream_ptr()), "SetupAdvectionScalar")
 
 
 def SetupPressureCorrection(domain, timeStep, nonOrthoMode=0, useFaceTransform=False, timeStepNorm=False):
@@ -1868,11 +1949,17 @@ def CopyPressureResultFromBlocks(domain):
 
 
 def CopyScalarResultToBlocks(domain):
-    raise NotImplementedError("passive scalar transport is not implemented in pict_b200")
+    """The blocks' passive scalar = scalarResult (extensions/PISO_multiblock_cuda_kernel.cu:6543-6733)."""
+    domain._check_ready()
+    _check_scalar(domain, "CopyScalarResultToBlocks")
+    check(_lib.load().pict_copy_scalar_result(ctypes.byref(domain._desc), 1, _stream_ptr()), "CopyScalarResultToBlocks")
 
 
 def CopyScalarResultFromBlocks(domain):
-    raise NotImplementedError("passive scalar transport is not implemented in pict_b200")
+    """scalarResult = the blocks' passive scalar."""
+    domain._check_ready()
+    _check_scalar(domain, "CopyScalarResultFromBlocks")
+    check(_lib.load().pict_copy_scalar_result(ctypes.byref(domain._desc), 0, _stream_ptr()), "CopyScalarResultFromBlocks")
 
 
 # ------------------------------------------------------------------------------------------------

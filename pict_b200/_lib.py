@@ -43,6 +43,10 @@ class Face(ctypes.Structure):
         ("velocity", c_vp),
         ("transform", c_vp),
         ("velocity_grad", c_vp),
+        ("scalar_static", c_i32),
+        ("scalar_neumann", ctypes.c_uint32),
+        ("scalar", c_vp),
+        ("scalar_grad", c_vp),
     ]
 
 
@@ -65,6 +69,8 @@ class BlockDesc(ctypes.Structure):
         ("source_grad", c_vp),
         ("face", Face * 6),
         ("face_transform", c_vp),
+        ("scalar", c_vp),
+        ("scalar_grad", c_vp),
     ]
 
 
@@ -95,6 +101,11 @@ class DomainDesc(ctypes.Structure):
         ("pressure_rhs", c_vp),
         ("pressure_rhs_div", c_vp),
         ("pressure_result", c_vp),
+        ("scalar_channels", c_i32),
+        ("scalar_viscosity_static", c_i32),
+        ("scalar_viscosity", c_vp),
+        ("scalar_rhs", c_vp),
+        ("scalar_result", c_vp),
     ]
 
 
@@ -186,6 +197,9 @@ SIGNATURES = {
     "pict_stencil_outer_product": (c_i32, [_PD, c_vp, c_vp, c_i32, c_vp, ctypes.c_double, c_vp]),
     "pict_pressure_matrix_grad": (c_i32, [_PD, c_vp, c_vp, c_vp, c_vp]),
     "pict_nonortho_grad": (c_i32, [_PD, c_i32, c_i32] + [c_vp] * 6),
+    "pict_setup_scalar_matrix": (c_i32, [_PD, ctypes.c_double, c_i32, c_i32, c_vp]),
+    "pict_setup_scalar_rhs": (c_i32, [_PD, ctypes.c_double, c_i32, c_vp]),
+    "pict_copy_scalar_result": (c_i32, [_PD, c_i32, c_vp]),
     "pict_csr_row_ptr": (c_i32, [_PD, c_vp, c_vp]),
     "pict_stencil_to_csr": (c_i32, [_PD, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "pict_csr_to_stencil": (c_i32, [_PD, c_vp, c_vp, c_vp, c_vp, c_vp]),

@@ -18,5 +18,8 @@ int cell_grid(int n, int threads);
 // what 0 advection matrix (C, A), 1 velocity RHS, 2 pressure matrix, 3 pressure RHS divergence.
 // Returns PICT_OK without launching when `flags` selects no term of that operator.
 pict_status_t nonortho_pass(const pict_domain_t* dom, int32_t flags, int32_t what, void* stream);
+// The same with a passive scalar channel: what 4 scalar matrix of channel `ch` (C, A), 5 scalar RHS
+// (all channels).
+pict_status_t nonortho_pass_ch(const pict_domain_t* dom, int32_t flags, int32_t what, int32_t ch, void* stream);
 
 }  // namespace pict

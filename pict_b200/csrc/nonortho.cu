@@ -64,8 +64,24 @@ __device__ __forceinline__ int conn_dir(const pict_block_t& B, int f, int d) {
     return B.face[f].conn_axes[rel] ^ (d & 1);
 }
 
-// data kinds of the corner values: structure only (matrices), velocity result, pressure result
-enum { NK_FLAG = 0, NK_VEL = 1, NK_P = 2 };
+// data kinds of the corner values: structure only (matrices), velocity result, pressure result, passive scalar result
+enum { NK_FLAG = 0, NK_VEL = 1, NK_P = 2, NK_SC = 3 };
+
+// passive scalar viscosity of channel c (getViscosity with forPassiveScalar, extensions/PISO_multiblock_cuda_kernel.cu:1788-1799):
+// the domain's scalar viscosity, else the domain viscosity
+template <typename T>
+__device__ __forceinline__ T scalar_nu(const pict_domain_t& dom, const pict_block_t& B, int c) {
+    if (dom.scalar_viscosity) {
+        const T* v = reinterpret_cast<const T*>(dom.scalar_viscosity);
+        return dom.scalar_viscosity_static ? v[0] : v[c];
+    }
+    return reinterpret_cast<const T*>(dom.sim_viscosity)[B.sim];
+}
+
+// boundary type of passive scalar channel c at a fixed face (getFixedBoundaryType, extensions/PISO_multiblock_cuda_kernel.cu:2353-2376)
+__device__ __forceinline__ bool scalar_neumann(const pict_domain_t& dom, int b, int f, int c) {
+    return (dom.blocks[b].face[f].scalar_neumann >> c) & 1u;
+}
 
 // fixed boundary data (getFixedBoundaryData, extensions/PISO_multiblock_cuda_kernel.cu:2379-2447): velocity
 // component c; the fixed boundary pressure is a static zero; the structure kind reads 1
@@ -74,6 +90,12 @@ __device__ __forceinline__ T fixed_data(const pict_block_t& B, int f, const int*
     if (KIND == NK_FLAG) return T(1);
     if (KIND == NK_P) return T(0);
     const pict_face_t& F = B.face[f];
+    if (KIND == NK_SC) {
+        const T* v = reinterpret_cast<const T*>(F.scalar);
+        if (!v) return T(0);
+        if (F.scalar_static) return v[c];
+        return v[(size_t)c * face_cells(B.size, f) + boundary_flat(q, B.size, f)];
+    }
     const T* v = reinterpret_cast<const T*>(F.velocity);
     if (F.vel_static) return v[c];
     return v[(size_t)c * face_cells(B.size, f) + boundary_flat(q, B.size, f)];
@@ -184,7 +206,7 @@ __device__ Corner<T> corner_value(const pict_domain_t& dom, int b0, const int* p
     r.cells = w.cells;
     if (w.cells == 0) {
         const pict_block_t& B = dom.blocks[w.fb];
-        r.neumann = (KIND == NK_P);
+        r.neumann = (KIND == NK_P) || (KIND == NK_SC && scalar_neumann(dom, w.fb, w.ff, comp));
         r.value = w.nfp == 1 ? fixed_data<T, D, KIND>(B, w.ff, w.fp[0], comp)
                              : (fixed_data<T, D, KIND>(B, w.ff, w.fp[0], comp) + fixed_data<T, D, KIND>(B, w.ff, w.fp[1], comp)) *
                                    T(0.5);
@@ -208,16 +230,18 @@ __device__ __forceinline__ T lap(const T* tr, int c1, int c2) {
 }
 
 // ---------------------------------------------------------------------------------------------
-// matrix terms: WHICH 0 = advection (viscosity, divided by det, C and A), 1 = pressure (1/A, P)
+// matrix terms: WHICH 0 = advection (viscosity, divided by det, C and A), 1 = pressure (1/A, P),
+// 2 = passive scalar channel ch (scalar viscosity, divided by det, C and A; corners on the channel's
+// Neumann faces take the one-sided treatment)
 // ---------------------------------------------------------------------------------------------
 template <typename T, int D, int WHICH>
-__global__ void k_nonortho_matrix(pict_domain_t dom, int flags) {
+__global__ void k_nonortho_matrix(pict_domain_t dom, int flags, int ch) {
     constexpr int K = 2 * D + 1;
     const int N = dom.num_cells;
-    T* M = reinterpret_cast<T*>(WHICH == 0 ? dom.C : dom.P);
+    T* M = reinterpret_cast<T*>(WHICH == 1 ? dom.P : dom.C);
     T* Ad = reinterpret_cast<T*>(dom.A);
     const bool incl_nb = flags & NO_DIRECT_MATRIX, incl_diag = flags & NO_CENTER_MATRIX;
-    const T sgn = WHICH == 0 ? T(-1) : T(1);
+    const T sgn = WHICH == 1 ? T(1) : T(-1);
     PICT_CELL_LOOP(i, N) {
         const int b = dom.cell_block[i];
         const pict_block_t& B = dom.blocks[b];
@@ -225,7 +249,7 @@ __global__ void k_nonortho_matrix(pict_domain_t dom, int flags) {
         int p[3];
         unflatten(l, B.size, p);
         const T* tr = cell_transform<T, D>(B, l);
-        const T raP = WHICH == 0 ? cell_viscosity<T>(dom, B, l) : T(1) / Ad[i];
+        const T raP = WHICH == 0 ? cell_viscosity<T>(dom, B, l) : WHICH == 1 ? T(1) / Ad[i] : scalar_nu<T>(dom, B, ch);
         T add[K];
 #pragma unroll
         for (int k = 0; k < K; ++k) add[k] = T(0);
@@ -249,7 +273,7 @@ __global__ void k_nonortho_matrix(pict_domain_t dom, int flags) {
             const pict_block_t& Bn = dom.blocks[nb];
             const int ln = flat3(Bn.size, q);
             const T* trn = cell_transform<T, D>(Bn, ln);
-            const T raN = WHICH == 0 ? cell_viscosity<T>(dom, Bn, ln) : T(1) / Ad[Bn.offset + ln];
+            const T raN = WHICH == 0 ? cell_viscosity<T>(dom, Bn, ln) : WHICH == 1 ? T(1) / Ad[Bn.offset + ln] : raP;
             const T fs = (f & 1) ? T(1) : T(-1);
 #pragma unroll
             for (int k = 1; k < D; ++k) {
@@ -260,8 +284,10 @@ __global__ void k_nonortho_matrix(pict_domain_t dom, int flags) {
                 for (int tup = 0; tup < 2; ++tup) {
                     const int tf = 2 * t + tup;
                     const T ts = tup ? T(1) : T(-1);
-                    const Corner<T> cv = corner_value<T, D, NK_FLAG>(dom, b, p, f, tf, false, 0, nullptr);
-                    const bool grad = WHICH == 0 ? cv.neumann : true;
+                    CornerWalk cv;
+                    corner_walk<D>(dom, b, p, f, tf, false, cv);
+                    // fixed velocity faces are Dirichlet; pressure faces are Neumann; scalar faces per channel
+                    const bool grad = WHICH == 0 ? false : WHICH == 1 ? true : (cv.cells < 1 && scalar_neumann(dom, cv.fb, cv.ff, ch));
                     if (cv.cells < 1) {
                         if (grad) {
                             const T v = fs * ts * alpha * T(0.25);
@@ -282,11 +308,11 @@ __global__ void k_nonortho_matrix(pict_domain_t dom, int flags) {
                 }
             }
         }
-        const T scale = WHICH == 0 ? T(1) / tr_det<T, D>(tr) : T(1);
+        const T scale = WHICH != 1 ? T(1) / tr_det<T, D>(tr) : T(1);
 #pragma unroll
         for (int k = 0; k < K; ++k)
             if (add[k] != T(0)) M[(size_t)k * N + i] += add[k] * scale;
-        if (WHICH == 0) Ad[i] = M[i];
+        if (WHICH != 1) Ad[i] = M[i];
     }
 }
 
@@ -343,11 +369,12 @@ __device__ T diagonal_data(const pict_domain_t& dom, int b, const int* p, int di
 
 template <typename T, int D, int KIND>
 __global__ void k_nonortho_rhs(pict_domain_t dom, int flags) {
-    constexpr int NC = KIND == NK_VEL ? D : 1;
+    const int NC = KIND == NK_VEL ? D : KIND == NK_SC ? dom.scalar_channels : 1;
     const int N = dom.num_cells;
     const T* Ad = reinterpret_cast<const T*>(dom.A);
-    const T* data = reinterpret_cast<const T*>(KIND == NK_VEL ? dom.velocity_result : dom.pressure_result);
-    T* out = reinterpret_cast<T*>(KIND == NK_VEL ? dom.velocity_rhs : dom.pressure_rhs_div);
+    const T* data = reinterpret_cast<const T*>(KIND == NK_VEL ? dom.velocity_result
+                                               : KIND == NK_SC ? dom.scalar_result : dom.pressure_result);
+    T* out = reinterpret_cast<T*>(KIND == NK_VEL ? dom.velocity_rhs : KIND == NK_SC ? dom.scalar_rhs : dom.pressure_rhs_div);
     const bool incl1 = flags & NO_DIRECT_RHS;
     PICT_CELL_LOOP(i, N) {
         const int b = dom.cell_block[i];
@@ -356,9 +383,10 @@ __global__ void k_nonortho_rhs(pict_domain_t dom, int flags) {
         int p[3];
         unflatten(l, B.size, p);
         const T* tr = cell_transform<T, D>(B, l);
-        const T raP = KIND == NK_VEL ? cell_viscosity<T>(dom, B, l) : T(1) / Ad[i];
+        const T raP0 = KIND == NK_VEL ? cell_viscosity<T>(dom, B, l) : KIND == NK_SC ? T(0) : T(1) / Ad[i];
 #pragma unroll 1
         for (int c = 0; c < NC; ++c) {
+            const T raP = KIND == NK_SC ? scalar_nu<T>(dom, B, c) : raP0;
             const T* dc = data + (size_t)c * N;
             T S = T(0);
 #pragma unroll
@@ -367,6 +395,7 @@ __global__ void k_nonortho_rhs(pict_domain_t dom, int flags) {
                 const T fs = (f & 1) ? T(1) : T(-1);
                 if (at_face(p, B.size, f) && face_fixed(B, f)) {
                     if (KIND == NK_P) continue;  // pressure: zero normal gradient at fixed faces
+                    if (KIND == NK_SC && scalar_neumann(dom, b, f, c)) continue;
                     // velocity (Dirichlet): tangential gradient of the boundary data
                     const pict_face_t& F = B.face[f];
                     const int bf = boundary_flat(p, B.size, f);
@@ -400,7 +429,7 @@ __global__ void k_nonortho_rhs(pict_domain_t dom, int flags) {
                 const pict_block_t& Bn = dom.blocks[nb];
                 const int ln = flat3(Bn.size, q);
                 const T* trn = cell_transform<T, D>(Bn, ln);
-                const T raN = KIND == NK_VEL ? cell_viscosity<T>(dom, Bn, ln) : T(1) / Ad[Bn.offset + ln];
+                const T raN = KIND == NK_VEL ? cell_viscosity<T>(dom, Bn, ln) : KIND == NK_SC ? raP : T(1) / Ad[Bn.offset + ln];
 #pragma unroll
                 for (int k = 1; k < D; ++k) {
                     const int t = (a + k) % D;
@@ -427,8 +456,8 @@ __global__ void k_nonortho_rhs(pict_domain_t dom, int flags) {
                     S -= fs * fa * tg;
                 }
             }
-            if (KIND == NK_VEL) out[(size_t)c * N + i] -= S / tr_det<T, D>(tr);
-            else out[i] += S;
+            if (KIND == NK_P) out[i] += S;
+            else out[(size_t)c * N + i] -= S / tr_det<T, D>(tr);
         }
     }
 }
@@ -732,28 +761,34 @@ static pict_status_t launch_nonortho_grad(const pict_domain_t* dom, int flags, i
 }
 
 template <typename T, int D>
-static pict_status_t launch_nonortho(const pict_domain_t* dom, int flags, int what, cudaStream_t st) {
+static pict_status_t launch_nonortho(const pict_domain_t* dom, int flags, int what, int ch, cudaStream_t st) {
     const int grid = cell_grid(dom->num_cells, 128);
     switch (what) {
-        case 0: k_nonortho_matrix<T, D, 0><<<grid, 128, 0, st>>>(*dom, flags); break;
+        case 0: k_nonortho_matrix<T, D, 0><<<grid, 128, 0, st>>>(*dom, flags, 0); break;
         case 1: k_nonortho_rhs<T, D, NK_VEL><<<grid, 128, 0, st>>>(*dom, flags); break;
-        case 2: k_nonortho_matrix<T, D, 1><<<grid, 128, 0, st>>>(*dom, flags); break;
+        case 2: k_nonortho_matrix<T, D, 1><<<grid, 128, 0, st>>>(*dom, flags, 0); break;
+        case 4: k_nonortho_matrix<T, D, 2><<<grid, 128, 0, st>>>(*dom, flags, ch); break;
+        case 5: k_nonortho_rhs<T, D, NK_SC><<<grid, 128, 0, st>>>(*dom, flags); break;
         default: k_nonortho_rhs<T, D, NK_P><<<grid, 128, 0, st>>>(*dom, flags); break;
     }
     return check_launch("nonortho");
 }
 
 pict_status_t nonortho_pass(const pict_domain_t* dom, int32_t flags, int32_t what, void* stream) {
-    const bool matrix = (what == 0 || what == 2);
+    return nonortho_pass_ch(dom, flags, what, 0, stream);
+}
+
+pict_status_t nonortho_pass_ch(const pict_domain_t* dom, int32_t flags, int32_t what, int32_t ch, void* stream) {
+    const bool matrix = (what == 0 || what == 2 || what == 4);
     if (matrix && !(flags & (NO_DIRECT_MATRIX | NO_CENTER_MATRIX))) return PICT_OK;
     if (!matrix && !(flags & (NO_DIRECT_RHS | NO_DIAGONAL_RHS))) return PICT_OK;
     cudaStream_t st = (cudaStream_t)stream;
     if (dom->dtype == PICT_F32) {
-        if (dom->dims == 2) return launch_nonortho<float, 2>(dom, flags, what, st);
-        if (dom->dims == 3) return launch_nonortho<float, 3>(dom, flags, what, st);
+        if (dom->dims == 2) return launch_nonortho<float, 2>(dom, flags, what, ch, st);
+        if (dom->dims == 3) return launch_nonortho<float, 3>(dom, flags, what, ch, st);
     } else if (dom->dtype == PICT_F64) {
-        if (dom->dims == 2) return launch_nonortho<double, 2>(dom, flags, what, st);
-        if (dom->dims == 3) return launch_nonortho<double, 3>(dom, flags, what, st);
+        if (dom->dims == 2) return launch_nonortho<double, 2>(dom, flags, what, ch, st);
+        if (dom->dims == 3) return launch_nonortho<double, 3>(dom, flags, what, ch, st);
     }
     return set_error(PICT_ERR_UNSUPPORTED, "non-orthogonal terms: unsupported dtype/dims");
 }

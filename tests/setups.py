@@ -269,11 +269,15 @@ def forcing_box(n=128, viscosity=1e-3, seed=3):
 # ------------------------------------------------------------------ builders
 
 def build_oracle(spec) -> po.ODomain:
-    d = po.ODomain(spec["dims"], spec["viscosity"])
+    d = po.ODomain(spec["dims"], spec["viscosity"], spec.get("scalar_channels", 0), spec.get("scalar_viscosity"))
     for b in spec["blocks"]:
         bi = d.create_block(size=b.get("size"), velocity=b.get("velocity"), pressure=b.get("pressure"),
                             coords=b.get("coords"))
         ob = d.blocks[bi]
+        if d.scalar_channels:
+            zyx = ob.velocity.shape[2:]
+            ob.scalar = np.zeros((1, d.scalar_channels) + zyx) if b.get("scalar") is None else \
+                np.asarray(b["scalar"], dtype=np.float64)
         if b.get("viscosity") is not None:
             ob.viscosity = np.asarray(b["viscosity"], dtype=np.float64)
         if b.get("source") is not None:
@@ -282,7 +286,8 @@ def build_oracle(spec) -> po.ODomain:
         if op[0] == "close_all":
             d.close_all(op[1])
         elif op[0] == "close":
-            d.close_boundary(op[1], op[2], None if len(op) < 4 else op[3])
+            d.close_boundary(op[1], op[2], None if len(op) < 4 else op[3], None if len(op) < 5 else op[4],
+                             None if len(op) < 6 else op[5])
         elif op[0] == "periodic":
             d.make_periodic(op[1], op[2])
         elif op[0] == "connect":
@@ -303,13 +308,18 @@ def build_product(spec, dtype=None, device="cuda", module=None):
         PISOtorch = module
     dtype = torch.float64 if dtype is None else dtype
     t = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=dtype, device=device).contiguous()
+    C = spec.get("scalar_channels", 0)
+    sv = spec.get("scalar_viscosity")
     dom = PISOtorch.Domain(spec["dims"], torch.tensor([spec["viscosity"]], dtype=dtype), name="test", dtype=dtype,
-                           device=torch.device(device), passiveScalarChannels=0)
+                           device=torch.device(device), passiveScalarChannels=C,
+                           scalarViscosity=None if sv is None else t(np.asarray(sv, dtype=np.float64).reshape(-1)))
     blocks = []
     for b in spec["blocks"]:
         kw = {}
         if b.get("velocity") is not None:
             kw["velocity"] = t(b["velocity"])
+        if C and b.get("scalar") is not None:
+            kw["passiveScalar"] = t(b["scalar"])
         if b.get("coords") is not None:
             kw["vertexCoordinates"] = t(b["coords"])
         if not kw:
@@ -326,7 +336,15 @@ def build_product(spec, dtype=None, device="cuda", module=None):
         if op[0] == "close_all":
             blocks[op[1]].CloseAllBoundaries()
         elif op[0] == "close":
-            blocks[op[1]].CloseBoundary(op[2], None if len(op) < 4 else t(op[3]))
+            vel = None if len(op) < 4 or op[3] is None else t(op[3])
+            if len(op) >= 5 and op[4] is not None:
+                blocks[op[1]].CloseBoundary(op[2], vel, t(op[4]))
+            else:
+                blocks[op[1]].CloseBoundary(op[2], vel)
+            if len(op) >= 6 and op[5] is not None:
+                bct = PISOtorch.BoundaryConditionType
+                types = [bct.NEUMANN if x == "neumann" else bct.DIRICHLET for x in op[5]]
+                blocks[op[1]].getBoundary(po.face_index(op[2])).setPassiveScalarType(types if len(types) > 1 else types[0])
         elif op[0] == "periodic":
             blocks[op[1]].MakePeriodic(op[2])
         elif op[0] == "connect":
