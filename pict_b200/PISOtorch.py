@@ -21,8 +21,9 @@ Differences in representation (not in results):
 Scope: the PISO path (orthogonal, and the non-orthogonal terms of ``nonOrthoFlags``) with fixed Dirichlet,
 periodic and connected block boundaries, per-cell transforms, block/global
 viscosity and velocity sources, in 2D and 3D, float32 and float64, with the gradients of all of it;
-velocity correctors 0/1 (finite differences), 4, 5 and 6 (finite volumes).  Passive scalar
-transport, face-transform pressure assembly and ILU preconditioning raise ``NotImplementedError``.
+velocity correctors 0/1 (finite differences), 4, 5 and 6 (finite volumes); passive scalar transport
+(forward).  The gradients of passive scalars, face-transform pressure assembly and ILU preconditioning
+raise ``NotImplementedError``.
 """
 from __future__ import annotations
 
@@ -568,7 +569,7 @@ class FixedBoundary(Boundary):
     def CreateVelocityGrad(self):
         self.setVelocityGrad(torch.zeros_like(self._velocity))
 
-    # -- passive scalar (stored, not transported) --
+    # -- passive scalar --
     def setPassiveScalar(self, t):
         dims = self.getSpatialDims()
         _check(t.is_cuda, "passiveScalar must be a CUDA tensor")
@@ -1621,6 +1622,12 @@ class Domain:
     def setPressureResult(self, t):
         self._set_global("pressureResult", t, self._N)
 
+    def CreateScalarRHS(self):
+        self.scalarRHS = torch.zeros(self._N * self._psc, dtype=self._dtype, device=self._device)
+
+    def CreateScalarResult(self):
+        self.scalarResult = torch.zeros(self._N * self._psc, dtype=self._dtype, device=self._device)
+
     def setScalarRHS(self, t):
         self._set_global("scalarRHS", t, self._N * self._psc)
 
@@ -1973,7 +1980,7 @@ def CopyScalarResultFromBlocks(domain):
 # kernels as the autograd Functions of pict_b200.PISOtorch_diff; with nonOrthoFlags the gradients of
 # the non-orthogonal terms are added as the reference adds them: the explicit right-hand-side terms
 # to velocityResultGrad / pressureResultGrad, the coefficients to the viscosity gradients / AGrad.
-# Passive scalars are not implemented.
+# The gradients of passive scalars are not implemented.
 # ------------------------------------------------------------------------------------------------
 
 def _need_grad(domain, name, n):

@@ -410,6 +410,87 @@ class Simulation:
             return True
         return self._PISO_split_step_ops(iterations, time_step)
 
+    def _advect_scalar(self, step, time_step, flags, non_ortho_branch=None):
+        """Passive scalar advection at the start of a step (PISOtorch_simulation.py:1085-1167).  The channels are
+        solved together with one matrix (BiCGStab with C right-hand sides) unless the scalar viscosity
+        or the boundary types differ per channel; without non_orthogonal the RHS is set up once, else
+        the blocks' scalar is copied to scalarResult for the explicit terms and advect_non_ortho_steps
+        solves are made.  Returns (solve ok, whether the scalar matrix also serves the velocity: the
+        reference reuses it when neither a scalar or block viscosity nor per-channel settings exist)."""
+        domain = self.domain
+        B = self._backend
+        if self.differentiable:
+            raise NotImplementedError("gradients of passive scalar transport are not implemented in pict_b200")
+        C = domain.getPassiveScalarChannels()
+        n = domain.getTotalSize()
+        split = not (domain.isPassiveScalarViscosityStatic() and domain.isAllFixedBoundariesPassiveScalarTypeStatic())
+        matrix_for_velocity = not (domain.hasPassiveScalarViscosity() or domain.hasBlockViscosity()
+                                   or domain.hasPassiveScalarBlockViscosity() or split)
+        matrices = []
+        if split:
+            for ch in range(C):
+                B.SetupAdvectionMatrix(domain, time_step, flags, forPassiveScalar=True, passiveScalarChannel=ch)
+                matrices.append(domain.C.clone())
+        else:
+            B.SetupAdvectionMatrix(domain, time_step, flags, forPassiveScalar=True, passiveScalarChannel=0)
+        ortho = not (self.non_orthogonal if non_ortho_branch is None else non_ortho_branch)
+        reuse = self.advect_reuse_result and not self.differentiable
+        if not ortho:
+            B.CopyScalarResultFromBlocks(domain)
+        solve_ok = True
+        for no_step in range(1 if ortho else self.advect_non_ortho_steps):
+            B.SetupAdvectionScalar(domain, time_step, 0 if ortho else flags)
+            self._run_prep_fn("POST_SCALAR_SETUP", domain=domain, no_step=no_step, local_step=step, time_step=time_step,
+                              total_step=self.total_step, total_time=self.total_time)
+            first = ortho or no_step == 0 or not reuse
+            with torch.no_grad() if self.exclude_advection_solve_gradients else nullcontext():
+                if split:
+                    xs = [None] * C if first else [x.clone() for x in torch.split(domain.scalarResult, n)]
+                    rhs = torch.split(domain.scalarRHS, n)
+                    parts = []
+                    for ch in range(C):
+                        sr, solve_ok = self.linear_solve(matrices[ch], rhs[ch], x=xs[ch], use_BiCG=self.advection_use_BiCG,
+                                                         use_scipy=self.scipy_solve_advection, tol=self.advection_tol)
+                        parts.append(sr)
+                    scalar_result = torch.cat(parts)
+                else:
+                    x = None if first else domain.scalarResult.clone()
+                    scalar_result, solve_ok = self.linear_solve(domain.C, domain.scalarRHS, x=x,
+                                                                use_BiCG=self.advection_use_BiCG,
+                                                                use_scipy=self.scipy_solve_advection,
+                                                                tol=self.advection_tol)
+            domain.setScalarResult(scalar_result)
+            domain.UpdateDomainData()
+            if not ortho and (not solve_ok or self._check_stop()):
+                return solve_ok, matrix_for_velocity
+        B.CopyScalarResultToBlocks(domain)
+        return solve_ok, matrix_for_velocity
+
+    def advect_static(self, iterations, time_step=None):
+        """Advect only the passive scalar with the current velocity (PISOtorch_simulation.py:907-983)."""
+        self._check_domain()
+        if isinstance(iterations, torch.Tensor):
+            iterations = int(iterations.numpy()[0])
+        if time_step is None:
+            time_step = self._get_time_step_torch()
+        domain = self.domain
+        if not domain.hasPassiveScalar():
+            raise ValueError("Domain has no passive scalar to advect.")
+        flags = self._non_ortho_flags()
+        solve_ok = True
+        for step in range(iterations):
+            self._run_prep_fn("PRE", domain=domain, local_step=step, time_step=time_step, total_step=self.total_step,
+                              total_time=self.total_time)
+            domain.UpdateDomainData()
+            # the reference's static advection always takes the non-orthogonal branch of the scalar solve
+            solve_ok, _ = self._advect_scalar(step, time_step, flags, non_ortho_branch=True)
+            self._run_prep_fn("POST", domain=domain, local_step=step, time_step=time_step, total_step=self.total_step,
+                              total_time=self.total_time)
+            if not solve_ok or self._check_stop():
+                break
+            self.end_step(time_step)
+        return solve_ok
+
     def _PISO_split_step_ops(self, iterations, time_step):
         """Operator-by-operator step, PISOtorch_simulation.py:1054-1327 (orthogonal branch, or the non-orthogonal
         branch PISOtorch_simulation.py:1194-1296 when the domain's metrics are not orthogonal)."""
@@ -428,11 +509,15 @@ class Simulation:
             self._run_prep_fn("PRE", domain=domain, local_step=step, time_step=time_step, total_step=self.total_step,
                               total_time=self.total_time)
             domain.UpdateDomainData()
+            matrix_for_velocity = False
             if self.advect_passive_scalar and domain.hasPassiveScalar():
-                raise NotImplementedError("passive scalar transport is not implemented in pict_b200")
+                solve_ok, matrix_for_velocity = self._advect_scalar(step, time_step, 0)
+                if not solve_ok or self._check_stop():
+                    return solve_ok
             self._run_prep_fn("PRE_VELOCITY_SETUP", domain=domain, local_step=step, time_step=time_step,
                               total_step=self.total_step, total_time=self.total_time)
-            B.SetupAdvectionMatrix(domain, time_step, 0)
+            if not matrix_for_velocity:
+                B.SetupAdvectionMatrix(domain, time_step, 0)
             B.SetupAdvectionVelocity(domain, time_step, 0, False)
             self._run_prep_fn("POST_VELOCITY_SETUP", domain=domain, no_step=0, local_step=step, time_step=time_step,
                               total_step=self.total_step, total_time=self.total_time)
@@ -503,11 +588,15 @@ class Simulation:
             self._run_prep_fn("PRE", domain=domain, local_step=step, time_step=time_step, total_step=self.total_step,
                               total_time=self.total_time)
             domain.UpdateDomainData()
+            matrix_for_velocity = False
             if self.advect_passive_scalar and domain.hasPassiveScalar():
-                raise NotImplementedError("passive scalar transport is not implemented in pict_b200")
+                solve_ok, matrix_for_velocity = self._advect_scalar(step, time_step, flags)
+                if not solve_ok or self._check_stop():
+                    return solve_ok
             self._run_prep_fn("PRE_VELOCITY_SETUP", domain=domain, local_step=step, time_step=time_step,
                               total_step=self.total_step, total_time=self.total_time)
-            B.SetupAdvectionMatrix(domain, time_step, flags)
+            if not matrix_for_velocity:
+                B.SetupAdvectionMatrix(domain, time_step, flags)
             B.CopyVelocityResultFromBlocks(domain)
             for no_step in range(self.advect_non_ortho_steps):
                 B.SetupAdvectionVelocity(domain, time_step, flags, False)
@@ -643,10 +732,8 @@ class Simulation:
         return solve_ok
 
     def run(self, iterations, static=False, log_domain=True):
-        """PISOtorch_simulation.py:1374-1518 without image/VTK output."""
+        """PISOtorch_simulation.py:1374-1518 without image/VTK output; ``static`` advects only the passive scalar."""
         self._check_domain()
-        if static:
-            raise NotImplementedError("passive scalar transport is not implemented in pict_b200")
         domain = self.domain
         if self.log_interval > 0 and (self.log_images or self.log_vtk):
             warnings.warn("image/VTK output is not part of pict_b200; log_images/log_vtk are ignored")
@@ -666,7 +753,9 @@ class Simulation:
             time_step = torch.tensor([ts], dtype=self._get_dtype())
         for it in range(1, iterations + 1):
             try:
-                if adaptive:
+                if static:
+                    sim_ok = self.advect_static(iterations=substeps, time_step=time_step)
+                elif adaptive:
                     sim_ok = self._PISO_adaptive_step()
                 else:
                     sim_ok = self._PISO_split_step(iterations=substeps, time_step=time_step)

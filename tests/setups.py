@@ -219,6 +219,55 @@ NONORTHO_CASES = ["distorted2d", "skewed_channel2d", "skewed_periodic2d", "skewe
                   "skewed_twoblock2d_rotated", "skewed_cavity3d", "skewed_channel3d"]
 NONORTHO_FLAG_SETS = [25, 27, 19]
 
+# passive scalar setups: channels, scalar viscosity, block scalars, Dirichlet and Neumann faces per channel,
+# static and varying boundary scalars, orthogonal and skewed grids, two blocks, 2D and 3D
+SCALAR_CASES = ["scalar_cavity2d", "scalar_inflow2d", "scalar_twoblock2d_rotated", "scalar_distorted2d",
+                "scalar_channel3d", "scalar_skewed_cavity3d"]
+
+
+def scalar_case(name, seed=0):
+    rng = np.random.default_rng(100 + seed)
+
+    def add(spec, C, sv, extra_ops):
+        spec["scalar_channels"] = C
+        spec["scalar_viscosity"] = sv
+        for b in spec["blocks"]:
+            zyx = np.asarray(b["velocity"]).shape[2:]
+            b["scalar"] = rng.random((1, C) + tuple(zyx))
+        spec["ops"] = list(spec["ops"]) + extra_ops
+        return spec
+
+    if name == "scalar_cavity2d":
+        return add(case("cavity2d"), 2, [2e-2, 5e-3],
+                   [("close", 0, "-y", np.array([[1.0, 0.0]]), np.array([[1.0, 0.5]])),
+                    ("close", 0, "+x", None, np.array([[0.2, 0.3]]), ["dirichlet", "neumann"])])
+    if name == "scalar_inflow2d":
+        spec = case("inflow2d")
+        ny = np.asarray(spec["blocks"][0]["velocity"]).shape[2]
+        inflow = [op for op in spec["ops"] if op[0] == "close" and op[2] == "-x"][0][3]
+        outflow = [op for op in spec["ops"] if op[0] == "close" and op[2] == "+x"][0][3]
+        s_in = np.zeros((1, 1, ny, 1))
+        s_in[0, 0, :, 0] = np.linspace(0.0, 1.0, ny)
+        return add(spec, 1, None, [("close", 0, "-x", inflow, s_in),
+                                   ("close", 0, "+x", outflow, np.array([[0.0]]), ["neumann"])])
+    if name == "scalar_twoblock2d_rotated":
+        return add(case("twoblock2d_rotated"), 2, [1e-2],
+                   [("close", 0, "-y", np.array([[1.0, 0.0]]), np.array([[1.0, -1.0]])),
+                    ("close", 1, "+x", None, np.array([[0.1, 0.0]]), ["neumann"])])
+    if name == "scalar_distorted2d":
+        return add(case("distorted2d"), 1, [1e-2],
+                   [("close", 0, "-y", np.array([[1.0, 0.0]]), np.array([[1.0]])),
+                    ("close", 0, "+y", None, np.array([[0.0]]), ["neumann"])])
+    if name == "scalar_channel3d":
+        return add(case("channel3d"), 1, None,
+                   [("close", 0, "-y", None, np.array([[1.0]])),
+                    ("close", 0, "+y", None, np.array([[0.5]]), ["neumann"])])
+    if name == "scalar_skewed_cavity3d":
+        return add(case("skewed_cavity3d"), 2, [1e-2, 2e-2],
+                   [("close", 0, "+y", np.array([[1.0, 0.0, 0.0]]), np.array([[1.0, 0.0]])),
+                    ("close", 0, "-x", None, np.array([[0.2, 0.4]]), ["neumann", "dirichlet"])])
+    raise KeyError(name)
+
 
 CASES_2D = ["cavity2d", "cavity2d_refined", "distorted2d", "periodic2d", "fullperiodic2d", "inflow2d", "twoblock2d",
             "twoblock2d_rotated"]
