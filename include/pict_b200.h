@@ -352,6 +352,11 @@ pict_status_t pict_setup_scalar_rhs(const pict_domain_t* dom, double dt, int32_t
 /* CopyScalarResultToBlocks (to_blocks=1) / CopyScalarResultFromBlocks (0). */
 pict_status_t pict_copy_scalar_result(const pict_domain_t* dom, int32_t to_blocks, void* stream);
 
+/* SGSviscosityIncompressibleSmagorinsky (extensions/PISOtorch.cpp:540-542 -> extensions/PISO_multiblock_cuda_kernel.cu:6896-7019):
+ * out [N] = coefficient * delta * |S| per cell from the blocks' velocity (delta: largest squared column
+ * length of the cell transform M, 1 without one). */
+pict_status_t pict_sgs_smagorinsky(const pict_domain_t* dom, double coefficient, void* out, void* stream);
+
 /* Gradients of the non-orthogonal terms (nonOrthoFlags; the non-orthogonal parts of the reference's *_GRAD
  * kernels, extensions/PISO_multiblock_cuda_kernel.cu:1992-2098, 3212-3392).  what 0: advection matrix, out_bar =
  * C_grad [K][N] with A_bar = A_grad [N] -> coef_bar = viscosity gradient [N] (per cell); 1: velocity RHS,

@@ -630,6 +630,43 @@ def advection_rhs(dom: ODomain, dt: float, non_ortho_flags: int = 0, u_result: O
 
 
 # --------------------------------------------------------------------------
+# Smagorinsky sub-grid-scale viscosity
+# --------------------------------------------------------------------------
+
+def sgs_smagorinsky(dom: ODomain, coefficient: float) -> np.ndarray:
+    """SGSviscosityIncompressibleSmagorinsky, kernel.cu:6896-7019, per cell [N]: coefficient * delta * |S| with
+    the velocity gradient of getBlockDataGradient (kernel.cu:2987-3031: neighbour differences along each
+    computational axis over 2 cells, 1.5 where one side is a fixed face holding the boundary velocity;
+    the same component across a connection) times Minv, |S| = sqrt(2 S:S), and delta the largest
+    squared column length of the cell's transform M (1 without a transform)."""
+    D = dom.dims
+    N = dom.N
+    u = dom.velocity_global()
+    bvel, _, _ = dom.boundary_cell_data()
+    g = np.zeros((N, D, D))
+    for k in range(D):
+        dist = np.full(N, 2.0)
+        vals = []
+        for up in (0, 1):
+            f = 2 * k + up
+            fixed = dom.fixed[f]
+            vals.append(np.where(fixed[None], bvel[f], u[:, np.maximum(dom.nb[f], 0)]))
+            dist = dist - np.where(fixed, 0.5, 0.0)
+        g[:, :, k] = ((vals[1] - vals[0]) / dist[None]).T
+    G = np.einsum("nck,nkj->ncj", g, dom.Minv)
+    S = 0.5 * (G + np.transpose(G, (0, 2, 1)))
+    norm = np.sqrt(2.0 * np.sum(S * S, axis=(1, 2)))
+    delta = np.ones(N)
+    for bi, b in enumerate(dom.blocks):
+        if b.transform is None:
+            continue
+        o = dom.offsets[bi]
+        M = b.transform.reshape(b.ncells, -1)[:, :D * D].reshape(-1, D, D)
+        delta[o:o + b.ncells] = np.max(np.sum(M * M, axis=1), axis=1)
+    return coefficient * delta * norm
+
+
+# --------------------------------------------------------------------------
 # passive scalars
 # --------------------------------------------------------------------------
 

@@ -2219,6 +2219,24 @@ def SetupAdvectionScalarGrad(domain, timeStep, nonOrthoFlags):
     raise NotImplementedError("passive scalar transport is not implemented in pict_b200")
 
 
+def SGSviscosityIncompressibleSmagorinsky(domain, coefficient):
+    """Smagorinsky sub-grid-scale viscosity per block (extensions/PISO_multiblock_cuda_kernel.cu:6896-7019): for each
+    block a tensor shaped like its pressure with coefficient * delta * |S|, |S| = sqrt(2 S:S) of the
+    blocks' velocity and delta the largest squared column length of the cell transform (1 without one).
+    ``coefficient`` is a host tensor of shape [1]."""
+    domain._check_ready()
+    _check(isinstance(coefficient, torch.Tensor) and not coefficient.is_cuda, "coefficient must be a host tensor")
+    _check(coefficient.dim() == 1 and coefficient.size(0) == 1, "coefficient tensor must have shape [1]")
+    out = torch.empty(domain.getTotalSize(), dtype=domain.getDtype(), device=domain.getDevice())
+    check(_lib.load().pict_sgs_smagorinsky(ctypes.byref(domain._desc), float(coefficient[0]), _ptr(out), _stream_ptr()),
+          "SGSviscosityIncompressibleSmagorinsky")
+    res = []
+    for b in domain.getBlocks():
+        n = b.pressure.numel()
+        res.append(out[b.globalOffset:b.globalOffset + n].reshape(b.pressure.shape).clone())
+    return res
+
+
 def ComputeVelocityDivergence(domain):
     """Flux divergence of the blocks' velocity (extensions/PISO_multiblock_cuda_kernel.cu:6333-6388)."""
     domain._check_ready()
