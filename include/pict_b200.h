@@ -351,6 +351,16 @@ pict_status_t pict_setup_scalar_matrix(const pict_domain_t* dom, double dt, int3
 pict_status_t pict_setup_scalar_rhs(const pict_domain_t* dom, double dt, int32_t non_ortho_flags, void* stream);
 /* CopyScalarResultToBlocks (to_blocks=1) / CopyScalarResultFromBlocks (0). */
 pict_status_t pict_copy_scalar_result(const pict_domain_t* dom, int32_t to_blocks, void* stream);
+/* Gradients of the passive scalar operators (SetupAdvectionMatrixGrad with forPassiveScalar,
+ * extensions/PISO_multiblock_cuda_kernel.cu:3869-4077; SetupAdvectionScalarGrad :4185-4278), including the
+ * non-orthogonal terms of `non_ortho_flags`.  what 0: in_bar = C_grad [K][N] and A_bar = A_grad [N] of
+ * `channel` -> u_bar [D][N] += (block velocity), nu_bar [N] += (the channel's scalar viscosity, per cell).
+ * what 1: in_bar = scalarRHS_grad [C][N] -> s_bar [C][N] = (block scalar), s_result_bar [C][N] +=
+ * (scalarResult, explicit terms), boundary_scalar_grad [2D][C][N] += and boundary_velocity_grad
+ * [2D][D][N] += (per adjacent cell), nu_bar [C][N] += (per cell). */
+pict_status_t pict_scalar_grad(const pict_domain_t* dom, double dt, int32_t non_ortho_flags, int32_t what, int32_t channel,
+                               const void* in_bar, const void* A_bar, void* u_bar, void* s_bar, void* s_result_bar,
+                               void* boundary_scalar_grad, void* boundary_velocity_grad, void* nu_bar, void* stream);
 
 /* SGSviscosityIncompressibleSmagorinsky (extensions/PISOtorch.cpp:540-542 -> extensions/PISO_multiblock_cuda_kernel.cu:6896-7019):
  * out [N] = coefficient * delta * |S| per cell from the blocks' velocity (delta: largest squared column

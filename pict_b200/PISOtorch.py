@@ -22,8 +22,8 @@ Scope: the PISO path (orthogonal, and the non-orthogonal terms of ``nonOrthoFlag
 periodic and connected block boundaries, per-cell transforms, block/global
 viscosity and velocity sources, in 2D and 3D, float32 and float64, with the gradients of all of it;
 velocity correctors 0/1 (finite differences), 4, 5 and 6 (finite volumes); passive scalar transport
-(forward).  The gradients of passive scalars, face-transform pressure assembly and ILU preconditioning
-raise ``NotImplementedError``.
+with its raw gradient operators.  Face-transform pressure assembly and ILU preconditioning raise
+``NotImplementedError``.
 """
 from __future__ import annotations
 
@@ -33,6 +33,7 @@ import warnings
 import weakref
 from typing import List, Optional
 
+import numpy as np
 import torch
 
 from . import _lib
@@ -569,6 +570,16 @@ class FixedBoundary(Boundary):
     def CreateVelocityGrad(self):
         self.setVelocityGrad(torch.zeros_like(self._velocity))
 
+    def setPassiveScalarGrad(self, t):
+        _check(self.passiveScalar is not None, "FixedBoundary does not have a passive scalar.")
+        _check(t.shape == self.passiveScalar.shape, "FixedBoundary passive scalar gradient must match the passive scalar.")
+        self.passiveScalarGrad = t
+        self._changed = True
+
+    def CreatePassiveScalarGrad(self):
+        if self.passiveScalar is not None:
+            self.setPassiveScalarGrad(torch.zeros_like(self.passiveScalar))
+
     # -- passive scalar --
     def setPassiveScalar(self, t):
         dims = self.getSpatialDims()
@@ -880,6 +891,16 @@ class Block:
     def CreateVelocityGrad(self):
         self.setVelocityGrad(torch.zeros_like(self.velocity))
 
+    def setPassiveScalarGrad(self, t):
+        _check(self.passiveScalar is not None, "Block does not have a passive scalar.")
+        _check(t.shape == self.passiveScalar.shape, "Block passive scalar gradient must match the passive scalar.")
+        self.passiveScalarGrad = t
+        self._changed = True
+
+    def CreatePassiveScalarGrad(self):
+        if self.passiveScalar is not None:
+            self.setPassiveScalarGrad(torch.zeros_like(self.passiveScalar))
+
     def setPressureGrad(self, t):
         self._check_tensor(t, 1, False, "PressureGrad")
         self.pressureGrad = t
@@ -926,6 +947,11 @@ class Block:
         for b in self.boundaries:
             if isinstance(b, FixedBoundary):
                 b.CreateVelocityGrad()
+
+    def CreatePassiveScalarGradOnBoundaries(self):
+        for b in self.boundaries:
+            if isinstance(b, FixedBoundary):
+                b.CreatePassiveScalarGrad()
 
     def DetachFwd(self):
         self.velocity = self.velocity.detach()
@@ -1673,12 +1699,48 @@ class Domain:
         for b in self.blocks:
             b.CreateVelocityGradOnBoundaries()
 
+    def CreatePassiveScalarGradOnBlocks(self):
+        for b in self.blocks:
+            b.CreatePassiveScalarGrad()
+
+    def CreatePassiveScalarGradOnBoundaries(self):
+        for b in self.blocks:
+            b.CreatePassiveScalarGradOnBoundaries()
+
     def CreateViscosityGrad(self):
-        """Zero gradient of the domain viscosity and of every block viscosity (Domain::CreateViscosityGrad,
-        extensions/domain_structs.cpp:2875-2882)."""
+        """Zero gradient of the domain viscosity, of every block viscosity and of the passive scalar
+        viscosity (Domain::CreateViscosityGrad, extensions/domain_structs.cpp:2875-2882)."""
         self.viscosityGrad = torch.zeros_like(self.viscosity)
         for b in self.blocks:
             b.CreateViscosityGrad()
+        self.CreatePassiveScalarViscosityGrad()
+
+    def CreatePassiveScalarViscosityGrad(self):
+        if self.passiveScalarViscosity is not None:
+            self.passiveScalarViscosityGrad = torch.zeros_like(self.passiveScalarViscosity)
+
+    def hasPassiveScalarViscosityGrad(self):
+        return self.passiveScalarViscosityGrad is not None
+
+    def setPassiveScalarViscosityGrad(self, t):
+        _check(self.passiveScalarViscosity is not None and t.shape == self.passiveScalarViscosity.shape,
+               "Scalar viscosity grad shape must match Scalar viscosity.")
+        self.passiveScalarViscosityGrad = t
+
+    def clearPassiveScalarViscosityGrad(self):
+        self.passiveScalarViscosityGrad = None
+
+    def setScalarRHSGrad(self, t):
+        self._grad_vec("scalarRHSGrad", t, self._N * self._psc)
+
+    def CreateScalarRHSGrad(self):
+        self.scalarRHSGrad = torch.zeros(self._N * self._psc, dtype=self._dtype, device=self._device)
+
+    def setScalarResultGrad(self, t):
+        self._grad_vec("scalarResultGrad", t, self._N * self._psc)
+
+    def CreateScalarResultGrad(self):
+        self.scalarResultGrad = torch.zeros(self._N * self._psc, dtype=self._dtype, device=self._device)
 
     def setViscosityGrad(self, t):
         self.viscosityGrad = t
@@ -1980,7 +2042,8 @@ def CopyScalarResultFromBlocks(domain):
 # kernels as the autograd Functions of pict_b200.PISOtorch_diff; with nonOrthoFlags the gradients of
 # the non-orthogonal terms are added as the reference adds them: the explicit right-hand-side terms
 # to velocityResultGrad / pressureResultGrad, the coefficients to the viscosity gradients / AGrad.
-# The gradients of passive scalars are not implemented.
+# Passive scalars have raw gradient operators (SetupAdvectionScalarGrad, the forPassiveScalar matrix
+# gradient, CopyScalarResultGrad*).
 # ------------------------------------------------------------------------------------------------
 
 def _need_grad(domain, name, n):
@@ -2033,13 +2096,96 @@ def _add_parameter_grads(domain, g):
     domain.UpdateDomainData()
 
 
+def _face_cells(block, f):
+    """Global indices of the block's cells on face f, in the face's flat order (x fastest, face axis dropped)."""
+    key = (f, block.globalOffset)
+    cache = block.__dict__.setdefault("_face_cells_cache", {})
+    if key not in cache:
+        dims = block.getSpatialDims()
+        zyx = list(block.pressure.shape[2:])
+        idx = np.arange(int(np.prod(zyx))).reshape(zyx)
+        ax = dims - 1 - (f >> 1)
+        sl = [slice(None)] * dims
+        sl[ax] = slice(-1, None) if f & 1 else slice(0, 1)
+        cache[key] = torch.as_tensor(idx[tuple(sl)].reshape(-1) + block.globalOffset, device=block.velocity.device)
+    return cache[key]
+
+
+def _add_boundary_scalar_grads(domain, sb):
+    """Per-adjacent-cell boundary scalar adjoints sb [2D][C][N] to the fixed faces' passive scalar gradients
+    (static scalars receive the sum; extensions/PISO_multiblock_cuda_kernel.cu:2448-2476)."""
+    C = domain.getPassiveScalarChannels()
+    for b in domain.getBlocks():
+        for f, bnd in enumerate(b.boundaries):
+            if not isinstance(bnd, FixedBoundary) or bnd.passiveScalar is None:
+                continue
+            g = bnd.passiveScalarGrad
+            if g is None or g.shape != bnd.passiveScalar.shape:
+                continue
+            vals = sb[f][:, _face_cells(b, f)]
+            add = vals.sum(dim=1).reshape(g.shape) if bnd.passiveScalar.dim() == 2 else vals.reshape(g.shape)
+            bnd.setPassiveScalarGrad(g + add)
+
+
+def _add_scalar_viscosity_grad(domain, per_channel):
+    """Scalar viscosity adjoint per channel [C] to passiveScalarViscosityGrad when it exists, else to the domain
+    viscosity gradient (scatterViscosity_GRAD, extensions/PISO_multiblock_cuda_kernel.cu:1832-1849)."""
+    g = domain.passiveScalarViscosityGrad
+    if g is not None:
+        add = per_channel.sum() if g.numel() == 1 else per_channel
+        domain.passiveScalarViscosityGrad = g + add.reshape(g.shape).to(g.device, g.dtype)
+    else:
+        v = domain.viscosityGrad if domain.viscosityGrad is not None else torch.zeros_like(domain.viscosity)
+        domain.viscosityGrad = v + per_channel.sum().reshape(v.shape).to(v.device, v.dtype)
+
+
+def SetupAdvectionScalarGrad(domain, timeStep, nonOrthoFlags):
+    """Gradient of SetupAdvectionScalar (extensions/PISO_multiblock_cuda_kernel.cu:4185-4278): scalarRHSGrad to the
+    blocks' passive scalar gradients (assigned, as in the reference), the fixed faces' scalar and velocity
+    gradients, the scalar viscosity gradient and, with non-orthogonal RHS flags, scalarResultGrad."""
+    from .PISOtorch_diff import _Grads, _p, _stream
+    flags = _non_ortho(nonOrthoFlags)
+    domain._check_ready()
+    _check_scalar(domain, "SetupAdvectionScalarGrad")
+    dt = _time_step(timeStep, domain)
+    g = _Grads(domain)
+    C, N, D = domain.getPassiveScalarChannels(), g.N, g.D
+    rb = _need_grad(domain, "scalarRHSGrad", C * N).contiguous()
+    sres = _need_grad(domain, "scalarResultGrad", C * N)
+    s_bar, sb, nu = g.z(C * N), g.z(2 * D * C * N), g.z(C * N)
+    check(_lib.load().pict_scalar_grad(ctypes.byref(domain._desc), dt, flags, 1, 0, _p(rb), None, None, _p(s_bar),
+                                       _p(sres), _p(sb), _p(g.vb), _p(nu), _stream()), "SetupAdvectionScalarGrad")
+    s_bar = s_bar.reshape(C, N)
+    for b in domain.getBlocks():
+        n = b.pressure.numel()
+        b.setPassiveScalarGrad(s_bar[:, b.globalOffset:b.globalOffset + n].reshape(b.passiveScalar.shape).contiguous())
+    _add_boundary_scalar_grads(domain, sb.reshape(2 * D, C, N))
+    _add_scalar_viscosity_grad(domain, nu.reshape(C, N).sum(dim=1))
+    _add_parameter_grads(domain, g)
+
+
 def SetupAdvectionMatrixGrad(domain, timeStep, nonOrthoFlags, forPassiveScalar=False, passiveScalarChannel=0):
     """Gradient of SetupAdvectionMatrix (extensions/PISO_multiblock_cuda_kernel.cu:3869-4077): AGrad and CGrad to the
-    velocity, viscosity and boundary velocity gradients."""
+    velocity, viscosity and boundary velocity gradients; with ``forPassiveScalar`` to the velocity and the
+    scalar viscosity gradient of ``passiveScalarChannel``."""
     from .PISOtorch_diff import _Grads, _p, _stream
-    if forPassiveScalar:
-        raise NotImplementedError("passive scalar transport is not implemented in pict_b200")
     flags = _non_ortho(nonOrthoFlags)
+    if forPassiveScalar:
+        domain._check_ready()
+        _check_scalar(domain, "SetupAdvectionMatrixGrad")
+        dt = _time_step(timeStep, domain)
+        ch = int(passiveScalarChannel)
+        _check(0 <= ch < domain.getPassiveScalarChannels(), "passiveScalarChannel out of range.")
+        g = _Grads(domain)
+        nu = g.z(g.N)
+        check(_lib.load().pict_scalar_grad(ctypes.byref(domain._desc), dt, flags, 0, ch, _p(domain.CGrad.coef.contiguous()),
+                                           _p(_need_grad(domain, "AGrad", g.N).contiguous()), _p(g.un), None, None,
+                                           None, None, _p(nu), _stream()), "SetupAdvectionMatrixGrad")
+        per = torch.zeros(domain.getPassiveScalarChannels(), dtype=nu.dtype, device=nu.device)
+        per[ch] = nu.sum()
+        _add_scalar_viscosity_grad(domain, per)
+        _add_parameter_grads(domain, g)
+        return
     domain._check_ready()
     dt = _time_step(timeStep, domain)
     g = _Grads(domain)
@@ -2208,15 +2354,25 @@ def CopyPressureResultGradFromBlocks(domain):
 
 
 def CopyScalarResultGradFromBlocks(domain):
-    raise NotImplementedError("passive scalar transport is not implemented in pict_b200")
+    """scalarResultGrad = the blocks' passive scalar gradients (gradient of CopyScalarResultToBlocks)."""
+    domain._check_ready()
+    _check_scalar(domain, "CopyScalarResultGradFromBlocks")
+    C = domain.getPassiveScalarChannels()
+    parts = [(b.passiveScalarGrad if b.passiveScalarGrad is not None and b.passiveScalarGrad.numel() > 0
+              else torch.zeros_like(b.passiveScalar)).reshape(C, -1) for b in domain.getBlocks()]
+    domain.scalarResultGrad = torch.cat(parts, dim=1).reshape(-1).contiguous()
 
 
 def CopyScalarResultGradToBlocks(domain):
-    raise NotImplementedError("passive scalar transport is not implemented in pict_b200")
-
-
-def SetupAdvectionScalarGrad(domain, timeStep, nonOrthoFlags):
-    raise NotImplementedError("passive scalar transport is not implemented in pict_b200")
+    """The blocks' passive scalar gradients = scalarResultGrad (gradient of CopyScalarResultFromBlocks)."""
+    domain._check_ready()
+    _check_scalar(domain, "CopyScalarResultGradToBlocks")
+    C, N = domain.getPassiveScalarChannels(), domain.getTotalSize()
+    g = _need_grad(domain, "scalarResultGrad", C * N).reshape(C, N)
+    for b in domain.getBlocks():
+        n = b.pressure.numel()
+        b.setPassiveScalarGrad(g[:, b.globalOffset:b.globalOffset + n].reshape(b.passiveScalar.shape).clone())
+    domain.UpdateDomainData()
 
 
 def SGSviscosityIncompressibleSmagorinsky(domain, coefficient):

@@ -21,5 +21,11 @@ pict_status_t nonortho_pass(const pict_domain_t* dom, int32_t flags, int32_t wha
 // The same with a passive scalar channel: what 4 scalar matrix of channel `ch` (C, A), 5 scalar RHS
 // (all channels).
 pict_status_t nonortho_pass_ch(const pict_domain_t* dom, int32_t flags, int32_t what, int32_t ch, void* stream);
+// Gradients of the non-orthogonal passive scalar terms: what 4 matrix of channel `ch` (out_bar = C_bar
+// [K][N], A_bar [N] -> coef_bar += scalar viscosity adjoint per cell [N]), 5 RHS (out_bar = scalarRHS_bar
+// [C][N] -> data_bar += scalarResult adjoint [C][N], coef_bar += [C][N], sb_bar += boundary scalar
+// adjoint [2D][C][N] per adjacent cell).
+pict_status_t nonortho_grad_scalar(const pict_domain_t* dom, int32_t flags, int32_t what, int32_t ch, const void* out_bar,
+                                   const void* A_bar, void* data_bar, void* coef_bar, void* sb_bar, void* stream);
 
 }  // namespace pict

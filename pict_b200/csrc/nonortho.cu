@@ -526,15 +526,16 @@ __device__ __forceinline__ void atomic_add(T* p, T v) {
     if (v != T(0)) atomicAdd(p, v);
 }
 
-// matrix terms: M_bar (C_grad / P_grad [K][N]) and, for the advection matrix, A_bar (A = C[0]) to the
-// coefficient adjoint: viscosity (WHICH 0) or A (WHICH 1) per cell
+// matrix terms: M_bar (C_grad / P_grad [K][N]) and, for the advection matrices, A_bar (A = C[0]) to the
+// coefficient adjoint: viscosity (WHICH 0), A (WHICH 1) or the scalar viscosity of channel ch (WHICH 2),
+// per cell
 template <typename T, int D, int WHICH>
-__global__ void k_nonortho_matrix_grad(pict_domain_t dom, int flags, const T* Mbar, const T* Abar, T* coef_bar) {
+__global__ void k_nonortho_matrix_grad(pict_domain_t dom, int flags, const T* Mbar, const T* Abar, T* coef_bar, int ch) {
     constexpr int K = 2 * D + 1;
     const int N = dom.num_cells;
     const T* Ad = reinterpret_cast<const T*>(dom.A);
     const bool incl_nb = flags & NO_DIRECT_MATRIX, incl_diag = flags & NO_CENTER_MATRIX;
-    const T sgn = WHICH == 0 ? T(-1) : T(1);
+    const T sgn = WHICH == 1 ? T(1) : T(-1);
     PICT_CELL_LOOP(i, N) {
         const int b = dom.cell_block[i];
         const pict_block_t& B = dom.blocks[b];
@@ -542,12 +543,12 @@ __global__ void k_nonortho_matrix_grad(pict_domain_t dom, int flags, const T* Mb
         int p[3];
         unflatten(l, B.size, p);
         const T* tr = cell_transform<T, D>(B, l);
-        const T raP = WHICH == 0 ? cell_viscosity<T>(dom, B, l) : T(1) / Ad[i];
-        const T scale = WHICH == 0 ? T(1) / tr_det<T, D>(tr) : T(1);
+        const T raP = WHICH == 0 ? cell_viscosity<T>(dom, B, l) : WHICH == 1 ? T(1) / Ad[i] : scalar_nu<T>(dom, B, ch);
+        const T scale = WHICH != 1 ? T(1) / tr_det<T, D>(tr) : T(1);
         T mb[K];
 #pragma unroll
         for (int k = 0; k < K; ++k) mb[k] = Mbar[(size_t)k * N + i] * scale;
-        if (WHICH == 0 && Abar) mb[0] += Abar[i] * scale;
+        if (WHICH != 1 && Abar) mb[0] += Abar[i] * scale;
         T raP_bar = T(0);
 #pragma unroll
         for (int f = 0; f < 2 * D; ++f) {
@@ -564,7 +565,7 @@ __global__ void k_nonortho_matrix_grad(pict_domain_t dom, int flags, const T* Mb
             const int ln = flat3(Bn.size, q);
             const int gN = Bn.offset + ln;
             const T* trn = cell_transform<T, D>(Bn, ln);
-            const T raN = WHICH == 0 ? cell_viscosity<T>(dom, Bn, ln) : T(1) / Ad[gN];
+            const T raN = WHICH == 0 ? cell_viscosity<T>(dom, Bn, ln) : WHICH == 1 ? T(1) / Ad[gN] : raP;
             const T fs = (f & 1) ? T(1) : T(-1);
 #pragma unroll
             for (int k = 1; k < D; ++k) {
@@ -579,7 +580,8 @@ __global__ void k_nonortho_matrix_grad(pict_domain_t dom, int flags, const T* Mb
                     const T ts = tup ? T(1) : T(-1);
                     CornerWalk w;
                     corner_walk<D>(dom, b, p, f, tf, false, w);
-                    const bool grad = WHICH == 0 ? false : true;  // fixed velocity faces are Dirichlet
+                    // fixed velocity faces are Dirichlet, pressure faces Neumann, scalar faces per channel
+                    const bool grad = WHICH == 0 ? false : WHICH == 1 ? true : (w.cells < 1 && scalar_neumann(dom, w.fb, w.ff, ch));
                     if (w.cells < 1) {
                         if (grad) {
                             const T v = fs * ts * T(0.25);
@@ -594,23 +596,25 @@ __global__ void k_nonortho_matrix_grad(pict_domain_t dom, int flags, const T* Mb
                 }
                 raP_bar += alpha_bar * aP * T(0.5);
                 const T rN_bar = alpha_bar * aN * T(0.5);
-                atomic_add(coef_bar + gN, WHICH == 0 ? rN_bar : rN_bar * (-raN * raN));
+                atomic_add(coef_bar + gN, WHICH != 1 ? rN_bar : rN_bar * (-raN * raN));
             }
         }
-        atomic_add(coef_bar + i, WHICH == 0 ? raP_bar : raP_bar * (-raP * raP));
+        atomic_add(coef_bar + i, WHICH != 1 ? raP_bar : raP_bar * (-raP * raP));
     }
 }
 
-// RHS terms: out_bar (velocityRHS_grad [D][N], the term entering as -S/det; or pressureRHSdiv_grad [N],
-// entering as +S) to the result field (data_bar), the coefficient adjoint (viscosity / A) and, for the
-// velocity, the fixed boundary velocity (vb_bar [2D][D][N], per adjacent cell)
+// RHS terms: out_bar (velocityRHS_grad [D][N] or scalarRHS_grad [C][N], the term entering as -S/det; or
+// pressureRHSdiv_grad [N], entering as +S) to the result field (data_bar), the coefficient adjoint
+// (viscosity [N], A [N], scalar viscosity [C][N]) and the fixed boundary data (velocity or scalar,
+// vb_bar [2D][D or C][N], per adjacent cell)
 template <typename T, int D, int KIND>
 __global__ void k_nonortho_rhs_grad(pict_domain_t dom, int flags, const T* out_bar, T* data_bar, T* coef_bar,
                                     T* vb_bar) {
-    constexpr int NC = KIND == NK_VEL ? D : 1;
+    const int NC = KIND == NK_VEL ? D : KIND == NK_SC ? dom.scalar_channels : 1;
     const int N = dom.num_cells;
     const T* Ad = reinterpret_cast<const T*>(dom.A);
-    const T* data = reinterpret_cast<const T*>(KIND == NK_VEL ? dom.velocity_result : dom.pressure_result);
+    const T* data = reinterpret_cast<const T*>(KIND == NK_VEL ? dom.velocity_result
+                                               : KIND == NK_SC ? dom.scalar_result : dom.pressure_result);
     const bool incl1 = flags & NO_DIRECT_RHS;
     PICT_CELL_LOOP(i, N) {
         const int b = dom.cell_block[i];
@@ -619,11 +623,14 @@ __global__ void k_nonortho_rhs_grad(pict_domain_t dom, int flags, const T* out_b
         int p[3];
         unflatten(l, B.size, p);
         const T* tr = cell_transform<T, D>(B, l);
-        const T raP = KIND == NK_VEL ? cell_viscosity<T>(dom, B, l) : T(1) / Ad[i];
+        const T raP0 = KIND == NK_VEL ? cell_viscosity<T>(dom, B, l) : KIND == NK_SC ? T(0) : T(1) / Ad[i];
         T raP_bar = T(0);
 #pragma unroll 1
         for (int c = 0; c < NC; ++c) {
-            const T sbar = KIND == NK_VEL ? -out_bar[(size_t)c * N + i] / tr_det<T, D>(tr) : out_bar[i];
+            const T raP = KIND == NK_SC ? scalar_nu<T>(dom, B, c) : raP0;
+            T* cb_c = coef_bar + (KIND == NK_SC ? (size_t)c * N : 0);
+            if (KIND == NK_SC) raP_bar = T(0);
+            const T sbar = KIND == NK_P ? out_bar[i] : -out_bar[(size_t)c * N + i] / tr_det<T, D>(tr);
             if (sbar == T(0)) continue;
             const T* dc = data + (size_t)c * N;
             T* dcb = data_bar + (size_t)c * N;
@@ -633,6 +640,7 @@ __global__ void k_nonortho_rhs_grad(pict_domain_t dom, int flags, const T* out_b
                 const T fs = (f & 1) ? T(1) : T(-1);
                 if (at_face(p, B.size, f) && face_fixed(B, f)) {
                     if (KIND == NK_P) continue;
+                    if (KIND == NK_SC && scalar_neumann(dom, b, f, c)) continue;
                     const pict_face_t& F = B.face[f];
                     const int bf = boundary_flat(p, B.size, f);
                     const T* btr = F.transform ? reinterpret_cast<const T*>(F.transform) + (size_t)bf * TS<D>::value : nullptr;
@@ -648,8 +656,8 @@ __global__ void k_nonortho_rhs_grad(pict_domain_t dom, int flags, const T* out_b
                         const T tg = df * (fixed_data<T, D, KIND>(B, f, hi, c) - fixed_data<T, D, KIND>(B, f, lo, c));
                         raP_bar += sbar * (-fs * bal * tg);
                         const T wv = sbar * (-fs * bal * raP) * df;
-                        atomic_add(vb_bar + ((size_t)f * D + c) * N + B.offset + flat3(B.size, hi), wv);
-                        atomic_add(vb_bar + ((size_t)f * D + c) * N + B.offset + flat3(B.size, lo), -wv);
+                        atomic_add(vb_bar + ((size_t)f * NC + c) * N + B.offset + flat3(B.size, hi), wv);
+                        atomic_add(vb_bar + ((size_t)f * NC + c) * N + B.offset + flat3(B.size, lo), -wv);
                     }
                     continue;
                 }
@@ -669,7 +677,7 @@ __global__ void k_nonortho_rhs_grad(pict_domain_t dom, int flags, const T* out_b
                 const int ln = flat3(Bn.size, q);
                 const int gN = Bn.offset + ln;
                 const T* trn = cell_transform<T, D>(Bn, ln);
-                const T raN = KIND == NK_VEL ? cell_viscosity<T>(dom, Bn, ln) : T(1) / Ad[gN];
+                const T raN = KIND == NK_VEL ? cell_viscosity<T>(dom, Bn, ln) : KIND == NK_SC ? raP : T(1) / Ad[gN];
 #pragma unroll
                 for (int k = 1; k < D; ++k) {
                     const int t = (a + k) % D;
@@ -684,7 +692,9 @@ __global__ void k_nonortho_rhs_grad(pict_domain_t dom, int flags, const T* out_b
                         const T ts = tup ? T(1) : T(-1);
                         CornerWalk w;
                         corner_walk<D>(dom, b, p, f, tf, incl1, w);
-                        const bool grad_bound = (w.cells == 0) && (KIND == NK_P);  // fixed velocity faces are Dirichlet
+                        // fixed velocity faces are Dirichlet, pressure faces Neumann, scalar faces per channel
+                        const bool grad_bound = (w.cells == 0) &&
+                                                (KIND == NK_P || (KIND == NK_SC && scalar_neumann(dom, w.fb, w.ff, c)));
                         if (grad_bound) {
                             const int to = tf ^ 1;
                             int cb;
@@ -711,7 +721,7 @@ __global__ void k_nonortho_rhs_grad(pict_domain_t dom, int flags, const T* out_b
                             const T wgt = w.nfp == 1 ? T(1) : T(0.5);
                             for (int k2 = 0; k2 < w.nfp; ++k2) {
                                 tg += ts * wgt * fixed_data<T, D, KIND>(Bf, w.ff, w.fp[k2], c);
-                                atomic_add(vb_bar + ((size_t)w.ff * D + c) * N + Bf.offset + flat3(Bf.size, w.fp[k2]),
+                                atomic_add(vb_bar + ((size_t)w.ff * NC + c) * N + Bf.offset + flat3(Bf.size, w.fp[k2]),
                                            tg_bar * ts * wgt);
                             }
                         } else {
@@ -727,30 +737,39 @@ __global__ void k_nonortho_rhs_grad(pict_domain_t dom, int flags, const T* out_b
                     const T fa_bar = sbar * (-fs * tg);
                     raP_bar += fa_bar * aP * T(0.5);
                     const T rN_bar = fa_bar * aN * T(0.5);
-                    atomic_add(coef_bar + gN, KIND == NK_VEL ? rN_bar : rN_bar * (-raN * raN));
+                    atomic_add(cb_c + gN, KIND == NK_P ? rN_bar * (-raN * raN) : rN_bar);
                 }
             }
+            if (KIND == NK_SC) atomic_add(cb_c + i, raP_bar);
         }
-        atomic_add(coef_bar + i, KIND == NK_VEL ? raP_bar : raP_bar * (-raP * raP));
+        if (KIND != NK_SC) atomic_add(coef_bar + i, KIND == NK_VEL ? raP_bar : raP_bar * (-raP0 * raP0));
     }
 }
 
 template <typename T, int D>
-static pict_status_t launch_nonortho_grad(const pict_domain_t* dom, int flags, int what, const void* out_bar,
+static pict_status_t launch_nonortho_grad(const pict_domain_t* dom, int flags, int what, int ch, const void* out_bar,
                                           const void* A_bar, void* data_bar, void* coef_bar, void* vb_bar,
                                           cudaStream_t st) {
     const int grid = cell_grid(dom->num_cells, 128);
     switch (what) {
         case 0:
             k_nonortho_matrix_grad<T, D, 0><<<grid, 128, 0, st>>>(*dom, flags, (const T*)out_bar, (const T*)A_bar,
-                                                                  (T*)coef_bar);
+                                                                  (T*)coef_bar, 0);
+            break;
+        case 4:
+            k_nonortho_matrix_grad<T, D, 2><<<grid, 128, 0, st>>>(*dom, flags, (const T*)out_bar, (const T*)A_bar,
+                                                                  (T*)coef_bar, ch);
+            break;
+        case 5:
+            k_nonortho_rhs_grad<T, D, NK_SC><<<grid, 128, 0, st>>>(*dom, flags, (const T*)out_bar, (T*)data_bar,
+                                                                   (T*)coef_bar, (T*)vb_bar);
             break;
         case 1:
             k_nonortho_rhs_grad<T, D, NK_VEL><<<grid, 128, 0, st>>>(*dom, flags, (const T*)out_bar, (T*)data_bar,
                                                                     (T*)coef_bar, (T*)vb_bar);
             break;
         case 2:
-            k_nonortho_matrix_grad<T, D, 1><<<grid, 128, 0, st>>>(*dom, flags, (const T*)out_bar, nullptr, (T*)coef_bar);
+            k_nonortho_matrix_grad<T, D, 1><<<grid, 128, 0, st>>>(*dom, flags, (const T*)out_bar, nullptr, (T*)coef_bar, 0);
             break;
         default:
             k_nonortho_rhs_grad<T, D, NK_P><<<grid, 128, 0, st>>>(*dom, flags, (const T*)out_bar, (T*)data_bar,
@@ -793,6 +812,22 @@ pict_status_t nonortho_pass_ch(const pict_domain_t* dom, int32_t flags, int32_t 
     return set_error(PICT_ERR_UNSUPPORTED, "non-orthogonal terms: unsupported dtype/dims");
 }
 
+pict_status_t nonortho_grad_scalar(const pict_domain_t* dom, int32_t flags, int32_t what, int32_t ch, const void* out_bar,
+                                   const void* A_bar, void* data_bar, void* coef_bar, void* sb_bar, void* stream) {
+    const bool matrix = what == 4;
+    if (matrix && !(flags & (NO_DIRECT_MATRIX | NO_CENTER_MATRIX))) return PICT_OK;
+    if (!matrix && !(flags & (NO_DIRECT_RHS | NO_DIAGONAL_RHS))) return PICT_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (dom->dtype == PICT_F32) {
+        if (dom->dims == 2) return launch_nonortho_grad<float, 2>(dom, flags, what, ch, out_bar, A_bar, data_bar, coef_bar, sb_bar, st);
+        if (dom->dims == 3) return launch_nonortho_grad<float, 3>(dom, flags, what, ch, out_bar, A_bar, data_bar, coef_bar, sb_bar, st);
+    } else if (dom->dtype == PICT_F64) {
+        if (dom->dims == 2) return launch_nonortho_grad<double, 2>(dom, flags, what, ch, out_bar, A_bar, data_bar, coef_bar, sb_bar, st);
+        if (dom->dims == 3) return launch_nonortho_grad<double, 3>(dom, flags, what, ch, out_bar, A_bar, data_bar, coef_bar, sb_bar, st);
+    }
+    return set_error(PICT_ERR_UNSUPPORTED, "nonortho_grad: unsupported dtype/dims");
+}
+
 }  // namespace pict
 
 using namespace pict;
@@ -810,14 +845,14 @@ extern "C" pict_status_t pict_nonortho_grad(const pict_domain_t* dom, int32_t fl
     cudaStream_t st = (cudaStream_t)stream;
     if (dom->dtype == PICT_F32) {
         if (dom->dims == 2)
-            return launch_nonortho_grad<float, 2>(dom, flags, what, out_bar, A_bar, data_bar, coef_bar, boundary_velocity_grad, st);
+            return launch_nonortho_grad<float, 2>(dom, flags, what, 0, out_bar, A_bar, data_bar, coef_bar, boundary_velocity_grad, st);
         if (dom->dims == 3)
-            return launch_nonortho_grad<float, 3>(dom, flags, what, out_bar, A_bar, data_bar, coef_bar, boundary_velocity_grad, st);
+            return launch_nonortho_grad<float, 3>(dom, flags, what, 0, out_bar, A_bar, data_bar, coef_bar, boundary_velocity_grad, st);
     } else if (dom->dtype == PICT_F64) {
         if (dom->dims == 2)
-            return launch_nonortho_grad<double, 2>(dom, flags, what, out_bar, A_bar, data_bar, coef_bar, boundary_velocity_grad, st);
+            return launch_nonortho_grad<double, 2>(dom, flags, what, 0, out_bar, A_bar, data_bar, coef_bar, boundary_velocity_grad, st);
         if (dom->dims == 3)
-            return launch_nonortho_grad<double, 3>(dom, flags, what, out_bar, A_bar, data_bar, coef_bar, boundary_velocity_grad, st);
+            return launch_nonortho_grad<double, 3>(dom, flags, what, 0, out_bar, A_bar, data_bar, coef_bar, boundary_velocity_grad, st);
     }
     return set_error(PICT_ERR_UNSUPPORTED, "nonortho_grad: unsupported dtype/dims");
 }

@@ -1,0 +1,96 @@
+"""Gradients of the passive scalar operators (SetupAdvectionMatrixGrad with forPassiveScalar,
+SetupAdvectionScalarGrad, CopyScalarResultGrad*) against the reference's own CUDA build (GPU).
+
+Fixtures: tests/golden/ref_scalar_grad_*.npz from tests/golden/make_ref_scalar_grad_fixtures.py (seeded
+gradient inputs, nonOrthoFlags 0, 25 and 27); the same function runs here with this library's module.
+Independent of the fixtures, a dot-product test checks that the scalar RHS gradient is the adjoint of
+the forward operator in the block scalar, the boundary scalars and the scalar result.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+import torch
+
+from setups import SCALAR_CASES, build_product, scalar_case
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+sys.path.insert(0, GOLDEN)
+import make_ref_scalar_grad_fixtures as G  # noqa: E402
+
+
+def _rel(a, b):
+    a, b = np.asarray(a, dtype=np.float64).reshape(-1), np.asarray(b, dtype=np.float64).reshape(-1)
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-30)
+
+
+@pytest.mark.parametrize("name", SCALAR_CASES)
+def test_scalar_grad_operators_match_reference(name):
+    from pict_b200 import PISOtorch as P
+    p = os.path.join(GOLDEN, "ref_scalar_grad_%s.npz" % name)
+    if not os.path.exists(p):
+        pytest.skip("fixture missing")
+    fx = np.load(p)
+    out = G.scalar_grad_fixture(P, name)
+    errs = {}
+    for key in fx.files:
+        assert key in out, key
+        assert out[key].size == fx[key].size, key
+        if np.abs(fx[key]).max() == 0 and np.abs(out[key]).max() == 0:
+            continue
+        errs[key] = _rel(out[key], fx[key])
+    worst = sorted(errs.items(), key=lambda kv: -kv[1])[:5]
+    print(name, {k: "%.1e" % v for k, v in worst})
+    assert max(errs.values()) < 1e-10, worst
+
+
+def _dot(a, b):
+    return float((a.double().reshape(-1) * b.double().reshape(-1)).sum())
+
+
+@pytest.mark.parametrize("flags", [0, 27])
+@pytest.mark.parametrize("name", ["scalar_cavity2d", "scalar_inflow2d", "scalar_skewed_cavity3d"])
+def test_scalar_rhs_gradient_is_the_adjoint(name, flags):
+    """scalarRHS is linear in the block scalar, the boundary scalars and the scalar result: the gradient
+    operator must return the transposed maps."""
+    from pict_b200 import PISOtorch as P
+    pd = build_product(scalar_case(name), torch.float64)
+    C, N = pd.getPassiveScalarChannels(), pd.getTotalSize()
+    ts = torch.tensor([0.05], dtype=torch.float64)
+    g = torch.Generator(device="cpu").manual_seed(7 + flags)
+    rnd = lambda *s: torch.randn(*s, generator=g, dtype=torch.float64).cuda()
+    blocks = pd.getBlocks()
+    fixed = [(b, bnd) for b in blocks for bnd in b.boundaries if isinstance(bnd, P.FixedBoundary)]
+    s0 = [b.passiveScalar.clone() for b in blocks]
+    sb0 = [bnd.passiveScalar.clone() for _, bnd in fixed]
+    r0 = rnd(C * N)
+    ds = [rnd(*x.shape) for x in s0]
+    dsb = [rnd(*x.shape) for x in sb0]
+    dr = rnd(C * N)
+
+    def rhs(eps):
+        for b, x, d in zip(blocks, s0, ds):
+            b.setPassiveScalar(x + eps * d)
+        for (_, bnd), x, d in zip(fixed, sb0, dsb):
+            bnd.setPassiveScalar(x + eps * d)
+        pd.setScalarResult(r0 + eps * dr)
+        pd.UpdateDomainData()
+        P.SetupAdvectionScalar(pd, ts, flags)
+        return pd.scalarRHS.clone()
+
+    w = rnd(C * N)
+    lin = _dot(w, rhs(1.0) - rhs(0.0))
+    pd.setScalarRHSGrad(w)
+    pd.CreateScalarResultGrad()
+    pd.CreatePassiveScalarGradOnBlocks()
+    pd.CreatePassiveScalarGradOnBoundaries()
+    pd.CreateVelocityGradOnBoundaries()
+    pd.CreateViscosityGrad()
+    pd.UpdateDomainData()
+    P.SetupAdvectionScalarGrad(pd, ts, flags)
+    adj = sum(_dot(b.passiveScalarGrad, d) for b, d in zip(blocks, ds))
+    adj += sum(_dot(bnd.passiveScalarGrad, d) for (_, bnd), d in zip(fixed, dsb))
+    adj += _dot(pd.scalarResultGrad, dr)
+    assert abs(lin - adj) <= 1e-11 * abs(lin), (lin, adj)

@@ -32,6 +32,20 @@ def test_library_loads_and_exports_all_declared_symbols():
     assert lib.pict_sizeof_domain() == ctypes.sizeof(_lib.DomainDesc)
 
 
+def test_binding_argument_counts_match_the_header():
+    """Every prototype of include/pict_b200.h has as many parameters as its ctypes signature."""
+    from pict_b200 import _lib
+    src = open(os.path.join(ROOT, "include", "pict_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    bad = {}
+    for name, params in re.findall(r"\b(pict_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", src):
+        params = params.strip()
+        n = 0 if params in ("", "void") else params.count(",") + 1
+        if name in _lib.SIGNATURES and len(_lib.SIGNATURES[name][1]) != n:
+            bad[name] = (n, len(_lib.SIGNATURES[name][1]))
+    assert not bad, bad
+
+
 def _pack_from_oracle(od):
     from pict_b200 import _lib
     arr = (_lib.BlockDesc * len(od.blocks))()
