@@ -116,6 +116,11 @@ def flatten_domain(domain, tensor_filter: List[str], empty: bool = False, exclus
             add(("VELOCITY_RHS",), domain.velocityRHS)
         elif name == "PRESSURE_RHS_DIV":
             add(("PRESSURE_RHS_DIV",), domain.pressureRHSdiv)
+        elif name == "PASSIVE_SCALAR_RESULT":
+            add(("PASSIVE_SCALAR_RESULT",), domain.scalarResult)
+        elif name == "PASSIVE_SCALAR_VISCOSITY":
+            if domain.passiveScalarViscosity is not None:
+                add(("PASSIVE_SCALAR_VISCOSITY",), domain.passiveScalarViscosity)
         else:
             for bi, b in enumerate(domain.getBlocks()):
                 if name == "VELOCITY":
@@ -130,6 +135,12 @@ def flatten_domain(domain, tensor_filter: List[str], empty: bool = False, exclus
                     for f in range(2 * domain.getSpatialDims()):
                         if _fixed(b, f):
                             add(("BOUNDARY_VELOCITY", bi, f), b.boundaries[f].velocity)
+                elif name == "PASSIVE_SCALAR" and b.passiveScalar is not None:
+                    add(("PASSIVE_SCALAR", bi), b.passiveScalar)
+                elif name == "BOUNDARY_PASSIVE_SCALAR":
+                    for f in range(2 * domain.getSpatialDims()):
+                        if _fixed(b, f) and b.boundaries[f].passiveScalar is not None:
+                            add(("BOUNDARY_PASSIVE_SCALAR", bi, f), b.boundaries[f].passiveScalar)
     return keys, ts
 
 
@@ -164,6 +175,14 @@ def set_domain_tensors_from_flat(domain, keys, tensors):
             blocks[key[1]].setViscosity(t)
         elif k == "BOUNDARY_VELOCITY":
             blocks[key[1]].boundaries[key[2]].setVelocity(t)
+        elif k == "PASSIVE_SCALAR_RESULT":
+            domain.setScalarResult(t)
+        elif k == "PASSIVE_SCALAR_VISCOSITY":
+            domain.setScalarViscosity(t)
+        elif k == "PASSIVE_SCALAR":
+            blocks[key[1]].setPassiveScalar(t)
+        elif k == "BOUNDARY_PASSIVE_SCALAR":
+            blocks[key[1]].boundaries[key[2]].setPassiveScalar(t)
 
 
 class _Grads:
@@ -308,9 +327,10 @@ _EXCLUDED_GRADIENTS["SetupAdvectionMatrix"] = (set(), set())
 
 def SetupAdvectionMatrix(domain, time_step, non_ortho_flags, forPassiveScalar=False, passiveScalarChannel=0):
     """A, C = advection matrix (PISOtorch_diff.py:377-441); differentiable w.r.t. velocity, boundary
-    velocity and viscosity."""
+    velocity and viscosity; with ``forPassiveScalar`` the matrix of a passive scalar channel, differentiable
+    w.r.t. velocity and the scalar viscosity (or the domain viscosity when there is none)."""
     if forPassiveScalar:
-        raise NotImplementedError("passive scalar transport is not implemented in pict_b200")
+        return _scalar_matrix_function(domain, time_step, non_ortho_flags, int(passiveScalarChannel))
     keys, tracked = flatten_domain(domain, ["VELOCITY", "BOUNDARY_VELOCITY", "VISCOSITY", "VISCOSITY_BLOCK"])
     dt = _dt(time_step)
 
@@ -343,8 +363,112 @@ def SetupAdvectionMatrix(domain, time_step, non_ortho_flags, forPassiveScalar=Fa
     return SetupAdvectionMatrixFunction.apply(*tracked)
 
 
+def _scalar_viscosity_grads(domain, keys, grads, per_channel):
+    """Put the per-channel scalar viscosity adjoint on the PASSIVE_SCALAR_VISCOSITY key, else on VISCOSITY."""
+    for i, key in enumerate(keys):
+        if key[0] == "PASSIVE_SCALAR_VISCOSITY":
+            sv = domain.passiveScalarViscosity
+            add = per_channel.sum() if sv.numel() == 1 else per_channel
+            grads[i] = add.reshape(sv.shape).to(sv.device, sv.dtype)
+            return grads
+    for i, key in enumerate(keys):
+        if key[0] == "VISCOSITY":
+            v = domain.viscosity
+            grads[i] = per_channel.sum().reshape(v.shape).to(v.device, v.dtype)
+    return grads
+
+
+def _scalar_matrix_function(domain, time_step, non_ortho_flags, channel):
+    """C, A of passive scalar channel `channel` (PISOtorch_diff.py:377-441 with forPassiveScalar)."""
+    keys, tracked = flatten_domain(domain, ["VELOCITY", "BOUNDARY_VELOCITY", "VISCOSITY", "PASSIVE_SCALAR_VISCOSITY"])
+    dt = _dt(time_step)
+
+    class SetupScalarMatrixFunction(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, *tracked_tensors):
+            domain.CreateA()
+            domain.C.CreateValue()
+            domain.UpdateDomainData()
+            PISOtorch.SetupAdvectionMatrix(domain, time_step, non_ortho_flags, forPassiveScalar=True,
+                                           passiveScalarChannel=channel)
+            ctx.saved = tracked_tensors
+            return domain.A, domain.C.coef
+
+        @staticmethod
+        @torch.autograd.function.once_differentiable
+        def backward(ctx, A_grad, C_grad):
+            if not any(ctx.needs_input_grad):
+                return (None,) * len(keys)
+            set_domain_tensors_from_flat(domain, keys, ctx.saved)
+            domain.UpdateDomainData()
+            g = _Grads(domain)
+            nu = g.z(g.N)
+            check(_lib.load().pict_scalar_grad(ctypes.byref(domain._desc), dt, int(non_ortho_flags), 0, channel,
+                                               _p(_zero_or(C_grad, domain.C.coef)), _p(_zero_or(A_grad, domain.A)),
+                                               _p(g.un), None, None, None, None, _p(nu), _stream()), "scalar matrix grad")
+            grads = g.to_inputs(keys)
+            per = torch.zeros(domain.getPassiveScalarChannels(), dtype=nu.dtype, device=nu.device)
+            per[channel] = nu.sum()
+            grads = _scalar_viscosity_grads(domain, keys, grads, per)
+            return tuple(_apply_exclusions("SetupAdvectionMatrix", keys, grads))
+
+    return SetupScalarMatrixFunction.apply(*tracked)
+
+
+_EXCLUDED_GRADIENTS["SetupAdvectionScalar"] = (set(), set())
+
+
 def SetupAdvectionScalar(domain, time_step, non_ortho_flags):
-    raise NotImplementedError("passive scalar transport is not implemented in pict_b200")
+    """scalarRHS (PISOtorch_diff.py:444-529); differentiable w.r.t. the blocks' and boundaries' passive scalar,
+    the boundary velocity, the scalar viscosity (or the domain viscosity) and, with non-orthogonal RHS
+    flags, the scalar result."""
+    is_non_ortho = check_non_ortho_rhs(non_ortho_flags)
+    keys, tracked = flatten_domain(domain, ["PASSIVE_SCALAR", "BOUNDARY_PASSIVE_SCALAR", "BOUNDARY_VELOCITY", "VISCOSITY",
+                                            "PASSIVE_SCALAR_VISCOSITY"]
+                                   + (["PASSIVE_SCALAR_RESULT"] if is_non_ortho else []))
+    dt = _dt(time_step)
+
+    class SetupAdvectionScalarFunction(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, *tracked_tensors):
+            domain.CreateScalarRHS()
+            domain.UpdateDomainData()
+            PISOtorch.SetupAdvectionScalar(domain, time_step, non_ortho_flags)
+            ctx.saved = tracked_tensors
+            return domain.scalarRHS
+
+        @staticmethod
+        @torch.autograd.function.once_differentiable
+        def backward(ctx, grad_rhs):
+            if not any(ctx.needs_input_grad):
+                return (None,) * len(keys)
+            set_domain_tensors_from_flat(domain, keys, ctx.saved)
+            domain.UpdateDomainData()
+            g = _Grads(domain)
+            C, N, D = domain.getPassiveScalarChannels(), g.N, g.D
+            s_bar, sres, sb, nu = g.z(C * N), g.z(C * N), g.z(2 * D * C * N), g.z(C * N)
+            check(_lib.load().pict_scalar_grad(ctypes.byref(domain._desc), dt, int(non_ortho_flags), 1, 0,
+                                               _p(grad_rhs.contiguous()), None, None, _p(s_bar), _p(sres), _p(sb),
+                                               _p(g.vb), _p(nu), _stream()), "scalar rhs grad")
+            grads = g.to_inputs(keys)
+            blocks = domain.getBlocks()
+            s_bar, sb = s_bar.reshape(C, N), sb.reshape(2 * D, C, N)
+            for i, key in enumerate(keys):
+                if key[0] == "PASSIVE_SCALAR":
+                    b = blocks[key[1]]
+                    grads[i] = s_bar[:, b.globalOffset:b.globalOffset + b.pressure.numel()].reshape(b.passiveScalar.shape)
+                elif key[0] == "BOUNDARY_PASSIVE_SCALAR":
+                    b = blocks[key[1]]
+                    bnd = b.boundaries[key[2]]
+                    vals = sb[key[2]][:, PISOtorch._face_cells(b, key[2])]
+                    grads[i] = vals.sum(dim=1).reshape(bnd.passiveScalar.shape) if bnd.passiveScalar.dim() == 2 \
+                        else vals.reshape(bnd.passiveScalar.shape)
+                elif key[0] == "PASSIVE_SCALAR_RESULT":
+                    grads[i] = sres
+            grads = _scalar_viscosity_grads(domain, keys, grads, nu.reshape(C, N).sum(dim=1))
+            return tuple(_apply_exclusions("SetupAdvectionScalar", keys, grads))
+
+    return SetupAdvectionScalarFunction.apply(*tracked)
 
 
 _EXCLUDED_GRADIENTS["SetupAdvectionVelocity"] = (set(), set())
@@ -731,11 +855,48 @@ def CopyPressureResultToBlocks(domain):
 
 
 def CopyScalarResultToBlocks(domain):
-    raise NotImplementedError("passive scalar transport is not implemented in pict_b200")
+    """Blocks' passive scalar = scalarResult."""
+    C = domain.getPassiveScalarChannels()
+
+    class CopyScalarResultToBlocksFunction(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, scalar_result):
+            for b in domain.getBlocks():
+                b.setPassiveScalar(torch.empty_like(b.passiveScalar))
+            domain.UpdateDomainData()
+            PISOtorch.CopyScalarResultToBlocks(domain)
+            return tuple(b.passiveScalar for b in domain.getBlocks())
+
+        @staticmethod
+        @torch.autograd.function.once_differentiable
+        def backward(ctx, *grads):
+            parts = [(torch.zeros_like(b.passiveScalar) if gs is None else gs).reshape(C, -1)
+                     for b, gs in zip(domain.getBlocks(), grads)]
+            return torch.cat(parts, dim=1).reshape(-1).contiguous()
+
+    CopyScalarResultToBlocksFunction.apply(domain.scalarResult)
 
 
 def CopyScalarResultFromBlocks(domain):
-    raise NotImplementedError("passive scalar transport is not implemented in pict_b200")
+    """scalarResult = blocks' passive scalar."""
+    C, N = domain.getPassiveScalarChannels(), domain.getTotalSize()
+
+    class CopyScalarResultFromBlocksFunction(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, *block_scalar):
+            domain.CreateScalarResult()
+            domain.UpdateDomainData()
+            PISOtorch.CopyScalarResultFromBlocks(domain)
+            return domain.scalarResult
+
+        @staticmethod
+        @torch.autograd.function.once_differentiable
+        def backward(ctx, sr_grad):
+            g = sr_grad.reshape(C, N)
+            return tuple(g[:, b.globalOffset:b.globalOffset + b.pressure.numel()].reshape(b.passiveScalar.shape).contiguous()
+                         for b in domain.getBlocks())
+
+    CopyScalarResultFromBlocksFunction.apply(*[b.passiveScalar for b in domain.getBlocks()])
 
 
 # ------------------------------------------------------------------------------------------ housekeeping

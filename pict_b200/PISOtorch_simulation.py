@@ -419,8 +419,6 @@ class Simulation:
         reference reuses it when neither a scalar or block viscosity nor per-channel settings exist)."""
         domain = self.domain
         B = self._backend
-        if self.differentiable:
-            raise NotImplementedError("gradients of passive scalar transport are not implemented in pict_b200")
         C = domain.getPassiveScalarChannels()
         n = domain.getTotalSize()
         split = not (domain.isPassiveScalarViscosityStatic() and domain.isAllFixedBoundariesPassiveScalarTypeStatic())
