@@ -153,6 +153,9 @@ typedef struct pict_solve_params {
     int32_t variant;           /* CG only: 0 classic order (extensions/cg_solver_kernel.cu:236-427, two reductions per iteration),
                                   1 single-reduction recurrence (Chronopoulos-Gear): same iterates in exact
                                   arithmetic, one grid-wide reduction per iteration */
+    int32_t residual_reset_steps; /* CG only: > 0 restarts the iteration (r = b - A x, p = r) before every
+                                     iteration i with (i+1) % residual_reset_steps == 0, as residualResetSteps
+                                     of extensions/cg_solver_kernel.cu:266-286; runs the classic order (variant 0) */
     double tolerance;
 } pict_solve_params_t;
 

@@ -1429,8 +1429,9 @@ def _crit(r):
     return float(np.sqrt(np.dot(r, r)) / math.sqrt(r.shape[0]))
 
 
-def cg(A, b, x0=None, tol=1e-5, maxit=5000, dtype=np.float64):
-    """cgSolveGPU without rank-deficiency, residual reset or best-result, extensions/cg_solver_kernel.cu:236-427."""
+def cg(A, b, x0=None, tol=1e-5, maxit=5000, dtype=np.float64, reset=0):
+    """cgSolveGPU without rank-deficiency or best-result, extensions/cg_solver_kernel.cu:236-427; `reset` > 0 restarts
+    the iteration (r = b - A x, p = r) before every iteration i with (i+1) % reset == 0 (:266-286)."""
     b = np.asarray(b, dtype=dtype)
     x = np.zeros_like(b) if x0 is None else np.array(x0, dtype=dtype)
     A = A.astype(dtype)
@@ -1439,6 +1440,10 @@ def cg(A, b, x0=None, tol=1e-5, maxit=5000, dtype=np.float64):
     rho = float(np.dot(r, r))
     info = SolveInfo(0.0, -1, False, True)
     for i in range(maxit):
+        if reset > 0 and (i + 1) % reset == 0:
+            r = b - A @ x
+            p = r.copy()
+            rho = float(np.dot(r, r))
         q = A @ p
         with np.errstate(divide="ignore", invalid="ignore"):  # a vanishing p.q gives inf / nan, as on the device
             alpha = np.float64(rho) / np.float64(np.dot(p, q))

@@ -2468,7 +2468,7 @@ class _Workspace:
 
 
 def _solve_params(nrhs, maxit, tol, conv, use_bicg, transpose, x_zero=False, subtract_mean=False,
-                  write_block_pressure=False, group_size=0, threads=0, variant=0):
+                  write_block_pressure=False, group_size=0, threads=0, variant=0, residual_reset=0):
     p = SolveParams()
     p.max_iterations = int(maxit)
     p.use_bicg = int(bool(use_bicg))
@@ -2481,6 +2481,7 @@ def _solve_params(nrhs, maxit, tol, conv, use_bicg, transpose, x_zero=False, sub
     p.subtract_mean = int(bool(subtract_mean))
     p.write_block_pressure = int(bool(write_block_pressure))
     p.variant = int(variant)
+    p.residual_reset_steps = max(int(residual_reset), 0)
     p.tolerance = float(tol)
     return p
 
@@ -2538,8 +2539,6 @@ def SolveLinear(A, RHS, x, maxIterations=1000, tolerance=1e-8, convergenceCriter
         raise NotImplementedError("matrixRankDeficient is not implemented in pict_b200")
     if returnBestResult:
         _warn_once("best", "returnBestResult is not implemented in pict_b200; the final iterate is returned")
-    if residualResetSteps:
-        _warn_once("reset", "residualResetSteps is ignored by pict_b200")
     if useBiCG and BiCGwithPreconditioner:
         _warn_once("ilu", "ILU preconditioning is not implemented in pict_b200; BiCGStab runs unpreconditioned")
     if domain.IsTensorChanged():
@@ -2554,7 +2553,7 @@ def SolveLinear(A, RHS, x, maxIterations=1000, tolerance=1e-8, convergenceCriter
         infos = decode_infos(info)
     else:
         for k in range(nb):
-            p = _solve_params(1, maxit, tol, conv, False, transposeA)
+            p = _solve_params(1, maxit, tol, conv, False, transposeA, residual_reset=int(residualResetSteps))
             info = solve_stencil(domain, coef, RHS[k * n:(k + 1) * n], x[k * n:(k + 1) * n], p)
             infos.extend(decode_infos(info))
     if printResidual:

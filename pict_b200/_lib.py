@@ -147,6 +147,7 @@ class SolveParams(ctypes.Structure):
         ("subtract_mean", c_i32),
         ("write_block_pressure", c_i32),
         ("variant", c_i32),
+        ("residual_reset_steps", c_i32),
         ("tolerance", ctypes.c_double),
     ]
 

@@ -80,6 +80,7 @@ struct KArgs {
     int x_zero;
     int sub_mean;
     int write_bp;
+    int reset;  // CG: restart period (0: none)
 };
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -356,6 +357,31 @@ __global__ void __launch_bounds__(KR_THREADS, 2) k_cg(KArgs<T> a) {
     }
 
     for (int it = 0; it < a.maxit; ++it) {
+        // restart (residualResetSteps, extensions/cg_solver_kernel.cu:266-286): r = b - A x, p = r, rho = r.r
+        if (a.reset > 0 && (it + 1) % a.reset == 0) {
+            for (int j = 0; j < S.n; ++j) {
+                if (!((s_active >> j) & 1u)) continue;
+                const pict_block_t& B = dom.blocks[S.block[j]];
+                double acc[1] = {0.0};
+                for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) {
+                    int p[3];
+                    unflatten(i - B.offset, B.size, p);
+                    const T ri = bv[i] - spmv_row<T, D, TRANS>(dom, coef, N, i, B, p, [&](int jj) { return x[jj]; });
+                    r[i] = ri;
+                    acc[0] += (double)ri * (double)ri;
+                }
+                warp_partial<1>(R, j, acc);
+            }
+            flush_partials<1>(R, S, s_active, part + phase * pstride);
+            if (!grid_barrier(a.ctrl, epoch, s_ctrl)) return;
+            system_sums<1>(part + phase * pstride, S, s_active, s_sum);
+            phase ^= 1;
+            if ((int)threadIdx.x < S.n && ((s_active >> threadIdx.x) & 1u)) {
+                s_rho[threadIdx.x] = s_sum[threadIdx.x][0];
+                s_beta[threadIdx.x] = 0.0;
+            }
+            __syncthreads();
+        }
         // phase 1: p <- r + beta p (on the fly for neighbours), q = A p, p.q
         for (int j = 0; j < S.n; ++j) {
             if (!((s_active >> j) & 1u)) continue;
@@ -1157,13 +1183,14 @@ static pict_status_t run_solve(const pict_domain_t* dom, const void* coef, const
         a.x_zero = prm->x_is_zero;
         a.sub_mean = prm->subtract_mean;
         a.write_bp = prm->write_block_pressure;
+        a.reset = prm->use_bicg ? 0 : (prm->residual_reset_steps > 0 ? prm->residual_reset_steps : 0);
         a.info = info + c0;
         a.nrhs = nrhs_total;
         void (*kern)(KArgs<T>) = nullptr;
         if (prm->use_bicg) {
             a.r = vec[0]; a.rw = vec[1]; a.p0 = vec[2]; a.p1 = vec[3]; a.v0 = vec[4]; a.v1 = vec[5]; a.t = vec[6];
             kern = nr == 1 ? k_bicgstab<T, D, 1, TRANS> : (nr == 2 ? k_bicgstab<T, D, 2, TRANS> : k_bicgstab<T, D, 3, TRANS>);
-        } else if (prm->variant == 1) {
+        } else if (prm->variant == 1 && a.reset == 0) {
             a.r = vec[0]; a.rw = vec[1]; a.p0 = vec[2]; a.p1 = vec[3]; a.v0 = vec[4]; a.v1 = vec[5]; a.t = vec[6];
             kern = k_cg1<T, D, TRANS>;
         } else {
