@@ -341,6 +341,7 @@ def run_pict(args, rank, world):
     wl = build_workload(args.workload, rank)
     doms = wl["domains"]
     batch = BatchDomain(doms, time_steps=wl["dts"])
+    batch.pack_state()  # block fields as views of two contiguous tensors: one host copy per field
     kw = dict(time_step=float(wl["dts"][0]), corrector_steps=wl["correctors"], advection_tol=wl["tol"],
               pressure_tol=wl["tol"], max_iterations=5000, **precision_kwargs(args, wl))
     tuned = None
@@ -585,29 +586,27 @@ def roofline_pass(st, batch, args, dev):
 
 def e2e_pass(st, batch, args, dev, cells, world):
     import torch
-    blocks = batch.getBlocks()
-    host_v = [torch.empty(b.velocity.shape, dtype=b.velocity.dtype, pin_memory=True) for b in blocks]
-    host_p = [torch.empty(b.pressure.shape, dtype=b.pressure.dtype, pin_memory=True) for b in blocks]
-    for hv, hp, b in zip(host_v, host_p, blocks):
-        hv.copy_(b.velocity)
-        hp.copy_(b.pressure)
+    # the batch state (all blocks' velocity and pressure) lives in two contiguous device tensors
+    # (BatchDomain.pack_state), so each direction is two copies per step
+    dev_state = [batch.velocity_arena, batch.pressure_arena]
+    host_state = [torch.empty(t.shape, dtype=t.dtype, pin_memory=True) for t in dev_state]
+    for h, t in zip(host_state, dev_state):
+        h.copy_(t)
     torch.cuda.synchronize()
-    h2d = sum(h.numel() * h.element_size() for h in host_v + host_p)
+    h2d = sum(h.numel() * h.element_size() for h in host_state)
     steps = max(1, min(args.steps, 20))
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(steps):
-        for hv, hp, b in zip(host_v, host_p, blocks):
-            b.velocity.copy_(hv, non_blocking=True)
-            b.pressure.copy_(hp, non_blocking=True)
+        for h, t in zip(host_state, dev_state):
+            t.copy_(h, non_blocking=True)
         if args.no_graph:
             st.step()
         else:
             st.replay()
-        for hv, hp, b in zip(host_v, host_p, blocks):
-            hv.copy_(b.velocity, non_blocking=True)
-            hp.copy_(b.pressure, non_blocking=True)
+        for h, t in zip(host_state, dev_state):
+            h.copy_(t, non_blocking=True)
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)

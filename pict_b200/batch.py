@@ -160,6 +160,32 @@ class BatchDomain:
         P._check(len(nus) == self.num_sims, "one viscosity per batched domain")
         self._sim_visc.copy_(torch.tensor([float(nus[i]) for i in self.order], dtype=self._dtype))
 
+    def pack_state(self):
+        """Place the velocity and the pressure of every block of the batch in one contiguous device tensor
+        each (batch block order, each block's field contiguous inside), and make the blocks' fields views
+        of them.  The member domains stay usable on their own; the whole batch state then moves between
+        host and device in one copy per field and direction instead of one per block.  Returns
+        (velocity_arena, pressure_arena)."""
+        blocks = self.getBlocks()
+        opts = dict(dtype=self._dtype, device=self._device)
+        va = torch.empty(sum(b.velocity.numel() for b in blocks), **opts)
+        pa = torch.empty(sum(b.pressure.numel() for b in blocks), **opts)
+        ov = op = 0
+        for b in blocks:
+            n = b.velocity.numel()
+            v = va[ov:ov + n].view(b.velocity.shape)
+            v.copy_(b.velocity)
+            b.setVelocity(v)
+            ov += n
+            n = b.pressure.numel()
+            p = pa[op:op + n].view(b.pressure.shape)
+            p.copy_(b.pressure)
+            b.setPressure(p)
+            op += n
+        self.velocity_arena, self.pressure_arena = va, pa
+        self.UpdateDomainData()
+        return va, pa
+
     def UpdateDomainData(self):
         """Re-pack after member tensors were replaced (pointers change)."""
         for d in self.domains:

@@ -76,3 +76,35 @@ def test_many_uneven_systems_single_reduction_cg():
             st.step()
         adv, ps = st.check()
         assert all(i.status == 0 for i in adv) and all(i.status == 0 for p in ps for i in p)
+
+
+def test_packed_batch_state_gives_the_same_steps():
+    """BatchDomain.pack_state moves the blocks' fields into two contiguous tensors (views): the batched
+    steps are unchanged, the member domains see the state through their blocks, and one copy of the
+    arenas moves the whole state."""
+    from pict_b200.batch import BatchDomain
+    from pict_b200.engine import PISOStepper
+    specs = [lid_cavity(n, viscosity=v) for n, v in [(20, 1e-2), (33, 2e-3)]] + [case("twoblock2d")]
+    dts = [0.01, 0.008, 0.01]
+    plain = [build_product(s, torch.float32) for s in specs]
+    packed = [build_product(s, torch.float32) for s in specs]
+    b1 = BatchDomain(plain, time_steps=dts)
+    b2 = BatchDomain(packed, time_steps=dts)
+    va, pa = b2.pack_state()
+    assert va.numel() == sum(b.velocity.numel() for b in b2.getBlocks())
+    s1 = PISOStepper(b1, time_step=dts[0], advection_tol=1e-6, pressure_tol=1e-6)
+    s2 = PISOStepper(b2, time_step=dts[0], advection_tol=1e-6, pressure_tol=1e-6)
+    for _ in range(3):
+        s1.step()
+        s2.step()
+    s1.check()
+    s2.check()
+    for d1, d2 in zip(plain, packed):
+        for x1, x2 in zip(d1.getBlocks(), d2.getBlocks()):
+            assert np.array_equal(_np(x1.velocity), _np(x2.velocity))
+            assert np.array_equal(_np(x1.pressure), _np(x2.pressure))
+    host = va.cpu()
+    va.zero_()
+    assert all(float(b.velocity.abs().max()) == 0.0 for b in b2.getBlocks())
+    va.copy_(host.cuda())
+    assert np.array_equal(_np(packed[0].getBlocks()[0].velocity), _np(plain[0].getBlocks()[0].velocity))
