@@ -156,6 +156,10 @@ typedef struct pict_solve_params {
     int32_t residual_reset_steps; /* CG only: > 0 restarts the iteration (r = b - A x, p = r) before every
                                      iteration i with (i+1) % residual_reset_steps == 0, as residualResetSteps
                                      of extensions/cg_solver_kernel.cu:266-286; runs the classic order (variant 0) */
+    int32_t return_best_result;   /* CG only: keep the iterate with the lowest criterion and return it when the
+                                     solve stops unconverged (at max_iterations, or after 100 iterations of a
+                                     non-falling criterion), reporting its iteration and criterion
+                                     (returnBestResult, extensions/cg_solver_kernel.cu:330-413); classic order */
     double tolerance;
 } pict_solve_params_t;
 

@@ -1429,9 +1429,11 @@ def _crit(r):
     return float(np.sqrt(np.dot(r, r)) / math.sqrt(r.shape[0]))
 
 
-def cg(A, b, x0=None, tol=1e-5, maxit=5000, dtype=np.float64, reset=0):
-    """cgSolveGPU without rank-deficiency or best-result, extensions/cg_solver_kernel.cu:236-427; `reset` > 0 restarts
-    the iteration (r = b - A x, p = r) before every iteration i with (i+1) % reset == 0 (:266-286)."""
+def cg(A, b, x0=None, tol=1e-5, maxit=5000, dtype=np.float64, reset=0, return_best=False):
+    """cgSolveGPU without rank-deficiency, extensions/cg_solver_kernel.cu:236-427; `reset` > 0 restarts the iteration
+    (r = b - A x, p = r) before every iteration i with (i+1) % reset == 0 (:266-286); `return_best` keeps the
+    iterate of the lowest criterion and returns it, with its iteration and criterion, when the solve stops
+    unconverged at maxit or after 100 iterations of a non-falling criterion (:330-413)."""
     b = np.asarray(b, dtype=dtype)
     x = np.zeros_like(b) if x0 is None else np.array(x0, dtype=dtype)
     A = A.astype(dtype)
@@ -1439,6 +1441,7 @@ def cg(A, b, x0=None, tol=1e-5, maxit=5000, dtype=np.float64, reset=0):
     p = r.copy()
     rho = float(np.dot(r, r))
     info = SolveInfo(0.0, -1, False, True)
+    best, best_it, best_x, last, rising = 0.0, -1, x, 0.0, 0
     for i in range(maxit):
         if reset > 0 and (i + 1) % reset == 0:
             r = b - A @ x
@@ -1452,10 +1455,17 @@ def cg(A, b, x0=None, tol=1e-5, maxit=5000, dtype=np.float64, reset=0):
         crit = _crit(r)
         if not math.isfinite(crit):
             return x, SolveInfo(crit, i, False, False)
+        if return_best:
+            if i == 0 or crit < best:
+                best, best_it, best_x = crit, i, x.copy()
+            rising = rising + 1 if (i > 0 and crit >= last) else 0
+            last = crit
         info = SolveInfo(crit, i, False, True)
         if crit < tol:
             info.converged = True
             break
+        if return_best and (i == maxit - 1 or rising >= 100):
+            return best_x, SolveInfo(best, best_it, False, True)
         rhop = rho
         rho = float(np.dot(r, r))
         with np.errstate(divide="ignore", invalid="ignore"):

@@ -2468,7 +2468,8 @@ class _Workspace:
 
 
 def _solve_params(nrhs, maxit, tol, conv, use_bicg, transpose, x_zero=False, subtract_mean=False,
-                  write_block_pressure=False, group_size=0, threads=0, variant=0, residual_reset=0):
+                  write_block_pressure=False, group_size=0, threads=0, variant=0, residual_reset=0,
+                  return_best=False):
     p = SolveParams()
     p.max_iterations = int(maxit)
     p.use_bicg = int(bool(use_bicg))
@@ -2482,6 +2483,7 @@ def _solve_params(nrhs, maxit, tol, conv, use_bicg, transpose, x_zero=False, sub
     p.write_block_pressure = int(bool(write_block_pressure))
     p.variant = int(variant)
     p.residual_reset_steps = max(int(residual_reset), 0)
+    p.return_best_result = int(bool(return_best))
     p.tolerance = float(tol)
     return p
 
@@ -2537,8 +2539,6 @@ def SolveLinear(A, RHS, x, maxIterations=1000, tolerance=1e-8, convergenceCriter
         raise NotImplementedError("only NORM2 and NORM2_NORMALIZED convergence criteria are implemented in pict_b200")
     if matrixRankDeficient:
         raise NotImplementedError("matrixRankDeficient is not implemented in pict_b200")
-    if returnBestResult:
-        _warn_once("best", "returnBestResult is not implemented in pict_b200; the final iterate is returned")
     if useBiCG and BiCGwithPreconditioner:
         _warn_once("ilu", "ILU preconditioning is not implemented in pict_b200; BiCGStab runs unpreconditioned")
     if domain.IsTensorChanged():
@@ -2553,7 +2553,8 @@ def SolveLinear(A, RHS, x, maxIterations=1000, tolerance=1e-8, convergenceCriter
         infos = decode_infos(info)
     else:
         for k in range(nb):
-            p = _solve_params(1, maxit, tol, conv, False, transposeA, residual_reset=int(residualResetSteps))
+            p = _solve_params(1, maxit, tol, conv, False, transposeA, residual_reset=int(residualResetSteps),
+                              return_best=bool(returnBestResult))
             info = solve_stencil(domain, coef, RHS[k * n:(k + 1) * n], x[k * n:(k + 1) * n], p)
             infos.extend(decode_infos(info))
     if printResidual:

@@ -148,6 +148,7 @@ class SolveParams(ctypes.Structure):
         ("write_block_pressure", c_i32),
         ("variant", c_i32),
         ("residual_reset_steps", c_i32),
+        ("return_best_result", c_i32),
         ("tolerance", ctypes.c_double),
     ]
 

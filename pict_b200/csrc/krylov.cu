@@ -81,6 +81,8 @@ struct KArgs {
     int sub_mean;
     int write_bp;
     int reset;  // CG: restart period (0: none)
+    int best;   // CG: keep and return the best iterate
+    T* xbest;
 };
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -294,6 +296,9 @@ __global__ void __launch_bounds__(KR_THREADS, 2) k_cg(KArgs<T> a) {
     __shared__ double s_rho[KR_SLOTS], s_beta[KR_SLOTS], s_alpha[KR_SLOTS];
     __shared__ unsigned s_active;  // bit per slot
     __shared__ pict_solve_info_t s_info[KR_SLOTS];
+    __shared__ double s_best[KR_SLOTS], s_last[KR_SLOTS];
+    __shared__ int s_best_it[KR_SLOTS], s_rising[KR_SLOTS];
+    __shared__ unsigned s_save, s_restore;
     load_slots(dom, S);
     __shared__ int s_ctrl[3];
     unsigned epoch = 0;
@@ -453,6 +458,7 @@ __global__ void __launch_bounds__(KR_THREADS, 2) k_cg(KArgs<T> a) {
         if (threadIdx.x < 32) {
             const int j = threadIdx.x;
             bool act = j < S.n && ((s_active >> j) & 1u);
+            bool save = false, restore = false;
             if (act) {
                 const double rr = s_sum[j][0];
                 const double crit = conv_crit(rr, a.normalized, S.ncell[j]);
@@ -460,10 +466,26 @@ __global__ void __launch_bounds__(KR_THREADS, 2) k_cg(KArgs<T> a) {
                 s_info[j].final_residual = crit;
                 bool fin = false;
                 if (!isfinite(crit)) { s_info[j].finite = 0; fin = true; }
-                else if (crit < a.tol) { s_info[j].converged = 1; fin = true; }
                 else {
-                    s_beta[j] = rr / s_rho[j];
-                    s_rho[j] = rr;
+                    if (a.best) {  // extensions/cg_solver_kernel.cu:330-346
+                        if (it == 0 || crit < s_best[j]) {
+                            s_best[j] = crit;
+                            s_best_it[j] = it;
+                            save = true;
+                        }
+                        s_rising[j] = (it > 0 && crit >= s_last[j]) ? s_rising[j] + 1 : 0;
+                        s_last[j] = crit;
+                    }
+                    if (crit < a.tol) { s_info[j].converged = 1; fin = true; }
+                    else if (a.best && (it == a.maxit - 1 || s_rising[j] >= 100)) {  // :399-413
+                        restore = true;
+                        s_info[j].used_iterations = s_best_it[j];
+                        s_info[j].final_residual = s_best[j];
+                        fin = true;
+                    } else {
+                        s_beta[j] = rr / s_rho[j];
+                        s_rho[j] = rr;
+                    }
                 }
                 if (fin) {
                     act = false;
@@ -471,9 +493,26 @@ __global__ void __launch_bounds__(KR_THREADS, 2) k_cg(KArgs<T> a) {
                 }
             }
             const unsigned m = __ballot_sync(0xffffffffu, act);
-            if (j == 0) s_active = m;
+            const unsigned ms = __ballot_sync(0xffffffffu, save);
+            const unsigned mr = __ballot_sync(0xffffffffu, restore);
+            if (j == 0) {
+                s_active = m;
+                s_save = ms;
+                s_restore = mr;
+            }
         }
         __syncthreads();
+        if (a.best && (s_save | s_restore)) {
+            // this CTA's tiles of the system: keep x as the best iterate / put the best iterate back
+            for (int j = 0; j < S.n; ++j) {
+                const bool sv = (s_save >> j) & 1u, rs = (s_restore >> j) & 1u;
+                if (!sv && !rs) continue;
+                for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) {
+                    if (sv) a.xbest[i] = x[i];
+                    if (rs) x[i] = a.xbest[i];
+                }
+            }
+        }
         T* tmp = pc; pc = pn; pn = tmp;
     }
     // ---- mean removal (PISOtorch_simulation.py:1243-1244) and copy into the blocks' pressure
@@ -1109,7 +1148,8 @@ static size_t vec_bytes(const pict_domain_t* dom, const pict_solve_params_t* prm
 }
 
 static size_t workspace_total(const pict_domain_t* dom, const pict_solve_params_t* prm) {
-    const int nvec = (prm->use_bicg || prm->variant == 1) ? 7 : 4;  // bicg / cg1: 7 vectors; cg: r p0 p1 q
+    // bicg / cg1: 7 vectors; cg: r p0 p1 q (+ the best iterate)
+    const int nvec = (prm->use_bicg || prm->variant == 1) ? 7 : (prm->return_best_result ? 5 : 4);
     return header_bytes(dom) + vec_bytes(dom, prm) * nvec;
 }
 
@@ -1155,7 +1195,7 @@ static pict_status_t run_solve(const pict_domain_t* dom, const void* coef, const
     double* partials = reinterpret_cast<double*>(base + align256(256));
     const size_t off = header_bytes(dom);
     const size_t vb = vec_bytes(dom, prm);
-    const int nvec = (prm->use_bicg || prm->variant == 1) ? 7 : 4;
+    const int nvec = (prm->use_bicg || prm->variant == 1) ? 7 : (prm->return_best_result ? 5 : 4);
     T* vec[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     for (int k = 0; k < nvec; ++k) vec[k] = reinterpret_cast<T*>(base + off + vb * k);
 
@@ -1184,18 +1224,22 @@ static pict_status_t run_solve(const pict_domain_t* dom, const void* coef, const
         a.sub_mean = prm->subtract_mean;
         a.write_bp = prm->write_block_pressure;
         a.reset = prm->use_bicg ? 0 : (prm->residual_reset_steps > 0 ? prm->residual_reset_steps : 0);
+        a.best = prm->use_bicg ? 0 : (prm->return_best_result ? 1 : 0);
+        a.xbest = nullptr;
         a.info = info + c0;
         a.nrhs = nrhs_total;
         void (*kern)(KArgs<T>) = nullptr;
         if (prm->use_bicg) {
             a.r = vec[0]; a.rw = vec[1]; a.p0 = vec[2]; a.p1 = vec[3]; a.v0 = vec[4]; a.v1 = vec[5]; a.t = vec[6];
             kern = nr == 1 ? k_bicgstab<T, D, 1, TRANS> : (nr == 2 ? k_bicgstab<T, D, 2, TRANS> : k_bicgstab<T, D, 3, TRANS>);
-        } else if (prm->variant == 1 && a.reset == 0) {
+        } else if (prm->variant == 1 && a.reset == 0 && a.best == 0) {
             a.r = vec[0]; a.rw = vec[1]; a.p0 = vec[2]; a.p1 = vec[3]; a.v0 = vec[4]; a.v1 = vec[5]; a.t = vec[6];
             kern = k_cg1<T, D, TRANS>;
         } else {
             a.r = vec[0]; a.p0 = vec[1]; a.p1 = vec[2]; a.t = vec[3];
             a.rw = nullptr; a.v0 = nullptr; a.v1 = nullptr;
+            if (a.best) a.xbest = vec[4];
+            if (a.best && !a.xbest) return set_error(PICT_ERR_ARG, "solve: no workspace vector for the best iterate");
             kern = k_cg<T, D, TRANS>;
         }
         // grid: every CTA owns at most KR_SLOTS tiles; all CTAs must be co-resident
