@@ -347,7 +347,7 @@ def build_oracle(spec) -> po.ODomain:
     return d
 
 
-def build_product(spec, dtype=None, device="cuda", module=None):
+def build_product(spec, dtype=None, device="cuda", module=None, prepare=True):
     """Build through the PISOtorch API of `module` (default: pict_b200.PISOtorch; the reference's own
     compiled module has the same API and is used by tests/golden/make_ref_fixtures.py)."""
     import torch
@@ -400,5 +400,115 @@ def build_product(spec, dtype=None, device="cuda", module=None):
             blocks[op[1]].ConnectBlock(op[2], blocks[op[3]], op[4], *op[5:])
         else:
             raise KeyError(op[0])
-    dom.PrepareSolve()
+    if prepare:
+        dom.PrepareSolve()
     return dom
+
+
+# ------------------------------------------------------------------ multi-block CNN structures
+
+MBCNN_CASES = ["grid2x2_2d", "rotated_chain2d", "periodic_layers2d", "swapped3d", "chain1d"]
+# 3D layouts whose connections cycle all three axes (the reference's MultiblockConv cannot pad these)
+MBCNN_CYCLE_CASES = ["rotated3d"]
+
+
+def mbcnn_case(name):
+    """Block layouts for the multi-block convolution: sizes and boundary operations only (fields zero)."""
+    def spec(dims, sizes, ops):
+        return dict(dims=dims, viscosity=1e-3, blocks=[dict(size=s) for s in sizes], ops=ops)
+
+    if name == "grid2x2_2d":
+        return spec(2, [[6, 5], [4, 5], [6, 7], [4, 7]],
+                    [("close_all", b) for b in range(4)] +
+                    [("connect", 0, "+x", 1, "-x", "-y"), ("connect", 0, "+y", 2, "-y", "-x"),
+                     ("connect", 1, "+y", 3, "-y", "-x"), ("connect", 2, "+x", 3, "-x", "-y")])
+    if name == "rotated_chain2d":
+        # +x of block 0 meets +y of block 1 with the axis inverted; -x of block 1 meets -y of block 2
+        return spec(2, [[5, 6], [6, 4], [7, 4]],
+                    [("close_all", b) for b in range(3)] +
+                    [("connect", 0, "+x", 1, "+y", "+x"), ("connect", 1, "-x", 2, "+x", "-y")])
+    if name == "periodic_layers2d":
+        return spec(2, [[8, 4], [8, 5]],
+                    [("periodic", 0, "x"), ("periodic", 1, "x"), ("close", 0, "-y"), ("close", 1, "+y"),
+                     ("connect", 0, "+y", 1, "-y", "-x")])
+    if name == "swapped3d":
+        # +x of block 0 meets -z of block 1 with x and z swapped; +y of block 0 meets -y of block 2 with z inverted
+        return spec(3, [[4, 5, 6], [6, 5, 3], [4, 3, 6]],
+                    [("close_all", b) for b in range(3)] +
+                    [("connect", 0, "+x", 1, "-z", "-y", "-x"), ("connect", 0, "+y", 2, "-y", "+z", "-x"),
+                     ("periodic", 2, "z")])
+    if name == "rotated3d":
+        # +x of block 0 meets -y of block 1 with the axes cycled (y -> z inverted, z -> x)
+        return spec(3, [[4, 5, 6], [6, 4, 5], [4, 4, 6]],
+                    [("close_all", b) for b in range(3)] +
+                    [("connect", 0, "+x", 1, "-y", "+z", "-x"), ("connect", 0, "+y", 2, "-y", "-z", "-x"),
+                     ("periodic", 2, "z")])
+    if name == "chain1d":
+        return spec(1, [[6], [5], [7]],
+                    [("close_all", b) for b in range(3)] +
+                    [("connect", 0, "+x", 1, "-x"), ("connect", 1, "+x", 2, "-x"), ("connect", 2, "+x", 0, "-x")])
+    raise KeyError(name)
+
+
+class _StandInSizes:
+    def __init__(self, size):
+        s = list(size) + [1] * (3 - len(size))
+        self.x, self.y, self.z, self.w = s[0], s[1], s[2], s[0] * s[1] * s[2]
+
+    def __getitem__(self, i):
+        return [self.x, self.y, self.z, self.w][i]
+
+
+class _StandInBoundary:
+    def __init__(self, btype, block=None, axes=None):
+        self.type = btype
+        self._block = block
+        self.axes = axes
+
+    def getConnectedBlock(self):
+        return self._block
+
+
+class _StandInBlock:
+    def __init__(self, dims, size):
+        self._dims = dims
+        self._sizes = _StandInSizes(size)
+        self.boundaries = []
+
+    def getSpatialDims(self):
+        return self._dims
+
+    def getSizes(self):
+        return self._sizes
+
+    def getBoundaries(self):
+        return list(self.boundaries)
+
+
+class _StandInDomain:
+    def __init__(self, dims, blocks):
+        self._dims = dims
+        self._blocks = blocks
+
+    def getSpatialDims(self):
+        return self._dims
+
+    def getBlocks(self):
+        return list(self._blocks)
+
+
+def build_structure(spec, boundary_type):
+    """Host-only object graph with the domain accessors a multi-block convolution reads (block sizes, boundary
+    types, connected blocks and axes), built from the oracle's domain so that connection axes are those of
+    ConnectBlock.  ``boundary_type`` is the BoundaryType enum whose FIXED / CONNECTED / PERIODIC tag the faces."""
+    od = build_oracle(spec)
+    blocks = [_StandInBlock(spec["dims"], ob.size) for ob in od.blocks]
+    for blk, ob in zip(blocks, od.blocks):
+        for bnd in ob.boundaries:
+            if bnd.kind == "fixed":
+                blk.boundaries.append(_StandInBoundary(boundary_type.FIXED))
+            elif bnd.kind == "connected":
+                blk.boundaries.append(_StandInBoundary(boundary_type.CONNECTED, blocks[bnd.block], list(bnd.axes)))
+            else:
+                blk.boundaries.append(_StandInBoundary(boundary_type.PERIODIC))
+    return _StandInDomain(spec["dims"], blocks)
