@@ -145,7 +145,8 @@ typedef struct pict_solve_params {
     int32_t nrhs;              /* right-hand sides per system sharing the matrix (BiCG: D components) */
     int32_t x_is_zero;         /* 1: skip the initial A*x (x must hold zeros) */
     int32_t transpose;         /* solve with A^T (adjoint solves) */
-    int32_t convergence;       /* PICT_CONV_*; only NORM2 and NORM2_NORMALIZED are supported */
+    int32_t convergence;       /* PICT_CONV_* (ComputeConvergenceCriterion, extensions/cg_solver_kernel.cu:77-110);
+                                  the ABS criteria with CG only (classic order) */
     int32_t group_size;        /* upper bound of CTAs of the persistent launch (0: automatic) */
     int32_t threads;           /* threads per CTA (0: automatic) */
     int32_t subtract_mean;     /* 1: x -= mean(x) per system after the solve (PISOtorch_simulation.py:1243-1244) */
@@ -160,6 +161,9 @@ typedef struct pict_solve_params {
                                      solve stops unconverged (at max_iterations, or after 100 iterations of a
                                      non-falling criterion), reporting its iteration and criterion
                                      (returnBestResult, extensions/cg_solver_kernel.cu:330-413); classic order */
+    int32_t rank_deficient;       /* CG only: iterate with the reference's rank-deficient operator A v + s |v|_1 e,
+                                     s = sum |diag A| / n^3 per system, and initial residual b - A x + s |x|_1 e
+                                     (matrixRankDeficient, extensions/cg_solver_kernel.cu:240-298); classic order */
     double tolerance;
 } pict_solve_params_t;
 

@@ -1429,30 +1429,61 @@ def _crit(r):
     return float(np.sqrt(np.dot(r, r)) / math.sqrt(r.shape[0]))
 
 
-def cg(A, b, x0=None, tol=1e-5, maxit=5000, dtype=np.float64, reset=0, return_best=False):
-    """cgSolveGPU without rank-deficiency, extensions/cg_solver_kernel.cu:236-427; `reset` > 0 restarts the iteration
+def criterion(r, conv="NORM2_NORMALIZED"):
+    """ComputeConvergenceCriterion, extensions/cg_solver_kernel.cu:77-110."""
+    n = r.size
+    if conv == "NORM2":
+        return float(np.linalg.norm(r))
+    if conv == "NORM2_NORMALIZED":
+        return float(np.linalg.norm(r)) / math.sqrt(n)
+    if conv == "ABS_SUM":
+        return float(np.abs(r).sum())
+    if conv == "ABS_MEAN":
+        return float(np.abs(r).sum()) / n
+    if conv == "ABS_MAX":
+        return float(np.abs(r).max())
+    raise KeyError(conv)
+
+
+def cg(A, b, x0=None, tol=1e-5, maxit=5000, dtype=np.float64, reset=0, return_best=False, conv="NORM2_NORMALIZED",
+       rank_deficient=False):
+    """cgSolveGPU, extensions/cg_solver_kernel.cu:236-427; `reset` > 0 restarts the iteration
     (r = b - A x, p = r) before every iteration i with (i+1) % reset == 0 (:266-286); `return_best` keeps the
     iterate of the lowest criterion and returns it, with its iteration and criterion, when the solve stops
-    unconverged at maxit or after 100 iterations of a non-falling criterion (:330-413)."""
+    unconverged at maxit or after 100 iterations of a non-falling criterion (:330-413); `conv` names the
+    convergence criterion (:77-110).  `rank_deficient` uses the reference's operator for singular Laplacians
+    (:240-298): with s = sum |diag A| / n^3, A p is replaced by A p + s |p|_1 e and the (re)started residual
+    is b - A x + s |x|_1 e (that sign, as the reference computes it)."""
     b = np.asarray(b, dtype=dtype)
     x = np.zeros_like(b) if x0 is None else np.array(x0, dtype=dtype)
     A = A.astype(dtype)
-    r = b - A @ x
+    n = b.size
+    s = float(np.abs(A.diagonal()).sum()) / n / n / n if rank_deficient else 0.0
+
+    def residual(x):
+        r = b - A @ x
+        if rank_deficient:
+            r = r + s * float(np.abs(x).sum())
+        return r
+
+    r = residual(x)
     p = r.copy()
     rho = float(np.dot(r, r))
     info = SolveInfo(0.0, -1, False, True)
     best, best_it, best_x, last, rising = 0.0, -1, x, 0.0, 0
     for i in range(maxit):
         if reset > 0 and (i + 1) % reset == 0:
-            r = b - A @ x
+            r = residual(x)
             p = r.copy()
             rho = float(np.dot(r, r))
         q = A @ p
+        if rank_deficient:
+            q = q + s * float(np.abs(p).sum())
         with np.errstate(divide="ignore", invalid="ignore"):  # a vanishing p.q gives inf / nan, as on the device
             alpha = np.float64(rho) / np.float64(np.dot(p, q))
         x = x + alpha * p
         r = r - alpha * q
-        crit = _crit(r)
+        crit = criterion(r, conv)
         if not math.isfinite(crit):
             return x, SolveInfo(crit, i, False, False)
         if return_best:

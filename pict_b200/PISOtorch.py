@@ -22,8 +22,10 @@ Scope: the PISO path (orthogonal, and the non-orthogonal terms of ``nonOrthoFlag
 periodic and connected block boundaries, per-cell transforms, block/global
 viscosity and velocity sources, in 2D and 3D, float32 and float64, with the gradients of all of it;
 velocity correctors 0/1 (finite differences), 4, 5 and 6 (finite volumes); passive scalar transport
-with its raw gradient operators.  Face-transform pressure assembly and ILU preconditioning raise
-``NotImplementedError``.
+with its raw gradient operators.  ``SolveLinear``'s CG takes every ``ConvergenceCriterion``, residual
+resets, ``returnBestResult`` and ``matrixRankDeficient``; BiCGStab takes the NORM2 criteria.  Face-transform
+pressure assembly and the ABS criteria with BiCGStab raise ``NotImplementedError``; ILU preconditioning is
+not built (BiCGStab runs unpreconditioned, with a warning).
 """
 from __future__ import annotations
 
@@ -2469,7 +2471,7 @@ class _Workspace:
 
 def _solve_params(nrhs, maxit, tol, conv, use_bicg, transpose, x_zero=False, subtract_mean=False,
                   write_block_pressure=False, group_size=0, threads=0, variant=0, residual_reset=0,
-                  return_best=False):
+                  return_best=False, rank_deficient=False):
     p = SolveParams()
     p.max_iterations = int(maxit)
     p.use_bicg = int(bool(use_bicg))
@@ -2484,6 +2486,7 @@ def _solve_params(nrhs, maxit, tol, conv, use_bicg, transpose, x_zero=False, sub
     p.variant = int(variant)
     p.residual_reset_steps = max(int(residual_reset), 0)
     p.return_best_result = int(bool(return_best))
+    p.rank_deficient = int(bool(rank_deficient))
     p.tolerance = float(tol)
     return p
 
@@ -2535,10 +2538,9 @@ def SolveLinear(A, RHS, x, maxIterations=1000, tolerance=1e-8, convergenceCriter
     maxit = int(_as_scalar(maxIterations))
     tol = float(_as_scalar(tolerance))
     conv = int(convergenceCriterion)
-    if conv not in (0, 1):
-        raise NotImplementedError("only NORM2 and NORM2_NORMALIZED convergence criteria are implemented in pict_b200")
-    if matrixRankDeficient:
-        raise NotImplementedError("matrixRankDeficient is not implemented in pict_b200")
+    _check(0 <= conv <= 4, "Unknown convergence criterion.")
+    if useBiCG and conv >= int(ConvergenceCriterion.ABS_SUM):
+        raise NotImplementedError("BiCGStab in pict_b200 takes the NORM2 and NORM2_NORMALIZED criteria (CG takes all)")
     if useBiCG and BiCGwithPreconditioner:
         _warn_once("ilu", "ILU preconditioning is not implemented in pict_b200; BiCGStab runs unpreconditioned")
     if domain.IsTensorChanged():
@@ -2554,7 +2556,7 @@ def SolveLinear(A, RHS, x, maxIterations=1000, tolerance=1e-8, convergenceCriter
     else:
         for k in range(nb):
             p = _solve_params(1, maxit, tol, conv, False, transposeA, residual_reset=int(residualResetSteps),
-                              return_best=bool(returnBestResult))
+                              return_best=bool(returnBestResult), rank_deficient=bool(matrixRankDeficient))
             info = solve_stencil(domain, coef, RHS[k * n:(k + 1) * n], x[k * n:(k + 1) * n], p)
             infos.extend(decode_infos(info))
     if printResidual:

@@ -149,6 +149,7 @@ class SolveParams(ctypes.Structure):
         ("variant", c_i32),
         ("residual_reset_steps", c_i32),
         ("return_best_result", c_i32),
+        ("rank_deficient", c_i32),
         ("tolerance", ctypes.c_double),
     ]
 

@@ -83,11 +83,19 @@ struct KArgs {
     int reset;  // CG: restart period (0: none)
     int best;   // CG: keep and return the best iterate
     T* xbest;
+    int abs_crit;  // classic CG: 0 NORM2 criteria, else PICT_CONV_ABS_SUM / _MEAN / _MAX
+    int rankdef;   // classic CG: operator A + s |.|_1 e (matrixRankDeficient)
 };
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
     return v;
 }
 
@@ -157,12 +165,13 @@ struct PhaseRed {
     double v[KR_SLOTS][KR_THREADS / 32][KR_NV];
 };
 
-template <int NV>
+// Component MAXK (if >= 0) is combined by maximum instead of sum (ABS_MAX criterion).
+template <int NV, int MAXK = -1>
 __device__ __forceinline__ void warp_partial(PhaseRed& R, int slot, const double (&acc)[NV]) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int k = 0; k < NV; ++k) {
-        const double w = warp_sum(acc[k]);
+        const double w = k == MAXK ? warp_max(acc[k]) : warp_sum(acc[k]);
         if (lane == 0) R.v[slot][warp][k] = w;
     }
 }
@@ -204,7 +213,7 @@ __device__ void load_slots(const pict_domain_t& dom, TileSlots& S) {
 
 // Sum the tile partials of each slot's system (one warp per slot, fixed order) into out[slot][k].
 // Only slots whose bit is set in `mask` are reduced.
-template <int NV>
+template <int NV, int MAXK = -1>
 __device__ void system_sums(const double* partials, const TileSlots& S, unsigned mask, double (*out)[KR_NV]) {
     const int lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
     for (int j = threadIdx.x >> 5; j < S.n; j += nwarps) {
@@ -214,11 +223,14 @@ __device__ void system_sums(const double* partials, const TileSlots& S, unsigned
         for (int k = 0; k < NV; ++k) acc[k] = 0.0;
         for (int t = S.t0[j] + lane; t < S.t1[j]; t += 32) {
 #pragma unroll
-            for (int k = 0; k < NV; ++k) acc[k] += __ldcg(partials + (size_t)t * KR_NV + k);
+            for (int k = 0; k < NV; ++k) {
+                const double v = __ldcg(partials + (size_t)t * KR_NV + k);
+                acc[k] = k == MAXK ? fmax(acc[k], v) : acc[k] + v;
+            }
         }
 #pragma unroll
         for (int k = 0; k < NV; ++k) {
-            const double s = warp_sum(acc[k]);
+            const double s = k == MAXK ? warp_max(acc[k]) : warp_sum(acc[k]);
             if (lane == 0) out[j][k] = s;
         }
     }
@@ -226,14 +238,14 @@ __device__ void system_sums(const double* partials, const TileSlots& S, unsigned
 }
 
 // Sum the warp partials of the slots in `mask` and write the tile partials (fixed order).
-template <int NV>
+template <int NV, int MAXK = -1>
 __device__ __forceinline__ void flush_partials(PhaseRed& R, const TileSlots& S, unsigned mask, double* partials) {
     __syncthreads();
     const int nwarps = blockDim.x >> 5;
     const int j = threadIdx.x / NV, k = threadIdx.x % NV;
     if (j < S.n && ((mask >> j) & 1u)) {
         double s = 0.0;
-        for (int w = 0; w < nwarps; ++w) s += R.v[j][w][k];
+        for (int w = 0; w < nwarps; ++w) s = k == MAXK ? fmax(s, R.v[j][w][k]) : s + R.v[j][w][k];
         partials[(size_t)S.tile[j] * KR_NV + k] = s;
     }
 }
@@ -273,6 +285,14 @@ __device__ __forceinline__ double conv_crit(double sq, int normalized, int n) {
     return normalized ? nrm / sqrt((double)n) : nrm;
 }
 
+// ComputeConvergenceCriterion (extensions/cg_solver_kernel.cu:77-110): abs = sum |r| (ABS_SUM, ABS_MEAN) or
+// max |r| (ABS_MAX); sq = r.r for the NORM2 criteria.
+__device__ __forceinline__ double conv_crit_any(double sq, double abs, int abs_crit, int normalized, int n) {
+    if (abs_crit == PICT_CONV_ABS_MEAN) return abs / (double)n;
+    if (abs_crit == PICT_CONV_ABS_SUM || abs_crit == PICT_CONV_ABS_MAX) return abs;
+    return conv_crit(sq, normalized, n);
+}
+
 __device__ __forceinline__ pict_solve_info_t fresh_info() {
     pict_solve_info_t inf;
     inf.final_residual = 0.0;
@@ -299,6 +319,7 @@ __global__ void __launch_bounds__(KR_THREADS, 2) k_cg(KArgs<T> a) {
     __shared__ double s_best[KR_SLOTS], s_last[KR_SLOTS];
     __shared__ int s_best_it[KR_SLOTS], s_rising[KR_SLOTS];
     __shared__ unsigned s_save, s_restore;
+    __shared__ double s_rds[KR_SLOTS], s_rdc[KR_SLOTS];  // rank-deficient scale s and constant s |v|_1
     load_slots(dom, S);
     __shared__ int s_ctrl[3];
     unsigned epoch = 0;
@@ -313,17 +334,41 @@ __global__ void __launch_bounds__(KR_THREADS, 2) k_cg(KArgs<T> a) {
     double* part = a.partials;
     const size_t pstride = (size_t)dom.num_tiles * KR_NV;
 
+    // ---- matrixRankDeficient (extensions/cg_solver_kernel.cu:240-253): s = sum |diag| / n^3 per system and
+    // the constant s |x|_1 that the reference adds to b - A x
+    if (a.rankdef) {
+        for (int j = 0; j < S.n; ++j) {
+            double acc[2] = {0.0, 0.0};
+            for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) {
+                acc[0] += fabs((double)coef[i]);
+                if (!a.x_zero) acc[1] += fabs((double)x[i]);
+            }
+            warp_partial<2>(R, j, acc);
+        }
+        flush_partials<2>(R, S, 0xffffffffu, part + phase * pstride);
+        if (!grid_barrier(a.ctrl, epoch, s_ctrl)) return;
+        system_sums<2>(part + phase * pstride, S, 0xffffffffu, s_sum);
+        phase ^= 1;
+        if ((int)threadIdx.x < S.n) {
+            const double n = (double)S.ncell[threadIdx.x];
+            s_rds[threadIdx.x] = s_sum[threadIdx.x][0] / n / n / n;
+            s_rdc[threadIdx.x] = s_rds[threadIdx.x] * s_sum[threadIdx.x][1];
+        }
+        __syncthreads();
+    }
     // ---- initial residual r = b - A x, |r|^2, |b|^2 per tile
     for (int j = 0; j < S.n; ++j) {
         const pict_block_t& B = dom.blocks[S.block[j]];
         double acc[2] = {0.0, 0.0};
         const int s0 = S.start[j], s1 = s0 + S.count[j];
+        const T rdc = a.rankdef ? (T)s_rdc[j] : T(0);
         for (int i = s0 + threadIdx.x; i < s1; i += blockDim.x) {
             int p[3];
             unflatten(i - B.offset, B.size, p);
             const T bi = bv[i];
             T ri = bi;
             if (!a.x_zero) ri -= spmv_row<T, D, TRANS>(dom, coef, N, i, B, p, [&](int jj) { return x[jj]; });
+            if (a.rankdef) ri += rdc;
             r[i] = ri;
             pc[i] = T(0);
             acc[0] += (double)ri * (double)ri;
@@ -364,14 +409,30 @@ __global__ void __launch_bounds__(KR_THREADS, 2) k_cg(KArgs<T> a) {
     for (int it = 0; it < a.maxit; ++it) {
         // restart (residualResetSteps, extensions/cg_solver_kernel.cu:266-286): r = b - A x, p = r, rho = r.r
         if (a.reset > 0 && (it + 1) % a.reset == 0) {
+            if (a.rankdef) {  // s |x|_1 for the restarted residual
+                for (int j = 0; j < S.n; ++j) {
+                    if (!((s_active >> j) & 1u)) continue;
+                    double acc[1] = {0.0};
+                    for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x)
+                        acc[0] += fabs((double)x[i]);
+                    warp_partial<1>(R, j, acc);
+                }
+                flush_partials<1>(R, S, s_active, part + phase * pstride);
+                if (!grid_barrier(a.ctrl, epoch, s_ctrl)) return;
+                system_sums<1>(part + phase * pstride, S, s_active, s_sum);
+                phase ^= 1;
+                if ((int)threadIdx.x < S.n) s_rdc[threadIdx.x] = s_rds[threadIdx.x] * s_sum[threadIdx.x][0];
+                __syncthreads();
+            }
             for (int j = 0; j < S.n; ++j) {
                 if (!((s_active >> j) & 1u)) continue;
                 const pict_block_t& B = dom.blocks[S.block[j]];
                 double acc[1] = {0.0};
+                const T rdc = a.rankdef ? (T)s_rdc[j] : T(0);
                 for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) {
                     int p[3];
                     unflatten(i - B.offset, B.size, p);
-                    const T ri = bv[i] - spmv_row<T, D, TRANS>(dom, coef, N, i, B, p, [&](int jj) { return x[jj]; });
+                    const T ri = bv[i] - spmv_row<T, D, TRANS>(dom, coef, N, i, B, p, [&](int jj) { return x[jj]; }) + rdc;
                     r[i] = ri;
                     acc[0] += (double)ri * (double)ri;
                 }
@@ -392,7 +453,7 @@ __global__ void __launch_bounds__(KR_THREADS, 2) k_cg(KArgs<T> a) {
             if (!((s_active >> j) & 1u)) continue;
             const pict_block_t& B = dom.blocks[S.block[j]];
             const T bt = (T)s_beta[j];
-            double acc[1] = {0.0};
+            double acc[3] = {0.0, 0.0, 0.0};
             const int s0 = S.start[j], cnt = S.count[j];
             for (int base = 0; base < cnt; base += KR_PASS) {
                 T pi[KR_U], qi[KR_U];
@@ -412,24 +473,39 @@ __global__ void __launch_bounds__(KR_THREADS, 2) k_cg(KArgs<T> a) {
                         pn[s0 + l] = pi[k];
                         q[s0 + l] = qi[k];
                         acc[0] += (double)pi[k] * (double)qi[k];
+                        if (a.rankdef) {
+                            acc[1] += fabs((double)pi[k]);
+                            acc[2] += (double)pi[k];
+                        }
                     }
                 }
             }
-            warp_partial<1>(R, j, acc);
+            if (a.rankdef) warp_partial<3>(R, j, acc);
+            else warp_partial<1>(R, j, reinterpret_cast<const double(&)[1]>(acc));
         }
-        flush_partials<1>(R, S, s_active, part + phase * pstride);
+        if (a.rankdef) flush_partials<3>(R, S, s_active, part + phase * pstride);
+        else flush_partials<1>(R, S, s_active, part + phase * pstride);
         if (!grid_barrier(a.ctrl, epoch, s_ctrl)) return;
         if (s_ctrl[0] == dom.num_sims) break;
-        system_sums<1>(part + phase * pstride, S, s_active, s_sum);
+        if (a.rankdef) system_sums<3>(part + phase * pstride, S, s_active, s_sum);
+        else system_sums<1>(part + phase * pstride, S, s_active, s_sum);
         phase ^= 1;
-        if ((int)threadIdx.x < S.n && ((s_active >> threadIdx.x) & 1u))
-            s_alpha[threadIdx.x] = s_rho[threadIdx.x] / s_sum[threadIdx.x][0];
+        if ((int)threadIdx.x < S.n && ((s_active >> threadIdx.x) & 1u)) {
+            const int j = threadIdx.x;
+            double pq = s_sum[j][0];
+            if (a.rankdef) {  // q = A p + s |p|_1 e (extensions/cg_solver_kernel.cu:293-298): p.q gains s |p|_1 sum(p)
+                s_rdc[j] = s_rds[j] * s_sum[j][1];
+                pq += s_rdc[j] * s_sum[j][2];
+            }
+            s_alpha[j] = s_rho[j] / pq;
+        }
         __syncthreads();
         // phase 2: x += alpha p, r -= alpha q, r.r
         for (int j = 0; j < S.n; ++j) {
             if (!((s_active >> j) & 1u)) continue;
             const T al = (T)s_alpha[j];
-            double acc[1] = {0.0};
+            const T rdc = a.rankdef ? (T)s_rdc[j] : T(0);
+            double acc[2] = {0.0, 0.0};
             const int s0 = S.start[j], cnt = S.count[j];
             for (int base = 0; base < cnt; base += KR_PASS) {
                 T xi[KR_U], ri[KR_U];
@@ -437,7 +513,7 @@ __global__ void __launch_bounds__(KR_THREADS, 2) k_cg(KArgs<T> a) {
                 for (int k = 0; k < KR_U; ++k) {
                     const int i = s0 + min(base + (int)threadIdx.x + k * KR_THREADS, cnt - 1);
                     xi[k] = x[i] + al * pn[i];
-                    ri[k] = r[i] - al * q[i];
+                    ri[k] = a.rankdef ? r[i] - al * (q[i] + rdc) : r[i] - al * q[i];
                 }
 #pragma unroll
                 for (int k = 0; k < KR_U; ++k) {
@@ -446,14 +522,24 @@ __global__ void __launch_bounds__(KR_THREADS, 2) k_cg(KArgs<T> a) {
                         x[s0 + l] = xi[k];
                         r[s0 + l] = ri[k];
                         acc[0] += (double)ri[k] * (double)ri[k];
+                        if (a.abs_crit) {
+                            const double v = fabs((double)ri[k]);
+                            acc[1] = a.abs_crit == PICT_CONV_ABS_MAX ? fmax(acc[1], v) : acc[1] + v;
+                        }
                     }
                 }
             }
-            warp_partial<1>(R, j, acc);
+            if (a.abs_crit == PICT_CONV_ABS_MAX) warp_partial<2, 1>(R, j, acc);
+            else if (a.abs_crit) warp_partial<2>(R, j, acc);
+            else warp_partial<1>(R, j, reinterpret_cast<const double(&)[1]>(acc));
         }
-        flush_partials<1>(R, S, s_active, part + phase * pstride);
+        if (a.abs_crit == PICT_CONV_ABS_MAX) flush_partials<2, 1>(R, S, s_active, part + phase * pstride);
+        else if (a.abs_crit) flush_partials<2>(R, S, s_active, part + phase * pstride);
+        else flush_partials<1>(R, S, s_active, part + phase * pstride);
         if (!grid_barrier(a.ctrl, epoch, s_ctrl)) return;
-        system_sums<1>(part + phase * pstride, S, s_active, s_sum);
+        if (a.abs_crit == PICT_CONV_ABS_MAX) system_sums<2, 1>(part + phase * pstride, S, s_active, s_sum);
+        else if (a.abs_crit) system_sums<2>(part + phase * pstride, S, s_active, s_sum);
+        else system_sums<1>(part + phase * pstride, S, s_active, s_sum);
         phase ^= 1;
         if (threadIdx.x < 32) {
             const int j = threadIdx.x;
@@ -461,7 +547,7 @@ __global__ void __launch_bounds__(KR_THREADS, 2) k_cg(KArgs<T> a) {
             bool save = false, restore = false;
             if (act) {
                 const double rr = s_sum[j][0];
-                const double crit = conv_crit(rr, a.normalized, S.ncell[j]);
+                const double crit = conv_crit_any(rr, s_sum[j][1], a.abs_crit, a.normalized, S.ncell[j]);
                 s_info[j].used_iterations = it;
                 s_info[j].final_residual = crit;
                 bool fin = false;
@@ -1226,13 +1312,15 @@ static pict_status_t run_solve(const pict_domain_t* dom, const void* coef, const
         a.reset = prm->use_bicg ? 0 : (prm->residual_reset_steps > 0 ? prm->residual_reset_steps : 0);
         a.best = prm->use_bicg ? 0 : (prm->return_best_result ? 1 : 0);
         a.xbest = nullptr;
+        a.abs_crit = prm->convergence >= PICT_CONV_ABS_SUM ? prm->convergence : 0;
+        a.rankdef = prm->use_bicg ? 0 : (prm->rank_deficient ? 1 : 0);
         a.info = info + c0;
         a.nrhs = nrhs_total;
         void (*kern)(KArgs<T>) = nullptr;
         if (prm->use_bicg) {
             a.r = vec[0]; a.rw = vec[1]; a.p0 = vec[2]; a.p1 = vec[3]; a.v0 = vec[4]; a.v1 = vec[5]; a.t = vec[6];
             kern = nr == 1 ? k_bicgstab<T, D, 1, TRANS> : (nr == 2 ? k_bicgstab<T, D, 2, TRANS> : k_bicgstab<T, D, 3, TRANS>);
-        } else if (prm->variant == 1 && a.reset == 0 && a.best == 0) {
+        } else if (prm->variant == 1 && a.reset == 0 && a.best == 0 && a.abs_crit == 0 && a.rankdef == 0) {
             a.r = vec[0]; a.rw = vec[1]; a.p0 = vec[2]; a.p1 = vec[3]; a.v0 = vec[4]; a.v1 = vec[5]; a.t = vec[6];
             kern = k_cg1<T, D, TRANS>;
         } else {
@@ -1332,8 +1420,12 @@ pict_status_t pict_solve(const pict_domain_t* dom, const void* coef, const void*
         return set_error(PICT_ERR_ARG, "solve: domain is not prepared");
     if (prm->nrhs < 1) return set_error(PICT_ERR_ARG, "solve: nrhs must be >= 1");
     if (prm->max_iterations < 0) return set_error(PICT_ERR_ARG, "solve: max_iterations must be >= 0");
-    if (!(prm->convergence == PICT_CONV_NORM2 || prm->convergence == PICT_CONV_NORM2_NORMALIZED))
-        return set_error(PICT_ERR_UNSUPPORTED, "solve: only NORM2 and NORM2_NORMALIZED convergence criteria are supported");
+    if (prm->convergence < PICT_CONV_NORM2 || prm->convergence > PICT_CONV_ABS_MAX)
+        return set_error(PICT_ERR_ARG, "solve: unknown convergence criterion");
+    if (prm->use_bicg && prm->convergence >= PICT_CONV_ABS_SUM)
+        return set_error(PICT_ERR_UNSUPPORTED, "solve: BiCGStab takes the NORM2 and NORM2_NORMALIZED criteria");
+    if (prm->use_bicg && prm->rank_deficient)
+        return set_error(PICT_ERR_UNSUPPORTED, "solve: rank_deficient applies to CG only");
     if (prm->variant != 0 && (prm->use_bicg || prm->variant != 1))
         return set_error(PICT_ERR_ARG, "solve: variant 1 (single-reduction) applies to CG only");
     if (!prm->use_bicg && prm->nrhs != 1)

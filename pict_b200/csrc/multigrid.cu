@@ -1030,6 +1030,8 @@ pict_status_t pict_pcg_mg(const pict_domain_t* dom, const pict_mg_level_t* level
     if (levels[0].num_cells != dom->num_cells || levels[0].num_blocks != dom->num_blocks || !dom->tiles ||
         dom->num_tiles <= 0)
         return set_error(PICT_ERR_ARG, "pcg_mg: level 0 must describe the domain (and tiles are needed)");
+    if (!(convergence == PICT_CONV_NORM2 || convergence == PICT_CONV_NORM2_NORMALIZED))
+        return set_error(PICT_ERR_UNSUPPORTED, "pcg_mg: takes the NORM2 and NORM2_NORMALIZED criteria");
     cudaStream_t st = (cudaStream_t)stream;
     const int norm = convergence == PICT_CONV_NORM2_NORMALIZED;
     char* ws = reinterpret_cast<char*>(workspace);
