@@ -145,16 +145,19 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden"))
     ap.add_argument("--quick", action="store_true")
+    ap.add_argument("--cases", nargs="*", default=None, help="only the operator fixtures of these setups")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
     R = ref_module()
     from setups import ALL_CASES
     summary = {}
-    for name in ALL_CASES:
+    for name in (ALL_CASES if args.cases is None else args.cases):
         fx = op_fixtures(R, name)
         np.savez_compressed(os.path.join(args.out, "ref_ops_%s.npz" % name), **fx)
         summary[name] = "ok"
         print("fixture", name, flush=True)
+    if args.cases is not None:
+        return
     timings = {}
     for (n, steps, dtype, tol, tag) in [(64, 100, torch.float32, 1e-6, "lid64_f32"), (64, 100, torch.float64, 1e-10, "lid64_f64")]:
         fx = lid_fixture(R, n, steps, dtype, tol)

@@ -147,6 +147,22 @@ def case(name, seed=0):
                             dict(coords=c2, velocity=_rand_field(rng, (1, 3, nz, ny, nx2), 0.3))],
                     ops=[("close_all", 0), ("close_all", 1), ("connect", 0, "+x", 1, "-x", "-y", "-z"),
                          ("close", 0, "+y", np.array([[1.0, 0.0, 0.0]]))])
+    if name == "ring4_2d":
+        # flow around a cylinder on an O-grid cut into four quarter blocks that connect in a ring (x clockwise
+        # around the cylinder, y radial, tanh-stretched towards the wall), no-slip on the cylinder and a
+        # uniform stream u = (1, 0) prescribed on the outer circle
+        na, nr = 6, 5
+        radii = 0.5 + stretched(nr, 1.5, 1.4, both=False)
+        blocks = []
+        for q in range(4):
+            th = np.linspace(np.pi / 2 * (4 - q), np.pi / 2 * (3 - q), na + 1)
+            R, TH = np.meshgrid(radii, th, indexing="ij")
+            coords = np.stack([R * np.cos(TH), R * np.sin(TH)])[None]
+            blocks.append(dict(coords=coords, velocity=_rand_field(rng, (1, 2, nr, na), 0.2)))
+        ops = [("close_all", q) for q in range(4)]
+        ops += [("connect", q, "+x", (q + 1) % 4, "-x", "-y") for q in range(4)]
+        ops += [("close", q, "+y", np.array([[1.0, 0.0]])) for q in range(4)]
+        return dict(dims=2, viscosity=2e-2, blocks=blocks, ops=ops)
     if name == "skewed_channel2d":
         # periodic in x, walls at +-y, skew growing with y (non-orthogonal at the upper wall)
         nx, ny = 10, 8
@@ -270,7 +286,7 @@ def scalar_case(name, seed=0):
 
 
 CASES_2D = ["cavity2d", "cavity2d_refined", "distorted2d", "periodic2d", "fullperiodic2d", "inflow2d", "twoblock2d",
-            "twoblock2d_rotated"]
+            "twoblock2d_rotated", "ring4_2d"]
 CASES_3D = ["channel3d", "cavity3d", "twoblock3d"]
 ALL_CASES = CASES_2D + CASES_3D
 
