@@ -238,12 +238,13 @@ def sample_indices(sides, k):
 
 def precision_kwargs(args, wl=None):
     """mixed: FP32 stencils / vectors, FP64 reductions and one FP64 refinement sweep of every pressure
-    solve to an RMS residual of 1e-9, pressure solves warm-started from the latest pressure; fp32: the
-    single FP32 pressure solve from zero (the reference's order)."""
+    solve to an RMS residual of 1e-9, pressure solves warm-started from the latest pressure and (unless
+    --warm-advection 0) advection solves from the current velocity; fp32: the single FP32 pressure solve
+    from zero (the reference's order)."""
     if args.precision == "mixed":
         return {"pressure_refine": 1, "refine_tol": (wl or {}).get("refine_tol", 1e-9), "warm_start_pressure": True,
                 "refine_solver": args.refine_solver, "pressure_first_solve": bool(args.first_solve),
-                "mg_iterations": args.mg_iterations}
+                "mg_iterations": args.mg_iterations, "warm_start_advection": bool(args.warm_advection)}
     return {}
 
 
@@ -459,7 +460,7 @@ def run_pict(args, rank, world):
             "config": {"workload": args.workload, "simulations": len(doms), "cells_per_gpu": cells,
                        "pass": "forward", "solver_tol": wl["tol"], "correctors": wl["correctors"],
                        "precision": args.precision + (" (FP32 fields and Krylov vectors, FP64 reductions, one FP64 "
-                                                      "refinement sweep of each pressure solve (multigrid-preconditioned CG corrections on near-isotropic grids), warm-started pressure solves)"
+                                                      "refinement sweep of each pressure solve (multigrid-preconditioned CG corrections on near-isotropic grids), warm-started pressure solves" + (", advection solves from the current velocity" if args.warm_advection else "") + ")"
                                                       if args.precision == "mixed" else " (FP32, FP64 reductions)"),
                        "cuda_graph": not args.no_graph, "l2": "working set > L2 (126 MB), no flush",
                        "autotune": tuned, "tile_cells": batch.tile_cells,
@@ -858,6 +859,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="pict", choices=["pict", "reference"])
+    ap.add_argument("--warm-advection", type=int, default=1,
+                    help="mixed precision: start each advection solve from the current velocity (1) or from zero (0)")
     ap.add_argument("--workload", default="batched_cavities_256",
                     choices=["batched_cavities_256", "lid_cavity_64", "channel3d_192"])
     ap.add_argument("--group-size", type=int, default=0)

@@ -49,7 +49,8 @@ class PISOStepper:
                  pressure_tol: Optional[float] = None, max_iterations: int = 5000, adv_group_size: int = 0,
                  p_group_size: int = 0, threads: int = 0, normalize_pressure: bool = True, cg_variant: int = 1,
                  pressure_refine: int = 0, refine_tol: Optional[float] = None, warm_start_pressure: bool = False,
-                 refine_solver: str = "cg", mg_iterations: int = 12, pressure_first_solve: bool = True):
+                 refine_solver: str = "cg", mg_iterations: int = 12, pressure_first_solve: bool = True,
+                 warm_start_advection: bool = False):
         self.domain = domain
         self.dims = domain.getSpatialDims()
         self.corrector_steps = int(corrector_steps)
@@ -59,8 +60,12 @@ class PISOStepper:
         self.max_iterations = int(max_iterations)
         self.normalize_pressure = normalize_pressure
         self.time_step = time_step
+        # warm start of the advection solve from the blocks' velocity (advect_use_prev_result of
+        # PISOtorch_simulation.py:1189): the same solution to the tolerance, fewer BiCGStab iterations
+        self.warm_start_advection = bool(warm_start_advection)
         self.adv_params = P._solve_params(self.dims, self.max_iterations, self.adv_tol, _lib.PICT_CONV_NORM2_NORMALIZED,
-                                          True, False, x_zero=True, group_size=adv_group_size, threads=threads)
+                                          True, False, x_zero=not self.warm_start_advection, group_size=adv_group_size,
+                                          threads=threads)
         # mixed precision: `pressure_refine` FP64 refinement sweeps after the first pressure solve, each
         # solving the correction of the FP64 residual to `refine_tol`
         self.pressure_refine = int(pressure_refine)
@@ -165,6 +170,8 @@ class PISOStepper:
         dt = self._dt(time_step)
         D = self.dims
         check(lib.pict_setup_advection(desc, dt, st), "advection setup")
+        if self.warm_start_advection:
+            check(lib.pict_copy_velocity_result_from_blocks(desc, st), "advection initial guess")
         check(lib.pict_solve(desc, P._ptr(d.C.coef), P._ptr(d.velocityRHS), P._ptr(d.velocityResult),
                              ctypes.byref(self.adv_params), P._ptr(self.info_adv), P._ptr(self.ws), self.ws_bytes, st),
               "advection solve")
@@ -250,6 +257,8 @@ class PISOStepper:
             return e
 
         check(lib.pict_setup_advection(desc, dt, st), "advection setup")
+        if self.warm_start_advection:
+            check(lib.pict_copy_velocity_result_from_blocks(desc, st), "advection initial guess")
         a = ev()
         check(lib.pict_solve(desc, P._ptr(d.C.coef), P._ptr(d.velocityRHS), P._ptr(d.velocityResult),
                              ctypes.byref(self.adv_params), P._ptr(self.info_adv), P._ptr(self.ws), self.ws_bytes, st),
