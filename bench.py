@@ -450,6 +450,8 @@ def run_pict(args, rank, world):
                "sample": "sides %s x 2 PISO steps each (FP64 NumPy/SciPy restatement, %.1f s)" % (
                    [int(wl["sides"][i]) for i in sel], tt)}
     iters_ref = [[max(i.usedIterations for i in r) for r in row] for row in st.refine_infos()]
+    # RMS residual of the FP32 correction solve relative to its right-hand side is what the iteration cap bounds
+    res_ref = [[max(float(i.finalResidual) for i in r) for r in row] for row in st.refine_infos()]
     iters_adv = [i.usedIterations for i in adv_infos]
     iters_p = [[i.usedIterations for i in p] for p in p_infos]
     if rank == 0:
@@ -477,7 +479,7 @@ def run_pict(args, rank, world):
             "solver_iterations": {"advection_max": int(max(iters_adv)), "advection_mean": float(np.mean(iters_adv)),
                                   "pressure_max": [int(max(p)) for p in iters_p],
                                   "pressure_mean": [float(np.mean(p)) for p in iters_p],
-                                  "refinement_max": iters_ref},
+                                  "refinement_max": iters_ref, "refinement_final_residual_max": res_ref},
         }
         print(json.dumps(line), flush=True)
 
