@@ -217,8 +217,8 @@ class PISOStepper:
     def kernels_per_step(self):
         """Kernels of this library launched per step: advection setup 1; per solve init-info, solver and
         finish-info 3; per corrector pressure setup 2 (matrix/RHS, divergence), correction 1, and the
-        refinement sweeps when enabled."""
-        n = 1 + 3
+        refinement sweeps when enabled; the copy of the initial guess of a warm-started advection solve 1."""
+        n = 1 + 3 + (1 if self.warm_start_advection else 0)
         n += self.corrector_steps * (2 + (3 if self.pressure_first_solve else 0) + 1)
         if self.pressure_refine > 0:  # per sweep: residual (+2 projection), solve, update; partials + finish
             if self._mg is not None:
