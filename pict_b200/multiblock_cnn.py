@@ -121,9 +121,8 @@ class MultiblockConv(torch.nn.Module):
             n += int(torch.tensor(s).prod())
         self._zero_index = n
         idx = [self._gather_index(bi, blocks, offsets) for bi in range(len(blocks))]
-        for bi, t in enumerate(idx):
-            self.register_buffer("_gather_%d" % bi, t, persistent=False)
-        self._num_blocks = len(blocks)
+        for bi, t in enumerate(idx):  # moved with the module by .to() / .cuda()
+            self.register_buffer("_gather_%d" % bi, t if device is None else t.to(device), persistent=False)
         self.conv_layer = conv(in_channels, out_channels, kernel_size, stride=stride, padding=0, dilation=dilation,
                                groups=groups, bias=bias, padding_mode=padding_mode, device=device, dtype=dtype)
 
@@ -228,7 +227,9 @@ class MultiblockConv(torch.nn.Module):
                          [torch.zeros(batch, ch, 1, dtype=ref.dtype, device=ref.device)], dim=2)
         out = []
         for bi in range(len(tensor_list)):
-            idx = getattr(self, "_gather_%d" % bi).to(ref.device)
+            idx = getattr(self, "_gather_%d" % bi)
+            if idx.device != ref.device:
+                idx = idx.to(ref.device)
             shape = [s + 2 * self.padding for s in self._shapes[bi]]
             out.append(flat.index_select(2, idx).reshape([batch, ch] + shape))
         return out
