@@ -1505,8 +1505,9 @@ def cg(A, b, x0=None, tol=1e-5, maxit=5000, dtype=np.float64, reset=0, return_be
     return x, info
 
 
-def bicgstab(A, b, x0=None, tol=1e-5, maxit=5000, dtype=np.float64):
-    """bicgstabSolveGPU without preconditioner, extensions/bicgstab_solver_kernel.cu:240-360."""
+def bicgstab(A, b, x0=None, tol=1e-5, maxit=5000, dtype=np.float64, conv="NORM2_NORMALIZED"):
+    """bicgstabSolveGPU without preconditioner, extensions/bicgstab_solver_kernel.cu:240-360; `conv` names the
+    convergence criterion (ComputeConvergenceCriterion, extensions/cg_solver_kernel.cu:77-110)."""
     b = np.asarray(b, dtype=dtype)
     x = np.zeros_like(b) if x0 is None else np.array(x0, dtype=dtype)
     A = A.astype(dtype)
@@ -1514,7 +1515,7 @@ def bicgstab(A, b, x0=None, tol=1e-5, maxit=5000, dtype=np.float64):
     rw = r.copy()
     p = r.copy()
     v = np.zeros_like(b)
-    nrmr0 = _crit(r)
+    nrmr0 = criterion(r, conv)
     if nrmr0 < tol:
         return x, SolveInfo(nrmr0, -1, True, True)
     rho = 0.0
@@ -1532,7 +1533,7 @@ def bicgstab(A, b, x0=None, tol=1e-5, maxit=5000, dtype=np.float64):
             alpha = f64(rho) / f64(np.dot(rw, v))
         r = r - alpha * v
         x = x + alpha * p
-        nrmr = _crit(r)
+        nrmr = criterion(r, conv)
         if not math.isfinite(nrmr):
             return x, SolveInfo(nrmr, i, False, False)
         info = SolveInfo(nrmr, i, False, True)
@@ -1545,7 +1546,7 @@ def bicgstab(A, b, x0=None, tol=1e-5, maxit=5000, dtype=np.float64):
             omega = f64(np.dot(t, r)) / f64(np.dot(t, t))
         x = x + omega * s
         r = r - omega * t
-        nrmr = _crit(r)
+        nrmr = criterion(r, conv)
         info.finalResidual = nrmr
         if nrmr < tol:
             info = SolveInfo(nrmr, i + 1, True, True)

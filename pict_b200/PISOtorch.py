@@ -23,9 +23,9 @@ periodic and connected block boundaries, per-cell transforms, block/global
 viscosity and velocity sources, in 2D and 3D, float32 and float64, with the gradients of all of it;
 velocity correctors 0/1 (finite differences), 4, 5 and 6 (finite volumes); passive scalar transport
 with its raw gradient operators.  ``SolveLinear``'s CG takes every ``ConvergenceCriterion``, residual
-resets, ``returnBestResult`` and ``matrixRankDeficient``; BiCGStab takes the NORM2 criteria.  Face-transform
-pressure assembly and the ABS criteria with BiCGStab raise ``NotImplementedError``; ILU preconditioning is
-not built (BiCGStab runs unpreconditioned, with a warning).
+resets, ``returnBestResult`` and ``matrixRankDeficient``; BiCGStab takes every criterion too.  Face-transform
+pressure assembly raises ``NotImplementedError``; ILU preconditioning is not built (BiCGStab runs
+unpreconditioned, with a warning).
 """
 from __future__ import annotations
 
@@ -2539,8 +2539,6 @@ def SolveLinear(A, RHS, x, maxIterations=1000, tolerance=1e-8, convergenceCriter
     tol = float(_as_scalar(tolerance))
     conv = int(convergenceCriterion)
     _check(0 <= conv <= 4, "Unknown convergence criterion.")
-    if useBiCG and conv >= int(ConvergenceCriterion.ABS_SUM):
-        raise NotImplementedError("BiCGStab in pict_b200 takes the NORM2 and NORM2_NORMALIZED criteria (CG takes all)")
     if useBiCG and BiCGwithPreconditioner:
         _warn_once("ilu", "ILU preconditioning is not implemented in pict_b200; BiCGStab runs unpreconditioned")
     if domain.IsTensorChanged():

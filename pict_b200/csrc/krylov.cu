@@ -165,13 +165,13 @@ struct PhaseRed {
     double v[KR_SLOTS][KR_THREADS / 32][KR_NV];
 };
 
-// Component MAXK (if >= 0) is combined by maximum instead of sum (ABS_MAX criterion).
-template <int NV, int MAXK = -1>
+// Components whose bit is set in MAXMASK are combined by maximum instead of sum (ABS_MAX criterion).
+template <int NV, unsigned MAXMASK = 0u>
 __device__ __forceinline__ void warp_partial(PhaseRed& R, int slot, const double (&acc)[NV]) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int k = 0; k < NV; ++k) {
-        const double w = k == MAXK ? warp_max(acc[k]) : warp_sum(acc[k]);
+        const double w = ((MAXMASK >> k) & 1u) ? warp_max(acc[k]) : warp_sum(acc[k]);
         if (lane == 0) R.v[slot][warp][k] = w;
     }
 }
@@ -213,7 +213,7 @@ __device__ void load_slots(const pict_domain_t& dom, TileSlots& S) {
 
 // Sum the tile partials of each slot's system (one warp per slot, fixed order) into out[slot][k].
 // Only slots whose bit is set in `mask` are reduced.
-template <int NV, int MAXK = -1>
+template <int NV, unsigned MAXMASK = 0u>
 __device__ void system_sums(const double* partials, const TileSlots& S, unsigned mask, double (*out)[KR_NV]) {
     const int lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
     for (int j = threadIdx.x >> 5; j < S.n; j += nwarps) {
@@ -225,12 +225,12 @@ __device__ void system_sums(const double* partials, const TileSlots& S, unsigned
 #pragma unroll
             for (int k = 0; k < NV; ++k) {
                 const double v = __ldcg(partials + (size_t)t * KR_NV + k);
-                acc[k] = k == MAXK ? fmax(acc[k], v) : acc[k] + v;
+                acc[k] = ((MAXMASK >> k) & 1u) ? fmax(acc[k], v) : acc[k] + v;
             }
         }
 #pragma unroll
         for (int k = 0; k < NV; ++k) {
-            const double s = k == MAXK ? warp_max(acc[k]) : warp_sum(acc[k]);
+            const double s = ((MAXMASK >> k) & 1u) ? warp_max(acc[k]) : warp_sum(acc[k]);
             if (lane == 0) out[j][k] = s;
         }
     }
@@ -238,14 +238,14 @@ __device__ void system_sums(const double* partials, const TileSlots& S, unsigned
 }
 
 // Sum the warp partials of the slots in `mask` and write the tile partials (fixed order).
-template <int NV, int MAXK = -1>
+template <int NV, unsigned MAXMASK = 0u>
 __device__ __forceinline__ void flush_partials(PhaseRed& R, const TileSlots& S, unsigned mask, double* partials) {
     __syncthreads();
     const int nwarps = blockDim.x >> 5;
     const int j = threadIdx.x / NV, k = threadIdx.x % NV;
     if (j < S.n && ((mask >> j) & 1u)) {
         double s = 0.0;
-        for (int w = 0; w < nwarps; ++w) s = k == MAXK ? fmax(s, R.v[j][w][k]) : s + R.v[j][w][k];
+        for (int w = 0; w < nwarps; ++w) s = ((MAXMASK >> k) & 1u) ? fmax(s, R.v[j][w][k]) : s + R.v[j][w][k];
         partials[(size_t)S.tile[j] * KR_NV + k] = s;
     }
 }
@@ -291,6 +291,13 @@ __device__ __forceinline__ double conv_crit_any(double sq, double abs, int abs_c
     if (abs_crit == PICT_CONV_ABS_MEAN) return abs / (double)n;
     if (abs_crit == PICT_CONV_ABS_SUM || abs_crit == PICT_CONV_ABS_MAX) return abs;
     return conv_crit(sq, normalized, n);
+}
+
+// One residual entry into the criterion partial: v^2 (NORM2 criteria), |v| (ABS_SUM / ABS_MEAN) or max |v| (ABS_MAX).
+__device__ __forceinline__ void crit_acc(double& acc, double v, int abs_crit) {
+    if (abs_crit == PICT_CONV_ABS_MAX) acc = fmax(acc, fabs(v));
+    else if (abs_crit) acc += fabs(v);
+    else acc += v * v;
 }
 
 __device__ __forceinline__ pict_solve_info_t fresh_info() {
@@ -529,15 +536,15 @@ __global__ void __launch_bounds__(KR_THREADS, 2) k_cg(KArgs<T> a) {
                     }
                 }
             }
-            if (a.abs_crit == PICT_CONV_ABS_MAX) warp_partial<2, 1>(R, j, acc);
+            if (a.abs_crit == PICT_CONV_ABS_MAX) warp_partial<2, 2u>(R, j, acc);
             else if (a.abs_crit) warp_partial<2>(R, j, acc);
             else warp_partial<1>(R, j, reinterpret_cast<const double(&)[1]>(acc));
         }
-        if (a.abs_crit == PICT_CONV_ABS_MAX) flush_partials<2, 1>(R, S, s_active, part + phase * pstride);
+        if (a.abs_crit == PICT_CONV_ABS_MAX) flush_partials<2, 2u>(R, S, s_active, part + phase * pstride);
         else if (a.abs_crit) flush_partials<2>(R, S, s_active, part + phase * pstride);
         else flush_partials<1>(R, S, s_active, part + phase * pstride);
         if (!grid_barrier(a.ctrl, epoch, s_ctrl)) return;
-        if (a.abs_crit == PICT_CONV_ABS_MAX) system_sums<2, 1>(part + phase * pstride, S, s_active, s_sum);
+        if (a.abs_crit == PICT_CONV_ABS_MAX) system_sums<2, 2u>(part + phase * pstride, S, s_active, s_sum);
         else if (a.abs_crit) system_sums<2>(part + phase * pstride, S, s_active, s_sum);
         else system_sums<1>(part + phase * pstride, S, s_active, s_sum);
         phase ^= 1;
@@ -866,9 +873,9 @@ __global__ void __launch_bounds__(KR_THREADS, 2) k_bicgstab(KArgs<T> a) {
     // ---- init: r = b - A x, rw = r, p = v = 0
     for (int j = 0; j < S.n; ++j) {
         const pict_block_t& B = dom.blocks[S.block[j]];
-        double acc[2 * NR];
+        double acc[3 * NR];  // r.r, b.b, and the ABS criterion partial of r
 #pragma unroll
-        for (int k = 0; k < 2 * NR; ++k) acc[k] = 0.0;
+        for (int k = 0; k < 3 * NR; ++k) acc[k] = 0.0;
         for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) {
             int p[3];
             unflatten(i - B.offset, B.size, p);
@@ -884,13 +891,35 @@ __global__ void __launch_bounds__(KR_THREADS, 2) k_bicgstab(KArgs<T> a) {
                 vc[c * NS + i] = T(0);
                 acc[c] += (double)ri * (double)ri;
                 acc[NR + c] += (double)bi * (double)bi;
+                if (a.abs_crit) crit_acc(acc[2 * NR + c], (double)ri, a.abs_crit);
             }
         }
-        warp_partial<2 * NR>(R, j, acc);
+        // the ABS criteria take a third group of partials; the host launches them with NR <= 2 (3 NR <= KR_NV)
+        constexpr unsigned kAbsMax = ((1u << NR) - 1u) << (2 * NR);
+        const double(&acc2)[2 * NR] = reinterpret_cast<const double(&)[2 * NR]>(acc);
+        if constexpr (3 * NR <= KR_NV) {
+            if (a.abs_crit == PICT_CONV_ABS_MAX) warp_partial<3 * NR, kAbsMax>(R, j, acc);
+            else if (a.abs_crit) warp_partial<3 * NR>(R, j, acc);
+            else warp_partial<2 * NR>(R, j, acc2);
+        } else {
+            warp_partial<2 * NR>(R, j, acc2);
+        }
     }
-    flush_partials<2 * NR>(R, S, 0xffffffffu, part + phase * pstride);
+    if constexpr (3 * NR <= KR_NV) {
+        if (a.abs_crit == PICT_CONV_ABS_MAX) flush_partials<3 * NR, ((1u << NR) - 1u) << (2 * NR)>(R, S, 0xffffffffu, part + phase * pstride);
+        else if (a.abs_crit) flush_partials<3 * NR>(R, S, 0xffffffffu, part + phase * pstride);
+        else flush_partials<2 * NR>(R, S, 0xffffffffu, part + phase * pstride);
+    } else {
+        flush_partials<2 * NR>(R, S, 0xffffffffu, part + phase * pstride);
+    }
     if (!grid_barrier(a.ctrl, epoch, s_ctrl)) return;
-    system_sums<2 * NR>(part + phase * pstride, S, 0xffffffffu, s_sum);
+    if constexpr (3 * NR <= KR_NV) {
+        if (a.abs_crit == PICT_CONV_ABS_MAX) system_sums<3 * NR, ((1u << NR) - 1u) << (2 * NR)>(part + phase * pstride, S, 0xffffffffu, s_sum);
+        else if (a.abs_crit) system_sums<3 * NR>(part + phase * pstride, S, 0xffffffffu, s_sum);
+        else system_sums<2 * NR>(part + phase * pstride, S, 0xffffffffu, s_sum);
+    } else {
+        system_sums<2 * NR>(part + phase * pstride, S, 0xffffffffu, s_sum);
+    }
     phase ^= 1;
     if (threadIdx.x < 32) {  // lane j: slot j
         const int j = threadIdx.x;
@@ -907,7 +936,8 @@ __global__ void __launch_bounds__(KR_THREADS, 2) k_bicgstab(KArgs<T> a) {
                     inf.used_iterations = 0;
                     fin = true;
                 } else {
-                    const double nrmr0 = conv_crit(s_sum[j][c], a.normalized, n);
+                    const double nrmr0 = conv_crit_any(s_sum[j][c], a.abs_crit ? s_sum[j][2 * NR + c] : 0.0, a.abs_crit,
+                                                       a.normalized, n);
                     if (nrmr0 < a.tol) {
                         inf.converged = 1;
                         inf.used_iterations = -1;
@@ -1035,15 +1065,18 @@ __global__ void __launch_bounds__(KR_THREADS, 2) k_bicgstab(KArgs<T> a) {
                         if (!((act >> c) & 1u)) continue;
                         r[c * NS + i] = sv[k][c];
                         x[c * NS + i] = xv[k][c];
-                        acc[c] += (double)sv[k][c] * (double)sv[k][c];
+                        crit_acc(acc[c], (double)sv[k][c], a.abs_crit);
                     }
                 }
             }
-            warp_partial<NR>(R, j, acc);
+            if (a.abs_crit == PICT_CONV_ABS_MAX) warp_partial<NR, (1u << NR) - 1u>(R, j, acc);
+            else warp_partial<NR>(R, j, acc);
         }
-        flush_partials<NR>(R, S, s_any, part + phase * pstride);
+        if (a.abs_crit == PICT_CONV_ABS_MAX) flush_partials<NR, (1u << NR) - 1u>(R, S, s_any, part + phase * pstride);
+        else flush_partials<NR>(R, S, s_any, part + phase * pstride);
         if (!grid_barrier(a.ctrl, epoch, s_ctrl)) return;
-        system_sums<NR>(part + phase * pstride, S, s_any, s_sum);
+        if (a.abs_crit == PICT_CONV_ABS_MAX) system_sums<NR, (1u << NR) - 1u>(part + phase * pstride, S, s_any, s_sum);
+        else system_sums<NR>(part + phase * pstride, S, s_any, s_sum);
         phase ^= 1;
         if (threadIdx.x < 32) {
             const int j = threadIdx.x;
@@ -1052,7 +1085,7 @@ __global__ void __launch_bounds__(KR_THREADS, 2) k_bicgstab(KArgs<T> a) {
                 const int n = S.ncell[j];
                 for (int c = 0; c < NR; ++c) {
                     if (!((act >> c) & 1u)) continue;
-                    const double nr = conv_crit(s_sum[j][c], a.normalized, n);
+                    const double nr = conv_crit_any(s_sum[j][c], s_sum[j][c], a.abs_crit, a.normalized, n);
                     s_info[j][c].used_iterations = it;
                     s_info[j][c].final_residual = nr;
                     bool fin = false;
@@ -1154,16 +1187,19 @@ __global__ void __launch_bounds__(KR_THREADS, 2) k_bicgstab(KArgs<T> a) {
                         if (!((act >> c) & 1u)) continue;
                         x[c * NS + i] = xv[k][c];
                         r[c * NS + i] = rv[k][c];
-                        acc[2 * c] += (double)rv[k][c] * (double)rv[k][c];
+                        crit_acc(acc[2 * c], (double)rv[k][c], a.abs_crit);
                         acc[2 * c + 1] += (double)wv[k][c] * (double)rv[k][c];
                     }
                 }
             }
-            warp_partial<2 * NR>(R, j, acc);
+            if (a.abs_crit == PICT_CONV_ABS_MAX) warp_partial<2 * NR, 0x15u>(R, j, acc);
+            else warp_partial<2 * NR>(R, j, acc);
         }
-        flush_partials<2 * NR>(R, S, s_any, part + phase * pstride);
+        if (a.abs_crit == PICT_CONV_ABS_MAX) flush_partials<2 * NR, 0x15u>(R, S, s_any, part + phase * pstride);
+        else flush_partials<2 * NR>(R, S, s_any, part + phase * pstride);
         if (!grid_barrier(a.ctrl, epoch, s_ctrl)) return;
-        system_sums<2 * NR>(part + phase * pstride, S, s_any, s_sum);
+        if (a.abs_crit == PICT_CONV_ABS_MAX) system_sums<2 * NR, 0x15u>(part + phase * pstride, S, s_any, s_sum);
+        else system_sums<2 * NR>(part + phase * pstride, S, s_any, s_sum);
         phase ^= 1;
         if (threadIdx.x < 32) {
             const int j = threadIdx.x;
@@ -1173,7 +1209,7 @@ __global__ void __launch_bounds__(KR_THREADS, 2) k_bicgstab(KArgs<T> a) {
                 for (int c = 0; c < NR; ++c) {
                     if (!((act >> c) & 1u)) continue;
                     s_rwr[j][c] = s_sum[j][2 * c + 1];
-                    const double nr = conv_crit(s_sum[j][2 * c], a.normalized, n);
+                    const double nr = conv_crit_any(s_sum[j][2 * c], s_sum[j][2 * c], a.abs_crit, a.normalized, n);
                     s_info[j][c].final_residual = nr;
                     if (nr < a.tol) {
                         s_info[j][c].converged = 1;
@@ -1225,7 +1261,9 @@ static size_t header_bytes(const pict_domain_t* dom) {
 }
 
 static int nrhs_per_launch(const pict_solve_params_t* prm) {
-    return prm->use_bicg ? (prm->nrhs > 3 ? 3 : prm->nrhs) : 1;
+    // BiCGStab with an ABS criterion keeps a third group of initial partials: at most 2 components per launch
+    const int cap = prm->convergence >= PICT_CONV_ABS_SUM ? 2 : 3;
+    return prm->use_bicg ? (prm->nrhs > cap ? cap : prm->nrhs) : 1;
 }
 
 static size_t vec_bytes(const pict_domain_t* dom, const pict_solve_params_t* prm) {
@@ -1422,8 +1460,6 @@ pict_status_t pict_solve(const pict_domain_t* dom, const void* coef, const void*
     if (prm->max_iterations < 0) return set_error(PICT_ERR_ARG, "solve: max_iterations must be >= 0");
     if (prm->convergence < PICT_CONV_NORM2 || prm->convergence > PICT_CONV_ABS_MAX)
         return set_error(PICT_ERR_ARG, "solve: unknown convergence criterion");
-    if (prm->use_bicg && prm->convergence >= PICT_CONV_ABS_SUM)
-        return set_error(PICT_ERR_UNSUPPORTED, "solve: BiCGStab takes the NORM2 and NORM2_NORMALIZED criteria");
     if (prm->use_bicg && prm->rank_deficient)
         return set_error(PICT_ERR_UNSUPPORTED, "solve: rank_deficient applies to CG only");
     if (prm->variant != 0 && (prm->use_bicg || prm->variant != 1))

@@ -34,6 +34,8 @@ MAXIT = 300
 # (a relative change of 1e-15 in b changes the 300th iterate at order one), so those solves are also recorded
 # after EARLY_MAXIT iterations, where they are still reproducible.
 EARLY_MAXIT = 40
+# BiCGStab (unpreconditioned) on the advection matrix with D seeded right-hand sides
+BICG_CRITERIA = [("NORM2_NORMALIZED", 1e-10), ("ABS_SUM", 1e-8), ("ABS_MEAN", 1e-11)]
 
 
 def rhs_vectors(n, seed):
@@ -70,6 +72,22 @@ def criteria_fixture(R, name, csr=True):
             out["x_" + key] = x.cpu().numpy()
             i = infos[0]
             out["info_" + key] = np.array([i.finalResidual, i.usedIterations, float(i.converged), float(i.isFiniteResidual)])
+    D = dom.getSpatialDims()
+    rb = np.random.default_rng(70 + CRITERIA_CASES.index(name)).standard_normal(D * n)
+    out["b_bicg"] = rb
+    if csr:
+        out["value_C"] = dom.C.value.cpu().numpy()
+        out["index_C"] = dom.C.index.cpu().numpy()
+        out["row_C"] = dom.C.row.cpu().numpy()
+    for conv, tol in BICG_CRITERIA:
+        x = torch.zeros(D * n, dtype=torch.float64, device="cuda")
+        infos = R.SolveLinear(dom.C, torch.tensor(rb, device="cuda"), x, torch.IntTensor([MAXIT]),
+                              torch.tensor([tol], dtype=torch.float64), getattr(R.ConvergenceCriterion, conv),
+                              True, False, 0, False, False, False, BiCGwithPreconditioner=False)
+        torch.cuda.synchronize()
+        out["x_bicg_" + conv] = x.cpu().numpy()
+        out["info_bicg_" + conv] = np.array([[i.finalResidual, i.usedIterations, float(i.converged),
+                                              float(i.isFiniteResidual)] for i in infos])
     return out
 
 

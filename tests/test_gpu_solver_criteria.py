@@ -56,14 +56,38 @@ def test_cg_abs_max_matches_oracle(name, rd):
     assert np.abs(x.cpu().numpy() - x_ref).max() <= 1e-6 * np.abs(x_ref).max()
 
 
-def test_bicgstab_rejects_abs_criteria():
+@pytest.mark.parametrize("name", CASES)
+def test_bicgstab_criteria_match_reference(name):
+    from pict_b200 import PISOtorch as P
+    from test_oracle_criteria_golden import BICG_CRITERIA, check_bicg
+    with np.load(os.path.join(GOLDEN, "ref_criteria_%s.npz" % name)) as z:
+        f = {k: z[k] for k in z.files}
+    ours = criteria_fixture(P, name, csr=False)
+    for conv, _ in BICG_CRITERIA:
+        check_bicg(ours["x_bicg_" + conv], ours["info_bicg_" + conv], f, conv)
+
+
+@pytest.mark.parametrize("name", ["cavity2d_refined", "channel3d"])
+def test_bicgstab_abs_max_matches_oracle(name):
+    """BiCGStab with ABS_MAX (max |r|) against the oracle, every component."""
+    import scipy.sparse as sp
+    import piso_oracle as po
     from pict_b200 import PISOtorch as P
     from setups import build_product, case
-    dom = build_product(case("cavity2d"), torch.float64)
-    ts = torch.tensor([0.05], dtype=torch.float64)
-    P.SetupAdvectionMatrix(dom, ts, 0)
-    n = dom.C.getRows()
-    x = torch.zeros(2 * n, dtype=torch.float64, device="cuda")
-    with pytest.raises(NotImplementedError):
-        P.SolveLinear(dom.C, torch.ones(2 * n, dtype=torch.float64, device="cuda"), x, 10, 1e-8,
-                      P.ConvergenceCriterion.ABS_MAX, True)
+    with np.load(os.path.join(GOLDEN, "ref_criteria_%s.npz" % name)) as z:
+        f = {k: z[k] for k in z.files}
+    n = f["b0"].size
+    C = sp.csr_matrix((f["value_C"], f["index_C"], f["row_C"]), shape=(n, n))
+    rb = f["b_bicg"]
+    D = rb.size // n
+    dom = build_product(case(name), torch.float64)
+    P.SetupAdvectionMatrix(dom, torch.tensor([0.05], dtype=torch.float64), 0)
+    x = torch.zeros(D * n, dtype=torch.float64, device="cuda")
+    infos = P.SolveLinear(dom.C, torch.tensor(rb, device="cuda"), x, 300, 1e-10, P.ConvergenceCriterion.ABS_MAX, True,
+                          BiCGwithPreconditioner=False)
+    for c in range(D):
+        xr, ir = po.bicgstab(C, rb[c * n:(c + 1) * n], tol=1e-10, maxit=300, conv="ABS_MAX")
+        assert infos[c].converged and ir.converged
+        assert abs(infos[c].usedIterations - ir.usedIterations) <= 1
+        xs = x[c * n:(c + 1) * n].cpu().numpy()
+        assert np.abs(xs - xr).max() <= 1e-6 * np.abs(xr).max()

@@ -41,6 +41,37 @@ def check_solve(x, info, f, key):
             assert np.abs(x - ref_x).max() <= 1e-7 * np.abs(ref_x).max(), key
 
 
+BICG_CRITERIA = [("NORM2_NORMALIZED", 1e-10), ("ABS_SUM", 1e-8), ("ABS_MEAN", 1e-11)]
+
+
+def check_bicg(x, infos, f, conv):
+    """BiCGStab solves of the D components against the fixture: per component the same iteration (or one
+    apart at the tolerance), convergence, and the solution to rounding."""
+    ref = f["info_bicg_" + conv]
+    ref_x = f["x_bicg_" + conv]
+    n = ref_x.size // len(ref)
+    for c, (inf, ri) in enumerate(zip(infos, ref)):
+        assert bool(inf[2]) == bool(ri[2]) and abs(int(inf[1]) - int(ri[1])) <= 1, (conv, c, inf, ri)
+        xs, rs = x[c * n:(c + 1) * n], ref_x[c * n:(c + 1) * n]
+        assert np.abs(xs - rs).max() <= 1e-6 * np.abs(rs).max(), (conv, c)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_bicgstab_criteria_match_reference(name):
+    with np.load(os.path.join(GOLDEN, "ref_criteria_%s.npz" % name)) as z:
+        f = {k: z[k] for k in z.files}
+    n = f["b0"].size
+    C = sp.csr_matrix((f["value_C"], f["index_C"], f["row_C"]), shape=(n, n))
+    D = f["b_bicg"].size // n
+    for conv, tol in BICG_CRITERIA:
+        xs, infos = [], []
+        for c in range(D):
+            x, inf = po.bicgstab(C, f["b_bicg"][c * n:(c + 1) * n], tol=tol, maxit=MAXIT, conv=conv)
+            xs.append(x)
+            infos.append((inf.finalResidual, inf.usedIterations, inf.converged))
+        check_bicg(np.concatenate(xs), infos, f, conv)
+
+
 @pytest.mark.parametrize("name", CASES)
 def test_oracle_cg_criteria_match_reference(name):
     with np.load(os.path.join(GOLDEN, "ref_criteria_%s.npz" % name)) as z:
