@@ -64,6 +64,65 @@ def make_cavity_domain(n, viscosity, dtype, device="cuda"):
     return dom
 
 
+def extras_pass():
+    """Device time of the operators around the step, CUDA events over 20 calls after 3 warm-ups, FP32: the
+    Smagorinsky viscosity and the passive scalar matrix / right-hand side on a 1024^2 cavity (seeded
+    velocity and scalar), and a 3x3 multi-block convolution (16 -> 16 channels, batch 4) over a 2x2 grid of
+    connected 512^2 blocks (its padding gather and the convolutions)."""
+    import torch
+    from pict_b200 import PISOtorch as P
+    from pict_b200.multiblock_cnn import MultiblockConv
+    dt, dev, n = torch.float32, "cuda", 1024
+    dom = P.Domain(2, torch.tensor([1e-3], dtype=dt), name="extras", dtype=dt, device=torch.device(dev),
+                   passiveScalarChannels=1)
+    g = torch.Generator().manual_seed(0)
+    vel = (torch.rand((1, 2, n, n), generator=g) - 0.5).to(dev, dt).contiguous()
+    sc = torch.rand((1, 1, n, n), generator=g).to(dev, dt).contiguous()
+    coords = torch.tensor(cavity_coords(n), dtype=dt, device=dev).contiguous()
+    blk = dom.CreateBlock(velocity=vel, passiveScalar=sc, vertexCoordinates=coords, name="cavity")
+    blk.CloseAllBoundaries()
+    dom.PrepareSolve()
+    ts = torch.tensor([0.5 / n], dtype=dt)
+    coef = torch.tensor([0.17 ** 2], dtype=dt)
+
+    def timed(fn, reps=20):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    out = {}
+    for key, fn in [("sgs_smagorinsky", lambda: P.SGSviscosityIncompressibleSmagorinsky(dom, coef)),
+                    ("scalar_matrix", lambda: P.SetupAdvectionMatrix(dom, ts, 0, True, 0)),
+                    ("scalar_rhs", lambda: P.SetupAdvectionScalar(dom, ts, 0))]:
+        ms = timed(fn)
+        out[key] = {"ms": ms, "cells": n * n, "cells_per_s": n * n / (ms * 1e-3)}
+    m = 512
+    grid = P.Domain(2, torch.tensor([1e-3], dtype=dt), name="grid", dtype=dt, device=torch.device(dev),
+                    passiveScalarChannels=0)
+    bl = [grid.CreateBlockWithSize(P.Int4(m, m, 1, 2), name="b%d" % i) for i in range(4)]
+    for b in bl:
+        b.CloseAllBoundaries()
+    bl[0].ConnectBlock("+x", bl[1], "-x", "-y")
+    bl[0].ConnectBlock("+y", bl[2], "-y", "-x")
+    bl[1].ConnectBlock("+y", bl[3], "-y", "-x")
+    bl[2].ConnectBlock("+x", bl[3], "-x", "-y")
+    conv = MultiblockConv(grid, "ZERO", 16, 16, 3, device=dev, dtype=dt)
+    xs = [torch.randn((4, 16, m, m), generator=g).to(dev) for _ in range(4)]
+    with torch.no_grad():
+        ms_pad = timed(lambda: conv.pad(xs))
+        ms_all = timed(lambda: conv(xs))
+    out["multiblock_conv"] = {"ms": ms_all, "ms_padding": ms_pad, "cells": 4 * m * m, "batch": 4, "channels": 16,
+                              "cells_per_s": 4 * 4 * m * m / (ms_all * 1e-3)}
+    print(json.dumps({"extras": out, "dtype": "f32", "unit": "ms per call"}), flush=True)
+
+
 def channel_arrays(nx, ny, nz, seed=2, stretch=2.0, u_center=20.0, amp=0.1, modes=12):
     """3D channel on [0, 4 pi] x [-1, 1] x [0, 4 pi / 3]: vertex coordinates [1, 3, nz+1, ny+1, nx+1]
     (uniform in x and z, tanh-stretched in y with factor `stretch`) and the initial velocity
@@ -861,6 +920,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="pict", choices=["pict", "reference"])
+    ap.add_argument("--extras", action="store_true",
+                    help="only time the operators around the step (scalar, SGS, multi-block convolution); own JSON line")
     ap.add_argument("--warm-advection", type=int, default=1,
                     help="mixed precision: start each advection solve from the current velocity (1) or from zero (0)")
     ap.add_argument("--workload", default="batched_cavities_256",
@@ -883,6 +944,9 @@ def main():
     ap.add_argument("--fb-steps", type=int, default=10, help="steps of the forward+backward rollout")
     ap.add_argument("--checkpoint", type=int, default=5, help="checkpoint interval of the rollout")
     args = ap.parse_args()
+    if args.extras:
+        extras_pass()
+        return
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
