@@ -249,10 +249,16 @@ pict_status_t pict_solve(const pict_domain_t* dom, const void* coef, const void*
  * call cudaMalloc, which synchronises the device).  The workspace is a fixed scratch array of
  * pict_solve_static_scratch_bytes() bytes (8 MiB) in the library's own device memory; the call
  * allocates nothing.  Solves whose pict_solve_workspace_bytes() exceeds it are rejected with
- * PICT_ERR_ARG.  The first call on a device looks up the scratch address for that device (make it
- * before any stream capture).  All calls on a device share the one scratch: calls that overlap in
- * time (two streams, two host threads) race and must be serialised by the caller.  Nothing in the
- * scratch has to start at zero; the barrier words are cleared by every call. */
+ * PICT_ERR_ARG; compare the two functions to know beforehand.  The workspace holds 4 vectors of the
+ * system size for CG (5 with return_best_result), 7 for the single-reduction CG (variant 1) and 7
+ * per right-hand side of a launch for BiCGStab: in FP32 about 520k, 290k and, for a 2D velocity
+ * solve, 150k cells.  Every call looks up the scratch address in the current CUDA context (the
+ * address is per context); the first call in a context loads the library's device code, so make
+ * it before any stream capture.  All calls on a device share the one scratch: calls that overlap
+ * in time (two streams, two host threads) race and must be serialised by the caller.  Nothing in
+ * the scratch has to start at zero; the barrier words are cleared by every call.  The array is
+ * part of the library's device code: every device that loads the library holds its 8 MiB until
+ * the process exits, whether or not this function is called. */
 int64_t pict_solve_static_scratch_bytes(void);
 pict_status_t pict_solve_static(const pict_domain_t* dom, const void* coef, const void* rhs, void* x,
                                 const pict_solve_params_t* params, void* info_out, void* stream);

@@ -7,13 +7,15 @@ sources are passed to ``torch.utils.cpp_extension.load`` by absolute path and
 only build products are written, into ``oracle/_ref/`` (git-ignored).
 
 The resulting module is the reference's pybind11 ``PISOtorch`` and is used by
-``oracle/ref_fixtures.py`` on a GPU machine to produce golden fixtures that pin
-the CPU oracle (``oracle/piso_oracle.py``).  It is never imported by the product
+the ``tests/golden/make_ref_*.py`` scripts on a GPU machine to produce golden
+fixtures that pin the CPU oracle (``oracle/piso_oracle.py``) and the CUDA path,
+and by ``bench.py``'s reference timings.  It is never imported by the product
 path (``pict_b200``).
 
 Usage::
 
-    python oracle/build_ref.py [--src <PICT checkout>/extensions]
+    python oracle/build_ref.py --src <PICT checkout>/extensions
+    PICT_REF_EXTENSIONS=<PICT checkout>/extensions python oracle/build_ref.py
 
 The source list and compiler flags follow the reference's extensions/setup.py:8-20
 (same sources, ``-O3 --use_fast_math`` for nvcc, ``-Ofast`` for the host
@@ -66,11 +68,12 @@ def build(src_dir, verbose=True):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--src", default=os.environ.get("PICT_REF_EXTENSIONS", "/root/reference/extensions"))
+    ap.add_argument("--src", default=os.environ.get("PICT_REF_EXTENSIONS"),
+                    help="the extensions/ folder of a PICT checkout (default: $PICT_REF_EXTENSIONS)")
     ap.add_argument("--quiet", action="store_true")
     args = ap.parse_args()
-    if not os.path.isdir(args.src):
-        print("reference sources not present at %s; nothing to build" % args.src)
+    if not args.src or not os.path.isdir(args.src):
+        print("reference sources not given or not present (%s); nothing to build" % args.src)
         return 0
     build(args.src, verbose=not args.quiet)
     print("built reference extension into", OUT)

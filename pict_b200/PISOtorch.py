@@ -68,6 +68,18 @@ class ConvergenceCriterion(enum.IntEnum):
     ABS_MAX = 4
 
 
+class NonOrthoFlags(enum.IntFlag):
+    """Bits of the ``nonOrthoFlags`` argument (extensions/PISO_multiblock_cuda.h:9-13).  The reference
+    declares a pybind11 enum of this name but leaves it commented out (extensions/PISOtorch.cpp:491-501),
+    so its callers pass plain ints; these members are the same ints, and the operators take either."""
+    NONE = 0
+    DIRECT_MATRIX = 1
+    DIRECT_RHS = 2
+    DIAGONAL_MATRIX = 4
+    DIAGONAL_RHS = 8
+    CENTER_MATRIX = 16
+
+
 # pybind11 export_values(): enum members are also module attributes
 DIRICHLET_VARYING = BoundaryType.DIRICHLET_VARYING
 FIXED = BoundaryType.FIXED

@@ -12,8 +12,11 @@ Matrices are the stencil coefficient tensors ``C.coef`` / ``P.coef`` (the refere
 ``value`` arrays); ``linear_solve_GPU`` differentiates with respect to them with the transposed
 solve and the stencil outer product -b_grad x^T (PISOtorch_diff.py:295-375).
 
-Not differentiable here (NotImplementedError, as for the non-orthogonal path): passive scalars,
-non-orthogonal corrections, ``apply_pressure_gradient``, ``timeStepNorm`` and face transforms.
+Passive scalars (matrix per channel, scalar RHS, result copies) and the non-orthogonal terms
+(nonOrthoFlags of the matrix and RHS operators) are differentiable through their adjoint kernels
+(scalar.cu, nonortho.cu).  Not differentiable here (NotImplementedError): face transforms
+(``useFaceTransform``), whose forward operators the reference marks experimental,
+``apply_pressure_gradient`` and ``timeStepNorm``.
 """
 from __future__ import annotations
 

@@ -11,12 +11,12 @@ execution paths produce the same step:
   the whole step to :class:`pict_b200.engine.PISOStepper`, which launches it
   without host synchronisation.
 
-Non-orthogonal correction terms are not implemented: with
-``non_orthogonal=True`` and a domain whose metrics are not orthogonal, the step follows the
-reference's non-orthogonal branch operator by operator (on orthogonal metrics the terms vanish
-identically and the fused step runs).  Image/VTK output belongs to the reference's
-post-processing utilities and is not part of this package; the corresponding
-arguments are accepted and ignored with a warning.
+With ``non_orthogonal=True`` and a domain whose metrics are not orthogonal, the step follows
+the reference's non-orthogonal branch operator by operator, with the non-orthogonal matrix and
+RHS terms (nonOrthoFlags) of the operators (on orthogonal metrics the terms vanish identically
+and the fused step runs).  Image/VTK output belongs to the reference's post-processing utilities
+and is not part of this package; the corresponding arguments are accepted and ignored with a
+warning.
 """
 from __future__ import annotations
 

@@ -1389,34 +1389,28 @@ static pict_status_t run_solve(const pict_domain_t* dom, const void* coef, const
 // binding without torch, or a loop that must not call cudaMalloc, which synchronises the device)
 // solve small systems with the workspace placed in this module's own device memory.
 // ---------------------------------------------------------------------------------------------
-constexpr size_t KR_STATIC_SCRATCH_BYTES = size_t(8) << 20;  // 8 MiB: e.g. FP32 CG up to ~290k cells
+// 8 MiB.  Which solves fit depends on the solver's vector count: 4 vectors of N values for CG, 5 with
+// returnBestResult, 7 for the single-reduction CG (variant 1), and 7 x (right-hand sides per launch)
+// for BiCGStab, plus a small header; e.g. FP32 CG fits ~520k cells, single-reduction CG ~290k,
+// a 2D BiCGStab velocity solve (2 components) ~150k.  Every device that loads the library holds
+// this array for the life of the process, whether or not pict_solve_static is ever called.
+constexpr size_t KR_STATIC_SCRATCH_BYTES = size_t(8) << 20;
 static __device__ __align__(256) unsigned char kr_static_scratch[KR_STATIC_SCRATCH_BYTES];
 
-constexpr int KR_MAX_DEVICES = 64;
-static std::mutex g_scratch_mutex;
-static void* g_scratch_ptr[KR_MAX_DEVICES] = {};
-
-// Device address of kr_static_scratch on the current device, looked up once per device.
+// Device address of kr_static_scratch in the current context.  Looked up on every call: the
+// address belongs to the context the module is loaded in (a context re-created after
+// cudaDeviceReset, or another context made current through the driver API, can place the module
+// elsewhere), and the lookup allocates nothing.  The first call in a context loads the module.
 static pict_status_t static_scratch(void** out) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, kr_static_scratch);
+    if (e != cudaSuccess || !p) {
+        char buf[256];
+        snprintf(buf, sizeof(buf), "solve_static: cudaGetSymbolAddress of the scratch failed: %s", cudaGetErrorString(e));
         cudaGetLastError();
-        return set_error(PICT_ERR_NO_DEVICE, "solve_static: no current CUDA device");
+        return set_error(e == cudaErrorNoDevice ? PICT_ERR_NO_DEVICE : PICT_ERR_CUDA, buf);
     }
-    if (dev < 0 || dev >= KR_MAX_DEVICES) return set_error(PICT_ERR_ARG, "solve_static: device ordinal out of range");
-    std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (!g_scratch_ptr[dev]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, kr_static_scratch);
-        if (e != cudaSuccess || !p) {
-            char buf[256];
-            snprintf(buf, sizeof(buf), "solve_static: cudaGetSymbolAddress of the scratch failed: %s", cudaGetErrorString(e));
-            cudaGetLastError();
-            return set_error(PICT_ERR_CUDA, buf);
-        }
-        g_scratch_ptr[dev] = p;
-    }
-    *out = g_scratch_ptr[dev];
+    *out = p;
     return PICT_OK;
 }
 

@@ -143,7 +143,7 @@ def lid_fixture(R, n, steps, dtype, tol, dt=0.01, viscosity=1e-3):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden"))
+    ap.add_argument("--out", required=True, help="directory the fixtures are written to")
     ap.add_argument("--quick", action="store_true")
     ap.add_argument("--cases", nargs="*", default=None, help="only the operator fixtures of these setups")
     args = ap.parse_args()

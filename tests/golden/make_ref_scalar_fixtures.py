@@ -114,7 +114,7 @@ def scalar_fixture(R, name):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden"))
+    ap.add_argument("--out", required=True, help="directory the fixtures are written to")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
     import PISOtorch as R

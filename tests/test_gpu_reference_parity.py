@@ -89,5 +89,6 @@ def test_lid_cavity_100_steps_fp32_vs_reference(variant):
     u, p = _fields(pd)
     eu, ep = _rel(u, fx["velocity"]), _rel(p, fx["pressure"])
     print("fp32 vs reference CUDA after 100 steps: velocity %.3e pressure %.3e" % (eu, ep))
-    # both sides stop at 1e-6 RMS residual in FP32 with different summation orders
-    assert eu < 2e-3 and ep < 2e-2
+    # relative velocity / pressure error bound of the FP32 step against the reference's FP32 CUDA build
+    # after 100 steps; both sides stop at 1e-6 RMS residual with different summation orders
+    assert eu < 1e-5 and ep < 1e-5

@@ -97,3 +97,15 @@ def test_topology_rejects_inconsistent_connections():
     nbr = np.empty((4, od2.N), dtype=np.int32)
     cb = np.empty(od2.N, dtype=np.int32)
     assert _lib.load().pict_build_topology(arr, 1, 2, od2.N, nbr.ctypes.data, cb.ctypes.data) != 0
+
+
+def test_non_ortho_flags_enum():
+    """NonOrthoFlags carries the bits of extensions/PISO_multiblock_cuda.h:9-13 and is accepted wherever
+    the operators take nonOrthoFlags; the driver's mode is the same int."""
+    from pict_b200 import PISOtorch as P
+    from pict_b200.PISOtorch_simulation import Simulation
+    F = P.NonOrthoFlags
+    assert (F.DIRECT_MATRIX, F.DIRECT_RHS, F.DIAGONAL_MATRIX, F.DIAGONAL_RHS, F.CENTER_MATRIX) == (1, 2, 4, 8, 16)
+    mode = F.CENTER_MATRIX | F.DIRECT_MATRIX | F.DIAGONAL_RHS
+    assert int(mode) == Simulation._NON_ORTHO_MODE == 25
+    assert P._non_ortho(mode) == 25 and P._non_ortho(F.NONE) == 0
