@@ -384,6 +384,23 @@ pict_status_t pict_scalar_grad(const pict_domain_t* dom, double dt, int32_t non_
  * length of the cell transform M, 1 without one). */
 pict_status_t pict_sgs_smagorinsky(const pict_domain_t* dom, double coefficient, void* out, void* stream);
 
+/* ---------------- advective outflow boundaries ----------------
+ * update_advective_boundaries followed by balance_boundary_fluxes (PISOtorch_simulation.py:145-312, the
+ * reference's host-side PyTorch code run through the driver's prep_fn before each step), on the device.
+ * faces: host array [num_faces][2] of (block, face) pairs, 1 <= num_faces <= PICT_MAX_OUTFLOW_FACES,
+ * each a fixed face whose boundary velocity is varying ([D][face cells]); char_velocity: host [D],
+ * the static characteristic velocity.  Each outflow face cell moves its boundary velocity towards
+ * the adjacent block cell by t = 1 - 1/(1 + 2 dt c), c the face-normal component of char_velocity
+ * (row `axis` of the boundary transform's inverse times it, if the face has a transform); then,
+ * unless the net outward flux of all fixed faces (FixedBoundary::GetFluxes, extensions/domain_structs.cpp:527-542,
+ * summed in FP64) is within `atol` of zero, the outflow faces' velocity is scaled by -(flux of the
+ * other fixed faces) / (flux of the outflow faces).  The reference's atol is 1% of the solver
+ * tolerance (1e-7 in FP32, 1e-10 in FP64).  Boundary velocities are updated in place.  One
+ * simulation per domain (num_sims == 1).  dt: the time step, or per system from dom->sim_dt. */
+#define PICT_MAX_OUTFLOW_FACES 16
+pict_status_t pict_advective_outflow(const pict_domain_t* dom, const int32_t* faces, int32_t num_faces,
+                                     const double* char_velocity, double dt, double atol, void* stream);
+
 /* Gradients of the non-orthogonal terms (nonOrthoFlags; the non-orthogonal parts of the reference's *_GRAD
  * kernels, extensions/PISO_multiblock_cuda_kernel.cu:1992-2098, 3212-3392).  what 0: advection matrix, out_bar =
  * C_grad [K][N] with A_bar = A_grad [N] -> coef_bar = viscosity gradient [N] (per cell); 1: velocity RHS,

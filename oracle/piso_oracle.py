@@ -1667,6 +1667,77 @@ def _piso_step_nonortho(dom, dt, corrector_steps, adv_tol, p_tol, method, maxit,
     return StepResult(Ccoef, A, rhs, u_star, P, h, div, p, u_cur, infos)
 
 
+def _face_broadcast(dom: ODomain, bi: int, face: int, v: np.ndarray) -> np.ndarray:
+    """A boundary tensor [1,C] (static) or [1,C,face zyx] as [1,C,face zyx]."""
+    b = dom.blocks[bi]
+    D = dom.dims
+    shape = list(b.velocity.shape[2:])
+    shape[D - 1 - (face >> 1)] = 1
+    v = np.asarray(v, dtype=np.float64)
+    if v.ndim == 2:
+        v = v.reshape(v.shape + (1,) * D)
+    return np.broadcast_to(v, v.shape[:2] + tuple(shape)).copy()
+
+
+def boundary_fluxes(dom: ODomain, bi: int, face: int) -> np.ndarray:
+    """FixedBoundary::GetFluxes (extensions/domain_structs.cpp:527-542): per face cell the face-normal
+    flux det * (M^-1 u)_axis of the boundary velocity, or u_axis without a boundary transform."""
+    D = dom.dims
+    axis = face >> 1
+    bnd = dom.blocks[bi].boundaries[face]
+    u = _face_broadcast(dom, bi, face, bnd.velocity)  # [1,D,zyx]
+    if bnd.transform is None:
+        return u[:, axis]
+    T = bnd.transform  # [1, zyx, T]
+    row = T[..., D * D + axis * D: D * D + (axis + 1) * D]
+    return T[..., -1] * np.einsum("...c,...c->...", row, np.moveaxis(u, 1, -1))
+
+
+def advective_outflow(dom: ODomain, faces, velm, dt: float, tol: Optional[float] = None):
+    """update_advective_boundaries with a static characteristic velocity, then balance_boundary_fluxes
+    (sim.py:145-312).  Every (block, face) of `faces` holds a varying Dirichlet velocity; it moves
+    towards the adjacent cell layer by t = 1 - 1/(1 + 2 dt c), c the face-normal component of `velm`
+    (in computational coordinates with a boundary transform: row `axis` of M^-1 times velm).  Then,
+    unless the net outward flux of all fixed faces is within 1% of the tolerance (default 1e-8, the
+    FP64 solver default of PISOtorch_diff.py:183-189) of zero, the free faces' velocities are scaled by
+    -(flux of the other fixed faces) / (flux of the free faces)."""
+    D = dom.dims
+    velm = np.asarray(velm, dtype=np.float64).reshape(1, D)
+    faces = [(int(b), int(f)) for b, f in faces]
+    for bi, face in faces:
+        b = dom.blocks[bi]
+        bnd = b.boundaries[face]
+        assert bnd.kind == "fixed" and np.asarray(bnd.velocity).ndim == D + 2, "outflow faces must be varying"
+        axis = face >> 1
+        ax = 2 + (D - 1 - axis)
+        layer = np.take(b.velocity, [b.velocity.shape[ax] - 1 if (face & 1) else 0], axis=ax)
+        if bnd.transform is not None:
+            row = bnd.transform[..., D * D + axis * D: D * D + (axis + 1) * D]  # [1, zyx, D]
+            c = np.einsum("...c,c->...", row, velm[0])[:, None]  # [1,1,zyx]
+        else:
+            c = velm[:, axis].reshape((1, 1) + (1,) * D)
+        t = 1.0 - 1.0 / (1.0 + 2.0 * dt * c)
+        vb = bnd.velocity
+        bnd.velocity = vb - t * (vb - layer)
+    fixed = free = 0.0
+    for bi, b in enumerate(dom.blocks):
+        for f, bnd in enumerate(b.boundaries):
+            if bnd.kind != "fixed":
+                continue
+            flux = float(np.sum(boundary_fluxes(dom, bi, f)))
+            flux = flux if (f & 1) else -flux
+            if (bi, f) in faces:
+                free += flux
+            else:
+                fixed += flux
+    tol = 1e-8 if tol is None else tol
+    if abs(fixed + free) > tol * 0.01:
+        scale = -fixed / free
+        for bi, face in faces:
+            bnd = dom.blocks[bi].boundaries[face]
+            bnd.velocity = bnd.velocity * scale
+
+
 def run_steps(dom: ODomain, steps: int, dt: float, **kw):
     res = None
     for _ in range(steps):

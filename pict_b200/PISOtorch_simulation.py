@@ -78,6 +78,151 @@ def get_max_time_step(domain, time_step_target, CFL_cond=0.8, with_transformatio
     return time_step_target / ss, ss
 
 
+def tensor_as_np(tensor):
+    return tensor.detach().cpu().numpy()
+
+
+def getVelocityResultMaxMag(domain):
+    """Largest velocity magnitude in domain.velocityResult, 0 for a zero field (PISOtorch_simulation.py:67-73)."""
+    vel = domain.velocityResult.reshape(domain.getSpatialDims(), domain.getTotalSize())
+    if float(torch.max(torch.abs(vel)).item()) > 0:
+        return float(torch.max(torch.linalg.vector_norm(vel, dim=0)).item())
+    return 0
+
+
+def getVelocityResultMaxVel(domain):
+    """Largest velocity component magnitude in domain.velocityResult (PISOtorch_simulation.py:75-78)."""
+    return float(torch.max(torch.abs(domain.velocityResult)).item())
+
+
+# ------------------------------------------------------------------ outflow boundaries (PISOtorch_simulation.py:80-312)
+# Written against the boundary interface only (GetFluxes, velocity, transform, setVelocity, ...), so the
+# same functions drive this package's domains and any object with the PISOtorch boundary interface.
+
+def _is_fixed_boundary(bound):
+    return type(bound).__name__ == "FixedBoundary"
+
+
+def _solver_tolerance(tol, dtype):
+    """Default solver tolerance by dtype (PISOtorch_diff.py:183-189)."""
+    if tol is None:
+        return 1e-8 if dtype == torch.float64 else 1e-5
+    return tol
+
+
+def get_fixed_boundary_flux(bound, bound_idx):
+    """Total flux through a Dirichlet face: the sum of FixedBoundary.GetFluxes() (PISOtorch_simulation.py:80-90)."""
+    if not _is_fixed_boundary(bound):
+        raise AssertionError("get_fixed_boundary_flux needs a FixedBoundary")
+    if int(bound.velocityType) != int(PISOtorch.BoundaryConditionType.DIRICHLET):
+        raise ValueError("Only DIRICHLET boundaries are supportet")
+    return torch.sum(bound.GetFluxes())
+
+
+def get_fixed_boundary_fluxes(list_idx_bound):
+    """Net outward flux of a list of (face index, FixedBoundary): the flux of an upper face (odd index)
+    counts positive, of a lower face negative (PISOtorch_simulation.py:92-107)."""
+    domain = list_idx_bound[0][1].getParentDomain()
+    total = torch.zeros([1], dtype=domain.getDtype(), device=domain.getDevice())
+    for face, bound in list_idx_bound:
+        if not _is_fixed_boundary(bound):
+            raise TypeError("boundary type not supported.")
+        flux = get_fixed_boundary_flux(bound, face)
+        total = total + flux if (face & 1) else total - flux
+    return total
+
+
+def get_advective_velocity(velms, velm_idx, bound, bound_idx):
+    """Face-normal transport velocity of an outflow face, [1,1] for a static velocity on an
+    untransformed face, else [1,1,(z),y,x] over the face cells: the face-normal component of the
+    characteristic velocity `velms` (one [1,D] or [1,D,(z),y,x] tensor, or a list indexed by
+    velm_idx), in computational coordinates (row `axis` of the face transform's inverse) when the face
+    carries a transform (PISOtorch_simulation.py:145-172)."""
+    velm = velms if isinstance(velms, torch.Tensor) else velms[velm_idx]
+    dims = bound.getSpatialDims()
+    axis = bound_idx >> 1
+    sizes = bound.getSizes()
+    face_shape = [int(sizes[dims - 1 - d]) for d in range(dims)]  # z, y, x
+    static = velm.dim() == 2
+    if not static:
+        assert all(velm.size(2 + d) == face_shape[d] for d in range(dims)), "varying velm size must match boundary"
+    has_transform = bound.hasTransform() if callable(getattr(bound, "hasTransform", None)) else bound.hasTransform
+    if not has_transform:
+        return velm[:, axis:axis + 1]
+    if static:
+        velm = velm.reshape([1, dims] + [1] * dims).expand([1, dims] + face_shape)
+    row = bound.transform[..., dims * dims + axis * dims: dims * dims + (axis + 1) * dims]  # [1,(z),y,x,D]
+    v = torch.movedim(velm, 1, -1)  # [1,(z),y,x,D]
+    adv = torch.matmul(row.reshape(-1, 1, dims), v.reshape(-1, dims, 1))
+    return adv.reshape([1, 1] + face_shape)
+
+
+def balance_boundary_fluxes(domain, free_bounds, tol=None):
+    """Scale the velocity of the free (outflow) faces so that the net flux through all Dirichlet faces
+    vanishes, unless it already does to 1% of the solver tolerance (PISOtorch_simulation.py:174-208)."""
+    with torch.no_grad():
+        faces = []
+        for block in domain.getBlocks():
+            faces.extend(block.getFixedBoundaries())
+        fixed = [fb for fb in faces if fb[1] not in free_bounds]
+        free = [fb for fb in faces if fb[1] in free_bounds]
+        fixed_flux = get_fixed_boundary_fluxes(fixed)
+        free_flux = get_fixed_boundary_fluxes(free)
+    atol = _solver_tolerance(tol, domain.getDtype()) * 0.01
+    if not torch.allclose(fixed_flux + free_flux, torch.zeros_like(fixed_flux), atol=atol):
+        scale = -fixed_flux / free_flux
+        for _, bound in free:
+            bound.setVelocity(bound.velocity * scale)
+
+
+def _face_layer(t, face):
+    """The cell layer of a block field [1,C,(z),y,x] next to `face` (kept as a size-1 axis)."""
+    dim = t.dim() - 1 - (face >> 1)
+    return t.narrow(dim, t.size(dim) - 1 if (face & 1) else 0, 1)
+
+
+def update_advective_boundaries(domain, bounds, velms, dt, tol=None):
+    """Advective outflow: every face in `bounds` (varying Dirichlet FixedBoundary objects) moves its
+    velocity (and passive scalar) towards the adjacent cell layer by the implicit upwind weight
+    t = 1 - 1/(1 + 2 dt c), c = get_advective_velocity(velms, ...), then the free faces are rescaled to
+    balance the domain's boundary fluxes (PISOtorch_simulation.py:210-312)."""
+    with torch.no_grad():
+        dims = domain.getSpatialDims()
+        assert isinstance(bounds, list) and len(bounds) > 0
+        assert (isinstance(velms, torch.Tensor) and velms.dim() == 2 and velms.size(0) == 1 and velms.size(1) == dims) \
+            or (isinstance(velms, list) and len(velms) == len(bounds) and all(
+                isinstance(v, torch.Tensor) and v.dim() in (2, dims + 2) and v.size(0) == 1 and v.size(1) == dims
+                for v in velms)), "velms tensors have wrong shape"
+        entries = []
+        for bi in range(domain.getNumBlocks()):
+            block = domain.getBlock(bi)
+            for face in range(2 * dims):
+                bound = block.getBoundary(face)
+                if _is_fixed_boundary(bound) and bound in bounds:
+                    entries.append((block, face, bound))
+        if len(entries) != len(bounds):
+            raise ValueError("Bounds passed as advective outflow are not (all) part of the domain.")
+        for block, face, bound in entries:
+            vel_layer = _face_layer(block.velocity, face)
+            alpha = dt * 2 * get_advective_velocity(velms, bounds.index(bound), bound, face)
+            t = 1 - 1 / (1 + alpha)
+            if bound.isVelocityStatic:
+                raise ValueError("outflow boundaries must be varying. Use FixedBoundary.makeVelocityVarying() to make the velocity varying.")
+            scalar_bound = None
+            if block.hasPassiveScalar() and bound.hasPassiveScalar():
+                if bound.isPassiveScalarStatic():
+                    raise ValueError("outflow boundary passive scalar must be varying.")
+                if any(int(c) != int(PISOtorch.BoundaryConditionType.DIRICHLET) for c in bound.passiveScalarTypes):
+                    raise ValueError("passive scalar outflow boundary condition must be Dirichlet.")
+                scalar_bound = bound.passiveScalar
+            vel = bound.velocity
+            bound.setVelocity(vel - t * (vel - vel_layer))
+            if scalar_bound is not None:
+                scalar_layer = _face_layer(block.passiveScalar, face)
+                bound.setPassiveScalar(scalar_bound - t * (scalar_bound - scalar_layer))
+    balance_boundary_fluxes(domain, bounds, tol=tol)
+
+
 def metrics_are_orthogonal(domain, rtol=1e-6):
     """True if every cell transform has mutually orthogonal Minv rows (non-orthogonal terms vanish)."""
     D = domain.getSpatialDims()

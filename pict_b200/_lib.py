@@ -204,6 +204,7 @@ SIGNATURES = {
     "pict_setup_scalar_rhs": (c_i32, [_PD, ctypes.c_double, c_i32, c_vp]),
     "pict_copy_scalar_result": (c_i32, [_PD, c_i32, c_vp]),
     "pict_sgs_smagorinsky": (c_i32, [_PD, ctypes.c_double, c_vp, c_vp]),
+    "pict_advective_outflow": (c_i32, [_PD, c_vp, c_i32, c_vp, ctypes.c_double, ctypes.c_double, c_vp]),
     "pict_scalar_grad": (c_i32, [_PD, ctypes.c_double, c_i32, c_i32, c_i32] + [c_vp] * 9),
     "pict_csr_row_ptr": (c_i32, [_PD, c_vp, c_vp]),
     "pict_stencil_to_csr": (c_i32, [_PD, c_vp, c_vp, c_vp, c_vp, c_vp]),

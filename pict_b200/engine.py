@@ -50,7 +50,8 @@ class PISOStepper:
                  p_group_size: int = 0, threads: int = 0, normalize_pressure: bool = True, cg_variant: int = 1,
                  pressure_refine: int = 0, refine_tol: Optional[float] = None, warm_start_pressure: bool = False,
                  refine_solver: str = "cg", mg_iterations: int = 12, pressure_first_solve: bool = True,
-                 warm_start_advection: bool = False):
+                 warm_start_advection: bool = False, outflow=None, outflow_velocity=None,
+                 outflow_tol: Optional[float] = None):
         self.domain = domain
         self.dims = domain.getSpatialDims()
         self.corrector_steps = int(corrector_steps)
@@ -91,6 +92,23 @@ class PISOStepper:
         self.r_params = P._solve_params(1, self.max_iterations, self.refine_tol, _lib.PICT_CONV_NORM2_NORMALIZED, False,
                                         False, x_zero=True, group_size=p_group_size, threads=threads,
                                         variant=cg_variant)
+        # advective outflow faces, updated on the device at the start of every step like the reference
+        # samples' prep_fn (update_advective_boundaries, PISOtorch_simulation.py:210-312): (block, face)
+        # pairs of varying Dirichlet faces, the static characteristic velocity [D] and the flux-balance
+        # tolerance (default: the solver default of the dtype, whose 1% is the balance threshold)
+        self.outflow = [(int(b), int(f)) for b, f in (outflow or [])]
+        if self.outflow:
+            for b, f in self.outflow:
+                bnd = domain.getBlock(b).getBoundary(f)
+                if not isinstance(bnd, P.FixedBoundary) or bnd.isVelocityStatic:
+                    raise ValueError("outflow face (%d, %d) must be a FixedBoundary with varying velocity" % (b, f))
+            vel = [1.0] + [0.0] * (self.dims - 1) if outflow_velocity is None else \
+                [float(v) for v in torch.as_tensor(outflow_velocity).reshape(-1).tolist()]
+            if len(vel) != self.dims:
+                raise ValueError("outflow_velocity must have %d components" % self.dims)
+            self._of_faces = (ctypes.c_int32 * (2 * len(self.outflow)))(*[v for bf in self.outflow for v in bf])
+            self._of_vel = (ctypes.c_double * self.dims)(*vel)
+            self._of_atol = 0.01 * (default_tolerance(dt) if outflow_tol is None else float(outflow_tol))
         self._graph = None
         self._graph_steps = 0
         self._prepare()
@@ -169,6 +187,7 @@ class PISOStepper:
         st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream if stream is None else stream)
         dt = self._dt(time_step)
         D = self.dims
+        self._outflow(desc, dt, st)
         check(lib.pict_setup_advection(desc, dt, st), "advection setup")
         if self.warm_start_advection:
             check(lib.pict_copy_velocity_result_from_blocks(desc, st), "advection initial guess")
@@ -185,6 +204,11 @@ class PISOStepper:
             check(lib.pict_correct_velocity(desc, dt, 1, 0, 1 if last else 0, st), "velocity correction")
         if self.corrector_steps == 0:
             check(lib.pict_copy_velocity_result_to_blocks(desc, st), "copy velocity")
+
+    def _outflow(self, desc, dt, st):
+        if self.outflow:
+            check(self.lib.pict_advective_outflow(desc, self._of_faces, len(self.outflow), self._of_vel, dt,
+                                                  self._of_atol, st), "advective outflow")
 
     def _refine_only(self, k, desc, st, events=None, ev=None):
         """FP64 refinement sweeps after the first pressure solve of corrector k: residual of the FP64
@@ -217,8 +241,9 @@ class PISOStepper:
     def kernels_per_step(self):
         """Kernels of this library launched per step: advection setup 1; per solve init-info, solver and
         finish-info 3; per corrector pressure setup 2 (matrix/RHS, divergence), correction 1, and the
-        refinement sweeps when enabled; the copy of the initial guess of a warm-started advection solve 1."""
-        n = 1 + 3 + (1 if self.warm_start_advection else 0)
+        refinement sweeps when enabled; the copy of the initial guess of a warm-started advection solve 1;
+        the advective outflow update 1."""
+        n = 1 + 3 + (1 if self.warm_start_advection else 0) + (1 if self.outflow else 0)
         n += self.corrector_steps * (2 + (3 if self.pressure_first_solve else 0) + 1)
         if self.pressure_refine > 0:  # per sweep: residual (+2 projection), solve, update; partials + finish
             if self._mg is not None:
@@ -250,6 +275,7 @@ class PISOStepper:
         st = ctypes.c_void_p(cs.cuda_stream)
         dt = self._dt(time_step)
         out = {"bicg": [], "cg": [], "mg": []}
+        self._outflow(desc, dt, st)
 
         def ev():
             e = torch.cuda.Event(enable_timing=True)
@@ -320,6 +346,7 @@ class PISOStepper:
         """
         d = self.domain
         saved = [(b.velocity.clone(), b.pressure.clone()) for b in d.getBlocks()]
+        saved_out = [d.getBlock(b).getBoundary(f).velocity.clone() for b, f in self.outflow]
         torch.cuda.synchronize()
         s = torch.cuda.Stream()
         s.wait_stream(torch.cuda.current_stream())
@@ -330,6 +357,8 @@ class PISOStepper:
         for b, (v, p) in zip(d.getBlocks(), saved):
             b.velocity.copy_(v)
             b.pressure.copy_(p)
+        for (b, f), v in zip(self.outflow, saved_out):
+            d.getBlock(b).getBoundary(f).velocity.copy_(v)
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g):
             for _ in range(steps):
