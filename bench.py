@@ -363,6 +363,33 @@ def run_reference(args, rank, world):
         }
         print(json.dumps(line), flush=True)
         return
+    if w == "cylinder_street":
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import piso_oracle as po
+        from pict_b200.cylinder_street import TIME_STEP, street_spec
+        spec = street_spec()
+        od = _oracle_street(po, spec)
+        for _ in range(args.warmup):
+            po.advective_outflow(od, spec["outflow"], spec["char_vel"], TIME_STEP, tol=1e-5)
+            po.piso_step(od, TIME_STEP, adv_tol=1e-6, p_tol=1e-6)
+        times = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            po.advective_outflow(od, spec["outflow"], spec["char_vel"], TIME_STEP, tol=1e-5)
+            po.piso_step(od, TIME_STEP, adv_tol=1e-6, p_tol=1e-6)
+            times.append(time.perf_counter() - t0)
+        value = od.N * len(times) / sum(times)
+        line = {
+            "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": w, "sample": "the full street, one PISO step with the outflow update per timed step"},
+            "cpu_baseline": {"value": value, "unit": "cell-steps/s", "cores": 1, "kind": "port",
+                             "sample": "full street x %d steps, FP64 NumPy/SciPy restatement" % args.steps},
+            "e2e": {"value": value, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
+        return
     if w == "batched_cavities_256":
         sides, re = batched_cavity_params(256, 6)
         dts = [0.5 / s for s in sides]
@@ -430,18 +457,20 @@ def run_pict(args, rank, world):
             its = np.array([i.usedIterations for i in p])
             warm_cg_bytes.append(float(np.sum((its + 1) * n_s) * per_cell))
     torch.cuda.synchronize()
+    G = graph_steps(args)
     if not args.no_graph:
-        st.capture(steps=1)
+        st.capture(steps=G)
     torch.cuda.synchronize()
 
-    def one_step():
+    def run_steps(k):
         if args.no_graph:
-            st.step()
+            for _ in range(k):
+                st.step()
         else:
-            st.replay()
+            for _ in range(k // G):
+                st.replay()
 
-    for _ in range(max(args.warmup, 3)):
-        one_step()
+    run_steps(max(args.warmup, 3) * G)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -454,8 +483,7 @@ def run_pict(args, rank, world):
     e1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.nvtx.range_push("piso_timed_steps")  # lets a profiler select exactly the timed launches
     e0.record()
-    for _ in range(args.steps):
-        one_step()
+    run_steps(args.steps)
     e1.record()
     torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
@@ -471,7 +499,10 @@ def run_pict(args, rank, world):
     roof = roofline_pass(st, batch, args, dev)
     roof["warmup_launch_algorithmic_bytes"] = warm_cg_bytes
 
-    # end-to-end through the public API with host buffers
+    # end-to-end through the public API with host buffers (a one-step graph: the state crosses the
+    # host between steps)
+    if not args.no_graph and G != 1:
+        st.capture(steps=1)
     e2e = e2e_pass(st, batch, args, dev, cells, world)
 
     # the same batched step in plain FP32 (pressure solves from zero to the workload tolerance, no
@@ -493,6 +524,13 @@ def run_pict(args, rank, world):
         err = None
     if err is not None and not args.skip_bwd and cavities:
         err["viscosity_grad"] = grad_check(wl)
+        err["viscosity_grad_timed_precision"] = grad_check_mixed(wl, args)
+
+    # the reference's own CUDA build on this GPU (stock operators, one simulation at a time)
+    ref_cuda = reference_cuda_pass(wl) if (rank == 0 and not args.skip_ref_cuda and cavities) else None
+
+    # the other configurations, timed briefly so that their throughput is in this line
+    extras = extras_pass_default(args) if (rank == 0 and not args.skip_extras and cavities) else None
 
     # CPU baseline (bounded sample, rank 0)
     cpu = None
@@ -523,7 +561,8 @@ def run_pict(args, rank, world):
                        "precision": args.precision + (" (FP32 fields and Krylov vectors, FP64 reductions, one FP64 "
                                                       "refinement sweep of each pressure solve (multigrid-preconditioned CG corrections on near-isotropic grids), warm-started pressure solves" + (", advection solves from the current velocity" if args.warm_advection else "") + ")"
                                                       if args.precision == "mixed" else " (FP32, FP64 reductions)"),
-                       "cuda_graph": not args.no_graph, "l2": "working set > L2 (126 MB), no flush",
+                       "cuda_graph": not args.no_graph, "cuda_graph_steps": None if args.no_graph else G,
+                       "l2": "working set > L2 (126 MB), no flush",
                        "autotune": tuned, "tile_cells": batch.tile_cells,
                        "parallelism": "independent batches per GPU" if world > 1 else "single GPU"},
             "clocks": clocks,
@@ -533,6 +572,8 @@ def run_pict(args, rank, world):
             "fwd_bwd": fb,
             "fp32_step": fp32,
             "plain": plain,
+            "reference_cuda": ref_cuda,
+            "extras": extras,
             "gpu_launches": st.kernels_per_step() * args.steps,
             "err": err,
             "solver_iterations": {"advection_max": int(max(iters_adv)), "advection_mean": float(np.mean(iters_adv)),
@@ -541,6 +582,242 @@ def run_pict(args, rank, world):
                                   "refinement_max": iters_ref, "refinement_final_residual_max": res_ref},
         }
         print(json.dumps(line), flush=True)
+
+
+def graph_steps(args):
+    """Steps per captured CUDA graph: --graph-steps when it divides --steps, else 1."""
+    g = max(1, int(args.graph_steps))
+    return g if args.steps % g == 0 else 1
+
+
+def street_stepper(dtype=None, tol=1e-6, graph=0):
+    """The full cylinder street (27,648 cells, FP32), projected to a divergence-free start through the
+    drop-in Simulation, and its fused stepper with the device outflow update."""
+    import torch
+    from pict_b200.cylinder_street import TIME_STEP, build_street, street_prep_fn, street_spec
+    from pict_b200.engine import PISOStepper
+    from pict_b200.PISOtorch_simulation import Simulation
+    dom, info = build_street(street_spec(), dtype=torch.float32 if dtype is None else dtype)
+    sim = Simulation(domain=dom, time_step=TIME_STEP, prep_fn=street_prep_fn(info), corrector_steps=2,
+                     advection_tol=tol, pressure_tol=tol, non_orthogonal=False)
+    sim.make_divergence_free()
+    st = PISOStepper(dom, time_step=TIME_STEP, advection_tol=tol, pressure_tol=tol, outflow=info["outflow"],
+                     outflow_velocity=info["char_vel"])
+    return dom, info, st
+
+
+def _graph_rate(st, cells, steps, g):
+    import torch
+    for _ in range(3):
+        st.step()
+    st.check()
+    st.capture(steps=g)
+    st.replay()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps // g):
+        st.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    st.check()
+    ms = e0.elapsed_time(e1)
+    return cells * steps / (ms * 1e-3), ms / steps
+
+
+def extras_pass_default(args):
+    """Brief timings of the other configurations on this GPU (CUDA events over graph replays):
+    the cylinder street (FP32, 200 steps) and the 192 x 96 x 96 channel (this run's precision, 10 steps)."""
+    import torch
+    out = {}
+    dom, info, st = street_stepper()
+    rate, ms = _graph_rate(st, dom.getTotalSize(), 200, 50)
+    out["cylinder_street"] = {"value": rate, "unit": "cell-steps/s", "ms_per_step": ms, "cells": dom.getTotalSize(),
+                              "steps": 200, "precision": "FP32, FP64 reductions, solves to 1e-6",
+                              "workload": "bench.py --workload cylinder_street"}
+    del st, dom
+    wl = build_workload("channel3d_192")
+    d = wl["domains"][0]
+    from pict_b200.engine import PISOStepper
+    st = PISOStepper(d, time_step=float(wl["dts"][0]), corrector_steps=wl["correctors"], advection_tol=wl["tol"],
+                     pressure_tol=wl["tol"], max_iterations=5000, **precision_kwargs(args, wl))
+    rate, ms = _graph_rate(st, d.getTotalSize(), 10, 5)
+    out["channel3d_192"] = {"value": rate, "unit": "cell-steps/s", "ms_per_step": ms, "cells": d.getTotalSize(),
+                            "steps": 10, "precision": args.precision + ", pressure refined to %g" % wl["refine_tol"],
+                            "workload": "bench.py --workload channel3d_192"}
+    del st, d, wl
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_street(args, rank, world):
+    """The cylinder street as its own bench line: the fused FP32 step with the device outflow update,
+    replayed as a CUDA graph; e2e with every block's velocity and pressure through pinned host buffers
+    each step; roofline of the solver groups; error against the FP64 oracle after 10 steps; CPU baseline
+    of the oracle step; optionally the Strouhal number from a longer run."""
+    import torch
+    import torch.distributed as dist
+    from pict_b200.cylinder_street import TIME_STEP, build_street, cylinder_forces, street_spec, strouhal
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    dom, info, st = street_stepper()
+    cells = dom.getTotalSize()
+    for _ in range(args.warmup):
+        st.step()
+    st.check()
+    G = graph_steps(args)
+    if not args.no_graph:
+        st.capture(steps=G)
+
+    def run_steps(k):
+        if args.no_graph:
+            for _ in range(k):
+                st.step()
+        else:
+            for _ in range(k // G):
+                st.replay()
+
+    run_steps(3 * G)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    sampler = ClockSampler(dev.index)
+    sampler.start()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    run_steps(args.steps)
+    e1.record()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    adv, ps = st.check()
+    ms = e0.elapsed_time(e1)
+    total_cells, ms_max = job_totals(cells, ms, world, dev)
+    value = total_cells * args.steps / (ms_max * 1e-3)
+    roof = roofline_pass(st, dom, args, dev)
+    # e2e: all block fields in and out through pinned host buffers every step
+    if not args.no_graph and G != 1:
+        st.capture(steps=1)
+    dev_state = [t for b in dom.getBlocks() for t in (b.velocity, b.pressure)]
+    host_state = [torch.empty(t.shape, dtype=t.dtype, pin_memory=True) for t in dev_state]
+    for h, t in zip(host_state, dev_state):
+        h.copy_(t)
+    torch.cuda.synchronize()
+    nbytes = sum(h.numel() * h.element_size() for h in host_state)
+    k = max(1, min(args.steps, 50))
+    e0.record()
+    for _ in range(k):
+        for h, t in zip(host_state, dev_state):
+            t.copy_(h, non_blocking=True)
+        st.step() if args.no_graph else st.replay()
+        for h, t in zip(host_state, dev_state):
+            h.copy_(t, non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_cells, e2e_ms = job_totals(cells, e0.elapsed_time(e1), world, dev)
+    e2e = {"value": e2e_cells * k / (e2e_ms * 1e-3), "unit": "cell-steps/s", "h2d_bytes_per_step": nbytes,
+           "d2h_bytes_per_step": nbytes, "steps": k}
+    shedding = None
+    if args.shedding_steps > 0 and rank == 0:
+        lift, drag = [], []
+        for s in range(args.shedding_steps // 10):
+            for _ in range(10):
+                st.step()
+            fx, fy = cylinder_forces(dom, info)
+            drag.append(fx)
+            lift.append(fy)
+        st.check()
+        stn = strouhal(lift, TIME_STEP, every=10)
+        shedding = {"steps": args.shedding_steps, "strouhal": stn, "drag_coefficient_mean_last_half":
+                    float(2 * np.mean(drag[len(drag) // 2:])), "lift_coefficient_amplitude_last_half":
+                    float(2 * (np.max(lift[len(lift) // 2:]) - np.min(lift[len(lift) // 2:])) / 2)}
+    err = cpu = None
+    if rank == 0 and not args.skip_err:
+        err = street_accuracy_check()
+    if rank == 0 and not args.skip_cpu:
+        cpu = street_oracle_rate()
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "cylinder_street", "cells_per_gpu": cells, "blocks": dom.getNumBlocks(),
+                           "pass": "forward", "solver_tol": 1e-6, "correctors": 2, "dt": TIME_STEP,
+                           "precision": "FP32 fields and Krylov vectors, FP64 reductions",
+                           "cuda_graph": not args.no_graph, "cuda_graph_steps": None if args.no_graph else G,
+                           "l2": "working set < L2: latency-bound, no flush (inputs re-read from L2)",
+                           "parallelism": "independent replicas per GPU" if world > 1 else "single GPU"},
+                "clocks": clocks, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "err": err,
+                "shedding": shedding, "gpu_launches": st.kernels_per_step() * args.steps,
+                "solver_iterations": {"advection_max": int(max(i.usedIterations for i in adv)),
+                                      "pressure_max": [int(max(i.usedIterations for i in p)) for p in ps]}}
+        print(json.dumps(line), flush=True)
+
+
+def street_accuracy_check(steps=10):
+    """FP32 street step against the FP64 oracle (1e-12 solves) on the full street after `steps` steps
+    from the same projected state."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import piso_oracle as po
+    from pict_b200.cylinder_street import TIME_STEP, street_spec
+    spec = street_spec()
+    dom, info, st = street_stepper()
+    od = _oracle_street(po, spec)
+    u = np.concatenate([b.velocity.double().cpu().numpy().reshape(2, -1) for b in dom.getBlocks()], axis=1)
+    od.set_velocity_global(u)
+    ob, of = info["outflow"][0]
+    od.blocks[ob].boundaries[of].velocity = dom.getBlock(ob).getBoundary(of).velocity.double().cpu().numpy()
+    for _ in range(steps):
+        st.step()
+        po.advective_outflow(od, info["outflow"], spec["char_vel"], TIME_STEP, tol=1e-5)
+        po.piso_step(od, TIME_STEP, adv_tol=1e-12, p_tol=1e-12)
+    st.check()
+    u = np.concatenate([b.velocity.double().cpu().numpy().reshape(2, -1) for b in dom.getBlocks()], axis=1)
+    p = np.concatenate([b.pressure.double().cpu().numpy().reshape(-1) for b in dom.getBlocks()])
+    ur, pr = od.velocity_global(), od.pressure_global()
+    return {"steps": steps, "velocity_rel_max": float(np.abs(u - ur).max() / np.abs(ur).max()),
+            "pressure_rel_max": float(np.abs(p - pr).max() / np.abs(pr).max()),
+            "reference": "FP64 oracle, solver tol 1e-12, from the same projected state"}
+
+
+def _oracle_street(po, spec):
+    od = po.ODomain(2, spec["viscosity"])
+    for b in spec["blocks"]:
+        od.create_block(coords=b["coords"], velocity=b["velocity"])
+    for op in spec["ops"]:
+        if op[0] == "close_all":
+            od.close_all(op[1])
+        elif op[0] == "connect":
+            od.connect(op[1], op[2], op[3], op[4], *op[5:])
+        elif op[0] == "close":
+            od.close_boundary(op[1], op[2], op[3])
+    od.prepare()
+    return od
+
+
+def street_oracle_rate(steps=2):
+    """FP64 oracle steps of the full street (CPU, one core), tolerances as the GPU step."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import piso_oracle as po
+    from pict_b200.cylinder_street import TIME_STEP, street_spec
+    spec = street_spec()
+    od = _oracle_street(po, spec)
+    po.advective_outflow(od, spec["outflow"], spec["char_vel"], TIME_STEP, tol=1e-5)
+    po.piso_step(od, TIME_STEP, adv_tol=1e-6, p_tol=1e-6)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        po.advective_outflow(od, spec["outflow"], spec["char_vel"], TIME_STEP, tol=1e-5)
+        po.piso_step(od, TIME_STEP, adv_tol=1e-6, p_tol=1e-6)
+    t = time.perf_counter() - t0
+    n = od.N
+    return {"value": n * steps / t, "unit": "cell-steps/s", "cores": 1, "kind": "port",
+            "sample": "full street, %d PISO steps with the outflow update (FP64 NumPy/SciPy restatement, %.1f s)" % (steps, t)}
 
 
 def solver_bytes_per_cell(kind, dims, esz, nrhs=1):
@@ -752,36 +1029,96 @@ def fwd_bwd_pass(st, batch, args, dev, cells, world):
             "grad": "initial velocity and per-simulation viscosity", "grad_finite": bool(torch.isfinite(g).all())}
 
 
-def plain_pass(wl, args, k=8, steps=10):
-    """The plain single-simulation FP32 step (one domain per simulation, CUDA graph) on k simulations
-    at evenly spaced size quantiles, run one after the other: sum(cells x steps) / sum(time)."""
+def plain_pass(wl, args, k=8, steps=10, fb_steps=10, checkpoint=5):
+    """The plain single-simulation FP32 step as the reference runs it: one domain per simulation, FP32
+    with FP64 reductions, advection and pressure solves from zero to the workload tolerance, no
+    refinement (CUDA graph), on k simulations at evenly spaced size quantiles, one after the other:
+    sum(cells x steps) / sum(time).  Also the same simulations' forward + backward (checkpointed rollout
+    of fb_steps steps, loss = final mean kinetic energy, gradient w.r.t. the initial velocity and the
+    viscosity), and the plain step with this build's mixed precision for comparison."""
     import torch
+    from pict_b200.adjoint import PISOAdjoint, rollout
     from pict_b200.engine import PISOStepper
     sel = sample_indices(wl["sides"], k)
-    tot_cells, tot_ms = 0, 0.0
-    for i in sel:
-        s = int(wl["sides"][i])
-        d = make_cavity_domain(s, 1.0 / wl["re"][i], torch.float32)
-        stp = PISOStepper(d, time_step=float(wl["dts"][i]), advection_tol=wl["tol"], pressure_tol=wl["tol"],
-                          **precision_kwargs(args))
-        for _ in range(3):
-            stp.step()
-        stp.capture(steps=1)
-        for _ in range(3):
-            stp.replay()
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(steps):
-            stp.replay()
-        e1.record()
-        torch.cuda.synchronize()
-        tot_ms += e0.elapsed_time(e1)
-        tot_cells += s * s * steps
-        del stp, d
-    return {"value": tot_cells / (tot_ms * 1e-3), "unit": "cell-steps/s",
-            "sample": "sides %s, %d steps each, one simulation at a time" % ([int(wl["sides"][i]) for i in sel], steps)}
+    res = {}
+    for mode in ("fp32", "mixed"):
+        tot_cells, tot_ms, fb_cells, fb_ms = 0, 0.0, 0, 0.0
+        for i in sel:
+            s = int(wl["sides"][i])
+            d = make_cavity_domain(s, 1.0 / wl["re"][i], torch.float32)
+            kw = precision_kwargs(args) if mode == "mixed" else {}
+            stp = PISOStepper(d, time_step=float(wl["dts"][i]), advection_tol=wl["tol"], pressure_tol=wl["tol"], **kw)
+            for _ in range(3):
+                stp.step()
+            stp.capture(steps=1)
+            for _ in range(3):
+                stp.replay()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(steps):
+                stp.replay()
+            e1.record()
+            torch.cuda.synchronize()
+            stp.check()
+            tot_ms += e0.elapsed_time(e1)
+            tot_cells += s * s * steps
+            if mode == "fp32" and not args.skip_bwd:
+                adj = PISOAdjoint(stp)
+                adj.use_graph = not args.no_graph
+                u0 = adj.velocity().clone()
+                nu0 = d._sim_visc.clone()
+                w = 1.0 / (s * s)
+
+                def run():
+                    u0r = u0.clone().requires_grad_(True)
+                    nur = nu0.clone().requires_grad_(True)
+                    out = rollout(adj, u0r, fb_steps, [fb_steps], checkpoint_every=checkpoint, nu=nur)
+                    (0.5 * w * (out[0] * out[0]).sum()).backward()
+                run()
+                torch.cuda.synchronize()
+                e0.record()
+                run()
+                e1.record()
+                torch.cuda.synchronize()
+                fb_ms += e0.elapsed_time(e1)
+                fb_cells += s * s * fb_steps
+                adj.set_velocity(u0)
+            del stp, d
+        res[mode] = (tot_cells / (tot_ms * 1e-3), fb_cells / (fb_ms * 1e-3) if fb_ms > 0 else None)
+    sample = "sides %s, one simulation at a time (its own domain and CUDA graph)" % [int(wl["sides"][i]) for i in sel]
+    out = {"value": res["fp32"][0], "unit": "cell-steps/s", "steps": steps, "sample": sample,
+           "precision": "FP32 fields and Krylov vectors, FP64 reductions, solves from zero to %g, no refinement" % wl["tol"],
+           "fwd_bwd": None if res["fp32"][1] is None else
+           {"value": res["fp32"][1], "unit": "cell-steps/s", "steps": fb_steps, "checkpoint_every": checkpoint,
+            "loss": "final mean kinetic energy", "grad": "initial velocity and viscosity"},
+           "mixed": {"value": res["mixed"][0], "unit": "cell-steps/s",
+                     "precision": "this build's mixed precision (FP64 refinement of the pressure solves)"}}
+    return out
+
+
+def reference_cuda_pass(wl, k=8, timeout=300):
+    """The reference's own CUDA build (oracle/_ref, compiled from its sources) timed on this GPU through
+    its stock operators: the 64 x 64 lid cavity and the plain sample's simulations one at a time
+    (oracle/time_ref_cuda.py, in a subprocess).  None when the build is absent."""
+    ref = os.path.join(ROOT, "oracle", "_ref")
+    if not (os.path.isdir(ref) and any(f.startswith("PISOtorch") and f.endswith(".so") for f in os.listdir(ref))):
+        return None
+    cmd = [sys.executable, os.path.join(ROOT, "oracle", "time_ref_cuda.py")]
+    if wl.get("sides") is not None:
+        sel = sample_indices(wl["sides"], k)
+        cmd += ["--sides", ",".join(str(int(wl["sides"][i])) for i in sel),
+                "--re", ",".join(repr(float(wl["re"][i])) for i in sel),
+                "--dts", ",".join(repr(float(wl["dts"][i])) for i in sel)]
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
+        line = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+        if r.returncode != 0 or not line:
+            return {"error": "rc %d: %s" % (r.returncode, (r.stderr or r.stdout)[-300:])}
+        return json.loads(line[-1])
+    except subprocess.TimeoutExpired:
+        return {"error": "timed out after %d s" % timeout}
 
 
 def grad_check(wl, steps=3):
@@ -875,43 +1212,104 @@ def channel_accuracy_check(wl, args, n=(24, 12, 12), steps=10):
             "reference": "FP64 oracle, solver tol 1e-12"}
 
 
-def accuracy_check(wl, args):
-    """Relative error of the FP32 batched step against the FP64 oracle (tight solves) on the two
-    smallest simulations after 10 steps."""
+_ORACLE_FIELDS = {}
+
+
+def accuracy_picks(sides):
+    """The smallest, the largest and the simulations at the 25/50/75 % size quantiles."""
+    order = np.argsort(sides)
+    n = len(order)
+    return [int(order[min(n - 1, int(q * (n - 1) + 0.5))]) for q in (0.0, 0.25, 0.5, 0.75, 1.0)]
+
+
+def accuracy_check(wl, args, steps=10):
+    """Per-field relative error of the batched FP32 step (this run's precision settings) against the FP64
+    oracle with 1e-12 solves after `steps` steps, per simulation, on the smallest and the largest
+    simulation and those at the 25/50/75 % size quantiles (advanced together as one batch)."""
     import torch
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import piso_oracle as po
     from pict_b200.batch import BatchDomain
     from pict_b200.engine import PISOStepper
-    order = np.argsort(wl["sides"])[:2]
-    doms = [make_cavity_domain(int(wl["sides"][i]), 1.0 / wl["re"][i], torch.float32) for i in order]
-    dts = [wl["dts"][i] for i in order]
+    picks = accuracy_picks(wl["sides"])
+    doms = [make_cavity_domain(int(wl["sides"][i]), 1.0 / wl["re"][i], torch.float32) for i in picks]
+    dts = [wl["dts"][i] for i in picks]
     b = BatchDomain(doms, time_steps=dts)
     st = PISOStepper(b, time_step=dts[0], advection_tol=wl["tol"], pressure_tol=wl["tol"], **precision_kwargs(args))
-    steps = 10
     for _ in range(steps):
         st.step()
     st.check()
-    out = {"steps": steps, "sims": [int(wl["sides"][i]) for i in order]}
-    eu, ep = [], []
-    for k, i in enumerate(order):
+    per = []
+    for k, i in enumerate(picks):
         s = int(wl["sides"][i])
-        d = po.ODomain(2, 1.0 / wl["re"][i])
-        bi = d.create_block(coords=cavity_coords(s))
-        d.close_all(bi)
-        d.close_boundary(bi, "-y", np.array([[1.0, 0.0]]))
-        d.prepare()
-        for _ in range(steps):
-            po.piso_step(d, dts[k], adv_tol=1e-12, p_tol=1e-12)
+        key = (s, float(wl["re"][i]), float(dts[k]), steps)
+        if key not in _ORACLE_FIELDS:  # the same simulations are checked for several precisions
+            d = po.ODomain(2, 1.0 / wl["re"][i])
+            bi = d.create_block(coords=cavity_coords(s))
+            d.close_all(bi)
+            d.close_boundary(bi, "-y", np.array([[1.0, 0.0]]))
+            d.prepare()
+            for _ in range(steps):
+                po.piso_step(d, dts[k], adv_tol=1e-12, p_tol=1e-12)
+            _ORACLE_FIELDS[key] = (d.velocity_global(), d.pressure_global())
         u = doms[k].getBlock(0).velocity.double().cpu().numpy().reshape(2, -1)
         p = doms[k].getBlock(0).pressure.double().cpu().numpy().reshape(-1)
-        ur, pr = d.velocity_global(), d.pressure_global()
-        eu.append(float(np.abs(u - ur).max() / np.abs(ur).max()))
-        ep.append(float(np.abs(p - pr).max() / np.abs(pr).max()))
-    out["velocity_rel_max"] = max(eu)
-    out["pressure_rel_max"] = max(ep)
-    out["reference"] = "FP64 oracle, solver tol 1e-12"
-    return out
+        ur, pr = _ORACLE_FIELDS[key]
+        per.append({"side": s, "re": float(wl["re"][i]),
+                    "velocity_rel_max": float(np.abs(u - ur).max() / np.abs(ur).max()),
+                    "pressure_rel_max": float(np.abs(p - pr).max() / np.abs(pr).max())})
+    return {"steps": steps, "per_simulation": per, "sims": [q["side"] for q in per],
+            "velocity_rel_max": max(q["velocity_rel_max"] for q in per),
+            "pressure_rel_max": max(q["pressure_rel_max"] for q in per),
+            "reference": "FP64 oracle, solver tol 1e-12; simulations at the size quantiles 0/25/50/75/100 %"}
+
+
+def grad_check_mixed(wl, args, steps=3, eps=1e-4):
+    """Viscosity gradient of the final mean kinetic energy through the timed precision (FP32 fields, FP64
+    reductions and pressure refinement) against central finite differences of the FP64 step (solves to
+    1e-12), on the two smallest simulations: the error of the FP32 adjoint itself."""
+    import torch
+    from pict_b200.batch import BatchDomain
+    from pict_b200.engine import PISOStepper
+    from pict_b200.adjoint import PISOAdjoint, rollout
+    order = np.argsort(wl["sides"])[:2]
+
+    def batch(dtype):
+        doms = [make_cavity_domain(int(wl["sides"][i]), 1.0 / wl["re"][i], dtype) for i in order]
+        return BatchDomain(doms, time_steps=[wl["dts"][i] for i in order])
+    b32 = batch(torch.float32)
+    st32 = PISOStepper(b32, time_step=float(wl["dts"][order[0]]), advection_tol=wl["tol"], pressure_tol=wl["tol"],
+                       **precision_kwargs(args))
+    # transposed solves to 1e-6 relative to their right-hand side (the loss gradient is ~1e-3 per cell)
+    adj = PISOAdjoint(st32, relative_tolerance=True)
+    n_s = torch.diff(b32._sim_cells.long()).cuda()
+    w32 = torch.repeat_interleave(1.0 / n_s.float(), n_s).repeat(2)
+    nu32 = b32._sim_visc.clone().requires_grad_(True)
+    out = rollout(adj, adj.velocity().clone(), steps, [steps], nu=nu32)
+    (0.5 * (w32 * out[0] * out[0]).sum()).backward()
+    b64 = batch(torch.float64)
+    st64 = PISOStepper(b64, time_step=float(wl["dts"][order[0]]), advection_tol=1e-12, pressure_tol=1e-12)
+    adj64 = PISOAdjoint(st64)
+    u0 = adj64.velocity().clone()
+    nu0 = b64._sim_visc.clone()
+    w = torch.repeat_interleave(1.0 / n_s.double(), n_s).repeat(2)
+    errs = []
+    for s in range(2):
+        def loss(e):
+            nu = nu0.clone()
+            nu[s] *= 1 + e
+            b64._sim_visc.copy_(nu)
+            adj64.set_velocity(u0)
+            for _ in range(steps):
+                st64.step()
+            st64.check()
+            u = adj64.velocity()
+            return float(0.5 * (w * u * u).sum())
+        fd = (loss(eps) - loss(-eps)) / (2 * eps)
+        ad = float(nu32.grad[s].double() * nu0[s])
+        errs.append(abs(ad - fd) / max(abs(fd), 1e-30))
+    return {"rel_err_vs_fd_max": max(errs), "sims": [int(wl["sides"][i]) for i in order], "steps": steps,
+            "dtype": "f32 adjoint (timed precision) vs FP64 central differences (relative step %g)" % eps}
 
 
 def main():
@@ -925,7 +1323,7 @@ def main():
     ap.add_argument("--warm-advection", type=int, default=1,
                     help="mixed precision: start each advection solve from the current velocity (1) or from zero (0)")
     ap.add_argument("--workload", default="batched_cavities_256",
-                    choices=["batched_cavities_256", "lid_cavity_64", "channel3d_192"])
+                    choices=["batched_cavities_256", "lid_cavity_64", "channel3d_192", "cylinder_street"])
     ap.add_argument("--group-size", type=int, default=0)
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
@@ -941,6 +1339,13 @@ def main():
     ap.add_argument("--skip-fp32", action="store_true")
     ap.add_argument("--autotune", type=int, default=1, help="1: pick tile size / CTA cap / CG variant by timing")
     ap.add_argument("--skip-plain", action="store_true")
+    ap.add_argument("--skip-ref-cuda", action="store_true", help="skip timing the reference's own CUDA build")
+    ap.add_argument("--skip-extras", action="store_true", help="skip the brief timings of the other configurations")
+    ap.add_argument("--graph-steps", type=int, default=10,
+                    help="steps per captured CUDA graph (1 if --steps is not a multiple)")
+    ap.add_argument("--shedding-steps", type=int, default=0,
+                    help="cylinder_street: further steps after the timed ones, lift recorded every 10 steps, for "
+                         "the Strouhal number")
     ap.add_argument("--fb-steps", type=int, default=10, help="steps of the forward+backward rollout")
     ap.add_argument("--checkpoint", type=int, default=5, help="checkpoint interval of the rollout")
     args = ap.parse_args()
@@ -960,7 +1365,10 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        run_pict(args, rank, world)
+        if args.workload == "cylinder_street":
+            run_street(args, rank, world)
+        else:
+            run_pict(args, rank, world)
     finally:
         if world > 1:
             import torch.distributed as dist

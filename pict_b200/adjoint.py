@@ -62,8 +62,14 @@ class PISOAdjoint:
     """
 
     def __init__(self, stepper: PISOStepper, adjoint_advection_tol: Optional[float] = None,
-                 adjoint_pressure_tol: Optional[float] = None):
+                 adjoint_pressure_tol: Optional[float] = None, relative_tolerance: bool = False):
         self.st = stepper
+        # relative_tolerance: every transposed solve first scales its right-hand side to unit RMS per
+        # system (on the device) and scales the solution back, so that the (absolute, RMS) tolerance acts
+        # relative to the adjoint's own magnitude; without it the adjoint solves stop at the absolute
+        # tolerance, as the reference's backward solves do (PISOtorch_diff.py:331-372), which for a
+        # small loss gradient is a loose relative tolerance
+        self.relative = bool(relative_tolerance)
         d = stepper.domain
         P._check(stepper.normalize_pressure, "the adjoint needs normalize_pressure=True (mean-free pressure)")
         self.dom = d
@@ -96,6 +102,10 @@ class PISOAdjoint:
         self.info = torch.zeros((D + 1) * self.ns * _lib.SOLVE_INFO_BYTES, dtype=torch.uint8, device=self.dev)
         self.block_scratch = torch.zeros(max(1, len(d.getBlocks())), dtype=torch.float64, device=self.dev)
         self.sim_nu_bar = z(self.ns)
+        sc = d._sim_cells.long().to(self.dev)
+        self._sim_start, self._sim_end = sc[:-1], sc[1:]
+        self._sim_n = (sc[1:] - sc[:-1]).double()
+        self._cell_sim = torch.repeat_interleave(torch.arange(self.ns, device=self.dev), sc[1:] - sc[:-1])
 
     # ------------------------------------------------------------------ state helpers
     def _stream(self):
@@ -205,8 +215,13 @@ class PISOAdjoint:
                 self.pbar.add_(pbar_out)
             check(lib.pict_sim_mean_project(desc, _p(self.pbar), s), "mean projection")
             self.lam.zero_()
+            if self.relative:
+                scale = self._rms_scale(self.pbar, 1)
+                self.pbar.div_(scale)
             check(lib.pict_solve(desc, _p(self.Pwork), _p(self.pbar), _p(self.lam), ctypes.byref(self.p_params),
                                  _p(info_p), P._ptr(st.ws), st.ws_bytes, s), "adjoint pressure solve")
+            if self.relative:
+                self.lam.mul_(scale)
             self._check_info(info_p, "adjoint pressure")
             check(lib.pict_divergence_grad(desc, _p(self.lam), _p(self.hbar), _p(self.vbbar), s), "divergence grad")
             U = tape.ustar if k == 0 else tape.U[k]
@@ -217,12 +232,26 @@ class PISOAdjoint:
             ucur = self.Ubar.clone() if k > 0 else self.Ubar
         # advection solve (transposed, all components) and assembly
         self.rhsbar.zero_()
+        if self.relative:
+            scale = self._rms_scale(self.Ubar, self.D)
+            self.Ubar.div_(scale)
         check(lib.pict_solve(desc, _p(tape.C), _p(self.Ubar), _p(self.rhsbar), ctypes.byref(self.adv_params),
                              _p(info_a), P._ptr(st.ws), st.ws_bytes, s), "adjoint advection solve")
+        if self.relative:
+            self.rhsbar.mul_(scale)
         self._check_info(info_a, "adjoint advection")
         check(lib.pict_advection_grad(desc, dt, _p(tape.ustar), _p(self.rhsbar), _p(self.Cbar), _p(self.Abar),
                                       _p(self.unbar), _p(self.nubar), _p(self.vbbar), src, s), "advection grad")
         return self.unbar.clone()
+
+    def _rms_scale(self, v, ncomp):
+        """Per-system RMS of v [ncomp*N] spread to every entry [ncomp*N] (FP64 sums, no host sync; the
+        cumulative sum keeps the per-system sums in a fixed order)."""
+        sq = (v.double().reshape(ncomp, self.N) ** 2).sum(0)
+        c = torch.cat([sq.new_zeros(1), torch.cumsum(sq, 0)])
+        rms = torch.sqrt((c[self._sim_end] - c[self._sim_start]) / (self._sim_n * ncomp))
+        rms = rms.clamp_min(float(torch.finfo(self.dtype).tiny) * 1e6).to(self.dtype)
+        return rms[self._cell_sim].repeat(ncomp)
 
     def _check_info(self, info, what):
         if not getattr(self, "check_solves", False):

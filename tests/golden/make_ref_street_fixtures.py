@@ -15,7 +15,8 @@ Written to ``--out``:
   20 steps, the outflow face velocity and the solver reports;
 * ``ref_street_full_f32.npz`` (unless --quick): the full street (27,648 cells) in FP32, --full-steps
   steps with 1e-6 solves, the force on the cylinder every 10 steps, the final fields and the
-  reference's wall-clock time per step.
+  reference's wall-clock time per step;
+* ``ref_street_full_f64.npz`` (unless --quick): the same in FP64 with 1e-10 solves, --full64-steps steps.
 
 Usage (GPU machine):  python tests/golden/make_ref_street_fixtures.py --out <dir> [--quick] [--full-steps N]
 """
@@ -51,7 +52,7 @@ def outflow_update(dom, info, dt):
                                 torch.tensor([dt], dtype=dom.getDtype()).cuda())
 
 
-def make_divergence_free(R, dom, info, tol):
+def make_divergence_free(R, dom, info, tol, maxit=1000):
     """Simulation.make_divergence_free with one corrector, orthogonal (PISOtorch_simulation.py:985-1052)."""
     ts = torch.tensor([1.0], dtype=dom.getDtype())
     dom.setA(torch.ones_like(dom.A))
@@ -62,7 +63,7 @@ def make_divergence_free(R, dom, info, tol):
     dom.UpdateDomainData()
     R.SetupPressureMatrix(dom, ts, 0, False)
     R.SetupPressureRHSdiv(dom, ts, 0, False, timeStepNorm=False)
-    p, inf = solve(R, dom.P, dom.pressureRHSdiv, False, tol, maxit=1000)
+    p, inf = solve(R, dom.P, dom.pressureRHSdiv, False, tol, maxit=maxit)
     p = p - torch.mean(p)
     dom.setPressureResult(p)
     dom.UpdateDomainData()
@@ -110,10 +111,12 @@ def reduced_fixture(R, steps=20, tol=1e-12):
     return out
 
 
-def full_fixture(R, steps, tol=1e-6, every=10):
+def full_fixture(R, steps, tol=1e-6, every=10, dtype=torch.float32):
     spec = street_spec()
-    dom, info = build_street(spec, module=R, dtype=torch.float32)
-    make_divergence_free(R, dom, info, tol)
+    dom, info = build_street(spec, module=R, dtype=dtype)
+    # the projection's iteration cap is the driver's 1000 (PISOtorch_simulation.py:985); tight FP64 solves
+    # of the full street need more
+    make_divergence_free(R, dom, info, tol, maxit=1000 if dtype == torch.float32 else 5000)
     forces, infos = [], []
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -136,17 +139,28 @@ def main():
     ap.add_argument("--out", required=True, help="directory the fixtures are written to")
     ap.add_argument("--quick", action="store_true", help="only the reduced FP64 fixture")
     ap.add_argument("--full-steps", type=int, default=2000)
+    ap.add_argument("--full64-steps", type=int, default=400)
+    ap.add_argument("--only", default="", help="comma list of fixtures to write: street16,full,full64")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
     R = ref_module()
-    fx = reduced_fixture(R)
-    np.savez_compressed(os.path.join(args.out, "ref_street16_f64.npz"), **fx)
-    print("fixture street16_f64: iterations", fx["infos"][:, 1].astype(int).tolist()[:12], flush=True)
-    if not args.quick:
-        fx = full_fixture(R, args.full_steps)
-        np.savez_compressed(os.path.join(args.out, "ref_street_full_f32.npz"), **fx)
-        print("fixture street_full_f32: %d steps in %.1f s (%.2f ms/step), all converged: %s, last forces %s"
-              % (fx["steps"], fx["seconds"], 1e3 * fx["seconds"] / fx["steps"], bool(fx["converged"].all()),
+    only = set(args.only.split(",")) if args.only else {"street16", "full", "full64"}
+    if "street16" in only:
+        fx = reduced_fixture(R)
+        np.savez_compressed(os.path.join(args.out, "ref_street16_f64.npz"), **fx)
+        print("fixture street16_f64: iterations", fx["infos"][:, 1].astype(int).tolist()[:12], flush=True)
+    if args.quick:
+        return
+    runs = []
+    if "full" in only:
+        runs.append(("ref_street_full_f32.npz", args.full_steps, 1e-6, torch.float32))
+    if "full64" in only:
+        runs.append(("ref_street_full_f64.npz", args.full64_steps, 1e-10, torch.float64))
+    for name, steps, tol, dtype in runs:
+        fx = full_fixture(R, steps, tol=tol, dtype=dtype)
+        np.savez_compressed(os.path.join(args.out, name), **fx)
+        print("fixture %s: %d steps in %.1f s (%.2f ms/step), all converged: %s, last forces %s"
+              % (name, fx["steps"], fx["seconds"], 1e3 * fx["seconds"] / fx["steps"], bool(fx["converged"].all()),
                  fx["forces"][-3:].tolist()), flush=True)
 
 

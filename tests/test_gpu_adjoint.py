@@ -140,3 +140,55 @@ def test_fp32_gradient_close_to_fp64():
     gu32, gn32 = res[1]
     assert float((gu32 - gu64).abs().max() / gu64.abs().max()) < 1e-4
     assert float((gn32 - gn64).abs().max() / gn64.abs().max()) < 1e-3
+
+
+def test_mixed_precision_viscosity_gradient_relative_adjoint():
+    """The timed precision (FP32 fields, FP64 reductions, FP64 pressure refinement) with adjoint solves to
+    1e-6 relative to their right-hand side: the viscosity gradient of the mean kinetic energy of two
+    cavities (a loss whose gradient is ~1e-3 per cell) within 1e-4 of central differences of the FP64
+    step, where adjoint solves to the same absolute tolerance are off by ~1e-2."""
+    from pict_b200.adjoint import PISOAdjoint, rollout
+    from pict_b200.batch import BatchDomain
+    from pict_b200.engine import PISOStepper
+    from setups import lid_cavity
+    sides, dts, steps = (32, 40), (0.5 / 32, 0.5 / 40), 3
+
+    def batch(dtype):
+        return BatchDomain([build_product(lid_cavity(s, viscosity=1.0 / 1500), dtype) for s in sides], time_steps=list(dts))
+    b32 = batch(torch.float32)
+    st32 = PISOStepper(b32, time_step=dts[0], advection_tol=1e-6, pressure_tol=1e-6, pressure_refine=1,
+                       refine_tol=1e-9, warm_start_pressure=True, pressure_first_solve=False, refine_solver="auto")
+    n_s = torch.diff(b32._sim_cells.long()).cuda()
+    grads = []
+    for relative in (True, False):
+        for b in b32.getBlocks():
+            b.velocity.zero_()
+            b.pressure.zero_()
+        adj = PISOAdjoint(st32, relative_tolerance=relative)
+        w = torch.repeat_interleave(1.0 / n_s.float(), n_s).repeat(2)
+        nu = b32._sim_visc.clone().requires_grad_(True)
+        out = rollout(adj, adj.velocity().clone(), steps, [steps], nu=nu)
+        (0.5 * (w * out[0] * out[0]).sum()).backward()
+        grads.append(nu.grad.double().cpu())
+    b64 = batch(torch.float64)
+    st64 = PISOStepper(b64, time_step=dts[0], advection_tol=1e-12, pressure_tol=1e-12)
+    adj64 = PISOAdjoint(st64)
+    u0 = adj64.velocity().clone()
+    nu0 = b64._sim_visc.clone()
+    w64 = torch.repeat_interleave(1.0 / n_s.double(), n_s).repeat(2)
+    for s in range(2):
+        def loss(e):
+            nu_ = nu0.clone()
+            nu_[s] *= 1 + e
+            b64._sim_visc.copy_(nu_)
+            adj64.set_velocity(u0)
+            for _ in range(steps):
+                st64.step()
+            st64.check()
+            u = adj64.velocity()
+            return float(0.5 * (w64 * u * u).sum())
+        fd = (loss(1e-4) - loss(-1e-4)) / 2e-4
+        rel = [abs(float(g[s]) * float(nu0[s]) - fd) / abs(fd) for g in grads]
+        print("sim %d: FD %.6e, relative error of the FP32 adjoint: relative solves %.2e, absolute solves %.2e"
+              % (s, fd, rel[0], rel[1]))
+        assert rel[0] < 1e-4
