@@ -760,8 +760,8 @@ def run_street(args, rank, world):
 
 
 def street_accuracy_check(steps=10):
-    """FP32 street step against the FP64 oracle (1e-12 solves) on the full street after `steps` steps
-    from the same projected state."""
+    """FP32 street step against the FP64 oracle (1e-10 solves: tighter ones stall at the FP64 floor of the
+    full street's pressure system) on the full street after `steps` steps from the same projected state."""
     import torch
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import piso_oracle as po
@@ -776,14 +776,14 @@ def street_accuracy_check(steps=10):
     for _ in range(steps):
         st.step()
         po.advective_outflow(od, info["outflow"], spec["char_vel"], TIME_STEP, tol=1e-5)
-        po.piso_step(od, TIME_STEP, adv_tol=1e-12, p_tol=1e-12)
+        po.piso_step(od, TIME_STEP, adv_tol=1e-10, p_tol=1e-10)
     st.check()
     u = np.concatenate([b.velocity.double().cpu().numpy().reshape(2, -1) for b in dom.getBlocks()], axis=1)
     p = np.concatenate([b.pressure.double().cpu().numpy().reshape(-1) for b in dom.getBlocks()])
     ur, pr = od.velocity_global(), od.pressure_global()
     return {"steps": steps, "velocity_rel_max": float(np.abs(u - ur).max() / np.abs(ur).max()),
             "pressure_rel_max": float(np.abs(p - pr).max() / np.abs(pr).max()),
-            "reference": "FP64 oracle, solver tol 1e-12, from the same projected state"}
+            "reference": "FP64 oracle, solver tol 1e-10, from the same projected state"}
 
 
 def _oracle_street(po, spec):
@@ -1334,7 +1334,9 @@ def main():
     ap.add_argument("--first-solve", type=int, default=0,
                     help="mixed precision: 1 = FP32 CG pressure solve before the refinement, 0 = refine from the "
                          "warm-start pressure")
-    ap.add_argument("--mg-iterations", type=int, default=12, help="multigrid PCG iterations per correction")
+    ap.add_argument("--mg-iterations", type=int, default=9,
+                    help="multigrid PCG iterations per correction (9: the fewest that reach the 1e-9 RMS refinement "
+                         "target on batched_cavities_256)")
     ap.add_argument("--skip-bwd", action="store_true")
     ap.add_argument("--skip-fp32", action="store_true")
     ap.add_argument("--autotune", type=int, default=1, help="1: pick tile size / CTA cap / CG variant by timing")

@@ -295,8 +295,15 @@ typedef struct pict_mg_level {
     int32_t num_tiles;         /* work tiles of the level (levels >= 1; level 0 runs on the domain's tiles) */
     int32_t max_block_cells;   /* cells of the largest block of the level */
     const int32_t* tiles;      /* [num_tiles][4]: system, block, first cell, cell count (device) */
+    int32_t max_block_sx;      /* largest x size (cells per row) of a block of the level */
+    int32_t pad0;
 } pict_mg_level_t;
 
+/* Process-wide choice of the 2D PCG SpMV kernel (no counterpart in the reference): 1 (default) stages
+ * each work tile's operands in shared memory with asynchronous bulk copies (cp.async.bulk on an mbarrier,
+ * double-buffered across the tiles of a persistent grid) wherever the operands are 16-byte aligned and
+ * the stage fits; 0 runs the gather kernel only.  Both give the same per-warp partial sums. */
+void pict_mg_set_bulk_staging(int32_t enable);
 /* Galerkin coarse operator R A P of `fine` into coarse->coef (aggregates of 2^D cells). */
 pict_status_t pict_mg_galerkin(const pict_mg_level_t* fine, const pict_mg_level_t* coarse, void* stream);
 int64_t pict_pcg_mg_workspace_bytes(const pict_domain_t* dom, const pict_mg_level_t* levels, int32_t num_levels);

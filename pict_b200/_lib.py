@@ -121,6 +121,8 @@ class MgLevel(ctypes.Structure):
         ("num_tiles", c_i32),
         ("max_block_cells", c_i32),
         ("tiles", c_vp),
+        ("max_block_sx", c_i32),
+        ("pad0", c_i32),
     ]
 
 
@@ -186,6 +188,7 @@ SIGNATURES = {
     "pict_refine_residual": (c_i32, [_PD, c_vp, c_vp, c_vp, c_vp, c_vp, c_i32, c_vp, c_vp]),
     "pict_refine_update": (c_i32, [_PD, c_vp, c_vp, c_vp]),
     "pict_refine_finish": (c_i32, [_PD, c_vp, c_vp, c_i32, c_i32, c_vp, c_vp]),
+    "pict_mg_set_bulk_staging": (None, [c_i32]),
     "pict_mg_galerkin": (c_i32, [ctypes.POINTER(MgLevel), ctypes.POINTER(MgLevel), c_vp]),
     "pict_pcg_mg_workspace_bytes": (ctypes.c_int64, [_PD, ctypes.POINTER(MgLevel), c_i32]),
     "pict_pcg_mg": (c_i32, [_PD, ctypes.POINTER(MgLevel), c_i32, c_vp, c_vp, c_i32, ctypes.c_double, c_i32, c_vp, c_vp,

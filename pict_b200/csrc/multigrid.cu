@@ -22,10 +22,14 @@
 // stored: x0 = w b / diag is formed where it is read.
 #include <cmath>
 #include <cstdio>
+#include "bulk.cuh"
 #include "common.cuh"
 #include "launch.h"
 
 namespace pict {
+
+// 1: 2D PCG SpMV with bulk-copy staging where it applies (default); 0: the gather kernel only
+static int g_mg_bulk = 1;
 
 // block of a level: first cell, sizes, periodic flags, system, and the coarsening shifts (log2 of the
 // factor, 0 or 1 per axis) from the next finer level
@@ -708,6 +712,176 @@ __global__ void __launch_bounds__(MG_TPB) k_pcg_spmv_dot(pict_domain_t dom, pict
     if ((threadIdx.x & 31) == 0) *mg_warp_part(part, 1) = acc;
 }
 
+// k_pcg_spmv_dot for 2D tiles with its operands staged by asynchronous bulk copies: a persistent grid
+// in which every CTA walks the tiles blockIdx.x, blockIdx.x + gridDim.x, ...; per tile one thread issues
+// bulk copies of z and p_old over the tile plus one block row on each side and of the K coefficient
+// rows of the tile, completing on the mbarrier of one of two stage buffers, so the next tile's copies
+// are in flight while the current tile is computed from shared memory.  A neighbour across a y-periodic
+// wrap lies outside the stage and is read from global memory.  Cells, arithmetic and per-warp partials
+// are those of k_pcg_spmv_dot.  A stage buffer holds z and p_old ([cap_h] each) and the coefficient rows
+// ([K][cap_t]); err is set if a wait gives up.
+constexpr long long MG_WAIT_LIMIT = 1ll << 22;
+constexpr int MG_BULK_MAX_TILES = 64;  // tiles per CTA of the persistent grid (descriptors kept in shared memory)
+
+template <typename T>
+__global__ void __launch_bounds__(MG_TPB) k_pcg_spmv_dot_bulk(pict_domain_t dom, pict_mg_level_t L,
+                                                              const T* __restrict__ z, const T* __restrict__ pold,
+                                                              T* __restrict__ pnew, T* __restrict__ q,
+                                                              const double* __restrict__ sc, int first,
+                                                              double* __restrict__ part, int cap_h, int cap_t,
+                                                              int* __restrict__ err) {
+    constexpr int K = 5;
+    extern __shared__ __align__(128) unsigned char mg_bulk_raw[];
+    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ MgTile s_tl[MG_BULK_MAX_TILES];
+    __shared__ MgBlock s_bk[MG_BULK_MAX_TILES];
+    const T* __restrict__ coef = reinterpret_cast<const T*>(L.coef);
+    const int N = L.num_cells;
+    const int nt = dom.num_tiles;
+    const int per_buf = 2 * cap_h + K * cap_t;
+    T* const stage = reinterpret_cast<T*>(mg_bulk_raw);
+    const T* const pv_src = first ? z : pold;  // the first direction starts from p_old = z (beta = 0)
+    // this CTA's tiles blockIdx.x + j gridDim.x and their blocks, loaded once (the host guarantees at most
+    // MG_BULK_MAX_TILES per CTA)
+    const int my_tiles = (int)blockIdx.x < nt ? (nt - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    for (int j = threadIdx.x; j < my_tiles; j += blockDim.x) {
+        s_tl[j] = mg_tile(dom.tiles, blockIdx.x + j * gridDim.x);
+        s_bk[j] = mg_block(L, s_tl[j].blk);
+    }
+
+    struct Runs {
+        BulkRun<T> z, p, c[K];
+        int lo;
+    };
+    auto runs_of = [&](const MgTile& tl, const MgBlock& B) {
+        Runs R;
+        R.lo = max(B.off, tl.s0 - B.sx);
+        const int hi = min(B.off + B.sx * B.sy, tl.s0 + tl.cnt + B.sx);
+        R.z = bulk_run(z, R.lo, hi - R.lo);
+        R.p = bulk_run(pv_src, R.lo, hi - R.lo);
+#pragma unroll
+        for (int f = 0; f < K; ++f) R.c[f] = bulk_run(coef, (long long)f * N + tl.s0, tl.cnt);
+        return R;
+    };
+    auto issue = [&](int j, int b) {  // one thread: tile j of this CTA into stage buffer b
+        const Runs R = runs_of(s_tl[j], s_bk[j]);
+        T* buf = stage + (size_t)b * per_buf;
+        uint32_t bytes = R.z.bytes + (first ? 0u : R.p.bytes);
+#pragma unroll
+        for (int f = 0; f < K; ++f) bytes += R.c[f].bytes;
+        fence_proxy_async_smem();
+        mbar_arrive_expect_tx(&bar[b], bytes);
+        bulk_issue(R.z, buf, &bar[b]);
+        if (!first) bulk_issue(R.p, buf + cap_h, &bar[b]);
+#pragma unroll
+        for (int f = 0; f < K; ++f) bulk_issue(R.c[f], buf + 2 * cap_h + f * cap_t, &bar[b]);
+    };
+
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && my_tiles > 0) issue(0, 0);
+    for (int k = 0; k < my_tiles; ++k) {
+        const int b = k & 1;
+        if (threadIdx.x == 0 && k + 1 < my_tiles) issue(k + 1, b ^ 1);
+        const MgTile tl = s_tl[k];
+        const MgBlock B = s_bk[k];
+        const int t = blockIdx.x + k * gridDim.x;
+        const Runs R = runs_of(tl, B);
+        T* const buf = stage + (size_t)b * per_buf;
+        T* const zs = buf;
+        T* const ps = first ? buf : buf + cap_h;
+        bulk_tail(R.z, zs);
+        if (!first) bulk_tail(R.p, ps);
+#pragma unroll
+        for (int f = 0; f < K; ++f) bulk_tail(R.c[f], buf + 2 * cap_h + f * cap_t);
+        const bool ok = mbar_wait(&bar[b], (k >> 1) & 1, MG_WAIT_LIMIT);
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) {
+                atomicExch(err, 1);
+                // the other buffer's copies may still be in flight: wait for them before the CTA ends
+                if (k + 1 < my_tiles) mbar_wait(&bar[b ^ 1], ((k + 1) >> 1) & 1, MG_WAIT_LIMIT);
+            }
+            __syncthreads();
+            return;
+        }
+        const T m = (T)sc[MG_SC * tl.sys + 4];
+        const T bt = first ? T(0) : (T)sc[MG_SC * tl.sys + 2];
+        const int hz = R.z.lead - R.lo, hp = R.p.lead - R.lo;  // stage index of global cell j: j + hz / j + hp
+        const T* const c0 = buf + 2 * cap_h + R.c[0].lead;
+        const T* const c1 = buf + 2 * cap_h + 1 * cap_t + R.c[1].lead;
+        const T* const c2 = buf + 2 * cap_h + 2 * cap_t + R.c[2].lead;
+        const T* const c3 = buf + 2 * cap_h + 3 * cap_t + R.c[3].lead;
+        const T* const c4 = buf + 2 * cap_h + 4 * cap_t + R.c[4].lead;
+        double acc = 0.0;
+        for (int base = 0; base < tl.cnt; base += MG_PASS) {
+            T pvk[MG_CPT], qvk[MG_CPT];
+#pragma unroll
+            for (int kk = 0; kk < MG_CPT; ++kk) {
+                const int l0 = base + kk * MG_TPB + (int)threadIdx.x;
+                const int l = l0 < tl.cnt ? l0 : tl.cnt - 1;
+                const int i = tl.s0 + l;
+                const int li = i - B.off;
+                const int y = li / B.sx, x = li - y * B.sx;
+                const T pi = (zs[i + hz] - m) + bt * ps[i + hp];
+                T qi = c0[l] * pi;
+                // -x, +x: in the stage (a periodic wrap stays in the row)
+                {
+                    const bool okm = x > 0 || B.px;
+                    const int jm = x > 0 ? i - 1 : (B.px ? i + B.sx - 1 : i);
+                    const T pj = (zs[jm + hz] - m) + bt * ps[jm + hp];
+                    qi += okm ? c1[l] * pj : T(0);
+                }
+                {
+                    const bool okp = x + 1 < B.sx || B.px;
+                    const int jp = x + 1 < B.sx ? i + 1 : (B.px ? i - B.sx + 1 : i);
+                    const T pj = (zs[jp + hz] - m) + bt * ps[jp + hp];
+                    qi += okp ? c2[l] * pj : T(0);
+                }
+                // -y, +y: in the stage, except across a periodic wrap
+                {
+                    const bool okm = y > 0 || B.py;
+                    T pj;
+                    if (y > 0) {
+                        pj = (zs[i - B.sx + hz] - m) + bt * ps[i - B.sx + hp];
+                    } else {
+                        const int j = B.py ? B.off + x + B.sx * (B.sy - 1) : i;
+                        pj = B.py ? (z[j] - m) + bt * pv_src[j] : pi;
+                    }
+                    qi += okm ? c3[l] * pj : T(0);
+                }
+                {
+                    const bool okp = y + 1 < B.sy || B.py;
+                    T pj;
+                    if (y + 1 < B.sy) {
+                        pj = (zs[i + B.sx + hz] - m) + bt * ps[i + B.sx + hp];
+                    } else {
+                        const int j = B.py ? B.off + x : i;
+                        pj = B.py ? (z[j] - m) + bt * pv_src[j] : pi;
+                    }
+                    qi += okp ? c4[l] * pj : T(0);
+                }
+                pvk[kk] = pi;
+                qvk[kk] = qi;
+            }
+#pragma unroll
+            for (int kk = 0; kk < MG_CPT; ++kk) {
+                const int l = base + kk * MG_TPB + (int)threadIdx.x;
+                if (l >= tl.cnt) continue;
+                pnew[tl.s0 + l] = pvk[kk];
+                q[tl.s0 + l] = qvk[kk];
+                acc += (double)pvk[kk] * (double)qvk[kk];
+            }
+        }
+        acc = mg_warp_sum(acc);
+        if ((threadIdx.x & 31) == 0) part[(size_t)t * MG_NW + (threadIdx.x >> 5)] = acc;
+        __syncthreads();  // stage buffer b is free for the tile after next
+    }
+}
+
 // per-warp partials of r.z, r.r, sum(z), sum(r) (one CTA per work tile)
 template <typename T>
 __global__ void __launch_bounds__(MG_TPB) k_pcg_dot4(pict_domain_t dom, const T* r, const T* z, double* part) {
@@ -818,7 +992,7 @@ __global__ void __launch_bounds__(MG_TPB) k_pcg_update(pict_domain_t dom, const 
 }
 
 __global__ void k_pcg_report(pict_domain_t dom, const double* sc, pict_solve_info_t* info, int iterations, double tol,
-                             int normalized) {
+                             int normalized, const int* err) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= dom.num_sims) return;
     const int n = dom.sim_cells[s + 1] - dom.sim_cells[s];
@@ -830,6 +1004,10 @@ __global__ void k_pcg_report(pict_domain_t dom, const double* sc, pict_solve_inf
     inf.finite = isfinite(crit) ? 1 : 0;
     inf.converged = (inf.finite && crit < tol) ? 1 : 0;
     inf.status = 0;
+    if (*err) {  // a stage wait gave up: report like a barrier timeout
+        inf.status = 1;
+        inf.converged = 0;
+    }
     info[s] = inf;
 }
 
@@ -844,6 +1022,7 @@ struct MgWork {
     char* q;
     double* part;
     double* sc;
+    int* err;
 };
 
 static size_t mg_carve(const pict_domain_t* dom, const pict_mg_level_t* levels, int nl, size_t esz, char* ws,
@@ -868,6 +1047,7 @@ static size_t mg_carve(const pict_domain_t* dom, const pict_mg_level_t* levels, 
     w->q = take(vb(N));
     w->part = reinterpret_cast<double*>(take(((size_t)4 * MG_NW * dom->num_tiles * 8 + 255) & ~(size_t)255));
     w->sc = reinterpret_cast<double*>(take(((size_t)MG_SC * dom->num_sims * 8 + 255) & ~(size_t)255));
+    w->err = reinterpret_cast<int*>(take(256));
     return o;
 }
 
@@ -893,6 +1073,7 @@ static pict_status_t run_pcg_mg(const pict_domain_t* dom, const pict_mg_level_t*
     T* q = reinterpret_cast<T*>(W.q);
     double* part = W.part;
     double* sc = W.sc;
+    int* err = W.err;
 
     const T wj = (T)omega, sp = (T)scale;
     const int nt = dom->num_tiles;
@@ -966,6 +1147,29 @@ static pict_status_t run_pcg_mg(const pict_domain_t* dom, const pict_mg_level_t*
         return check_launch("pcg_mg vcycle");
     };
 
+    // bulk-staged SpMV (2D): stage buffers sized by the domain's tile size and longest block row; every
+    // operand's base must be 16-byte aligned (bulk copies start on 16-byte boundaries)
+    auto al16 = [](const void* ptr) { return ((uintptr_t)ptr & 15) == 0; };
+    const int cap_h = ((dom->tile_cells + 2 * levels[0].max_block_sx + 8 + 7) / 8) * 8;
+    const int cap_t = ((dom->tile_cells + 8 + 7) / 8) * 8;
+    const size_t bulk_smem = 2 * (size_t)(2 * cap_h + (2 * D + 1) * cap_t) * sizeof(T);
+    int bulk_grid = 0;
+    if (D == 2 && g_mg_bulk && levels[0].max_block_sx > 0 && bulk_smem <= 200 * 1024 && al16(levels[0].coef) &&
+        al16(z) && al16(pbuf[0]) && al16(pbuf[1])) {
+        cudaError_t e = cudaFuncSetAttribute(k_pcg_spmv_dot_bulk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)bulk_smem);
+        int per_sm = 0;
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_spmv_dot_bulk<T>, MG_TPB, bulk_smem);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            per_sm = 0;
+        }
+        bulk_grid = per_sm * device_sm_count();
+        if (bulk_grid > nt) bulk_grid = nt;
+        if ((long long)bulk_grid * MG_BULK_MAX_TILES < nt) bulk_grid = 0;  // descriptors would not fit
+    }
+    if (cudaMemsetAsync(err, 0, sizeof(int), st) != cudaSuccess) return check_launch("pcg_mg error word");
     if (iterations == 0) cudaMemsetAsync(xout, 0, sizeof(T) * N, st);
     pict_status_t s = vcycle(rhs, false, nullptr, nullptr, 0);
     if (s) return s;
@@ -975,7 +1179,11 @@ static pict_status_t run_pcg_mg(const pict_domain_t* dom, const pict_mg_level_t*
         T* pnew = pbuf[it & 1];
         const T* pold = it ? pbuf[(it + 1) & 1] : z;
         T* rn = rbuf[it & 1];
-        k_pcg_spmv_dot<T, D><<<nt, MG_TPB, 0, st>>>(*dom, levels[0], z, pold, pnew, q, sc, it == 0, part);
+        if (bulk_grid > 0)
+            k_pcg_spmv_dot_bulk<T><<<bulk_grid, MG_TPB, bulk_smem, st>>>(*dom, levels[0], z, pold, pnew, q, sc, it == 0,
+                                                                         part, cap_h, cap_t, err);
+        else
+            k_pcg_spmv_dot<T, D><<<nt, MG_TPB, 0, st>>>(*dom, levels[0], z, pold, pnew, q, sc, it == 0, part);
         k_pcg_scalars<1><<<swg, 128, 0, st>>>(*dom, part, 1, sc);
         if (it + 1 < iterations) {
             s = vcycle(r, true, rn, pnew, it == 0);
@@ -987,7 +1195,7 @@ static pict_status_t run_pcg_mg(const pict_domain_t* dom, const pict_mg_level_t*
         k_pcg_scalars<4><<<swg, 128, 0, st>>>(*dom, part, 2, sc);
         r = rn;
     }
-    k_pcg_report<<<sg, 128, 0, st>>>(*dom, sc, info, iterations, tol, normalized);
+    k_pcg_report<<<sg, 128, 0, st>>>(*dom, sc, info, iterations, tol, normalized, err);
     return check_launch("pcg_mg");
 }
 
@@ -996,6 +1204,8 @@ static pict_status_t run_pcg_mg(const pict_domain_t* dom, const pict_mg_level_t*
 using namespace pict;
 
 extern "C" {
+
+void pict_mg_set_bulk_staging(int32_t enable) { g_mg_bulk = enable ? 1 : 0; }
 
 pict_status_t pict_mg_galerkin(const pict_mg_level_t* fine, const pict_mg_level_t* coarse, void* stream) {
     if (!fine || !coarse || !fine->coef || !coarse->coef || !fine->blocks || !coarse->blocks || !coarse->cell_block)

@@ -117,6 +117,7 @@ class MGHierarchy:
             L.cell_block = cb.data_ptr()
             L.coef = coef.data_ptr() if coef is not None else None
             L.max_block_cells = int(n.max())
+            L.max_block_sx = int(sizes[:, 0].max())
             tiles_t = None
             if lvl > 0:
                 tiles_t = torch.tensor(level_tiles(offs, n, sims), dtype=torch.int32, device=device)
