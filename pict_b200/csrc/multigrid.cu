@@ -38,7 +38,12 @@ struct MgBlock {
 };
 
 constexpr int MG_BT = 12;  // ints per block-table entry
-constexpr int MG_SC = 6;   // per-system PCG scalars: rho, alpha, beta, |r|^2, mean(z), unused
+constexpr int MG_SC = 6;   // per-system PCG scalars: rho, alpha, beta, |r|^2, mean(z), done
+
+// A system is done once its residual met the tolerance: sc[5] = iterations at that point + 1 (0 while
+// iterating).  The kernels of later iterations skip the tiles / blocks of done systems, so their iterate
+// and report stay those of the converged iteration.
+__device__ __forceinline__ bool mg_done(const double* sc, int sys) { return sc && sc[MG_SC * sys + 5] != 0.0; }
 
 __device__ __forceinline__ MgBlock mg_block(const pict_mg_level_t& L, int b) {
     const int* t = L.blocks + MG_BT * b;
@@ -217,9 +222,11 @@ __global__ void __launch_bounds__(MG_TPB, 4) k_mg_restrict(pict_mg_level_t F, pi
                                                            const T* __restrict__ r, const T* __restrict__ q,
                                                            T* __restrict__ rn, T* __restrict__ x,
                                                            const T* __restrict__ p, const double* __restrict__ sc,
-                                                           int first, T* __restrict__ bc, T w, int cap) {
+                                                           int first, T* __restrict__ bc, T w, int cap,
+                                                           const double* __restrict__ dn) {
     extern __shared__ __align__(16) unsigned char mg_stage_raw[];
     const MgTile tl = mg_tile(C.tiles, blockIdx.x);
+    if (mg_done(dn, tl.sys)) return;
     const MgBlock Bc = mg_block(C, tl.blk), Bf = mg_block(F, tl.blk);
     const T* __restrict__ cf = reinterpret_cast<const T*>(F.coef);
     const int Nf = F.num_cells;
@@ -360,9 +367,10 @@ template <typename T, int D, bool DOT>
 __global__ void __launch_bounds__(MG_TPB, 4) k_mg_prolong(pict_mg_level_t F, pict_mg_level_t C, const int32_t* tiles,
                                                           const T* __restrict__ bv, const T* __restrict__ ec,
                                                           T* __restrict__ out, T s, T w, double* __restrict__ part,
-                                                          int cap) {
+                                                          int cap, const double* __restrict__ dn) {
     extern __shared__ __align__(16) unsigned char mg_stage_raw[];
     const MgTile tl = mg_tile(tiles, blockIdx.x);
+    if (mg_done(dn, tl.sys)) return;
     const MgBlock Bf = mg_block(F, tl.blk), Bc = mg_block(C, tl.blk);
     const T* __restrict__ cf = reinterpret_cast<const T*>(F.coef);
     const int N = F.num_cells;
@@ -512,7 +520,8 @@ static size_t mg_sub_smem(const pict_mg_level_t* lv, int n, size_t esz) {
 
 template <typename T, int D>
 __global__ void __launch_bounds__(MG_SUB_THREADS) k_mg_subcycle(MgSub S, const T* __restrict__ bin,
-                                                                T* __restrict__ xout, T w, T sp, int sweeps) {
+                                                                T* __restrict__ xout, T w, T sp, int sweeps,
+                                                                const double* __restrict__ dn) {
     constexpr int K = 2 * D + 1;
     extern __shared__ __align__(16) unsigned char mg_sub_raw[];
     T* sm = reinterpret_cast<T*>(mg_sub_raw);
@@ -520,6 +529,7 @@ __global__ void __launch_bounds__(MG_SUB_THREADS) k_mg_subcycle(MgSub S, const T
     __shared__ double s_red[32];
     __shared__ double s_mean;
     const int b = blockIdx.x;
+    if (mg_done(dn, mg_block(S.lv[0], b).sys)) return;
     if (threadIdx.x == 0) {
         int o = 0;
         for (int k = 0; k < S.n; ++k) {
@@ -672,6 +682,7 @@ __global__ void __launch_bounds__(MG_TPB) k_pcg_spmv_dot(pict_domain_t dom, pict
     const T* __restrict__ coef = reinterpret_cast<const T*>(L.coef);
     const int N = L.num_cells;
     const MgTile tl = mg_tile(dom.tiles, blockIdx.x);
+    if (mg_done(sc, tl.sys)) return;
     const MgBlock B = mg_block(L, tl.blk);
     const T m = (T)sc[MG_SC * tl.sys + 4];
     const T bt = first ? T(0) : (T)sc[MG_SC * tl.sys + 2];
@@ -735,6 +746,8 @@ __global__ void __launch_bounds__(MG_TPB) k_pcg_spmv_dot_bulk(pict_domain_t dom,
     __shared__ __align__(8) uint64_t bar[2];
     __shared__ MgTile s_tl[MG_BULK_MAX_TILES];
     __shared__ MgBlock s_bk[MG_BULK_MAX_TILES];
+    __shared__ int s_tix[MG_BULK_MAX_TILES];  // tile index of each live (not yet converged) tile
+    __shared__ int s_nlive;
     const T* __restrict__ coef = reinterpret_cast<const T*>(L.coef);
     const int N = L.num_cells;
     const int nt = dom.num_tiles;
@@ -743,10 +756,19 @@ __global__ void __launch_bounds__(MG_TPB) k_pcg_spmv_dot_bulk(pict_domain_t dom,
     const T* const pv_src = first ? z : pold;  // the first direction starts from p_old = z (beta = 0)
     // this CTA's tiles blockIdx.x + j gridDim.x and their blocks, loaded once (the host guarantees at most
     // MG_BULK_MAX_TILES per CTA)
-    const int my_tiles = (int)blockIdx.x < nt ? (nt - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
-    for (int j = threadIdx.x; j < my_tiles; j += blockDim.x) {
-        s_tl[j] = mg_tile(dom.tiles, blockIdx.x + j * gridDim.x);
-        s_bk[j] = mg_block(L, s_tl[j].blk);
+    const int all_tiles = (int)blockIdx.x < nt ? (nt - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    if (threadIdx.x == 0) {  // the live tiles, in order (tiles of converged systems are skipped)
+        int n = 0;
+        for (int j = 0; j < all_tiles; ++j) {
+            const int t = blockIdx.x + j * gridDim.x;
+            const MgTile tl = mg_tile(dom.tiles, t);
+            if (mg_done(sc, tl.sys)) continue;
+            s_tl[n] = tl;
+            s_bk[n] = mg_block(L, tl.blk);
+            s_tix[n] = t;
+            ++n;
+        }
+        s_nlive = n;
     }
 
     struct Runs {
@@ -783,13 +805,14 @@ __global__ void __launch_bounds__(MG_TPB) k_pcg_spmv_dot_bulk(pict_domain_t dom,
         mbar_fence_init();
     }
     __syncthreads();
+    const int my_tiles = s_nlive;
     if (threadIdx.x == 0 && my_tiles > 0) issue(0, 0);
     for (int k = 0; k < my_tiles; ++k) {
         const int b = k & 1;
         if (threadIdx.x == 0 && k + 1 < my_tiles) issue(k + 1, b ^ 1);
         const MgTile tl = s_tl[k];
         const MgBlock B = s_bk[k];
-        const int t = blockIdx.x + k * gridDim.x;
+        const int t = s_tix[k];
         const Runs R = runs_of(tl, B);
         T* const buf = stage + (size_t)b * per_buf;
         T* const zs = buf;
@@ -884,8 +907,10 @@ __global__ void __launch_bounds__(MG_TPB) k_pcg_spmv_dot_bulk(pict_domain_t dom,
 
 // per-warp partials of r.z, r.r, sum(z), sum(r) (one CTA per work tile)
 template <typename T>
-__global__ void __launch_bounds__(MG_TPB) k_pcg_dot4(pict_domain_t dom, const T* r, const T* z, double* part) {
+__global__ void __launch_bounds__(MG_TPB) k_pcg_dot4(pict_domain_t dom, const T* r, const T* z, double* part,
+                                                     const double* __restrict__ dn) {
     const MgTile tl = mg_tile(dom.tiles, blockIdx.x);
+    if (mg_done(dn, tl.sys)) return;
     double a = 0.0, c = 0.0, sz = 0.0, sr = 0.0;
     for (int i = tl.s0 + threadIdx.x; i < tl.s0 + tl.cnt; i += MG_TPB) {
         const double ri = (double)r[i], zi = (double)z[i];
@@ -914,10 +939,12 @@ __global__ void __launch_bounds__(MG_TPB) k_pcg_dot4(pict_domain_t dom, const T*
 // The preconditioned residual z is used mean-free (z - m): the constant mode of a singular system is
 // undetermined.  sc[s*MG_SC + {0: rho, 1: alpha, 2: beta, 3: |r|^2, 4: m}]
 template <int STRIDE>
-__global__ void k_pcg_scalars(pict_domain_t dom, const double* __restrict__ part, int stage, double* sc) {
+__global__ void k_pcg_scalars(pict_domain_t dom, const double* __restrict__ part, int stage, double* sc, int it,
+                              double tol, int normalized) {
     const int lane = threadIdx.x & 31;
     const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (s >= dom.num_sims) return;
+    if (stage != 0 && sc[MG_SC * s + 5] != 0.0) return;  // converged earlier: keep its scalars
     double v[4] = {0.0, 0.0, 0.0, 0.0}, u[STRIDE];
 #pragma unroll
     for (int k = 0; k < STRIDE; ++k) u[k] = 0.0;
@@ -959,6 +986,9 @@ __global__ void k_pcg_scalars(pict_domain_t dom, const double* __restrict__ part
     S[0] = rho;
     S[3] = v[1];
     S[4] = m;
+    // converged: iterations done so far (0 after the initial cycle, it + 1 after iteration it) plus one
+    const double crit = normalized ? sqrt(v[1]) / sqrt((double)n) : sqrt(v[1]);
+    S[5] = (crit < tol) ? (stage == 0 ? 1.0 : (double)(it + 2)) : 0.0;
 }
 
 // rn = r - alpha q, x += alpha p (x = alpha p when first), and the per-warp partials of
@@ -970,6 +1000,7 @@ __global__ void __launch_bounds__(MG_TPB) k_pcg_update(pict_domain_t dom, const 
                                                        const T* __restrict__ p, const double* __restrict__ sc, int first,
                                                        double* __restrict__ part) {
     const MgTile tl = mg_tile(dom.tiles, blockIdx.x);
+    if (mg_done(sc, tl.sys)) return;
     const T al = (T)sc[MG_SC * tl.sys + 1];
     double c2 = 0.0, sr = 0.0;
     for (int l = threadIdx.x; l < tl.cnt; l += MG_TPB) {
@@ -1000,7 +1031,7 @@ __global__ void k_pcg_report(pict_domain_t dom, const double* sc, pict_solve_inf
     const double crit = normalized ? nrm / sqrt((double)n) : nrm;
     pict_solve_info_t inf;
     inf.final_residual = crit;
-    inf.used_iterations = iterations;
+    inf.used_iterations = sc[MG_SC * s + 5] != 0.0 ? (int)sc[MG_SC * s + 5] - 1 : iterations;
     inf.finite = isfinite(crit) ? 1 : 0;
     inf.converged = (inf.finite && crit < tol) ? 1 : 0;
     inf.status = 0;
@@ -1122,8 +1153,8 @@ static pict_status_t run_pcg_mg(const pict_domain_t* dom, const pict_mg_level_t*
         if (lc == 0) {
             if (upd) k_pcg_update<T><<<nt, MG_TPB, 0, st>>>(*dom, r, q, rn, xout, p, sc, first, part);
             k_mg_subcycle<T, D><<<levels[0].num_blocks, MG_SUB_THREADS, sub_smem, st>>>(sub, rnew, z, wj, sp,
-                                                                                     coarse_sweeps);
-            k_pcg_dot4<T><<<nt, MG_TPB, 0, st>>>(*dom, rnew, z, part);
+                                                                                     coarse_sweeps, sc);
+            k_pcg_dot4<T><<<nt, MG_TPB, 0, st>>>(*dom, rnew, z, part, sc);
             return check_launch("pcg_mg vcycle");
         }
         for (int l = 0; l < lc; ++l) {
@@ -1131,19 +1162,19 @@ static pict_status_t run_pcg_mg(const pict_domain_t* dom, const pict_mg_level_t*
             const pict_mg_level_t& C = levels[l + 1];
             if (l == 0 && upd)
                 k_mg_restrict<T, D, true><<<C.num_tiles, MG_TPB, stage3, st>>>(F, C, r, q, rn, xout, p, sc, first,
-                                                                                lb[1], wj, cap);
+                                                                                lb[1], wj, cap, sc);
             else
                 k_mg_restrict<T, D, false><<<C.num_tiles, MG_TPB, stage3, st>>>(
-                    F, C, l == 0 ? r : lb[l], nullptr, nullptr, nullptr, nullptr, nullptr, 0, lb[l + 1], wj, cap);
+                    F, C, l == 0 ? r : lb[l], nullptr, nullptr, nullptr, nullptr, nullptr, 0, lb[l + 1], wj, cap, sc);
         }
         // levels lc.. in one launch (one CTA per block)
         k_mg_subcycle<T, D><<<levels[lc].num_blocks, MG_SUB_THREADS, sub_smem, st>>>(sub, lb[lc], lx[lc], wj, sp,
-                                                                                  coarse_sweeps);
+                                                                                  coarse_sweeps, sc);
         for (int l = lc - 1; l >= 1; --l)
             k_mg_prolong<T, D, false><<<levels[l].num_tiles, MG_TPB, stage3, st>>>(
-                levels[l], levels[l + 1], levels[l].tiles, lb[l], lx[l + 1], lx[l], sp, wj, nullptr, cap);
+                levels[l], levels[l + 1], levels[l].tiles, lb[l], lx[l + 1], lx[l], sp, wj, nullptr, cap, sc);
         k_mg_prolong<T, D, true><<<nt, MG_TPB, stage3, st>>>(levels[0], levels[1], dom->tiles, rnew, lx[1], z, sp, wj,
-                                                             part, cap);
+                                                             part, cap, sc);
         return check_launch("pcg_mg vcycle");
     };
 
@@ -1169,11 +1200,13 @@ static pict_status_t run_pcg_mg(const pict_domain_t* dom, const pict_mg_level_t*
         if (bulk_grid > nt) bulk_grid = nt;
         if ((long long)bulk_grid * MG_BULK_MAX_TILES < nt) bulk_grid = 0;  // descriptors would not fit
     }
-    if (cudaMemsetAsync(err, 0, sizeof(int), st) != cudaSuccess) return check_launch("pcg_mg error word");
-    if (iterations == 0) cudaMemsetAsync(xout, 0, sizeof(T) * N, st);
+    // x from zero (a system that is done before its first update keeps x = 0); no system is done yet
+    if (cudaMemsetAsync(err, 0, sizeof(int), st) != cudaSuccess || cudaMemsetAsync(xout, 0, sizeof(T) * N, st) != cudaSuccess ||
+        cudaMemsetAsync(sc, 0, sizeof(double) * MG_SC * dom->num_sims, st) != cudaSuccess)
+        return check_launch("pcg_mg initial state");
     pict_status_t s = vcycle(rhs, false, nullptr, nullptr, 0);
     if (s) return s;
-    k_pcg_scalars<4><<<swg, 128, 0, st>>>(*dom, part, 0, sc);
+    k_pcg_scalars<4><<<swg, 128, 0, st>>>(*dom, part, 0, sc, 0, tol, normalized);
     const T* r = rhs;
     for (int it = 0; it < iterations; ++it) {
         T* pnew = pbuf[it & 1];
@@ -1184,7 +1217,7 @@ static pict_status_t run_pcg_mg(const pict_domain_t* dom, const pict_mg_level_t*
                                                                          part, cap_h, cap_t, err);
         else
             k_pcg_spmv_dot<T, D><<<nt, MG_TPB, 0, st>>>(*dom, levels[0], z, pold, pnew, q, sc, it == 0, part);
-        k_pcg_scalars<1><<<swg, 128, 0, st>>>(*dom, part, 1, sc);
+        k_pcg_scalars<1><<<swg, 128, 0, st>>>(*dom, part, 1, sc, it, tol, normalized);
         if (it + 1 < iterations) {
             s = vcycle(r, true, rn, pnew, it == 0);
             if (s) return s;
@@ -1192,7 +1225,7 @@ static pict_status_t run_pcg_mg(const pict_domain_t* dom, const pict_mg_level_t*
             // last iteration: only the update and |r|^2 (r.z and sum(z) are not used)
             k_pcg_update<T><<<nt, MG_TPB, 0, st>>>(*dom, r, q, rn, xout, pnew, sc, it == 0, part);
         }
-        k_pcg_scalars<4><<<swg, 128, 0, st>>>(*dom, part, 2, sc);
+        k_pcg_scalars<4><<<swg, 128, 0, st>>>(*dom, part, 2, sc, it, tol, normalized);
         r = rn;
     }
     k_pcg_report<<<sg, 128, 0, st>>>(*dom, sc, info, iterations, tol, normalized, err);
