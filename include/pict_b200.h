@@ -244,6 +244,13 @@ pict_status_t pict_solve(const pict_domain_t* dom, const void* coef, const void*
                          const pict_solve_params_t* params, void* info_out, void* workspace,
                          int64_t workspace_bytes, void* stream);
 
+/* Process-wide choice of the launch form of the single-reduction CG (variant 1; no counterpart in the
+ * reference): 1 (default) solves each system with one thread-block cluster (16 CTAs, else 8) when a
+ * domain holds few systems (at most 8) of at most 262,144 cells, reducing the inner products through
+ * distributed shared memory with one cluster barrier per iteration and no grid-wide barrier; 0 always
+ * uses the persistent grid; 2 uses clusters whenever they fit. */
+void pict_krylov_set_cluster_mode(int32_t mode);
+
 /* pict_solve without a caller-provided workspace (no counterpart in the reference).  For callers
  * that hold no device allocator (a plain C or ctypes binding without torch, or a loop that must not
  * call cudaMalloc, which synchronises the device).  The workspace is a fixed scratch array of

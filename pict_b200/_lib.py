@@ -189,6 +189,7 @@ SIGNATURES = {
     "pict_refine_update": (c_i32, [_PD, c_vp, c_vp, c_vp]),
     "pict_refine_finish": (c_i32, [_PD, c_vp, c_vp, c_i32, c_i32, c_vp, c_vp]),
     "pict_mg_set_bulk_staging": (None, [c_i32]),
+    "pict_krylov_set_cluster_mode": (None, [c_i32]),
     "pict_mg_galerkin": (c_i32, [ctypes.POINTER(MgLevel), ctypes.POINTER(MgLevel), c_vp]),
     "pict_pcg_mg_workspace_bytes": (ctypes.c_int64, [_PD, ctypes.POINTER(MgLevel), c_i32]),
     "pict_pcg_mg": (c_i32, [_PD, ctypes.POINTER(MgLevel), c_i32, c_vp, c_vp, c_i32, ctypes.c_double, c_i32, c_vp, c_vp,

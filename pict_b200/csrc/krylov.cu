@@ -33,8 +33,11 @@
 #include <cmath>
 #include <cstdio>
 #include <mutex>
+#include <cooperative_groups.h>
 #include "common.cuh"
 #include "launch.h"
+
+namespace cgrp = cooperative_groups;
 
 #ifndef PICT_SPIN_LIMIT
 #define PICT_SPIN_LIMIT (1ll << 26)
@@ -55,7 +58,7 @@ constexpr int KR_PASS = KR_U * KR_THREADS;
 // BiCGStab: increments and reads are always separated by a grid barrier).  The single-reduction CG
 // has one barrier per iteration, so completions of iteration i go to CTRL_DONE_PAR + (i & 1) and are
 // read only after the barrier of iteration i+1.
-enum { CTRL_ERR = 0, CTRL_DONE = 1, CTRL_BAR_COUNT = 2, CTRL_DONE_PAR = 4 };
+enum { CTRL_ERR = 0, CTRL_DONE = 1, CTRL_BAR_COUNT = 2, CTRL_DONE_PAR = 4, CTRL_SCHED = 8 };
 
 template <typename T>
 struct KArgs {
@@ -1233,6 +1236,227 @@ __global__ void __launch_bounds__(KR_THREADS, 2) k_bicgstab(KArgs<T> a) {
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Cluster CG: the single-reduction recurrence of k_cg1, one thread-block cluster per system.
+//
+// The cluster's first CTA takes the next system from a counter in the workspace (systems are ordered
+// largest first) and hands it to every CTA of the cluster through distributed shared memory; the CTAs
+// sweep that system's tiles round robin (rank, rank + CL, ...) and reduce the iteration's inner
+// products through distributed shared memory: every CTA writes its partials into the first CTA's shared
+// memory, one cluster barrier (hardware, release / acquire at cluster scope, which also orders the
+// vectors written to global memory by the other CTAs of the cluster), then every CTA sums the partials
+// in rank order, so all CTAs take the same decisions from the same numbers.  No grid-wide barrier:
+// systems advance independently and a cluster that finishes one takes the next.
+// ---------------------------------------------------------------------------------------------
+constexpr int KC_MAX_CL = 16;
+constexpr int KC_NV = 4;  // values per CTA partial (one layout for every reduction: the two buffers never overlap)
+
+struct ClusterRed {
+    double part[2][KC_MAX_CL][KC_NV];
+};
+
+// sum of NV <= KC_NV values over the cluster (block sum, then partials through distributed shared memory,
+// alternating between two buffers: a CTA writes buffer e & 1 only after every CTA passed the barrier of
+// reduction e - 1, i.e. finished reading buffer (e - 2) & 1)
+template <int NV>
+__device__ __forceinline__ void cluster_sum(cgrp::cluster_group& cl, ClusterRed& red, int& epoch,
+                                            double (&v)[NV]) {
+    static_assert(NV <= KC_NV, "cluster_sum: too many values");
+    __shared__ double s_tot[NV];
+    block_sum<NV>(v);
+    const int par = epoch & 1;
+    ++epoch;
+    if (threadIdx.x == 0) {
+        ClusterRed* r0 = cl.map_shared_rank(&red, 0);
+#pragma unroll
+        for (int k = 0; k < NV; ++k) r0->part[par][cl.block_rank()][k] = v[k];
+    }
+    cl.sync();
+    if (threadIdx.x < 32) {  // half-warp h sums value k = h, h + 2, ...: lane r loads rank r's partial, then a
+        // fixed butterfly over the 16 lanes (one remote load per lane, all in flight together)
+        const ClusterRed* r0 = cl.map_shared_rank(&red, 0);
+        const unsigned r = threadIdx.x & 15, h = threadIdx.x >> 4;
+#pragma unroll
+        for (int k0 = 0; k0 < NV; k0 += 2) {
+            const int k = k0 + (int)h;
+            double t = (r < cl.num_blocks() && k < NV) ? r0->part[par][r][k < NV ? k : 0] : 0.0;
+#pragma unroll
+            for (int o = 8; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+            if (r == 0 && k < NV) s_tot[k] = t;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; ++k) v[k] = s_tot[k];
+    __syncthreads();
+}
+
+template <typename T, int D, bool TRANS>
+__global__ void __launch_bounds__(KR_THREADS, 2) k_cg1_cluster(KArgs<T> a) {
+    cgrp::cluster_group cl = cgrp::this_cluster();
+    const int CL = (int)cl.num_blocks();
+    const int rank = (int)cl.block_rank();
+    const pict_domain_t& dom = a.dom;
+    const int N = dom.num_cells;
+    __shared__ ClusterRed red;
+    __shared__ int s_sys;
+    int epoch = 0;
+    const T* __restrict__ coef = a.coef;
+    const T* __restrict__ bv = a.b;
+    T* __restrict__ x = a.x;
+    T* __restrict__ p = a.t;
+    cl.sync();  // every CTA of the cluster runs before any distributed shared memory access
+
+    for (;;) {
+        if (rank == 0 && threadIdx.x == 0) {
+            const int sys = atomicAdd(a.ctrl + CTRL_SCHED, 1);
+            for (int r = 0; r < CL; ++r) *cl.map_shared_rank(&s_sys, r) = sys;
+        }
+        cl.sync();
+        const int sys = s_sys;
+        if (sys >= dom.num_sims) break;
+        const int t0 = dom.sim_tiles[sys], t1 = dom.sim_tiles[sys + 1];
+        const int n = dom.sim_cells[sys + 1] - dom.sim_cells[sys];
+        T* rc = a.r;   // r_i
+        T* rn = a.rw;  // r_{i+1}
+        T* wc = a.p0;
+        T* wn = a.p1;
+        T* sc = a.v0;
+        T* sn = a.v1;
+        // the tiles of this CTA: t0 + rank, t0 + rank + CL, ...
+#define KC_TILES(t, blk, s0, cnt)                                                                   \
+    for (int t = t0 + rank; t < t1; t += CL)                                                        \
+        for (int blk = dom.tiles[4 * t + 1], s0 = dom.tiles[4 * t + 2], cnt = dom.tiles[4 * t + 3]; \
+             cnt > 0; cnt = 0)
+
+        // ---- init: r0 = b - A x0 (when x0 != 0), w0 = A r0, g0, d0, |b|^2
+        if (!a.x_zero) {
+            KC_TILES(t, blk, s0, cnt) {
+                const pict_block_t& B = dom.blocks[blk];
+                for (int i = s0 + threadIdx.x; i < s0 + cnt; i += blockDim.x) {
+                    int q[3];
+                    unflatten(i - B.offset, B.size, q);
+                    rc[i] = bv[i] - spmv_row<T, D, TRANS>(dom, coef, N, i, B, q, [&](int jj) { return x[jj]; });
+                }
+            }
+            cl.sync();
+        }
+        const T* r0 = a.x_zero ? bv : rc;
+        double acc3[3] = {0.0, 0.0, 0.0};
+        KC_TILES(t, blk, s0, cnt) {
+            const pict_block_t& B = dom.blocks[blk];
+            for (int i = s0 + threadIdx.x; i < s0 + cnt; i += blockDim.x) {
+                int q[3];
+                unflatten(i - B.offset, B.size, q);
+                const T ri = r0[i];
+                const T wi = spmv_row<T, D, TRANS>(dom, coef, N, i, B, q, [&](int jj) { return r0[jj]; });
+                wc[i] = wi;
+                sc[i] = T(0);
+                p[i] = T(0);
+                const T bi = bv[i];
+                acc3[0] += (double)ri * (double)ri;
+                acc3[1] += (double)wi * (double)ri;
+                acc3[2] += (double)bi * (double)bi;
+            }
+        }
+        cluster_sum<3>(cl, red, epoch, acc3);
+        if (a.x_zero) {
+            KC_TILES(t, blk, s0, cnt) {
+                for (int i = s0 + threadIdx.x; i < s0 + cnt; i += blockDim.x) {
+                    rc[i] = bv[i];
+                    x[i] = T(0);
+                }
+            }
+        }
+        pict_solve_info_t inf = fresh_info();
+        double g = acc3[0], alpha = acc3[0] / acc3[1], beta = 0.0;
+        bool active = true;
+        if (acc3[2] == 0.0) {
+            inf.converged = 1;
+            inf.used_iterations = 0;
+            active = false;
+            KC_TILES(t, blk, s0, cnt) {
+                for (int i = s0 + threadIdx.x; i < s0 + cnt; i += blockDim.x) x[i] = T(0);
+            }
+        }
+        if (active) cl.sync();  // rc / x of the x_zero start visible before the first sweep reads neighbours
+        for (int it = 0; active && it < a.maxit; ++it) {
+            const T al = (T)alpha, bt = (T)beta;
+            double acc[2] = {0.0, 0.0};
+            KC_TILES(t, blk, s0, cnt) {
+                const pict_block_t& B = dom.blocks[blk];
+                for (int base = 0; base < cnt; base += KR_PASS) {
+                    T rni[KR_U], wni[KR_U], pi[KR_U], si[KR_U], xi[KR_U];
+#pragma unroll
+                    for (int k = 0; k < KR_U; ++k) {
+                        const int i = s0 + min(base + (int)threadIdx.x + k * KR_THREADS, cnt - 1);
+                        int q[3];
+                        unflatten(i - B.offset, B.size, q);
+                        pi[k] = rc[i] + bt * p[i];
+                        si[k] = wc[i] + bt * sc[i];
+                        rni[k] = rc[i] - al * si[k];
+                        xi[k] = x[i] + al * pi[k];
+                        wni[k] = spmv_row<T, D, TRANS>(dom, coef, N, i, B, q,
+                                                       [&](int jj) { return rc[jj] - al * (wc[jj] + bt * sc[jj]); });
+                    }
+#pragma unroll
+                    for (int k = 0; k < KR_U; ++k) {
+                        const int l = base + (int)threadIdx.x + k * KR_THREADS;
+                        if (l < cnt) {
+                            const int i = s0 + l;
+                            x[i] = xi[k];
+                            p[i] = pi[k];
+                            sn[i] = si[k];
+                            rn[i] = rni[k];
+                            wn[i] = wni[k];
+                            acc[0] += (double)rni[k] * (double)rni[k];
+                            acc[1] += (double)wni[k] * (double)rni[k];
+                        }
+                    }
+                }
+            }
+            cluster_sum<2>(cl, red, epoch, acc);
+            const double gn = acc[0], d = acc[1];
+            const double crit = conv_crit(gn, a.normalized, n);
+            inf.used_iterations = it;
+            inf.final_residual = crit;
+            if (!isfinite(crit)) { inf.finite = 0; active = false; }
+            else if (crit < a.tol) { inf.converged = 1; active = false; }
+            else {
+                const double bnew = gn / g;
+                alpha = gn / (d - bnew * gn / alpha);
+                beta = bnew;
+                g = gn;
+            }
+            T* t0p = rc; rc = rn; rn = t0p;
+            T* t1p = wc; wc = wn; wn = t1p;
+            T* t2p = sc; sc = sn; sn = t2p;
+        }
+        if (a.sub_mean || a.write_bp) {
+            double m[1] = {0.0};
+            if (a.sub_mean) {
+                KC_TILES(t, blk, s0, cnt) {
+                    for (int i = s0 + threadIdx.x; i < s0 + cnt; i += blockDim.x) m[0] += (double)x[i];
+                }
+                cluster_sum<1>(cl, red, epoch, m);
+            }
+            const T mean = a.sub_mean ? (T)(m[0] / (double)n) : T(0);
+            KC_TILES(t, blk, s0, cnt) {
+                const pict_block_t& B = dom.blocks[blk];
+                T* pb = reinterpret_cast<T*>(B.pressure);
+                for (int i = s0 + threadIdx.x; i < s0 + cnt; i += blockDim.x) {
+                    const T v = x[i] - mean;
+                    x[i] = v;
+                    if (a.write_bp) pb[i - B.offset] = v;
+                }
+            }
+        }
+#undef KC_TILES
+        if (rank == 0 && threadIdx.x == 0) a.info[sys] = inf;
+        cl.sync();  // every CTA is done with s_sys and the vectors of this system
+    }
+}
+
 __global__ void k_init_info(pict_solve_info_t* info, int n) {
     PICT_CELL_LOOP(i, n) {
         info[i].final_residual = 0.0;
@@ -1275,6 +1499,47 @@ static size_t workspace_total(const pict_domain_t* dom, const pict_solve_params_
     // bicg / cg1: 7 vectors; cg: r p0 p1 q (+ the best iterate)
     const int nvec = (prm->use_bicg || prm->variant == 1) ? 7 : (prm->return_best_result ? 5 : 4);
     return header_bytes(dom) + vec_bytes(dom, prm) * nvec;
+}
+
+// 0: persistent grid only; 1: clusters where they apply (default); 2: clusters whenever possible
+static int g_cluster_mode = 1;
+
+// Launch k_cg1_cluster with clusters of `cl` CTAs, as many clusters as fit on the device at once (at most
+// one per system).  Returns PICT_ERR_UNSUPPORTED (nothing launched) if no cluster of that size fits.
+template <typename T, int D, bool TRANS>
+static pict_status_t launch_cg1_cluster(KArgs<T>& a, int cl, cudaStream_t st) {
+    auto kern = k_cg1_cluster<T, D, TRANS>;
+    if (cl > 8 && cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+        cudaGetLastError();
+        return PICT_ERR_UNSUPPORTED;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.blockDim = dim3(KR_THREADS);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cl;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cfg.gridDim = dim3(cl);
+    int ncl = 0;
+    if (cudaOccupancyMaxActiveClusters(&ncl, kern, &cfg) != cudaSuccess || ncl < 1) {
+        cudaGetLastError();
+        return PICT_ERR_UNSUPPORTED;
+    }
+    if (ncl > a.dom.num_sims) ncl = a.dom.num_sims;
+    cfg.gridDim = dim3(ncl * cl);
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, kern, a);
+    if (e != cudaSuccess) {
+        char buf[256];
+        snprintf(buf, sizeof(buf), "cluster CG launch (%d clusters of %d): %s", ncl, cl, cudaGetErrorString(e));
+        cudaGetLastError();
+        return set_error(PICT_ERR_CUDA, buf);
+    }
+    return PICT_OK;
 }
 
 template <typename KernelT>
@@ -1361,6 +1626,22 @@ static pict_status_t run_solve(const pict_domain_t* dom, const void* coef, const
         } else if (prm->variant == 1 && a.reset == 0 && a.best == 0 && a.abs_crit == 0 && a.rankdef == 0) {
             a.r = vec[0]; a.rw = vec[1]; a.p0 = vec[2]; a.p1 = vec[3]; a.v0 = vec[4]; a.v1 = vec[5]; a.t = vec[6];
             kern = k_cg1<T, D, TRANS>;
+            // one thread-block cluster per system where systems are small enough for one cluster's SMs to
+            // stream: latency-bound small systems, or many systems that fill the device between them
+            // few systems: with many, the lockstep grid amortises one barrier per iteration over all of
+            // them while each cluster would pay its own per system
+            const bool few_small = dom->num_sims <= 8 && dom->max_sim_cells <= 262144;
+            if (g_cluster_mode == 2 || (g_cluster_mode == 1 && few_small)) {
+                s = launch_cg1_cluster<T, D, TRANS>(a, 16, st);
+                if (s == PICT_ERR_UNSUPPORTED) s = launch_cg1_cluster<T, D, TRANS>(a, 8, st);
+                if (s == PICT_OK) {
+                    k_finish_info<<<1, 128, 0, st>>>(info, ninfo, ctrl);
+                    s = check_launch("finish_info");
+                    if (s) return s;
+                    continue;
+                }
+                if (s != PICT_ERR_UNSUPPORTED) return s;
+            }
         } else {
             a.r = vec[0]; a.p0 = vec[1]; a.p1 = vec[2]; a.t = vec[3];
             a.rw = nullptr; a.v0 = nullptr; a.v1 = nullptr;
@@ -1421,6 +1702,8 @@ using namespace pict;
 extern "C" {
 
 int64_t pict_solve_static_scratch_bytes(void) { return (int64_t)KR_STATIC_SCRATCH_BYTES; }
+
+void pict_krylov_set_cluster_mode(int32_t mode) { g_cluster_mode = mode < 0 ? 0 : (mode > 2 ? 2 : mode); }
 
 pict_status_t pict_solve_static(const pict_domain_t* dom, const void* coef, const void* rhs, void* x,
                                 const pict_solve_params_t* prm, void* info_out, void* stream) {
