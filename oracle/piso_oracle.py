@@ -40,6 +40,7 @@ from typing import List, Optional
 
 import numpy as np
 import scipy.sparse as sp
+import scipy.sparse.linalg as spla
 
 FACE_NAMES = ["-x", "+x", "-y", "+y", "-z", "+z"]
 AXIS_NAMES = ["x", "y", "z"]
@@ -1544,6 +1545,92 @@ def bicgstab(A, b, x0=None, tol=1e-5, maxit=5000, dtype=np.float64, conv="NORM2_
         t = A @ s
         with np.errstate(divide="ignore", invalid="ignore"):
             omega = f64(np.dot(t, r)) / f64(np.dot(t, t))
+        x = x + omega * s
+        r = r - omega * t
+        nrmr = criterion(r, conv)
+        info.finalResidual = nrmr
+        if nrmr < tol:
+            info = SolveInfo(nrmr, i + 1, True, True)
+            break
+    return x, info
+
+
+def ilu0(val, index, row):
+    """Incomplete LU factorisation with zero fill (csrilu02, extensions/bicgstab_solver_kernel.cu:196-208):
+    the IKJ elimination restricted to the sparsity pattern of the CSR matrix (rows sorted by column).  Returns
+    the factor values on the same pattern: L strictly below the diagonal (unit diagonal implied), U on and
+    above it."""
+    f = np.array(val, dtype=np.float64 if np.asarray(val).dtype == np.float64 else np.asarray(val).dtype)
+    n = len(row) - 1
+    pos = [dict((int(index[k]), k) for k in range(row[i], row[i + 1])) for i in range(n)]
+    diag = [pos[i][i] for i in range(n)]
+    for i in range(n):
+        for k in range(row[i], row[i + 1]):
+            c = int(index[k])
+            if c >= i:
+                break
+            f[k] = f[k] / f[diag[c]]
+            for j in range(k + 1, row[i + 1]):
+                m = pos[c].get(int(index[j]))
+                if m is not None:
+                    f[j] -= f[k] * f[m]
+    return f
+
+
+def _ilu_apply(L, U, y, transpose):
+    """z = (L U)^-1 y, or (L U)^-T y: the two triangular solves of one preconditioner application
+    (extensions/bicgstab_solver_kernel.cu:270-276, 313-319)."""
+    if not transpose:
+        return spla.spsolve_triangular(U, spla.spsolve_triangular(L, y, lower=True, unit_diagonal=True), lower=False)
+    return spla.spsolve_triangular(L.T.tocsr(), spla.spsolve_triangular(U.T.tocsr(), y, lower=True), lower=False,
+                                   unit_diagonal=True)
+
+
+def bicgstab_ilu(val, index, row, b, tol=1e-5, maxit=5000, transpose=False, conv="NORM2_NORMALIZED"):
+    """bicgstabSolveGPU with the ILU(0) preconditioner (extensions/bicgstab_solver_kernel.cu:240-360): right
+    preconditioning, p^ = M^-1 p and s^ = M^-1 s with M = L U of ilu0(), from x = 0; `transpose` solves with
+    A^T and M^T.  Iteration bookkeeping as bicgstab()."""
+    val = np.asarray(val, dtype=np.float64)
+    n = len(row) - 1
+    A = sp.csr_matrix((val, np.asarray(index), np.asarray(row)), shape=(n, n))
+    f = ilu0(val, index, row)
+    F = sp.csr_matrix((f, np.asarray(index), np.asarray(row)), shape=(n, n))
+    L = sp.tril(F, -1, format="csr")
+    U = sp.triu(F, 0, format="csr")
+    if transpose:
+        A = A.T.tocsr()
+    b = np.asarray(b, dtype=np.float64)
+    x = np.zeros_like(b)
+    r = b.copy()
+    rw = r.copy()
+    p = r.copy()
+    v = np.zeros_like(b)
+    nrmr0 = criterion(r, conv)
+    if nrmr0 < tol:
+        return x, SolveInfo(nrmr0, -1, True, True)
+    rho = alpha = omega = 0.0
+    info = SolveInfo(0.0, -1, False, True)
+    for i in range(maxit):
+        rhop = rho
+        rho = float(np.dot(rw, r))
+        if i > 0:
+            beta = (rho / rhop) * (alpha / omega)
+            p = r + beta * (p - omega * v)
+        pw = _ilu_apply(L, U, p, transpose)
+        v = A @ pw
+        alpha = rho / float(np.dot(rw, v))
+        r = r - alpha * v
+        x = x + alpha * pw
+        nrmr = criterion(r, conv)
+        if not math.isfinite(nrmr):
+            return x, SolveInfo(nrmr, i, False, False)
+        info = SolveInfo(nrmr, i, False, True)
+        if nrmr < tol:
+            info.converged = True
+            break
+        s = _ilu_apply(L, U, r, transpose)
+        t = A @ s
+        omega = float(np.dot(t, r)) / float(np.dot(t, t))
         x = x + omega * s
         r = r - omega * t
         nrmr = criterion(r, conv)

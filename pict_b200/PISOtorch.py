@@ -2551,12 +2551,16 @@ def SolveLinear(A, RHS, x, maxIterations=1000, tolerance=1e-8, convergenceCriter
     tol = float(_as_scalar(tolerance))
     conv = int(convergenceCriterion)
     _check(0 <= conv <= 4, "Unknown convergence criterion.")
-    if useBiCG and BiCGwithPreconditioner:
-        _warn_once("ilu", "ILU preconditioning is not implemented in pict_b200; BiCGStab runs unpreconditioned")
     if domain.IsTensorChanged():
         raise RuntimeError("Domain's tensors have been changed, use UpdateDomain() to set the new pointers.")
     domain._desc = domain._make_desc()
     nb = RHS.size(0) // n
+    if useBiCG and BiCGwithPreconditioner:
+        infos = _solve_bicgstab_ilu(domain, A, RHS, x, nb, maxit, tol, conv, bool(transposeA))
+        if printResidual:
+            for i, inf in enumerate(infos):
+                print("BiCG (ILU) RHS %d: %s" % (i, inf))
+        return infos
     infos = []
     coef = A.coef.contiguous()
     if useBiCG:
@@ -2573,6 +2577,57 @@ def SolveLinear(A, RHS, x, maxIterations=1000, tolerance=1e-8, convergenceCriter
         for i, inf in enumerate(infos):
             print("%sCG RHS %d: %s" % ("Bi" if useBiCG else "", i, inf))
     return infos
+
+
+def _ilu_plan(domain):
+    """Host analysis of the domain's CSR pattern for the ILU(0) solves (pict_ilu_analyze), once per domain:
+    device arrays of the pattern, diagonal and transposed positions and level orders, host level starts."""
+    plan = getattr(domain, "_ilu", None)
+    row, index = domain._csr_structure()
+    if plan is not None and plan["row"] is row:
+        return plan
+    lib = _lib.load()
+    rh = row.cpu().numpy().astype(np.int32)
+    ih = index.cpu().numpy().astype(np.int32)
+    n, nnz = rh.size - 1, ih.size
+    diag = np.empty(n, np.int32)
+    tpos = np.empty(nnz, np.int32)
+    of, ob = np.empty(n, np.int32), np.empty(n, np.int32)
+    pf, pb = np.empty(n + 1, np.int32), np.empty(n + 1, np.int32)
+    nlf, nlb = ctypes.c_int32(0), ctypes.c_int32(0)
+    check(lib.pict_ilu_analyze(n, rh.ctypes.data, ih.ctypes.data, diag.ctypes.data, tpos.ctypes.data, of.ctypes.data,
+                               pf.ctypes.data, ob.ctypes.data, pb.ctypes.data, ctypes.byref(nlf), ctypes.byref(nlb)),
+          "ilu_analyze")
+    dev = domain.getDevice()
+    t = lambda a: torch.from_numpy(a).to(dev)
+    plan = {"row": row, "index": index, "index_out": torch.empty_like(index), "n": n, "nnz": nnz, "diag": t(diag),
+            "tpos": t(tpos), "order_f": t(of),
+            "order_b": t(ob), "ptr_f": pf[:nlf.value + 1].copy(), "ptr_b": pb[:nlb.value + 1].copy(),
+            "nlf": nlf.value, "nlb": nlb.value}
+    domain._ilu = plan
+    return plan
+
+
+def _solve_bicgstab_ilu(domain, A, RHS, x, nb, maxit, tol, conv, transpose):
+    """BiCGStab with the ILU(0) right preconditioner (pict_bicgstab_ilu) on the CSR form of A; nb right-hand
+    sides solved one after another with the same factors, as the reference's bicgstabSolveGPU does."""
+    _check(domain._desc.num_sims == 1, "SolveLinear: the preconditioned BiCGStab takes single-simulation domains")
+    lib = _lib.load()
+    plan = _ilu_plan(domain)
+    n, nnz = plan["n"], plan["nnz"]
+    dtype = domain.getDtype()
+    aval = torch.empty(nnz, dtype=dtype, device=domain.getDevice())
+    check(lib.pict_stencil_to_csr(ctypes.byref(domain._desc), _ptr(A.coef.contiguous()), _ptr(plan["row"]), _ptr(aval),
+                                  _ptr(plan["index_out"]), _stream_ptr()), "stencil_to_csr")
+    ws = torch.empty(int(lib.pict_bicgstab_ilu_workspace_bytes(n, nnz, _dtype_code(dtype))), dtype=torch.uint8,
+                     device=domain.getDevice())
+    info = (ctypes.c_uint8 * (_lib.SOLVE_INFO_BYTES * nb))()
+    check(lib.pict_bicgstab_ilu(n, nnz, _dtype_code(dtype), _ptr(plan["row"]), _ptr(plan["index"]), _ptr(plan["diag"]),
+                                _ptr(plan["tpos"]), _ptr(plan["order_f"]), plan["ptr_f"].ctypes.data, plan["nlf"],
+                                _ptr(plan["order_b"]), plan["ptr_b"].ctypes.data, plan["nlb"], _ptr(aval), _ptr(RHS),
+                                _ptr(x), nb, maxit, tol, conv, 0, int(transpose), ctypes.addressof(info), _ptr(ws),
+                                ws.numel(), _stream_ptr()), "bicgstab_ilu")
+    return decode_infos(torch.frombuffer(bytearray(info), dtype=torch.uint8))
 
 
 def SparseOuterProduct(a, b, out_pattern):

@@ -258,14 +258,28 @@ def _linear_solve_wrapper(csrMat, rhs, result, maxit_torch, tol_torch, convergen
                           matrix_rank_deficient, residual_reset_step, transpose, print_residual, return_best_result,
                           is_FWD=None, debug_out=False, double_fallback=False, BiCG_with_preconditioner=True,
                           BiCG_precondition_fallback=False):
-    """Solve with the persistent Krylov kernels and check the reports (PISOtorch_diff.py:245-293).
-    An all-zero right-hand side gives x = 0."""
+    """Solve and check the reports (PISOtorch_diff.py:245-293).  An all-zero right-hand side gives x = 0.
+    BiCGStab runs with the ILU(0) preconditioner when BiCG_with_preconditioner is set; with
+    BiCG_precondition_fallback an unpreconditioned BiCGStab solve that did not succeed is repeated from zero
+    with the preconditioner (PISOtorch_diff.py:276-286)."""
     if bool(rhs.eq(0).all()):
         result.zero_()
         return []
+    use_pre = bool(use_BiCG and BiCG_with_preconditioner)
     infos = PISOtorch.SolveLinear(csrMat, rhs, result, maxit_torch, tol_torch, convergence_criterion, use_BiCG,
                                   matrix_rank_deficient, residual_reset_step, transpose, print_residual,
-                                  return_best_result, BiCGwithPreconditioner=False)
+                                  return_best_result, BiCGwithPreconditioner=use_pre)
+
+    def not_solved(sinfos):
+        return (not return_best_result and any(not i.converged for i in sinfos)) or \
+            (return_best_result and any(not i.isFiniteResidual for i in sinfos))
+
+    if BiCG_precondition_fallback and use_BiCG and not use_pre and not_solved(infos):
+        _LOG.warning("Not preconditioned BiCG solve failed, trying preconditioned.")
+        result.zero_()
+        infos = PISOtorch.SolveLinear(csrMat, rhs, result, maxit_torch, tol_torch, convergence_criterion, use_BiCG,
+                                      matrix_rank_deficient, residual_reset_step, transpose, print_residual,
+                                      return_best_result, BiCGwithPreconditioner=True)
     _check_solver_return_infos(infos, transpose, use_BiCG, float(tol_torch.reshape(-1)[0]) if isinstance(tol_torch, torch.Tensor) else tol_torch,
                                int(maxit_torch.reshape(-1)[0]) if isinstance(maxit_torch, torch.Tensor) else maxit_torch,
                                return_best_result, is_FWD)
@@ -295,7 +309,8 @@ def linear_solve_GPU(csrMat, rhs, transpose=False, use_BiCG=False, tol=None, max
         def forward(ctx, A_coef, b):
             x = torch.zeros_like(b)
             _linear_solve_wrapper(A, b.detach(), x, maxit_torch, tol_torch, conv, use_BiCG, False, 0, transpose, False,
-                                  return_best_result, is_FWD=True)
+                                  return_best_result, is_FWD=True, BiCG_with_preconditioner=BiCG_with_preconditioner,
+                                  BiCG_precondition_fallback=BiCG_precondition_fallback)
             ctx.save_for_backward(A_coef, x)
             return x
 
@@ -308,7 +323,9 @@ def linear_solve_GPU(csrMat, rhs, transpose=False, use_BiCG=False, tol=None, max
                 grad_b = torch.zeros_like(grad_x)
                 Aw = PISOtorch.StencilMatrix(A._domain(), A_coef)
                 _linear_solve_wrapper(Aw, grad_x.contiguous(), grad_b, maxit_torch, tol_torch, conv, use_BiCG, False, 0,
-                                      not transpose, False, return_best_result, is_FWD=False)
+                                      not transpose, False, return_best_result, is_FWD=False,
+                                      BiCG_with_preconditioner=BiCG_with_preconditioner,
+                                      BiCG_precondition_fallback=BiCG_precondition_fallback)
                 if ctx.needs_input_grad[0]:
                     d = A._domain()
                     grad_A = torch.zeros_like(A_coef)

@@ -488,13 +488,23 @@ class Simulation:
             if bool(rhs.eq(0).all()):
                 x.zero_()
                 return x, True
+            pre = bool(use_BiCG and self.preconditionBiCG)
             infos = PISOtorch.SolveLinear(csrMat, rhs, x, max_iter, tol, PISOtorch.ConvergenceCriterion.NORM2_NORMALIZED,
                                           use_BiCG, False, residual_reset_step, False, False, return_best_result,
-                                          BiCGwithPreconditioner=False)
+                                          BiCGwithPreconditioner=pre)
+            if self.BiCG_precondition_fallback and use_BiCG and not pre and _not_solved(infos, return_best_result):
+                # PISOtorch_diff.py:276-286: repeat a failed unpreconditioned BiCGStab solve, preconditioned
+                _LOG.warning("Not preconditioned BiCG solve failed, trying preconditioned.")
+                x.zero_()
+                infos = PISOtorch.SolveLinear(csrMat, rhs, x, max_iter, tol, PISOtorch.ConvergenceCriterion.NORM2_NORMALIZED,
+                                              use_BiCG, False, residual_reset_step, False, False, return_best_result,
+                                              BiCGwithPreconditioner=True)
             _check_infos(infos, use_BiCG, tol, max_iter, return_best_result)
             return x, True
         return self._backend.linear_solve_GPU(csrMat, rhs, transpose=False, use_BiCG=use_BiCG, tol=tol,
-                                              max_iter=max_iter, return_best_result=return_best_result), True
+                                              max_iter=max_iter, return_best_result=return_best_result,
+                                              BiCG_with_preconditioner=self.preconditionBiCG,
+                                              BiCG_precondition_fallback=self.BiCG_precondition_fallback), True
 
     # ------------------------------------------------------------------ step
     def _fused_eligible(self):
@@ -921,6 +931,11 @@ class Simulation:
             if self._check_stop() or not sim_ok:
                 break
         return sim_ok
+
+
+def _not_solved(infos, return_best_result):
+    return (not return_best_result and any(not i.converged for i in infos)) or \
+        (return_best_result and any(not i.isFiniteResidual for i in infos))
 
 
 def _check_infos(infos, use_BiCG, tol, max_iter, return_best_result):

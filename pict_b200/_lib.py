@@ -190,6 +190,12 @@ SIGNATURES = {
     "pict_refine_finish": (c_i32, [_PD, c_vp, c_vp, c_i32, c_i32, c_vp, c_vp]),
     "pict_mg_set_bulk_staging": (None, [c_i32]),
     "pict_krylov_set_cluster_mode": (None, [c_i32]),
+    "pict_ilu_analyze": (c_i32, [c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "pict_bicgstab_ilu_workspace_bytes": (ctypes.c_int64, [c_i32, c_i32, c_i32]),
+    "pict_ilu0_factor": (c_i32, [c_i32, c_i32, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_i32, c_vp, c_vp, c_vp]),
+    "pict_bicgstab_ilu": (c_i32, [c_i32, c_i32, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_i32, c_vp, c_vp, c_i32,
+                                  c_vp, c_vp, c_vp, c_i32, c_i32, ctypes.c_double, c_i32, c_i32, c_i32, c_vp, c_vp,
+                                  ctypes.c_int64, c_vp]),
     "pict_mg_galerkin": (c_i32, [ctypes.POINTER(MgLevel), ctypes.POINTER(MgLevel), c_vp]),
     "pict_pcg_mg_workspace_bytes": (ctypes.c_int64, [_PD, ctypes.POINTER(MgLevel), c_i32]),
     "pict_pcg_mg": (c_i32, [_PD, ctypes.POINTER(MgLevel), c_i32, c_vp, c_vp, c_i32, ctypes.c_double, c_i32, c_vp, c_vp,
