@@ -398,16 +398,22 @@ pict_status_t pict_scalar_grad(const pict_domain_t* dom, double dt, int32_t non_
  * length of the cell transform M, 1 without one). */
 pict_status_t pict_sgs_smagorinsky(const pict_domain_t* dom, double coefficient, void* out, void* stream);
 
-/* ---------------- ILU(0)-preconditioned BiCGStab ----------------
+/* ---------------- preconditioned BiCGStab ----------------
  * SolveLinear with useBiCG and BiCGwithPreconditioner (bicgstabSolveGPU, extensions/bicgstab_solver_kernel.cu:47-395),
  * the fallback of the reference's solve wrapper (PISOtorch_diff.py:276-286), on the CSR form of a stencil matrix
  * (pict_csr_row_ptr / pict_stencil_to_csr; rows sorted by column) of a single-system domain.
+ * Preconditioners: PICT_PRECOND_AS_REFERENCE, the operator the reference's build applies (M = T T, T the lower
+ * triangle of the matrix including its diagonal: two forward sweeps per application; it sets up csrilu02 factors
+ * at extensions/bicgstab_solver_kernel.cu:150-208 but its triangular solves do not apply them); PICT_PRECOND_ILU0,
+ * M = L U of the zero-fill incomplete LU factors (what the reference's set-up intends).
  * pict_ilu_analyze (host arrays): diagonal and transposed-entry positions, rows grouped by forward / backward
  *   dependency level (order [n], level starts ptr [n + 1]); the pattern must be structurally symmetric.
  * pict_ilu0_factor: ILU(0) factors (IKJ order, unit lower factor) of the CSR values `a` into `f`, level by level.
- * pict_bicgstab_ilu: right-preconditioned BiCGStab (M = L U; with transpose the operator and preconditioner are
- *   transposed) in the reference's loop order and reporting; rhs, x [nrhs][n] (device), info_host [nrhs]
+ * pict_bicgstab_ilu: right-preconditioned BiCGStab (preconditioner: PICT_PRECOND_*; with transpose the operator and
+ *   preconditioner are transposed) in the reference's loop order and reporting; rhs, x [nrhs][n] (device), info_host [nrhs]
  *   (host); synchronises the stream once per reduction; workspace of pict_bicgstab_ilu_workspace_bytes(). */
+#define PICT_PRECOND_AS_REFERENCE 0
+#define PICT_PRECOND_ILU0 1
 pict_status_t pict_ilu_analyze(int32_t n, const int32_t* row, const int32_t* index, int32_t* diag, int32_t* tpos,
                                int32_t* order_f, int32_t* ptr_f, int32_t* order_b, int32_t* ptr_b, int32_t* nlev_f,
                                int32_t* nlev_b);
@@ -420,8 +426,8 @@ pict_status_t pict_bicgstab_ilu(int32_t n, int32_t nnz, int32_t dtype, const int
                                 const int32_t* ptr_f_host, int32_t nlev_f, const int32_t* order_b,
                                 const int32_t* ptr_b_host, int32_t nlev_b, const void* aval, const void* rhs, void* x,
                                 int32_t nrhs, int32_t max_iterations, double tolerance, int32_t convergence,
-                                int32_t x_is_zero, int32_t transpose, void* info_host, void* workspace,
-                                int64_t workspace_bytes, void* stream);
+                                int32_t x_is_zero, int32_t transpose, int32_t preconditioner, void* info_host,
+                                void* workspace, int64_t workspace_bytes, void* stream);
 
 /* ---------------- advective outflow boundaries ----------------
  * update_advective_boundaries followed by balance_boundary_fluxes (PISOtorch_simulation.py:145-312, the

@@ -1577,28 +1577,41 @@ def ilu0(val, index, row):
     return f
 
 
-def _ilu_apply(L, U, y, transpose):
-    """z = (L U)^-1 y, or (L U)^-T y: the two triangular solves of one preconditioner application
-    (extensions/bicgstab_solver_kernel.cu:270-276, 313-319)."""
+def _precond_apply(kind, A, L, U, y, transpose):
+    """One application of the BiCGStab preconditioner, z = M^-1 y (or M^-T y; transposed triangular solves
+    at extensions/bicgstab_solver_kernel.cu:270-276, 313-319).  kind "as_reference": the operator the
+    reference's build applies, M = T T with T = tril(A) including the diagonal (the matrix values; the
+    csrilu02 factors of :196-208 are not what its solves read), reproducing its iterations, residuals and
+    solutions; kind "ilu0": M = L U of ilu0()."""
+    if kind == "as_reference":
+        T = sp.tril(A, 0, format="csr")
+        if transpose:
+            Tt = T.T.tocsr()
+            return spla.spsolve_triangular(Tt, spla.spsolve_triangular(Tt, y, lower=False), lower=False)
+        return spla.spsolve_triangular(T, spla.spsolve_triangular(T, y, lower=True), lower=True)
     if not transpose:
         return spla.spsolve_triangular(U, spla.spsolve_triangular(L, y, lower=True, unit_diagonal=True), lower=False)
     return spla.spsolve_triangular(L.T.tocsr(), spla.spsolve_triangular(U.T.tocsr(), y, lower=True), lower=False,
                                    unit_diagonal=True)
 
 
-def bicgstab_ilu(val, index, row, b, tol=1e-5, maxit=5000, transpose=False, conv="NORM2_NORMALIZED"):
-    """bicgstabSolveGPU with the ILU(0) preconditioner (extensions/bicgstab_solver_kernel.cu:240-360): right
-    preconditioning, p^ = M^-1 p and s^ = M^-1 s with M = L U of ilu0(), from x = 0; `transpose` solves with
+def bicgstab_ilu(val, index, row, b, tol=1e-5, maxit=5000, transpose=False, conv="NORM2_NORMALIZED",
+                 preconditioner="as_reference"):
+    """bicgstabSolveGPU with its preconditioner (extensions/bicgstab_solver_kernel.cu:240-360): right
+    preconditioning, p^ = M^-1 p and s^ = M^-1 s (M per _precond_apply), from x = 0; `transpose` solves with
     A^T and M^T.  Iteration bookkeeping as bicgstab()."""
     val = np.asarray(val, dtype=np.float64)
     n = len(row) - 1
-    A = sp.csr_matrix((val, np.asarray(index), np.asarray(row)), shape=(n, n))
-    f = ilu0(val, index, row)
-    F = sp.csr_matrix((f, np.asarray(index), np.asarray(row)), shape=(n, n))
-    L = sp.tril(F, -1, format="csr")
-    U = sp.triu(F, 0, format="csr")
-    if transpose:
-        A = A.T.tocsr()
+    A0 = sp.csr_matrix((val, np.asarray(index), np.asarray(row)), shape=(n, n))
+    L = U = None
+    if preconditioner == "ilu0":
+        f = ilu0(val, index, row)
+        F = sp.csr_matrix((f, np.asarray(index), np.asarray(row)), shape=(n, n))
+        L = sp.tril(F, -1, format="csr")
+        U = sp.triu(F, 0, format="csr")
+    elif preconditioner != "as_reference":
+        raise KeyError(preconditioner)
+    A = A0.T.tocsr() if transpose else A0
     b = np.asarray(b, dtype=np.float64)
     x = np.zeros_like(b)
     r = b.copy()
@@ -1616,7 +1629,7 @@ def bicgstab_ilu(val, index, row, b, tol=1e-5, maxit=5000, transpose=False, conv
         if i > 0:
             beta = (rho / rhop) * (alpha / omega)
             p = r + beta * (p - omega * v)
-        pw = _ilu_apply(L, U, p, transpose)
+        pw = _precond_apply(preconditioner, A0, L, U, p, transpose)
         v = A @ pw
         alpha = rho / float(np.dot(rw, v))
         r = r - alpha * v
@@ -1628,7 +1641,7 @@ def bicgstab_ilu(val, index, row, b, tol=1e-5, maxit=5000, transpose=False, conv
         if nrmr < tol:
             info.converged = True
             break
-        s = _ilu_apply(L, U, r, transpose)
+        s = _precond_apply(preconditioner, A0, L, U, r, transpose)
         t = A @ s
         omega = float(np.dot(t, r)) / float(np.dot(t, t))
         x = x + omega * s

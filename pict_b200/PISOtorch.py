@@ -68,6 +68,34 @@ class ConvergenceCriterion(enum.IntEnum):
     ABS_MAX = 4
 
 
+class BiCGPreconditioner(enum.IntEnum):
+    """Preconditioner of SolveLinear(useBiCG=True, BiCGwithPreconditioner=True); no counterpart in the
+    reference's module, which has one fixed behaviour.  AS_REFERENCE (default): the operator the
+    reference's build applies, M = T T with T the lower triangle of the matrix including its diagonal
+    (extensions/bicgstab_solver_kernel.cu:150-208 sets up csrilu02 factors, but its triangular solves apply
+    the unfactorised lower triangle twice), so solves, iteration counts and reports equal the reference's.
+    ILU0: M = L U of the zero-fill incomplete LU factors, the preconditioner the reference's set-up
+    intends (fewer iterations)."""
+    AS_REFERENCE = 0
+    ILU0 = 1
+
+
+_bicg_preconditioner = BiCGPreconditioner.AS_REFERENCE
+
+
+def SetBiCGPreconditioner(kind):
+    """Select the preconditioner of preconditioned BiCGStab solves (BiCGPreconditioner); returns the
+    previous one."""
+    global _bicg_preconditioner
+    prev = _bicg_preconditioner
+    _bicg_preconditioner = BiCGPreconditioner(kind)
+    return prev
+
+
+def GetBiCGPreconditioner():
+    return _bicg_preconditioner
+
+
 class NonOrthoFlags(enum.IntFlag):
     """Bits of the ``nonOrthoFlags`` argument (extensions/PISO_multiblock_cuda.h:9-13).  The reference
     declares a pybind11 enum of this name but leaves it commented out (extensions/PISOtorch.cpp:491-501),
@@ -2609,8 +2637,9 @@ def _ilu_plan(domain):
 
 
 def _solve_bicgstab_ilu(domain, A, RHS, x, nb, maxit, tol, conv, transpose):
-    """BiCGStab with the ILU(0) right preconditioner (pict_bicgstab_ilu) on the CSR form of A; nb right-hand
-    sides solved one after another with the same factors, as the reference's bicgstabSolveGPU does."""
+    """BiCGStab with the right preconditioner selected by SetBiCGPreconditioner (pict_bicgstab_ilu) on the
+    CSR form of A; nb right-hand sides solved one after another with the same preconditioner, as the
+    reference's bicgstabSolveGPU does."""
     _check(domain._desc.num_sims == 1, "SolveLinear: the preconditioned BiCGStab takes single-simulation domains")
     lib = _lib.load()
     plan = _ilu_plan(domain)
@@ -2625,7 +2654,8 @@ def _solve_bicgstab_ilu(domain, A, RHS, x, nb, maxit, tol, conv, transpose):
     check(lib.pict_bicgstab_ilu(n, nnz, _dtype_code(dtype), _ptr(plan["row"]), _ptr(plan["index"]), _ptr(plan["diag"]),
                                 _ptr(plan["tpos"]), _ptr(plan["order_f"]), plan["ptr_f"].ctypes.data, plan["nlf"],
                                 _ptr(plan["order_b"]), plan["ptr_b"].ctypes.data, plan["nlb"], _ptr(aval), _ptr(RHS),
-                                _ptr(x), nb, maxit, tol, conv, 0, int(transpose), ctypes.addressof(info), _ptr(ws),
+                                _ptr(x), nb, maxit, tol, conv, 0, int(transpose), int(_bicg_preconditioner),
+                                ctypes.addressof(info), _ptr(ws),
                                 ws.numel(), _stream_ptr()), "bicgstab_ilu")
     return decode_infos(torch.frombuffer(bytearray(info), dtype=torch.uint8))
 

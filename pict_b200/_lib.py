@@ -20,6 +20,8 @@ PICT_FACE_PERIODIC = 1
 PICT_FACE_CONNECTED = 2
 PICT_CONV_NORM2 = 0
 PICT_CONV_NORM2_NORMALIZED = 1
+PICT_PRECOND_AS_REFERENCE = 0
+PICT_PRECOND_ILU0 = 1
 
 
 class PictLibraryError(RuntimeError):
@@ -194,8 +196,8 @@ SIGNATURES = {
     "pict_bicgstab_ilu_workspace_bytes": (ctypes.c_int64, [c_i32, c_i32, c_i32]),
     "pict_ilu0_factor": (c_i32, [c_i32, c_i32, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_i32, c_vp, c_vp, c_vp]),
     "pict_bicgstab_ilu": (c_i32, [c_i32, c_i32, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_i32, c_vp, c_vp, c_i32,
-                                  c_vp, c_vp, c_vp, c_i32, c_i32, ctypes.c_double, c_i32, c_i32, c_i32, c_vp, c_vp,
-                                  ctypes.c_int64, c_vp]),
+                                  c_vp, c_vp, c_vp, c_i32, c_i32, ctypes.c_double, c_i32, c_i32, c_i32, c_i32, c_vp,
+                                  c_vp, ctypes.c_int64, c_vp]),
     "pict_mg_galerkin": (c_i32, [ctypes.POINTER(MgLevel), ctypes.POINTER(MgLevel), c_vp]),
     "pict_pcg_mg_workspace_bytes": (ctypes.c_int64, [_PD, ctypes.POINTER(MgLevel), c_i32]),
     "pict_pcg_mg": (c_i32, [_PD, ctypes.POINTER(MgLevel), c_i32, c_vp, c_vp, c_i32, ctypes.c_double, c_i32, c_vp, c_vp,

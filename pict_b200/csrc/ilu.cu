@@ -14,8 +14,13 @@
 //
 // The solve is the reference's right-preconditioned BiCGStab loop (residual checks after both half
 // steps, the same reported iterations), driven from the host with the scalars read back per reduction.
-// Preconditioner: M = L U, applied as U^-1 L^-1 (for the transposed operator M^T = U^T L^T, applied as
-// L^-T U^-T).
+// Two preconditioners:
+//  * PICT_PRECOND_AS_REFERENCE: the operator the reference's build applies, M = T T with T the lower
+//    triangle of A including its diagonal (the matrix values, not the factors), applied as two forward
+//    sweeps T^-1 T^-1 (transposed: two backward sweeps T^-T T^-T).  This reproduces the reference's
+//    preconditioned solves (iterations, residuals, solutions) on the recorded systems;
+//  * PICT_PRECOND_ILU0: M = L U of the ILU(0) factors, applied as U^-1 L^-1 (transposed: M^T = U^T L^T,
+//    applied as L^-T U^-T).
 #include <cmath>
 #include <cstdio>
 #include <vector>
@@ -180,9 +185,20 @@ struct IluSolver {
         return check_launch("ilu triangular solve");
     }
 
-    // out = M^-1 in (M = L U), or M^-T in; y: scratch
-    pict_status_t apply(const T* f, const T* in, T* y, T* out, bool tr) {
+    // out = M^-1 in, or M^-T in; y: scratch.  ilu: M = L U of the factors f; else M = T T, T the lower
+    // triangle (with diagonal) of the matrix values f
+    pict_status_t apply(const T* f, const T* in, T* y, T* out, bool tr, bool ilu) {
         pict_status_t s;
+        if (!ilu) {
+            if (!tr) {
+                s = trsv<true, false, false>(f, in, y);  // T y = in
+                if (s) return s;
+                return trsv<true, false, false>(f, y, out);  // T out = y
+            }
+            s = trsv<false, false, true>(f, in, y);  // T^T y = in
+            if (s) return s;
+            return trsv<false, false, true>(f, y, out);  // T^T out = y
+        }
         if (!tr) {
             s = trsv<true, true, false>(f, in, y);  // L y = in
             if (s) return s;
@@ -215,8 +231,8 @@ static pict_status_t ilu_factor(const IluPlan& P, const T* a, T* f, cudaStream_t
 
 template <typename T>
 static pict_status_t run_bicgstab_ilu(const IluPlan& P, const T* aval, const T* rhs, T* x, int nrhs, int maxit,
-                                      double tol, int conv, int x_zero, int tr, pict_solve_info_t* info_host,
-                                      char* ws, cudaStream_t st) {
+                                      double tol, int conv, int x_zero, int tr, int kind,
+                                      pict_solve_info_t* info_host, char* ws, cudaStream_t st) {
     const size_t vb = (((size_t)P.n * sizeof(T)) + 255) & ~(size_t)255;
     char* o = ws;
     T* f = reinterpret_cast<T*>(o);
@@ -226,8 +242,13 @@ static pict_status_t run_bicgstab_ilu(const IluPlan& P, const T* aval, const T* 
     o += 8 * vb;
     double* part = reinterpret_cast<double*>(o);
     double* scal = part + ILU_RED_BLOCKS;
-    pict_status_t st_ = ilu_factor<T>(P, aval, f, st);
-    if (st_) return st_;
+    const bool ilu = kind == PICT_PRECOND_ILU0;
+    pict_status_t st_ = PICT_OK;
+    if (ilu) {
+        if ((st_ = ilu_factor<T>(P, aval, f, st))) return st_;
+    } else {
+        f = const_cast<T*>(aval);  // the sweeps read the matrix values themselves
+    }
     IluSolver<T> S{P, st, part, scal};
     const int n = P.n;
     const int g = cell_grid(n, ILU_THREADS);
@@ -264,7 +285,7 @@ static pict_status_t run_bicgstab_ilu(const IluPlan& P, const T* aval, const T* 
                 const double beta = (rho / rhop) * (alpha / omega);
                 k_bicg_dir<T><<<g, ILU_THREADS, 0, st>>>(n, r, (T)beta, (T)omega, v, p);
             }
-            if ((st_ = S.apply(f, p, y, pw, tr))) return st_;
+            if ((st_ = S.apply(f, p, y, pw, tr, ilu))) return st_;
             if ((st_ = S.spmv(aval, pw, v, tr))) return st_;
             if ((st_ = S.reduce(0, rw, v, &tmp))) return st_;
             alpha = rho / tmp;
@@ -284,7 +305,7 @@ static pict_status_t run_bicgstab_ilu(const IluPlan& P, const T* aval, const T* 
                 inf.converged = 1;
                 break;
             }
-            if ((st_ = S.apply(f, r, y, s, tr))) return st_;
+            if ((st_ = S.apply(f, r, y, s, tr, ilu))) return st_;
             if ((st_ = S.spmv(aval, s, t, tr))) return st_;
             if ((st_ = S.reduce(0, t, r, &tmp))) return st_;
             if ((st_ = S.reduce(0, t, t, &tmp2))) return st_;
@@ -392,15 +413,15 @@ pict_status_t pict_ilu0_factor(int32_t n, int32_t nnz, int32_t dtype, const int3
     return ilu_factor<float>(P, (const float*)a, (float*)f, st);
 }
 
-// BiCGStab with the ILU(0) right preconditioner on the CSR matrix (row, index, aval) of a single-system
+// BiCGStab with a right preconditioner (PICT_PRECOND_*) on the CSR matrix (row, index, aval) of a single-system
 // domain; rhs, x: [nrhs][n] (device); info_host: [nrhs] (host).  Synchronises the stream per reduction.
 pict_status_t pict_bicgstab_ilu(int32_t n, int32_t nnz, int32_t dtype, const int32_t* row, const int32_t* index,
                                 const int32_t* diag, const int32_t* tpos, const int32_t* order_f,
                                 const int32_t* ptr_f_host, int32_t nlev_f, const int32_t* order_b,
                                 const int32_t* ptr_b_host, int32_t nlev_b, const void* aval, const void* rhs, void* x,
                                 int32_t nrhs, int32_t max_iterations, double tolerance, int32_t convergence,
-                                int32_t x_is_zero, int32_t transpose, void* info_host, void* workspace,
-                                int64_t workspace_bytes, void* stream) {
+                                int32_t x_is_zero, int32_t transpose, int32_t preconditioner, void* info_host,
+                                void* workspace, int64_t workspace_bytes, void* stream) {
     if (n <= 0 || !row || !index || !diag || !tpos || !order_f || !ptr_f_host || !order_b || !ptr_b_host || !aval ||
         !rhs || !x || !info_host || !workspace || nrhs < 1)
         return set_error(PICT_ERR_ARG, "bicgstab_ilu: invalid argument");
@@ -408,6 +429,8 @@ pict_status_t pict_bicgstab_ilu(int32_t n, int32_t nnz, int32_t dtype, const int
         return set_error(PICT_ERR_ARG, "bicgstab_ilu: workspace too small");
     if (convergence < PICT_CONV_NORM2 || convergence > PICT_CONV_ABS_MAX)
         return set_error(PICT_ERR_ARG, "bicgstab_ilu: unknown convergence criterion");
+    if (preconditioner != PICT_PRECOND_AS_REFERENCE && preconditioner != PICT_PRECOND_ILU0)
+        return set_error(PICT_ERR_ARG, "bicgstab_ilu: unknown preconditioner");
     IluPlan P;
     P.n = n;
     P.nnz = nnz;
@@ -426,9 +449,9 @@ pict_status_t pict_bicgstab_ilu(int32_t n, int32_t nnz, int32_t dtype, const int
     char* ws = reinterpret_cast<char*>(workspace);
     if (dtype == PICT_F64)
         return run_bicgstab_ilu<double>(P, (const double*)aval, (const double*)rhs, (double*)x, nrhs, max_iterations,
-                                        tolerance, convergence, x_is_zero, transpose, info, ws, st);
+                                        tolerance, convergence, x_is_zero, transpose, preconditioner, info, ws, st);
     return run_bicgstab_ilu<float>(P, (const float*)aval, (const float*)rhs, (float*)x, nrhs, max_iterations, tolerance,
-                                   convergence, x_is_zero, transpose, info, ws, st);
+                                   convergence, x_is_zero, transpose, preconditioner, info, ws, st);
 }
 
 }  // extern "C"

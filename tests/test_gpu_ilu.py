@@ -1,11 +1,15 @@
-"""ILU(0)-preconditioned BiCGStab on the device (GPU), through SolveLinear(useBiCG=True,
+"""Preconditioned BiCGStab on the device (GPU), through SolveLinear(useBiCG=True,
 BiCGwithPreconditioner=True) and the C-ABI factorisation:
 
-* pict_ilu0_factor against the oracle's ilu0() on the advection matrices of five setups (FP64 to round-off);
-* solutions against the reference's own CUDA build (tests/golden/ref_ilu_*.npz) and the oracle's
-  preconditioned BiCGStab, plain and transposed, FP64 and FP32, with at most the oracle's iterations + 1;
-* the preconditioned fallback of the linear-solve wrapper (PISOtorch_diff.py:276-286): an unpreconditioned
-  BiCGStab solve that stops unconverged at max_iter is repeated preconditioned and converges.
+* the default preconditioner (BiCGPreconditioner.AS_REFERENCE, the operator the reference's build applies)
+  reproduces the reference build's preconditioned solves (tests/golden/ref_ilu_*.npz): the same iteration
+  counts (FP64; FP32 within one), solutions to 1e-10 (FP64), plain and transposed;
+* ILU0: pict_ilu0_factor against the oracle's ilu0() on the advection matrices of five setups (FP64 to
+  round-off); solutions against the reference's and the oracle's ILU(0) solve, with at most the oracle's
+  iterations + 1;
+* the preconditioned fallback of the linear-solve wrapper (PISOtorch_diff.py:276-286) and of
+  Simulation.linear_solve: an unpreconditioned BiCGStab solve that stops unconverged at max_iter is repeated
+  preconditioned and converges.
 """
 import os
 
@@ -71,10 +75,46 @@ def test_ilu0_factor_matches_oracle(name, dtype):
     assert np.abs(_np(f) - ref).max() <= bound * np.abs(ref).max()
 
 
+@pytest.fixture
+def ilu0_mode():
+    from pict_b200 import PISOtorch as P
+    prev = P.SetBiCGPreconditioner(P.BiCGPreconditioner.ILU0)
+    yield
+    P.SetBiCGPreconditioner(prev)
+
+
 @pytest.mark.parametrize("transpose", [False, True])
 @pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
 @pytest.mark.parametrize("name", ILU_CASES)
-def test_ilu_bicgstab_matches_reference_and_oracle(name, dtype, transpose):
+def test_preconditioned_bicgstab_reproduces_reference(name, dtype, transpose):
+    from pict_b200 import PISOtorch as P
+    assert P.GetBiCGPreconditioner() == P.BiCGPreconditioner.AS_REFERENCE
+    fx = _load("ref_ilu_%s.npz" % name)
+    pd = _advection(name, dtype)
+    D = pd.getSpatialDims()
+    tag = "f64" if dtype == torch.float64 else "f32"
+    tol = 1e-10 if dtype == torch.float64 else 1e-6
+    b = torch.tensor(fx["b"], dtype=dtype, device="cuda")
+    x, infos = _solve(pd, b, tol, transpose, True)
+    assert all(i.converged and i.isFiniteResidual for i in infos)
+    n = pd.C.getRows()
+    xs = _np(x).reshape(D, n)
+    key = "%s_t%d_p1" % (tag, int(transpose))
+    ref = fx["x_" + key].reshape(D, n)
+    rinfo = fx["info_" + key]
+    for c in range(D):
+        if dtype == torch.float64:
+            assert infos[c].usedIterations == int(rinfo[c, 1])
+            assert np.abs(xs[c] - ref[c]).max() <= 1e-10 * np.abs(ref[c]).max()
+        else:
+            assert abs(infos[c].usedIterations - int(rinfo[c, 1])) <= 1
+            assert np.abs(xs[c] - ref[c]).max() <= 5e-5 * np.abs(ref[c]).max()
+
+
+@pytest.mark.parametrize("transpose", [False, True])
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+@pytest.mark.parametrize("name", ILU_CASES)
+def test_ilu0_bicgstab_matches_reference_and_oracle(name, dtype, transpose, ilu0_mode):
     fx = _load("ref_ilu_%s.npz" % name)
     pd = _advection(name, dtype)
     D = pd.getSpatialDims()
@@ -90,7 +130,8 @@ def test_ilu_bicgstab_matches_reference_and_oracle(name, dtype, transpose):
     idx, row = pd.C.index.cpu().numpy(), pd.C.row.cpu().numpy()
     bref = fx["b"].reshape(D, n)
     for c in range(D):
-        xo, io = po.bicgstab_ilu(val, idx, row, bref[c], tol=tol, maxit=300, transpose=transpose)
+        xo, io = po.bicgstab_ilu(val, idx, row, bref[c], tol=tol, maxit=300, transpose=transpose,
+                                 preconditioner="ilu0")
         scale = np.abs(ref[c]).max()
         bound = 1e-8 if dtype == torch.float64 else 5e-5
         assert np.abs(xs[c] - ref[c]).max() <= bound * scale
@@ -114,7 +155,7 @@ def _shifted_laplacian(n=48):
     return pd, M, b
 
 
-def test_preconditioned_fallback_recovers_a_failed_solve():
+def test_preconditioned_fallback_recovers_a_failed_solve(ilu0_mode):
     from pict_b200 import PISOtorch as P
     from pict_b200 import PISOtorch_diff as PD
     from pict_b200.engine import LinsolveError
@@ -145,7 +186,7 @@ def test_preconditioned_fallback_recovers_a_failed_solve():
     assert np.sqrt(np.mean(r * r)) < tol
 
 
-def test_simulation_fallback_flag_reaches_solve():
+def test_simulation_fallback_flag_reaches_solve(ilu0_mode):
     """Simulation.linear_solve passes preconditionBiCG / BiCG_precondition_fallback to the solve
     (PISOtorch_simulation.py:896-903): a too-small iteration cap fails without the fallback and succeeds
     with it."""

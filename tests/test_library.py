@@ -109,3 +109,21 @@ def test_non_ortho_flags_enum():
     mode = F.CENTER_MATRIX | F.DIRECT_MATRIX | F.DIAGONAL_RHS
     assert int(mode) == Simulation._NON_ORTHO_MODE == 25
     assert P._non_ortho(mode) == 25 and P._non_ortho(F.NONE) == 0
+
+
+def test_bicg_preconditioner_switch():
+    """SetBiCGPreconditioner selects the preconditioned BiCGStab's operator and returns the previous one;
+    the default is the operator the reference's build applies."""
+    from pict_b200 import PISOtorch as P
+    from pict_b200 import _lib
+    B = P.BiCGPreconditioner
+    assert (int(B.AS_REFERENCE), int(B.ILU0)) == (_lib.PICT_PRECOND_AS_REFERENCE, _lib.PICT_PRECOND_ILU0)
+    assert P.GetBiCGPreconditioner() == B.AS_REFERENCE
+    prev = P.SetBiCGPreconditioner(B.ILU0)
+    try:
+        assert prev == B.AS_REFERENCE and P.GetBiCGPreconditioner() == B.ILU0
+        with pytest.raises(ValueError):
+            P.SetBiCGPreconditioner(7)
+    finally:
+        P.SetBiCGPreconditioner(prev)
+    assert P.GetBiCGPreconditioner() == B.AS_REFERENCE

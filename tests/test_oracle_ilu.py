@@ -2,8 +2,10 @@
 
 * ilu0() is exact LU where the pattern admits no fill (tridiagonal), and in general reproduces A on its
   sparsity pattern ((L U)_ij = A_ij for every stored (i, j)), the defining property of ILU(0);
-* the preconditioned BiCGStab oracle solves the advection systems of the reference's own CUDA build
-  (tests/golden/ref_ilu_*.npz, made by tests/golden/make_ref_ilu_fixtures.py) to the same solution;
+* the preconditioned BiCGStab oracle with the operator the reference's build applies (M = tril(A)^2)
+  reproduces that build's preconditioned solves (tests/golden/ref_ilu_*.npz, made by
+  tests/golden/make_ref_ilu_fixtures.py): iterations, final residuals, solutions; with ILU(0) it reaches
+  the same solutions in fewer iterations;
 * pict_ilu_analyze (host code of the C-ABI library, no device call) returns the diagonal and transposed
   positions and level orders that make every dependency of a row sit in an earlier level.
 """
@@ -58,12 +60,36 @@ def test_ilu0_reproduces_matrix_on_pattern(name):
     assert (LU - A).count_nonzero() > 0 or n < 8
 
 
-@pytest.mark.parametrize("name", ILU_CASES)
-def test_oracle_ilu_bicgstab_matches_reference_solution(name):
+def _ref_fixture(name):
     p = os.path.join(GOLDEN, "ref_ilu_%s.npz" % name)
     if not os.path.exists(p):
         pytest.skip("fixture missing")
-    fx = np.load(p)
+    return np.load(p)
+
+
+@pytest.mark.parametrize("name", ILU_CASES)
+def test_oracle_preconditioned_bicgstab_reproduces_reference(name):
+    """The operator the reference's build applies (M = tril(A)^2) gives its solves: the same iteration
+    counts, final residuals and solutions (FP64, plain and transposed)."""
+    fx = _ref_fixture(name)
+    od, (val, idx, row) = _advection_csr(name)
+    n = row.size - 1
+    D = od.dims
+    b = fx["b"].reshape(D, n)
+    for transpose in (False, True):
+        ref = fx["x_f64_t%d_p1" % int(transpose)].reshape(D, n)
+        info = fx["info_f64_t%d_p1" % int(transpose)]
+        for c in range(D):
+            x, io = po.bicgstab_ilu(val, idx, row, b[c], tol=1e-10, maxit=300, transpose=transpose,
+                                    preconditioner="as_reference")
+            assert io.converged and io.usedIterations == int(info[c, 1])
+            assert abs(io.finalResidual - info[c, 0]) <= 1e-8 * info[c, 0]
+            assert np.abs(x - ref[c]).max() <= 1e-12 * np.abs(ref[c]).max()
+
+
+@pytest.mark.parametrize("name", ILU_CASES)
+def test_oracle_ilu0_bicgstab_matches_reference_solution(name):
+    fx = _ref_fixture(name)
     od, (val, idx, row) = _advection_csr(name)
     n = row.size - 1
     D = od.dims
@@ -72,10 +98,10 @@ def test_oracle_ilu_bicgstab_matches_reference_solution(name):
         ref = fx["x_f64_t%d_p1" % int(transpose)].reshape(D, n)
         ref_unpre = fx["info_f64_t%d_p0" % int(transpose)]
         for c in range(D):
-            x, info = po.bicgstab_ilu(val, idx, row, b[c], tol=1e-10, maxit=300, transpose=transpose)
+            x, info = po.bicgstab_ilu(val, idx, row, b[c], tol=1e-10, maxit=300, transpose=transpose,
+                                      preconditioner="ilu0")
             assert info.converged
-            # the reference's preconditioned solve takes as many iterations as its unpreconditioned one;
-            # a working ILU(0) takes at most as many
+            # ILU(0) takes at most as many iterations as the unpreconditioned solve
             assert info.usedIterations <= int(ref_unpre[c, 1])
             assert np.abs(x - ref[c]).max() <= 1e-8 * np.abs(ref[c]).max()
 
