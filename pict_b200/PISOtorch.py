@@ -23,9 +23,8 @@ periodic and connected block boundaries, per-cell transforms, block/global
 viscosity and velocity sources, in 2D and 3D, float32 and float64, with the gradients of all of it;
 velocity correctors 0/1 (finite differences), 4, 5 and 6 (finite volumes); passive scalar transport
 with its raw gradient operators.  ``SolveLinear``'s CG takes every ``ConvergenceCriterion``, residual
-resets, ``returnBestResult`` and ``matrixRankDeficient``; BiCGStab takes every criterion too.  Face-transform
-pressure assembly raises ``NotImplementedError``; ILU preconditioning is not built (BiCGStab runs
-unpreconditioned, with a warning).
+resets, ``returnBestResult`` and ``matrixRankDeficient``; BiCGStab takes every criterion too, unpreconditioned
+or preconditioned (``BiCGPreconditioner``).  Face-transform pressure assembly raises ``NotImplementedError``.
 """
 from __future__ import annotations
 
@@ -2244,11 +2243,12 @@ def SetupAdvectionMatrixGrad(domain, timeStep, nonOrthoFlags, forPassiveScalar=F
 def SetupAdvectionVelocityGrad(domain, timeStep, nonOrthoFlags, applyPressureGradient=False):
     """Gradient of SetupAdvectionVelocity (extensions/PISO_multiblock_cuda_kernel.cu:4388-4478): velocityRHSGrad to the
     velocity, source, viscosity and boundary velocity gradients, and with non-orthogonal RHS flags to
-    velocityResultGrad (the explicit terms read domain.velocityResult)."""
+    velocityResultGrad (the explicit terms read domain.velocityResult).  applyPressureGradient is accepted
+    like the reference's kernel accepts it, which does not differentiate the pressure term (-dt grad p):
+    the outputs are the same with and without it.  PISOtorch_diff.SetupAdvectionVelocity adds the
+    gradient of that term with respect to the blocks' pressure."""
     from .PISOtorch_diff import _Grads, _p, _stream
     flags = _non_ortho(nonOrthoFlags)
-    if applyPressureGradient:
-        raise NotImplementedError("SetupAdvectionVelocityGrad: no gradient with applyPressureGradient")
     domain._check_ready()
     dt = _time_step(timeStep, domain)
     g = _Grads(domain)
@@ -2280,7 +2280,7 @@ def SetupPressureMatrixGrad(domain, timeStep, nonOrthoMode=0, useFaceTransform=F
     domain.AGrad = Ab + add
 
 
-def _pressure_rhs_grad(domain, dt, with_rhs, what, flags=0):
+def _pressure_rhs_grad(domain, dt, with_rhs, what, flags=0, time_step_norm=False):
     from .PISOtorch_diff import _Grads, _p, _stream
     lib = _lib.load()
     g = _Grads(domain)
@@ -2294,6 +2294,10 @@ def _pressure_rhs_grad(domain, dt, with_rhs, what, flags=0):
         pb = _need_grad(domain, "pressureResultGrad", N)
         Ab = _need_grad(domain, "AGrad", N)
         _nonortho_grad(domain, flags, 3, div_grad, data_bar=pb, coef_bar=Ab, name=what)
+    if time_step_norm:
+        # the divergence was divided by the time step, the non-orthogonal terms added after it are not
+        # (k_computePressureRHSdivergenceFromFlux_GRAD, extensions/PISO_multiblock_cuda_kernel.cu:5424-5448)
+        div_grad = (div_grad / dt).contiguous()
     check(lib.pict_divergence_grad(desc, _p(div_grad), _p(hb), _p(g.vb), st), what)
     # the divergence gradient stays in pressureRHSGrad, as the reference scatters it there in place
     domain.pressureRHSGrad = hb
@@ -2314,22 +2318,24 @@ def _pressure_rhs_grad(domain, dt, with_rhs, what, flags=0):
 def SetupPressureRHSGrad(domain, timeStep, nonOrthoMode=0, useFaceTransform=False, timeStepNorm=False):
     """Gradient of SetupPressureRHS (h = H/A and its divergence, extensions/PISO_multiblock_cuda_kernel.cu:5243-5453):
     pressureRHSGrad and pressureRHSdivGrad to AGrad, CGrad, velocityResultGrad and the velocity, source,
-    viscosity and boundary velocity gradients."""
+    viscosity and boundary velocity gradients; with timeStepNorm the divergence's gradient is divided by
+    the time step."""
     flags = _non_ortho(nonOrthoMode)
-    if useFaceTransform or timeStepNorm:
-        raise NotImplementedError("SetupPressureRHSGrad: no gradient with face transforms / timeStepNorm")
+    if useFaceTransform:
+        raise NotImplementedError("SetupPressureRHSGrad: no gradient with face transforms")
     domain._check_ready()
-    _pressure_rhs_grad(domain, _time_step(timeStep, domain), True, "SetupPressureRHSGrad", flags)
+    _pressure_rhs_grad(domain, _time_step(timeStep, domain), True, "SetupPressureRHSGrad", flags, bool(timeStepNorm))
 
 
 def SetupPressureRHSdivGrad(domain, timeStep, nonOrthoMode=0, useFaceTransform=False, timeStepNorm=False):
     """Gradient of SetupPressureRHSdiv (extensions/PISO_multiblock_cuda_kernel.cu:5423-5453): pressureRHSdivGrad to
     pressureRHSGrad and the boundary velocity gradients."""
     flags = _non_ortho(nonOrthoMode)
-    if useFaceTransform or timeStepNorm:
-        raise NotImplementedError("SetupPressureRHSdivGrad: no gradient with face transforms / timeStepNorm")
+    if useFaceTransform:
+        raise NotImplementedError("SetupPressureRHSdivGrad: no gradient with face transforms")
     domain._check_ready()
-    _pressure_rhs_grad(domain, _time_step(timeStep, domain), False, "SetupPressureRHSdivGrad", flags)
+    _pressure_rhs_grad(domain, _time_step(timeStep, domain), False, "SetupPressureRHSdivGrad", flags,
+                       bool(timeStepNorm))
 
 
 def SetupPressureCorrectionGrad(domain, timeStep, nonOrthoMode=0, useFaceTransform=False, timeStepNorm=False):
@@ -2340,12 +2346,11 @@ def SetupPressureCorrectionGrad(domain, timeStep, nonOrthoMode=0, useFaceTransfo
 
 def CorrectVelocityGrad(domain, timeStep, timeStepNorm=False):
     """Gradient of CorrectVelocity (FD version, extensions/PISO_multiblock_cuda_kernel.cu:6251-6293): velocityResultGrad
-    to pressureRHSGrad and AGrad (assigned, as in the reference) and the blocks' pressure gradients (added)."""
+    to pressureRHSGrad and AGrad (assigned, as in the reference) and the blocks' pressure gradients (added);
+    with timeStepNorm the pressure and A gradients carry the time step factor."""
     from .PISOtorch_diff import _p, _stream
-    if timeStepNorm:
-        raise NotImplementedError("CorrectVelocityGrad: no gradient with timeStepNorm")
     domain._check_ready()
-    _time_step(timeStep, domain)
+    dt = _time_step(timeStep, domain)
     lib = _lib.load()
     N, D = domain.getTotalSize(), domain.getSpatialDims()
     z = lambda n: torch.zeros(n, dtype=domain.getDtype(), device=domain.getDevice())
@@ -2353,10 +2358,13 @@ def CorrectVelocityGrad(domain, timeStep, timeStepNorm=False):
     p_glob = z(N)
     check(lib.pict_copy_field(ctypes.byref(domain._desc), 1, 0, _p(p_glob), 0, _stream()), "CorrectVelocityGrad")
     Ab, pb, hb = z(N), z(N), z(D * N)
-    check(lib.pict_correct_velocity_grad(ctypes.byref(domain._desc), _p(domain.A), _p(p_glob), _p(ug), _p(Ab), _p(pb),
-                                         _p(hb), _stream()), "CorrectVelocityGrad")
+    # timeStepNorm: the pressure update was multiplied by the time step, the pressureRHS term was not
+    # (PISO_update_velocity_GRAD, extensions/PISO_multiblock_cuda_kernel.cu:6270-6283)
+    ug_update = (ug * dt).contiguous() if timeStepNorm else ug
+    check(lib.pict_correct_velocity_grad(ctypes.byref(domain._desc), _p(domain.A), _p(p_glob), _p(ug_update), _p(Ab),
+                                         _p(pb), _p(hb), _stream()), "CorrectVelocityGrad")
     domain.AGrad = Ab
-    domain.pressureRHSGrad = hb
+    domain.pressureRHSGrad = ug.clone() if timeStepNorm else hb
     for b in domain.getBlocks():
         if b.pressureGrad is None or b.pressureGrad.shape != b.pressure.shape:
             b.setPressureGrad(torch.zeros_like(b.pressure))

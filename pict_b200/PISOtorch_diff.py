@@ -14,9 +14,11 @@ solve and the stencil outer product -b_grad x^T (PISOtorch_diff.py:295-375).
 
 Passive scalars (matrix per channel, scalar RHS, result copies) and the non-orthogonal terms
 (nonOrthoFlags of the matrix and RHS operators) are differentiable through their adjoint kernels
-(scalar.cu, nonortho.cu).  Not differentiable here (NotImplementedError): face transforms
-(``useFaceTransform``), whose forward operators the reference marks experimental,
-``apply_pressure_gradient`` and ``timeStepNorm``.
+(scalar.cu, nonortho.cu), and so are the ``timeStepNorm`` forms of the pressure operators and of the
+corrector.  ``SetupAdvectionVelocity(apply_pressure_gradient=True)`` also returns the gradient with respect
+to the blocks' pressure, which the reference's wrapper does not track.  Not differentiable here
+(NotImplementedError): face transforms (``useFaceTransform``), whose forward operators the reference marks
+experimental.
 """
 from __future__ import annotations
 
@@ -496,10 +498,13 @@ _EXCLUDED_GRADIENTS["SetupAdvectionVelocity"] = (set(), set())
 
 def SetupAdvectionVelocity(domain, time_step, non_ortho_flags, apply_pressure_gradient=False):
     """velocityRHS (PISOtorch_diff.py:531-613); differentiable w.r.t. velocity, source, boundary velocity
-    and viscosity, and with non-orthogonal RHS flags w.r.t. the velocity result."""
+    and viscosity, with non-orthogonal RHS flags w.r.t. the velocity result, and with
+    apply_pressure_gradient (velocityRHS -= dt grad p) w.r.t. the blocks' pressure (the reference's
+    wrapper does not track the pressure there, so it gets no gradient from this operator)."""
     is_non_ortho = check_non_ortho_rhs(non_ortho_flags)
     keys, tracked = flatten_domain(domain, ["VELOCITY", "VELOCITY_SOURCE", "BOUNDARY_VELOCITY", "VISCOSITY",
-                                            "VISCOSITY_BLOCK"] + (["VELOCITY_RESULT"] if is_non_ortho else []))
+                                            "VISCOSITY_BLOCK"] + (["VELOCITY_RESULT"] if is_non_ortho else [])
+                                   + (["PRESSURE"] if apply_pressure_gradient else []))
     dt = _dt(time_step)
 
     class SetupAdvectionVelocityFunction(torch.autograd.Function):
@@ -516,8 +521,6 @@ def SetupAdvectionVelocity(domain, time_step, non_ortho_flags, apply_pressure_gr
         def backward(ctx, grad_rhs):
             if not any(ctx.needs_input_grad):
                 return (None,) * len(keys)
-            if apply_pressure_gradient:
-                raise NotImplementedError("SetupAdvectionVelocity: no gradient with apply_pressure_gradient")
             set_domain_tensors_from_flat(domain, keys, ctx.saved)
             domain.UpdateDomainData()
             g = _Grads(domain)
@@ -532,15 +535,44 @@ def SetupAdvectionVelocity(domain, time_step, non_ortho_flags, apply_pressure_gr
             if is_non_ortho:
                 _nonortho_grad(domain, non_ortho_flags, 1, rb, data_bar=Ub, coef_bar=g.nu, vb=g.vb)
             grads = g.to_inputs(keys)
+            if apply_pressure_gradient:
+                # velocityRHS -= dt G p: the adjoint of the corrector's pressure term -G p / A with A = 1 / dt
+                p_bar = _pressure_term_adjoint(domain, rb, torch.full_like(zA, 1.0 / dt))
             for i, key in enumerate(keys):
                 if key[0] == "VELOCITY_RESULT":
                     grads[i] = Ub
+                elif key[0] == "PRESSURE":
+                    grads[i] = p_bar[key[1]]
             return tuple(_apply_exclusions("SetupAdvectionVelocity", keys, grads))
 
     return SetupAdvectionVelocityFunction.apply(*tracked)
 
 
-def _pressure_rhs_backward(domain, dt, keys, h_grad, div_grad, P_grad, want_A, want_C, want_U, flags=0):
+def _pressure_term_adjoint(domain, u_bar, A):
+    """Gradient with respect to the blocks' pressure of -G p / A (G the corrector's finite-difference
+    pressure gradient) for the output gradient u_bar [D][N]: one tensor per block."""
+    lib = _lib.load()
+    N, D = domain.getTotalSize(), domain.getSpatialDims()
+    z = lambda n: torch.zeros(n, dtype=domain.getDtype(), device=domain.getDevice())
+    Ab, pb, hb = z(N), z(N), z(D * N)
+    check(lib.pict_correct_velocity_grad(ctypes.byref(domain._desc), _p(A.contiguous()), _p(z(N)),
+                                         _p(u_bar.contiguous()), _p(Ab), _p(pb), _p(hb), _stream()),
+          "pressure term grad")
+    saved = [b.pressureGrad for b in domain.getBlocks()]
+    for b in domain.getBlocks():
+        b.setPressureGrad(torch.zeros_like(b.pressure))
+    domain.UpdateDomainData()
+    check(lib.pict_copy_field(ctypes.byref(domain._desc), 4, 1, _p(pb), 0, _stream()), "scatter pressure grad")
+    out = [b.pressureGrad.clone() for b in domain.getBlocks()]
+    for b, g in zip(domain.getBlocks(), saved):
+        if isinstance(g, torch.Tensor) and g.is_cuda and g.shape == b.pressure.shape:
+            b.setPressureGrad(g)
+    domain.UpdateDomainData()
+    return out
+
+
+def _pressure_rhs_backward(domain, dt, keys, h_grad, div_grad, P_grad, want_A, want_C, want_U, flags=0,
+                           time_step_norm=False):
     """Shared backward of SetupPressureCorrection / Matrix / RHS / RHSdiv.  With non-orthogonal flags the
     matrix terms add to the A gradient and the explicit RHS terms (read from the pressure result saved by
     the forward pass) to the pressure result and A gradients."""
@@ -556,7 +588,9 @@ def _pressure_rhs_backward(domain, dt, keys, h_grad, div_grad, P_grad, want_A, w
     Pr = g.z(N)
     if div_grad is not None:
         db = div_grad.contiguous()
-        check(lib.pict_divergence_grad(desc, _p(db), _p(hb), _p(g.vb), s), "divergence grad")
+        # timeStepNorm divides the divergence by the time step, not the non-orthogonal terms added after it
+        dbd = (db / dt).contiguous() if time_step_norm else db
+        check(lib.pict_divergence_grad(desc, _p(dbd), _p(hb), _p(g.vb), s), "divergence grad")
         if check_non_ortho_rhs(flags):
             _nonortho_grad(domain, flags, 3, db, data_bar=Pr, coef_bar=Ab)
     if P_grad is not None:
@@ -611,13 +645,13 @@ def SetupPressureCorrection(domain, time_step, non_ortho_flags, use_face_transfo
         def backward(ctx, P_grad, rhs_grad, div_grad):
             if not any(ctx.needs_input_grad):
                 return (None,) * len(keys)
-            if use_face_transform or timeStepNorm:
-                raise NotImplementedError("SetupPressureCorrection: no gradient with face transforms / timeStepNorm")
+            if use_face_transform:
+                raise NotImplementedError("SetupPressureCorrection: no gradient with face transforms")
             set_domain_tensors_from_flat(domain, keys, ctx.saved)
             domain.setPressureRHS(ctx.h)
             domain.UpdateDomainData()
             grads = _pressure_rhs_backward(domain, dt, keys, rhs_grad, div_grad, P_grad, True, True, True,
-                                           non_ortho_flags)
+                                           non_ortho_flags, timeStepNorm)
             return tuple(_apply_exclusions("SetupPressureCorrection", keys, grads))
 
     return SetupPressureCorrectionFunction.apply(*tracked)
@@ -676,13 +710,13 @@ def SetupPressureRHS(domain, time_step, non_ortho_flags, use_face_transform=Fals
         @staticmethod
         @torch.autograd.function.once_differentiable
         def backward(ctx, rhs_grad, div_grad):
-            if use_face_transform or timeStepNorm:
-                raise NotImplementedError("SetupPressureRHS: no gradient with face transforms / timeStepNorm")
+            if use_face_transform:
+                raise NotImplementedError("SetupPressureRHS: no gradient with face transforms")
             set_domain_tensors_from_flat(domain, keys, ctx.saved)
             domain.setPressureRHS(ctx.h)
             domain.UpdateDomainData()
             grads = _pressure_rhs_backward(domain, dt, keys, rhs_grad, div_grad, None, True, True, True,
-                                           non_ortho_flags)
+                                           non_ortho_flags, timeStepNorm)
             return tuple(_apply_exclusions("SetupPressureRHS", keys, grads))
 
     return SetupPressureRHSFunction.apply(*tracked)
@@ -711,14 +745,15 @@ def SetupPressureRHSdiv(domain, time_step, non_ortho_flags, use_face_transform=F
         @staticmethod
         @torch.autograd.function.once_differentiable
         def backward(ctx, div_grad):
-            if use_face_transform or timeStepNorm:
-                raise NotImplementedError("SetupPressureRHSdiv: no gradient with face transforms / timeStepNorm")
+            if use_face_transform:
+                raise NotImplementedError("SetupPressureRHSdiv: no gradient with face transforms")
             set_domain_tensors_from_flat(domain, keys, ctx.saved)
             domain.UpdateDomainData()
             g = _Grads(domain)
             hb = g.z(g.D * g.N)
             db = div_grad.contiguous()
-            check(_lib.load().pict_divergence_grad(ctypes.byref(domain._desc), _p(db), _p(hb),
+            dbd = (db / dt).contiguous() if timeStepNorm else db
+            check(_lib.load().pict_divergence_grad(ctypes.byref(domain._desc), _p(dbd), _p(hb),
                                                    _p(g.vb), _stream()), "divergence grad")
             Pr, Ab = g.z(g.N), g.z(g.N)
             if is_non_ortho:
@@ -762,8 +797,8 @@ def CorrectVelocity(domain, time_step, version, timeStepNorm=False):
         def backward(ctx, u_grad):
             if not any(ctx.needs_input_grad):
                 return (None,) * len(keys)
-            if timeStepNorm or version not in (0, 1, 5, 6):
-                raise NotImplementedError("CorrectVelocity: no gradient for version %d or with timeStepNorm" % version)
+            if version not in (0, 1, 5, 6):
+                raise NotImplementedError("CorrectVelocity: no gradient for version %d" % version)
             set_domain_tensors_from_flat(domain, keys, ctx.saved)
             domain.UpdateDomainData()
             lib = _lib.load()
@@ -772,9 +807,14 @@ def CorrectVelocity(domain, time_step, version, timeStepNorm=False):
             p_glob = z(N)
             check(lib.pict_copy_field(ctypes.byref(domain._desc), 1, 0, _p(p_glob), 0, _stream()), "gather pressure")
             Ab, pb, hb = z(N), z(N), z(D * N)
+            ug = u_grad.contiguous()
+            # timeStepNorm multiplies the pressure update (not pressureRHS) by the time step
+            ug_update = (ug * _dt(time_step)).contiguous() if timeStepNorm else ug
             check(lib.pict_correct_velocity_grad(ctypes.byref(domain._desc), _p(domain.A), _p(p_glob),
-                                                 _p(u_grad.contiguous()), _p(Ab), _p(pb), _p(hb), _stream()),
+                                                 _p(ug_update), _p(Ab), _p(pb), _p(hb), _stream()),
                   "correct velocity grad")
+            if timeStepNorm:
+                hb = ug.clone()
             for b in domain.getBlocks():
                 b.setPressureGrad(torch.zeros_like(b.pressure))
             domain.UpdateDomainData()

@@ -10,12 +10,16 @@ SetupAdvectionVelocity :531-613, CopyVelocityResultToBlocks :697-729, CopyPressu
 :765-800, SetupPressureCorrection :802-895, CorrectVelocity :1160-1236; driver order
 PISOtorch_simulation.py:1170-1312 with the pressure mean removal as a torch op).
 
+Variants: "plain" (the driver's defaults), "tsnorm" (pressure normalised by the time step: timeStepNorm in
+SetupPressureCorrection(Grad) and CorrectVelocity(Grad)) and "pgrad" (applyPressureGradient in
+SetupAdvectionVelocity(Grad), which subtracts dt grad p of the blocks' pressure from the velocity RHS).
+
 Loss: sum(w * u^T) over the blocks' velocity after T steps, w seeded.  Saved per setup: the gradient
 with respect to the initial block velocities, the domain viscosity, block viscosity, block velocity
 source and the boundary velocities of fixed faces.  ``tests/test_gpu_reference_grads.py`` compares the
 adjoint of this build against these fixtures.
 
-Usage (GPU machine):  python tests/golden/make_ref_grad_fixtures.py --out <dir>
+Usage (GPU machine):  python tests/golden/make_ref_grad_fixtures.py --out <dir> [--variants plain,tsnorm,pgrad]
 """
 import argparse
 import os
@@ -34,6 +38,12 @@ DT = 0.05
 T = 2
 TOL = 1e-12
 GRAD_CASES = ["cavity2d", "periodic2d", "inflow2d", "twoblock2d_rotated"]
+VARIANTS = {"plain": dict(ts_norm=False, pgrad=False), "tsnorm": dict(ts_norm=True, pgrad=False),
+            "pgrad": dict(ts_norm=False, pgrad=True)}
+
+
+def fixture_name(variant, name):
+    return "ref_grads_%s.npz" % name if variant == "plain" else "ref_grads_%s_%s.npz" % (variant, name)
 
 
 def solve(R, A, rhs, use_bicg, transpose=False, tol=TOL, maxit=5000):
@@ -60,7 +70,7 @@ def fixed_faces(dom):
     return out
 
 
-def forward_step(R, dom, ts):
+def forward_step(R, dom, ts, ts_norm=False, pgrad=False):
     blocks = dom.getBlocks()
     st = {"vel": [b.velocity for b in blocks]}
     dom.CreateA()
@@ -69,7 +79,7 @@ def forward_step(R, dom, ts):
     R.SetupAdvectionMatrix(dom, ts, 0)
     dom.CreateVelocityRHS()
     dom.UpdateDomainData()
-    R.SetupAdvectionVelocity(dom, ts, 0, False)
+    R.SetupAdvectionVelocity(dom, ts, 0, pgrad)
     st["A"], st["Cval"] = dom.A, dom.C.value
     x = solve(R, dom.C, dom.velocityRHS, True)
     dom.setVelocityResult(x)
@@ -82,7 +92,7 @@ def forward_step(R, dom, ts):
         dom.CreatePressureRHSdiv()
         dom.P.CreateValue()
         dom.UpdateDomainData()
-        R.SetupPressureCorrection(dom, ts, 0, False, timeStepNorm=False)
+        R.SetupPressureCorrection(dom, ts, 0, False, timeStepNorm=ts_norm)
         c["h"], c["Pval"] = dom.pressureRHS, dom.P.value
         p0 = solve(R, dom.P, dom.pressureRHSdiv, False)
         p = p0 - torch.mean(p0)
@@ -93,7 +103,7 @@ def forward_step(R, dom, ts):
         c["p0"], c["pb"] = p0, [b.pressure for b in blocks]
         dom.CreateVelocityResult()
         dom.UpdateDomainData()
-        R.CorrectVelocity(dom, ts, version=1, timeStepNorm=False)
+        R.CorrectVelocity(dom, ts, version=1, timeStepNorm=ts_norm)
         cors.append(c)
     st["cors"] = cors
     dom.CreateVelocityOnBlocks()
@@ -141,7 +151,7 @@ def block_velocity_grads(dom):
     return [b.velocityGrad.clone() for b in dom.getBlocks()]
 
 
-def backward_step(R, dom, ts, st, ubar_blocks, acc):
+def backward_step(R, dom, ts, st, ubar_blocks, acc, ts_norm=False, pgrad=False):
     blocks = dom.getBlocks()
     # CopyVelocityResultToBlocks
     for b, g in zip(blocks, ubar_blocks):
@@ -164,7 +174,7 @@ def backward_step(R, dom, ts, st, ubar_blocks, acc):
         dom.CreatePressureGradOnBlocks()
         dom.CreatePressureRHSGrad()
         dom.UpdateDomainData()
-        R.CorrectVelocityGrad(dom, ts, False)
+        R.CorrectVelocityGrad(dom, ts, ts_norm)
         Abar += dom.AGrad
         pbar_b = [b.pressureGrad.clone() for b in blocks]
         hbar = dom.pressureRHSGrad.clone()
@@ -196,7 +206,7 @@ def backward_step(R, dom, ts, st, ubar_blocks, acc):
         dom.CreateVelocitySourceGradOnBlocks()
         dom.CreateVelocityGradOnBoundaries()
         dom.UpdateDomainData()
-        R.SetupPressureCorrectionGrad(dom, ts, 0, False, False)
+        R.SetupPressureCorrectionGrad(dom, ts, 0, False, ts_norm)
         Abar += dom.AGrad
         Cbar += dom.CGrad.value
         for g, bg in zip(un, block_velocity_grads(dom)):
@@ -221,7 +231,7 @@ def backward_step(R, dom, ts, st, ubar_blocks, acc):
     dom.CreateVelocityGradOnBoundaries()
     dom.CreateVelocitySourceGradOnBlocks()
     dom.UpdateDomainData()
-    R.SetupAdvectionVelocityGrad(dom, ts, 0, False)
+    R.SetupAdvectionVelocityGrad(dom, ts, 0, pgrad)
     for g, bg in zip(un, block_velocity_grads(dom)):
         g += bg
     acc.add(dom)
@@ -239,19 +249,19 @@ def backward_step(R, dom, ts, st, ubar_blocks, acc):
     return un
 
 
-def grad_fixture(R, name):
+def grad_fixture(R, name, ts_norm=False, pgrad=False):
     from setups import build_product, case
     dom = build_product(case(name), torch.float64, module=R)
     ts = torch.tensor([DT], dtype=torch.float64)
     blocks = dom.getBlocks()
     u0 = [b.velocity.clone() for b in blocks]
-    tapes = [forward_step(R, dom, ts) for _ in range(T)]
+    tapes = [forward_step(R, dom, ts, ts_norm, pgrad) for _ in range(T)]
     g = torch.Generator(device="cpu").manual_seed(17)
     w = [torch.randn(b.velocity.shape, generator=g, dtype=torch.float64).cuda() for b in dom.getBlocks()]
     acc = Acc(dom)
     ubar = [x.clone() for x in w]
     for st in reversed(tapes):
-        ubar = backward_step(R, dom, ts, st, ubar, acc)
+        ubar = backward_step(R, dom, ts, st, ubar, acc, ts_norm, pgrad)
     out = {"T": T, "dt": DT, "tol": TOL,
            "u0": np.concatenate([x.cpu().numpy().reshape(-1) for x in u0]),
            "w": np.concatenate([x.cpu().numpy().reshape(-1) for x in w]),
@@ -271,14 +281,16 @@ def grad_fixture(R, name):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", required=True, help="directory the fixtures are written to")
+    ap.add_argument("--variants", default="plain,tsnorm,pgrad", help="comma-separated subset of %s" % list(VARIANTS))
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
     import PISOtorch as R
-    for name in GRAD_CASES:
-        fx = grad_fixture(R, name)
-        np.savez_compressed(os.path.join(args.out, "ref_grads_%s.npz" % name), **fx)
-        print("gradient fixture", name, {k: float(np.abs(v).max()) for k, v in fx.items() if isinstance(v, np.ndarray)},
-              flush=True)
+    for variant in args.variants.split(","):
+        for name in GRAD_CASES:
+            fx = grad_fixture(R, name, **VARIANTS[variant])
+            np.savez_compressed(os.path.join(args.out, fixture_name(variant, name)), **fx)
+            print("gradient fixture", variant, name,
+                  {k: float(np.abs(v).max()) for k, v in fx.items() if isinstance(v, np.ndarray)}, flush=True)
 
 
 if __name__ == "__main__":

@@ -25,15 +25,18 @@ def _rel(a, b):
     return np.abs(a - b).max() / max(np.abs(b).max(), 1e-30)
 
 
+@pytest.mark.parametrize("variant", list(G.VARIANTS))
 @pytest.mark.parametrize("name", G.GRAD_CASES)
-def test_raw_grad_operators_reproduce_reference_gradients(name):
+def test_raw_grad_operators_reproduce_reference_gradients(name, variant):
+    """variant "tsnorm": timeStepNorm in the pressure and corrector operators and their gradients;
+    "pgrad": applyPressureGradient in SetupAdvectionVelocity(Grad)."""
     from pict_b200 import PISOtorch as P
     from setups import case
-    p = os.path.join(GOLDEN, "ref_grads_%s.npz" % name)
+    p = os.path.join(GOLDEN, G.fixture_name(variant, name))
     if not os.path.exists(p):
         pytest.skip("fixture missing")
     fx = np.load(p)
-    out = G.grad_fixture(P, name)
+    out = G.grad_fixture(P, name, **G.VARIANTS[variant])
     static_src = {"grad_source_%d" % k for k, b in enumerate(case(name)["blocks"])
                   if b.get("source") is not None and np.asarray(b["source"]).ndim == 2}
     errs = {}
