@@ -250,6 +250,13 @@ pict_status_t pict_solve(const pict_domain_t* dom, const void* coef, const void*
  * distributed shared memory with one cluster barrier per iteration and no grid-wide barrier; 0 always
  * uses the persistent grid; 2 uses clusters whenever they fit. */
 void pict_krylov_set_cluster_mode(int32_t mode);
+/* BiCGStab kernel (no counterpart in the reference): 0 (default) four grid barriers per iteration for every
+ * solve; 1 two barriers per iteration (NORM2 / NORM2_NORMALIZED criteria, up to two right-hand sides per launch;
+ * the half step forms s on the fly, the full step forms the next search direction on the fly with rho' from the
+ * recurrence rw.r - alpha rw.v - omega rw.t) with one CTA per SM, 2 the same with two CTAs per SM.  All follow
+ * bicgstabSolveGPU's iteration and reports.  Variants 1 and 2 take one more workspace vector per right-hand side
+ * (pict_solve_workspace_bytes follows the current choice). */
+void pict_krylov_set_bicgstab_variant(int32_t variant);
 
 /* pict_solve without a caller-provided workspace (no counterpart in the reference).  For callers
  * that hold no device allocator (a plain C or ctypes binding without torch, or a loop that must not

@@ -73,6 +73,7 @@ struct KArgs {
     T* v0;
     T* v1;
     T* t;
+    T* r1;  // two-barrier BiCGStab: second residual buffer
     int* ctrl;
     double* partials;  // [2][num_tiles][KR_NV]
     pict_solve_info_t* info;
@@ -1237,6 +1238,377 @@ __global__ void __launch_bounds__(KR_THREADS, 2) k_bicgstab(KArgs<T> a) {
 }
 
 // ---------------------------------------------------------------------------------------------
+// BiCGStab with two grid barriers per iteration (NORM2 criteria, up to two right-hand sides per launch).
+//
+// Same iterates, stopping rule and reports as k_bicgstab, in two sweeps per iteration:
+//  * half step: s = r - alpha v formed on the fly (also for the neighbours), t = A s, and the inner
+//    products s.s, t.s, t.t, rw.t; after the barrier the half-step convergence test on |s|, then
+//    omega = t.s / t.t and rho' = rw.r' by the recurrence rw.r - alpha rw.v - omega rw.t, which gives
+//    beta = (rho' / rho)(alpha / omega) before r' exists;
+//  * full step merged with the next search direction: x += alpha p + omega s, r' = s - omega t (into
+//    the other residual buffer: the neighbours still read r), p' = r' + beta (p - omega v) formed on the
+//    fly from r, v, t and p of the neighbours, v' = A p', and the exact |r'|^2, rw.r', rw.v'.  After the
+//    barrier the full-step convergence test on the exact |r'|, and the next alpha uses the exact rho'.
+// The four-barrier kernel stores s and r' between its phases: per iteration and right-hand side this one
+// moves 14 instead of 20 vectors (plus the two stencil passes) and waits at half the barriers.  Systems
+// that converge at the full step spend the search direction of one iteration they do not take.
+// Completions are counted only after the full-step barrier and read at the half-step barrier (a barrier
+// separates every increment from every read, so all CTAs take the same exit).
+// ---------------------------------------------------------------------------------------------
+template <typename T, int D, int NR, bool TRANS, int MINB>
+__global__ void __launch_bounds__(KR_THREADS, MINB) k_bicgstab2(KArgs<T> a) {
+    static_assert(4 * NR <= KR_NV, "two-barrier BiCGStab: at most two right-hand sides per launch");
+    const pict_domain_t& dom = a.dom;
+    const int N = dom.num_cells;
+    const size_t NS = (size_t)N;
+    __shared__ TileSlots S;
+    __shared__ PhaseRed R;
+    __shared__ double s_sum[KR_SLOTS][KR_NV];
+    __shared__ double s_rho[KR_SLOTS][NR], s_rwv[KR_SLOTS][NR], s_alpha[KR_SLOTS][NR], s_omega[KR_SLOTS][NR],
+        s_beta[KR_SLOTS][NR];
+    __shared__ unsigned s_act[KR_SLOTS];   // bit per component still iterating
+    __shared__ unsigned s_half[KR_SLOTS];  // bit per component that stopped at this iteration's half step
+    __shared__ unsigned s_any;             // bit per slot with an iterating or half-step component
+    __shared__ pict_solve_info_t s_info[KR_SLOTS][NR];
+    load_slots(dom, S);
+    __shared__ int s_ctrl[3];
+    unsigned epoch = 0;
+    const T* __restrict__ coef = a.coef;
+    T* __restrict__ x = a.x;
+    const T* __restrict__ rw = a.rw;
+    T* __restrict__ tv = a.t;
+    T* rc = a.r;
+    T* rn = a.r1;
+    T* pc = a.p0;
+    T* pn = a.p1;
+    T* vc = a.v0;
+    T* vn = a.v1;
+    int phase = 0;
+    double* part = a.partials;
+    const size_t pstride = (size_t)dom.num_tiles * KR_NV;
+    const int total = dom.num_sims * NR;
+
+    // ---- init: r = b - A x, rw = r, p = v = 0; r.r and b.b
+    for (int j = 0; j < S.n; ++j) {
+        const pict_block_t& B = dom.blocks[S.block[j]];
+        double acc[2 * NR];
+#pragma unroll
+        for (int k = 0; k < 2 * NR; ++k) acc[k] = 0.0;
+        for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) {
+            int p[3];
+            unflatten(i - B.offset, B.size, p);
+#pragma unroll
+            for (int c = 0; c < NR; ++c) {
+                const T* xc = x + c * NS;
+                const T bi = a.b[c * NS + i];
+                T ri = bi;
+                if (!a.x_zero) ri -= spmv_row<T, D, TRANS>(dom, coef, N, i, B, p, [&](int jj) { return xc[jj]; });
+                rc[c * NS + i] = ri;
+                a.rw[c * NS + i] = ri;
+                pc[c * NS + i] = T(0);
+                vc[c * NS + i] = T(0);
+                acc[c] += (double)ri * (double)ri;
+                acc[NR + c] += (double)bi * (double)bi;
+            }
+        }
+        warp_partial<2 * NR>(R, j, acc);
+    }
+    flush_partials<2 * NR>(R, S, 0xffffffffu, part + phase * pstride);
+    if (!grid_barrier(a.ctrl, epoch, s_ctrl)) return;
+    system_sums<2 * NR>(part + phase * pstride, S, 0xffffffffu, s_sum);
+    phase ^= 1;
+    if (threadIdx.x < 32) {  // lane j: slot j
+        const int j = threadIdx.x;
+        unsigned act = 0;
+        if (j < S.n) {
+            const int n = S.ncell[j];
+            for (int c = 0; c < NR; ++c) {
+                pict_solve_info_t inf = fresh_info();
+                s_rho[j][c] = s_sum[j][c];
+                s_rwv[j][c] = 0.0; s_alpha[j][c] = 0.0; s_omega[j][c] = 0.0; s_beta[j][c] = 0.0;
+                bool fin = false;
+                if (s_sum[j][NR + c] == 0.0) {
+                    inf.converged = 1;
+                    inf.used_iterations = 0;
+                    fin = true;
+                } else {
+                    const double nrmr0 = conv_crit(s_sum[j][c], a.normalized, n);
+                    if (nrmr0 < a.tol) {
+                        inf.converged = 1;
+                        inf.used_iterations = -1;
+                        inf.final_residual = nrmr0;
+                        fin = true;
+                    } else {
+                        act |= 1u << c;
+                    }
+                }
+                if (fin && S.owner[j]) atomicAdd(a.ctrl + CTRL_DONE, 1);
+                s_info[j][c] = inf;
+            }
+            s_act[j] = act;
+            s_half[j] = 0u;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, act != 0);
+        if (j == 0) s_any = m;
+    }
+    __syncthreads();
+    for (int j = 0; j < S.n; ++j) {
+        for (int c = 0; c < NR; ++c) {
+            const bool zero_rhs = s_info[j][c].converged && s_info[j][c].used_iterations == 0;
+            if (a.x_zero || zero_rhs)
+                for (int i = S.start[j] + threadIdx.x; i < S.start[j] + S.count[j]; i += blockDim.x) x[c * NS + i] = T(0);
+        }
+    }
+
+    // ---- first search direction: p = r, v = A r, rw.v
+    for (int j = 0; j < S.n; ++j) {
+        if (!((s_any >> j) & 1u)) continue;
+        const unsigned act = s_act[j];
+        const pict_block_t& B = dom.blocks[S.block[j]];
+        double acc[NR];
+#pragma unroll
+        for (int c = 0; c < NR; ++c) acc[c] = 0.0;
+        const int s0 = S.start[j], cnt = S.count[j];
+        for (int base = 0; base < cnt; base += KR_PASS) {
+            T pv[KR_U][NR], vv[KR_U][NR], wv[KR_U][NR];
+#pragma unroll
+            for (int k = 0; k < KR_U; ++k) {
+                const int i = s0 + min(base + (int)threadIdx.x + k * KR_THREADS, cnt - 1);
+                int p[3];
+                unflatten(i - B.offset, B.size, p);
+#pragma unroll
+                for (int c = 0; c < NR; ++c) {
+                    pv[k][c] = vv[k][c] = wv[k][c] = T(0);
+                    if (!((act >> c) & 1u)) continue;
+                    const T* rcc = rc + c * NS;
+                    pv[k][c] = rcc[i];
+                    vv[k][c] = spmv_row<T, D, TRANS>(dom, coef, N, i, B, p, [&](int jj) { return rcc[jj]; });
+                    wv[k][c] = rw[c * NS + i];
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < KR_U; ++k) {
+                const int l = base + (int)threadIdx.x + k * KR_THREADS;
+                if (l >= cnt) continue;
+                const int i = s0 + l;
+#pragma unroll
+                for (int c = 0; c < NR; ++c) {
+                    if (!((act >> c) & 1u)) continue;
+                    pc[c * NS + i] = pv[k][c];
+                    vc[c * NS + i] = vv[k][c];
+                    acc[c] += (double)wv[k][c] * (double)vv[k][c];
+                }
+            }
+        }
+        warp_partial<NR>(R, j, acc);
+    }
+    flush_partials<NR>(R, S, s_any, part + phase * pstride);
+    if (!grid_barrier(a.ctrl, epoch, s_ctrl)) return;
+    system_sums<NR>(part + phase * pstride, S, s_any, s_sum);
+    phase ^= 1;
+    if ((int)threadIdx.x < S.n) {
+        const int j = threadIdx.x;
+        for (int c = 0; c < NR; ++c)
+            if ((s_act[j] >> c) & 1u) s_rwv[j][c] = s_sum[j][c];
+    }
+    __syncthreads();
+    if (s_ctrl[0] == total) goto done;
+
+    for (int it = 0; it < a.maxit; ++it) {
+        if ((int)threadIdx.x < S.n) {
+            const int j = threadIdx.x;
+            for (int c = 0; c < NR; ++c)
+                if ((s_act[j] >> c) & 1u) s_alpha[j][c] = s_rho[j][c] / s_rwv[j][c];
+        }
+        __syncthreads();
+        // half step: s = r - alpha v on the fly, t = A s; s.s, t.s, t.t, rw.t
+        for (int j = 0; j < S.n; ++j) {
+            if (!((s_any >> j) & 1u)) continue;
+            const unsigned act = s_act[j];
+            const pict_block_t& B = dom.blocks[S.block[j]];
+            double acc[4 * NR];
+#pragma unroll
+            for (int k = 0; k < 4 * NR; ++k) acc[k] = 0.0;
+            const int s0 = S.start[j], cnt = S.count[j];
+            for (int base = 0; base < cnt; base += KR_PASS) {
+                T sv[KR_U][NR], tt[KR_U][NR], wv[KR_U][NR];
+#pragma unroll
+                for (int k = 0; k < KR_U; ++k) {
+                    const int i = s0 + min(base + (int)threadIdx.x + k * KR_THREADS, cnt - 1);
+                    int p[3];
+                    unflatten(i - B.offset, B.size, p);
+#pragma unroll
+                    for (int c = 0; c < NR; ++c) {
+                        sv[k][c] = tt[k][c] = wv[k][c] = T(0);
+                        if (!((act >> c) & 1u)) continue;
+                        const T al = (T)s_alpha[j][c];
+                        const T* rcc = rc + c * NS;
+                        const T* vcc = vc + c * NS;
+                        sv[k][c] = rcc[i] - al * vcc[i];
+                        tt[k][c] = spmv_row<T, D, TRANS>(dom, coef, N, i, B, p,
+                                                         [&](int jj) { return rcc[jj] - al * vcc[jj]; });
+                        wv[k][c] = rw[c * NS + i];
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < KR_U; ++k) {
+                    const int l = base + (int)threadIdx.x + k * KR_THREADS;
+                    if (l >= cnt) continue;
+                    const int i = s0 + l;
+#pragma unroll
+                    for (int c = 0; c < NR; ++c) {
+                        if (!((act >> c) & 1u)) continue;
+                        tv[c * NS + i] = tt[k][c];
+                        const double sd = (double)sv[k][c], td = (double)tt[k][c];
+                        acc[4 * c] += sd * sd;
+                        acc[4 * c + 1] += td * sd;
+                        acc[4 * c + 2] += td * td;
+                        acc[4 * c + 3] += (double)wv[k][c] * td;
+                    }
+                }
+            }
+            warp_partial<4 * NR>(R, j, acc);
+        }
+        flush_partials<4 * NR>(R, S, s_any, part + phase * pstride);
+        if (!grid_barrier(a.ctrl, epoch, s_ctrl)) return;
+        if (s_ctrl[0] == total) break;
+        system_sums<4 * NR>(part + phase * pstride, S, s_any, s_sum);
+        phase ^= 1;
+        if (threadIdx.x < 32) {
+            const int j = threadIdx.x;
+            unsigned act = j < S.n ? s_act[j] : 0u;
+            unsigned half = 0u;
+            if (act) {
+                const int n = S.ncell[j];
+                for (int c = 0; c < NR; ++c) {
+                    if (!((act >> c) & 1u)) continue;
+                    const double ss = s_sum[j][4 * c], ts = s_sum[j][4 * c + 1], tt = s_sum[j][4 * c + 2],
+                                 wt = s_sum[j][4 * c + 3];
+                    const double nr = conv_crit(ss, a.normalized, n);
+                    s_info[j][c].used_iterations = it;
+                    s_info[j][c].final_residual = nr;
+                    bool stop = false;
+                    if (!isfinite(nr)) { s_info[j][c].finite = 0; stop = true; }
+                    else if (nr < a.tol) { s_info[j][c].converged = 1; stop = true; }
+                    if (stop) {
+                        half |= 1u << c;
+                        act &= ~(1u << c);
+                        continue;
+                    }
+                    const double om = ts / tt;
+                    const double rho_next = s_rho[j][c] - s_alpha[j][c] * s_rwv[j][c] - om * wt;
+                    s_omega[j][c] = om;
+                    s_beta[j][c] = (rho_next / s_rho[j][c]) * (s_alpha[j][c] / om);
+                }
+                s_act[j] = act;
+                s_half[j] = half;
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, (act | half) != 0);
+            if (j == 0) s_any = m;
+        }
+        __syncthreads();
+        // full step and next direction: x += alpha p + omega s, r' = s - omega t, p' = r' + beta (p - omega v),
+        // v' = A p'; |r'|^2, rw.r', rw.v'.  Components that stopped at the half step take x += alpha p only.
+        for (int j = 0; j < S.n; ++j) {
+            if (!((s_any >> j) & 1u)) continue;
+            const unsigned act = s_act[j], half = s_half[j];
+            const pict_block_t& B = dom.blocks[S.block[j]];
+            double acc[3 * NR];
+#pragma unroll
+            for (int k = 0; k < 3 * NR; ++k) acc[k] = 0.0;
+            const int s0 = S.start[j], cnt = S.count[j];
+            for (int base = 0; base < cnt; base += KR_PASS) {
+                // own-cell results are stored as they are formed (x, r' and p' are not read at neighbours in
+                // this sweep; r' and p' go to the other buffers), which keeps the register footprint small
+#pragma unroll 1
+                for (int k = 0; k < KR_U; ++k) {
+                    const int l = base + (int)threadIdx.x + k * KR_THREADS;
+                    const bool valid = l < cnt;
+                    const int i = s0 + min(l, cnt - 1);
+                    int p[3];
+                    unflatten(i - B.offset, B.size, p);
+#pragma unroll
+                    for (int c = 0; c < NR; ++c) {
+                        const bool on = (act >> c) & 1u, hf = (half >> c) & 1u;
+                        if (!on && !hf) continue;
+                        const T al = (T)s_alpha[j][c];
+                        const T* rcc = rc + c * NS;
+                        const T* vcc = vc + c * NS;
+                        const T* pcc = pc + c * NS;
+                        T xi = x[c * NS + i] + al * pcc[i];
+                        if (!on) {
+                            if (valid) x[c * NS + i] = xi;
+                            continue;
+                        }
+                        const T om = (T)s_omega[j][c], bt = (T)s_beta[j][c];
+                        const T* tcc = tv + c * NS;
+                        const T si = rcc[i] - al * vcc[i];
+                        xi = xi + om * si;
+                        auto rnew = [&](int jj) { return (rcc[jj] - al * vcc[jj]) - om * tcc[jj]; };
+                        auto pnew = [&](int jj) { return rnew(jj) + bt * (pcc[jj] - om * vcc[jj]); };
+                        const T ri = rnew(i);
+                        const T pi = pnew(i);
+                        const T vi = spmv_row<T, D, TRANS>(dom, coef, N, i, B, p, pnew);
+                        if (!valid) continue;
+                        x[c * NS + i] = xi;
+                        rn[c * NS + i] = ri;
+                        pn[c * NS + i] = pi;
+                        vn[c * NS + i] = vi;
+                        const double rd = (double)ri, wd = (double)rw[c * NS + i];
+                        acc[3 * c] += rd * rd;
+                        acc[3 * c + 1] += wd * rd;
+                        acc[3 * c + 2] += wd * (double)vi;
+                    }
+                }
+            }
+            warp_partial<3 * NR>(R, j, acc);
+        }
+        flush_partials<3 * NR>(R, S, s_any, part + phase * pstride);
+        if (!grid_barrier(a.ctrl, epoch, s_ctrl)) return;
+        system_sums<3 * NR>(part + phase * pstride, S, s_any, s_sum);
+        phase ^= 1;
+        if (threadIdx.x < 32) {
+            const int j = threadIdx.x;
+            unsigned act = j < S.n ? s_act[j] : 0u;
+            unsigned fin = j < S.n ? s_half[j] : 0u;
+            if (act) {
+                const int n = S.ncell[j];
+                for (int c = 0; c < NR; ++c) {
+                    if (!((act >> c) & 1u)) continue;
+                    const double nr = conv_crit(s_sum[j][3 * c], a.normalized, n);
+                    s_info[j][c].final_residual = nr;
+                    if (nr < a.tol) {
+                        s_info[j][c].converged = 1;
+                        s_info[j][c].used_iterations = it + 1;
+                        act &= ~(1u << c);
+                        fin |= 1u << c;
+                    } else {
+                        s_rho[j][c] = s_sum[j][3 * c + 1];
+                        s_rwv[j][c] = s_sum[j][3 * c + 2];
+                    }
+                }
+                s_act[j] = act;
+            }
+            if (j < S.n) {
+                s_half[j] = 0u;
+                if (fin && S.owner[j]) atomicAdd(a.ctrl + CTRL_DONE, __popc(fin));
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, act != 0);
+            if (j == 0) s_any = m;
+        }
+        __syncthreads();
+        T* tr = rc; rc = rn; rn = tr;
+        T* tp = pc; pc = pn; pn = tp;
+        T* tq = vc; vc = vn; vn = tq;
+    }
+done:
+    if ((int)threadIdx.x < S.n && S.owner[threadIdx.x]) {
+        const int j = threadIdx.x;
+        for (int c = 0; c < NR; ++c) a.info[S.sim[j] * a.nrhs + c] = s_info[j][c];
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
 // Cluster CG: the single-reduction recurrence of k_cg1, one thread-block cluster per system.
 //
 // The cluster's first CTA takes the next system from a counter in the workspace (systems are ordered
@@ -1495,14 +1867,28 @@ static size_t vec_bytes(const pict_domain_t* dom, const pict_solve_params_t* prm
     return align256(esz * (size_t)dom->num_cells * nrhs_per_launch(prm));
 }
 
+// BiCGStab kernel choice (pict_krylov_set_bicgstab_variant), see below
+static int g_bicgstab_variant = 0;
+
+// bicg: 7 vectors (8 for the two-barrier kernel: two residual buffers); cg1: 7; cg: r p0 p1 q (+ the best iterate)
+static int workspace_vectors(const pict_solve_params_t* prm) {
+    if (prm->use_bicg) return g_bicgstab_variant != 0 ? 8 : 7;
+    return prm->variant == 1 ? 7 : (prm->return_best_result ? 5 : 4);
+}
+
 static size_t workspace_total(const pict_domain_t* dom, const pict_solve_params_t* prm) {
-    // bicg / cg1: 7 vectors; cg: r p0 p1 q (+ the best iterate)
-    const int nvec = (prm->use_bicg || prm->variant == 1) ? 7 : (prm->return_best_result ? 5 : 4);
-    return header_bytes(dom) + vec_bytes(dom, prm) * nvec;
+    return header_bytes(dom) + vec_bytes(dom, prm) * workspace_vectors(prm);
 }
 
 // 0: persistent grid only; 1: clusters where they apply (default); 2: clusters whenever possible
 static int g_cluster_mode = 1;
+// BiCGStab kernel: 0 (default) the four-barrier form for every solve; 1 the two-barrier form (NORM2
+// criteria, up to two right-hand sides per launch) with one 512-thread CTA per SM and 128 registers per
+// thread, 2 the same with two CTAs per SM (64 registers, some spilled).  Measured on the batch of 256
+// cavities (mixed-precision step): 8.22 ms per step with 0, 9.04 with 1, 8.63 with 2 -- the merged sweep
+// gathers r, v, t and p at every neighbour, which costs more than the two barriers it saves; on single
+// small domains (cylinder street, 64^2 cavity) 1 is 1-3% faster.  The workspace size depends on the choice
+// (pict_solve_workspace_bytes): switch before sizing the workspace.
 
 // Launch k_cg1_cluster with clusters of `cl` CTAs, as many clusters as fit on the device at once (at most
 // one per system).  Returns PICT_ERR_UNSUPPORTED (nothing launched) if no cluster of that size fits.
@@ -1584,8 +1970,8 @@ static pict_status_t run_solve(const pict_domain_t* dom, const void* coef, const
     double* partials = reinterpret_cast<double*>(base + align256(256));
     const size_t off = header_bytes(dom);
     const size_t vb = vec_bytes(dom, prm);
-    const int nvec = (prm->use_bicg || prm->variant == 1) ? 7 : (prm->return_best_result ? 5 : 4);
-    T* vec[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    const int nvec = workspace_vectors(prm);
+    T* vec[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     for (int k = 0; k < nvec; ++k) vec[k] = reinterpret_cast<T*>(base + off + vb * k);
 
     const int nrhs_total = prm->nrhs;
@@ -1618,11 +2004,18 @@ static pict_status_t run_solve(const pict_domain_t* dom, const void* coef, const
         a.abs_crit = prm->convergence >= PICT_CONV_ABS_SUM ? prm->convergence : 0;
         a.rankdef = prm->use_bicg ? 0 : (prm->rank_deficient ? 1 : 0);
         a.info = info + c0;
+        a.r1 = nullptr;
         a.nrhs = nrhs_total;
         void (*kern)(KArgs<T>) = nullptr;
         if (prm->use_bicg) {
             a.r = vec[0]; a.rw = vec[1]; a.p0 = vec[2]; a.p1 = vec[3]; a.v0 = vec[4]; a.v1 = vec[5]; a.t = vec[6];
-            kern = nr == 1 ? k_bicgstab<T, D, 1, TRANS> : (nr == 2 ? k_bicgstab<T, D, 2, TRANS> : k_bicgstab<T, D, 3, TRANS>);
+            a.r1 = vec[7];  // null with the four-barrier kernel (7 vectors)
+            if (g_bicgstab_variant == 1 && a.abs_crit == 0 && nr <= 2)
+                kern = nr == 1 ? k_bicgstab2<T, D, 1, TRANS, 1> : k_bicgstab2<T, D, 2, TRANS, 1>;
+            else if (g_bicgstab_variant == 2 && a.abs_crit == 0 && nr <= 2)
+                kern = nr == 1 ? k_bicgstab2<T, D, 1, TRANS, 2> : k_bicgstab2<T, D, 2, TRANS, 2>;
+            else
+                kern = nr == 1 ? k_bicgstab<T, D, 1, TRANS> : (nr == 2 ? k_bicgstab<T, D, 2, TRANS> : k_bicgstab<T, D, 3, TRANS>);
         } else if (prm->variant == 1 && a.reset == 0 && a.best == 0 && a.abs_crit == 0 && a.rankdef == 0) {
             a.r = vec[0]; a.rw = vec[1]; a.p0 = vec[2]; a.p1 = vec[3]; a.v0 = vec[4]; a.v1 = vec[5]; a.t = vec[6];
             kern = k_cg1<T, D, TRANS>;
@@ -1704,6 +2097,7 @@ extern "C" {
 int64_t pict_solve_static_scratch_bytes(void) { return (int64_t)KR_STATIC_SCRATCH_BYTES; }
 
 void pict_krylov_set_cluster_mode(int32_t mode) { g_cluster_mode = mode < 0 ? 0 : (mode > 2 ? 2 : mode); }
+void pict_krylov_set_bicgstab_variant(int32_t variant) { g_bicgstab_variant = variant < 0 ? 0 : (variant > 2 ? 2 : variant); }
 
 pict_status_t pict_solve_static(const pict_domain_t* dom, const void* coef, const void* rhs, void* x,
                                 const pict_solve_params_t* prm, void* info_out, void* stream) {
