@@ -189,7 +189,7 @@ def build_workload(name, rank=0, dtype=None):
         sides, re = batched_cavity_params(256, rank_seed(rank))
         doms = [make_cavity_domain(int(s), 1.0 / r, dtype) for s, r in zip(sides, re)]
         dts = [0.5 / s for s in sides]
-        return dict(domains=doms, dts=dts, sides=sides, re=re, tol=1e-6, correctors=2, refine_tol=1e-9)
+        return dict(domains=doms, dts=dts, sides=sides, re=re, tol=1e-6, correctors=2, refine_tol=5e-10)
     if name == "lid_cavity_64":
         doms = [make_cavity_domain(64, 1e-3, dtype)]
         return dict(domains=doms, dts=[0.01], sides=np.array([64]), re=np.array([1000.0]), tol=1e-6, correctors=2)
@@ -301,7 +301,8 @@ def precision_kwargs(args, wl=None):
     --warm-advection 0) advection solves from the current velocity; fp32: the single FP32 pressure solve
     from zero (the reference's order)."""
     if args.precision == "mixed":
-        return {"pressure_refine": 1, "refine_tol": (wl or {}).get("refine_tol", 1e-9), "warm_start_pressure": True,
+        rt = getattr(args, "refine_tol", 0.0) or (wl or {}).get("refine_tol", 1e-9)
+        return {"pressure_refine": 1, "refine_tol": rt, "warm_start_pressure": True,
                 "refine_solver": args.refine_solver, "pressure_first_solve": bool(args.first_solve),
                 "mg_iterations": args.mg_iterations, "warm_start_advection": bool(args.warm_advection)}
     return {}
@@ -559,7 +560,7 @@ def run_pict(args, rank, world):
             "config": {"workload": args.workload, "simulations": len(doms), "cells_per_gpu": cells,
                        "pass": "forward", "solver_tol": wl["tol"], "correctors": wl["correctors"],
                        "precision": args.precision + (" (FP32 fields and Krylov vectors, FP64 reductions, one FP64 "
-                                                      "refinement sweep of each pressure solve to %g RMS (multigrid-preconditioned CG corrections on near-isotropic grids, at most %d iterations, each system stopping at the target), warm-started pressure solves" % (wl.get("refine_tol", 1e-9), args.mg_iterations) + (", advection solves from the current velocity" if args.warm_advection else "") + ")"
+                                                      "refinement sweep of each pressure solve to %g RMS (multigrid-preconditioned CG corrections on near-isotropic grids, at most %d iterations, each system stopping at the target), warm-started pressure solves" % (st.refine_tol, st.mg_iterations) + (", advection solves from the current velocity" if args.warm_advection else "") + ")"
                                                       if args.precision == "mixed" else " (FP32, FP64 reductions)"),
                        "cuda_graph": not args.no_graph, "cuda_graph_steps": None if args.no_graph else G,
                        "l2": "working set > L2 (126 MB), no flush",
@@ -1338,9 +1339,11 @@ def main():
     ap.add_argument("--first-solve", type=int, default=0,
                     help="mixed precision: 1 = FP32 CG pressure solve before the refinement, 0 = refine from the "
                          "warm-start pressure")
-    ap.add_argument("--mg-iterations", type=int, default=12,
+    ap.add_argument("--mg-iterations", type=int, default=0,
                     help="cap of the multigrid PCG iterations per correction (each system stops once its RMS residual "
-                         "meets the refinement target)")
+                         "meets the refinement target); 0: 8 where the finest level smooths with two sweeps, else 12")
+    ap.add_argument("--refine-tol", type=float, default=0.0,
+                    help="RMS residual target of the FP64 pressure refinement (0: the workload's)")
     ap.add_argument("--skip-bwd", action="store_true")
     ap.add_argument("--skip-fp32", action="store_true")
     ap.add_argument("--autotune", type=int, default=1, help="1: pick tile size / CTA cap / CG variant by timing")

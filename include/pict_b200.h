@@ -310,7 +310,9 @@ typedef struct pict_mg_level {
     int32_t max_block_cells;   /* cells of the largest block of the level */
     const int32_t* tiles;      /* [num_tiles][4]: system, block, first cell, cell count (device) */
     int32_t max_block_sx;      /* largest x size (cells per row) of a block of the level */
-    int32_t pad0;
+    int32_t sweeps;            /* damped-Jacobi sweeps of each smoothing step at this level when the restriction
+                                  and prolongation tile kernels handle it: 2 where every tile's shared-memory
+                                  stage holds two halo rows (2D, not y-periodic), else 1 (0 reads as 1) */
 } pict_mg_level_t;
 
 /* Process-wide choice of the 2D PCG SpMV kernel (no counterpart in the reference): 1 (default) stages
@@ -318,11 +320,16 @@ typedef struct pict_mg_level {
  * double-buffered across the tiles of a persistent grid) wherever the operands are 16-byte aligned and
  * the stage fits; 0 runs the gather kernel only.  Both give the same per-warp partial sums. */
 void pict_mg_set_bulk_staging(int32_t enable);
+/* Process-wide cap on the smoothing sweeps of the V-cycle (no counterpart in the reference): 2 (default) two
+ * damped-Jacobi sweeps before and after the coarse correction where a level allows it (pict_mg_level_t.sweeps)
+ * and always inside the one-launch sub-cycle; 1 one sweep everywhere. */
+void pict_mg_set_smoothing_sweeps(int32_t sweeps);
 /* Galerkin coarse operator R A P of `fine` into coarse->coef (aggregates of 2^D cells). */
 pict_status_t pict_mg_galerkin(const pict_mg_level_t* fine, const pict_mg_level_t* coarse, void* stream);
 int64_t pict_pcg_mg_workspace_bytes(const pict_domain_t* dom, const pict_mg_level_t* levels, int32_t num_levels);
-/* `iterations` preconditioned CG iterations on levels[0].coef x = rhs from x = 0, V(1,1)-cycle with damped
- * Jacobi (omega), prolongation scaled by prolong_scale, coarse_sweeps Jacobi sweeps on the coarsest
+/* `iterations` preconditioned CG iterations on levels[0].coef x = rhs from x = 0, V-cycle with one or two
+ * damped-Jacobi sweeps (omega) before and after the coarse correction, prolongation scaled by prolong_scale,
+ * coarse_sweeps Jacobi sweeps on the coarsest
  * level; per-system report (final RMS / 2-norm residual of the recursion) in info_out[num_sims]. */
 pict_status_t pict_pcg_mg(const pict_domain_t* dom, const pict_mg_level_t* levels, int32_t num_levels, const void* rhs,
                           void* x, int32_t iterations, double tolerance, int32_t convergence, void* info_out,

@@ -7,9 +7,10 @@
 // strong in (semi-coarsening on stretched grids, full coarsening on isotropic ones; aggregates of up to
 // 2^D cells, ceil(n/2) cells per coarsened axis); the coarse operator is the Galerkin product R A P with
 // piecewise-constant prolongation P and R = P^T, computed on the device from the fine stencil.  The
-// V-cycle uses one damped-Jacobi sweep before and after the coarse correction (symmetric), a fixed
-// number of Jacobi sweeps on the coarsest level and a scaled prolongation (aggregation coarse
-// operators are too stiff by about 2).  The constant mode of the singular (Neumann / periodic) block
+// V-cycle uses two damped-Jacobi sweeps before and after the coarse correction (one on levels whose tiles
+// cannot stage the halo rows of two; the same number before and after, so the preconditioner stays
+// symmetric), a fixed number of Jacobi sweeps on the coarsest level and a scaled prolongation
+// (aggregation coarse operators are too stiff by about 2).  The constant mode of the singular (Neumann / periodic) block
 // operators is removed on the coarsest level and from every preconditioned residual (folded into the
 // inner products and into the search direction, which the SpMV forms on the fly).  The preconditioned
 // CG runs a fixed number of iterations with per-system scalars; every inner product is reduced per warp
@@ -30,6 +31,8 @@ namespace pict {
 
 // 1: 2D PCG SpMV with bulk-copy staging where it applies (default); 0: the gather kernel only
 static int g_mg_bulk = 1;
+// cap on the damped-Jacobi sweeps of each smoothing step: 2 (default) where a level allows it, 1 everywhere
+static int g_mg_sweeps = 2;
 
 // block of a level: first cell, sizes, periodic flags, system, and the coarsening shifts (log2 of the
 // factor, 0 or 1 per axis) from the next finer level
@@ -211,19 +214,21 @@ __device__ __forceinline__ double* mg_warp_part(double* part, int stride) {
     return part + ((size_t)blockIdx.x * MG_NW + (threadIdx.x >> 5)) * stride;
 }
 
-// b_c = R (b - A x0) over the children of each coarse cell.  UPD (finest level): b = r - alpha q is
-// formed on the fly and stored to rn, and x += alpha p (x = alpha p when first) for the children.
+// b_c = R (b - A x_s) over the children of each coarse cell, x_s the pre-smoothed iterate: x0 (nu = 1) or
+// x1 = x0 + w (b - A x0) / diag (nu = 2), both from zero.  UPD (finest level): b = r - alpha q is formed on
+// the fly and stored to rn, and x += alpha p (x = alpha p when first) for the children.
 //
-// 2D tiles whose fine rows (children rows plus one halo row on each side) fit the stage (cap cells) take
-// the staged path: b and x0 of those rows are formed once into shared memory, then each coarse cell
-// sums its children's residuals from there (a y-periodic wrap forms x0 of that neighbour from global).
+// 2D tiles whose fine rows (children rows plus nu halo rows on each side) fit the stage (cap cells) take
+// the staged path: b and diag of those rows go to shared memory once, x_s is formed there, then each coarse
+// cell sums its children's residuals from there (a y-periodic wrap, nu = 1 only, forms x0 of that
+// neighbour from global).  nu = 2 is taken only where every tile of the level fits the stage.
 template <typename T, int D, bool UPD>
 __global__ void __launch_bounds__(MG_TPB, 4) k_mg_restrict(pict_mg_level_t F, pict_mg_level_t C,
                                                            const T* __restrict__ r, const T* __restrict__ q,
                                                            T* __restrict__ rn, T* __restrict__ x,
                                                            const T* __restrict__ p, const double* __restrict__ sc,
                                                            int first, T* __restrict__ bc, T w, int cap,
-                                                           const double* __restrict__ dn) {
+                                                           const double* __restrict__ dn, int nu) {
     extern __shared__ __align__(16) unsigned char mg_stage_raw[];
     const MgTile tl = mg_tile(C.tiles, blockIdx.x);
     if (mg_done(dn, tl.sys)) return;
@@ -236,11 +241,11 @@ __global__ void __launch_bounds__(MG_TPB, 4) k_mg_restrict(pict_mg_level_t F, pi
     int ylo = 0, yhi = -1;
     if (D == 2) {
         const int lc0 = tl.s0 - Bc.off, lc1 = lc0 + tl.cnt - 1;
-        ylo = max(0, ((lc0 / Bc.sx) << Bc.shy) - 1);
-        yhi = min(Bf.sy - 1, ((lc1 / Bc.sx + 1) << Bc.shy));
+        ylo = max(0, ((lc0 / Bc.sx) << Bc.shy) - nu);
+        yhi = min(Bf.sy - 1, ((lc1 / Bc.sx + 1) << Bc.shy) - 1 + nu);
     }
     if (D == 2 && (yhi - ylo + 1) * sx <= cap) {
-        T* s_x0 = reinterpret_cast<T*>(mg_stage_raw);
+        T* s_x0 = reinterpret_cast<T*>(mg_stage_raw);  // x_s: x0 (nu = 1) or x1 (nu = 2)
         T* s_b = s_x0 + cap;
         T* s_d = s_b + cap;
         const int lo = Bf.off + ylo * sx, nh = (yhi - ylo + 1) * sx;
@@ -251,7 +256,7 @@ __global__ void __launch_bounds__(MG_TPB, 4) k_mg_restrict(pict_mg_level_t F, pi
         for (int e = threadIdx.x; e < nh; e += MG_TPB) {
             const int i = lo + e;
             const T bi = rhs(i), di = cf[i];
-            s_x0[e] = mg_x0(di, bi, w);
+            if (nu == 1) s_x0[e] = mg_x0(di, bi, w);
             s_b[e] = bi;
             s_d[e] = di;
             if (UPD) {
@@ -269,6 +274,34 @@ __global__ void __launch_bounds__(MG_TPB, 4) k_mg_restrict(pict_mg_level_t F, pi
             }
         }
         __syncthreads();
+        if (nu == 2) {
+            // x1 = x0 + w (b - A x0) / diag on the stage, x0 = w b / diag formed from the staged b and diag.
+            // Rows of the stage's edge whose outer neighbour row lies outside the stage get a value that no
+            // child reads (children rows are at least one row inside); the block's own edges are fixed faces.
+            auto x0s = [&](int c) { return mg_x0(s_d[c], s_b[c], w); };
+            int ey = (int)threadIdx.x / sx, ex = (int)threadIdx.x - ey * sx;
+            for (int e = threadIdx.x; e < nh; e += MG_TPB) {
+                const int i = lo + e, yg = ylo + ey;
+                const T di = s_d[e], xi = x0s(e);
+                const T xm = ex > 0 ? x0s(e - 1) : x0s(e + sx - 1);
+                const T xp = ex + 1 < sx ? x0s(e + 1) : x0s(e - sx + 1);
+                const bool hm = ey > 0, hp = ey + 1 < nh / sx;
+                const T ym = hm ? x0s(e - sx) : T(0), yp = hp ? x0s(e + sx) : T(0);
+                T ax = di * xi;
+                ax += (ex > 0 || Bf.px) ? cf[(size_t)Nf + i] * xm : T(0);
+                ax += (ex + 1 < sx || Bf.px) ? cf[(size_t)2 * Nf + i] * xp : T(0);
+                ax += (yg > 0 && hm) ? cf[(size_t)3 * Nf + i] * ym : T(0);
+                ax += (yg + 1 < Bf.sy && hp) ? cf[(size_t)4 * Nf + i] * yp : T(0);
+                s_x0[e] = xi + ((di != T(0)) ? mg_div(w * (s_b[e] - ax), di) : T(0));
+                ex += dr;
+                ey += dq;
+                if (ex >= sx) {
+                    ex -= sx;
+                    ++ey;
+                }
+            }
+            __syncthreads();
+        }
         auto far = [&](int xq, int yq) -> T {
             const int j = Bf.off + xq + sx * yq;
             return mg_x0(cf[j], rhs(j), w);
@@ -355,19 +388,24 @@ __global__ void __launch_bounds__(MG_TPB, 4) k_mg_restrict(pict_mg_level_t F, pi
     }
 }
 
-// post-smoothing with the coarse correction: x' = x0 + s P e_c (formed on the fly, also for the
-// neighbours), out = x' + w (b - A x') / diag.  DOT (finest level): per-warp partials of b.out, b.b,
-// sum(out), sum(b).
+// post-smoothing with the coarse correction: x' = x_s + s P e_c (formed on the fly, also for the
+// neighbours), then nu damped-Jacobi sweeps x <- x + w (b - A x) / diag.  x_s is the pre-smoothed iterate
+// of the restriction, recomputed here: x0 = w b / diag (nu = 1) or x1 = x0 + w (b - A x0) / diag (nu = 2).
+// DOT (finest level): per-warp partials of b.out, b.b, sum(out), sum(b).
 //
-// 2D tiles whose rows plus one halo row on each side fit the stage (cap cells) take the staged path:
-// x' of every cell of [first - sx, last + sx] is formed once into shared memory (with b and diag), then
-// the stencil reads its neighbours there; a y-periodic wrap reaches outside the stage and forms x' of
-// that neighbour from global memory.
+// 2D tiles take a staged path where their rows plus the halo rows fit the stage.
+// nu = 1 (cap cells per array): x' of every cell of [first - sx, last + sx] is formed once into shared memory (with b and diag),
+// then the stencil reads its neighbours there; a y-periodic wrap reaches outside the stage and forms x'
+// of that neighbour from global memory.  nu = 2: b and diag of [first - 3 sx, last + 3 sx] are staged,
+// x1 (the pre-smoothed iterate) of [first - 2 sx, last + 2 sx], then the first post sweep of
+// [first - sx, last + sx] (x' formed from x1 and e_c on the fly), then the second sweep of the tile's
+// cells, in four arrays of 3 cap / 4 cells; taken only where every tile of the level fits (no y-periodic
+// wrap).
 template <typename T, int D, bool DOT>
 __global__ void __launch_bounds__(MG_TPB, 4) k_mg_prolong(pict_mg_level_t F, pict_mg_level_t C, const int32_t* tiles,
                                                           const T* __restrict__ bv, const T* __restrict__ ec,
                                                           T* __restrict__ out, T s, T w, double* __restrict__ part,
-                                                          int cap, const double* __restrict__ dn) {
+                                                          int cap, const double* __restrict__ dn, int nu) {
     extern __shared__ __align__(16) unsigned char mg_stage_raw[];
     const MgTile tl = mg_tile(tiles, blockIdx.x);
     if (mg_done(dn, tl.sys)) return;
@@ -376,7 +414,91 @@ __global__ void __launch_bounds__(MG_TPB, 4) k_mg_prolong(pict_mg_level_t F, pic
     const int N = F.num_cells;
     double a = 0.0, c2 = 0.0, sz = 0.0, sr = 0.0;
     const int sx = Bf.sx;
-    if (D == 2 && tl.cnt + 2 * sx <= cap) {
+    const int cap4 = (3 * cap) / 4;  // four arrays in the shared memory of three of `cap` cells
+    if (D == 2 && nu == 2 && tl.cnt + 6 * sx <= cap4) {
+        T* s_x = reinterpret_cast<T*>(mg_stage_raw);
+        T* s_b = s_x + cap4;
+        T* s_d = s_b + cap4;
+        T* s_y = s_d + cap4;  // x1
+        const int nf = sx * Bf.sy;
+        const int lo = max(Bf.off, tl.s0 - 3 * sx), hi = min(Bf.off + nf, tl.s0 + tl.cnt + 3 * sx);
+        for (int e = threadIdx.x; e < hi - lo; e += MG_TPB) {
+            s_b[e] = bv[lo + e];
+            s_d[e] = cf[lo + e];
+        }
+        __syncthreads();
+        // one damped-Jacobi sweep over the global cells [g0, g1) of a stage-resident iterate given by xin(c)
+        // (c: stage index); neighbours outside the block are fixed faces (no y-periodic wrap on this path)
+        auto sweep = [&](int g0, int g1, auto&& xin, T* dst) {
+            const int dq = MG_TPB / sx, dr = MG_TPB - dq * sx;
+            int l = g0 - Bf.off + (int)threadIdx.x;
+            int y = l / sx, x = l - y * sx;
+            for (int i = g0 + (int)threadIdx.x; i < g1; i += MG_TPB) {
+                const int c = i - lo;
+                const T di = s_d[c], xi = xin(c);
+                const T xm = x > 0 ? xin(c - 1) : xin(c + sx - 1);
+                const T xp = x + 1 < sx ? xin(c + 1) : xin(c - sx + 1);
+                const T ym = y > 0 ? xin(c - sx) : T(0);
+                const T yp = y + 1 < Bf.sy ? xin(c + sx) : T(0);
+                T acc = di * xi;
+                acc += (x > 0 || Bf.px) ? cf[(size_t)N + i] * xm : T(0);
+                acc += (x + 1 < sx || Bf.px) ? cf[(size_t)2 * N + i] * xp : T(0);
+                acc += y > 0 ? cf[(size_t)3 * N + i] * ym : T(0);
+                acc += y + 1 < Bf.sy ? cf[(size_t)4 * N + i] * yp : T(0);
+                dst[c] = xi + ((di != T(0)) ? mg_div(w * (s_b[c] - acc), di) : T(0));
+                x += dr;
+                y += dq;
+                if (x >= sx) {
+                    x -= sx;
+                    ++y;
+                }
+            }
+        };
+        const int a1 = max(Bf.off, tl.s0 - 2 * sx), b1 = min(Bf.off + nf, tl.s0 + tl.cnt + 2 * sx);
+        const int a2 = max(Bf.off, tl.s0 - sx), b2 = min(Bf.off + nf, tl.s0 + tl.cnt + sx);
+        // x1 = x0 + w (b - A x0) / diag, x0 = w b / diag
+        sweep(a1, b1, [&](int c) { return mg_x0(s_d[c], s_b[c], w); }, s_y);
+        __syncthreads();
+        // x' = x1 + s P e_c; first post sweep into s_x
+        auto xprime = [&](int c) {
+            const int l = c + lo - Bf.off;
+            const int y = l / sx, x = l - y * sx;
+            return s_y[c] + s * ec[Bc.off + (x >> Bc.shx) + Bc.sx * (y >> Bc.shy)];
+        };
+        sweep(a2, b2, xprime, s_x);
+        __syncthreads();
+        // second post sweep of the tile's cells
+        const int dq = MG_TPB / sx, dr = MG_TPB - dq * sx;
+        int l = tl.s0 - Bf.off + (int)threadIdx.x;
+        int y = l / sx, x = l - y * sx;
+        for (int k = threadIdx.x; k < tl.cnt; k += MG_TPB) {
+            const int i = tl.s0 + k, c = i - lo;
+            const T xi = s_x[c], di = s_d[c], bi = s_b[c];
+            const T xm = x > 0 ? s_x[c - 1] : s_x[c + sx - 1];
+            const T xp = x + 1 < sx ? s_x[c + 1] : s_x[c - sx + 1];
+            const T ym = y > 0 ? s_x[c - sx] : T(0);
+            const T yp = y + 1 < Bf.sy ? s_x[c + sx] : T(0);
+            T acc = di * xi;
+            acc += (x > 0 || Bf.px) ? cf[(size_t)N + i] * xm : T(0);
+            acc += (x + 1 < sx || Bf.px) ? cf[(size_t)2 * N + i] * xp : T(0);
+            acc += y > 0 ? cf[(size_t)3 * N + i] * ym : T(0);
+            acc += y + 1 < Bf.sy ? cf[(size_t)4 * N + i] * yp : T(0);
+            const T zi = xi + ((di != T(0)) ? mg_div(w * (bi - acc), di) : T(0));
+            out[i] = zi;
+            if (DOT) {
+                a += (double)bi * (double)zi;
+                c2 += (double)bi * (double)bi;
+                sz += (double)zi;
+                sr += (double)bi;
+            }
+            x += dr;
+            y += dq;
+            if (x >= sx) {
+                x -= sx;
+                ++y;
+            }
+        }
+    } else if (D == 2 && tl.cnt + 2 * sx <= cap) {
         T* s_x = reinterpret_cast<T*>(mg_stage_raw);
         T* s_b = s_x + cap;
         T* s_d = s_b + cap;
@@ -493,8 +615,8 @@ __global__ void __launch_bounds__(MG_TPB, 4) k_mg_prolong(pict_mg_level_t F, pic
 
 // ---------------------------------------------------------------------------------------------
 // The V-cycle below a size cutoff in one launch: one CTA per block runs the levels lv[0..n-1] of its
-// block (restriction down to the coarsest, `sweeps` damped-Jacobi sweeps from zero and mean removal on
-// the coarsest, prolongation and post-smoothing up) with every level's right-hand side, iterate and
+// block (nu pre-smoothing sweeps from zero and restriction down to the coarsest, `sweeps` damped-Jacobi
+// sweeps from zero and mean removal on the coarsest, prolongation and nu post-smoothing sweeps up) with every level's right-hand side, iterate and
 // stencil in shared memory (the stencils are loaded once, at the start).  bin: right-hand side of lv[0]
 // (global), xout: its iterate.
 // ---------------------------------------------------------------------------------------------
@@ -518,10 +640,28 @@ static size_t mg_sub_smem(const pict_mg_level_t* lv, int n, size_t esz) {
     return c * esz;
 }
 
+// one damped-Jacobi sweep of a sub-cycle level in shared memory: xd = xs + w (b - A xs) / diag
+template <typename T, int D>
+__device__ __forceinline__ void mg_sub_sweep(const MgBlock& B, int n, const T* sc, const T* sb, const T* xs, T* xd,
+                                             T w) {
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+        int x, y, z;
+        mg_unflatten(B, e, x, y, z);
+        T acc = sc[e] * xs[e];
+#pragma unroll
+        for (int f = 0; f < 2 * D; ++f) {
+            const int j = mg_nbr(B, x, y, z, f);
+            if (j >= 0) acc += sc[(f + 1) * n + e] * xs[j - B.off];
+        }
+        const T d = sc[e];
+        xd[e] = xs[e] + ((d != T(0)) ? mg_div(w * (sb[e] - acc), d) : T(0));
+    }
+}
+
 template <typename T, int D>
 __global__ void __launch_bounds__(MG_SUB_THREADS) k_mg_subcycle(MgSub S, const T* __restrict__ bin,
                                                                 T* __restrict__ xout, T w, T sp, int sweeps,
-                                                                const double* __restrict__ dn) {
+                                                                const double* __restrict__ dn, int nu) {
     constexpr int K = 2 * D + 1;
     extern __shared__ __align__(16) unsigned char mg_sub_raw[];
     T* sm = reinterpret_cast<T*>(mg_sub_raw);
@@ -564,6 +704,12 @@ __global__ void __launch_bounds__(MG_SUB_THREADS) k_mg_subcycle(MgSub S, const T
         T* sbc = sm + s_off[k + 1];
         for (int e = threadIdx.x; e < nf; e += blockDim.x) sx[e] = mg_x0(sc[e], sb[e], w);
         __syncthreads();
+        if (nu == 2) {  // second pre-smoothing sweep (through the scratch vector)
+            mg_sub_sweep<T, D>(Bf, nf, sc, sb, sx, scr, w);
+            __syncthreads();
+            for (int e = threadIdx.x; e < nf; e += blockDim.x) sx[e] = scr[e];
+            __syncthreads();
+        }
         for (int E = threadIdx.x; E < nc; E += blockDim.x) {
             int X, Y, Z;
             mg_unflatten(Bc, E, X, Y, Z);
@@ -645,19 +791,14 @@ __global__ void __launch_bounds__(MG_SUB_THREADS) k_mg_subcycle(MgSub S, const T
             scr[e] = sx[e] + sp * sxc[(x >> Bc.shx) + Bc.sx * ((y >> Bc.shy) + Bc.sy * (z >> Bc.shz))];
         }
         __syncthreads();
-        for (int e = threadIdx.x; e < nf; e += blockDim.x) {
-            int x, y, z;
-            mg_unflatten(Bf, e, x, y, z);
-            T acc = sc[e] * scr[e];
-#pragma unroll
-            for (int f = 0; f < 2 * D; ++f) {
-                const int j = mg_nbr(Bf, x, y, z, f);
-                if (j >= 0) acc += sc[(f + 1) * nf + e] * scr[j - Bf.off];
-            }
-            const T d = sc[e];
-            sx[e] = scr[e] + ((d != T(0)) ? mg_div(w * (sb[e] - acc), d) : T(0));
-        }
+        mg_sub_sweep<T, D>(Bf, nf, sc, sb, scr, sx, w);
         __syncthreads();
+        if (nu == 2) {  // second post-smoothing sweep
+            mg_sub_sweep<T, D>(Bf, nf, sc, sb, sx, scr, w);
+            __syncthreads();
+            for (int e = threadIdx.x; e < nf; e += blockDim.x) sx[e] = scr[e];
+            __syncthreads();
+        }
     }
     {
         const MgBlock B = mg_block(S.lv[0], b);
@@ -1146,6 +1287,14 @@ static pict_status_t run_pcg_mg(const pict_domain_t* dom, const pict_mg_level_t*
         if (e != cudaSuccess) return set_error(PICT_ERR_CUDA, "pcg_mg: stage shared memory");
     }
 
+    // smoothing sweeps per level of the tile kernels: the level's own choice (every tile's stage holds the
+    // halo rows of two sweeps) capped by the process-wide setting; level 0 also needs the domain's tiles to
+    // fit the four-array stage of the two-sweep prolongation.  The one-launch sub-cycle takes the setting.
+    int nu[16];
+    for (int l = 0; l < nl; ++l) nu[l] = (D == 2 && g_mg_sweeps >= 2 && levels[l].sweeps >= 2) ? 2 : 1;
+    if (nu[0] == 2 && dom->tile_cells + 6 * levels[0].max_block_sx > (3 * cap) / 4) nu[0] = 1;
+    const int nu_sub = g_mg_sweeps >= 2 ? 2 : 1;
+
     // z = M r_new (V-cycle) and the per-warp partials of r_new.z, |r_new|^2, sum(z), sum(r_new).  upd:
     // the finest restriction first forms r_new = r - alpha q (stored to rn) and x += alpha p.
     auto vcycle = [&](const T* r, bool upd, T* rn, const T* p, int first) -> pict_status_t {
@@ -1153,7 +1302,7 @@ static pict_status_t run_pcg_mg(const pict_domain_t* dom, const pict_mg_level_t*
         if (lc == 0) {
             if (upd) k_pcg_update<T><<<nt, MG_TPB, 0, st>>>(*dom, r, q, rn, xout, p, sc, first, part);
             k_mg_subcycle<T, D><<<levels[0].num_blocks, MG_SUB_THREADS, sub_smem, st>>>(sub, rnew, z, wj, sp,
-                                                                                     coarse_sweeps, sc);
+                                                                                     coarse_sweeps, sc, nu_sub);
             k_pcg_dot4<T><<<nt, MG_TPB, 0, st>>>(*dom, rnew, z, part, sc);
             return check_launch("pcg_mg vcycle");
         }
@@ -1162,19 +1311,20 @@ static pict_status_t run_pcg_mg(const pict_domain_t* dom, const pict_mg_level_t*
             const pict_mg_level_t& C = levels[l + 1];
             if (l == 0 && upd)
                 k_mg_restrict<T, D, true><<<C.num_tiles, MG_TPB, stage3, st>>>(F, C, r, q, rn, xout, p, sc, first,
-                                                                                lb[1], wj, cap, sc);
+                                                                                lb[1], wj, cap, sc, nu[0]);
             else
                 k_mg_restrict<T, D, false><<<C.num_tiles, MG_TPB, stage3, st>>>(
-                    F, C, l == 0 ? r : lb[l], nullptr, nullptr, nullptr, nullptr, nullptr, 0, lb[l + 1], wj, cap, sc);
+                    F, C, l == 0 ? r : lb[l], nullptr, nullptr, nullptr, nullptr, nullptr, 0, lb[l + 1], wj, cap, sc,
+                    nu[l]);
         }
         // levels lc.. in one launch (one CTA per block)
         k_mg_subcycle<T, D><<<levels[lc].num_blocks, MG_SUB_THREADS, sub_smem, st>>>(sub, lb[lc], lx[lc], wj, sp,
-                                                                                  coarse_sweeps, sc);
+                                                                                  coarse_sweeps, sc, nu_sub);
         for (int l = lc - 1; l >= 1; --l)
             k_mg_prolong<T, D, false><<<levels[l].num_tiles, MG_TPB, stage3, st>>>(
-                levels[l], levels[l + 1], levels[l].tiles, lb[l], lx[l + 1], lx[l], sp, wj, nullptr, cap, sc);
+                levels[l], levels[l + 1], levels[l].tiles, lb[l], lx[l + 1], lx[l], sp, wj, nullptr, cap, sc, nu[l]);
         k_mg_prolong<T, D, true><<<nt, MG_TPB, stage3, st>>>(levels[0], levels[1], dom->tiles, rnew, lx[1], z, sp, wj,
-                                                             part, cap, sc);
+                                                             part, cap, sc, nu[0]);
         return check_launch("pcg_mg vcycle");
     };
 
@@ -1239,6 +1389,7 @@ using namespace pict;
 extern "C" {
 
 void pict_mg_set_bulk_staging(int32_t enable) { g_mg_bulk = enable ? 1 : 0; }
+void pict_mg_set_smoothing_sweeps(int32_t sweeps) { g_mg_sweeps = sweeps >= 2 ? 2 : 1; }
 
 pict_status_t pict_mg_galerkin(const pict_mg_level_t* fine, const pict_mg_level_t* coarse, void* stream) {
     if (!fine || !coarse || !fine->coef || !coarse->coef || !fine->blocks || !coarse->blocks || !coarse->cell_block)

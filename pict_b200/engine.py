@@ -49,7 +49,7 @@ class PISOStepper:
                  pressure_tol: Optional[float] = None, max_iterations: int = 5000, adv_group_size: int = 0,
                  p_group_size: int = 0, threads: int = 0, normalize_pressure: bool = True, cg_variant: int = 1,
                  pressure_refine: int = 0, refine_tol: Optional[float] = None, warm_start_pressure: bool = False,
-                 refine_solver: str = "cg", mg_iterations: int = 12, pressure_first_solve: bool = True,
+                 refine_solver: str = "cg", mg_iterations: int = 0, pressure_first_solve: bool = True,
                  warm_start_advection: bool = False, outflow=None, outflow_velocity=None,
                  outflow_tol: Optional[float] = None):
         self.domain = domain
@@ -150,6 +150,14 @@ class PISOStepper:
                             raise ValueError("strongly anisotropic grid")
                     self._mg = hierarchy_for(d)
                     self._mg_ws = torch.empty(self._mg.workspace_bytes(self.desc), dtype=torch.uint8, device=dev)
+                    if self.mg_iterations <= 0:
+                        # cap of the PCG iterations (each system stops at the target): a correction takes at
+                        # most ~5 with two smoothing sweeps on the finest level, ~9 with one
+                        from .multigrid import STAGE_CELLS
+                        L0 = self._mg.levels[0]
+                        two = int(L0.sweeps) >= 2 and \
+                            int(self.desc.tile_cells) + 6 * int(L0.max_block_sx) <= (3 * STAGE_CELLS) // 4
+                        self.mg_iterations = 8 if two else 12
                 except ValueError as e:
                     if self.refine_solver == "mg":
                         warnings.warn("multigrid refinement not available (%s); using CG" % e)

@@ -20,6 +20,7 @@ from ._lib import MgLevel, check
 
 MAX_LEVELS = 16
 TILE_CELLS = 512           # cells per work tile of the coarse levels
+STAGE_CELLS = 4096         # cells per array of the shared-memory stage of the 2D restriction / prolongation
 SUB_MAX_CELLS = 2048       # the V-cycle runs in one CTA per block from the first level whose blocks have at
 SUB_MAX_SMEM = 160 * 1024  # most this many cells and whose sub-cycle fits this much shared memory
 
@@ -53,6 +54,31 @@ def axis_strengths(domain) -> np.ndarray:
         alpha = det[:, None] * (minv ** 2).sum(dim=2)
         out[k, :D] = alpha.mean(dim=0).cpu().numpy()
     return out
+
+
+def two_sweep_fits(fine_sizes, fine_per, coarse_offs, coarse_sizes, coarse_shifts, coarse_tiles, fine_tiles,
+                   dims: int) -> bool:
+    """True if the tile kernels can smooth level l with two Jacobi sweeps: 2D, no y-periodic block, every
+    coarse tile's fine rows plus two halo rows on each side fit the restriction's stage, and every tile of
+    level l plus three halo rows on each side fits the four-array stage of the prolongation (fine_tiles None:
+    the domain's tiles, checked at launch)."""
+    if dims != 2 or bool(fine_per[:, 1].any()):
+        return False
+    t = coarse_tiles.reshape(-1, 4)
+    for sim, b, s0, cnt in t:
+        sxc = int(coarse_sizes[b, 0])
+        lc0 = int(s0) - int(coarse_offs[b])
+        lc1 = lc0 + int(cnt) - 1
+        shy = int(coarse_shifts[b, 1])
+        ylo = max(0, ((lc0 // sxc) << shy) - 2)
+        yhi = min(int(fine_sizes[b, 1]) - 1, ((lc1 // sxc + 1) << shy) + 1)
+        if (yhi - ylo + 1) * int(fine_sizes[b, 0]) > STAGE_CELLS:
+            return False
+    if fine_tiles is not None:
+        for sim, b, s0, cnt in fine_tiles.reshape(-1, 4):
+            if int(cnt) + 6 * int(fine_sizes[b, 0]) > (3 * STAGE_CELLS) // 4:
+                return False
+    return True
 
 
 def level_tiles(offs, counts, sims, tile: int = TILE_CELLS) -> np.ndarray:
@@ -92,6 +118,7 @@ class MGHierarchy:
         self.levels_py = []   # keep tensors alive
         self.shifts = []
         levels = []
+        host_geo = []         # per level: sizes, periodic flags, offsets, shifts, tiles (host copies)
         for lvl in range(MAX_LEVELS):
             n = sizes.prod(axis=1)
             offs = np.concatenate([[0], np.cumsum(n)[:-1]])
@@ -126,6 +153,8 @@ class MGHierarchy:
             levels.append(L)
             self.levels_py.append((blocks_t, cb, coef, tiles_t))
             self.shifts.append(shifts.copy())
+            host_geo.append((sizes.copy(), per.copy(), offs.copy(), shifts.copy(),
+                             level_tiles(offs, n, sims) if lvl > 0 else None))
             if (sizes[:, :dims] <= min_size).all():
                 break
             # choose the axes to halve per block
@@ -142,6 +171,11 @@ class MGHierarchy:
             sizes = np.where(shifts == 1, (sizes + 1) // 2, sizes)
         if int(sizes[:, :dims].prod(axis=1).max()) > 256:
             raise ValueError("multigrid not applicable: coarsest blocks too large")
+        for l in range(len(levels) - 1):
+            fs, fp, _, _, ft = host_geo[l]
+            cs, _, co, csh, ct = host_geo[l + 1]
+            levels[l].sweeps = 2 if two_sweep_fits(fs, fp, co, cs, csh, ct, ft, dims) else 1
+        levels[-1].sweeps = 1
         self.num_levels = len(levels)
         self.levels = (MgLevel * self.num_levels)(*levels)
         self.cells = [int(L.num_cells) for L in levels]

@@ -243,3 +243,41 @@ def test_bulk_staged_spmv_equals_gather_kernel(dtype, tile, layout):
     assert diff < (1e-5 if dtype == torch.float32 else 1e-12)
     for a, c in zip(ig, ib):
         assert abs(a.finalResidual - c.finalResidual) <= 1e-3 * abs(a.finalResidual) + 1e-30
+
+
+@pytest.mark.parametrize("sides", [(64, 48, 100, 37), (256, 181, 90)])
+def test_two_sweep_smoothing_needs_fewer_iterations(sides):
+    """Two damped-Jacobi sweeps per smoothing step (the default where the tiles' stages allow it) keep the
+    preconditioner symmetric and reach a 1e-6 residual reduction in fewer PCG iterations than one sweep."""
+    from pict_b200 import PISOtorch as P
+    from pict_b200 import _lib
+    from pict_b200.multigrid import hierarchy_for
+    lib = _lib.load()
+    b, st = _prepared_batch(torch.float32, sides=sides)
+    mg = hierarchy_for(b)
+    assert mg.levels[0].sweeps == 2
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    mg.setup(b.P.coef, s)
+    g = torch.Generator(device="cpu").manual_seed(5)
+    rhs = torch.randn(b.getTotalSize(), generator=g).cuda()
+    sc = b._sim_cells.cpu().numpy()
+    for k in range(len(sc) - 1):
+        rhs[sc[k]:sc[k + 1]] -= rhs[sc[k]:sc[k + 1]].mean()
+    r0 = [float(rhs[sc[k]:sc[k + 1]].double().norm()) / np.sqrt(sc[k + 1] - sc[k]) for k in range(len(sc) - 1)]
+    tol = 1e-6 * min(r0)
+    used = {}
+    try:
+        for nu in (1, 2):
+            lib.pict_mg_set_smoothing_sweeps(nu)
+            x = torch.zeros_like(rhs)
+            info = torch.zeros(b.num_sims * 24, dtype=torch.uint8, device="cuda")
+            ws = torch.empty(mg.workspace_bytes(b._desc), dtype=torch.uint8, device="cuda")
+            mg.solve(b._desc, rhs, x, 40, tol, info, ws, s)
+            infos = P.decode_infos(info)
+            torch.cuda.synchronize()
+            assert all(i.converged and i.isFiniteResidual for i in infos), infos
+            used[nu] = [i.usedIterations for i in infos]
+    finally:
+        lib.pict_mg_set_smoothing_sweeps(2)
+    assert all(a <= c for a, c in zip(used[2], used[1])), used
+    assert max(used[2]) < max(used[1]), used

@@ -127,3 +127,25 @@ def test_bicg_preconditioner_switch():
     finally:
         P.SetBiCGPreconditioner(prev)
     assert P.GetBiCGPreconditioner() == B.AS_REFERENCE
+
+
+def test_two_sweep_stage_fit():
+    """Host check of the multigrid levels that take two smoothing sweeps: 2D, not y-periodic, every tile's
+    stage (rows plus two halo rows; the prolongation's three) within the shared-memory stage."""
+    import numpy as np
+    from pict_b200.multigrid import level_tiles, two_sweep_fits
+
+    def case(nx, ny, per_y=0, dims=2, tile=512):
+        fine = np.array([[nx, ny, 1]])
+        coarse = np.array([[(nx + 1) // 2, (ny + 1) // 2, 1]])
+        per = np.array([[0, per_y, 0]])
+        sh = np.array([[1, 1, 0]])
+        ct = level_tiles([0], [coarse[0, 0] * coarse[0, 1]], [0], tile)
+        ft = level_tiles([0], [nx * ny], [0], tile)
+        return two_sweep_fits(fine, per, np.array([0]), coarse, sh, ct, ft, dims)
+
+    assert case(256, 256)
+    assert case(181, 200)
+    assert not case(256, 256, per_y=1)
+    assert not case(256, 256, dims=3)
+    assert not case(1024, 64)
