@@ -324,6 +324,11 @@ void pict_mg_set_bulk_staging(int32_t enable);
  * damped-Jacobi sweeps before and after the coarse correction where a level allows it (pict_mg_level_t.sweeps)
  * and always inside the one-launch sub-cycle; 1 one sweep everywhere. */
 void pict_mg_set_smoothing_sweeps(int32_t sweeps);
+/* Process-wide choice (no counterpart in the reference): 1 (default) when pict_pcg_mg is called on a stream
+ * under capture, the PCG iterations after the first are captured as the body (two iterations) of a conditional
+ * WHILE node that ends once every system has met the tolerance or the cap is reached, so a replay launches only
+ * the iterations the systems need; 0 captures the fixed sequence of `iterations` iterations. */
+void pict_mg_set_graph_loop(int32_t enable);
 /* Galerkin coarse operator R A P of `fine` into coarse->coef (aggregates of 2^D cells). */
 pict_status_t pict_mg_galerkin(const pict_mg_level_t* fine, const pict_mg_level_t* coarse, void* stream);
 int64_t pict_pcg_mg_workspace_bytes(const pict_domain_t* dom, const pict_mg_level_t* levels, int32_t num_levels);

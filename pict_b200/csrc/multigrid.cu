@@ -33,6 +33,11 @@ namespace pict {
 static int g_mg_bulk = 1;
 // cap on the damped-Jacobi sweeps of each smoothing step: 2 (default) where a level allows it, 1 everywhere
 static int g_mg_sweeps = 2;
+// 1 (default): under stream capture the PCG iterations after the first become a conditional WHILE node of the
+// graph that stops once every system has converged; 0: the fixed launch sequence of `iterations` iterations
+static int g_mg_graph_loop = 1;
+// per device: the stream the loop body is captured on (created outside capture, on the first solve)
+static cudaStream_t g_mg_body_stream[64];
 
 // block of a level: first cell, sizes, periodic flags, system, and the coarsening shifts (log2 of the
 // factor, 0 or 1 per axis) from the next finer level
@@ -1079,9 +1084,11 @@ __global__ void __launch_bounds__(MG_TPB) k_pcg_dot4(pict_domain_t dom, const T*
 // stage 2: rho' = r.(z - m), beta = rho'/rho, rho = rho', |r|^2, m
 // The preconditioned residual z is used mean-free (z - m): the constant mode of a singular system is
 // undetermined.  sc[s*MG_SC + {0: rho, 1: alpha, 2: beta, 3: |r|^2, 4: m}]
+// it: the PCG iteration; inside a graph's conditional loop it is an offset to the device counter ctr
 template <int STRIDE>
 __global__ void k_pcg_scalars(pict_domain_t dom, const double* __restrict__ part, int stage, double* sc, int it,
-                              double tol, int normalized) {
+                              double tol, int normalized, const int* __restrict__ ctr) {
+    if (ctr) it += *ctr;
     const int lane = threadIdx.x & 31;
     const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (s >= dom.num_sims) return;
@@ -1183,6 +1190,24 @@ __global__ void k_pcg_report(pict_domain_t dom, const double* sc, pict_solve_inf
     info[s] = inf;
 }
 
+// Condition of the graph's PCG loop (one CTA): ctr = init (init > 0) or ctr += step, then keep looping
+// while a system is still iterating and the next two iterations (ctr, ctr + 1) are within the cap.
+__global__ void k_pcg_loop_cond(pict_domain_t dom, const double* __restrict__ sc, int* ctr, int init, int step,
+                                int limit, cudaGraphConditionalHandle h) {
+    __shared__ int s_any;
+    if (threadIdx.x == 0) s_any = 0;
+    __syncthreads();
+    int any = 0;
+    for (int s = threadIdx.x; s < dom.num_sims; s += blockDim.x) any |= sc[MG_SC * s + 5] == 0.0;
+    if (__syncthreads_or(any) && threadIdx.x == 0) s_any = 1;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int c = init > 0 ? init : *ctr + step;
+        *ctr = c;
+        cudaGraphSetConditional(h, (s_any && c + 2 <= limit) ? 1u : 0u);
+    }
+}
+
 // workspace: levels >= 1: b, x | finest: r (two, alternating), z, p (two, alternating), q | per-warp
 // partials | scalars.  Returns the bytes; fills the pointers when ws != nullptr.
 struct MgWork {
@@ -1219,7 +1244,7 @@ static size_t mg_carve(const pict_domain_t* dom, const pict_mg_level_t* levels, 
     w->q = take(vb(N));
     w->part = reinterpret_cast<double*>(take(((size_t)4 * MG_NW * dom->num_tiles * 8 + 255) & ~(size_t)255));
     w->sc = reinterpret_cast<double*>(take(((size_t)MG_SC * dom->num_sims * 8 + 255) & ~(size_t)255));
-    w->err = reinterpret_cast<int*>(take(256));
+    w->err = reinterpret_cast<int*>(take(256));  // [0] stage-wait error, [1] iteration counter of the graph loop
     return o;
 }
 
@@ -1297,7 +1322,7 @@ static pict_status_t run_pcg_mg(const pict_domain_t* dom, const pict_mg_level_t*
 
     // z = M r_new (V-cycle) and the per-warp partials of r_new.z, |r_new|^2, sum(z), sum(r_new).  upd:
     // the finest restriction first forms r_new = r - alpha q (stored to rn) and x += alpha p.
-    auto vcycle = [&](const T* r, bool upd, T* rn, const T* p, int first) -> pict_status_t {
+    auto vcycle = [&](const T* r, bool upd, T* rn, const T* p, int first, cudaStream_t st) -> pict_status_t {
         const T* rnew = upd ? rn : r;
         if (lc == 0) {
             if (upd) k_pcg_update<T><<<nt, MG_TPB, 0, st>>>(*dom, r, q, rn, xout, p, sc, first, part);
@@ -1354,29 +1379,93 @@ static pict_status_t run_pcg_mg(const pict_domain_t* dom, const pict_mg_level_t*
     if (cudaMemsetAsync(err, 0, sizeof(int), st) != cudaSuccess || cudaMemsetAsync(xout, 0, sizeof(T) * N, st) != cudaSuccess ||
         cudaMemsetAsync(sc, 0, sizeof(double) * MG_SC * dom->num_sims, st) != cudaSuccess)
         return check_launch("pcg_mg initial state");
-    pict_status_t s = vcycle(rhs, false, nullptr, nullptr, 0);
+    pict_status_t s = vcycle(rhs, false, nullptr, nullptr, 0, st);
     if (s) return s;
-    k_pcg_scalars<4><<<swg, 128, 0, st>>>(*dom, part, 0, sc, 0, tol, normalized);
-    const T* r = rhs;
-    for (int it = 0; it < iterations; ++it) {
-        T* pnew = pbuf[it & 1];
-        const T* pold = it ? pbuf[(it + 1) & 1] : z;
-        T* rn = rbuf[it & 1];
+    k_pcg_scalars<4><<<swg, 128, 0, st>>>(*dom, part, 0, sc, 0, tol, normalized, nullptr);
+    // one PCG iteration; it >= 0: iteration `it` with its buffers and reports fixed at launch (the last one
+    // only updates); it < 0: an iteration of the graph loop with buffer parity `par`, its number read from the
+    // device counter plus `off`
+    int* ctr = err + 1;
+    auto iteration = [&](int it, int par, int off, cudaStream_t st) -> pict_status_t {
+        const bool fixed = it >= 0;
+        const int first = it == 0;
+        T* pnew = pbuf[par];
+        const T* pold = first ? z : pbuf[par ^ 1];
+        T* rn = rbuf[par];
+        const T* r = first ? rhs : rbuf[par ^ 1];
+        const int* c = fixed ? nullptr : ctr;
+        const int itv = fixed ? it : off;
         if (bulk_grid > 0)
-            k_pcg_spmv_dot_bulk<T><<<bulk_grid, MG_TPB, bulk_smem, st>>>(*dom, levels[0], z, pold, pnew, q, sc, it == 0,
+            k_pcg_spmv_dot_bulk<T><<<bulk_grid, MG_TPB, bulk_smem, st>>>(*dom, levels[0], z, pold, pnew, q, sc, first,
                                                                          part, cap_h, cap_t, err);
         else
-            k_pcg_spmv_dot<T, D><<<nt, MG_TPB, 0, st>>>(*dom, levels[0], z, pold, pnew, q, sc, it == 0, part);
-        k_pcg_scalars<1><<<swg, 128, 0, st>>>(*dom, part, 1, sc, it, tol, normalized);
-        if (it + 1 < iterations) {
-            s = vcycle(r, true, rn, pnew, it == 0);
-            if (s) return s;
+            k_pcg_spmv_dot<T, D><<<nt, MG_TPB, 0, st>>>(*dom, levels[0], z, pold, pnew, q, sc, first, part);
+        k_pcg_scalars<1><<<swg, 128, 0, st>>>(*dom, part, 1, sc, itv, tol, normalized, c);
+        if (!fixed || it + 1 < iterations) {
+            pict_status_t e = vcycle(r, true, rn, pnew, first, st);
+            if (e) return e;
         } else {
             // last iteration: only the update and |r|^2 (r.z and sum(z) are not used)
-            k_pcg_update<T><<<nt, MG_TPB, 0, st>>>(*dom, r, q, rn, xout, pnew, sc, it == 0, part);
+            k_pcg_update<T><<<nt, MG_TPB, 0, st>>>(*dom, r, q, rn, xout, pnew, sc, first, part);
         }
-        k_pcg_scalars<4><<<swg, 128, 0, st>>>(*dom, part, 2, sc, it, tol, normalized);
-        r = rn;
+        k_pcg_scalars<4><<<swg, 128, 0, st>>>(*dom, part, 2, sc, itv, tol, normalized, c);
+        return check_launch("pcg_mg iteration");
+    };
+    // under stream capture: iteration 0, then iterations (1, 2), (3, 4), ... as the body of a conditional
+    // WHILE node that ends once every system has converged, then (cap even) the last iteration
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) return check_launch("pcg_mg capture status");
+    if (cs == cudaStreamCaptureStatusNone && dev < 64 && !g_mg_body_stream[dev])
+        if (cudaStreamCreateWithFlags(&g_mg_body_stream[dev], cudaStreamNonBlocking) != cudaSuccess) {
+            cudaGetLastError();
+            g_mg_body_stream[dev] = nullptr;
+        }
+    const bool loop = g_mg_graph_loop && cs == cudaStreamCaptureStatusActive && iterations >= 3 && dev < 64 &&
+                      g_mg_body_stream[dev];
+    if (!loop) {
+        for (int it = 0; it < iterations; ++it)
+            if ((s = iteration(it, it & 1, 0, st))) return s;
+    } else {
+        if ((s = iteration(0, 0, 0, st))) return s;
+        cudaGraph_t graph = nullptr;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t ndeps = 0;
+        cudaGraphConditionalHandle h;
+        if (cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps) != cudaSuccess ||
+            cudaGraphConditionalHandleCreate(&h, graph, 0, 0) != cudaSuccess)
+            return check_launch("pcg_mg conditional handle");
+        k_pcg_loop_cond<<<1, 256, 0, st>>>(*dom, sc, ctr, 1, 0, iterations, h);
+        if ((s = check_launch("pcg_mg loop condition"))) return s;
+        if (cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps) != cudaSuccess)
+            return check_launch("pcg_mg capture info");
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        if (cudaGraphAddNode(&node, graph, deps, ndeps, &cp) != cudaSuccess)
+            return check_launch("pcg_mg conditional node");
+        cudaStream_t bs = g_mg_body_stream[dev];
+        if (cudaStreamBeginCaptureToGraph(bs, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeRelaxed) != cudaSuccess)
+            return check_launch("pcg_mg loop body capture");
+        pict_status_t sb = iteration(-1, 1, 0, bs);
+        if (!sb) sb = iteration(-1, 0, 1, bs);
+        if (!sb) {
+            k_pcg_loop_cond<<<1, 256, 0, bs>>>(*dom, sc, ctr, 0, 2, iterations, h);
+            sb = check_launch("pcg_mg loop condition");
+        }
+        cudaGraph_t body = nullptr;
+        const cudaError_t ee = cudaStreamEndCapture(bs, &body);
+        if (sb) return sb;
+        if (ee != cudaSuccess) return check_launch("pcg_mg loop body end capture");
+        if (cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies) != cudaSuccess)
+            return check_launch("pcg_mg capture dependencies");
+        if ((iterations - 1) % 2 == 1)
+            if ((s = iteration(iterations - 1, (iterations - 1) & 1, 0, st))) return s;
     }
     k_pcg_report<<<sg, 128, 0, st>>>(*dom, sc, info, iterations, tol, normalized, err);
     return check_launch("pcg_mg");
@@ -1390,6 +1479,7 @@ extern "C" {
 
 void pict_mg_set_bulk_staging(int32_t enable) { g_mg_bulk = enable ? 1 : 0; }
 void pict_mg_set_smoothing_sweeps(int32_t sweeps) { g_mg_sweeps = sweeps >= 2 ? 2 : 1; }
+void pict_mg_set_graph_loop(int32_t enable) { g_mg_graph_loop = enable ? 1 : 0; }
 
 pict_status_t pict_mg_galerkin(const pict_mg_level_t* fine, const pict_mg_level_t* coarse, void* stream) {
     if (!fine || !coarse || !fine->coef || !coarse->coef || !fine->blocks || !coarse->blocks || !coarse->cell_block)

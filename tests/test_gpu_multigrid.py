@@ -281,3 +281,38 @@ def test_two_sweep_smoothing_needs_fewer_iterations(sides):
         lib.pict_mg_set_smoothing_sweeps(2)
     assert all(a <= c for a, c in zip(used[2], used[1])), used
     assert max(used[2]) < max(used[1]), used
+
+
+def test_graph_loop_equals_fixed_iterations():
+    """A captured mixed-precision step whose multigrid PCG loop is a conditional WHILE node (stopping once every
+    system has converged) gives the same fields and reports as the captured fixed iteration sequence."""
+    import bench
+    from pict_b200 import _lib
+    from pict_b200.batch import BatchDomain
+    from pict_b200.engine import PISOStepper
+    lib = _lib.load()
+    out = []
+    try:
+        for loop in (0, 1):
+            lib.pict_mg_set_graph_loop(loop)
+            doms = [bench.make_cavity_domain(n, 1e-3, torch.float32) for n in (96, 64, 40, 33)]
+            b = BatchDomain(doms, time_steps=[0.5 / n for n in (96, 64, 40, 33)])
+            st = PISOStepper(b, time_step=0.01, advection_tol=1e-6, pressure_tol=1e-6, pressure_refine=1,
+                             refine_tol=5e-10, warm_start_pressure=True, refine_solver="mg",
+                             pressure_first_solve=False)
+            assert st._mg is not None
+            for _ in range(2):
+                st.step()
+            st.capture(steps=3)
+            for _ in range(2):
+                st.replay()
+            torch.cuda.synchronize()
+            st.check()
+            rep = [[(i.usedIterations, i.finalResidual) for i in r] for row in st.refine_infos() for r in row]
+            out.append(([torch.cat([d.getBlock(0).velocity.reshape(-1), d.getBlock(0).pressure.reshape(-1)])
+                         for d in doms], rep))
+    finally:
+        lib.pict_mg_set_graph_loop(1)
+    for a, c in zip(out[0][0], out[1][0]):
+        assert torch.equal(a, c)
+    assert out[0][1] == out[1][1]
