@@ -189,7 +189,7 @@ def build_workload(name, rank=0, dtype=None):
         sides, re = batched_cavity_params(256, rank_seed(rank))
         doms = [make_cavity_domain(int(s), 1.0 / r, dtype) for s, r in zip(sides, re)]
         dts = [0.5 / s for s in sides]
-        return dict(domains=doms, dts=dts, sides=sides, re=re, tol=1e-6, correctors=2, refine_tol=5e-10)
+        return dict(domains=doms, dts=dts, sides=sides, re=re, tol=1e-6, correctors=2, refine_tol=5e-10, adv_tol=5e-7)
     if name == "lid_cavity_64":
         doms = [make_cavity_domain(64, 1e-3, dtype)]
         return dict(domains=doms, dts=[0.01], sides=np.array([64]), re=np.array([1000.0]), tol=1e-6, correctors=2)
@@ -213,16 +213,27 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.lines = []
+        self.m = 0
 
-    def start(self):
+    def start(self, wait=5.0):
+        """Start sampling every 50 ms and wait (up to `wait` s) for the first sample, so that the timed region
+        that follows is covered."""
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < wait:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
+        self.m = len(self.lines)
+
+    def need(self, k=2):
+        """True while fewer than k samples were read since the timed region started."""
+        return self.proc is not None and len(self.lines) - self.m < k
 
     def _read(self):
         for line in self.proc.stdout:
@@ -238,7 +249,7 @@ class ClockSampler:
             self.proc.kill()
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in self.lines[self.m:]:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
                 continue
@@ -252,6 +263,16 @@ class ClockSampler:
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
                 "samples": len(sm)}
+
+
+def keep_busy(sampler, work, limit_s=3.0):
+    """After a timed region shorter than the sampling interval: repeat untimed `work` (the same steps) until
+    two clock samples under load were read, so the clocks reported are those of the loaded GPU."""
+    import torch
+    t0 = time.time()
+    while sampler.need(2) and time.time() - t0 < limit_s:
+        work()
+        torch.cuda.synchronize()
 
 
 # ------------------------------------------------------------------------------------------ helpers
@@ -304,8 +325,19 @@ def precision_kwargs(args, wl=None):
         rt = getattr(args, "refine_tol", 0.0) or (wl or {}).get("refine_tol", 1e-9)
         return {"pressure_refine": 1, "refine_tol": rt, "warm_start_pressure": True,
                 "refine_solver": args.refine_solver, "pressure_first_solve": bool(args.first_solve),
-                "mg_iterations": args.mg_iterations, "warm_start_advection": bool(args.warm_advection)}
+                "mg_iterations": args.mg_iterations,
+                "warm_start_advection": "increment" if args.warm_advection == 2 else bool(args.warm_advection)}
     return {}
+
+
+def adv_tol(args, wl):
+    """RMS residual target of the advection solves: --adv-tol, else (mixed precision) the workload's adv_tol,
+    else its solver tolerance."""
+    if getattr(args, "adv_tol", 0.0):
+        return args.adv_tol
+    if args.precision == "mixed" and wl.get("adv_tol"):
+        return wl["adv_tol"]
+    return wl["tol"]
 
 
 def rank_seed(rank):
@@ -430,7 +462,7 @@ def run_pict(args, rank, world):
     doms = wl["domains"]
     batch = BatchDomain(doms, time_steps=wl["dts"])
     batch.pack_state()  # block fields as views of two contiguous tensors: one host copy per field
-    kw = dict(time_step=float(wl["dts"][0]), corrector_steps=wl["correctors"], advection_tol=wl["tol"],
+    kw = dict(time_step=float(wl["dts"][0]), corrector_steps=wl["correctors"], advection_tol=adv_tol(args, wl),
               pressure_tol=wl["tol"], max_iterations=5000, **precision_kwargs(args, wl))
     tuned = None
     if args.autotune:
@@ -488,6 +520,7 @@ def run_pict(args, rank, world):
     e1.record()
     torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
+    keep_busy(sampler, lambda: run_steps(G))
     if world > 1:
         dist.barrier()
     clocks = sampler.stop()
@@ -558,9 +591,10 @@ def run_pict(args, rank, world):
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": args.workload, "simulations": len(doms), "cells_per_gpu": cells,
-                       "pass": "forward", "solver_tol": wl["tol"], "correctors": wl["correctors"],
+                       "pass": "forward", "solver_tol": wl["tol"], "advection_tol": st.adv_tol,
+                       "correctors": wl["correctors"],
                        "precision": args.precision + (" (FP32 fields and Krylov vectors, FP64 reductions, one FP64 "
-                                                      "refinement sweep of each pressure solve to %g RMS (multigrid-preconditioned CG corrections on near-isotropic grids, at most %d iterations, each system stopping at the target), warm-started pressure solves" % (st.refine_tol, st.mg_iterations) + (", advection solves from the current velocity" if args.warm_advection else "") + ")"
+                                                      "refinement sweep of each pressure solve to %g RMS (multigrid-preconditioned CG corrections on near-isotropic grids, at most %d iterations, each system stopping at the target), warm-started pressure solves" % (st.refine_tol, st.mg_iterations) + (", advection solves from the current velocity plus the previous step's advection increment" if args.warm_advection == 2 else (", advection solves from the current velocity" if args.warm_advection else "")) + ")"
                                                       if args.precision == "mixed" else " (FP32, FP64 reductions)"),
                        "cuda_graph": not args.no_graph, "cuda_graph_steps": None if args.no_graph else G,
                        "l2": "working set > L2 (126 MB), no flush",
@@ -694,6 +728,7 @@ def run_street(args, rank, world):
     run_steps(args.steps)
     e1.record()
     torch.cuda.synchronize()
+    keep_busy(sampler, lambda: run_steps(G))
     if world > 1:
         dist.barrier()
     clocks = sampler.stop()
@@ -1240,7 +1275,8 @@ def accuracy_check(wl, args, steps=10):
     doms = [make_cavity_domain(int(wl["sides"][i]), 1.0 / wl["re"][i], torch.float32) for i in picks]
     dts = [wl["dts"][i] for i in picks]
     b = BatchDomain(doms, time_steps=dts)
-    st = PISOStepper(b, time_step=dts[0], advection_tol=wl["tol"], pressure_tol=wl["tol"], **precision_kwargs(args, wl))
+    st = PISOStepper(b, time_step=dts[0], advection_tol=adv_tol(args, wl), pressure_tol=wl["tol"],
+                     **precision_kwargs(args, wl))
     for _ in range(steps):
         st.step()
     st.check()
@@ -1325,8 +1361,9 @@ def main():
     ap.add_argument("--impl", default="pict", choices=["pict", "reference"])
     ap.add_argument("--extras", action="store_true",
                     help="only time the operators around the step (scalar, SGS, multi-block convolution); own JSON line")
-    ap.add_argument("--warm-advection", type=int, default=1,
-                    help="mixed precision: start each advection solve from the current velocity (1) or from zero (0)")
+    ap.add_argument("--warm-advection", type=int, default=2,
+                    help="mixed precision: start each advection solve from the current velocity (1), from it plus "
+                         "the previous step's advection increment (2), or from zero (0)")
     ap.add_argument("--workload", default="batched_cavities_256",
                     choices=["batched_cavities_256", "lid_cavity_64", "channel3d_192", "cylinder_street"])
     ap.add_argument("--group-size", type=int, default=0)
@@ -1342,6 +1379,8 @@ def main():
     ap.add_argument("--mg-iterations", type=int, default=0,
                     help="cap of the multigrid PCG iterations per correction (each system stops once its RMS residual "
                          "meets the refinement target); 0: 8 where the finest level smooths with two sweeps, else 12")
+    ap.add_argument("--adv-tol", type=float, default=0.0,
+                    help="RMS residual target of the advection solves (0: the workload's)")
     ap.add_argument("--refine-tol", type=float, default=0.0,
                     help="RMS residual target of the FP64 pressure refinement (0: the workload's)")
     ap.add_argument("--skip-bwd", action="store_true")

@@ -228,6 +228,11 @@ pict_status_t pict_correct_velocity(const pict_domain_t* dom, double dt, int32_t
 /* Copy{Velocity,Pressure}Result{To,From}Blocks (extensions/PISOtorch.cpp:561-566 -> extensions/PISO_multiblock_cuda_kernel.cu:6543-6733). */
 pict_status_t pict_copy_velocity_result_to_blocks(const pict_domain_t* dom, void* stream);
 pict_status_t pict_copy_velocity_result_from_blocks(const pict_domain_t* dom, void* stream);
+/* Initial guess of the advection solve (no counterpart in the reference, whose driver can start the solve from
+ * the previous result, PISOtorch_simulation.py advect_use_prev_result): after_solve = 0 sets
+ * velocityResult = block velocity + increment; after_solve = 1 stores increment = velocityResult - block
+ * velocity (the step's advection increment, the next step's guess).  increment: [D][N], zero on the first step. */
+pict_status_t pict_advection_guess(const pict_domain_t* dom, void* increment, int32_t after_solve, void* stream);
 pict_status_t pict_copy_pressure_result_to_blocks(const pict_domain_t* dom, void* stream);
 pict_status_t pict_copy_pressure_result_from_blocks(const pict_domain_t* dom, void* stream);
 /* ComputeVelocityDivergence (extensions/PISOtorch.cpp:556 -> extensions/PISO_multiblock_cuda_kernel.cu:6333): div of the blocks' velocity, out [N]. */

@@ -180,6 +180,7 @@ SIGNATURES = {
     "pict_correct_velocity": (c_i32, [_PD, ctypes.c_double, c_i32, c_i32, c_i32, c_vp]),
     "pict_copy_velocity_result_to_blocks": (c_i32, [_PD, c_vp]),
     "pict_copy_velocity_result_from_blocks": (c_i32, [_PD, c_vp]),
+    "pict_advection_guess": (c_i32, [_PD, c_vp, c_i32, c_vp]),
     "pict_copy_pressure_result_to_blocks": (c_i32, [_PD, c_vp]),
     "pict_copy_pressure_result_from_blocks": (c_i32, [_PD, c_vp]),
     "pict_velocity_divergence": (c_i32, [_PD, c_vp, c_vp]),

@@ -449,6 +449,26 @@ __global__ void k_copy_result(pict_domain_t dom, int D) {
     }
 }
 
+// Initial guess of the advection solve from the previous step's increment: velocityResult = u + incr
+// (SUB = false), or after the solve incr = velocityResult - u (SUB = true), u the blocks' velocity
+template <typename T, bool SUB>
+__global__ void k_advection_increment(pict_domain_t dom, int D, T* __restrict__ incr) {
+    const int N = dom.num_cells;
+    T* g = reinterpret_cast<T*>(dom.velocity_result);
+    PICT_CELL_LOOP(i, N) {
+        const pict_block_t& B = dom.blocks[dom.cell_block[i]];
+        const int l = i - B.offset;
+        const int nc = B.size[0] * B.size[1] * B.size[2];
+        const T* bf = reinterpret_cast<const T*>(B.velocity);
+        for (int c = 0; c < D; ++c) {
+            const T u = bf[(size_t)c * nc + l];
+            const size_t k = (size_t)c * N + i;
+            if (SUB) incr[k] = g[k] - u;
+            else g[k] = u + incr[k];
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------------------------
 // transforms from vertex coordinates (extensions/grid_gen.cu:284-339 and 383-466)
 // ---------------------------------------------------------------------------------------------
@@ -817,6 +837,14 @@ static pict_status_t launch_correct(const pict_domain_t* dom, double dt, int ver
 }
 
 template <typename T, int D>
+static pict_status_t launch_increment(const pict_domain_t* dom, int sub, void* incr, cudaStream_t st) {
+    const int grid = cell_grid(dom->num_cells, 256);
+    if (sub) k_advection_increment<T, true><<<grid, 256, 0, st>>>(*dom, D, reinterpret_cast<T*>(incr));
+    else k_advection_increment<T, false><<<grid, 256, 0, st>>>(*dom, D, reinterpret_cast<T*>(incr));
+    return check_launch("advection increment");
+}
+
+template <typename T, int D>
 static pict_status_t launch_copy(const pict_domain_t* dom, int which, cudaStream_t st) {
     const int grid = cell_grid(dom->num_cells, 256);
     switch (which) {
@@ -876,6 +904,12 @@ pict_status_t pict_copy_velocity_result_to_blocks(const pict_domain_t* dom, void
     pict_status_t s = check_dom(dom);
     if (s) return s;
     PICT_DISPATCH(dom, launch_copy, dom, 0, (cudaStream_t)stream);
+}
+pict_status_t pict_advection_guess(const pict_domain_t* dom, void* increment, int32_t after_solve, void* stream) {
+    pict_status_t s = check_dom(dom);
+    if (s) return s;
+    if (!increment) return set_error(PICT_ERR_ARG, "advection_guess: NULL increment");
+    PICT_DISPATCH(dom, launch_increment, dom, after_solve ? 1 : 0, increment, (cudaStream_t)stream);
 }
 pict_status_t pict_copy_velocity_result_from_blocks(const pict_domain_t* dom, void* stream) {
     pict_status_t s = check_dom(dom);

@@ -62,8 +62,12 @@ class PISOStepper:
         self.normalize_pressure = normalize_pressure
         self.time_step = time_step
         # warm start of the advection solve from the blocks' velocity (advect_use_prev_result of
-        # PISOtorch_simulation.py:1189): the same solution to the tolerance, fewer BiCGStab iterations
+        # PISOtorch_simulation.py:1189): the same solution to the tolerance, fewer BiCGStab iterations.
+        # "increment": from the blocks' velocity plus the previous step's advection increment u* - u (the
+        # increment changes slowly; on viscous-dominated cavities 8-9 instead of 11-12 iterations)
+        self.advection_increment = warm_start_advection == "increment"
         self.warm_start_advection = bool(warm_start_advection)
+        self._adv_incr = None
         self.adv_params = P._solve_params(self.dims, self.max_iterations, self.adv_tol, _lib.PICT_CONV_NORM2_NORMALIZED,
                                           True, False, x_zero=not self.warm_start_advection, group_size=adv_group_size,
                                           threads=threads)
@@ -197,11 +201,11 @@ class PISOStepper:
         D = self.dims
         self._outflow(desc, dt, st)
         check(lib.pict_setup_advection(desc, dt, st), "advection setup")
-        if self.warm_start_advection:
-            check(lib.pict_copy_velocity_result_from_blocks(desc, st), "advection initial guess")
+        self._advection_guess(desc, st)
         check(lib.pict_solve(desc, P._ptr(d.C.coef), P._ptr(d.velocityRHS), P._ptr(d.velocityResult),
                              ctypes.byref(self.adv_params), P._ptr(self.info_adv), P._ptr(self.ws), self.ws_bytes, st),
               "advection solve")
+        self._advection_increment(desc, st)
         for k in range(self.corrector_steps):
             if k == 0:
                 check(lib.pict_setup_pressure_correction(desc, dt, 0, 0, st), "pressure setup")
@@ -212,6 +216,19 @@ class PISOStepper:
             check(lib.pict_correct_velocity(desc, dt, 1, 0, 1 if last else 0, st), "velocity correction")
         if self.corrector_steps == 0:
             check(lib.pict_copy_velocity_result_to_blocks(desc, st), "copy velocity")
+
+    def _advection_guess(self, desc, st):
+        if self.advection_increment:
+            if self._adv_incr is None:
+                d = self.domain
+                self._adv_incr = torch.zeros(self.dims * d.getTotalSize(), dtype=d.getDtype(), device=d.getDevice())
+            check(self.lib.pict_advection_guess(desc, P._ptr(self._adv_incr), 0, st), "advection initial guess")
+        elif self.warm_start_advection:
+            check(self.lib.pict_copy_velocity_result_from_blocks(desc, st), "advection initial guess")
+
+    def _advection_increment(self, desc, st):
+        if self.advection_increment:
+            check(self.lib.pict_advection_guess(desc, P._ptr(self._adv_incr), 1, st), "advection increment")
 
     def _outflow(self, desc, dt, st):
         if self.outflow:
@@ -251,7 +268,8 @@ class PISOStepper:
         finish-info 3; per corrector pressure setup 2 (matrix/RHS, divergence), correction 1, and the
         refinement sweeps when enabled; the copy of the initial guess of a warm-started advection solve 1;
         the advective outflow update 1."""
-        n = 1 + 3 + (1 if self.warm_start_advection else 0) + (1 if self.outflow else 0)
+        n = 1 + 3 + (1 if self.warm_start_advection else 0) + (1 if self.advection_increment else 0) + \
+            (1 if self.outflow else 0)
         n += self.corrector_steps * (2 + (3 if self.pressure_first_solve else 0) + 1)
         if self.pressure_refine > 0:  # per sweep: residual (+2 projection), solve, update; partials + finish
             if self._mg is not None:
@@ -291,13 +309,13 @@ class PISOStepper:
             return e
 
         check(lib.pict_setup_advection(desc, dt, st), "advection setup")
-        if self.warm_start_advection:
-            check(lib.pict_copy_velocity_result_from_blocks(desc, st), "advection initial guess")
+        self._advection_guess(desc, st)
         a = ev()
         check(lib.pict_solve(desc, P._ptr(d.C.coef), P._ptr(d.velocityRHS), P._ptr(d.velocityResult),
                              ctypes.byref(self.adv_params), P._ptr(self.info_adv), P._ptr(self.ws), self.ws_bytes, st),
               "advection solve")
         b = ev()
+        self._advection_increment(desc, st)
         out["bicg"].append((a, b, self.info_adv.clone()))
         for k in range(self.corrector_steps):
             if k == 0:
@@ -355,6 +373,7 @@ class PISOStepper:
         d = self.domain
         saved = [(b.velocity.clone(), b.pressure.clone()) for b in d.getBlocks()]
         saved_out = [d.getBlock(b).getBoundary(f).velocity.clone() for b, f in self.outflow]
+        saved_incr = None if self._adv_incr is None else self._adv_incr.clone()
         torch.cuda.synchronize()
         s = torch.cuda.Stream()
         s.wait_stream(torch.cuda.current_stream())
@@ -367,6 +386,11 @@ class PISOStepper:
             b.pressure.copy_(p)
         for (b, f), v in zip(self.outflow, saved_out):
             d.getBlock(b).getBoundary(f).velocity.copy_(v)
+        if self._adv_incr is not None:
+            if saved_incr is None:
+                self._adv_incr.zero_()
+            else:
+                self._adv_incr.copy_(saved_incr)
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g):
             for _ in range(steps):
