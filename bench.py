@@ -1379,6 +1379,10 @@ def main():
     ap.add_argument("--mg-iterations", type=int, default=0,
                     help="cap of the multigrid PCG iterations per correction (each system stops once its RMS residual "
                          "meets the refinement target); 0: 8 where the finest level smooths with two sweeps, else 12")
+    ap.add_argument("--mg-graph-loop", type=int, default=1,
+                    help="1: the multigrid PCG loop as a conditional node of the captured step (stops at convergence); "
+                         "0: the fixed launch sequence (what a profiler that cannot profile kernel nodes of graphs "
+                         "with conditional nodes needs)")
     ap.add_argument("--adv-tol", type=float, default=0.0,
                     help="RMS residual target of the advection solves (0: the workload's)")
     ap.add_argument("--refine-tol", type=float, default=0.0,
@@ -1412,6 +1416,9 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    if not args.mg_graph_loop:
+        from pict_b200 import _lib
+        _lib.load().pict_mg_set_graph_loop(0)
     try:
         if args.workload == "cylinder_street":
             run_street(args, rank, world)

@@ -261,9 +261,13 @@ __global__ void __launch_bounds__(MG_TPB, 4) k_mg_restrict(pict_mg_level_t F, pi
         for (int e = threadIdx.x; e < nh; e += MG_TPB) {
             const int i = lo + e;
             const T bi = rhs(i), di = cf[i];
-            if (nu == 1) s_x0[e] = mg_x0(di, bi, w);
+            if (nu == 1) {
+                s_x0[e] = mg_x0(di, bi, w);
+                s_d[e] = di;
+            } else {
+                s_d[e] = (di != T(0)) ? mg_div(w, di) : T(0);  // w / diag
+            }
             s_b[e] = bi;
-            s_d[e] = di;
             if (UPD) {
                 const int par = (xx >> Bc.shx) + Bc.sx * (yy >> Bc.shy);
                 if (par >= lc0 && par <= lc1) {
@@ -280,14 +284,14 @@ __global__ void __launch_bounds__(MG_TPB, 4) k_mg_restrict(pict_mg_level_t F, pi
         }
         __syncthreads();
         if (nu == 2) {
-            // x1 = x0 + w (b - A x0) / diag on the stage, x0 = w b / diag formed from the staged b and diag.
+            // x1 = x0 + w (b - A x0) / diag on the stage, x0 = (w / diag) b formed from the staged b and w / diag.
             // Rows of the stage's edge whose outer neighbour row lies outside the stage get a value that no
             // child reads (children rows are at least one row inside); the block's own edges are fixed faces.
-            auto x0s = [&](int c) { return mg_x0(s_d[c], s_b[c], w); };
+            auto x0s = [&](int c) { return s_d[c] * s_b[c]; };
             int ey = (int)threadIdx.x / sx, ex = (int)threadIdx.x - ey * sx;
             for (int e = threadIdx.x; e < nh; e += MG_TPB) {
                 const int i = lo + e, yg = ylo + ey;
-                const T di = s_d[e], xi = x0s(e);
+                const T di = cf[i], xi = x0s(e);
                 const T xm = ex > 0 ? x0s(e - 1) : x0s(e + sx - 1);
                 const T xp = ex + 1 < sx ? x0s(e + 1) : x0s(e - sx + 1);
                 const bool hm = ey > 0, hp = ey + 1 < nh / sx;
@@ -297,7 +301,7 @@ __global__ void __launch_bounds__(MG_TPB, 4) k_mg_restrict(pict_mg_level_t F, pi
                 ax += (ex + 1 < sx || Bf.px) ? cf[(size_t)2 * Nf + i] * xp : T(0);
                 ax += (yg > 0 && hm) ? cf[(size_t)3 * Nf + i] * ym : T(0);
                 ax += (yg + 1 < Bf.sy && hp) ? cf[(size_t)4 * Nf + i] * yp : T(0);
-                s_x0[e] = xi + ((di != T(0)) ? mg_div(w * (s_b[e] - ax), di) : T(0));
+                s_x0[e] = xi + s_d[e] * (s_b[e] - ax);
                 ex += dr;
                 ey += dq;
                 if (ex >= sx) {
@@ -328,7 +332,7 @@ __global__ void __launch_bounds__(MG_TPB, 4) k_mg_restrict(pict_mg_level_t F, pi
                 const T xp = xs + 1 < sx ? s_x0[c + 1] : s_x0[c - sx + 1];
                 const T ym = ys > 0 ? s_x0[c - sx] : (Bf.py ? far(xs, Bf.sy - 1) : T(0));
                 const T yp = ys + 1 < Bf.sy ? s_x0[c + sx] : (Bf.py ? far(xs, 0) : T(0));
-                T ax = s_d[c] * xi;
+                T ax = (nu == 2 ? cf[i] : s_d[c]) * xi;
                 ax += (xs > 0 || Bf.px) ? cf[(size_t)Nf + i] * xm : T(0);
                 ax += (xs + 1 < sx || Bf.px) ? cf[(size_t)2 * Nf + i] * xp : T(0);
                 ax += (ys > 0 || Bf.py) ? cf[(size_t)3 * Nf + i] * ym : T(0);
@@ -421,36 +425,39 @@ __global__ void __launch_bounds__(MG_TPB, 4) k_mg_prolong(pict_mg_level_t F, pic
     const int sx = Bf.sx;
     const int cap4 = (3 * cap) / 4;  // four arrays in the shared memory of three of `cap` cells
     if (D == 2 && nu == 2 && tl.cnt + 6 * sx <= cap4) {
-        T* s_x = reinterpret_cast<T*>(mg_stage_raw);
+        T* s_x = reinterpret_cast<T*>(mg_stage_raw);  // x0, then the first post sweep
         T* s_b = s_x + cap4;
-        T* s_d = s_b + cap4;
-        T* s_y = s_d + cap4;  // x1
+        T* s_r = s_b + cap4;                           // w / diag
+        T* s_y = s_r + cap4;                           // x1, then x' = x1 + s P e_c
         const int nf = sx * Bf.sy;
         const int lo = max(Bf.off, tl.s0 - 3 * sx), hi = min(Bf.off + nf, tl.s0 + tl.cnt + 3 * sx);
         for (int e = threadIdx.x; e < hi - lo; e += MG_TPB) {
-            s_b[e] = bv[lo + e];
-            s_d[e] = cf[lo + e];
+            const T d = cf[lo + e], bb = bv[lo + e];
+            const T r = (d != T(0)) ? mg_div(w, d) : T(0);
+            s_b[e] = bb;
+            s_r[e] = r;
+            s_x[e] = r * bb;
         }
         __syncthreads();
-        // one damped-Jacobi sweep over the global cells [g0, g1) of a stage-resident iterate given by xin(c)
-        // (c: stage index); neighbours outside the block are fixed faces (no y-periodic wrap on this path)
-        auto sweep = [&](int g0, int g1, auto&& xin, T* dst) {
+        // one damped-Jacobi sweep over the global cells [g0, g1): dst = src + (w / diag) (b - A src), src and dst
+        // on the stage; neighbours outside the block are fixed faces (no y-periodic wrap on this path)
+        auto sweep = [&](int g0, int g1, const T* src, T* dst) {
             const int dq = MG_TPB / sx, dr = MG_TPB - dq * sx;
             int l = g0 - Bf.off + (int)threadIdx.x;
             int y = l / sx, x = l - y * sx;
             for (int i = g0 + (int)threadIdx.x; i < g1; i += MG_TPB) {
                 const int c = i - lo;
-                const T di = s_d[c], xi = xin(c);
-                const T xm = x > 0 ? xin(c - 1) : xin(c + sx - 1);
-                const T xp = x + 1 < sx ? xin(c + 1) : xin(c - sx + 1);
-                const T ym = y > 0 ? xin(c - sx) : T(0);
-                const T yp = y + 1 < Bf.sy ? xin(c + sx) : T(0);
-                T acc = di * xi;
+                const T xi = src[c];
+                const T xm = x > 0 ? src[c - 1] : src[c + sx - 1];
+                const T xp = x + 1 < sx ? src[c + 1] : src[c - sx + 1];
+                const T ym = y > 0 ? src[c - sx] : T(0);
+                const T yp = y + 1 < Bf.sy ? src[c + sx] : T(0);
+                T acc = cf[i] * xi;
                 acc += (x > 0 || Bf.px) ? cf[(size_t)N + i] * xm : T(0);
                 acc += (x + 1 < sx || Bf.px) ? cf[(size_t)2 * N + i] * xp : T(0);
                 acc += y > 0 ? cf[(size_t)3 * N + i] * ym : T(0);
                 acc += y + 1 < Bf.sy ? cf[(size_t)4 * N + i] * yp : T(0);
-                dst[c] = xi + ((di != T(0)) ? mg_div(w * (s_b[c] - acc), di) : T(0));
+                dst[c] = xi + s_r[c] * (s_b[c] - acc);
                 x += dr;
                 y += dq;
                 if (x >= sx) {
@@ -461,16 +468,24 @@ __global__ void __launch_bounds__(MG_TPB, 4) k_mg_prolong(pict_mg_level_t F, pic
         };
         const int a1 = max(Bf.off, tl.s0 - 2 * sx), b1 = min(Bf.off + nf, tl.s0 + tl.cnt + 2 * sx);
         const int a2 = max(Bf.off, tl.s0 - sx), b2 = min(Bf.off + nf, tl.s0 + tl.cnt + sx);
-        // x1 = x0 + w (b - A x0) / diag, x0 = w b / diag
-        sweep(a1, b1, [&](int c) { return mg_x0(s_d[c], s_b[c], w); }, s_y);
+        sweep(a1, b1, s_x, s_y);  // x1: the pre-smoothed iterate of the restriction
         __syncthreads();
-        // x' = x1 + s P e_c; first post sweep into s_x
-        auto xprime = [&](int c) {
-            const int l = c + lo - Bf.off;
-            const int y = l / sx, x = l - y * sx;
-            return s_y[c] + s * ec[Bc.off + (x >> Bc.shx) + Bc.sx * (y >> Bc.shy)];
-        };
-        sweep(a2, b2, xprime, s_x);
+        {  // x' = x1 + s P e_c
+            const int dq = MG_TPB / sx, dr = MG_TPB - dq * sx;
+            int l = a1 - Bf.off + (int)threadIdx.x;
+            int y = l / sx, x = l - y * sx;
+            for (int i = a1 + (int)threadIdx.x; i < b1; i += MG_TPB) {
+                s_y[i - lo] += s * ec[Bc.off + (x >> Bc.shx) + Bc.sx * (y >> Bc.shy)];
+                x += dr;
+                y += dq;
+                if (x >= sx) {
+                    x -= sx;
+                    ++y;
+                }
+            }
+        }
+        __syncthreads();
+        sweep(a2, b2, s_y, s_x);  // first post sweep
         __syncthreads();
         // second post sweep of the tile's cells
         const int dq = MG_TPB / sx, dr = MG_TPB - dq * sx;
@@ -478,17 +493,17 @@ __global__ void __launch_bounds__(MG_TPB, 4) k_mg_prolong(pict_mg_level_t F, pic
         int y = l / sx, x = l - y * sx;
         for (int k = threadIdx.x; k < tl.cnt; k += MG_TPB) {
             const int i = tl.s0 + k, c = i - lo;
-            const T xi = s_x[c], di = s_d[c], bi = s_b[c];
+            const T xi = s_x[c], bi = s_b[c];
             const T xm = x > 0 ? s_x[c - 1] : s_x[c + sx - 1];
             const T xp = x + 1 < sx ? s_x[c + 1] : s_x[c - sx + 1];
             const T ym = y > 0 ? s_x[c - sx] : T(0);
             const T yp = y + 1 < Bf.sy ? s_x[c + sx] : T(0);
-            T acc = di * xi;
+            T acc = cf[i] * xi;
             acc += (x > 0 || Bf.px) ? cf[(size_t)N + i] * xm : T(0);
             acc += (x + 1 < sx || Bf.px) ? cf[(size_t)2 * N + i] * xp : T(0);
             acc += y > 0 ? cf[(size_t)3 * N + i] * ym : T(0);
             acc += y + 1 < Bf.sy ? cf[(size_t)4 * N + i] * yp : T(0);
-            const T zi = xi + ((di != T(0)) ? mg_div(w * (bi - acc), di) : T(0));
+            const T zi = xi + s_r[c] * (bi - acc);
             out[i] = zi;
             if (DOT) {
                 a += (double)bi * (double)zi;
