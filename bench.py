@@ -323,7 +323,8 @@ def precision_kwargs(args, wl=None):
     from zero (the reference's order)."""
     if args.precision == "mixed":
         rt = getattr(args, "refine_tol", 0.0) or (wl or {}).get("refine_tol", 1e-9)
-        return {"pressure_refine": 1, "refine_tol": rt, "warm_start_pressure": True,
+        return {"pressure_refine": 1, "refine_tol": rt,
+                "warm_start_pressure": "increment" if getattr(args, "warm_pressure", 2) == 2 else True,
                 "refine_solver": args.refine_solver, "pressure_first_solve": bool(args.first_solve),
                 "mg_iterations": args.mg_iterations,
                 "warm_start_advection": "increment" if args.warm_advection == 2 else bool(args.warm_advection)}
@@ -594,7 +595,7 @@ def run_pict(args, rank, world):
                        "pass": "forward", "solver_tol": wl["tol"], "advection_tol": st.adv_tol,
                        "correctors": wl["correctors"],
                        "precision": args.precision + (" (FP32 fields and Krylov vectors, FP64 reductions, one FP64 "
-                                                      "refinement sweep of each pressure solve to %g RMS (multigrid-preconditioned CG corrections on near-isotropic grids, at most %d iterations, each system stopping at the target), warm-started pressure solves" % (st.refine_tol, st.mg_iterations) + (", advection solves from the current velocity plus the previous step's advection increment" if args.warm_advection == 2 else (", advection solves from the current velocity" if args.warm_advection else "")) + ")"
+                                                      "refinement sweep of each pressure solve to %g RMS (multigrid-preconditioned CG corrections on near-isotropic grids, at most %d iterations, each system stopping at the target), warm-started pressure solves" % (st.refine_tol, st.mg_iterations) + (" (later correctors from the previous corrector's pressure plus the previous step's corrector increment)" if st.pressure_increment else "") + (", advection solves from the current velocity plus the previous step's advection increment" if args.warm_advection == 2 else (", advection solves from the current velocity" if args.warm_advection else "")) + ")"
                                                       if args.precision == "mixed" else " (FP32, FP64 reductions)"),
                        "cuda_graph": not args.no_graph, "cuda_graph_steps": None if args.no_graph else G,
                        "l2": "working set > L2 (126 MB), no flush",
@@ -1383,6 +1384,9 @@ def main():
                     help="1: the multigrid PCG loop as a conditional node of the captured step (stops at convergence); "
                          "0: the fixed launch sequence (what a profiler that cannot profile kernel nodes of graphs "
                          "with conditional nodes needs)")
+    ap.add_argument("--warm-pressure", type=int, default=2,
+                    help="mixed precision: refinement of corrector k >= 1 starts from corrector k-1's pressure (1) "
+                         "or from it plus the previous step's corrector increment (2)")
     ap.add_argument("--adv-tol", type=float, default=0.0,
                     help="RMS residual target of the advection solves (0: the workload's)")
     ap.add_argument("--refine-tol", type=float, default=0.0,

@@ -79,6 +79,11 @@ class PISOStepper:
         # warm start: every pressure solve starts from pressureResult (the previous corrector's or step's
         # mean-free pressure) instead of zero; same solution, fewer iterations
         self.warm_start_pressure = bool(warm_start_pressure)
+        # "increment": corrector k >= 1 of the refined solve starts from corrector k-1's pressure plus the previous
+        # step's difference between the two (the pressure changes little between steps, the correction between
+        # correctors even less; on the batched cavities its initial residual falls 10-90x)
+        self.pressure_increment = warm_start_pressure == "increment"
+        self._p_delta = None
         self.p_params = P._solve_params(1, self.max_iterations, self.p_tol, _lib.PICT_CONV_NORM2_NORMALIZED, False,
                                         False, x_zero=not self.warm_start_pressure,
                                         subtract_mean=normalize_pressure and not refine,
@@ -189,7 +194,34 @@ class PISOStepper:
                                  ctypes.byref(self.p_params), P._ptr(self.info_p[k]), P._ptr(self.ws), self.ws_bytes,
                                  st), "pressure solve")
         if self.pressure_refine > 0:
-            self._refine_only(k, desc, st)
+            if self.pressure_increment and k > 0 and not self.pressure_first_solve:
+                self._refine_only(k, desc, st, x_init=self._pressure_guess(k, st))
+                self._pressure_delta(k, st)
+            else:
+                self._refine_only(k, desc, st)
+
+    def _pressure_guess(self, k, st):
+        """Starting pressure of corrector k >= 1: pressureResult (corrector k-1's) plus the previous step's
+        corrector-k increment; keeps corrector k-1's pressure for the next increment."""
+        d = self.domain
+        n = d.getTotalSize()
+        if self._p_delta is None:
+            self._p_delta = torch.zeros(max(self.corrector_steps - 1, 1), n, dtype=d.getDtype(), device=d.getDevice())
+            self._p_prev = torch.zeros(n, dtype=d.getDtype(), device=d.getDevice())
+            self._p_guess = torch.zeros(n, dtype=d.getDtype(), device=d.getDevice())
+        code = _lib.PICT_F64 if d.getDtype() == torch.float64 else _lib.PICT_F32
+        check(self.lib.pict_vector_axpy(n, code, 0.0, P._ptr(d.pressureResult), P._ptr(d.pressureResult),
+                                        P._ptr(self._p_prev), st), "pressure warm start")
+        check(self.lib.pict_vector_axpy(n, code, 1.0, P._ptr(d.pressureResult), P._ptr(self._p_delta[k - 1]),
+                                        P._ptr(self._p_guess), st), "pressure warm start")
+        return self._p_guess
+
+    def _pressure_delta(self, k, st):
+        d = self.domain
+        n = d.getTotalSize()
+        code = _lib.PICT_F64 if d.getDtype() == torch.float64 else _lib.PICT_F32
+        check(self.lib.pict_vector_axpy(n, code, -1.0, P._ptr(d.pressureResult), P._ptr(self._p_prev),
+                                        P._ptr(self._p_delta[k - 1]), st), "pressure increment")
 
     def step(self, time_step=None, stream=None):
         """Launch one PISO step (no host synchronisation)."""
@@ -235,7 +267,7 @@ class PISOStepper:
             check(self.lib.pict_advective_outflow(desc, self._of_faces, len(self.outflow), self._of_vel, dt,
                                                   self._of_atol, st), "advective outflow")
 
-    def _refine_only(self, k, desc, st, events=None, ev=None):
+    def _refine_only(self, k, desc, st, events=None, ev=None, x_init=None):
         """FP64 refinement sweeps after the first pressure solve of corrector k: residual of the FP64
         accumulator, FP32 correction solve, accumulation; then the mean-free result into
         pressureResult and the blocks' pressure."""
@@ -243,8 +275,9 @@ class PISOStepper:
         lib = self.lib
         x64 = ctypes.c_void_p(self._x64.data_ptr())
         for m in range(self.pressure_refine):
+            start = (d.pressureResult if x_init is None else x_init) if m == 0 else None
             check(lib.pict_refine_residual(desc, P._ptr(d.P.coef), P._ptr(d.pressureRHSdiv),
-                                           P._ptr(d.pressureResult) if m == 0 else None, x64, P._ptr(self._res),
+                                           P._ptr(start), x64, P._ptr(self._res),
                                            int(self.normalize_pressure), ctypes.c_void_p(self._tile_scratch.data_ptr()),
                                            st), "refine residual")
             a = ev() if ev else None
@@ -330,7 +363,12 @@ class PISOStepper:
                 b = ev()
                 out["cg"].append((a, b, self.info_p[k].clone()))
             if self.pressure_refine > 0:
-                self._refine_only(k, desc, st, events=out["mg" if self._mg is not None else "cg"], ev=ev)
+                evs = out["mg" if self._mg is not None else "cg"]
+                if self.pressure_increment and k > 0 and not self.pressure_first_solve:
+                    self._refine_only(k, desc, st, events=evs, ev=ev, x_init=self._pressure_guess(k, st))
+                    self._pressure_delta(k, st)
+                else:
+                    self._refine_only(k, desc, st, events=evs, ev=ev)
             last = k == self.corrector_steps - 1
             check(lib.pict_correct_velocity(desc, dt, 1, 0, 1 if last else 0, st), "velocity correction")
         return out
@@ -374,6 +412,7 @@ class PISOStepper:
         saved = [(b.velocity.clone(), b.pressure.clone()) for b in d.getBlocks()]
         saved_out = [d.getBlock(b).getBoundary(f).velocity.clone() for b, f in self.outflow]
         saved_incr = None if self._adv_incr is None else self._adv_incr.clone()
+        saved_pd = None if self._p_delta is None else self._p_delta.clone()
         torch.cuda.synchronize()
         s = torch.cuda.Stream()
         s.wait_stream(torch.cuda.current_stream())
@@ -391,6 +430,11 @@ class PISOStepper:
                 self._adv_incr.zero_()
             else:
                 self._adv_incr.copy_(saved_incr)
+        if self._p_delta is not None:
+            if saved_pd is None:
+                self._p_delta.zero_()
+            else:
+                self._p_delta.copy_(saved_pd)
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g):
             for _ in range(steps):

@@ -120,3 +120,27 @@ def test_advection_increment_guess_same_step_fewer_iterations():
     assert sum(out[1][0][2:]) < sum(out[0][0][2:]), out[0][0] + out[1][0]
     for u0, u1 in zip(out[0][1], out[1][1]):
         assert float((u0 - u1).abs().max()) <= 1e-4 * float(u0.abs().max())
+
+
+def test_pressure_increment_warm_start_same_step():
+    """The refinement of the second corrector started from the first corrector's pressure plus the previous
+    step's corrector increment gives the same fields (to the refinement tolerance) in no more iterations."""
+    import bench
+    from pict_b200.batch import BatchDomain
+    from pict_b200.engine import PISOStepper
+    out = []
+    for ws in (True, "increment"):
+        doms = [bench.make_cavity_domain(n, 1.0 / re, torch.float32) for n, re in ((128, 150.0), (96, 2000.0))]
+        b = BatchDomain(doms, time_steps=[0.5 / 128, 0.5 / 96])
+        st = PISOStepper(b, time_step=0.5 / 128, advection_tol=1e-6, pressure_tol=1e-6, pressure_refine=1,
+                         refine_tol=5e-10, warm_start_pressure=ws, refine_solver="mg", pressure_first_solve=False)
+        its = []
+        for _ in range(8):
+            st.step()
+            its.append(sum(i.usedIterations for i in st.refine_infos()[1][0]))
+        st.check()
+        out.append((its, [torch.cat([d.getBlock(0).velocity.reshape(-1), d.getBlock(0).pressure.reshape(-1)])
+                          for d in doms]))
+    assert sum(out[1][0][2:]) < sum(out[0][0][2:]), out[0][0] + out[1][0]
+    for a, c in zip(out[0][1], out[1][1]):
+        assert float((a - c).abs().max()) <= 1e-4 * float(a.abs().max())
