@@ -296,10 +296,10 @@ pict_status_t pict_refine_residual(const pict_domain_t* dom, const void* coef, c
                                    double* x64, void* residual, int32_t project_mean, double* tile_scratch,
                                    void* stream);
 pict_status_t pict_refine_update(const pict_domain_t* dom, double* x64, const void* correction, void* stream);
-/* out = x + alpha y over n values of `dtype` (out may alias x or y); the step's warm starts combine vectors with
- * it (no counterpart in the reference). */
-pict_status_t pict_vector_axpy(int32_t n, int32_t dtype, double alpha, const void* x, const void* y, void* out,
-                               void* stream);
+/* out = alpha x + beta y over n values of `dtype` (out may alias x or y); the step's warm starts combine vectors
+ * with it (no counterpart in the reference). */
+pict_status_t pict_vector_axpby(int32_t n, int32_t dtype, double alpha, const void* x, double beta, const void* y,
+                                void* out, void* stream);
 pict_status_t pict_refine_finish(const pict_domain_t* dom, const double* x64, void* x, int32_t subtract_mean,
                                  int32_t write_block_pressure, double* tile_scratch, void* stream);
 

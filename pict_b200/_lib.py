@@ -191,7 +191,7 @@ SIGNATURES = {
     "pict_refine_residual": (c_i32, [_PD, c_vp, c_vp, c_vp, c_vp, c_vp, c_i32, c_vp, c_vp]),
     "pict_refine_update": (c_i32, [_PD, c_vp, c_vp, c_vp]),
     "pict_refine_finish": (c_i32, [_PD, c_vp, c_vp, c_i32, c_i32, c_vp, c_vp]),
-    "pict_vector_axpy": (c_i32, [c_i32, c_i32, ctypes.c_double, c_vp, c_vp, c_vp, c_vp]),
+    "pict_vector_axpby": (c_i32, [c_i32, c_i32, ctypes.c_double, c_vp, ctypes.c_double, c_vp, c_vp, c_vp]),
     "pict_mg_set_bulk_staging": (None, [c_i32]),
     "pict_mg_set_smoothing_sweeps": (None, [c_i32]),
     "pict_mg_set_graph_loop": (None, [c_i32]),

@@ -119,10 +119,11 @@ __global__ void k_tile_subtract_mean(pict_domain_t dom, T* v, const double* part
     for (int i = s0 + threadIdx.x; i < s0 + cnt; i += blockDim.x) v[i] -= m;
 }
 
-// out = x + alpha y over n values
+// out = alpha x + beta y over n values
 template <typename T>
-__global__ void k_vector_axpy(int n, T alpha, const T* __restrict__ x, const T* __restrict__ y, T* __restrict__ out) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += blockDim.x * gridDim.x) out[i] = x[i] + alpha * y[i];
+__global__ void k_vector_axpby(int n, T alpha, const T* x, T beta, const T* y, T* out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += blockDim.x * gridDim.x)
+        out[i] = alpha * x[i] + beta * y[i];
 }
 
 }  // namespace pict
@@ -131,17 +132,18 @@ using namespace pict;
 
 extern "C" {
 
-pict_status_t pict_vector_axpy(int32_t n, int32_t dtype, double alpha, const void* x, const void* y, void* out,
-                               void* stream) {
-    if (n < 0 || !x || !y || !out) return set_error(PICT_ERR_ARG, "vector_axpy: invalid argument");
+pict_status_t pict_vector_axpby(int32_t n, int32_t dtype, double alpha, const void* x, double beta, const void* y,
+                                void* out, void* stream) {
+    if (n < 0 || !x || !y || !out) return set_error(PICT_ERR_ARG, "vector_axpby: invalid argument");
     if (n == 0) return PICT_OK;
     cudaStream_t st = (cudaStream_t)stream;
     const int grid = cell_grid(n, 256);
     if (dtype == PICT_F64)
-        k_vector_axpy<double><<<grid, 256, 0, st>>>(n, alpha, (const double*)x, (const double*)y, (double*)out);
+        k_vector_axpby<double><<<grid, 256, 0, st>>>(n, alpha, (const double*)x, beta, (const double*)y, (double*)out);
     else
-        k_vector_axpy<float><<<grid, 256, 0, st>>>(n, (float)alpha, (const float*)x, (const float*)y, (float*)out);
-    return check_launch("vector_axpy");
+        k_vector_axpby<float><<<grid, 256, 0, st>>>(n, (float)alpha, (const float*)x, (float)beta, (const float*)y,
+                                                   (float*)out);
+    return check_launch("vector_axpby");
 }
 
 pict_status_t pict_refine_residual(const pict_domain_t* dom, const void* coef, const void* rhs, const void* x_init,
