@@ -56,7 +56,7 @@ __device__ __forceinline__ void pressure_grad_fd(const pict_domain_t& dom, const
 }
 
 template <typename T, int D, bool MATRIX, bool RHS>
-__global__ void k_adv_setup(pict_domain_t dom, double dt_arg, int apply_pgrad) {
+__global__ void __launch_bounds__(256, 6) k_adv_setup(pict_domain_t dom, double dt_arg, int apply_pgrad) {
     constexpr int K = 2 * D + 1;
     const int N = dom.num_cells;
     T* C = reinterpret_cast<T*>(dom.C);
@@ -145,7 +145,7 @@ __global__ void k_adv_setup(pict_domain_t dom, double dt_arg, int apply_pgrad) {
 // ---------------------------------------------------------------------------------------------
 
 template <typename T, int D, bool MATRIX, bool RHS>
-__global__ void k_pressure_setup(pict_domain_t dom, double dt_arg) {
+__global__ void __launch_bounds__(256, 6) k_pressure_setup(pict_domain_t dom, double dt_arg) {
     const int N = dom.num_cells;
     const T* C = reinterpret_cast<const T*>(dom.C);
     const T* A = reinterpret_cast<const T*>(dom.A);
