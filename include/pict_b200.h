@@ -426,6 +426,25 @@ pict_status_t pict_scalar_grad(const pict_domain_t* dom, double dt, int32_t non_
  * length of the cell transform M, 1 without one). */
 pict_status_t pict_sgs_smagorinsky(const pict_domain_t* dom, double coefficient, void* out, void* stream);
 
+/* ---------------- multi-block convolution padding (MultiblockConv, lib/modules/multiblock_cnn.py:92-369) --------
+ * Fields are [batch][channels][cells] per block.  src_ptrs / out_ptrs / gout_ptrs / gsrc_ptrs: HOST arrays of the
+ * num_blocks (1..64) blocks' device pointers, src_cells / out_cells: HOST arrays of their cells (unpadded /
+ * padded); they travel in the kernel parameters.  batch_channels: batch x channels.
+ * pict_mb_pad_gather: for the n padded cells j, out[out_block[j]][c][out_pos[j]] = src[src_block[j]][c][src_loc[j]],
+ *   0 where src_block[j] < 0 (fixed faces, unreachable corners).
+ * pict_mb_pad_scatter_sum: its gradient, for the n source cells g = (src_block[g], src_loc[g]):
+ *   gsrc[..][c][..] = sum over k in [reader_ptr[g], reader_ptr[g + 1]) of gout[reader_block[k]][c][reader_pos[k]]
+ *   (every source cell written; a fixed order: deterministic).  The index arrays are device arrays. */
+pict_status_t pict_mb_pad_gather(int32_t n, int32_t batch_channels, int32_t dtype, int32_t num_blocks,
+                                 const int32_t* out_block, const int32_t* out_pos, const int32_t* src_block,
+                                 const int32_t* src_loc, const void* const* src_ptrs, const int64_t* src_cells,
+                                 void* const* out_ptrs, const int64_t* out_cells, void* stream);
+pict_status_t pict_mb_pad_scatter_sum(int32_t n, int32_t batch_channels, int32_t dtype, int32_t num_blocks,
+                                      const int32_t* src_block, const int32_t* src_loc, const int32_t* reader_ptr,
+                                      const int32_t* reader_block, const int32_t* reader_pos,
+                                      const void* const* gout_ptrs, const int64_t* out_cells, void* const* gsrc_ptrs,
+                                      const int64_t* src_cells, void* stream);
+
 /* ---------------- preconditioned BiCGStab ----------------
  * SolveLinear with useBiCG and BiCGwithPreconditioner (bicgstabSolveGPU, extensions/bicgstab_solver_kernel.cu:47-395),
  * the fallback of the reference's solve wrapper (PISOtorch_diff.py:276-286), on the CSR form of a stencil matrix

@@ -197,6 +197,9 @@ SIGNATURES = {
     "pict_mg_set_graph_loop": (None, [c_i32]),
     "pict_krylov_set_cluster_mode": (None, [c_i32]),
     "pict_krylov_set_bicgstab_variant": (None, [c_i32]),
+    "pict_mb_pad_gather": (c_i32, [c_i32, c_i32, c_i32, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "pict_mb_pad_scatter_sum": (c_i32, [c_i32, c_i32, c_i32, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
+                                        c_vp]),
     "pict_ilu_analyze": (c_i32, [c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "pict_bicgstab_ilu_workspace_bytes": (ctypes.c_int64, [c_i32, c_i32, c_i32]),
     "pict_ilu0_factor": (c_i32, [c_i32, c_i32, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_i32, c_vp, c_vp, c_vp]),

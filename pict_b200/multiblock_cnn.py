@@ -3,9 +3,11 @@
 A ``MultiblockConv`` applies one ``torch.nn.ConvNd`` to every block of a domain, padding each block with
 the cells of the blocks it is connected to (across ``ConnectedBoundary`` faces, with their axis
 permutations and inversions, and across periodic faces) and with zeros at fixed faces, so that a
-network sees the domain as one field.  The padding of a block is a fixed gather: built once at
-construction as an index map into the concatenation of all blocks' cells (plus one zero), it costs
-one ``index_select`` per block and call, and its gradient is the matching scatter-add.
+network sees the domain as one field.  The padding of every block is a fixed gather, built once at
+construction as a map from each padded cell to its source (block, cell) or zero.  On CUDA tensors it is one
+launch of this library for all blocks, reading the blocks in place (``pict_mb_pad_gather``), and its gradient
+is one gather-sum over the inverse map (``pict_mb_pad_scatter_sum``, deterministic).  On CPU tensors the same
+map runs as ``index_select`` over the concatenated blocks.
 
 Which block fills a padding region follows the reference's walk (lib/modules/multiblock_cnn.py:158-264):
 from the block, each axis in order x, y, z, lower then upper face; a connected or periodic face makes
@@ -25,11 +27,14 @@ addresses in the solver's stencils).
 """
 from __future__ import annotations
 
+import ctypes
 from typing import List
 
+import numpy as np
 import torch
 
 from . import PISOtorch as P
+from . import _lib
 
 __all__ = ["MultiblockConv", "MultiblockConv_naive", "MultiblockReLU"]
 
@@ -123,6 +128,7 @@ class MultiblockConv(torch.nn.Module):
         idx = [self._gather_index(bi, blocks, offsets) for bi in range(len(blocks))]
         for bi, t in enumerate(idx):  # moved with the module by .to() / .cuda()
             self.register_buffer("_gather_%d" % bi, t if device is None else t.to(device), persistent=False)
+        self._build_device_map(idx, offsets, n)
         self.conv_layer = conv(in_channels, out_channels, kernel_size, stride=stride, padding=0, dilation=dilation,
                                groups=groups, bias=bias, padding_mode=padding_mode, device=device, dtype=dtype)
 
@@ -195,6 +201,42 @@ class MultiblockConv(torch.nn.Module):
             grid = [torch.cat(grid[i * 3:i * 3 + 3], dim=cat_dim + 2) for i in range(len(grid) // 3)]
         return grid[0].reshape(-1).contiguous()
 
+    def _build_device_map(self, idx, offsets, n):
+        """The map of the library's padding kernels: per padded cell (output block, position) <- (source block,
+        cell) or -1, and its inverse (the padded cells reading each source cell, CSR)."""
+        nb = len(idx)
+        starts = np.asarray(offsets + [n], dtype=np.int64)
+        ob, pos, sb, loc = [], [], [], []
+        for bi, t in enumerate(idx):
+            g = t.cpu().numpy().astype(np.int64)
+            b = np.searchsorted(starts, g, side="right") - 1
+            zero = g >= n
+            ob.append(np.full(g.size, bi, np.int32))
+            pos.append(np.arange(g.size, dtype=np.int32))
+            sb.append(np.where(zero, -1, b).astype(np.int32))
+            loc.append(np.where(zero, 0, g - starts[np.minimum(b, nb - 1)]).astype(np.int32))
+        ob, pos, sb, loc = (np.concatenate(a) for a in (ob, pos, sb, loc))
+        gsrc = np.concatenate([t.cpu().numpy() for t in idx]).astype(np.int64)
+        keep = gsrc < n
+        order = np.argsort(gsrc[keep], kind="stable")
+        readers = np.nonzero(keep)[0][order]
+        counts = np.bincount(gsrc[keep], minlength=n)
+        rptr = np.concatenate([[0], np.cumsum(counts)]).astype(np.int32)
+        cell_block = np.repeat(np.arange(nb, dtype=np.int32), np.diff(starts))
+        cell_loc = (np.arange(n, dtype=np.int64) - starts[cell_block]).astype(np.int32)
+        t32 = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.int32))
+        maps = {"ob": ob, "pos": pos, "sb": sb, "loc": loc, "cb": cell_block, "cl": cell_loc, "rptr": rptr,
+                "rob": ob[readers], "rpos": pos[readers]}
+        for k, v in maps.items():
+            self.register_buffer("_pad_%s" % k, t32(v) if self.device is None else t32(v).to(self.device),
+                                 persistent=False)
+        pad = self.padding
+        self._src_cells = [int(np.prod(s)) for s in self._shapes]
+        self._out_cells = [int(np.prod([x + 2 * pad for x in s])) for s in self._shapes]
+
+    def _pad_device(self, tensor_list):
+        return _PadFunction.apply(self, *tensor_list)
+
     # ---- forward ----
     def forward(self, tensor_list: List[torch.Tensor], domain=None):
         if domain is not None:
@@ -221,6 +263,9 @@ class MultiblockConv(torch.nn.Module):
     def pad(self, tensor_list: List[torch.Tensor]) -> List[torch.Tensor]:
         """Every block's tensor with ``padding`` cells added on each side from its neighbours (zeros at fixed
         faces and unreachable corners)."""
+        if all(t.is_cuda for t in tensor_list) and tensor_list[0].dtype in (torch.float32, torch.float64) and \
+                len(tensor_list) <= 64:
+            return list(self._pad_device(tensor_list))
         batch, ch = tensor_list[0].size(0), tensor_list[0].size(1)
         ref = tensor_list[0]
         flat = torch.cat([t.reshape(batch, ch, -1) for t in tensor_list] +
@@ -233,6 +278,64 @@ class MultiblockConv(torch.nn.Module):
             shape = [s + 2 * self.padding for s in self._shapes[bi]]
             out.append(flat.index_select(2, idx).reshape([batch, ch] + shape))
         return out
+
+
+def _host_ptrs(tensors):
+    return (ctypes.c_void_p * len(tensors))(*[t.data_ptr() for t in tensors])
+
+
+def _host_cells(cells):
+    return (ctypes.c_int64 * len(cells))(*cells)
+
+
+class _PadFunction(torch.autograd.Function):
+    """The padding of all blocks in one launch (pict_mb_pad_gather) and its gradient in one launch
+    (pict_mb_pad_scatter_sum); the blocks' pointers travel in the kernel parameters."""
+
+    @staticmethod
+    def forward(ctx, layer, *tensors):
+        lib = _lib.load()
+        dev = tensors[0].device
+        dtype = tensors[0].dtype
+        batch, ch = tensors[0].size(0), tensors[0].size(1)
+        srcs = [t.contiguous() for t in tensors]
+        pad = layer.padding
+        outs = [torch.empty([batch, ch] + [x + 2 * pad for x in s], dtype=dtype, device=dev) for s in layer._shapes]
+        for k in ("ob", "pos", "sb", "loc"):
+            if getattr(layer, "_pad_" + k).device != dev:
+                setattr(layer, "_pad_" + k, getattr(layer, "_pad_" + k).to(dev))
+        code = _lib.PICT_F64 if dtype == torch.float64 else _lib.PICT_F32
+        stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+        _lib.check(lib.pict_mb_pad_gather(int(layer._pad_ob.numel()), batch * ch, code, len(srcs),
+                                          layer._pad_ob.data_ptr(), layer._pad_pos.data_ptr(), layer._pad_sb.data_ptr(),
+                                          layer._pad_loc.data_ptr(), _host_ptrs(srcs), _host_cells(layer._src_cells),
+                                          _host_ptrs(outs), _host_cells(layer._out_cells), stream),
+                   "multi-block padding")
+        ctx.layer = layer
+        ctx.meta = (batch, ch, dtype, dev, [t.shape for t in srcs])
+        return tuple(outs)
+
+    @staticmethod
+    @torch.autograd.function.once_differentiable
+    def backward(ctx, *gouts):
+        layer = ctx.layer
+        batch, ch, dtype, dev, shapes = ctx.meta
+        lib = _lib.load()
+        g = [torch.zeros([batch, ch] + [x + 2 * layer.padding for x in s], dtype=dtype, device=dev) if x is None
+             else x.contiguous() for x, s in zip(gouts, layer._shapes)]
+        gs = [torch.empty(sh, dtype=dtype, device=dev) for sh in shapes]
+        for k in ("cb", "cl", "rptr", "rob", "rpos"):
+            if getattr(layer, "_pad_" + k).device != dev:
+                setattr(layer, "_pad_" + k, getattr(layer, "_pad_" + k).to(dev))
+        code = _lib.PICT_F64 if dtype == torch.float64 else _lib.PICT_F32
+        stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+        _lib.check(lib.pict_mb_pad_scatter_sum(int(layer._pad_cb.numel()), batch * ch, code, len(gs),
+                                               layer._pad_cb.data_ptr(), layer._pad_cl.data_ptr(),
+                                               layer._pad_rptr.data_ptr(), layer._pad_rob.data_ptr(),
+                                               layer._pad_rpos.data_ptr(), _host_ptrs(g), _host_cells(layer._out_cells),
+                                               _host_ptrs(gs), _host_cells(layer._src_cells), stream),
+                   "multi-block padding gradient")
+        return (None, *gs)
 
 
 class MultiblockConv_naive(torch.nn.Module):
