@@ -338,6 +338,10 @@ void pict_mg_set_smoothing_sweeps(int32_t sweeps);
  * WHILE node that ends once every system has met the tolerance or the cap is reached, so a replay launches only
  * the iterations the systems need; 0 captures the fixed sequence of `iterations` iterations. */
 void pict_mg_set_graph_loop(int32_t enable);
+/* Process-wide choice (no counterpart in the reference): 1 (default) the kernels of pict_pcg_mg are launched with
+ * programmatic stream serialization (each one waits for its predecessor's writes at its first instruction and lets
+ * the next one launch at once, so launch latency overlaps the predecessor's last CTAs); 0 plain launches. */
+void pict_mg_set_dependent_launch(int32_t enable);
 /* Galerkin coarse operator R A P of `fine` into coarse->coef (aggregates of 2^D cells). */
 pict_status_t pict_mg_galerkin(const pict_mg_level_t* fine, const pict_mg_level_t* coarse, void* stream);
 int64_t pict_pcg_mg_workspace_bytes(const pict_domain_t* dom, const pict_mg_level_t* levels, int32_t num_levels);

@@ -195,6 +195,7 @@ SIGNATURES = {
     "pict_mg_set_bulk_staging": (None, [c_i32]),
     "pict_mg_set_smoothing_sweeps": (None, [c_i32]),
     "pict_mg_set_graph_loop": (None, [c_i32]),
+    "pict_mg_set_dependent_launch": (None, [c_i32]),
     "pict_krylov_set_cluster_mode": (None, [c_i32]),
     "pict_krylov_set_bicgstab_variant": (None, [c_i32]),
     "pict_mb_pad_gather": (c_i32, [c_i32, c_i32, c_i32, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),

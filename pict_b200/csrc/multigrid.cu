@@ -38,6 +38,28 @@ static int g_mg_sweeps = 2;
 static int g_mg_graph_loop = 1;
 // per device: the stream the loop body is captured on (created outside capture, on the first solve)
 static cudaStream_t g_mg_body_stream[64];
+// 1 (default): the PCG loop's kernels are launched with programmatic stream serialization (each waits for its
+// predecessor in mg_pdl_entry); 0: plain launches
+static int g_mg_pdl = 1;
+
+template <typename... KArgs, typename... Args>
+static void mg_launch(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args... args) {
+    if (!g_mg_pdl) {
+        k<<<grid, block, smem, st>>>(args...);
+        return;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k, args...);
+}
 
 // block of a level: first cell, sizes, periodic flags, system, and the coarsening shifts (log2 of the
 // factor, 0 or 1 per axis) from the next finer level
@@ -46,12 +68,26 @@ struct MgBlock {
 };
 
 constexpr int MG_BT = 12;  // ints per block-table entry
-constexpr int MG_SC = 6;   // per-system PCG scalars: rho, alpha, beta, |r|^2, mean(z), done
+constexpr int MG_SC = 7;   // per-system PCG scalars: rho, alpha, beta, |r|^2, mean(z), done, update pending
 
 // A system is done once its residual met the tolerance: sc[5] = iterations at that point + 1 (0 while
 // iterating).  The kernels of later iterations skip the tiles / blocks of done systems, so their iterate
 // and report stay those of the converged iteration.
 __device__ __forceinline__ bool mg_done(const double* sc, int sys) { return sc && sc[MG_SC * sys + 5] != 0.0; }
+
+// A system whose new residual |r - alpha q| met the tolerance at this iteration's scalar stage (before its
+// V-cycle) is done with its update x += alpha p, r -= alpha q still to apply: the finest restriction (or the
+// update kernel) applies it and skips the rest; the end-of-iteration scalar stage clears the flag.
+__device__ __forceinline__ bool mg_pending(const double* sc, int sys) { return sc && sc[MG_SC * sys + 6] != 0.0; }
+
+// First statement of every kernel of the PCG loop: wait for the previous kernel of the stream (its writes are
+// visible after the wait), then let the next one launch (programmatic dependent launch: its CTAs are
+// scheduled while this kernel's last CTAs run, and wait here in turn).  Without the launch attribute both are
+// no-ops.
+__device__ __forceinline__ void mg_pdl_entry() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
 
 __device__ __forceinline__ MgBlock mg_block(const pict_mg_level_t& L, int b) {
     const int* t = L.blocks + MG_BT * b;
@@ -234,13 +270,32 @@ __global__ void __launch_bounds__(MG_TPB, 4) k_mg_restrict(pict_mg_level_t F, pi
                                                            const T* __restrict__ p, const double* __restrict__ sc,
                                                            int first, T* __restrict__ bc, T w, int cap,
                                                            const double* __restrict__ dn, int nu) {
+    mg_pdl_entry();
     extern __shared__ __align__(16) unsigned char mg_stage_raw[];
     const MgTile tl = mg_tile(C.tiles, blockIdx.x);
-    if (mg_done(dn, tl.sys)) return;
+    const bool pend = UPD && mg_pending(sc, tl.sys);
+    if (mg_done(dn, tl.sys) && !pend) return;
     const MgBlock Bc = mg_block(C, tl.blk), Bf = mg_block(F, tl.blk);
     const T* __restrict__ cf = reinterpret_cast<const T*>(F.coef);
     const int Nf = F.num_cells;
     const T al = UPD ? (T)sc[MG_SC * tl.sys + 1] : T(0);
+    if (UPD && pend) {  // converged at this iteration: the update of the children, no restriction
+        for (int k = threadIdx.x; k < tl.cnt; k += MG_TPB) {
+            int X, Y, Z;
+            mg_unflatten(Bc, tl.s0 + k - Bc.off, X, Y, Z);
+#pragma unroll
+            for (int c = 0; c < (1 << D); ++c) {
+                const int dx = c & 1, dy = (c >> 1) & 1, dz = (c >> 2) & 1;
+                const int xs = (X << Bc.shx) + dx, ys = (Y << Bc.shy) + dy, zs = (Z << Bc.shz) + dz;
+                if ((dx && !Bc.shx) || (dy && !Bc.shy) || (dz && !Bc.shz) || xs >= Bf.sx || ys >= Bf.sy || zs >= Bf.sz)
+                    continue;
+                const int i = Bf.off + xs + Bf.sx * (ys + Bf.sy * zs);
+                rn[i] = r[i] - al * q[i];
+                x[i] = first ? al * p[i] : x[i] + al * p[i];
+            }
+        }
+        return;
+    }
     const MgRhs<T, UPD> rhs{r, q, al};
     const int sx = Bf.sx;
     int ylo = 0, yhi = -1;
@@ -415,6 +470,7 @@ __global__ void __launch_bounds__(MG_TPB, 4) k_mg_prolong(pict_mg_level_t F, pic
                                                           const T* __restrict__ bv, const T* __restrict__ ec,
                                                           T* __restrict__ out, T s, T w, double* __restrict__ part,
                                                           int cap, const double* __restrict__ dn, int nu) {
+    mg_pdl_entry();
     extern __shared__ __align__(16) unsigned char mg_stage_raw[];
     const MgTile tl = mg_tile(tiles, blockIdx.x);
     if (mg_done(dn, tl.sys)) return;
@@ -682,6 +738,7 @@ template <typename T, int D>
 __global__ void __launch_bounds__(MG_SUB_THREADS) k_mg_subcycle(MgSub S, const T* __restrict__ bin,
                                                                 T* __restrict__ xout, T w, T sp, int sweeps,
                                                                 const double* __restrict__ dn, int nu) {
+    mg_pdl_entry();
     constexpr int K = 2 * D + 1;
     extern __shared__ __align__(16) unsigned char mg_sub_raw[];
     T* sm = reinterpret_cast<T*>(mg_sub_raw);
@@ -839,7 +896,8 @@ template <typename T, int D>
 __global__ void __launch_bounds__(MG_TPB) k_pcg_spmv_dot(pict_domain_t dom, pict_mg_level_t L, const T* __restrict__ z,
                                                          const T* __restrict__ pold, T* __restrict__ pnew,
                                                          T* __restrict__ q, const double* __restrict__ sc, int first,
-                                                         double* __restrict__ part) {
+                                                         double* __restrict__ part, const T* __restrict__ r) {
+    mg_pdl_entry();
     const T* __restrict__ coef = reinterpret_cast<const T*>(L.coef);
     const int N = L.num_cells;
     const MgTile tl = mg_tile(dom.tiles, blockIdx.x);
@@ -847,7 +905,7 @@ __global__ void __launch_bounds__(MG_TPB) k_pcg_spmv_dot(pict_domain_t dom, pict
     const MgBlock B = mg_block(L, tl.blk);
     const T m = (T)sc[MG_SC * tl.sys + 4];
     const T bt = first ? T(0) : (T)sc[MG_SC * tl.sys + 2];
-    double acc = 0.0;
+    double acc = 0.0, arq = 0.0, aqq = 0.0;
     for (int base = 0; base < tl.cnt; base += MG_PASS) {
         T pv[MG_CPT], qv[MG_CPT];
 #pragma unroll
@@ -877,11 +935,21 @@ __global__ void __launch_bounds__(MG_TPB) k_pcg_spmv_dot(pict_domain_t dom, pict
             if (l >= tl.cnt) continue;
             pnew[tl.s0 + l] = pv[k];
             q[tl.s0 + l] = qv[k];
-            acc += (double)pv[k] * (double)qv[k];
+            const double qd = (double)qv[k];
+            acc += (double)pv[k] * qd;
+            arq += (double)r[tl.s0 + l] * qd;
+            aqq += qd * qd;
         }
     }
     acc = mg_warp_sum(acc);
-    if ((threadIdx.x & 31) == 0) *mg_warp_part(part, 1) = acc;
+    arq = mg_warp_sum(arq);
+    aqq = mg_warp_sum(aqq);
+    if ((threadIdx.x & 31) == 0) {
+        double* P = mg_warp_part(part, 3);
+        P[0] = acc;
+        P[1] = arq;
+        P[2] = aqq;
+    }
 }
 
 // k_pcg_spmv_dot for 2D tiles with its operands staged by asynchronous bulk copies: a persistent grid
@@ -901,7 +969,8 @@ __global__ void __launch_bounds__(MG_TPB) k_pcg_spmv_dot_bulk(pict_domain_t dom,
                                                               T* __restrict__ pnew, T* __restrict__ q,
                                                               const double* __restrict__ sc, int first,
                                                               double* __restrict__ part, int cap_h, int cap_t,
-                                                              int* __restrict__ err) {
+                                                              int* __restrict__ err, const T* __restrict__ r) {
+    mg_pdl_entry();
     constexpr int K = 5;
     extern __shared__ __align__(128) unsigned char mg_bulk_raw[];
     __shared__ __align__(8) uint64_t bar[2];
@@ -1000,7 +1069,7 @@ __global__ void __launch_bounds__(MG_TPB) k_pcg_spmv_dot_bulk(pict_domain_t dom,
         const T* const c2 = buf + 2 * cap_h + 2 * cap_t + R.c[2].lead;
         const T* const c3 = buf + 2 * cap_h + 3 * cap_t + R.c[3].lead;
         const T* const c4 = buf + 2 * cap_h + 4 * cap_t + R.c[4].lead;
-        double acc = 0.0;
+        double acc = 0.0, arq = 0.0, aqq = 0.0;
         for (int base = 0; base < tl.cnt; base += MG_PASS) {
             T pvk[MG_CPT], qvk[MG_CPT];
 #pragma unroll
@@ -1057,11 +1126,21 @@ __global__ void __launch_bounds__(MG_TPB) k_pcg_spmv_dot_bulk(pict_domain_t dom,
                 if (l >= tl.cnt) continue;
                 pnew[tl.s0 + l] = pvk[kk];
                 q[tl.s0 + l] = qvk[kk];
-                acc += (double)pvk[kk] * (double)qvk[kk];
+                const double qd = (double)qvk[kk];
+                acc += (double)pvk[kk] * qd;
+                arq += (double)r[tl.s0 + l] * qd;
+                aqq += qd * qd;
             }
         }
         acc = mg_warp_sum(acc);
-        if ((threadIdx.x & 31) == 0) part[(size_t)t * MG_NW + (threadIdx.x >> 5)] = acc;
+        arq = mg_warp_sum(arq);
+        aqq = mg_warp_sum(aqq);
+        if ((threadIdx.x & 31) == 0) {
+            double* P = part + ((size_t)t * MG_NW + (threadIdx.x >> 5)) * 3;
+            P[0] = acc;
+            P[1] = arq;
+            P[2] = aqq;
+        }
         __syncthreads();  // stage buffer b is free for the tile after next
     }
 }
@@ -1070,6 +1149,7 @@ __global__ void __launch_bounds__(MG_TPB) k_pcg_spmv_dot_bulk(pict_domain_t dom,
 template <typename T>
 __global__ void __launch_bounds__(MG_TPB) k_pcg_dot4(pict_domain_t dom, const T* r, const T* z, double* part,
                                                      const double* __restrict__ dn) {
+    mg_pdl_entry();
     const MgTile tl = mg_tile(dom.tiles, blockIdx.x);
     if (mg_done(dn, tl.sys)) return;
     double a = 0.0, c = 0.0, sz = 0.0, sr = 0.0;
@@ -1103,11 +1183,15 @@ __global__ void __launch_bounds__(MG_TPB) k_pcg_dot4(pict_domain_t dom, const T*
 template <int STRIDE>
 __global__ void k_pcg_scalars(pict_domain_t dom, const double* __restrict__ part, int stage, double* sc, int it,
                               double tol, int normalized, const int* __restrict__ ctr) {
+    mg_pdl_entry();
     if (ctr) it += *ctr;
     const int lane = threadIdx.x & 31;
     const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (s >= dom.num_sims) return;
-    if (stage != 0 && sc[MG_SC * s + 5] != 0.0) return;  // converged earlier: keep its scalars
+    if (stage != 0 && sc[MG_SC * s + 5] != 0.0) {  // converged earlier: keep its scalars
+        if (stage == 2 && lane == 0) sc[MG_SC * s + 6] = 0.0;  // its last update has been applied
+        return;
+    }
     double v[4] = {0.0, 0.0, 0.0, 0.0}, u[STRIDE];
 #pragma unroll
     for (int k = 0; k < STRIDE; ++k) u[k] = 0.0;
@@ -1133,12 +1217,24 @@ __global__ void k_pcg_scalars(pict_domain_t dom, const double* __restrict__ part
         for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
     if (lane != 0) return;
     double* S = sc + MG_SC * s;
+    const int n = dom.sim_cells[s + 1] - dom.sim_cells[s];
     if (stage == 1) {
+        // alpha from p.q; with STRIDE 3 also |r - alpha q|^2 = |r|^2 - 2 alpha r.q + alpha^2 q.q: a system that
+        // meets the tolerance here is done after this iteration's update (its V-cycle is skipped)
         const double a = v[0];
-        S[1] = (a != 0.0 && S[0] != 0.0 && isfinite(a)) ? S[0] / a : 0.0;
+        const double al = (a != 0.0 && S[0] != 0.0 && isfinite(a)) ? S[0] / a : 0.0;
+        S[1] = al;
+        if (STRIDE >= 3) {
+            const double r2 = fmax(S[3] - 2.0 * al * v[1] + al * al * v[2], 0.0);
+            const double crit1 = normalized ? sqrt(r2) / sqrt((double)n) : sqrt(r2);
+            if (crit1 < tol) {
+                S[3] = r2;
+                S[5] = (double)(it + 2);
+                S[6] = 1.0;
+            }
+        }
         return;
     }
-    const int n = dom.sim_cells[s + 1] - dom.sim_cells[s];
     const double m = v[2] / (double)n;
     const double rho = v[0] - m * v[3];
     if (stage == 0) {
@@ -1162,8 +1258,9 @@ __global__ void __launch_bounds__(MG_TPB) k_pcg_update(pict_domain_t dom, const 
                                                        const T* __restrict__ q, T* __restrict__ rn, T* __restrict__ x,
                                                        const T* __restrict__ p, const double* __restrict__ sc, int first,
                                                        double* __restrict__ part) {
+    mg_pdl_entry();
     const MgTile tl = mg_tile(dom.tiles, blockIdx.x);
-    if (mg_done(sc, tl.sys)) return;
+    if (mg_done(sc, tl.sys) && !mg_pending(sc, tl.sys)) return;
     const T al = (T)sc[MG_SC * tl.sys + 1];
     double c2 = 0.0, sr = 0.0;
     for (int l = threadIdx.x; l < tl.cnt; l += MG_TPB) {
@@ -1187,6 +1284,7 @@ __global__ void __launch_bounds__(MG_TPB) k_pcg_update(pict_domain_t dom, const 
 
 __global__ void k_pcg_report(pict_domain_t dom, const double* sc, pict_solve_info_t* info, int iterations, double tol,
                              int normalized, const int* err) {
+    mg_pdl_entry();
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= dom.num_sims) return;
     const int n = dom.sim_cells[s + 1] - dom.sim_cells[s];
@@ -1209,6 +1307,7 @@ __global__ void k_pcg_report(pict_domain_t dom, const double* sc, pict_solve_inf
 // while a system is still iterating and the next two iterations (ctr, ctr + 1) are within the cap.
 __global__ void k_pcg_loop_cond(pict_domain_t dom, const double* __restrict__ sc, int* ctr, int init, int step,
                                 int limit, cudaGraphConditionalHandle h) {
+    mg_pdl_entry();
     __shared__ int s_any;
     if (threadIdx.x == 0) s_any = 0;
     __syncthreads();
@@ -1340,30 +1439,30 @@ static pict_status_t run_pcg_mg(const pict_domain_t* dom, const pict_mg_level_t*
     auto vcycle = [&](const T* r, bool upd, T* rn, const T* p, int first, cudaStream_t st) -> pict_status_t {
         const T* rnew = upd ? rn : r;
         if (lc == 0) {
-            if (upd) k_pcg_update<T><<<nt, MG_TPB, 0, st>>>(*dom, r, q, rn, xout, p, sc, first, part);
-            k_mg_subcycle<T, D><<<levels[0].num_blocks, MG_SUB_THREADS, sub_smem, st>>>(sub, rnew, z, wj, sp,
+            if (upd) mg_launch(k_pcg_update<T>, nt, MG_TPB, 0, st, *dom, r, q, rn, xout, p, sc, first, part);
+            mg_launch(k_mg_subcycle<T, D>, levels[0].num_blocks, MG_SUB_THREADS, sub_smem, st, sub, rnew, z, wj, sp,
                                                                                      coarse_sweeps, sc, nu_sub);
-            k_pcg_dot4<T><<<nt, MG_TPB, 0, st>>>(*dom, rnew, z, part, sc);
+            mg_launch(k_pcg_dot4<T>, nt, MG_TPB, 0, st, *dom, rnew, z, part, sc);
             return check_launch("pcg_mg vcycle");
         }
         for (int l = 0; l < lc; ++l) {
             const pict_mg_level_t& F = levels[l];
             const pict_mg_level_t& C = levels[l + 1];
             if (l == 0 && upd)
-                k_mg_restrict<T, D, true><<<C.num_tiles, MG_TPB, stage3, st>>>(F, C, r, q, rn, xout, p, sc, first,
+                mg_launch(k_mg_restrict<T, D, true>, C.num_tiles, MG_TPB, stage3, st, F, C, r, q, rn, xout, p, sc, first,
                                                                                 lb[1], wj, cap, sc, nu[0]);
             else
-                k_mg_restrict<T, D, false><<<C.num_tiles, MG_TPB, stage3, st>>>(
+                mg_launch(k_mg_restrict<T, D, false>, C.num_tiles, MG_TPB, stage3, st, 
                     F, C, l == 0 ? r : lb[l], nullptr, nullptr, nullptr, nullptr, nullptr, 0, lb[l + 1], wj, cap, sc,
                     nu[l]);
         }
         // levels lc.. in one launch (one CTA per block)
-        k_mg_subcycle<T, D><<<levels[lc].num_blocks, MG_SUB_THREADS, sub_smem, st>>>(sub, lb[lc], lx[lc], wj, sp,
+        mg_launch(k_mg_subcycle<T, D>, levels[lc].num_blocks, MG_SUB_THREADS, sub_smem, st, sub, lb[lc], lx[lc], wj, sp,
                                                                                   coarse_sweeps, sc, nu_sub);
         for (int l = lc - 1; l >= 1; --l)
-            k_mg_prolong<T, D, false><<<levels[l].num_tiles, MG_TPB, stage3, st>>>(
+            mg_launch(k_mg_prolong<T, D, false>, levels[l].num_tiles, MG_TPB, stage3, st, 
                 levels[l], levels[l + 1], levels[l].tiles, lb[l], lx[l + 1], lx[l], sp, wj, nullptr, cap, sc, nu[l]);
-        k_mg_prolong<T, D, true><<<nt, MG_TPB, stage3, st>>>(levels[0], levels[1], dom->tiles, rnew, lx[1], z, sp, wj,
+        mg_launch(k_mg_prolong<T, D, true>, nt, MG_TPB, stage3, st, levels[0], levels[1], dom->tiles, rnew, lx[1], z, sp, wj,
                                                              part, cap, sc, nu[0]);
         return check_launch("pcg_mg vcycle");
     };
@@ -1396,7 +1495,7 @@ static pict_status_t run_pcg_mg(const pict_domain_t* dom, const pict_mg_level_t*
         return check_launch("pcg_mg initial state");
     pict_status_t s = vcycle(rhs, false, nullptr, nullptr, 0, st);
     if (s) return s;
-    k_pcg_scalars<4><<<swg, 128, 0, st>>>(*dom, part, 0, sc, 0, tol, normalized, nullptr);
+    mg_launch(k_pcg_scalars<4>, swg, 128, 0, st, *dom, part, 0, sc, 0, tol, normalized, nullptr);
     // one PCG iteration; it >= 0: iteration `it` with its buffers and reports fixed at launch (the last one
     // only updates); it < 0: an iteration of the graph loop with buffer parity `par`, its number read from the
     // device counter plus `off`
@@ -1411,19 +1510,19 @@ static pict_status_t run_pcg_mg(const pict_domain_t* dom, const pict_mg_level_t*
         const int* c = fixed ? nullptr : ctr;
         const int itv = fixed ? it : off;
         if (bulk_grid > 0)
-            k_pcg_spmv_dot_bulk<T><<<bulk_grid, MG_TPB, bulk_smem, st>>>(*dom, levels[0], z, pold, pnew, q, sc, first,
-                                                                         part, cap_h, cap_t, err);
+            mg_launch(k_pcg_spmv_dot_bulk<T>, bulk_grid, MG_TPB, bulk_smem, st, *dom, levels[0], z, pold, pnew, q, sc, first,
+                                                                         part, cap_h, cap_t, err, r);
         else
-            k_pcg_spmv_dot<T, D><<<nt, MG_TPB, 0, st>>>(*dom, levels[0], z, pold, pnew, q, sc, first, part);
-        k_pcg_scalars<1><<<swg, 128, 0, st>>>(*dom, part, 1, sc, itv, tol, normalized, c);
+            mg_launch(k_pcg_spmv_dot<T, D>, nt, MG_TPB, 0, st, *dom, levels[0], z, pold, pnew, q, sc, first, part, r);
+        mg_launch(k_pcg_scalars<3>, swg, 128, 0, st, *dom, part, 1, sc, itv, tol, normalized, c);
         if (!fixed || it + 1 < iterations) {
             pict_status_t e = vcycle(r, true, rn, pnew, first, st);
             if (e) return e;
         } else {
             // last iteration: only the update and |r|^2 (r.z and sum(z) are not used)
-            k_pcg_update<T><<<nt, MG_TPB, 0, st>>>(*dom, r, q, rn, xout, pnew, sc, first, part);
+            mg_launch(k_pcg_update<T>, nt, MG_TPB, 0, st, *dom, r, q, rn, xout, pnew, sc, first, part);
         }
-        k_pcg_scalars<4><<<swg, 128, 0, st>>>(*dom, part, 2, sc, itv, tol, normalized, c);
+        mg_launch(k_pcg_scalars<4>, swg, 128, 0, st, *dom, part, 2, sc, itv, tol, normalized, c);
         return check_launch("pcg_mg iteration");
     };
     // under stream capture: iteration 0, then iterations (1, 2), (3, 4), ... as the body of a conditional
@@ -1451,7 +1550,7 @@ static pict_status_t run_pcg_mg(const pict_domain_t* dom, const pict_mg_level_t*
         if (cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps) != cudaSuccess ||
             cudaGraphConditionalHandleCreate(&h, graph, 0, 0) != cudaSuccess)
             return check_launch("pcg_mg conditional handle");
-        k_pcg_loop_cond<<<1, 256, 0, st>>>(*dom, sc, ctr, 1, 0, iterations, h);
+        mg_launch(k_pcg_loop_cond, 1, 256, 0, st, *dom, sc, ctr, 1, 0, iterations, h);
         if ((s = check_launch("pcg_mg loop condition"))) return s;
         if (cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps) != cudaSuccess)
             return check_launch("pcg_mg capture info");
@@ -1470,7 +1569,7 @@ static pict_status_t run_pcg_mg(const pict_domain_t* dom, const pict_mg_level_t*
         pict_status_t sb = iteration(-1, 1, 0, bs);
         if (!sb) sb = iteration(-1, 0, 1, bs);
         if (!sb) {
-            k_pcg_loop_cond<<<1, 256, 0, bs>>>(*dom, sc, ctr, 0, 2, iterations, h);
+            mg_launch(k_pcg_loop_cond, 1, 256, 0, bs, *dom, sc, ctr, 0, 2, iterations, h);
             sb = check_launch("pcg_mg loop condition");
         }
         cudaGraph_t body = nullptr;
@@ -1482,7 +1581,7 @@ static pict_status_t run_pcg_mg(const pict_domain_t* dom, const pict_mg_level_t*
         if ((iterations - 1) % 2 == 1)
             if ((s = iteration(iterations - 1, (iterations - 1) & 1, 0, st))) return s;
     }
-    k_pcg_report<<<sg, 128, 0, st>>>(*dom, sc, info, iterations, tol, normalized, err);
+    mg_launch(k_pcg_report, sg, 128, 0, st, *dom, sc, info, iterations, tol, normalized, err);
     return check_launch("pcg_mg");
 }
 
@@ -1495,6 +1594,7 @@ extern "C" {
 void pict_mg_set_bulk_staging(int32_t enable) { g_mg_bulk = enable ? 1 : 0; }
 void pict_mg_set_smoothing_sweeps(int32_t sweeps) { g_mg_sweeps = sweeps >= 2 ? 2 : 1; }
 void pict_mg_set_graph_loop(int32_t enable) { g_mg_graph_loop = enable ? 1 : 0; }
+void pict_mg_set_dependent_launch(int32_t enable) { g_mg_pdl = enable ? 1 : 0; }
 
 pict_status_t pict_mg_galerkin(const pict_mg_level_t* fine, const pict_mg_level_t* coarse, void* stream) {
     if (!fine || !coarse || !fine->coef || !coarse->coef || !fine->blocks || !coarse->blocks || !coarse->cell_block)
