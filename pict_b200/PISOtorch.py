@@ -2017,11 +2017,12 @@ def CorrectVelocity(domain, timeStep, version=0, timeStepNorm=False):
     """u = H/A - grad(p)/A (extensions/PISO_multiblock_cuda_kernel.cu:6163-6201).  version 0/1: finite-difference
     pressure gradient (:5947-5980); 4: mean of the two face fluxes with orthogonal metrics (:6053-6160,
     always scaled by the time step); 5 / 6: finite-volume pressure gradient from interpolated cell
-    fluxes / staggered face transforms (:6013-6050).  Versions 2 and 3 are the reference's smoothing
-    kernels, which it marks as not to be used; they are rejected."""
+    fluxes / staggered face transforms (:6013-6050).  Every other number, including 2 and 3 (the
+    reference's smoothing kernels, which it marks as not to be used and does not dispatch), takes the
+    reference's default branch: the finite-difference corrector of version 1."""
     version = int(version)
-    if version not in (0, 1, 4, 5, 6):
-        raise NotImplementedError("CorrectVelocity: version %d is not implemented in pict_b200 (0/1, 4, 5, 6 are)" % version)
+    if version not in (4, 5, 6):
+        version = 1
     domain._check_ready()
     if version in (5, 6):
         for b in domain.getBlocks():

@@ -62,8 +62,7 @@ __global__ void __launch_bounds__(256, 6) k_adv_setup(pict_domain_t dom, double 
     T* C = reinterpret_cast<T*>(dom.C);
     T* A = reinterpret_cast<T*>(dom.A);
     T* vrhs = reinterpret_cast<T*>(dom.velocity_rhs);
-    PICT_CELL_LOOP(i, N) {
-        const int b = dom.cell_block[i];
+    for_each_cell(dom, [&](const int i, const int b) {
         const pict_block_t& B = dom.blocks[b];
         const int l = i - B.offset;
         const int nc = B.size[0] * B.size[1] * B.size[2];
@@ -137,7 +136,7 @@ __global__ void __launch_bounds__(256, 6) k_adv_setup(pict_domain_t dom, double 
             }
         }
         (void)K;
-    }
+    });
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -152,8 +151,7 @@ __global__ void __launch_bounds__(256, 6) k_pressure_setup(pict_domain_t dom, do
     T* P = reinterpret_cast<T*>(dom.P);
     const T* vres = reinterpret_cast<const T*>(dom.velocity_result);
     T* prhs = reinterpret_cast<T*>(dom.pressure_rhs);
-    PICT_CELL_LOOP(i, N) {
-        const int b = dom.cell_block[i];
+    for_each_cell(dom, [&](const int i, const int b) {
         const pict_block_t& B = dom.blocks[b];
         const int l = i - B.offset;
         const int nc = B.size[0] * B.size[1] * B.size[2];
@@ -215,7 +213,7 @@ __global__ void __launch_bounds__(256, 6) k_pressure_setup(pict_domain_t dom, do
                 prhs[(size_t)c * N + i] = raP * (u[c] / dt - H[c] + s);
             }
         }
-    }
+    });
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -226,8 +224,7 @@ __global__ void __launch_bounds__(256, 6) k_pressure_setup(pict_domain_t dom, do
 template <typename T, int D, bool SRC_GLOBAL>
 __global__ void k_flux_divergence(pict_domain_t dom, const T* field, T* out, double dt_arg, int time_step_norm) {
     const int N = dom.num_cells;
-    PICT_CELL_LOOP(i, N) {
-        const int b = dom.cell_block[i];
+    for_each_cell(dom, [&](const int i, const int b) {
         const pict_block_t& B = dom.blocks[b];
         const int l = i - B.offset;
         int p[3];
@@ -257,7 +254,7 @@ __global__ void k_flux_divergence(pict_domain_t dom, const T* field, T* out, dou
         }
         if (time_step_norm) div /= sim_time_step<T>(dom, B.sim, dt_arg);
         out[i] = div;
-    }
+    });
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -352,8 +349,7 @@ __global__ void k_correct_velocity(pict_domain_t dom, double dt_arg, int time_st
     const T* A = reinterpret_cast<const T*>(dom.A);
     const T* prhs = reinterpret_cast<const T*>(dom.pressure_rhs);
     T* vres = reinterpret_cast<T*>(dom.velocity_result);
-    PICT_CELL_LOOP(i, N) {
-        const int b = dom.cell_block[i];
+    for_each_cell(dom, [&](const int i, const int b) {
         const pict_block_t& B = dom.blocks[b];
         const int l = i - B.offset;
         const int nc = B.size[0] * B.size[1] * B.size[2];
@@ -374,7 +370,7 @@ __global__ void k_correct_velocity(pict_domain_t dom, double dt_arg, int time_st
             vres[(size_t)c * N + i] = v;
             if (write_block) ub[(size_t)c * nc + l] = v;
         }
-    }
+    });
 }
 
 // Version 4 (PISO_update_velocity_v4_orthogonal, extensions/PISO_multiblock_cuda_kernel.cu:6053-6160): per axis the mean of
@@ -388,8 +384,7 @@ __global__ void k_correct_velocity_v4(pict_domain_t dom, double dt_arg, int writ
     const T* A = reinterpret_cast<const T*>(dom.A);
     const T* prhs = reinterpret_cast<const T*>(dom.pressure_rhs);
     T* vres = reinterpret_cast<T*>(dom.velocity_result);
-    PICT_CELL_LOOP(i, N) {
-        const int b = dom.cell_block[i];
+    for_each_cell(dom, [&](const int i, const int b) {
         const pict_block_t& B = dom.blocks[b];
         const int l = i - B.offset;
         const int nc = B.size[0] * B.size[1] * B.size[2];
@@ -425,7 +420,7 @@ __global__ void k_correct_velocity_v4(pict_domain_t dom, double dt_arg, int writ
             vres[(size_t)d * N + i] = v;
             if (write_block) ub[(size_t)d * nc + l] = v;
         }
-    }
+    });
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -436,8 +431,8 @@ template <typename T, bool TO_BLOCKS, bool VECTOR>
 __global__ void k_copy_result(pict_domain_t dom, int D) {
     const int N = dom.num_cells;
     T* g = reinterpret_cast<T*>(VECTOR ? dom.velocity_result : dom.pressure_result);
-    PICT_CELL_LOOP(i, N) {
-        const pict_block_t& B = dom.blocks[dom.cell_block[i]];
+    for_each_cell(dom, [&](const int i, const int b) {
+        const pict_block_t& B = dom.blocks[b];
         const int l = i - B.offset;
         const int nc = B.size[0] * B.size[1] * B.size[2];
         T* bf = reinterpret_cast<T*>(VECTOR ? B.velocity : B.pressure);
@@ -446,7 +441,7 @@ __global__ void k_copy_result(pict_domain_t dom, int D) {
             if (TO_BLOCKS) bf[(size_t)c * nc + l] = g[(size_t)c * N + i];
             else g[(size_t)c * N + i] = bf[(size_t)c * nc + l];
         }
-    }
+    });
 }
 
 // Initial guess of the advection solve from the previous step's increment: velocityResult = u + incr
@@ -455,8 +450,8 @@ template <typename T, bool SUB>
 __global__ void k_advection_increment(pict_domain_t dom, int D, T* __restrict__ incr) {
     const int N = dom.num_cells;
     T* g = reinterpret_cast<T*>(dom.velocity_result);
-    PICT_CELL_LOOP(i, N) {
-        const pict_block_t& B = dom.blocks[dom.cell_block[i]];
+    for_each_cell(dom, [&](const int i, const int b) {
+        const pict_block_t& B = dom.blocks[b];
         const int l = i - B.offset;
         const int nc = B.size[0] * B.size[1] * B.size[2];
         const T* bf = reinterpret_cast<const T*>(B.velocity);
@@ -466,7 +461,7 @@ __global__ void k_advection_increment(pict_domain_t dom, int D, T* __restrict__ 
             if (SUB) incr[k] = g[k] - u;
             else g[k] = u + incr[k];
         }
-    }
+    });
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -699,7 +694,7 @@ __global__ void k_csr_to_stencil(pict_domain_t dom, const T* val, const int32_t*
 
 template <typename T, int D>
 static pict_status_t launch_adv(const pict_domain_t* dom, double dt, bool matrix, bool rhs, int pgrad, cudaStream_t st) {
-    const int grid = cell_grid(dom->num_cells, 256);
+    const int grid = domain_grid(dom, 256);
     if (matrix && rhs) k_adv_setup<T, D, true, true><<<grid, 256, 0, st>>>(*dom, dt, pgrad);
     else if (matrix) k_adv_setup<T, D, true, false><<<grid, 256, 0, st>>>(*dom, dt, pgrad);
     else k_adv_setup<T, D, false, true><<<grid, 256, 0, st>>>(*dom, dt, pgrad);
@@ -709,7 +704,7 @@ static pict_status_t launch_adv(const pict_domain_t* dom, double dt, bool matrix
 template <typename T, int D>
 static pict_status_t launch_pressure(const pict_domain_t* dom, double dt, bool matrix, bool rhs, bool div,
                                      int tsn, cudaStream_t st) {
-    const int grid = cell_grid(dom->num_cells, 256);
+    const int grid = domain_grid(dom, 256);
     if (matrix && rhs) k_pressure_setup<T, D, true, true><<<grid, 256, 0, st>>>(*dom, dt);
     else if (matrix) k_pressure_setup<T, D, true, false><<<grid, 256, 0, st>>>(*dom, dt);
     else if (rhs) k_pressure_setup<T, D, false, true><<<grid, 256, 0, st>>>(*dom, dt);
@@ -826,7 +821,7 @@ pict_status_t pict_setup_pressure_correction(const pict_domain_t* dom, double dt
 
 template <typename T, int D>
 static pict_status_t launch_correct(const pict_domain_t* dom, double dt, int version, int tsn, int wb, cudaStream_t st) {
-    const int grid = cell_grid(dom->num_cells, 256);
+    const int grid = domain_grid(dom, 256);
     switch (version) {
         case 4: k_correct_velocity_v4<T, D><<<grid, 256, 0, st>>>(*dom, dt, wb); break;
         case 5: k_correct_velocity<T, D, 0><<<grid, 256, 0, st>>>(*dom, dt, tsn, wb); break;
@@ -838,7 +833,7 @@ static pict_status_t launch_correct(const pict_domain_t* dom, double dt, int ver
 
 template <typename T, int D>
 static pict_status_t launch_increment(const pict_domain_t* dom, int sub, void* incr, cudaStream_t st) {
-    const int grid = cell_grid(dom->num_cells, 256);
+    const int grid = domain_grid(dom, 256);
     if (sub) k_advection_increment<T, true><<<grid, 256, 0, st>>>(*dom, D, reinterpret_cast<T*>(incr));
     else k_advection_increment<T, false><<<grid, 256, 0, st>>>(*dom, D, reinterpret_cast<T*>(incr));
     return check_launch("advection increment");
@@ -846,7 +841,7 @@ static pict_status_t launch_increment(const pict_domain_t* dom, int sub, void* i
 
 template <typename T, int D>
 static pict_status_t launch_copy(const pict_domain_t* dom, int which, cudaStream_t st) {
-    const int grid = cell_grid(dom->num_cells, 256);
+    const int grid = domain_grid(dom, 256);
     switch (which) {
         case 0: k_copy_result<T, true, true><<<grid, 256, 0, st>>>(*dom, D); break;
         case 1: k_copy_result<T, false, true><<<grid, 256, 0, st>>>(*dom, D); break;
@@ -858,7 +853,7 @@ static pict_status_t launch_copy(const pict_domain_t* dom, int which, cudaStream
 
 template <typename T, int D>
 static pict_status_t launch_vel_div(const pict_domain_t* dom, void* out, cudaStream_t st) {
-    k_flux_divergence<T, D, false><<<cell_grid(dom->num_cells, 256), 256, 0, st>>>(*dom, nullptr,
+    k_flux_divergence<T, D, false><<<domain_grid(dom, 256), 256, 0, st>>>(*dom, nullptr,
                                                                                   reinterpret_cast<T*>(out), 1.0, 0);
     return check_launch("velocity_divergence");
 }

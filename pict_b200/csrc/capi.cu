@@ -43,6 +43,13 @@ int cell_grid(int n, int threads) {
     return g;
 }
 
+int domain_grid(const pict_domain_t* dom, int threads) {
+    if (!dom->tiles || dom->num_tiles <= 0 || dom->tile_cells <= 0) return cell_grid(dom->num_cells, threads);
+    const long long total = (long long)dom->num_tiles * ((dom->tile_cells + threads - 1) / threads);
+    const long long cap = (long long)device_sm_count() * 16;
+    return (int)(total < cap ? (total < 1 ? 1 : total) : cap);
+}
+
 }  // namespace pict
 
 extern "C" {

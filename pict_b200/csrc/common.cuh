@@ -127,15 +127,25 @@ struct Nbr {
     int back;   // face of the neighbour pointing back to this cell
 };
 
+// A cell that is not on face f of its block has its neighbour inside the block at l +- stride of
+// the face's axis (the table holds the same index there), so the table is read on block faces only.
 __device__ __forceinline__ Nbr neighbour(const pict_domain_t& dom, const pict_block_t& B, int b, const int* p,
                                          int i, int f) {
     Nbr n;
-    n.j = dom.nbr[(size_t)f * dom.num_cells + i];
     n.b = b;
     n.comp = f >> 1;
     n.flip = 1;
     n.back = f ^ 1;
-    if (n.j >= 0 && at_face(p, B.size, f) && B.face[f].type == PICT_FACE_CONNECTED) {
+    if (!at_face(p, B.size, f)) {
+        const int a = f >> 1;
+        const int stride = a == 0 ? 1 : (a == 1 ? B.size[0] : B.size[0] * B.size[1]);
+        const int s = (f & 1) ? stride : -stride;
+        n.j = i + s;
+        n.l = i - B.offset + s;
+        return n;
+    }
+    n.j = dom.nbr[(size_t)f * dom.num_cells + i];
+    if (n.j >= 0 && B.face[f].type == PICT_FACE_CONNECTED) {
         const pict_face_t& F = B.face[f];
         n.b = F.conn_block;
         n.comp = F.conn_axes[0] >> 1;
@@ -193,5 +203,28 @@ __device__ __forceinline__ void load_global_vec(const T* v, int N, int j, T* u) 
 
 // grid-stride loop helper
 #define PICT_CELL_LOOP(i, N) for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < (N); i += blockDim.x * gridDim.x)
+
+// Per-cell loop over a domain, f(i, b) with i the global cell and b its block.  With the domain's work
+// tiles (runs of at most tile_cells cells of one block, covering every cell once) the grid strides over
+// (tile, chunk of blockDim cells) pairs, so a CTA's block index is one uniform load of the tile instead
+// of a per-cell read of cell_block that every other load of the cell waits for; without tiles, a
+// grid-stride loop over the cells.  The host sizes the grid with domain_grid().
+template <typename F>
+__device__ __forceinline__ void for_each_cell(const pict_domain_t& dom, F&& f) {
+    if (dom.tiles != nullptr && dom.num_tiles > 0 && dom.tile_cells > 0) {
+        const int4* tl = reinterpret_cast<const int4*>(dom.tiles);
+        const int per = (dom.tile_cells + blockDim.x - 1) / blockDim.x;
+        const int total = dom.num_tiles * per;
+        for (int v = blockIdx.x; v < total; v += gridDim.x) {
+            const int t = v / per;
+            const int4 d = tl[t];  // system, block, first cell, cell count
+            const int k = (v - t * per) * blockDim.x + threadIdx.x;
+            if (k < d.w) f(d.z + k, d.y);
+        }
+    } else {
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < dom.num_cells; i += blockDim.x * gridDim.x)
+            f(i, dom.cell_block[i]);
+    }
+}
 
 }  // namespace pict

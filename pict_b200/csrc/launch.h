@@ -14,6 +14,9 @@ pict_status_t check_launch(const char* what);
 int device_sm_count();
 // grid for a grid-stride per-cell kernel: enough CTAs to cover N, capped at a few waves
 int cell_grid(int n, int threads);
+// grid for a kernel that walks a domain's cells with for_each_cell (common.cuh): one CTA per chunk of
+// `threads` cells of a work tile when the domain carries tiles, capped like cell_grid
+int domain_grid(const pict_domain_t* dom, int threads);
 // Non-orthogonal terms (nonortho.cu), added after the orthogonal kernel of an operator:
 // what 0 advection matrix (C, A), 1 velocity RHS, 2 pressure matrix, 3 pressure RHS divergence.
 // Returns PICT_OK without launching when `flags` selects no term of that operator.

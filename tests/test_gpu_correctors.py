@@ -63,8 +63,19 @@ def test_corrector_version_checks():
     from setups import build_product, case
     pd = build_product(case("distorted2d"), torch.float64)
     ts = torch.tensor([0.05], dtype=torch.float64)
-    with pytest.raises(NotImplementedError):
-        P.CorrectVelocity(pd, ts, version=2)
+    # numbers other than 4, 5, 6 take the reference's default branch, the finite-difference corrector
+    g = torch.Generator(device="cpu").manual_seed(3)
+    for b in pd.getBlocks():
+        b.setPressure(torch.randn(b.pressure.shape, generator=g, dtype=torch.float64).cuda())
+    N, D = pd.getTotalSize(), pd.getSpatialDims()
+    pd.setA(1 + torch.rand(N, generator=g, dtype=torch.float64).cuda())
+    pd.setPressureRHS(torch.randn(D * N, generator=g, dtype=torch.float64).cuda())
+    pd.UpdateDomainData()
+    P.CorrectVelocity(pd, ts, version=1)
+    u1 = pd.velocityResult.clone()
+    for v in (2, 3, 7):
+        P.CorrectVelocity(pd, ts, version=v)
+        assert torch.isfinite(u1).all() and torch.equal(pd.velocityResult, u1)
     b = pd.getBlock(0)
     b.setTransform(b.transform, None)  # drop the face transforms
     pd.UpdateDomainData()
