@@ -17,8 +17,9 @@ operators of ``libpict_b200`` (adjoint.cu) plus two transposed Krylov solves:
 Gradients with respect to the simulation parameters accumulate over all steps: per-cell viscosity
 (reduced to the system / block viscosity), velocity source, boundary velocity of fixed faces.
 
-``rollout()`` keeps only every ``checkpoint_every``-th velocity during the forward pass and, in the
-backward pass, recomputes each window from its checkpoint with taping before reversing it.
+``rollout()`` keeps only every ``checkpoint_every``-th velocity during the forward pass, tapes the last
+window as it runs and, in the backward pass, reverses that window directly and recomputes each earlier
+window from its checkpoint with taping before reversing it.
 """
 from __future__ import annotations
 
@@ -58,7 +59,9 @@ class PISOAdjoint:
 
     ``adjoint_advection_tol`` / ``adjoint_pressure_tol`` default to the forward tolerances.  With
     ``use_graph = True`` the untaped forward steps of :func:`rollout` replay the stepper's captured
-    one-step CUDA graph.
+    one-step CUDA graph, and its backward pass replays CUDA graphs of the taped step into each slot of
+    the checkpoint window and of the adjoint step from it, captured on first use (like the stepper's
+    graph they hold the time step and the tolerances of their capture).
     """
 
     def __init__(self, stepper: PISOStepper, adjoint_advection_tol: Optional[float] = None,
@@ -162,6 +165,44 @@ class PISOAdjoint:
     def new_tape(self):
         return StepTape(self.N, self.D, self.K, self.nc, self.dtype, self.dev)
 
+    def tapes(self, n):
+        """The adjoint's own tapes for a checkpoint window of n steps (kept, so that the graphs captured
+        for a window slot keep their buffers)."""
+        pool = self.__dict__.setdefault("_tape_pool", [])
+        while len(pool) < n:
+            pool.append(self.new_tape())
+        return pool[:n]
+
+    # ------------------------------------------------------------------ graphed steps of the backward pass
+    def _capture(self, fn):
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            out = fn()
+        return g, out
+
+    def step_taped_graphed(self, slot: int, tape: StepTape):
+        """step_taped(tape) as a CUDA graph replay (captured on the first call for this slot).  Capturing
+        launches nothing, so the first call captures and then replays."""
+        graphs = self.__dict__.setdefault("_taped_graphs", {})
+        if slot not in graphs or graphs[slot][1] is not tape:
+            graphs[slot] = (self._capture(lambda: self.step_taped(tape))[0], tape)
+        graphs[slot][0].replay()
+
+    def backward_step_graphed(self, slot: int, tape: StepTape, ubar):
+        """backward_step(tape, ubar) as a CUDA graph replay with a fixed input buffer per slot; returns
+        dL/du^n in the graph's output buffer (valid until the next replay of this slot)."""
+        graphs = self.__dict__.setdefault("_back_graphs", {})
+        if slot not in graphs or graphs[slot][2] is not tape:
+            ub = torch.empty(self.D * self.N, dtype=self.dtype, device=self.dev)
+            ub.copy_(ubar)
+            g, out = self._capture(lambda: self.backward_step(tape, ub))
+            graphs[slot] = (g, ub, tape, out)
+        g, ub, _, out = graphs[slot]
+        ub.copy_(ubar)
+        g.replay()
+        return out
+
     def step_taped(self, tape: StepTape, time_step=None):
         st = self.st
         d = st.domain
@@ -173,9 +214,11 @@ class PISOAdjoint:
         check(lib.pict_setup_advection(desc, dt, s), "advection setup")
         tape.C.copy_(d.C.coef.reshape(-1))
         tape.A.copy_(d.A)
+        st._advection_guess(desc, s)  # the stepper's initial guess (its solves converge to the same tolerance)
         check(lib.pict_solve(desc, P._ptr(d.C.coef), P._ptr(d.velocityRHS), P._ptr(d.velocityResult),
                              ctypes.byref(st.adv_params), P._ptr(st.info_adv), P._ptr(st.ws), st.ws_bytes, s),
               "advection solve")
+        st._advection_increment(desc, s)
         tape.ustar.copy_(d.velocityResult)
         for k in range(self.nc):
             if k > 0:
@@ -287,10 +330,24 @@ class _Rollout(torch.autograd.Function):
         ckpt = {0: u0.detach().clone()}
         outs = []
         rec = sorted(set(int(r) for r in record))
-        one_step = st.replay if (getattr(adj, "use_graph", False) and st._graph is not None
-                                 and st._graph_steps == 1) else st.step
+        use_graph = getattr(adj, "use_graph", False) and st._graph is not None
+        one_step = st.replay if (use_graph and st._graph_steps == 1) else st.step
+        # the last checkpoint window is taped as it runs, so the backward pass reverses it without
+        # recomputing it (the taped step is the stepper's step plus the tape copies; domains with an
+        # advective outflow update, which the taped step leaves out, keep the recomputation)
+        w_last = ((steps - 1) // checkpoint_every) * checkpoint_every
+        tape_last = not st.outflow
+        graphed = use_graph and not getattr(adj, "check_solves", False)
+        tapes = adj.tapes(steps - w_last) if tape_last else None
         for t in range(1, steps + 1):
-            one_step()
+            if tape_last and t - 1 >= w_last:
+                slot = t - 1 - w_last
+                if graphed:
+                    adj.step_taped_graphed(slot, tapes[slot])
+                else:
+                    adj.step_taped(tapes[slot])
+            else:
+                one_step()
             if t % checkpoint_every == 0 and t < steps:
                 ckpt[t] = adj.velocity()
             if t in rec:
@@ -305,6 +362,9 @@ class _Rollout(torch.autograd.Function):
         ctx.ckpt = ckpt
         ctx.has_nu = nu is not None
         ctx.has_src = src is not None
+        # the tapes hold this pass's last window until another pass (or a recomputation) reuses them
+        ctx.tape_token = object() if tape_last else None
+        adj._tape_owner = ctx.tape_token
         return tuple(outs)
 
     @staticmethod
@@ -315,18 +375,34 @@ class _Rollout(torch.autograd.Function):
         gmap = {t: g for t, g in zip(rec, grads)}
         adj.zero_parameter_grads()
         ubar = torch.zeros(adj.D * adj.N, dtype=adj.dtype, device=adj.dev)
-        tapes = [adj.new_tape() for _ in range(min(K, steps))]
+        tapes = adj.tapes(min(K, steps))
+        # graphed: the taped and adjoint steps replay per-slot CUDA graphs (the solves' reports are then
+        # not read back between steps, so check_solves keeps the eager path)
+        graphed = (getattr(adj, "use_graph", False) and adj.st._graph is not None
+                   and not getattr(adj, "check_solves", False))
         starts = list(range(0, steps, K))
         for w0 in reversed(starts):
             w1 = min(w0 + K, steps)
-            adj.set_velocity(ctx.ckpt[w0])
-            for t in range(w0, w1):
-                adj.step_taped(tapes[t - w0])
+            taped = (w0 == starts[-1] and ctx.tape_token is not None
+                     and getattr(adj, "_tape_owner", None) is ctx.tape_token)
+            adj._tape_owner = None
+            if not taped:
+                adj.set_velocity(ctx.ckpt[w0])
+                for t in range(w0, w1):
+                    if graphed:
+                        adj.step_taped_graphed(t - w0, tapes[t - w0])
+                    else:
+                        adj.step_taped(tapes[t - w0])
             for t in reversed(range(w0, w1)):
                 g = gmap.get(t + 1)
                 if g is not None:
                     ubar = ubar + g.reshape(-1)
-                ubar = adj.backward_step(tapes[t - w0], ubar)
+                if graphed:
+                    ubar = adj.backward_step_graphed(t - w0, tapes[t - w0], ubar)
+                else:
+                    ubar = adj.backward_step(tapes[t - w0], ubar)
+        if graphed:
+            ubar = ubar.clone()  # the last replay's output buffer is reused by the next backward pass
         # the recomputation moved the domain state; restore the end of the forward pass
         adj.set_velocity(ctx.final[0])
         adj.set_pressure(ctx.final[1])
@@ -340,7 +416,8 @@ def rollout(adj: PISOAdjoint, u0, steps: int, record: Sequence[int], checkpoint_
     """Run `steps` PISO steps from the global velocity u0 [D*N] and return the velocities after the
     steps listed in `record` (tuple of [D*N] tensors), differentiable with respect to u0, the system
     viscosities nu [num_sims] (descriptor order) and a per-cell velocity source src [D*N].
-    The forward keeps every `checkpoint_every`-th velocity; the backward recomputes each window.
+    The forward keeps every `checkpoint_every`-th velocity and tapes the last window; the backward
+    recomputes each earlier window.
     The backward also adds the parameter gradients to the gradient tensors that are allocated on the
     domain (block viscosityGrad / velocitySourceGrad, boundary velocityGrad), and leaves the domain in
     the state at the end of the forward pass."""

@@ -124,6 +124,53 @@ def test_checkpointed_rollout_matches_stepwise_tape():
     assert torch.allclose(grads[0], grads[1], rtol=1e-10, atol=1e-14)
 
 
+def test_rollout_last_window_taped_or_recomputed():
+    """The forward pass tapes its last checkpoint window, which the backward pass then reverses without
+    recomputing it.  When another rollout reuses the tapes before the backward pass, that window is
+    recomputed from its checkpoint instead: same gradients either way, and the domain ends in the state
+    at the end of its own forward pass."""
+    from pict_b200.adjoint import rollout
+    pd, st, adj = _setup("twoblock2d_rotated")
+    g = torch.Generator(device="cpu").manual_seed(7)
+    u0 = adj.velocity().clone()
+    w = torch.randn(u0.numel(), generator=g, dtype=torch.float64).cuda()
+    u0a = u0.clone().requires_grad_(True)
+    (w * rollout(adj, u0a, 5, [5], checkpoint_every=2)[0]).sum().backward()
+    u0b = u0.clone().requires_grad_(True)
+    out_b = rollout(adj, u0b, 5, [5], checkpoint_every=2)[0]
+    rollout(adj, (0.5 * u0).requires_grad_(True), 3, [3], checkpoint_every=2)  # reuses the tapes
+    (w * out_b).sum().backward()
+    assert torch.allclose(u0b.grad, u0a.grad, rtol=1e-8, atol=1e-12 * float(u0a.grad.abs().max()))
+    assert torch.equal(adj.velocity(), out_b.detach())
+
+
+def test_graphed_rollout_equals_eager():
+    """With use_graph the backward pass replays per-slot CUDA graphs of the taped step and of the adjoint
+    step: its gradients equal the eager pass's, also on a second pass through the same graphs, with a last
+    checkpoint window shorter than the others and losses at two steps."""
+    from pict_b200.adjoint import rollout
+    pd, st, adj = _setup("twoblock2d_rotated")
+    adj.check_solves = False
+    st.capture(steps=1)
+    g = torch.Generator(device="cpu").manual_seed(5)
+    u0 = adj.velocity().clone()
+    nu0 = pd._sim_visc.clone()
+    ws = [torch.randn(u0.numel(), generator=g, dtype=torch.float64).cuda() for _ in range(2)]
+    res = []
+    for graphed in (False, True, True):
+        adj.use_graph = graphed
+        u0r = u0.clone().requires_grad_(True)
+        nur = nu0.clone().requires_grad_(True)
+        outs = rollout(adj, u0r, 7, [4, 7], checkpoint_every=3, nu=nur)
+        sum((w * o).sum() for w, o in zip(ws, outs)).backward()
+        res.append((u0r.grad.clone(), nur.grad.clone()))
+        pd._sim_visc.copy_(nu0)
+    for gu, gn in res[1:]:
+        assert torch.allclose(gu, res[0][0], rtol=1e-8, atol=1e-12 * float(res[0][0].abs().max()))
+        assert torch.allclose(gn, res[0][1], rtol=1e-8)
+    assert len(adj._taped_graphs) == 3 and len(adj._back_graphs) == 3
+
+
 def test_fp32_gradient_close_to_fp64():
     from pict_b200.adjoint import rollout
     res = []
