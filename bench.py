@@ -960,35 +960,60 @@ def roofline_pass(st, batch, args, dev):
     return top
 
 
-def e2e_pass(st, batch, args, dev, cells, world):
+def e2e_pass(st, batch, args, dev, cells, world, chunks=4):
+    """The step with the batch state crossing the host every step: each step's result (all blocks' velocity
+    and pressure) is read back into pinned host buffers, and the next step's input is uploaded from them.
+    The state moves in `chunks` slices per field: the upload of a slice for the next step starts as soon as
+    its download is done, on a second stream, so uploads overlap the remaining downloads (PCIe is full
+    duplex); the step waits for every upload."""
     import torch
     # the batch state (all blocks' velocity and pressure) lives in two contiguous device tensors
-    # (BatchDomain.pack_state), so each direction is two copies per step
+    # (BatchDomain.pack_state), so each direction is `chunks` copies per field per step
     dev_state = [batch.velocity_arena, batch.pressure_arena]
     host_state = [torch.empty(t.shape, dtype=t.dtype, pin_memory=True) for t in dev_state]
     for h, t in zip(host_state, dev_state):
         h.copy_(t)
     torch.cuda.synchronize()
     h2d = sum(h.numel() * h.element_size() for h in host_state)
+    pieces = []
+    for h, t in zip(host_state, dev_state):
+        hv, tv = h.view(-1), t.view(-1)
+        n = tv.numel()
+        for a in range(chunks):
+            sl = slice(a * n // chunks, (a + 1) * n // chunks)
+            pieces.append((hv[sl], tv[sl]))
+    main = torch.cuda.current_stream()
+    up = torch.cuda.Stream()
     steps = max(1, min(args.steps, 20))
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record()
-    for _ in range(steps):
-        for h, t in zip(host_state, dev_state):
-            t.copy_(h, non_blocking=True)
+    for h, t in pieces:
+        t.copy_(h, non_blocking=True)
+    for k in range(steps):
         if args.no_graph:
             st.step()
         else:
             st.replay()
-        for h, t in zip(host_state, dev_state):
+        downs = []
+        for h, t in pieces:
             h.copy_(t, non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(main)
+            downs.append(ev)
+        if k + 1 < steps:
+            with torch.cuda.stream(up):
+                for (h, t), ev in zip(pieces, downs):
+                    up.wait_event(ev)
+                    t.copy_(h, non_blocking=True)
+            main.wait_stream(up)
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     total_cells, ms_max = job_totals(cells, ms, world, dev)
     return {"value": total_cells * steps / (ms_max * 1e-3), "unit": "cell-steps/s", "h2d_bytes_per_step": h2d,
-            "d2h_bytes_per_step": h2d, "steps": steps}
+            "d2h_bytes_per_step": h2d, "steps": steps,
+            "copies": "%d slices per field and direction; uploads on a second stream overlap the downloads" % chunks}
 
 
 def fp32_pass(batch, wl, args, dev, cells, world):
@@ -1026,44 +1051,79 @@ def fp32_pass(batch, wl, args, dev, cells, world):
     return out
 
 
+def adjoint_pressure_tol(batch, st):
+    """Relative tolerance of the transposed pressure solves of the timed forward+backward: the forward
+    pressure tolerance, but not below 1e-5 in FP32, where the multigrid-preconditioned CG on FP32 vectors
+    levels off between 1e-6 and 6e-6 on the largest cavities (and plain CG between 1e-6 and 9e-5)."""
+    import torch
+    return max(st.p_tol, 1e-5) if batch.getDtype() == torch.float32 else st.p_tol
+
+
 def fwd_bwd_pass(st, batch, args, dev, cells, world):
     """Forward + backward of a checkpointed rollout: loss = mean over simulations of the final mean
-    kinetic energy, gradient with respect to the initial velocity and every simulation's viscosity."""
+    kinetic energy, gradient with respect to the initial velocity and every simulation's viscosity.
+
+    Timed with the transposed solves relative to their right-hand sides (advection to the forward tolerance,
+    pressure to adjoint_pressure_tol; the configuration whose gradient error err.viscosity_grad_timed_precision
+    reports), and again with the
+    reference's backward semantics (the same tolerances as absolute RMS residuals: for a loss this small
+    the adjoint solves then stop almost at once, so that number is faster and less accurate)."""
     import torch
+    from pict_b200 import PISOtorch as P
     from pict_b200.adjoint import PISOAdjoint, rollout
-    adj = PISOAdjoint(st)
-    adj.use_graph = not args.no_graph
     R, K = args.fb_steps, args.checkpoint
     D = batch.getSpatialDims()
     n_s = torch.diff(batch._sim_cells.long()).to(dev)
     ns = n_s.numel()
     w = torch.repeat_interleave(1.0 / (ns * n_s.to(batch.getDtype())), n_s).repeat(D)
-    u0 = adj.velocity().clone()
+    rel = PISOAdjoint(st, relative_tolerance=True, adjoint_pressure_tol=adjoint_pressure_tol(batch, st))
+    u0 = rel.velocity().clone()
     nu0 = batch._sim_visc.clone()
 
-    def run():
-        u0r = u0.clone().requires_grad_(True)
-        nur = nu0.clone().requires_grad_(True)
-        out = rollout(adj, u0r, R, [R], checkpoint_every=K, nu=nur)
-        loss = 0.5 * (w * out[0] * out[0]).sum()
-        loss.backward()
-        return nur.grad
+    def timed(adj):
+        adj.use_graph = not args.no_graph
 
-    run()
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record()
-    g = run()
-    e1.record()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    adj.set_velocity(u0)
-    batch._sim_visc.copy_(nu0)
-    total_cells, ms_max = job_totals(cells, ms, world, dev)
+        def run():
+            u0r = u0.clone().requires_grad_(True)
+            nur = nu0.clone().requires_grad_(True)
+            out = rollout(adj, u0r, R, [R], checkpoint_every=K, nu=nur)
+            loss = 0.5 * (w * out[0] * out[0]).sum()
+            loss.backward()
+            return nur.grad
+
+        run()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        g = run()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        infos = P.decode_infos(adj.info)
+        adv, pr = infos[:D * ns], infos[D * ns:]
+        adj.set_velocity(u0)
+        batch._sim_visc.copy_(nu0)
+        total_cells, ms_max = job_totals(cells, ms, world, dev)
+        return ms_max, total_cells, bool(torch.isfinite(g).all()), {
+            "advection_max": int(max(i.usedIterations for i in adv)),
+            "advection_mean": float(np.mean([i.usedIterations for i in adv])),
+            "pressure_max": int(max(i.usedIterations for i in pr)),
+            "pressure_mean": float(np.mean([i.usedIterations for i in pr]))}
+
+    ms_max, total_cells, finite, its = timed(rel)
+    ms_abs, _, _, its_abs = timed(PISOAdjoint(st))
     return {"value": total_cells * R / (ms_max * 1e-3), "unit": "cell-steps/s", "steps": R, "checkpoint_every": K,
             "ms": ms_max, "loss": "mean over simulations of the final mean kinetic energy",
-            "grad": "initial velocity and per-simulation viscosity", "grad_finite": bool(torch.isfinite(g).all())}
+            "adjoint_solves": "relative to their right-hand sides: advection to the forward tolerance %g, pressure "
+                              "to %g by %s" % (rel.adv_params.tolerance, rel.p_tol, "multigrid-preconditioned CG"
+                                               if rel.p_mg else "persistent CG"),
+            "adjoint_iterations_last_step": its,
+            "grad": "initial velocity and per-simulation viscosity", "grad_finite": finite,
+            "absolute_adjoint_tolerances": {
+                "value": total_cells * R / (ms_abs * 1e-3), "unit": "cell-steps/s", "ms": ms_abs,
+                "adjoint_iterations_last_step": its_abs,
+                "note": "the reference's backward semantics: the same tolerances as absolute RMS residuals"}}
 
 
 def plain_pass(wl, args, k=8, steps=10, fb_steps=10, checkpoint=5):
@@ -1322,8 +1382,9 @@ def grad_check_mixed(wl, args, steps=3, eps=1e-4):
     b32 = batch(torch.float32)
     st32 = PISOStepper(b32, time_step=float(wl["dts"][order[0]]), advection_tol=wl["tol"], pressure_tol=wl["tol"],
                        **precision_kwargs(args, wl))
-    # transposed solves to 1e-6 relative to their right-hand side (the loss gradient is ~1e-3 per cell)
-    adj = PISOAdjoint(st32, relative_tolerance=True)
+    # transposed solves relative to their right-hand side (the loss gradient is ~1e-3 per cell), the
+    # pressure ones to the tolerance the timed forward+backward uses
+    adj = PISOAdjoint(st32, relative_tolerance=True, adjoint_pressure_tol=adjoint_pressure_tol(b32, st32))
     n_s = torch.diff(b32._sim_cells.long()).cuda()
     w32 = torch.repeat_interleave(1.0 / n_s.float(), n_s).repeat(2)
     nu32 = b32._sim_visc.clone().requires_grad_(True)

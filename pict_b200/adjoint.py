@@ -9,7 +9,7 @@ operators of ``libpict_b200`` (adjoint.cu) plus two transposed Krylov solves:
     per corrector k = K-1 .. 0:
         CorrectVelocity^T      -> h_bar, A_bar, p_bar
         mean removal^T         -> p_bar - mean(p_bar)
-        CG on P^T lambda = p_bar
+        CG on P^T lambda = p_bar (P is symmetric: multigrid-preconditioned on the stepper's hierarchy)
         divergence^T, H/A^T, P(A)^T (with -lambda x^T)  -> A_bar, C_bar, U_bar, parameter gradients
     BiCGStab on C^T rhs_bar = u*_bar (all components in one launch)
     advection^T (with -rhs_bar u*^T)   -> gradient of the step's input velocity and parameters
@@ -61,11 +61,14 @@ class PISOAdjoint:
     ``use_graph = True`` the untaped forward steps of :func:`rollout` replay the stepper's captured
     one-step CUDA graph, and its backward pass replays CUDA graphs of the taped step into each slot of
     the checkpoint window and of the adjoint step from it, captured on first use (like the stepper's
-    graph they hold the time step and the tolerances of their capture).
+    graph they hold the time step and the tolerances of their capture).  ``adjoint_pressure_solver``:
+    the transposed pressure solves run as multigrid-preconditioned CG on the stepper's hierarchy where it
+    has one ("auto", the default, or "mg"), or as the persistent CG ("cg").
     """
 
     def __init__(self, stepper: PISOStepper, adjoint_advection_tol: Optional[float] = None,
-                 adjoint_pressure_tol: Optional[float] = None, relative_tolerance: bool = False):
+                 adjoint_pressure_tol: Optional[float] = None, relative_tolerance: bool = False,
+                 adjoint_pressure_solver: str = "auto", adjoint_mg_iterations: int = 24):
         self.st = stepper
         # relative_tolerance: every transposed solve first scales its right-hand side to unit RMS per
         # system (on the device) and scales the solution back, so that the (absolute, RMS) tolerance acts
@@ -92,6 +95,16 @@ class PISOAdjoint:
                                           True, x_zero=True, group_size=ap.group_size)
         self.p_params = P._solve_params(1, stepper.max_iterations, ptol, _lib.PICT_CONV_NORM2_NORMALIZED, False, True,
                                         x_zero=True, group_size=pp.group_size, variant=pp.variant)
+        # adjoint pressure solves: the pressure matrix is symmetric, so the transposed solve is the forward
+        # operator and the stepper's multigrid hierarchy preconditions it ("auto": where the stepper has one,
+        # "mg": required, "cg": the persistent CG); each system stops at the same RMS criterion, within
+        # adjoint_mg_iterations iterations (under graph capture only the iterations still needed run)
+        P._check(adjoint_pressure_solver in ("auto", "mg", "cg"), "adjoint_pressure_solver: auto, mg or cg")
+        P._check(adjoint_pressure_solver != "mg" or stepper._mg is not None,
+                 "adjoint_pressure_solver='mg' needs a stepper with a multigrid hierarchy (refine_solver='auto'/'mg')")
+        self.p_mg = stepper._mg is not None and adjoint_pressure_solver != "cg"
+        self.p_tol = ptol
+        self.p_mg_iterations = int(adjoint_mg_iterations)
         N, D, K = self.N, self.D, self.K
         z = lambda n: torch.zeros(n, dtype=self.dtype, device=self.dev)
         # per-step work
@@ -247,6 +260,8 @@ class PISOAdjoint:
         self.Cbar.zero_()
         self.unbar.zero_()
         check(lib.pict_setup_pressure_matrix(desc, 0, s), "adjoint pressure matrix")
+        if self.p_mg:
+            st._mg.setup(self.Pwork, s)  # coarse operators of this step's pressure matrix
         ucur = ubar.contiguous()
         info_p = self.info[self.D * self.ns * _lib.SOLVE_INFO_BYTES:]
         info_a = self.info[:self.D * self.ns * _lib.SOLVE_INFO_BYTES]
@@ -261,8 +276,11 @@ class PISOAdjoint:
             if self.relative:
                 scale = self._rms_scale(self.pbar, 1)
                 self.pbar.div_(scale)
-            check(lib.pict_solve(desc, _p(self.Pwork), _p(self.pbar), _p(self.lam), ctypes.byref(self.p_params),
-                                 _p(info_p), P._ptr(st.ws), st.ws_bytes, s), "adjoint pressure solve")
+            if self.p_mg:
+                st._mg.solve(dsc, self.pbar, self.lam, self.p_mg_iterations, self.p_tol, info_p, st._mg_ws, s)
+            else:
+                check(lib.pict_solve(desc, _p(self.Pwork), _p(self.pbar), _p(self.lam), ctypes.byref(self.p_params),
+                                     _p(info_p), P._ptr(st.ws), st.ws_bytes, s), "adjoint pressure solve")
             if self.relative:
                 self.lam.mul_(scale)
             self._check_info(info_p, "adjoint pressure")
