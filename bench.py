@@ -1053,10 +1053,13 @@ def fp32_pass(batch, wl, args, dev, cells, world):
 
 def adjoint_pressure_tol(batch, st):
     """Relative tolerance of the transposed pressure solves of the timed forward+backward: the forward
-    pressure tolerance, but not below 1e-5 in FP32, where the multigrid-preconditioned CG on FP32 vectors
-    levels off between 1e-6 and 6e-6 on the largest cavities (and plain CG between 1e-6 and 9e-5)."""
+    pressure tolerance.  Where the stepper has no multigrid hierarchy the adjoint solve is the plain FP32 CG,
+    which levels off between 1e-6 and 9e-5 on the largest cavities, so it stops at 1e-5 in FP32 there; the
+    multigrid solve is refined in FP64 and reaches the forward tolerance."""
     import torch
-    return max(st.p_tol, 1e-5) if batch.getDtype() == torch.float32 else st.p_tol
+    if st._mg is None and batch.getDtype() == torch.float32:
+        return max(st.p_tol, 1e-5)
+    return st.p_tol
 
 
 def fwd_bwd_pass(st, batch, args, dev, cells, world):

@@ -9,7 +9,8 @@ operators of ``libpict_b200`` (adjoint.cu) plus two transposed Krylov solves:
     per corrector k = K-1 .. 0:
         CorrectVelocity^T      -> h_bar, A_bar, p_bar
         mean removal^T         -> p_bar - mean(p_bar)
-        CG on P^T lambda = p_bar (P is symmetric: multigrid-preconditioned on the stepper's hierarchy)
+        CG on P^T lambda = p_bar (P is symmetric: multigrid-preconditioned on the stepper's hierarchy,
+            from the previous adjoint step's lambda with one FP64 refinement sweep)
         divergence^T, H/A^T, P(A)^T (with -lambda x^T)  -> A_bar, C_bar, U_bar, parameter gradients
     BiCGStab on C^T rhs_bar = u*_bar (all components in one launch)
     advection^T (with -rhs_bar u*^T)   -> gradient of the step's input velocity and parameters
@@ -92,7 +93,7 @@ class PISOAdjoint:
         ptol = stepper.p_tol if adjoint_pressure_tol is None else float(adjoint_pressure_tol)
         ap, pp = stepper.adv_params, stepper.p_params
         self.adv_params = P._solve_params(self.D, stepper.max_iterations, atol, _lib.PICT_CONV_NORM2_NORMALIZED, True,
-                                          True, x_zero=True, group_size=ap.group_size)
+                                          True, x_zero=False, group_size=ap.group_size)
         self.p_params = P._solve_params(1, stepper.max_iterations, ptol, _lib.PICT_CONV_NORM2_NORMALIZED, False, True,
                                         x_zero=True, group_size=pp.group_size, variant=pp.variant)
         # adjoint pressure solves: the pressure matrix is symmetric, so the transposed solve is the forward
@@ -118,6 +119,16 @@ class PISOAdjoint:
         self.info = torch.zeros((D + 1) * self.ns * _lib.SOLVE_INFO_BYTES, dtype=torch.uint8, device=self.dev)
         self.block_scratch = torch.zeros(max(1, len(d.getBlocks())), dtype=torch.float64, device=self.dev)
         self.sim_nu_bar = z(self.ns)
+        # warm starts of the transposed solves: the solutions of the previous adjoint step (the next time
+        # step), which the adjoint variables follow smoothly; zero at the start of every backward pass
+        self._rhs_prev = z(D * N)
+        self._lam_prev = [z(N) for _ in range(self.nc)]
+        if self.p_mg:
+            # the multigrid pressure solve from the warm start: one FP64 refinement sweep (FP64 residual,
+            # FP32 correction solve, FP64 accumulation), so the residual can fall below the FP32 level
+            self._lam64 = torch.zeros(N, dtype=torch.float64, device=self.dev)
+            self._pres, self._pcorr = z(N), z(N)
+            self._tile_scratch = torch.zeros(max(1, int(stepper.desc.num_tiles)), dtype=torch.float64, device=self.dev)
         sc = d._sim_cells.long().to(self.dev)
         self._sim_start, self._sim_end = sc[:-1], sc[1:]
         self._sim_n = (sc[1:] - sc[:-1]).double()
@@ -168,6 +179,12 @@ class PISOAdjoint:
         src = src.contiguous()
         check(self.lib.pict_copy_field(ctypes.byref(self.st.domain._desc), FIELD_SOURCE, 1, _p(src), 0,
                                        self._stream()), "set source")
+
+    def reset_warm_starts(self):
+        """Start the transposed solves of the next adjoint step from zero (the first step of a backward pass)."""
+        self._rhs_prev.zero_()
+        for v in self._lam_prev:
+            v.zero_()
 
     def zero_parameter_grads(self):
         self.nubar.zero_()
@@ -272,17 +289,26 @@ class PISOAdjoint:
             if k == self.nc - 1 and pbar_out is not None:
                 self.pbar.add_(pbar_out)
             check(lib.pict_sim_mean_project(desc, _p(self.pbar), s), "mean projection")
-            self.lam.zero_()
             if self.relative:
                 scale = self._rms_scale(self.pbar, 1)
                 self.pbar.div_(scale)
             if self.p_mg:
-                st._mg.solve(dsc, self.pbar, self.lam, self.p_mg_iterations, self.p_tol, info_p, st._mg_ws, s)
+                guess = self._lam_prev[k] / scale if self.relative else self._lam_prev[k]
+                x64 = ctypes.c_void_p(self._lam64.data_ptr())
+                scratch = ctypes.c_void_p(self._tile_scratch.data_ptr())
+                check(lib.pict_refine_residual(desc, _p(self.Pwork), _p(self.pbar), _p(guess), x64, _p(self._pres), 1,
+                                               scratch, s), "adjoint pressure residual")
+                st._mg.solve(dsc, self._pres, self._pcorr, self.p_mg_iterations, self.p_tol, info_p, st._mg_ws, s)
+                check(lib.pict_refine_update(desc, x64, _p(self._pcorr), s), "adjoint pressure update")
+                check(lib.pict_refine_finish(desc, x64, _p(self.lam), 1, 0, scratch, s), "adjoint pressure finish")
             else:
+                self.lam.zero_()
                 check(lib.pict_solve(desc, _p(self.Pwork), _p(self.pbar), _p(self.lam), ctypes.byref(self.p_params),
                                      _p(info_p), P._ptr(st.ws), st.ws_bytes, s), "adjoint pressure solve")
             if self.relative:
                 self.lam.mul_(scale)
+            if self.p_mg:
+                self._lam_prev[k].copy_(self.lam)
             self._check_info(info_p, "adjoint pressure")
             check(lib.pict_divergence_grad(desc, _p(self.lam), _p(self.hbar), _p(self.vbbar), s), "divergence grad")
             U = tape.ustar if k == 0 else tape.U[k]
@@ -292,14 +318,17 @@ class PISOAdjoint:
                   "pressure rhs grad")
             ucur = self.Ubar.clone() if k > 0 else self.Ubar
         # advection solve (transposed, all components) and assembly
-        self.rhsbar.zero_()
         if self.relative:
             scale = self._rms_scale(self.Ubar, self.D)
             self.Ubar.div_(scale)
+            torch.div(self._rhs_prev, scale, out=self.rhsbar)
+        else:
+            self.rhsbar.copy_(self._rhs_prev)
         check(lib.pict_solve(desc, _p(tape.C), _p(self.Ubar), _p(self.rhsbar), ctypes.byref(self.adv_params),
                              _p(info_a), P._ptr(st.ws), st.ws_bytes, s), "adjoint advection solve")
         if self.relative:
             self.rhsbar.mul_(scale)
+        self._rhs_prev.copy_(self.rhsbar)
         self._check_info(info_a, "adjoint advection")
         check(lib.pict_advection_grad(desc, dt, _p(tape.ustar), _p(self.rhsbar), _p(self.Cbar), _p(self.Abar),
                                       _p(self.unbar), _p(self.nubar), _p(self.vbbar), src, s), "advection grad")
@@ -392,6 +421,7 @@ class _Rollout(torch.autograd.Function):
         steps, K, rec = ctx.steps, ctx.K, ctx.rec
         gmap = {t: g for t, g in zip(rec, grads)}
         adj.zero_parameter_grads()
+        adj.reset_warm_starts()
         ubar = torch.zeros(adj.D * adj.N, dtype=adj.dtype, device=adj.dev)
         tapes = adj.tapes(min(K, steps))
         # graphed: the taped and adjoint steps replay per-slot CUDA graphs (the solves' reports are then
