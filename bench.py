@@ -960,7 +960,7 @@ def roofline_pass(st, batch, args, dev):
     return top
 
 
-def e2e_pass(st, batch, args, dev, cells, world, chunks=4):
+def e2e_pass(st, batch, args, dev, cells, world, chunks=8):
     """The step with the batch state crossing the host every step: each step's result (all blocks' velocity
     and pressure) is read back into pinned host buffers, and the next step's input is uploaded from them.
     The state moves in `chunks` slices per field: the upload of a slice for the next step starts as soon as
